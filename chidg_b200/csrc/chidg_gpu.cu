@@ -1,0 +1,1097 @@
+// chidg_gpu.cu -- host side of the B200-native ChiDG linear-solve path:
+// C ABI objects (context, chidg_matrix, chidg_vector, preconditioners) and the
+// programme builders that turn the reference's block-ILU0 / RAS+ILU0 loops into
+// level-scheduled GPU sweeps.  The FGMRES driver lives in fgmres.cu.
+#include "chidg_gpu_internal.cuh"
+
+#include <algorithm>
+#include <chrono>
+#include <climits>
+#include <cstdio>
+#include <cstring>
+#include <map>
+
+using namespace chidg;
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+int chidg::fail(chidg_gpu_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
+int chidg::cuda_fail(chidg_gpu_ctx* ctx, cudaError_t e, const char* what) {
+    return fail(ctx, CHIDG_GPU_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+int chidg::check_launch(chidg_gpu_ctx* ctx, const char* what) {
+    ctx->launches++;
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(ctx, e, what);
+    return CHIDG_GPU_OK;
+}
+int chidg::ensure(chidg_gpu_ctx* ctx, Buffer& buf, size_t bytes) {
+    if (buf.bytes >= bytes && buf.ptr) return CHIDG_GPU_OK;
+    if (buf.ptr) { cudaFree(buf.ptr); buf.ptr = nullptr; buf.bytes = 0; }
+    if (bytes == 0) return CHIDG_GPU_OK;
+    const cudaError_t e = cudaMalloc(&buf.ptr, bytes);
+    if (e != cudaSuccess) { cudaGetLastError(); return fail(ctx, CHIDG_GPU_ENOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed"); }
+    buf.bytes = bytes;
+    return CHIDG_GPU_OK;
+}
+void chidg::release(Buffer& buf) {
+    if (buf.ptr) cudaFree(buf.ptr);
+    buf.ptr = nullptr;
+    buf.bytes = 0;
+}
+int chidg::grid_for(int64_t n, int threads, int cap) {
+    int64_t g = (n + threads - 1) / threads;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return (int)g;
+}
+
+// Two-pass reductions into ctx->d_scal[slot..slot+nq).
+int chidg::reduce_partials(chidg_gpu_ctx* ctx, const double* partial, int ncta, int nq, int slot, bool do_sqrt) {
+    k_reduce_partials<<<1, 1024, 0, ctx->stream>>>(partial, ncta, nq, ctx->d_scal + slot, do_sqrt ? 1 : 0);
+    return check_launch(ctx, "k_reduce_partials");
+}
+int chidg::fetch_scalars(chidg_gpu_ctx* ctx, int slot, int count, double* out) {
+    cudaError_t e = cudaMemcpyAsync(ctx->h_scal + slot, ctx->d_scal + slot, sizeof(double) * count, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "scalar download");
+    e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "stream synchronize");
+    std::memcpy(out, ctx->h_scal + slot, sizeof(double) * count);
+    return CHIDG_GPU_OK;
+}
+int chidg::push_scalars(chidg_gpu_ctx* ctx, int slot, int count, const double* in) {
+    // The pinned staging slots are private to this call: wait for earlier
+    // copies out of the same slots before overwriting them.
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "stream synchronize");
+    std::memcpy(ctx->h_scal + slot, in, sizeof(double) * count);
+    e = cudaMemcpyAsync(ctx->d_scal + slot, ctx->h_scal + slot, sizeof(double) * count, cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "scalar upload");
+    return CHIDG_GPU_OK;
+}
+
+// dot products of x with nq vectors y + q*ystride, results in d_scal[slot+q]
+template <typename T>
+int chidg::mdot(chidg_gpu_ctx* ctx, int64_t n, const T* x, const T* y, int64_t ystride, int nq, int slot) {
+    const int threads = 256;
+    const int ncta = grid_for(n, threads, ctx->nsm * 4);
+    int st = ensure(ctx, ctx->partial, sizeof(double) * (size_t)ncta * std::max(nq, 1));
+    if (st) return st;
+    k_mdot_partial<T><<<ncta, threads, 0, ctx->stream>>>(n, x, y, ystride, nq, (double*)ctx->partial.ptr);
+    st = check_launch(ctx, "k_mdot_partial");
+    if (st) return st;
+    return reduce_partials(ctx, (const double*)ctx->partial.ptr, ncta, nq, slot, false);
+}
+template int chidg::mdot<double>(chidg_gpu_ctx*, int64_t, const double*, const double*, int64_t, int, int);
+template int chidg::mdot<float>(chidg_gpu_ctx*, int64_t, const float*, const float*, int64_t, int, int);
+
+extern "C" int chidg_gpu_ctx_create(int device, void* stream, chidg_gpu_ctx** out) {
+    if (!out) return CHIDG_GPU_EINVAL;
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || device < 0 || device >= ndev) { cudaGetLastError(); return CHIDG_GPU_EINVAL; }
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) return CHIDG_GPU_ECUDA;
+    auto* ctx = new chidg_gpu_ctx();
+    ctx->device = device;
+    if (stream) { ctx->stream = (cudaStream_t)stream; ctx->own_stream = false; }
+    else {
+        e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) { delete ctx; return CHIDG_GPU_ECUDA; }
+        ctx->own_stream = true;
+    }
+    cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device);
+    if (cudaMalloc(&ctx->d_status, sizeof(int) * 4) != cudaSuccess ||
+        cudaMalloc(&ctx->d_scal, sizeof(double) * kScalSlots) != cudaSuccess ||
+        cudaMallocHost(&ctx->h_scal, sizeof(double) * kScalSlots) != cudaSuccess ||
+        cudaMallocHost(&ctx->h_status, sizeof(int) * 4) != cudaSuccess) {
+        cudaGetLastError();
+        chidg_gpu_ctx_destroy(ctx);
+        return CHIDG_GPU_ENOMEM;
+    }
+    *out = ctx;
+    return CHIDG_GPU_OK;
+}
+
+extern "C" int chidg_gpu_ctx_destroy(chidg_gpu_ctx* ctx) {
+    if (!ctx) return CHIDG_GPU_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    release(ctx->partial);
+    release(ctx->partial2);
+    if (ctx->d_status) cudaFree(ctx->d_status);
+    if (ctx->d_scal) cudaFree(ctx->d_scal);
+    if (ctx->h_scal) cudaFreeHost(ctx->h_scal);
+    if (ctx->h_status) cudaFreeHost(ctx->h_status);
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return CHIDG_GPU_OK;
+}
+extern "C" int chidg_gpu_ctx_sync(chidg_gpu_ctx* ctx) {
+    if (!ctx) return CHIDG_GPU_EINVAL;
+    cudaSetDevice(ctx->device);
+    const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    return e == cudaSuccess ? CHIDG_GPU_OK : cuda_fail(ctx, e, "stream synchronize");
+}
+extern "C" int chidg_gpu_last_error(chidg_gpu_ctx* ctx, char* buf, int32_t buflen) {
+    if (!ctx || !buf || buflen <= 0) return CHIDG_GPU_EINVAL;
+    std::snprintf(buf, (size_t)buflen, "%s", ctx->err.c_str());
+    return CHIDG_GPU_OK;
+}
+extern "C" int chidg_gpu_error_element(chidg_gpu_ctx* ctx, int32_t* elem) {
+    if (!ctx || !elem) return CHIDG_GPU_EINVAL;
+    *elem = ctx->err_elem;
+    return CHIDG_GPU_OK;
+}
+extern "C" int chidg_gpu_launch_count(chidg_gpu_ctx* ctx, int64_t* count) {
+    if (!ctx || !count) return CHIDG_GPU_EINVAL;
+    *count = ctx->launches;
+    return CHIDG_GPU_OK;
+}
+extern "C" int chidg_gpu_host_alloc(size_t bytes, void** out) {
+    if (!out) return CHIDG_GPU_EINVAL;
+    const cudaError_t e = cudaMallocHost(out, bytes);
+    if (e != cudaSuccess) { cudaGetLastError(); *out = nullptr; return CHIDG_GPU_ENOMEM; }
+    return CHIDG_GPU_OK;
+}
+extern "C" int chidg_gpu_host_free(void* p) {
+    if (p) cudaFreeHost(p);
+    return CHIDG_GPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// chidg_matrix_t
+// ---------------------------------------------------------------------------
+template <typename T>
+static int upload_array(chidg_gpu_ctx* ctx, Buffer& buf, const std::vector<T>& v) {
+    int st = ensure(ctx, buf, std::max<size_t>(sizeof(T) * v.size(), sizeof(T)));
+    if (st) return st;
+    if (v.empty()) return CHIDG_GPU_OK;
+    const cudaError_t e = cudaMemcpy(buf.ptr, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
+    return e == cudaSuccess ? CHIDG_GPU_OK : cuda_fail(ctx, e, "pattern upload");
+}
+
+static int block_dim_for(int bmax) {
+    // G = floor(512 / b) column groups of b threads, rounded up to whole warps
+    const int G = std::max(1, 512 / std::max(bmax, 1));
+    int t = G * bmax;
+    t = ((t + 31) / 32) * 32;
+    return std::min(std::max(t, 32), 1024);
+}
+
+extern "C" int chidg_gpu_matrix_create(chidg_gpu_ctx* ctx, const chidg_gpu_pattern* pat, chidg_gpu_matrix** out) {
+    if (!ctx || !pat || !out) return CHIDG_GPU_EINVAL;
+    *out = nullptr;
+    cudaSetDevice(ctx->device);
+    if (pat->nelem <= 0 || pat->ntime <= 0 || pat->nblocks <= 0 || !pat->elem_nvars || !pat->elem_nterms ||
+        !pat->blk_row_elem || !pat->blk_row_time || !pat->blk_col_elem || !pat->blk_col_time || !pat->blk_kind)
+        return fail(ctx, CHIDG_GPU_EINVAL, "matrix_create: incomplete pattern");
+    auto* A = new chidg_gpu_matrix();
+    A->ctx = ctx;
+    A->nelem = pat->nelem;
+    A->ntime = pat->ntime;
+    A->nrow = pat->nelem * pat->ntime;
+    A->nvars.assign(pat->elem_nvars, pat->elem_nvars + A->nelem);
+    A->nterms.assign(pat->elem_nterms, pat->elem_nterms + A->nelem);
+    A->proc.assign(A->nelem, 0);
+    if (pat->elem_proc) A->proc.assign(pat->elem_proc, pat->elem_proc + A->nelem);
+    A->eoff.resize(A->nelem);
+    int64_t off = 0;
+    A->max_b = 0;
+    for (int e = 0; e < A->nelem; ++e) {
+        if (A->nvars[e] <= 0 || A->nterms[e] <= 0 || A->proc[e] < 0) { delete A; return fail(ctx, CHIDG_GPU_EINVAL, "matrix_create: bad element sizes"); }
+        A->eoff[e] = off;
+        off += (int64_t)A->ntime * A->bsize(e);
+        A->max_b = std::max(A->max_b, A->bsize(e));
+    }
+    if (A->max_b > 1024) { delete A; return fail(ctx, CHIDG_GPU_EINVAL, "matrix_create: block size above 1024"); }
+    A->n = off;
+    const int64_t nb = pat->nblocks;
+    A->nblk = nb;
+    A->re.assign(pat->blk_row_elem, pat->blk_row_elem + nb);
+    A->rt.assign(pat->blk_row_time, pat->blk_row_time + nb);
+    A->ce.assign(pat->blk_col_elem, pat->blk_col_elem + nb);
+    A->ct.assign(pat->blk_col_time, pat->blk_col_time + nb);
+    A->kind.assign(pat->blk_kind, pat->blk_kind + nb);
+    A->voff.resize(nb);
+    int64_t v = 0;
+    for (int64_t k = 0; k < nb; ++k) {
+        if (A->re[k] < 0 || A->re[k] >= A->nelem || A->ce[k] < 0 || A->ce[k] >= A->nelem ||
+            A->rt[k] < 0 || A->rt[k] >= A->ntime || A->ct[k] < 0 || A->ct[k] >= A->ntime ||
+            A->kind[k] < 0 || A->kind[k] > 3) { delete A; return fail(ctx, CHIDG_GPU_EINVAL, "matrix_create: block index out of range"); }
+        if (A->kind[k] == CHIDG_BLK_LOCAL && A->ct[k] != A->rt[k]) { delete A; return fail(ctx, CHIDG_GPU_EINVAL, "matrix_create: LOCAL block across time levels"); }
+        A->voff[k] = v;
+        v += (int64_t)A->bsize(A->re[k]) * A->bsize(A->ce[k]);
+    }
+    A->nval = v;
+    A->rowblk.assign(A->nrow, {});
+    A->lblk.assign(A->nrow, {});
+    A->diag.assign(A->nrow, -1);
+    for (int kd = 0; kd < 4; ++kd)
+        for (int64_t k = 0; k < nb; ++k) {
+            if (A->kind[k] != kd) continue;
+            const int r = A->row(A->re[k], A->rt[k]);
+            A->rowblk[r].push_back((int32_t)k);
+            if (kd == CHIDG_BLK_LOCAL) {
+                A->lblk[r].push_back((int32_t)k);
+                if (A->ce[k] == A->re[k]) {
+                    if (A->diag[r] >= 0) { delete A; return fail(ctx, CHIDG_GPU_EINVAL, "matrix_create: two DIAG blocks in a row"); }
+                    A->diag[r] = (int32_t)k;
+                }
+            }
+        }
+    for (int r = 0; r < A->nrow; ++r)
+        if (A->diag[r] < 0) { delete A; return fail(ctx, CHIDG_GPU_EINVAL, "matrix_create: row without DIAG block"); }
+    // CSR in row order for the matvec
+    std::vector<int64_t> row_ptr(A->nrow + 1), bvoff, bxoff, yoff(A->nrow), dvoff(A->nrow);
+    std::vector<int32_t> bnc, rb(A->nrow);
+    A->max_row_cols = 0;
+    int64_t cur = 0;
+    for (int r = 0; r < A->nrow; ++r) {
+        const int e = r / A->ntime, t = r % A->ntime;
+        row_ptr[r] = cur;
+        int cols = 0;
+        for (int32_t k : A->rowblk[r]) {
+            bvoff.push_back(A->voff[k]);
+            bxoff.push_back(A->seg(A->ce[k], A->ct[k]));
+            bnc.push_back(A->bsize(A->ce[k]));
+            cols += A->bsize(A->ce[k]);
+            ++cur;
+        }
+        A->max_row_cols = std::max(A->max_row_cols, cols);
+        yoff[r] = A->seg(e, t);
+        rb[r] = A->bsize(e);
+        dvoff[r] = A->voff[A->diag[r]];
+    }
+    row_ptr[A->nrow] = cur;
+    int st;
+    if ((st = upload_array(ctx, A->d_row_ptr, row_ptr)) || (st = upload_array(ctx, A->d_blk_voff, bvoff)) ||
+        (st = upload_array(ctx, A->d_blk_xoff, bxoff)) || (st = upload_array(ctx, A->d_blk_nc, bnc)) ||
+        (st = upload_array(ctx, A->d_row_yoff, yoff)) || (st = upload_array(ctx, A->d_row_b, rb)) ||
+        (st = upload_array(ctx, A->d_diag_voff, dvoff)) ||
+        (st = upload_array(ctx, A->d_elem_nvars, A->nvars)) || (st = upload_array(ctx, A->d_elem_nterms, A->nterms))) {
+        chidg_gpu_matrix_destroy(A);
+        return st;
+    }
+    if ((st = ensure(ctx, A->val, sizeof(double) * (size_t)A->nval))) { chidg_gpu_matrix_destroy(A); return st; }
+    cudaMemsetAsync(A->val.ptr, 0, sizeof(double) * (size_t)A->nval, ctx->stream);
+    A->mv_threads = block_dim_for(A->max_b);
+    A->stamp = 1;
+    *out = A;
+    return CHIDG_GPU_OK;
+}
+
+extern "C" int chidg_gpu_matrix_destroy(chidg_gpu_matrix* A) {
+    if (!A) return CHIDG_GPU_OK;
+    cudaSetDevice(A->ctx->device);
+    cudaStreamSynchronize(A->ctx->stream);
+    for (Buffer* b : {&A->val, &A->val32, &A->val16, &A->d_row_ptr, &A->d_blk_voff, &A->d_blk_xoff, &A->d_blk_nc,
+                      &A->d_row_yoff, &A->d_row_b, &A->d_diag_voff, &A->d_elem_nvars, &A->d_elem_nterms, &A->row_sq})
+        release(*b);
+    delete A;
+    return CHIDG_GPU_OK;
+}
+extern "C" int chidg_gpu_matrix_nvalues(chidg_gpu_matrix* A, int64_t* n) {
+    if (!A || !n) return CHIDG_GPU_EINVAL;
+    *n = A->nval;
+    return CHIDG_GPU_OK;
+}
+extern "C" int chidg_gpu_matrix_nvec(chidg_gpu_matrix* A, int64_t* n) {
+    if (!A || !n) return CHIDG_GPU_EINVAL;
+    *n = A->n;
+    return CHIDG_GPU_OK;
+}
+extern "C" int chidg_gpu_matrix_stamp(chidg_gpu_matrix* A, int64_t* s) {
+    if (!A || !s) return CHIDG_GPU_EINVAL;
+    *s = A->stamp;
+    return CHIDG_GPU_OK;
+}
+extern "C" int chidg_gpu_matrix_upload(chidg_gpu_matrix* A, const double* host) {
+    if (!A || !host) return CHIDG_GPU_EINVAL;
+    chidg_gpu_ctx* ctx = A->ctx;
+    cudaSetDevice(ctx->device);
+    const cudaError_t e = cudaMemcpyAsync(A->val.ptr, host, sizeof(double) * (size_t)A->nval, cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "matrix upload");
+    A->stamp++;
+    return CHIDG_GPU_OK;
+}
+extern "C" int chidg_gpu_matrix_upload_blocks(chidg_gpu_matrix* A, const double* const* ptrs) {
+    if (!A || !ptrs) return CHIDG_GPU_EINVAL;
+    chidg_gpu_ctx* ctx = A->ctx;
+    cudaSetDevice(ctx->device);
+    double* d = (double*)A->val.ptr;
+    for (int64_t k = 0; k < A->nblk; ++k) {
+        if (!ptrs[k]) return fail(ctx, CHIDG_GPU_EINVAL, "upload_blocks: null block pointer");
+        const size_t bytes = sizeof(double) * (size_t)A->bsize(A->re[k]) * A->bsize(A->ce[k]);
+        const cudaError_t e = cudaMemcpyAsync(d + A->voff[k], ptrs[k], bytes, cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "block upload");
+    }
+    A->stamp++;
+    return CHIDG_GPU_OK;
+}
+extern "C" int chidg_gpu_matrix_upload_device(chidg_gpu_matrix* A, const double* dev) {
+    if (!A || !dev) return CHIDG_GPU_EINVAL;
+    chidg_gpu_ctx* ctx = A->ctx;
+    cudaSetDevice(ctx->device);
+    const cudaError_t e = cudaMemcpyAsync(A->val.ptr, dev, sizeof(double) * (size_t)A->nval, cudaMemcpyDeviceToDevice, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "matrix device copy");
+    A->stamp++;
+    return CHIDG_GPU_OK;
+}
+extern "C" int chidg_gpu_matrix_download(chidg_gpu_matrix* A, double* host) {
+    if (!A || !host) return CHIDG_GPU_EINVAL;
+    chidg_gpu_ctx* ctx = A->ctx;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = cudaMemcpyAsync(host, A->val.ptr, sizeof(double) * (size_t)A->nval, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    return e == cudaSuccess ? CHIDG_GPU_OK : cuda_fail(ctx, e, "matrix download");
+}
+extern "C" int chidg_gpu_matrix_clear(chidg_gpu_matrix* A) {
+    if (!A) return CHIDG_GPU_EINVAL;
+    cudaSetDevice(A->ctx->device);
+    const cudaError_t e = cudaMemsetAsync(A->val.ptr, 0, sizeof(double) * (size_t)A->nval, A->ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(A->ctx, e, "matrix clear");
+    A->stamp++;
+    return CHIDG_GPU_OK;
+}
+extern "C" int chidg_gpu_matrix_scale_diagonal(chidg_gpu_matrix* A, const double* mass, const double* scale) {
+    if (!A || !mass || !scale) return CHIDG_GPU_EINVAL;
+    chidg_gpu_ctx* ctx = A->ctx;
+    cudaSetDevice(ctx->device);
+    std::vector<int64_t> moff(A->nelem), soff(A->nelem);
+    int64_t m = 0, s = 0;
+    for (int e = 0; e < A->nelem; ++e) {
+        moff[e] = m; m += (int64_t)A->nterms[e] * A->nterms[e];
+        soff[e] = s; s += A->nvars[e];
+    }
+    Buffer dm, ds, dmo, dso;
+    int st;
+    if ((st = ensure(ctx, dm, sizeof(double) * m)) || (st = ensure(ctx, ds, sizeof(double) * s)) ||
+        (st = upload_array(ctx, dmo, moff)) || (st = upload_array(ctx, dso, soff))) {
+        release(dm); release(ds); release(dmo); release(dso);
+        return st;
+    }
+    cudaMemcpy(dm.ptr, mass, sizeof(double) * m, cudaMemcpyHostToDevice);
+    cudaMemcpy(ds.ptr, scale, sizeof(double) * s, cudaMemcpyHostToDevice);
+    k_scale_diagonal<<<A->nrow, 256, 0, ctx->stream>>>((double*)A->val.ptr, (const int64_t*)A->d_diag_voff.ptr,
+                                                      (const int32_t*)A->d_elem_nvars.ptr, (const int32_t*)A->d_elem_nterms.ptr,
+                                                      (const int64_t*)dmo.ptr, (const double*)dm.ptr, (const double*)ds.ptr,
+                                                      (const int64_t*)dso.ptr, A->ntime);
+    st = check_launch(ctx, "k_scale_diagonal");
+    cudaStreamSynchronize(ctx->stream);
+    release(dm); release(ds); release(dmo); release(dso);
+    if (st) return st;
+    A->stamp++;
+    return CHIDG_GPU_OK;
+}
+
+// Low-precision copies of A for the mixed-precision inner solves.
+int chidg::matrix_lowp(chidg_gpu_matrix* A, int precision) {
+    chidg_gpu_ctx* ctx = A->ctx;
+    if (precision == CHIDG_GPU_FP64) return CHIDG_GPU_OK;
+    if (A->val32_stamp == A->stamp) return CHIDG_GPU_OK;
+    int st = ensure(ctx, A->val32, sizeof(float) * (size_t)A->nval);
+    if (st) return st;
+    k_convert<double, float><<<grid_for(A->nval, 256, ctx->nsm * 8), 256, 0, ctx->stream>>>(A->nval, (const double*)A->val.ptr, (float*)A->val32.ptr);
+    st = check_launch(ctx, "k_convert A->fp32");
+    if (st) return st;
+    A->val32_stamp = A->stamp;
+    return CHIDG_GPU_OK;
+}
+
+// y = alpha * A x + beta * z, optional per-row sums of squares of y
+template <typename TA, typename TV>
+int chidg::matvec_launch(chidg_gpu_matrix* A, const TA* val, const TV* x, TV* y, const TV* z, double alpha, double beta, double* row_sq) {
+    chidg_gpu_ctx* ctx = A->ctx;
+    using ACC = typename AccOf<TV>::type;
+    const size_t smem = sizeof(ACC) * ((size_t)A->max_row_cols + A->mv_threads) + 64;
+    k_matvec<TA, TV, TV, ACC><<<A->nrow, A->mv_threads, smem, ctx->stream>>>(
+        val, (const int64_t*)A->d_row_ptr.ptr, (const int64_t*)A->d_blk_voff.ptr, (const int64_t*)A->d_blk_xoff.ptr,
+        (const int32_t*)A->d_blk_nc.ptr, (const int64_t*)A->d_row_yoff.ptr, (const int32_t*)A->d_row_b.ptr, x, y, z, alpha, beta, row_sq);
+    return check_launch(ctx, "k_matvec");
+}
+template int chidg::matvec_launch<double, double>(chidg_gpu_matrix*, const double*, const double*, double*, const double*, double, double, double*);
+template int chidg::matvec_launch<float, float>(chidg_gpu_matrix*, const float*, const float*, float*, const float*, double, double, double*);
+
+int chidg::set_matvec_smem(chidg_gpu_matrix* A) {
+    // allow > 48 KB dynamic shared memory when a row has many wide blocks
+    const size_t smem = sizeof(double) * ((size_t)A->max_row_cols + A->mv_threads) + 64;
+    if (smem > 48 * 1024) {
+        cudaFuncSetAttribute(k_matvec<double, double, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_matvec<float, float, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    }
+    return CHIDG_GPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// chidg_vector_t
+// ---------------------------------------------------------------------------
+extern "C" int chidg_gpu_vector_create(chidg_gpu_matrix* A, chidg_gpu_vector** out) {
+    if (!A || !out) return CHIDG_GPU_EINVAL;
+    *out = nullptr;
+    chidg_gpu_ctx* ctx = A->ctx;
+    cudaSetDevice(ctx->device);
+    auto* x = new chidg_gpu_vector();
+    x->A = A;
+    x->ctx = ctx;
+    x->n = A->n;
+    int st = ensure(ctx, x->buf, sizeof(double) * (size_t)x->n);
+    if (st) { delete x; return st; }
+    cudaMemsetAsync(x->buf.ptr, 0, sizeof(double) * (size_t)x->n, ctx->stream);
+    *out = x;
+    return CHIDG_GPU_OK;
+}
+extern "C" int chidg_gpu_vector_destroy(chidg_gpu_vector* x) {
+    if (!x) return CHIDG_GPU_OK;
+    cudaSetDevice(x->ctx->device);
+    cudaStreamSynchronize(x->ctx->stream);
+    release(x->buf);
+    delete x;
+    return CHIDG_GPU_OK;
+}
+extern "C" int chidg_gpu_vector_upload(chidg_gpu_vector* x, const double* host) {
+    if (!x || !host) return CHIDG_GPU_EINVAL;
+    cudaSetDevice(x->ctx->device);
+    const cudaError_t e = cudaMemcpyAsync(x->buf.ptr, host, sizeof(double) * (size_t)x->n, cudaMemcpyHostToDevice, x->ctx->stream);
+    return e == cudaSuccess ? CHIDG_GPU_OK : cuda_fail(x->ctx, e, "vector upload");
+}
+extern "C" int chidg_gpu_vector_download(chidg_gpu_vector* x, double* host) {
+    if (!x || !host) return CHIDG_GPU_EINVAL;
+    cudaSetDevice(x->ctx->device);
+    cudaError_t e = cudaMemcpyAsync(host, x->buf.ptr, sizeof(double) * (size_t)x->n, cudaMemcpyDeviceToHost, x->ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(x->ctx->stream);
+    return e == cudaSuccess ? CHIDG_GPU_OK : cuda_fail(x->ctx, e, "vector download");
+}
+extern "C" int chidg_gpu_vector_upload_device(chidg_gpu_vector* x, const double* dev) {
+    if (!x || !dev) return CHIDG_GPU_EINVAL;
+    cudaSetDevice(x->ctx->device);
+    const cudaError_t e = cudaMemcpyAsync(x->buf.ptr, dev, sizeof(double) * (size_t)x->n, cudaMemcpyDeviceToDevice, x->ctx->stream);
+    return e == cudaSuccess ? CHIDG_GPU_OK : cuda_fail(x->ctx, e, "vector device copy");
+}
+extern "C" int chidg_gpu_vector_device_ptr(chidg_gpu_vector* x, double** dev) {
+    if (!x || !dev) return CHIDG_GPU_EINVAL;
+    *dev = (double*)x->buf.ptr;
+    return CHIDG_GPU_OK;
+}
+extern "C" int chidg_gpu_vector_clear(chidg_gpu_vector* x) {
+    if (!x) return CHIDG_GPU_EINVAL;
+    cudaSetDevice(x->ctx->device);
+    const cudaError_t e = cudaMemsetAsync(x->buf.ptr, 0, sizeof(double) * (size_t)x->n, x->ctx->stream);
+    return e == cudaSuccess ? CHIDG_GPU_OK : cuda_fail(x->ctx, e, "vector clear");
+}
+extern "C" int chidg_gpu_vector_copy(chidg_gpu_vector* dst, const chidg_gpu_vector* src) {
+    if (!dst || !src || dst->n != src->n) return CHIDG_GPU_EINVAL;
+    cudaSetDevice(dst->ctx->device);
+    const cudaError_t e = cudaMemcpyAsync(dst->buf.ptr, src->buf.ptr, sizeof(double) * (size_t)dst->n, cudaMemcpyDeviceToDevice, dst->ctx->stream);
+    return e == cudaSuccess ? CHIDG_GPU_OK : cuda_fail(dst->ctx, e, "vector copy");
+}
+extern "C" int chidg_gpu_vector_axpy(chidg_gpu_vector* y, double a, const chidg_gpu_vector* x) {
+    if (!y || !x || y->n != x->n) return CHIDG_GPU_EINVAL;
+    chidg_gpu_ctx* ctx = y->ctx;
+    cudaSetDevice(ctx->device);
+    k_axpby<double, double><<<grid_for(y->n, 256, ctx->nsm * 8), 256, 0, ctx->stream>>>(y->n, a, nullptr, (const double*)x->buf.ptr, 1.0, (double*)y->buf.ptr);
+    return check_launch(ctx, "k_axpby");
+}
+extern "C" int chidg_gpu_vector_scale(chidg_gpu_vector* x, double a) {
+    if (!x) return CHIDG_GPU_EINVAL;
+    chidg_gpu_ctx* ctx = x->ctx;
+    cudaSetDevice(ctx->device);
+    k_axpby<double, double><<<grid_for(x->n, 256, ctx->nsm * 8), 256, 0, ctx->stream>>>(x->n, a, nullptr, (const double*)x->buf.ptr, 0.0, (double*)x->buf.ptr);
+    return check_launch(ctx, "k_axpby");
+}
+extern "C" int chidg_gpu_vector_dot(const chidg_gpu_vector* x, const chidg_gpu_vector* y, double* out) {
+    if (!x || !y || !out || x->n != y->n) return CHIDG_GPU_EINVAL;
+    chidg_gpu_ctx* ctx = x->ctx;
+    cudaSetDevice(ctx->device);
+    int st = mdot<double>(ctx, x->n, (const double*)x->buf.ptr, (const double*)y->buf.ptr, 0, 1, kSlotTmp);
+    if (st) return st;
+    return fetch_scalars(ctx, kSlotTmp, 1, out);
+}
+extern "C" int chidg_gpu_vector_norm(const chidg_gpu_vector* x, double* out) {
+    if (!x || !out) return CHIDG_GPU_EINVAL;
+    double s;
+    int st = chidg_gpu_vector_dot(x, x, &s);
+    if (st) return st;
+    *out = std::sqrt(s);
+    return CHIDG_GPU_OK;
+}
+extern "C" int chidg_gpu_matvec(chidg_gpu_matrix* A, const chidg_gpu_vector* x, chidg_gpu_vector* y) {
+    if (!A || !x || !y || x->n != A->n || y->n != A->n || x == y) return CHIDG_GPU_EINVAL;
+    cudaSetDevice(A->ctx->device);
+    set_matvec_smem(A);
+    return matvec_launch<double, double>(A, (const double*)A->val.ptr, (const double*)x->buf.ptr, (double*)y->buf.ptr,
+                                         nullptr, 1.0, 0.0, nullptr);
+}
+
+// ---------------------------------------------------------------------------
+// Preconditioner programmes
+// ---------------------------------------------------------------------------
+namespace {
+
+// transposed LOCAL block: first LOCAL block of row (p,t) whose column is e
+// (type_domain_matrix.f90:592-627)
+int find_trans(const chidg_gpu_matrix* A, int p, int t, int e) {
+    for (int32_t kk : A->lblk[A->row(p, t)])
+        if (A->ce[kk] == e) return kk;
+    return -1;
+}
+
+}  // namespace
+
+// ILU0 / Jacobi on a single rank: one programme row per matrix row.
+static int build_ilu0(const chidg_gpu_matrix* A, bool jacobi, IluProgram& P, std::string& err) {
+    P = IluProgram();
+    P.n_ext = A->n;
+    P.nlocal_rows = A->nrow;
+    // programme row id == matrix row id (e*ntime+t)
+    for (int r = 0; r < A->nrow; ++r) {
+        const int e = r / A->ntime, t = r % A->ntime;
+        P.prow_b.push_back(A->bsize(e));
+        P.prow_elem.push_back(e);
+        P.v_off.push_back(A->seg(e, t));
+        P.z_off.push_back(A->seg(e, t));
+        P.diagA_off.push_back(A->voff[A->diag[r]]);
+        P.diag_blk.push_back(A->diag[r]);
+        P.lo.emplace_back();
+        P.up.emplace_back();
+    }
+    if (jacobi) return CHIDG_GPU_OK;
+    for (int r = 0; r < A->nrow; ++r) {
+        const int e = r / A->ntime, t = r % A->ntime;
+        for (int32_t k : A->lblk[r]) {
+            const int p = A->ce[k];
+            if (p < e) {   // type_domain_matrix.f90:295-302, single rank
+                const int kt = find_trans(A, p, t, e);
+                if (kt < 0) { err = "ilu0: no transposed block found"; return CHIDG_GPU_EINVAL; }
+                IluEntry en;
+                en.parent = A->row(p, t);
+                en.a_off = A->voff[k];
+                en.t_off = A->voff[kt];
+                en.nc = A->bsize(p);
+                en.blk = k;
+                P.lo[r].push_back(en);
+            } else if (p > e) {
+                IluEntry en;
+                en.parent = A->row(p, t);
+                en.a_off = A->voff[k];
+                en.nc = A->bsize(p);
+                en.blk = k;
+                P.up[r].push_back(en);
+            }
+        }
+    }
+    return CHIDG_GPU_OK;
+}
+
+// RAS+ILU0: subdomain s plays MPI rank s.  Local rows in local element order,
+// then the overlap rows received from each neighbour rank, as the reference
+// builds them (RASILU0/type_RASILU0_send_comm.f90:66-275 selects the sent
+// blocks, RASILU0/type_RASILU0_recv_dom_comm.f90:59-305 classifies them).
+static int build_rasilu0(const chidg_gpu_matrix* A, IluProgram& P, std::string& err) {
+    P = IluProgram();
+    if (A->ntime != 1) { err = "rasilu0: single time level only"; return CHIDG_GPU_EINVAL; }
+    int nsub = 0;
+    for (int e = 0; e < A->nelem; ++e) nsub = std::max(nsub, A->proc[e] + 1);
+    std::vector<std::vector<int>> elems(nsub);
+    std::vector<int> lidx(A->nelem);
+    for (int e = 0; e < A->nelem; ++e) { lidx[e] = (int)elems[A->proc[e]].size(); elems[A->proc[e]].push_back(e); }
+    // does element f (owned by q) have a face neighbour on rank s?
+    auto touches = [&](int f, int s) {
+        for (int32_t k : A->lblk[A->row(f, 0)])
+            if (A->ce[k] != f && A->proc[A->ce[k]] == s) return true;
+        return false;
+    };
+    int64_t ov_cursor = A->n;
+    P.nlocal_rows = 0;
+    for (int s = 0; s < nsub; ++s) {
+        // local rows
+        std::vector<int> local_prow(elems[s].size());
+        for (size_t i = 0; i < elems[s].size(); ++i) {
+            const int e = elems[s][i];
+            const int pr = (int)P.prow_b.size();
+            local_prow[i] = pr;
+            P.prow_b.push_back(A->bsize(e));
+            P.prow_elem.push_back(e);
+            P.v_off.push_back(A->seg(e, 0));
+            P.z_off.push_back(A->seg(e, 0));
+            P.diagA_off.push_back(A->voff[A->diag[A->row(e, 0)]]);
+            P.diag_blk.push_back(A->diag[A->row(e, 0)]);
+            P.lo.emplace_back();
+            P.up.emplace_back();
+            P.nlocal_rows++;
+        }
+        // overlap rows, per neighbour rank in order of first appearance
+        std::vector<int> comm;
+        for (int e : elems[s])
+            for (int32_t k : A->lblk[A->row(e, 0)]) {
+                const int pp = A->proc[A->ce[k]];
+                if (pp != s && std::find(comm.begin(), comm.end(), pp) == comm.end()) comm.push_back(pp);
+            }
+        std::map<int, int> ov_prow;   // element -> overlap programme row (unique per subdomain)
+        struct OvInfo { int f; int pr; std::vector<int32_t> lower_blk, upper_blk; };
+        std::vector<std::vector<OvInfo>> ovs(comm.size());
+        for (size_t ic = 0; ic < comm.size(); ++ic) {
+            const int q = comm[ic];
+            for (int f : elems[q]) {
+                if (!touches(f, s)) continue;
+                const int pr = (int)P.prow_b.size();
+                P.prow_b.push_back(A->bsize(f));
+                P.prow_elem.push_back(f);
+                P.v_off.push_back(A->seg(f, 0));      // halo of v
+                P.z_off.push_back(ov_cursor);
+                ov_cursor += A->bsize(f);
+                P.diagA_off.push_back(A->voff[A->diag[A->row(f, 0)]]);
+                P.diag_blk.push_back(-1);
+                P.lo.emplace_back();
+                P.up.emplace_back();
+                ov_prow[f] = pr;
+                OvInfo oi;
+                oi.f = f;
+                oi.pr = pr;
+                // received blocks: (1) coupling to rank s, (2) coupling to other sent
+                // neighbours on q; the diagonal is handled separately
+                std::vector<int32_t> recv;
+                for (int32_t k : A->lblk[A->row(f, 0)])
+                    if (A->ce[k] != f && A->proc[A->ce[k]] == s) recv.push_back(k);
+                for (int32_t k : A->lblk[A->row(f, 0)]) {
+                    const int nb = A->ce[k];
+                    if (nb == f || A->proc[nb] != q) continue;
+                    if (touches(nb, s)) recv.push_back(k);
+                }
+                for (int32_t k : recv) {
+                    const int par = A->ce[k];
+                    if (A->proc[par] == s) oi.lower_blk.push_back(k);     // coupled to the receiver: lower
+                    else if (par < f) oi.lower_blk.push_back(k);          // same owner, lower local index
+                    else if (par > f) oi.upper_blk.push_back(k);
+                }
+                ovs[ic].push_back(oi);
+            }
+        }
+        // local entries (type_domain_matrix.f90:295-302 with rank s)
+        for (size_t i = 0; i < elems[s].size(); ++i) {
+            const int e = elems[s][i];
+            const int pr = local_prow[i];
+            for (int32_t k : A->lblk[A->row(e, 0)]) {
+                const int p = A->ce[k];
+                if (p == e) continue;
+                const int pp = A->proc[p];
+                const bool lo = (pp == s && lidx[p] < (int)i) || (pp < s);
+                const bool up = (pp == s && lidx[p] > (int)i) || (pp > s);
+                if (lo) {
+                    if (pp != s) continue;   // parent_proc /= IRANK: skipped by factor and forward sweep
+                    if (i == 0) continue;    // the factor loop starts at the second row
+                    const int kt = find_trans(A, p, 0, e);
+                    if (kt < 0) { err = "rasilu0: no transposed block found"; return CHIDG_GPU_EINVAL; }
+                    IluEntry en;
+                    en.parent = local_prow[lidx[p]];
+                    en.a_off = A->voff[k];
+                    en.t_off = A->voff[kt];
+                    en.nc = A->bsize(p);
+                    en.blk = k;
+                    P.lo[pr].push_back(en);
+                } else if (up) {
+                    IluEntry en;
+                    if (pp == s) en.parent = local_prow[lidx[p]];
+                    else {
+                        auto it = ov_prow.find(p);
+                        if (it == ov_prow.end()) { err = "rasilu0: upper block to an element outside the overlap"; return CHIDG_GPU_EINVAL; }
+                        en.parent = it->second;
+                    }
+                    en.a_off = A->voff[k];
+                    en.nc = A->bsize(p);
+                    en.blk = k;
+                    P.up[pr].push_back(en);
+                }
+            }
+        }
+        // overlap entries
+        for (auto& O : ovs)
+            for (auto& oi : O) {
+                for (int32_t k : oi.lower_blk) {
+                    const int par = A->ce[k];
+                    const int kt = find_trans(A, par, 0, oi.f);
+                    if (kt < 0) { err = "rasilu0: no transposed block found for overlap block"; return CHIDG_GPU_EINVAL; }
+                    IluEntry en;
+                    if (A->proc[par] == s) en.parent = local_prow[lidx[par]];
+                    else {
+                        auto it = ov_prow.find(par);
+                        if (it == ov_prow.end()) { err = "rasilu0: overlap parent missing"; return CHIDG_GPU_EINVAL; }
+                        en.parent = it->second;
+                    }
+                    en.a_off = A->voff[k];
+                    en.t_off = A->voff[kt];
+                    en.nc = A->bsize(par);
+                    en.blk = -1;
+                    P.lo[oi.pr].push_back(en);
+                }
+                for (int32_t k : oi.upper_blk) {
+                    const int par = A->ce[k];
+                    auto it = ov_prow.find(par);
+                    if (it == ov_prow.end()) { err = "rasilu0: overlap parent missing"; return CHIDG_GPU_EINVAL; }
+                    IluEntry en;
+                    en.parent = it->second;
+                    en.a_off = A->voff[k];
+                    en.nc = A->bsize(par);
+                    en.blk = -1;
+                    P.up[oi.pr].push_back(en);
+                }
+            }
+    }
+    P.n_ext = ov_cursor;
+    return CHIDG_GPU_OK;
+}
+
+// Levels, LD slots, GEMM tasks, device upload.
+static int finalize_program(chidg_gpu_ctx* ctx, const chidg_gpu_matrix* A, IluProgram& P) {
+    const int np = (int)P.prow_b.size();
+    P.nprow = np;
+    // forward / factor levels: programme rows are listed in the reference's
+    // processing order, so every lower parent precedes its row
+    std::vector<int> lf(np, 0), lb(np, 0);
+    for (int pr = 0; pr < np; ++pr) {
+        int l = 0;
+        for (auto& en : P.lo[pr]) {
+            if (en.parent >= pr) return fail(ctx, CHIDG_GPU_EINVAL, "ilu programme: lower parent after its row");
+            l = std::max(l, lf[en.parent] + 1);
+        }
+        lf[pr] = l;
+    }
+    for (int pr = np - 1; pr >= 0; --pr) {
+        int l = 0;
+        for (auto& en : P.up[pr]) {
+            if (en.parent <= pr) return fail(ctx, CHIDG_GPU_EINVAL, "ilu programme: upper parent before its row");
+            l = std::max(l, lb[en.parent] + 1);
+        }
+        lb[pr] = l;
+    }
+    auto bucket = [&](const std::vector<int>& lev, std::vector<int32_t>& rows, std::vector<int>& ptr) {
+        int nl = 0;
+        for (int v : lev) nl = std::max(nl, v + 1);
+        ptr.assign(nl + 1, 0);
+        for (int v : lev) ptr[v + 1]++;
+        for (int l = 0; l < nl; ++l) ptr[l + 1] += ptr[l];
+        rows.assign(lev.size(), 0);
+        std::vector<int> cur(ptr.begin(), ptr.end() - 1);
+        for (int pr = 0; pr < (int)lev.size(); ++pr) rows[cur[lev[pr]]++] = pr;
+    };
+    bucket(lf, P.fwd_rows, P.fwd_ptr);
+    bucket(lb, P.bwd_rows, P.bwd_ptr);
+    // LD slots: per programme row [inv(D)][L_1][L_2]...
+    P.dinv_off.assign(np, 0);
+    int64_t ld = 0;
+    for (int pr = 0; pr < np; ++pr) {
+        const int b = P.prow_b[pr];
+        P.dinv_off[pr] = ld;
+        ld += (int64_t)b * b;
+        for (auto& en : P.lo[pr]) { en.l_off = ld; ld += (int64_t)b * en.nc; }
+    }
+    P.ld_size = ld;
+    // flatten entry lists
+    std::vector<int32_t> lo_ptr(np + 1, 0), up_ptr(np + 1, 0), lo_par, up_par, lo_nc, up_nc;
+    std::vector<int64_t> lo_L, up_U;
+    for (int pr = 0; pr < np; ++pr) {
+        for (auto& en : P.lo[pr]) { lo_par.push_back(en.parent); lo_nc.push_back(en.nc); lo_L.push_back(en.l_off); }
+        for (auto& en : P.up[pr]) { up_par.push_back(en.parent); up_nc.push_back(en.nc); up_U.push_back(en.a_off); }
+        lo_ptr[pr + 1] = (int32_t)lo_par.size();
+        up_ptr[pr + 1] = (int32_t)up_par.size();
+    }
+    P.max_lo_cols = 0;
+    P.max_up_cols = 0;
+    P.max_b = 0;
+    for (int pr = 0; pr < np; ++pr) {
+        int c = 0;
+        for (auto& en : P.lo[pr]) c += en.nc;
+        P.max_lo_cols = std::max(P.max_lo_cols, c);
+        c = 0;
+        for (auto& en : P.up[pr]) c += en.nc;
+        P.max_up_cols = std::max(P.max_up_cols, c);
+        P.max_b = std::max(P.max_b, P.prow_b[pr]);
+    }
+    // factorisation tasks per forward level
+    std::vector<GemmTask> ltasks, stasks;
+    std::vector<GemmPair> lpairs, spairs;
+    P.ltask_ptr.assign(P.fwd_ptr.size(), 0);
+    P.stask_ptr.assign(P.fwd_ptr.size(), 0);
+    const int nlev = (int)P.fwd_ptr.size() - 1;
+    for (int l = 0; l < nlev; ++l) {
+        for (int i = P.fwd_ptr[l]; i < P.fwd_ptr[l + 1]; ++i) {
+            const int pr = P.fwd_rows[i];
+            const int b = P.prow_b[pr];
+            for (auto& en : P.lo[pr]) {
+                // L = A_lower * inv(D_parent)      (precon_ILU0.f90:231)
+                GemmTask t{};
+                t.c_off = en.l_off; t.cinit_off = -1; t.m = b; t.n = en.nc;
+                t.q_begin = (int32_t)lpairs.size();
+                lpairs.push_back(GemmPair{en.a_off, P.dinv_off[en.parent], en.nc, 0});
+                t.q_end = (int32_t)lpairs.size();
+                t.elem = P.prow_elem[pr];
+                ltasks.push_back(t);
+            }
+            // D = A_diag - sum L * A(parent, itranspose)   (:238-239)
+            GemmTask t{};
+            t.c_off = P.dinv_off[pr]; t.cinit_off = P.diagA_off[pr]; t.m = b; t.n = b;
+            t.q_begin = (int32_t)spairs.size();
+            for (auto& en : P.lo[pr]) spairs.push_back(GemmPair{en.l_off, en.t_off, en.nc, 0});
+            t.q_end = (int32_t)spairs.size();
+            t.elem = P.prow_elem[pr];
+            stasks.push_back(t);
+        }
+        P.ltask_ptr[l + 1] = (int)ltasks.size();
+        P.stask_ptr[l + 1] = (int)stasks.size();
+    }
+    int st;
+    if ((st = upload_array(ctx, P.d_prow_b, P.prow_b)) || (st = upload_array(ctx, P.d_prow_elem, P.prow_elem)) ||
+        (st = upload_array(ctx, P.d_v_off, P.v_off)) || (st = upload_array(ctx, P.d_z_off, P.z_off)) ||
+        (st = upload_array(ctx, P.d_dinv_off, P.dinv_off)) || (st = upload_array(ctx, P.d_lo_ptr, lo_ptr)) ||
+        (st = upload_array(ctx, P.d_lo_L, lo_L)) || (st = upload_array(ctx, P.d_lo_par, lo_par)) ||
+        (st = upload_array(ctx, P.d_lo_nc, lo_nc)) || (st = upload_array(ctx, P.d_up_ptr, up_ptr)) ||
+        (st = upload_array(ctx, P.d_up_U, up_U)) || (st = upload_array(ctx, P.d_up_par, up_par)) ||
+        (st = upload_array(ctx, P.d_up_nc, up_nc)) || (st = upload_array(ctx, P.d_fwd_rows, P.fwd_rows)) ||
+        (st = upload_array(ctx, P.d_bwd_rows, P.bwd_rows)) || (st = upload_array(ctx, P.d_ltasks, ltasks)) ||
+        (st = upload_array(ctx, P.d_lpairs, lpairs)) || (st = upload_array(ctx, P.d_stasks, stasks)) ||
+        (st = upload_array(ctx, P.d_spairs, spairs)))
+        return st;
+    P.rows.prow_b = (const int32_t*)P.d_prow_b.ptr;
+    P.rows.v_off = (const int64_t*)P.d_v_off.ptr;
+    P.rows.z_off = (const int64_t*)P.d_z_off.ptr;
+    P.rows.dinv_off = (const int64_t*)P.d_dinv_off.ptr;
+    P.rows.lo_ptr = (const int32_t*)P.d_lo_ptr.ptr;
+    P.rows.lo_L = (const int64_t*)P.d_lo_L.ptr;
+    P.rows.lo_par = (const int32_t*)P.d_lo_par.ptr;
+    P.rows.lo_nc = (const int32_t*)P.d_lo_nc.ptr;
+    P.rows.up_ptr = (const int32_t*)P.d_up_ptr.ptr;
+    P.rows.up_U = (const int64_t*)P.d_up_U.ptr;
+    P.rows.up_par = (const int32_t*)P.d_up_par.ptr;
+    P.rows.up_nc = (const int32_t*)P.d_up_nc.ptr;
+    P.sweep_threads = block_dim_for(P.max_b);
+    (void)A;
+    return CHIDG_GPU_OK;
+}
+
+void chidg::release_program(IluProgram& P) {
+    for (Buffer* b : {&P.d_prow_b, &P.d_prow_elem, &P.d_v_off, &P.d_z_off, &P.d_dinv_off, &P.d_lo_ptr, &P.d_lo_L,
+                      &P.d_lo_par, &P.d_lo_nc, &P.d_up_ptr, &P.d_up_U, &P.d_up_par, &P.d_up_nc, &P.d_fwd_rows,
+                      &P.d_bwd_rows, &P.d_ltasks, &P.d_lpairs, &P.d_stasks, &P.d_spairs})
+        release(*b);
+}
+
+extern "C" int chidg_gpu_precon_create(chidg_gpu_matrix* A, int32_t kind, chidg_gpu_precon** out) {
+    if (!A || !out) return CHIDG_GPU_EINVAL;
+    *out = nullptr;
+    chidg_gpu_ctx* ctx = A->ctx;
+    cudaSetDevice(ctx->device);
+    if (kind < CHIDG_PRECON_IDENTITY || kind > CHIDG_PRECON_RASILU0) return fail(ctx, CHIDG_GPU_EINVAL, "precon_create: unknown kind");
+    auto* M = new chidg_gpu_precon();
+    M->ctx = ctx;
+    M->A = A;
+    M->kind = kind;
+    if (kind != CHIDG_PRECON_IDENTITY) {
+        std::string err;
+        int st = (kind == CHIDG_PRECON_RASILU0) ? build_rasilu0(A, M->P, err)
+                                                : build_ilu0(A, kind == CHIDG_PRECON_JACOBI, M->P, err);
+        if (st) { delete M; return fail(ctx, st, err); }
+        st = finalize_program(ctx, A, M->P);
+        if (st) { release_program(M->P); delete M; return st; }
+    }
+    *out = M;
+    return CHIDG_GPU_OK;
+}
+
+extern "C" int chidg_gpu_precon_destroy(chidg_gpu_precon* M) {
+    if (!M) return CHIDG_GPU_OK;
+    cudaSetDevice(M->ctx->device);
+    cudaStreamSynchronize(M->ctx->stream);
+    release_program(M->P);
+    for (Buffer* b : {&M->LD, &M->LD32, &M->LD16, &M->zx, &M->zx32, &M->piv_scratch}) release(*b);
+    delete M;
+    return CHIDG_GPU_OK;
+}
+extern "C" int chidg_gpu_precon_stamp(chidg_gpu_precon* M, int64_t* s) {
+    if (!M || !s) return CHIDG_GPU_EINVAL;
+    *s = M->stamp;
+    return CHIDG_GPU_OK;
+}
+
+static int launch_inverse(chidg_gpu_precon* M, int row_begin, int count) {
+    chidg_gpu_ctx* ctx = M->ctx;
+    IluProgram& P = M->P;
+    double* LD = (double*)M->LD.ptr;
+    const int bmax = P.max_b;
+    if (bmax <= 32)
+        k_block_inverse<1, 1, 32><<<count, 1024, 0, ctx->stream>>>(LD, (const int64_t*)P.d_dinv_off.ptr, (const int32_t*)P.d_prow_b.ptr,
+                                                                  (const int32_t*)P.d_prow_elem.ptr, (const int32_t*)P.d_fwd_rows.ptr, row_begin, ctx->d_status);
+    else if (bmax <= 64)
+        k_block_inverse<2, 2, 32><<<count, 1024, 0, ctx->stream>>>(LD, (const int64_t*)P.d_dinv_off.ptr, (const int32_t*)P.d_prow_b.ptr,
+                                                                  (const int32_t*)P.d_prow_elem.ptr, (const int32_t*)P.d_fwd_rows.ptr, row_begin, ctx->d_status);
+    else if (bmax <= 96)
+        k_block_inverse<3, 3, 32><<<count, 1024, 0, ctx->stream>>>(LD, (const int64_t*)P.d_dinv_off.ptr, (const int32_t*)P.d_prow_b.ptr,
+                                                                  (const int32_t*)P.d_prow_elem.ptr, (const int32_t*)P.d_fwd_rows.ptr, row_begin, ctx->d_status);
+    else if (bmax <= 160)
+        k_block_inverse<5, 10, 16><<<count, 512, 0, ctx->stream>>>(LD, (const int64_t*)P.d_dinv_off.ptr, (const int32_t*)P.d_prow_b.ptr,
+                                                                  (const int32_t*)P.d_prow_elem.ptr, (const int32_t*)P.d_fwd_rows.ptr, row_begin, ctx->d_status);
+    else {
+        int st = ensure(ctx, M->piv_scratch, sizeof(int) * 1024 * (size_t)std::max(count, 1));
+        if (st) return st;
+        k_block_inverse_global<<<count, 512, 0, ctx->stream>>>(LD, (const int64_t*)P.d_dinv_off.ptr, (const int32_t*)P.d_prow_b.ptr,
+                                                             (const int32_t*)P.d_prow_elem.ptr, (const int32_t*)P.d_fwd_rows.ptr, row_begin,
+                                                             ctx->d_status, (int*)M->piv_scratch.ptr);
+    }
+    return check_launch(ctx, "k_block_inverse");
+}
+
+// precon%update: FP64 factorisation level by level, then the low-precision
+// copies of the factors when requested.
+extern "C" int chidg_gpu_precon_update(chidg_gpu_precon* M, chidg_gpu_matrix* A, int32_t precision) {
+    if (!M || !A || A != M->A) return CHIDG_GPU_EINVAL;
+    chidg_gpu_ctx* ctx = M->ctx;
+    cudaSetDevice(ctx->device);
+    if (precision < CHIDG_GPU_FP64 || precision > CHIDG_GPU_MIXED_BF16) return fail(ctx, CHIDG_GPU_EINVAL, "precon_update: bad precision");
+    ctx->err_elem = -1;
+    if (M->kind == CHIDG_PRECON_IDENTITY) { M->stamp = A->stamp; M->precision = precision; return CHIDG_GPU_OK; }
+    IluProgram& P = M->P;
+    int st = ensure(ctx, M->LD, sizeof(double) * (size_t)P.ld_size);
+    if (st) return st;
+    int big = INT_MAX;
+    cudaMemcpyAsync(ctx->d_status, &big, sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
+    const int nlev = (int)P.fwd_ptr.size() - 1;
+    const int tiles_1d = (P.max_b + GT_M - 1) / GT_M;
+    for (int l = 0; l < nlev; ++l) {
+        const int nl = P.ltask_ptr[l + 1] - P.ltask_ptr[l];
+        if (nl > 0) {
+            k_task_gemm<double, double, double><<<nl * tiles_1d * tiles_1d, 256, 0, ctx->stream>>>(
+                (const GemmTask*)P.d_ltasks.ptr + P.ltask_ptr[l], (const GemmPair*)P.d_lpairs.ptr, tiles_1d, tiles_1d,
+                (const double*)A->val.ptr, (const double*)M->LD.ptr, nullptr, (double*)M->LD.ptr, 1.0);
+            if ((st = check_launch(ctx, "k_task_gemm L"))) return st;
+        }
+        const int ns = P.stask_ptr[l + 1] - P.stask_ptr[l];
+        if (ns > 0) {
+            k_task_gemm<double, double, double><<<ns * tiles_1d * tiles_1d, 256, 0, ctx->stream>>>(
+                (const GemmTask*)P.d_stasks.ptr + P.stask_ptr[l], (const GemmPair*)P.d_spairs.ptr, tiles_1d, tiles_1d,
+                (const double*)M->LD.ptr, (const double*)A->val.ptr, (const double*)A->val.ptr, (double*)M->LD.ptr, -1.0);
+            if ((st = check_launch(ctx, "k_task_gemm S"))) return st;
+        }
+        const int nr = P.fwd_ptr[l + 1] - P.fwd_ptr[l];
+        if ((st = launch_inverse(M, P.fwd_ptr[l], nr))) return st;
+    }
+    cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "precon update");
+    if (ctx->h_status[0] != INT_MAX) {
+        ctx->err_elem = ctx->h_status[0];
+        return fail(ctx, CHIDG_GPU_ESINGULAR, "inv: Matrix is numerically singular! (element " + std::to_string(ctx->h_status[0]) + ")");
+    }
+    if (precision != CHIDG_GPU_FP64) {
+        if ((st = matrix_lowp(A, precision))) return st;
+        if (precision == CHIDG_GPU_MIXED_FP32) {
+            if ((st = ensure(ctx, M->LD32, sizeof(float) * (size_t)P.ld_size))) return st;
+            k_convert<double, float><<<grid_for(P.ld_size, 256, ctx->nsm * 8), 256, 0, ctx->stream>>>(P.ld_size, (const double*)M->LD.ptr, (float*)M->LD32.ptr);
+        } else {
+            if ((st = ensure(ctx, M->LD16, sizeof(__nv_bfloat16) * (size_t)P.ld_size))) return st;
+            k_convert<double, __nv_bfloat16><<<grid_for(P.ld_size, 256, ctx->nsm * 8), 256, 0, ctx->stream>>>(P.ld_size, (const double*)M->LD.ptr, (__nv_bfloat16*)M->LD16.ptr);
+        }
+        if ((st = check_launch(ctx, "k_convert LD"))) return st;
+    }
+    M->precision = precision;
+    M->stamp = A->stamp;
+    return CHIDG_GPU_OK;
+}
+
+// z = M^{-1} v in the given arithmetic.  TV is the vector type; factors come
+// from LD (FP64), LD32 or LD16 by precision; U blocks from A (FP64 or FP32).
+template <typename TV>
+int chidg::precon_apply_impl(chidg_gpu_precon* M, const TV* v, TV* z, int precision) {
+    chidg_gpu_ctx* ctx = M->ctx;
+    chidg_gpu_matrix* A = M->A;
+    const int64_t n = A->n;
+    if (M->kind == CHIDG_PRECON_IDENTITY) {
+        const cudaError_t e = cudaMemcpyAsync(z, v, sizeof(TV) * (size_t)n, cudaMemcpyDeviceToDevice, ctx->stream);
+        return e == cudaSuccess ? CHIDG_GPU_OK : cuda_fail(ctx, e, "identity apply");
+    }
+    IluProgram& P = M->P;
+    using ACC = typename AccOf<TV>::type;
+    // work buffer: the output itself when there are no overlap rows
+    TV* zx = z;
+    if (P.n_ext != n) {
+        Buffer& wb = (sizeof(TV) == 8) ? M->zx : M->zx32;
+        int st = ensure(ctx, wb, sizeof(TV) * (size_t)P.n_ext);
+        if (st) return st;
+        zx = (TV*)wb.ptr;
+    }
+    const int threads = P.sweep_threads;
+    const size_t smem_f = sizeof(ACC) * ((size_t)P.max_lo_cols + threads) + 64;
+    const size_t smem_b = sizeof(ACC) * ((size_t)P.max_up_cols + P.max_b + threads) + 64;
+    const int nf = (int)P.fwd_ptr.size() - 1, nb = (int)P.bwd_ptr.size() - 1;
+    int st;
+    for (int l = 0; l < nf; ++l) {
+        const int cnt = P.fwd_ptr[l + 1] - P.fwd_ptr[l];
+        if (precision == CHIDG_GPU_MIXED_BF16 && sizeof(TV) == 4)
+            k_ilu_forward<__nv_bfloat16, TV, ACC><<<cnt, threads, smem_f, ctx->stream>>>(P.rows, (const __nv_bfloat16*)M->LD16.ptr, (const int32_t*)P.d_fwd_rows.ptr, P.fwd_ptr[l], v, zx);
+        else if (sizeof(TV) == 4)
+            k_ilu_forward<float, TV, ACC><<<cnt, threads, smem_f, ctx->stream>>>(P.rows, (const float*)M->LD32.ptr, (const int32_t*)P.d_fwd_rows.ptr, P.fwd_ptr[l], v, zx);
+        else
+            k_ilu_forward<double, TV, ACC><<<cnt, threads, smem_f, ctx->stream>>>(P.rows, (const double*)M->LD.ptr, (const int32_t*)P.d_fwd_rows.ptr, P.fwd_ptr[l], v, zx);
+        if ((st = check_launch(ctx, "k_ilu_forward"))) return st;
+    }
+    for (int l = 0; l < nb; ++l) {
+        const int cnt = P.bwd_ptr[l + 1] - P.bwd_ptr[l];
+        if (precision == CHIDG_GPU_MIXED_BF16 && sizeof(TV) == 4)
+            k_ilu_backward<__nv_bfloat16, float, TV, ACC><<<cnt, threads, smem_b, ctx->stream>>>(P.rows, (const __nv_bfloat16*)M->LD16.ptr, (const float*)A->val32.ptr, (const int32_t*)P.d_bwd_rows.ptr, P.bwd_ptr[l], zx);
+        else if (sizeof(TV) == 4)
+            k_ilu_backward<float, float, TV, ACC><<<cnt, threads, smem_b, ctx->stream>>>(P.rows, (const float*)M->LD32.ptr, (const float*)A->val32.ptr, (const int32_t*)P.d_bwd_rows.ptr, P.bwd_ptr[l], zx);
+        else
+            k_ilu_backward<double, double, TV, ACC><<<cnt, threads, smem_b, ctx->stream>>>(P.rows, (const double*)M->LD.ptr, (const double*)A->val.ptr, (const int32_t*)P.d_bwd_rows.ptr, P.bwd_ptr[l], zx);
+        if ((st = check_launch(ctx, "k_ilu_backward"))) return st;
+    }
+    if (zx != z) {
+        const cudaError_t e = cudaMemcpyAsync(z, zx, sizeof(TV) * (size_t)n, cudaMemcpyDeviceToDevice, ctx->stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "precon output copy");
+    }
+    return CHIDG_GPU_OK;
+}
+template int chidg::precon_apply_impl<double>(chidg_gpu_precon*, const double*, double*, int);
+template int chidg::precon_apply_impl<float>(chidg_gpu_precon*, const float*, float*, int);
+
+int chidg::precon_set_smem(chidg_gpu_precon* M) {
+    IluProgram& P = M->P;
+    const int threads = P.sweep_threads;
+    const size_t sf = sizeof(double) * ((size_t)P.max_lo_cols + threads) + 64;
+    const size_t sb = sizeof(double) * ((size_t)P.max_up_cols + P.max_b + threads) + 64;
+    if (sf > 48 * 1024) cudaFuncSetAttribute(k_ilu_forward<double, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sf);
+    if (sb > 48 * 1024) cudaFuncSetAttribute(k_ilu_backward<double, double, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
+    return CHIDG_GPU_OK;
+}
+
+extern "C" int chidg_gpu_precon_apply(chidg_gpu_precon* M, chidg_gpu_matrix* A, const chidg_gpu_vector* v, chidg_gpu_vector* z) {
+    if (!M || !A || !v || !z || A != M->A || v->n != A->n || z->n != A->n || v == z) return CHIDG_GPU_EINVAL;
+    cudaSetDevice(M->ctx->device);
+    if (M->kind != CHIDG_PRECON_IDENTITY && M->stamp == 0) return fail(M->ctx, CHIDG_GPU_ESTATE, "precon_apply: preconditioner not updated");
+    precon_set_smem(M);
+    return precon_apply_impl<double>(M, (const double*)v->buf.ptr, (double*)z->buf.ptr, CHIDG_GPU_FP64);
+}
+
+extern "C" int chidg_gpu_precon_download_LD(chidg_gpu_precon* M, double* host) {
+    if (!M || !host) return CHIDG_GPU_EINVAL;
+    chidg_gpu_ctx* ctx = M->ctx;
+    cudaSetDevice(ctx->device);
+    chidg_gpu_matrix* A = M->A;
+    if (M->kind == CHIDG_PRECON_IDENTITY || M->stamp == 0) return fail(ctx, CHIDG_GPU_ESTATE, "download_LD: no factors");
+    std::vector<double> ld((size_t)M->P.ld_size);
+    cudaError_t e = cudaMemcpyAsync(ld.data(), M->LD.ptr, sizeof(double) * ld.size(), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "LD download");
+    std::memset(host, 0, sizeof(double) * (size_t)A->nval);
+    const IluProgram& P = M->P;
+    for (int pr = 0; pr < P.nprow; ++pr) {
+        if (P.diag_blk[pr] < 0) continue;   // overlap rows live only inside the preconditioner
+        const int b = P.prow_b[pr];
+        std::memcpy(host + A->voff[P.diag_blk[pr]], ld.data() + P.dinv_off[pr], sizeof(double) * b * b);
+        for (const auto& en : P.lo[pr])
+            if (en.blk >= 0) std::memcpy(host + A->voff[en.blk], ld.data() + en.l_off, sizeof(double) * (size_t)b * en.nc);
+    }
+    return CHIDG_GPU_OK;
+}

@@ -1,0 +1,131 @@
+// chidg_gpu_internal.cuh -- internal objects behind the C ABI handles.
+#pragma once
+#include "../../include/chidg_gpu.h"
+#include "kernels.cuh"
+
+#include <cmath>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace chidg {
+
+struct Buffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+// device scalar slots (ctx->d_scal): results of reductions read by the host
+constexpr int kScalSlots = 8192;
+constexpr int kSlotTmp = 0;        // one-off dots / norms
+constexpr int kSlotNormBefore = 1; // ||w||^2 before orthogonalisation
+constexpr int kSlotWnorm = 2;      // ||w||^2 after orthogonalisation
+constexpr int kSlotR0 = 3;         // ||r0||^2
+constexpr int kSlotH = 16;         // h(1:j, j) of the current pass (up to 4000 entries)
+constexpr int kSlotY = 4096;       // y coefficients of the solution update
+
+template <typename T> struct AccOf { using type = double; };
+template <> struct AccOf<float> { using type = float; };
+
+struct IluEntry {
+    int parent = -1;         // programme row of the coupled element
+    int64_t a_off = 0;       // block in A (lower: A_lower; upper: U)
+    int64_t t_off = 0;       // lower only: A(parent, itranspose)
+    int64_t l_off = 0;       // lower only: L slot in LD
+    int nc = 0;              // columns (= parent's block size)
+    int32_t blk = -1;        // matrix block id (LD download), -1 for overlap copies
+};
+
+struct IluProgram {
+    int nprow = 0;
+    int nlocal_rows = 0;
+    int64_t n_ext = 0;       // work vector length: n + overlap rows
+    int64_t ld_size = 0;
+    int max_lo_cols = 0, max_up_cols = 0, max_b = 0;
+    int sweep_threads = 32;
+    std::vector<int32_t> prow_b, prow_elem, diag_blk;
+    std::vector<int64_t> v_off, z_off, diagA_off, dinv_off;
+    std::vector<std::vector<IluEntry>> lo, up;
+    std::vector<int32_t> fwd_rows, bwd_rows;
+    std::vector<int> fwd_ptr, bwd_ptr;
+    std::vector<int> ltask_ptr, stask_ptr;
+    Buffer d_prow_b, d_prow_elem, d_v_off, d_z_off, d_dinv_off, d_lo_ptr, d_lo_L, d_lo_par, d_lo_nc, d_up_ptr,
+        d_up_U, d_up_par, d_up_nc, d_fwd_rows, d_bwd_rows, d_ltasks, d_lpairs, d_stasks, d_spairs;
+    IluRows rows{};
+};
+
+}  // namespace chidg
+
+struct chidg_gpu_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int nsm = 148;
+    std::string err;
+    int32_t err_elem = -1;
+    int64_t launches = 0;
+    int* d_status = nullptr;
+    int* h_status = nullptr;
+    double* d_scal = nullptr;
+    double* h_scal = nullptr;
+    chidg::Buffer partial, partial2;
+};
+
+struct chidg_gpu_matrix {
+    chidg_gpu_ctx* ctx = nullptr;
+    int nelem = 0, ntime = 0, nrow = 0;
+    int64_t n = 0, nval = 0, nblk = 0;
+    std::vector<int32_t> nvars, nterms, proc, re, rt, ce, ct, kind;
+    std::vector<int64_t> eoff, voff;
+    std::vector<std::vector<int32_t>> rowblk, lblk;
+    std::vector<int32_t> diag;
+    int max_row_cols = 0, max_b = 0, mv_threads = 32;
+    chidg::Buffer val, val32, val16;
+    int64_t val32_stamp = -1;
+    chidg::Buffer d_row_ptr, d_blk_voff, d_blk_xoff, d_blk_nc, d_row_yoff, d_row_b, d_diag_voff, d_elem_nvars,
+        d_elem_nterms, row_sq;
+    int64_t stamp = 0;
+
+    int bsize(int e) const { return nvars[e] * nterms[e]; }
+    int64_t seg(int e, int t) const { return eoff[e] + (int64_t)t * bsize(e); }
+    int row(int e, int t) const { return e * ntime + t; }
+};
+
+struct chidg_gpu_vector {
+    chidg_gpu_matrix* A = nullptr;
+    chidg_gpu_ctx* ctx = nullptr;
+    int64_t n = 0;
+    chidg::Buffer buf;
+};
+
+struct chidg_gpu_precon {
+    chidg_gpu_ctx* ctx = nullptr;
+    chidg_gpu_matrix* A = nullptr;
+    int kind = 0;
+    int precision = 0;
+    int64_t stamp = 0;
+    chidg::IluProgram P;
+    chidg::Buffer LD, LD32, LD16, zx, zx32, piv_scratch;
+};
+
+namespace chidg {
+int fail(chidg_gpu_ctx* ctx, int code, const std::string& msg);
+int cuda_fail(chidg_gpu_ctx* ctx, cudaError_t e, const char* what);
+int check_launch(chidg_gpu_ctx* ctx, const char* what);
+int ensure(chidg_gpu_ctx* ctx, Buffer& buf, size_t bytes);
+void release(Buffer& buf);
+int grid_for(int64_t n, int threads, int cap);
+int reduce_partials(chidg_gpu_ctx* ctx, const double* partial, int ncta, int nq, int slot, bool do_sqrt);
+int fetch_scalars(chidg_gpu_ctx* ctx, int slot, int count, double* out);
+int push_scalars(chidg_gpu_ctx* ctx, int slot, int count, const double* in);
+template <typename T>
+int mdot(chidg_gpu_ctx* ctx, int64_t n, const T* x, const T* y, int64_t ystride, int nq, int slot);
+int matrix_lowp(chidg_gpu_matrix* A, int precision);
+template <typename TA, typename TV>
+int matvec_launch(chidg_gpu_matrix* A, const TA* val, const TV* x, TV* y, const TV* z, double alpha, double beta, double* row_sq);
+int set_matvec_smem(chidg_gpu_matrix* A);
+template <typename TV>
+int precon_apply_impl(chidg_gpu_precon* M, const TV* v, TV* z, int precision);
+int precon_set_smem(chidg_gpu_precon* M);
+void release_program(IluProgram& P);
+}  // namespace chidg

@@ -1,0 +1,715 @@
+// kernels.cuh -- sm_100a kernels of the ChiDG implicit linear-solve path.
+//
+// Data layout in HBM (see also the host builders in chidg_gpu.cu):
+//  * A: every block of the pattern, packed in pattern order, each block
+//    column-major nrows x ncols (the reference's densematrix_t%mat storage,
+//    so a host upload is one contiguous copy).  FP64, plus an FP32 copy with
+//    the same packing for the mixed-precision inner solves.
+//  * vectors: element-major, then time, field, mode (densevector_t layout).
+//  * ILU programme: one "programme row" per matrix row (ILU0/Jacobi) or per
+//    subdomain row / overlap row (RAS).  LD holds, per programme row, the
+//    inverted diagonal and one L block per lower entry.  U blocks are read
+//    from A.  Rows are grouped into dependency levels for the factorisation
+//    and the two triangular sweeps.
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+namespace chidg {
+
+// ---------------------------------------------------------------------------
+// conversions
+// ---------------------------------------------------------------------------
+template <typename T> __device__ __forceinline__ double to_d(T v);
+template <> __device__ __forceinline__ double to_d<double>(double v) { return v; }
+template <> __device__ __forceinline__ double to_d<float>(float v) { return (double)v; }
+template <> __device__ __forceinline__ double to_d<__nv_bfloat16>(__nv_bfloat16 v) { return (double)__bfloat162float(v); }
+template <typename T> __device__ __forceinline__ float to_f(T v);
+template <> __device__ __forceinline__ float to_f<double>(double v) { return (float)v; }
+template <> __device__ __forceinline__ float to_f<float>(float v) { return v; }
+template <> __device__ __forceinline__ float to_f<__nv_bfloat16>(__nv_bfloat16 v) { return __bfloat162float(v); }
+template <typename ACC, typename T> __device__ __forceinline__ ACC cvt(T v);
+template <> __device__ __forceinline__ double cvt<double, double>(double v) { return v; }
+template <> __device__ __forceinline__ double cvt<double, float>(float v) { return (double)v; }
+template <> __device__ __forceinline__ double cvt<double, __nv_bfloat16>(__nv_bfloat16 v) { return (double)__bfloat162float(v); }
+template <> __device__ __forceinline__ float cvt<float, double>(double v) { return (float)v; }
+template <> __device__ __forceinline__ float cvt<float, float>(float v) { return v; }
+template <> __device__ __forceinline__ float cvt<float, __nv_bfloat16>(__nv_bfloat16 v) { return __bfloat162float(v); }
+template <typename T> __device__ __forceinline__ T from_d(double v);
+template <> __device__ __forceinline__ double from_d<double>(double v) { return v; }
+template <> __device__ __forceinline__ float from_d<float>(double v) { return (float)v; }
+template <> __device__ __forceinline__ __nv_bfloat16 from_d<__nv_bfloat16>(double v) { return __float2bfloat16_rn((float)v); }
+
+// Streaming load of matrix data: each block is read once per sweep and the
+// arrays are far larger than L2, so do not let them evict the vectors.
+template <typename T> __device__ __forceinline__ T ld_stream(const T* p) { return __ldcs(p); }
+template <> __device__ __forceinline__ __nv_bfloat16 ld_stream<__nv_bfloat16>(const __nv_bfloat16* p) {
+    unsigned short u = __ldcs(reinterpret_cast<const unsigned short*>(p));
+    return __ushort_as_bfloat16(u);
+}
+
+// ---------------------------------------------------------------------------
+// block reductions (deterministic: fixed tree for a fixed blockDim)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+// returns the block sum in thread 0 (other threads: garbage). scratch >= 32 doubles.
+__device__ __forceinline__ double block_sum(double v, double* scratch) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) scratch[w] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (w == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        s = (lane < nw) ? scratch[lane] : 0.0;
+        s = warp_sum(s);
+    }
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// chidg_mv: one CTA per matrix row (element, time level).
+//   y_row = alpha * sum_k A_k x_{col(k)} + beta * z_row
+// Thread t owns output entry r = t % b and the column stripe c = g, g+G, ...
+// (g = t / b), so consecutive threads read consecutive addresses of every
+// column-major block.  The x segments of the row's blocks are staged in
+// shared memory once.  Optionally writes the row's sum of squares of y.
+// ---------------------------------------------------------------------------
+template <typename TA, typename TX, typename TY, typename ACC>
+__global__ void k_matvec(const TA* __restrict__ val, const int64_t* __restrict__ row_ptr,
+                         const int64_t* __restrict__ blk_voff, const int64_t* __restrict__ blk_xoff,
+                         const int32_t* __restrict__ blk_nc, const int64_t* __restrict__ row_yoff,
+                         const int32_t* __restrict__ row_b, const TX* __restrict__ x,
+                         TY* __restrict__ y, const TY* __restrict__ z, double alpha, double beta,
+                         double* __restrict__ row_sumsq) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ACC* xs = reinterpret_cast<ACC*>(smem_raw);
+    const int row = blockIdx.x;
+    const int b = row_b[row];
+    const int64_t k0 = row_ptr[row], k1 = row_ptr[row + 1];
+    const int tid = threadIdx.x;
+    int off = 0;
+    for (int64_t k = k0; k < k1; ++k) {
+        const int nc = blk_nc[k];
+        const TX* xp = x + blk_xoff[k];
+        for (int c = tid; c < nc; c += blockDim.x) xs[off + c] = cvt<ACC>(xp[c]);
+        off += nc;
+    }
+    const int ncols_total = off;
+    __syncthreads();
+    const int G = blockDim.x / b;
+    const int r = tid % b, g = tid / b;
+    ACC acc = 0;
+    if (g < G) {
+        off = 0;
+        for (int64_t k = k0; k < k1; ++k) {
+            const int nc = blk_nc[k];
+            const TA* Ab = val + blk_voff[k] + r;
+            const ACC* xb = xs + off;
+            int c = g;
+            for (; c + 3 * G < nc; c += 4 * G) {
+                const TA a0 = ld_stream(Ab + (int64_t)c * b);
+                const TA a1 = ld_stream(Ab + (int64_t)(c + G) * b);
+                const TA a2 = ld_stream(Ab + (int64_t)(c + 2 * G) * b);
+                const TA a3 = ld_stream(Ab + (int64_t)(c + 3 * G) * b);
+                acc += cvt<ACC>(a0) * xb[c];
+                acc += cvt<ACC>(a1) * xb[c + G];
+                acc += cvt<ACC>(a2) * xb[c + 2 * G];
+                acc += cvt<ACC>(a3) * xb[c + 3 * G];
+            }
+            for (; c < nc; c += G) acc += cvt<ACC>(ld_stream(Ab + (int64_t)c * b)) * xb[c];
+            off += nc;
+        }
+    }
+    ACC* red = xs + ncols_total;
+    if (g < G) red[g * b + r] = acc;
+    __syncthreads();
+    double sq = 0.0;
+    if (tid < b) {
+        ACC s = 0;
+        for (int gg = 0; gg < G; ++gg) s += red[gg * b + tid];
+        double out = alpha * (double)s;
+        const int64_t yo = row_yoff[row] + tid;
+        if (z != nullptr) out += beta * to_d(z[yo]);
+        const TY o = from_d<TY>(out);
+        y[yo] = o;
+        const double od = to_d(o);
+        sq = od * od;
+    }
+    if (row_sumsq != nullptr) {
+        __syncthreads();
+        double* scratch = reinterpret_cast<double*>(smem_raw);
+        const double s = block_sum(sq, scratch);
+        if (tid == 0) row_sumsq[row] = s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// BLAS-1.  All reductions are two-pass: per-CTA partials in fixed order, then
+// one CTA sums the partials in fixed order, so results are reproducible.
+// ---------------------------------------------------------------------------
+// partial[q * gridDim.x + blockIdx.x] = sum_i x[i] * y_q[i],  y_q = y + q * ystride
+template <typename T>
+__global__ void k_mdot_partial(int64_t n, const T* __restrict__ x, const T* __restrict__ y,
+                               int64_t ystride, int nq, double* __restrict__ partial) {
+    __shared__ double scratch[32];
+    for (int q = 0; q < nq; ++q) {
+        const T* yq = y + (int64_t)q * ystride;
+        double s = 0.0;
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+            s += to_d(x[i]) * to_d(yq[i]);
+        s = block_sum(s, scratch);
+        if (threadIdx.x == 0) partial[(int64_t)q * gridDim.x + blockIdx.x] = s;
+    }
+}
+// out[q] = sum_c partial[q * ncta + c]  (optionally sqrt)
+static __global__ void k_reduce_partials(const double* __restrict__ partial, int ncta, int nq,
+                                  double* __restrict__ out, int do_sqrt) {
+    __shared__ double scratch[32];
+    for (int q = 0; q < nq; ++q) {
+        double s = 0.0;
+        for (int c = threadIdx.x; c < ncta; c += blockDim.x) s += partial[(int64_t)q * ncta + c];
+        s = block_sum(s, scratch);
+        if (threadIdx.x == 0) out[q] = do_sqrt ? sqrt(s) : s;
+        __syncthreads();
+    }
+}
+// w[i] = w[i] - sum_q h[q] * v_q[i]  (CGS update, h on device), with sum of squares partials
+template <typename T>
+__global__ void k_maxpy_sub_norm(int64_t n, T* __restrict__ w, const T* __restrict__ v, int64_t vstride,
+                                 int nq, const double* __restrict__ h, double* __restrict__ partial) {
+    __shared__ double scratch[32];
+    __shared__ double hs[128];
+    double sq = 0.0;
+    for (int q0 = 0; q0 < nq; q0 += 128) {
+        const int qn = min(128, nq - q0);
+        __syncthreads();
+        for (int q = threadIdx.x; q < qn; q += blockDim.x) hs[q] = h[q0 + q];
+        __syncthreads();
+        const bool last = (q0 + 128 >= nq);
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+            double acc = to_d(w[i]);
+            for (int q = 0; q < qn; ++q) acc = acc - hs[q] * to_d(v[(int64_t)(q0 + q) * vstride + i]);
+            const T o = from_d<T>(acc);
+            w[i] = o;
+            if (last) { const double od = to_d(o); sq += od * od; }
+        }
+    }
+    if (partial != nullptr) {
+        sq = block_sum(sq, scratch);
+        if (threadIdx.x == 0) partial[blockIdx.x] = sq;
+    }
+}
+// MGS single step: w -= h[0] * v (h on device), with sum-of-squares partials
+// x = x0 + sum_q y[q] * z_q   (y on device)
+template <typename T>
+__global__ void k_lincomb(int64_t n, T* __restrict__ x, const T* __restrict__ x0, const T* __restrict__ z,
+                          int64_t zstride, int nq, const double* __restrict__ y) {
+    __shared__ double ys[128];
+    for (int q0 = 0; q0 < nq || q0 == 0; q0 += 128) {
+        const int qn = min(128, nq - q0);
+        __syncthreads();
+        for (int q = threadIdx.x; q < qn; q += blockDim.x) ys[q] = y[q0 + q];
+        __syncthreads();
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+            double acc = (q0 == 0) ? (x0 ? to_d(x0[i]) : 0.0) : to_d(x[i]);
+            for (int q = 0; q < qn; ++q) acc = acc + ys[q] * to_d(z[(int64_t)(q0 + q) * zstride + i]);
+            x[i] = from_d<T>(acc);
+        }
+        if (nq == 0) break;
+    }
+}
+// y = a * x + b * y, with the scalars either given or read from device memory
+// (a = 1 / *adiv when adiv != nullptr).
+template <typename TX, typename TY>
+__global__ void k_axpby(int64_t n, double a, const double* adiv, const TX* x, double b, TY* y) {
+    const double aa = adiv ? 1.0 / (*adiv) : a;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double yv = (b == 0.0) ? 0.0 : b * to_d(y[i]);
+        y[i] = from_d<TY>(aa * to_d(x[i]) + yv);
+    }
+}
+template <typename TS, typename TD>
+__global__ void k_convert(int64_t n, const TS* __restrict__ s, TD* __restrict__ d) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        d[i] = from_d<TD>(to_d(s[i]));
+}
+
+// ---------------------------------------------------------------------------
+// Pseudo-transient term: DIAG(e,t)[field block] += scale[e*nvars+f] * mass_e
+// (chidg_matrix%scale_diagonal).  One CTA per (element, time).
+// ---------------------------------------------------------------------------
+static __global__ void k_scale_diagonal(double* __restrict__ val, const int64_t* __restrict__ diag_voff,
+                                 const int32_t* __restrict__ elem_nvars, const int32_t* __restrict__ elem_nterms,
+                                 const int64_t* __restrict__ mass_off, const double* __restrict__ mass,
+                                 const double* __restrict__ scale, const int64_t* __restrict__ scale_off, int ntime) {
+    const int row = blockIdx.x;
+    const int e = row / ntime;
+    const int nv = elem_nvars[e], nt = elem_nterms[e];
+    const int b = nv * nt;
+    double* D = val + diag_voff[row];
+    const double* M = mass + mass_off[e];
+    for (int idx = threadIdx.x; idx < nv * nt * nt; idx += blockDim.x) {
+        const int f = idx / (nt * nt);
+        const int rem = idx % (nt * nt);
+        const int i = rem % nt, j = rem / nt;
+        const double s = scale[scale_off[e] + f];
+        D[(int64_t)(f * nt + i) + (int64_t)(f * nt + j) * b] += s * M[i + j * nt];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// ILU programme: factorisation
+// ---------------------------------------------------------------------------
+struct GemmTask {            // C(m x n) = [Cinit] + sgn * sum_q A_q(m x k_q) B_q(k_q x n)
+    int64_t c_off;           // into the output arena
+    int64_t cinit_off;       // into the Cinit arena, or -1 (start from zero)
+    int32_t m, n;
+    int32_t q_begin, q_end;  // pairs
+    int32_t elem;            // element id for status reporting
+    int32_t pad;
+};
+struct GemmPair {
+    int64_t a_off, b_off;
+    int32_t k;
+    int32_t pad;
+};
+
+// Tiled FP64 SIMT GEMM over a list of tasks.  64x64 output tile per CTA,
+// 256 threads each accumulating a 4x4 register tile, K staged 16 at a time.
+// All operands column-major with leading dimension = their row count.
+constexpr int GT_M = 64, GT_N = 64, GT_K = 16;
+template <typename TA, typename TB, typename TC>
+__global__ void __launch_bounds__(256) k_task_gemm(const GemmTask* __restrict__ tasks, const GemmPair* __restrict__ pairs,
+                                                   int tiles_m, int tiles_n,
+                                                   const TA* Abase, const TB* Bbase,
+                                                   const double* Cinit, TC* Cbase, double sgn) {
+    __shared__ double As[GT_K][GT_M + 1];
+    __shared__ double Bs[GT_K][GT_N + 1];
+    const int tiles = tiles_m * tiles_n;
+    const GemmTask t = tasks[blockIdx.x / tiles];
+    const int tile = blockIdx.x % tiles;
+    const int i0 = (tile % tiles_m) * GT_M, j0 = (tile / tiles_m) * GT_N;
+    if (i0 >= t.m || j0 >= t.n) return;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    double acc[4][4];
+    #pragma unroll
+    for (int a = 0; a < 4; ++a)
+        #pragma unroll
+        for (int c = 0; c < 4; ++c) acc[a][c] = 0.0;
+    for (int q = t.q_begin; q < t.q_end; ++q) {
+        const GemmPair pr = pairs[q];
+        const TA* A = Abase + pr.a_off;   // m x k
+        const TB* B = Bbase + pr.b_off;   // k x n
+        for (int k0 = 0; k0 < pr.k; k0 += GT_K) {
+            // A tile: 64 rows x 16 k  (column-major => consecutive threads walk rows)
+            for (int idx = threadIdx.x; idx < GT_M * GT_K; idx += 256) {
+                const int ii = idx % GT_M, kk = idx / GT_M;
+                const int gi = i0 + ii, gk = k0 + kk;
+                As[kk][ii] = (gi < t.m && gk < pr.k) ? to_d(A[gi + (int64_t)gk * t.m]) : 0.0;
+            }
+            // B tile: 16 k x 64 cols
+            for (int idx = threadIdx.x; idx < GT_K * GT_N; idx += 256) {
+                const int kk = idx % GT_K, jj = idx / GT_K;
+                const int gk = k0 + kk, gj = j0 + jj;
+                Bs[kk][jj] = (gk < pr.k && gj < t.n) ? to_d(B[gk + (int64_t)gj * pr.k]) : 0.0;
+            }
+            __syncthreads();
+            #pragma unroll
+            for (int kk = 0; kk < GT_K; ++kk) {
+                double av[4], bv[4];
+                #pragma unroll
+                for (int a = 0; a < 4; ++a) av[a] = As[kk][tx + 16 * a];
+                #pragma unroll
+                for (int c = 0; c < 4; ++c) bv[c] = Bs[kk][ty + 16 * c];
+                #pragma unroll
+                for (int a = 0; a < 4; ++a)
+                    #pragma unroll
+                    for (int c = 0; c < 4; ++c) acc[a][c] = fma(av[a], bv[c], acc[a][c]);
+            }
+            __syncthreads();
+        }
+    }
+    #pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const int gj = j0 + ty + 16 * c;
+        if (gj >= t.n) continue;
+        #pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const int gi = i0 + tx + 16 * a;
+            if (gi >= t.m) continue;
+            const int64_t o = gi + (int64_t)gj * t.m;
+            double v = sgn * acc[a][c];
+            if (t.cinit_off >= 0) v = Cinit[t.cinit_off + o] + v;
+            Cbase[t.c_off + o] = from_d<TC>(v);
+        }
+    }
+}
+
+// In-place inverse of one diagonal block per CTA: Gauss-Jordan with partial
+// (row) pivoting, restated from the textbook algorithm.  The pivot of column
+// k is the entry of largest magnitude among rows not yet used as pivots
+// (first such row on ties), which is the pivot DGETRF selects.  Rows are not
+// swapped physically: each thread keeps a fixed RPL x CPW register tile
+// (rows lane + 32*ri, columns warp + NW*cj) and the permutation is undone
+// when the result is written.  A zero pivot records the element in *status
+// (ESINGULAR) and leaves garbage, never traps.
+template <int RPL, int CPW, int NW>
+__global__ void __launch_bounds__(NW * 32) k_block_inverse(double* __restrict__ LD, const int64_t* __restrict__ dinv_off,
+                                                           const int32_t* __restrict__ prow_b,
+                                                           const int32_t* __restrict__ prow_elem,
+                                                           const int32_t* __restrict__ rows, int row_begin,
+                                                           int* __restrict__ status) {
+    constexpr int RMAX = 32 * RPL, CMAX = NW * CPW;
+    __shared__ double colbuf[2][RMAX];
+    __shared__ double rowbuf[2][CMAX];
+    __shared__ int used[RMAX];
+    __shared__ int pivrow[CMAX > RMAX ? CMAX : RMAX];
+    __shared__ int qinv[RMAX];
+    __shared__ int s_p;
+    __shared__ double s_piv;
+    const int prow = rows[row_begin + blockIdx.x];
+    const int b = prow_b[prow];
+    double* D = LD + dinv_off[prow];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double a[RPL][CPW];
+    #pragma unroll
+    for (int ri = 0; ri < RPL; ++ri)
+        #pragma unroll
+        for (int cj = 0; cj < CPW; ++cj) {
+            const int i = lane + 32 * ri, j = w + NW * cj;
+            a[ri][cj] = (i < b && j < b) ? D[i + (int64_t)j * b] : 0.0;
+        }
+    for (int i = threadIdx.x; i < RMAX; i += blockDim.x) used[i] = 0;
+    bool singular = false;
+    __syncthreads();
+    for (int k = 0; k < b; ++k) {
+        const int wk = k % NW, ck = k / NW, buf = k & 1;
+        if (w == wk) {
+            double best = -1.0;
+            int bi = 0x7fffffff;
+            #pragma unroll
+            for (int ri = 0; ri < RPL; ++ri) {
+                const int i = lane + 32 * ri;
+                double v = -1.0;
+                #pragma unroll
+                for (int cj = 0; cj < CPW; ++cj) if (cj == ck) v = fabs(a[ri][cj]);
+                if (!(v == v)) v = INFINITY;   // a NaN entry is taken as pivot so the NaN propagates
+                if (i < b && !used[i] && (v > best || (v == best && i < bi))) { best = v; bi = i; }
+            }
+            #pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+            }
+            if (lane == (bi & 31)) {
+                const int rp = bi >> 5;
+                double pv = 0.0;
+                #pragma unroll
+                for (int ri = 0; ri < RPL; ++ri)
+                    #pragma unroll
+                    for (int cj = 0; cj < CPW; ++cj) if (ri == rp && cj == ck) pv = a[ri][cj];
+                s_p = bi;
+                s_piv = pv;
+                used[bi] = 1;
+                pivrow[k] = bi;
+            }
+        }
+        __syncthreads();
+        const int p = s_p;
+        double piv = s_piv;
+        if (piv == 0.0) { singular = true; piv = 1.0; }
+        const double rp = 1.0 / piv;
+        if (lane == (p & 31)) {
+            const int rip = p >> 5;
+            #pragma unroll
+            for (int cj = 0; cj < CPW; ++cj) {
+                const int j = w + NW * cj;
+                double v = 0.0;
+                #pragma unroll
+                for (int ri = 0; ri < RPL; ++ri) if (ri == rip) v = a[ri][cj];
+                if (j == k) v = 1.0;
+                if (j < CMAX) rowbuf[buf][j] = v * rp;
+            }
+        }
+        if (w == wk) {
+            #pragma unroll
+            for (int ri = 0; ri < RPL; ++ri) {
+                const int i = lane + 32 * ri;
+                double v = 0.0;
+                #pragma unroll
+                for (int cj = 0; cj < CPW; ++cj) if (cj == ck) v = a[ri][cj];
+                colbuf[buf][i] = (i == p) ? 0.0 : v;
+            }
+        }
+        __syncthreads();
+        #pragma unroll
+        for (int ri = 0; ri < RPL; ++ri) {
+            const int i = lane + 32 * ri;
+            const double f = colbuf[buf][i];
+            #pragma unroll
+            for (int cj = 0; cj < CPW; ++cj) {
+                const int j = w + NW * cj;
+                const double rv = rowbuf[buf][j];
+                if (i == p) a[ri][cj] = rv;
+                else {
+                    const double base = (j == k) ? 0.0 : a[ri][cj];
+                    a[ri][cj] = fma(-f, rv, base);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < b; k += blockDim.x) qinv[pivrow[k]] = k;
+    __syncthreads();
+    #pragma unroll
+    for (int ri = 0; ri < RPL; ++ri)
+        #pragma unroll
+        for (int cj = 0; cj < CPW; ++cj) {
+            const int i = lane + 32 * ri, j = w + NW * cj;
+            if (i < b && j < b) D[qinv[i] + (int64_t)pivrow[j] * b] = a[ri][cj];
+        }
+    if (singular && threadIdx.x == 0) atomicMin(status, prow_elem[prow]);
+}
+
+// Same algorithm for blocks too large for the register tiles (b > 160):
+// one CTA, matrix kept in global memory (L2 resident), explicit row swaps.
+static __global__ void k_block_inverse_global(double* __restrict__ LD, const int64_t* __restrict__ dinv_off,
+                                       const int32_t* __restrict__ prow_b, const int32_t* __restrict__ prow_elem,
+                                       const int32_t* __restrict__ rows, int row_begin, int* __restrict__ status,
+                                       int* __restrict__ piv_scratch) {
+    __shared__ double sv[32];
+    __shared__ int si[32];
+    __shared__ int s_p;
+    __shared__ double colk[1024];
+    const int prow = rows[row_begin + blockIdx.x];
+    const int b = prow_b[prow];
+    double* D = LD + dinv_off[prow];
+    int* piv = piv_scratch + (int64_t)blockIdx.x * 1024;
+    bool singular = false;
+    for (int k = 0; k < b; ++k) {
+        double best = -1.0; int bi = 0x7fffffff;
+        for (int i = k + threadIdx.x; i < b; i += blockDim.x) {
+            double v = fabs(D[i + (int64_t)k * b]);
+            if (!(v == v)) v = INFINITY;
+            if (v > best || (v == best && i < bi)) { best = v; bi = i; }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+        }
+        if ((threadIdx.x & 31) == 0) { sv[threadIdx.x >> 5] = best; si[threadIdx.x >> 5] = bi; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double bb = -1.0; int ii = 0x7fffffff;
+            for (int q = 0; q < (int)(blockDim.x >> 5); ++q)
+                if (sv[q] > bb || (sv[q] == bb && si[q] < ii)) { bb = sv[q]; ii = si[q]; }
+            s_p = ii;
+            piv[k] = ii;
+        }
+        __syncthreads();
+        const int p = s_p;
+        if (p != k)
+            for (int j = threadIdx.x; j < b; j += blockDim.x) {
+                const double t = D[k + (int64_t)j * b];
+                D[k + (int64_t)j * b] = D[p + (int64_t)j * b];
+                D[p + (int64_t)j * b] = t;
+            }
+        __syncthreads();
+        double pv = D[k + (int64_t)k * b];
+        if (pv == 0.0) { singular = true; pv = 1.0; }
+        const double rp = 1.0 / pv;
+        __syncthreads();
+        for (int i = threadIdx.x; i < b; i += blockDim.x) colk[i] = (i == k) ? 0.0 : D[i + (int64_t)k * b];
+        __syncthreads();
+        for (int j = threadIdx.x; j < b; j += blockDim.x) {
+            const double v = (j == k) ? 1.0 : D[k + (int64_t)j * b];
+            D[k + (int64_t)j * b] = v * rp;
+        }
+        __syncthreads();
+        // row k is final for this step; every other row reads its multiplier
+        // from the saved column, so column k can be overwritten in place
+        for (int idx = threadIdx.x; idx < b * b; idx += blockDim.x) {
+            const int i = idx % b, j = idx / b;
+            if (i == k) continue;
+            const double base = (j == k) ? 0.0 : D[i + (int64_t)j * b];
+            D[i + (int64_t)j * b] = base - colk[i] * D[k + (int64_t)j * b];
+        }
+        __syncthreads();
+    }
+    // undo the row interchanges as column interchanges, last first
+    for (int k = b - 1; k >= 0; --k) {
+        const int p = piv[k];
+        if (p != k)
+            for (int i = threadIdx.x; i < b; i += blockDim.x) {
+                const double t = D[i + (int64_t)k * b];
+                D[i + (int64_t)k * b] = D[i + (int64_t)p * b];
+                D[i + (int64_t)p * b] = t;
+            }
+        __syncthreads();
+    }
+    if (singular && threadIdx.x == 0) atomicMin(status, prow_elem[prow]);
+}
+
+// ---------------------------------------------------------------------------
+// ILU programme: triangular sweeps, one CTA per programme row of a level.
+//  forward:  z_r = v_r - sum_lower L z_parent                 (precon_ILU0.f90:336-359)
+//  backward: z_r = Dinv_r (z_r - sum_upper U z_parent)         (precon_ILU0.f90:363-398)
+// Thread layout as in k_matvec.  TL = factor storage, TU = A storage.
+// ---------------------------------------------------------------------------
+struct IluRows {
+    const int32_t* prow_b;
+    const int64_t* v_off;      // source of v (vector offset of the element row)
+    const int64_t* z_off;      // work offset (extended vector)
+    const int64_t* dinv_off;   // in LD
+    const int32_t* lo_ptr;     // [nprow+1]
+    const int64_t* lo_L;       // L block in LD
+    const int32_t* lo_par;     // parent programme row
+    const int32_t* lo_nc;
+    const int32_t* up_ptr;
+    const int64_t* up_U;       // U block in A
+    const int32_t* up_par;
+    const int32_t* up_nc;
+};
+
+template <typename TL, typename TX, typename ACC>
+__global__ void k_ilu_forward(IluRows R, const TL* __restrict__ LD, const int32_t* __restrict__ rows, int row_begin,
+                              const TX* __restrict__ v, TX* __restrict__ zx) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ACC* xs = reinterpret_cast<ACC*>(smem_raw);
+    const int pr = rows[row_begin + blockIdx.x];
+    const int b = R.prow_b[pr];
+    const int q0 = R.lo_ptr[pr], q1 = R.lo_ptr[pr + 1];
+    const int tid = threadIdx.x;
+    int off = 0;
+    for (int q = q0; q < q1; ++q) {
+        const int nc = R.lo_nc[q];
+        const TX* zp = zx + R.z_off[R.lo_par[q]];
+        for (int c = tid; c < nc; c += blockDim.x) xs[off + c] = cvt<ACC>(zp[c]);
+        off += nc;
+    }
+    const int ncols_total = off;
+    __syncthreads();
+    const int G = blockDim.x / b;
+    const int r = tid % b, g = tid / b;
+    ACC acc = 0;
+    if (g < G) {
+        off = 0;
+        for (int q = q0; q < q1; ++q) {
+            const int nc = R.lo_nc[q];
+            const TL* Lb = LD + R.lo_L[q] + r;
+            const ACC* xb = xs + off;
+            int c = g;
+            for (; c + 3 * G < nc; c += 4 * G) {
+                const TL a0 = ld_stream(Lb + (int64_t)c * b);
+                const TL a1 = ld_stream(Lb + (int64_t)(c + G) * b);
+                const TL a2 = ld_stream(Lb + (int64_t)(c + 2 * G) * b);
+                const TL a3 = ld_stream(Lb + (int64_t)(c + 3 * G) * b);
+                acc += cvt<ACC>(a0) * xb[c];
+                acc += cvt<ACC>(a1) * xb[c + G];
+                acc += cvt<ACC>(a2) * xb[c + 2 * G];
+                acc += cvt<ACC>(a3) * xb[c + 3 * G];
+            }
+            for (; c < nc; c += G) acc += cvt<ACC>(ld_stream(Lb + (int64_t)c * b)) * xb[c];
+            off += nc;
+        }
+    }
+    ACC* red = xs + ncols_total;
+    if (g < G) red[g * b + r] = acc;
+    __syncthreads();
+    if (tid < b) {
+        ACC s = 0;
+        for (int gg = 0; gg < G; ++gg) s += red[gg * b + tid];
+        const double out = to_d(v[R.v_off[pr] + tid]) - (double)s;
+        zx[R.z_off[pr] + tid] = from_d<TX>(out);
+    }
+}
+
+template <typename TL, typename TU, typename TX, typename ACC>
+__global__ void k_ilu_backward(IluRows R, const TL* __restrict__ LD, const TU* __restrict__ Aval,
+                               const int32_t* __restrict__ rows, int row_begin, TX* __restrict__ zx) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ACC* xs = reinterpret_cast<ACC*>(smem_raw);
+    const int pr = rows[row_begin + blockIdx.x];
+    const int b = R.prow_b[pr];
+    const int q0 = R.up_ptr[pr], q1 = R.up_ptr[pr + 1];
+    const int tid = threadIdx.x;
+    int off = 0;
+    for (int q = q0; q < q1; ++q) {
+        const int nc = R.up_nc[q];
+        const TX* zp = zx + R.z_off[R.up_par[q]];
+        for (int c = tid; c < nc; c += blockDim.x) xs[off + c] = cvt<ACC>(zp[c]);
+        off += nc;
+    }
+    const int ncols_total = off;
+    ACC* tvec = xs + ncols_total;          // b entries
+    ACC* red = tvec + b;                   // G*b entries
+    __syncthreads();
+    const int G = blockDim.x / b;
+    const int r = tid % b, g = tid / b;
+    ACC acc = 0;
+    if (g < G) {
+        off = 0;
+        for (int q = q0; q < q1; ++q) {
+            const int nc = R.up_nc[q];
+            const TU* Ub = Aval + R.up_U[q] + r;
+            const ACC* xb = xs + off;
+            int c = g;
+            for (; c + 3 * G < nc; c += 4 * G) {
+                const TU a0 = ld_stream(Ub + (int64_t)c * b);
+                const TU a1 = ld_stream(Ub + (int64_t)(c + G) * b);
+                const TU a2 = ld_stream(Ub + (int64_t)(c + 2 * G) * b);
+                const TU a3 = ld_stream(Ub + (int64_t)(c + 3 * G) * b);
+                acc += cvt<ACC>(a0) * xb[c];
+                acc += cvt<ACC>(a1) * xb[c + G];
+                acc += cvt<ACC>(a2) * xb[c + 2 * G];
+                acc += cvt<ACC>(a3) * xb[c + 3 * G];
+            }
+            for (; c < nc; c += G) acc += cvt<ACC>(ld_stream(Ub + (int64_t)c * b)) * xb[c];
+            off += nc;
+        }
+        red[g * b + r] = acc;
+    }
+    __syncthreads();
+    if (tid < b) {
+        ACC s = 0;
+        for (int gg = 0; gg < G; ++gg) s += red[gg * b + tid];
+        const double t = to_d(zx[R.z_off[pr] + tid]) - (double)s;
+        tvec[tid] = cvt<ACC>(from_d<TX>(t));
+    }
+    __syncthreads();
+    acc = 0;
+    if (g < G) {
+        const TL* Db = LD + R.dinv_off[pr] + r;
+        int c = g;
+        for (; c + 3 * G < b; c += 4 * G) {
+            const TL a0 = ld_stream(Db + (int64_t)c * b);
+            const TL a1 = ld_stream(Db + (int64_t)(c + G) * b);
+            const TL a2 = ld_stream(Db + (int64_t)(c + 2 * G) * b);
+            const TL a3 = ld_stream(Db + (int64_t)(c + 3 * G) * b);
+            acc += cvt<ACC>(a0) * tvec[c];
+            acc += cvt<ACC>(a1) * tvec[c + G];
+            acc += cvt<ACC>(a2) * tvec[c + 2 * G];
+            acc += cvt<ACC>(a3) * tvec[c + 3 * G];
+        }
+        for (; c < b; c += G) acc += cvt<ACC>(ld_stream(Db + (int64_t)c * b)) * tvec[c];
+    }
+    __syncthreads();
+    if (g < G) red[g * b + r] = acc;
+    __syncthreads();
+    if (tid < b) {
+        ACC s = 0;
+        for (int gg = 0; gg < G; ++gg) s += red[gg * b + tid];
+        zx[R.z_off[pr] + tid] = from_d<TX>((double)s);
+    }
+}
+
+}  // namespace chidg

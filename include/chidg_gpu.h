@@ -1,0 +1,230 @@
+/*
+ * chidg_gpu.h -- C ABI of the B200-native implicit linear-solve path for ChiDG.
+ *
+ * The entry points are what ChiDG's Fortran host code binds through
+ * iso_c_binding when the container backend is 'cuda' (a third option next to
+ * 'native' and 'petsc', selected by mod_io::backend).  Each group below names
+ * the reference interface it replaces (paths relative to the ChiDG source
+ * tree).  The Fortran binding module is interfaces/chidg_gpu_mod.f90.
+ *
+ * Conventions
+ *  - Every function returns an int status: CHIDG_GPU_OK (0) or an error code.
+ *    Nothing here aborts; the Fortran shim maps a nonzero code onto
+ *    chidg_signal(FATAL, ...) exactly where the reference would stop
+ *    (src/tools/messenger.f90:968-977).
+ *  - Host arrays are owned by the caller and only read (or written, for
+ *    outputs) during the call.  Device objects are opaque library handles,
+ *    released by the matching _destroy call (the reference's tear_down/release).
+ *  - Handles are not thread safe.  A context owns one CUDA stream (the caller
+ *    may pass its own); all work of objects made from that context is ordered
+ *    on it.  Concurrency comes from several contexts.
+ *  - Element numbering is 0-based over all domains of the mesh (flattened
+ *    reference element order).  The vector of an element holds ntime levels
+ *    of nvars fields x nterms modes: time-major, then field, then mode
+ *    (densevector_t%get_time_start, src/containers/type_densevector.f90:208).
+ *  - A block couples row (element, time) to column (element, time); it is an
+ *    nrows x ncols column-major FP64 array (Fortran storage of
+ *    densematrix_t%mat), nrows = nvars*nterms of the row element.
+ */
+#ifndef CHIDG_GPU_H
+#define CHIDG_GPU_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define CHIDG_GPU_OK            0
+#define CHIDG_GPU_EINVAL        1  /* bad argument / inconsistent pattern            */
+#define CHIDG_GPU_ENOMEM        2  /* device or pinned host allocation failed        */
+#define CHIDG_GPU_ESINGULAR     3  /* zero pivot in a block inverse (mod_inv::inv)   */
+#define CHIDG_GPU_ENONFINITE    4  /* NaN/Inf residual (type_newton.f90:197-200)     */
+#define CHIDG_GPU_ETIMEOUT      5  /* a bounded device wait ran out                  */
+#define CHIDG_GPU_ENOTCONVERGED 6  /* iteration cap reached before tol/rtol          */
+#define CHIDG_GPU_ECUDA         7  /* CUDA runtime error (message via last_error)    */
+#define CHIDG_GPU_ESTATE        8  /* object used in the wrong state                 */
+
+/* ---- block kinds: the four storage groups of domain_matrix_t
+ *      (src/containers/type_domain_matrix.f90:32-40) ---------------------- */
+#define CHIDG_BLK_LOCAL   0   /* lblks: interior face neighbours + DIAG      */
+#define CHIDG_BLK_CHIMERA 1   /* chi_blks                                    */
+#define CHIDG_BLK_BC      2   /* bc_blks                                     */
+#define CHIDG_BLK_HB      3   /* hb_blks (cross time-level coupling)         */
+
+/* ---- preconditioner kinds: names of create_preconditioner
+ *      (src/preconditioners/mod_preconditioner.f90:49-108) ---------------- */
+#define CHIDG_PRECON_IDENTITY 0   /* 'identity' */
+#define CHIDG_PRECON_JACOBI   1   /* 'jacobi'   */
+#define CHIDG_PRECON_ILU0     2   /* 'ilu0'     */
+#define CHIDG_PRECON_RASILU0  3   /* 'rasilu0'  */
+
+/* ---- precision modes ----------------------------------------------------- */
+#define CHIDG_GPU_FP64        0   /* everything FP64 (the plain GPU path)               */
+#define CHIDG_GPU_MIXED_FP32  1   /* FP64 outer FGMRES; FP32 inner FGMRES, matvec and
+                                     ILU factors with FP32 accumulation                 */
+#define CHIDG_GPU_MIXED_BF16  2   /* as MIXED_FP32 but the ILU factors stored in BF16   */
+
+#define CHIDG_ORTH_CGS 0
+#define CHIDG_ORTH_MGS 1
+
+typedef struct chidg_gpu_ctx    chidg_gpu_ctx;
+typedef struct chidg_gpu_matrix chidg_gpu_matrix;
+typedef struct chidg_gpu_vector chidg_gpu_vector;
+typedef struct chidg_gpu_precon chidg_gpu_precon;
+
+/* Block pattern of a chidg_matrix_t.  Blocks are listed row by row in the
+ * reference storage order: for each (element, time) row the lblks in face
+ * order XI_MIN, XI_MAX, ETA_MIN, ETA_MAX, ZETA_MIN, ZETA_MAX, DIAG (boundary
+ * faces absent), then chi_blks, bc_blks, hb_blks
+ * (type_domain_matrix.f90:102-632).  elem_proc gives the MPI rank that owns
+ * each element (its RAS subdomain); NULL means every element on rank 0. */
+typedef struct {
+    int32_t        nelem;
+    int32_t        ntime;
+    const int32_t* elem_nvars;     /* [nelem] */
+    const int32_t* elem_nterms;    /* [nelem] */
+    const int32_t* elem_proc;      /* [nelem] or NULL */
+    int64_t        nblocks;
+    const int32_t* blk_row_elem;   /* [nblocks] */
+    const int32_t* blk_row_time;   /* [nblocks] */
+    const int32_t* blk_col_elem;   /* [nblocks] eparent */
+    const int32_t* blk_col_time;   /* [nblocks] tparent */
+    const int32_t* blk_kind;       /* [nblocks] CHIDG_BLK_* */
+} chidg_gpu_pattern;
+
+/* Options of linear_solver_t (src/linear_solvers/type_linear_solver.f90:21-40,
+ * set by linear_solver%set :113-131). */
+typedef struct {
+    double  tol;                      /* absolute, |p(j+1)| < tol            */
+    double  rtol;                     /* relative to the first r0 norm       */
+    int32_t nmax;                     /* iteration cap, <= 0 = unlimited     */
+    int32_t nkrylov;                  /* restart length                      */
+    int32_t orthogonalization;        /* CHIDG_ORTH_CGS / CHIDG_ORTH_MGS     */
+    int32_t inner_fgmres;             /* 1 = inner FGMRES correction         */
+    double  inner_tol;
+    double  inner_rtol;
+    int32_t inner_nmax;
+    int32_t inner_nkrylov;
+    int32_t inner_orthogonalization;
+    int32_t use_controller;           /* 1 = refresh M only if A's stamp changed
+                                         (solver_controller%update_preconditioner);
+                                         0 = refresh on every call, as without a
+                                         controller (type_fgmres.f90:118-122)   */
+    int32_t precision;                /* CHIDG_GPU_FP64 / _MIXED_FP32 / _MIXED_BF16 */
+    int32_t mixed_inner_nkrylov;      /* mixed: Krylov length of the FP32 inner solve */
+    double  mixed_inner_rtol;         /* mixed: relative tolerance of the inner solve */
+    int32_t mixed_inner_nmax;         /* mixed: iteration cap of the inner solve      */
+} chidg_gpu_fgmres_opts;
+
+/* Result of one solve: fgmres_t%niter, %residual_norm and the |p(j+1)|
+ * history the reference prints at verbosity >= 4. */
+typedef struct {
+    int32_t niter;           /* outer iterations (fgmres_t%niter)               */
+    int32_t nrestart;
+    int32_t inner_iters;     /* total inner iterations (inner FGMRES / mixed)   */
+    int32_t nhist;           /* entries written into hist                       */
+    double  residual_norm;   /* true ||b - A x|| in FP64 (print_report)         */
+    double  res_estimate;    /* |p(j+1)| at exit                                */
+    double  r0norm_initial;
+    double  seconds;         /* wall time of the call                           */
+} chidg_gpu_fgmres_result;
+
+/* ---- context ------------------------------------------------------------ */
+/* Create a context on `device`.  `stream` is a cudaStream_t to order work on,
+ * or NULL to let the library create one. */
+int chidg_gpu_ctx_create(int device, void* stream, chidg_gpu_ctx** out);
+int chidg_gpu_ctx_destroy(chidg_gpu_ctx* ctx);
+int chidg_gpu_ctx_sync(chidg_gpu_ctx* ctx);
+/* Copy the last error message (NUL-terminated) into buf. */
+int chidg_gpu_last_error(chidg_gpu_ctx* ctx, char* buf, int32_t buflen);
+/* Element id (0-based) of the last ESINGULAR / ENONFINITE, or -1. */
+int chidg_gpu_error_element(chidg_gpu_ctx* ctx, int32_t* elem);
+/* Number of kernels this context has launched so far. */
+int chidg_gpu_launch_count(chidg_gpu_ctx* ctx, int64_t* count);
+/* Page-locked host memory for the upload / download calls. */
+int chidg_gpu_host_alloc(size_t bytes, void** out);
+int chidg_gpu_host_free(void* p);
+
+/* ---- chidg_matrix_t (src/containers/type_chidg_matrix.f90) --------------- */
+/* replaces chidg_matrix%init (:221-248) for backend='cuda' */
+int chidg_gpu_matrix_create(chidg_gpu_ctx* ctx, const chidg_gpu_pattern* pat,
+                            chidg_gpu_matrix** out);
+int chidg_gpu_matrix_destroy(chidg_gpu_matrix* A);
+/* Number of FP64 values of the packed block array (sum of nrows*ncols). */
+int chidg_gpu_matrix_nvalues(chidg_gpu_matrix* A, int64_t* nvalues);
+/* Vector length (sum over elements of ntime*nvars*nterms). */
+int chidg_gpu_matrix_nvec(chidg_gpu_matrix* A, int64_t* n);
+/* Upload all blocks, packed in pattern order, each column-major (the
+ * storage that chidg_matrix%store* fills, :575-747).  `host` may be pageable
+ * or pinned host memory.  Updates the stamp (chidg_matrix_t%stamp). */
+int chidg_gpu_matrix_upload(chidg_gpu_matrix* A, const double* host);
+/* Same, one host pointer per block (each densematrix_t%mat allocation). */
+int chidg_gpu_matrix_upload_blocks(chidg_gpu_matrix* A, const double* const* block_ptrs);
+/* Same, from a packed device array already resident on this GPU. */
+int chidg_gpu_matrix_upload_device(chidg_gpu_matrix* A, const double* dev);
+/* Download the packed blocks into host memory. */
+int chidg_gpu_matrix_download(chidg_gpu_matrix* A, double* host);
+/* chidg_matrix%clear (:841): zero all blocks, bump the stamp. */
+int chidg_gpu_matrix_clear(chidg_gpu_matrix* A);
+/* chidg_matrix%scale_diagonal (:769-792), the pseudo-transient term: for
+ * every element e and time t, add scale[e] * mass_e to each field's
+ * nterms x nterms diagonal sub-block of the DIAG block.  mass is packed per
+ * element, nterms*nterms column-major; bump the stamp. */
+int chidg_gpu_matrix_scale_diagonal(chidg_gpu_matrix* A, const double* mass,
+                                    const double* scale);
+int chidg_gpu_matrix_stamp(chidg_gpu_matrix* A, int64_t* stamp);
+
+/* ---- chidg_vector_t (src/containers/type_chidg_vector.f90) --------------- */
+int chidg_gpu_vector_create(chidg_gpu_matrix* A, chidg_gpu_vector** out);
+int chidg_gpu_vector_destroy(chidg_gpu_vector* x);
+int chidg_gpu_vector_upload(chidg_gpu_vector* x, const double* host);
+int chidg_gpu_vector_download(chidg_gpu_vector* x, double* host);
+/* Attach/read device memory directly (n doubles on this GPU). */
+int chidg_gpu_vector_upload_device(chidg_gpu_vector* x, const double* dev);
+int chidg_gpu_vector_device_ptr(chidg_gpu_vector* x, double** dev);
+int chidg_gpu_vector_clear(chidg_gpu_vector* x);                               /* %clear  */
+int chidg_gpu_vector_copy(chidg_gpu_vector* dst, const chidg_gpu_vector* src); /* =       */
+int chidg_gpu_vector_axpy(chidg_gpu_vector* y, double a, const chidg_gpu_vector* x); /* y += a x */
+int chidg_gpu_vector_scale(chidg_gpu_vector* x, double a);                      /* x = a x */
+/* operator_chidg_dot.f90:30-97 (dot) and type_chidg_vector.f90:1237-1305 (norm) */
+int chidg_gpu_vector_dot(const chidg_gpu_vector* x, const chidg_gpu_vector* y, double* out);
+int chidg_gpu_vector_norm(const chidg_gpu_vector* x, double* out);
+
+/* ---- chidg_mv (src/containers/operator_chidg_mv.f90:46-645) --------------- */
+/* y = A x over lblks, chi_blks, bc_blks and hb_blks (hb at tparent). */
+int chidg_gpu_matvec(chidg_gpu_matrix* A, const chidg_gpu_vector* x, chidg_gpu_vector* y);
+
+/* ---- preconditioner_t (src/preconditioners/type_preconditioner.f90:21-121) */
+/* create + init: precon_ILU0%init (precon_ILU0.f90:64-90),
+ * precon_RASILU0%init (RASILU0/precon_RASILU0.f90:139-182), precon_jacobi%init. */
+int chidg_gpu_precon_create(chidg_gpu_matrix* A, int32_t kind, chidg_gpu_precon** out);
+int chidg_gpu_precon_destroy(chidg_gpu_precon* M);                  /* %tear_down */
+/* %update(A,b): ILU0 factorisation (precon_ILU0.f90:111-265) or RAS
+ * factorisation with overlap rows (precon_RASILU0.f90:205-415).  `precision`
+ * selects the factor storage: CHIDG_GPU_FP64, _MIXED_FP32 or _MIXED_BF16. */
+int chidg_gpu_precon_update(chidg_gpu_precon* M, chidg_gpu_matrix* A, int32_t precision);
+/* %apply(A,v) -> z: precon_ILU0.f90:286-411 / precon_RASILU0.f90:454-625. */
+int chidg_gpu_precon_apply(chidg_gpu_precon* M, chidg_gpu_matrix* A,
+                           const chidg_gpu_vector* v, chidg_gpu_vector* z);
+/* Packed factor blocks (L blocks and inverted diagonals at the positions of
+ * the matrix's LOCAL blocks, zero elsewhere), as precon_ILU0_t%LD holds them. */
+int chidg_gpu_precon_download_LD(chidg_gpu_precon* M, double* host);
+int chidg_gpu_precon_stamp(chidg_gpu_precon* M, int64_t* stamp);
+
+/* ---- fgmres_t%solve (src/linear_solvers/type_fgmres.f90:81-310) ----------- */
+/* Solve A x = b.  x is zeroed on entry (:132-136).  M is refreshed as the
+ * options say; opts == NULL uses the reference defaults of linear_solver_t. */
+int chidg_gpu_fgmres_solve(chidg_gpu_matrix* A, chidg_gpu_precon* M,
+                           const chidg_gpu_vector* b, chidg_gpu_vector* x,
+                           const chidg_gpu_fgmres_opts* opts,
+                           chidg_gpu_fgmres_result* result,
+                           double* hist, int32_t hist_cap);
+/* Fill opts with the reference defaults (type_linear_solver.f90:23-40). */
+int chidg_gpu_fgmres_default_opts(chidg_gpu_fgmres_opts* opts);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CHIDG_GPU_H */
