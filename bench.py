@@ -1,0 +1,429 @@
+"""Benchmark of the B200 linear-solve path on the 24^3 P2 Euler-sized workload.
+
+One step = one Newton linear solve: the block-ILU0 factorisation of a freshly
+assembled Jacobian followed by FGMRES(50) to a relative residual of 1e-8 and
+the true-residual check, all in FP64 (the plain GPU path).  Workload: 24x24x24
+hex box, 5 fields, P2 (27 modes) -> 13 824 elements, 93 312 blocks of
+135 x 135, 13.6 GB of FP64 blocks, seeded synthetic values with the ChiDG
+block layout (no reference-assembled Jacobians exist in this environment).
+
+Prints one JSON line (rank 0).  `value` times the solves with A and b resident
+in HBM; `e2e` times the same solves through the C ABI from pinned host
+buffers, host->device upload of A and b and download of x included.
+`--impl reference` times the CPU FP64 oracle (the restatement of the
+reference solver; the Fortran original cannot be built here) on the host
+cores with bounded samples of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Newton-Krylov solves/s + p50/p99 latency, mixed vs FP64 GPU at 1e-8 residual"
+NX = NY = NZ = 24
+P = 2
+NVARS = 5
+SEED_A, SEED_B = 1, 2
+SOLVER = dict(tol=0.0, rtol=1e-8, nkrylov=50, inner_fgmres=0, nmax=500, orthogonalization="CGS",
+              use_controller=0)
+MIXED = dict(nkrylov=10, mixed_inner_nkrylov=30, mixed_inner_rtol=1e-2, mixed_inner_nmax=60)
+SAMPLE_N = 8            # cpu sample: 8^3 box with the same block size
+
+
+def workload_config(extra=None):
+    cfg = {"workload": "24^3 hex box, 5 fields, P2 (135x135 blocks, 93312 blocks, 13.6 GB FP64), "
+                       "block-ILU0 factorisation + FGMRES(50) to rtol 1e-8, CGS, no inner FGMRES",
+           "elements": NX * NY * NZ, "block": NVARS * (P + 1) ** 3, "blocks": 93312,
+           "matrix_bytes_fp64": 13604889600, "l2_flush": "inputs larger than L2 (13.6 GB matrix)",
+           "parallelism": "replicas", "values": "seeded synthetic Jacobian (ChiDG block layout)"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+# ---------------------------------------------------------------------------
+# algorithmic work
+# ---------------------------------------------------------------------------
+def counts(pat):
+    b = int(pat.bsize()[0])
+    E = pat.nelem
+    local = pat.blk_kind == 0
+    nL = int((local & (pat.blk_col_elem < pat.blk_row_elem)).sum())
+    nU = int((local & (pat.blk_col_elem > pat.blk_row_elem)).sum())
+    NB = pat.nblocks
+    return b, E, nL, nU, NB
+
+
+def matvec_bytes(pat, sA=8, sv=8):
+    b, E, nL, nU, NB = counts(pat)
+    return NB * b * b * sA + (NB + E) * b * sv
+
+
+def ilu_apply_bytes(pat, sL=8, sA=8, sv=8):
+    b, E, nL, nU, NB = counts(pat)
+    return (nL + E) * b * b * sL + nU * b * b * sA + 4 * E * b * sv
+
+
+def factor_flops(pat):
+    b, E, nL, nU, NB = counts(pat)
+    return 4 * nL * b ** 3 + 2 * E * b ** 3
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, 1590.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas only: no data-path collective)
+# ---------------------------------------------------------------------------
+def dist_init(n_gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return rank, world, local, pg
+
+
+def barrier(pg, local):
+    if pg is not None:
+        import torch
+        pg.barrier(device_ids=[local])
+        torch.cuda.synchronize()
+
+
+def allmax(pg, v, local):
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# CPU legs (oracle)
+# ---------------------------------------------------------------------------
+def cpu_sample_solve(seed_a=SEED_A, seed_b=SEED_B, n=SAMPLE_N):
+    """One full FGMRES(50)+ILU0 FP64 solve of an n^3 P2 box on one host core."""
+    from chidg_b200 import mesh
+    from oracle import oracle as O
+    pat = mesh.box_pattern(n, n, n, NVARS, mesh.nterms_of_order(P))
+    A = O.OracleMatrix(pat)
+    A.set_values(mesh.synth_values(pat, seed=seed_a, nthreads=1))
+    b = mesh.synth_vector(A.n, seed=seed_b, nthreads=1)
+    opts = {k: v for k, v in SOLVER.items() if k != "orthogonalization"}
+    t0 = time.perf_counter()
+    x, res = O.fgmres(A, O.OraclePrecon(A, "ilu0"), b, O.default_opts(**opts))
+    dt = time.perf_counter() - t0
+    return dt, res["niter"]
+
+
+def cpu_solves_per_s(dt_sample, n_sample=SAMPLE_N):
+    """Scale a sample solve to the 24^3 workload: time grows with the element
+    count at equal iteration count (every kernel is linear in the elements)."""
+    return 1.0 / (dt_sample * (NX * NY * NZ) / n_sample ** 3)
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    cores = max(1, len(os.sched_getaffinity(0)))
+    threads = min(cores, 16)
+
+    def one(results, i):
+        results[i] = cpu_sample_solve()
+
+    times = []
+    for step in range(args.warmup + args.steps):
+        results = [None] * threads
+        th = [threading.Thread(target=one, args=(results, i)) for i in range(threads)]
+        t0 = time.perf_counter()
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        wall = time.perf_counter() - t0
+        if step >= args.warmup:
+            times.append(wall)
+    per_step = float(np.mean(times))
+    niter = results[0][1]
+    # `threads` independent sample solves per step, each 1/27 of the workload
+    value = threads * cpu_solves_per_s(per_step)
+    sample = (f"{threads} concurrent {SAMPLE_N}^3 P2 FGMRES(50)+ILU0 FP64 solves ({niter} iterations each) per step, "
+              f"scaled by element count to 24^3")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config({"precision": "fp64", "implementation": "CPU FP64 oracle (restated reference solver)"}),
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU leg
+# ---------------------------------------------------------------------------
+def run_gpu(args):
+    import torch
+
+    from chidg_b200 import _lib, api, mesh
+    rank, world, local, pg = dist_init(args.gpus)
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    ctx = api.Context(local, stream=stream.cuda_stream)
+    pat = mesh.box_pattern(NX, NY, NZ, NVARS, mesh.nterms_of_order(P))
+    nval = pat.value_offsets()[1]
+    n = pat.vector_size()
+
+    # pinned host copies of the inputs (the e2e leg uploads these every step)
+    hv = torch.empty(nval, dtype=torch.float64, pin_memory=True)
+    hb = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    hx = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    mesh.synth_values(pat, seed=SEED_A + 1000 * rank, out=hv.numpy())
+    mesh.synth_vector(n, seed=SEED_B + 1000 * rank, out=hb.numpy())
+
+    A = api.ChidgMatrix(pat, ctx)
+    A.upload(hv.numpy())
+    b = api.ChidgVector(A, hb.numpy())
+    x = api.ChidgVector(A)
+    M = api.create_preconditioner("ilu0")
+    solver = api.create_linear_solver("fgmres", **SOLVER)
+    L = ctx.L
+
+    def solve():
+        solver.solve(A, x, b, M)
+
+    # warm-up
+    for _ in range(args.warmup):
+        solve()
+    niters = []
+    lat = []
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    clocks = ClockSampler(local)
+    barrier(pg, local)
+    torch.cuda.synchronize()
+    launches0 = ctx.launches()
+    ctx.set_profiling(True)
+    clocks.start()
+    ev[0].record(stream)
+    for _ in range(args.steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        solve()
+        e1.record(stream)
+        niters.append(solver.niter)
+        lat.append((e0, e1))
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    kt = ctx.kernel_times()
+    ctx.set_profiling(False)
+    launches = ctx.launches() - launches0
+    barrier(pg, local)
+    elapsed_ms = ev[0].elapsed_time(ev[1])
+    lat_ms = [a.elapsed_time(bb) for a, bb in lat]
+    elapsed_ms = allmax(pg, elapsed_ms, local)
+    value = world * args.steps / (elapsed_ms / 1000.0)
+    resid = solver.residual_norm / solver.r0norm_initial
+
+    # ---- end to end through the C ABI from pinned host buffers ----
+    nb_e2e = max(1, min(args.steps, 3))
+    barrier(pg, local)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(nb_e2e):
+        ctx.check(L.chidg_gpu_matrix_upload(A.h, api._ptr(hv.numpy())), "upload A")
+        ctx.check(L.chidg_gpu_vector_upload(b.h, api._ptr(hb.numpy())), "upload b")
+        solve()
+        ctx.check(L.chidg_gpu_vector_download(x.h, api._ptr(hx.numpy())), "download x")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = allmax(pg, e0.elapsed_time(e1), local)
+    e2e_value = world * nb_e2e / (e2e_ms / 1000.0)
+
+    # ---- mixed precision (same workload, same 1e-8 target) ----
+    mixed = {}
+    if not args.no_mixed:
+        for prec in ("mixed_fp32", "mixed_bf16"):
+            ms = api.create_linear_solver("fgmres", **{**SOLVER, **MIXED, "precision": prec})
+            xm = api.ChidgVector(A)
+            ms.solve(A, xm, b, M)                      # warm-up
+            torch.cuda.synchronize()
+            m0 = torch.cuda.Event(enable_timing=True)
+            m1 = torch.cuda.Event(enable_timing=True)
+            nm = max(1, min(args.steps, 3))
+            m0.record(stream)
+            for _ in range(nm):
+                ms.solve(A, xm, b, M)
+            m1.record(stream)
+            torch.cuda.synchronize()
+            t = m0.elapsed_time(m1) / nm
+            xm_h = xm.download()
+            x_h = x.download()
+            mixed[prec] = {"solves_per_s": 1000.0 / t, "ms_per_solve": t, "outer_iters": ms.niter,
+                           "inner_iters": ms.inner_iters,
+                           "true_rel_residual": ms.residual_norm / ms.r0norm_initial,
+                           "rel_err_vs_fp64_solution": float(np.linalg.norm(xm_h - x_h) / np.linalg.norm(x_h)),
+                           "speedup_vs_fp64": (elapsed_ms / args.steps) / t}
+        M = api.create_preconditioner("ilu0")   # drop low-precision factors
+
+    if rank != 0:
+        return 0
+
+    hbm, bf16, peak_kind = measured_peaks()
+    mv_ms, mv_n = kt["matvec"]
+    f_ms, f_n = kt["ilu_forward"]
+    bw_ms, bw_n = kt["ilu_backward"]
+    fa_ms, fa_n = kt["factor"]
+    mvb = matvec_bytes(pat)
+    ilub = ilu_apply_bytes(pat)
+    kernels = {
+        "matvec": {"launches": mv_n, "total_ms": mv_ms, "avg_ms": mv_ms / max(mv_n, 1),
+                   "gbs": mvb / (mv_ms / max(mv_n, 1) / 1e3) / 1e9 if mv_n else None},
+        "ilu_apply": {"launches": f_n, "total_ms": f_ms + bw_ms, "avg_ms": (f_ms + bw_ms) / max(f_n, 1),
+                      "gbs": ilub / ((f_ms + bw_ms) / max(f_n, 1) / 1e3) / 1e9 if f_n else None},
+        "factor": {"launches": fa_n, "total_ms": fa_ms, "avg_ms": fa_ms / max(fa_n, 1),
+                   "tflops": factor_flops(pat) / (fa_ms / max(fa_n, 1) / 1e3) / 1e12 if fa_n else None},
+    }
+    # dominant memory-bound kernel by total time: ILU sweeps or matvec
+    if kernels["ilu_apply"]["total_ms"] >= kernels["matvec"]["total_ms"]:
+        dom, dbytes, dms = "ilu_apply (k_ilu_forward+k_ilu_backward, all levels)", ilub, kernels["ilu_apply"]["avg_ms"]
+    else:
+        dom, dbytes, dms = "matvec (k_matvec)", mvb, kernels["matvec"]["avg_ms"]
+    achieved = dbytes / (dms / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            with open(tpath) as f:
+                traffic = json.load(f).get(dom.split()[0])
+        except (OSError, ValueError):
+            traffic = None
+    cpu = None
+    if not args.no_cpu and world == 1:
+        dt, it = cpu_sample_solve()
+        cpu = {"value": cpu_solves_per_s(dt), "unit": "solves/s", "cores": 1, "kind": "port",
+               "sample": f"one {SAMPLE_N}^3 P2 FGMRES(50)+ILU0 FP64 solve on 1 core ({it} iterations, {dt:.1f} s), "
+                         f"scaled by element count to 24^3"}
+    lat_sorted = sorted(lat_ms)
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config({"precision": "fp64", "fgmres_iterations": niters,
+                                   "true_rel_residual": resid}),
+        "latency_ms": {"p50": float(np.percentile(lat_sorted, 50)), "p99": float(np.percentile(lat_sorted, 99))},
+        "clocks": clk,
+        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(nval * 8 + n * 8),
+                "d2h_bytes_per_step": int(n * 8), "steps": nb_e2e},
+        "gpu_launches": launches,
+        "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": dbytes},
+        "kernels": kernels,
+        "mixed": mixed,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision legs")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -57,6 +57,8 @@ PROTOTYPES = {
     "chidg_gpu_last_error": (C.c_int, [VP, C.c_char_p, C.c_int32]),
     "chidg_gpu_error_element": (C.c_int, [VP, I32P]),
     "chidg_gpu_launch_count": (C.c_int, [VP, I64P]),
+    "chidg_gpu_ctx_set_profiling": (C.c_int, [VP, C.c_int32]),
+    "chidg_gpu_ctx_kernel_time": (C.c_int, [VP, C.c_int32, DP, I64P]),
     "chidg_gpu_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(VP)]),
     "chidg_gpu_host_free": (C.c_int, [VP]),
     "chidg_gpu_matrix_create": (C.c_int, [VP, C.POINTER(Pattern), C.POINTER(VP)]),

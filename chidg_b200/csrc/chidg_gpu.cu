@@ -50,6 +50,60 @@ int chidg::grid_for(int64_t n, int threads, int cap) {
     return (int)g;
 }
 
+// CUDA-event timing of kernel classes (chidg_gpu_ctx_set_profiling).
+static cudaEvent_t prof_event(chidg_gpu_ctx* ctx) {
+    if (!ctx->prof_pool.empty()) {
+        cudaEvent_t e = ctx->prof_pool.back();
+        ctx->prof_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+int chidg::prof_begin(chidg_gpu_ctx* ctx, int cls) {
+    if (!ctx->profiling) return -1;
+    EvPair p{prof_event(ctx), prof_event(ctx), cls};
+    cudaEventRecord(p.a, ctx->stream);
+    ctx->prof_pending.push_back(p);
+    return (int)ctx->prof_pending.size() - 1;
+}
+void chidg::prof_end(chidg_gpu_ctx* ctx, int h) {
+    if (h < 0 || h >= (int)ctx->prof_pending.size()) return;
+    cudaEventRecord(ctx->prof_pending[h].b, ctx->stream);
+}
+void chidg::prof_resolve(chidg_gpu_ctx* ctx) {
+    for (auto& p : ctx->prof_pending) {
+        float ms = 0.f;
+        if (cudaEventSynchronize(p.b) == cudaSuccess && cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+            ctx->prof_ms[p.cls] += ms;
+            ctx->prof_count[p.cls]++;
+        }
+        cudaGetLastError();
+        ctx->prof_pool.push_back(p.a);
+        ctx->prof_pool.push_back(p.b);
+    }
+    ctx->prof_pending.clear();
+}
+extern "C" int chidg_gpu_ctx_set_profiling(chidg_gpu_ctx* ctx, int32_t on) {
+    if (!ctx) return CHIDG_GPU_EINVAL;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    prof_resolve(ctx);
+    for (int c = 0; c < kProfClasses; ++c) { ctx->prof_ms[c] = 0.0; ctx->prof_count[c] = 0; }
+    ctx->profiling = on != 0;
+    return CHIDG_GPU_OK;
+}
+extern "C" int chidg_gpu_ctx_kernel_time(chidg_gpu_ctx* ctx, int32_t cls, double* total_ms, int64_t* count) {
+    if (!ctx || cls < 0 || cls >= kProfClasses || !total_ms || !count) return CHIDG_GPU_EINVAL;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    prof_resolve(ctx);
+    *total_ms = ctx->prof_ms[cls];
+    *count = ctx->prof_count[cls];
+    return CHIDG_GPU_OK;
+}
+
 // Two-pass reductions into ctx->d_scal[slot..slot+nq).
 int chidg::reduce_partials(chidg_gpu_ctx* ctx, const double* partial, int ncta, int nq, int slot, bool do_sqrt) {
     k_reduce_partials<<<1, 1024, 0, ctx->stream>>>(partial, ncta, nq, ctx->d_scal + slot, do_sqrt ? 1 : 0);
@@ -122,6 +176,8 @@ extern "C" int chidg_gpu_ctx_destroy(chidg_gpu_ctx* ctx) {
     if (!ctx) return CHIDG_GPU_OK;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    prof_resolve(ctx);
+    for (cudaEvent_t e : ctx->prof_pool) cudaEventDestroy(e);
     release(ctx->partial);
     release(ctx->partial2);
     if (ctx->d_status) cudaFree(ctx->d_status);
@@ -409,10 +465,12 @@ template <typename TA, typename TV>
 int chidg::matvec_launch(chidg_gpu_matrix* A, const TA* val, const TV* x, TV* y, const TV* z, double alpha, double beta, double* row_sq) {
     chidg_gpu_ctx* ctx = A->ctx;
     using ACC = typename AccOf<TV>::type;
-    const size_t smem = sizeof(ACC) * ((size_t)A->max_row_cols + A->mv_threads) + 64;
+    const size_t smem = sizeof(ACC) * ((size_t)A->max_row_cols + A->mv_threads) + 512;
+    const int ph = prof_begin(ctx, sizeof(TA) == 8 ? kProfMatvec : kProfMatvec32);
     k_matvec<TA, TV, TV, ACC><<<A->nrow, A->mv_threads, smem, ctx->stream>>>(
         val, (const int64_t*)A->d_row_ptr.ptr, (const int64_t*)A->d_blk_voff.ptr, (const int64_t*)A->d_blk_xoff.ptr,
         (const int32_t*)A->d_blk_nc.ptr, (const int64_t*)A->d_row_yoff.ptr, (const int32_t*)A->d_row_b.ptr, x, y, z, alpha, beta, row_sq);
+    prof_end(ctx, ph);
     return check_launch(ctx, "k_matvec");
 }
 template int chidg::matvec_launch<double, double>(chidg_gpu_matrix*, const double*, const double*, double*, const double*, double, double, double*);
@@ -420,7 +478,7 @@ template int chidg::matvec_launch<float, float>(chidg_gpu_matrix*, const float*,
 
 int chidg::set_matvec_smem(chidg_gpu_matrix* A) {
     // allow > 48 KB dynamic shared memory when a row has many wide blocks
-    const size_t smem = sizeof(double) * ((size_t)A->max_row_cols + A->mv_threads) + 64;
+    const size_t smem = sizeof(double) * ((size_t)A->max_row_cols + A->mv_threads) + 512;
     if (smem > 48 * 1024) {
         cudaFuncSetAttribute(k_matvec<double, double, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         cudaFuncSetAttribute(k_matvec<float, float, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -960,6 +1018,7 @@ extern "C" int chidg_gpu_precon_update(chidg_gpu_precon* M, chidg_gpu_matrix* A,
     cudaMemcpyAsync(ctx->d_status, &big, sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
     const int nlev = (int)P.fwd_ptr.size() - 1;
     const int tiles_1d = (P.max_b + GT_M - 1) / GT_M;
+    const int ph = prof_begin(ctx, kProfFactor);
     for (int l = 0; l < nlev; ++l) {
         const int nl = P.ltask_ptr[l + 1] - P.ltask_ptr[l];
         if (nl > 0) {
@@ -978,6 +1037,7 @@ extern "C" int chidg_gpu_precon_update(chidg_gpu_precon* M, chidg_gpu_matrix* A,
         const int nr = P.fwd_ptr[l + 1] - P.fwd_ptr[l];
         if ((st = launch_inverse(M, P.fwd_ptr[l], nr))) return st;
     }
+    prof_end(ctx, ph);
     cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
     cudaError_t e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "precon update");
@@ -1023,10 +1083,11 @@ int chidg::precon_apply_impl(chidg_gpu_precon* M, const TV* v, TV* z, int precis
         zx = (TV*)wb.ptr;
     }
     const int threads = P.sweep_threads;
-    const size_t smem_f = sizeof(ACC) * ((size_t)P.max_lo_cols + threads) + 64;
-    const size_t smem_b = sizeof(ACC) * ((size_t)P.max_up_cols + P.max_b + threads) + 64;
+    const size_t smem_f = sizeof(ACC) * ((size_t)P.max_lo_cols + threads) + 512;
+    const size_t smem_b = sizeof(ACC) * ((size_t)P.max_up_cols + P.max_b + threads) + 512;
     const int nf = (int)P.fwd_ptr.size() - 1, nb = (int)P.bwd_ptr.size() - 1;
     int st;
+    int ph = prof_begin(ctx, sizeof(TV) == 8 ? kProfIluForward : kProfIlu32);
     for (int l = 0; l < nf; ++l) {
         const int cnt = P.fwd_ptr[l + 1] - P.fwd_ptr[l];
         if (precision == CHIDG_GPU_MIXED_BF16 && sizeof(TV) == 4)
@@ -1036,6 +1097,10 @@ int chidg::precon_apply_impl(chidg_gpu_precon* M, const TV* v, TV* z, int precis
         else
             k_ilu_forward<double, TV, ACC><<<cnt, threads, smem_f, ctx->stream>>>(P.rows, (const double*)M->LD.ptr, (const int32_t*)P.d_fwd_rows.ptr, P.fwd_ptr[l], v, zx);
         if ((st = check_launch(ctx, "k_ilu_forward"))) return st;
+    }
+    if (sizeof(TV) == 8) {
+        prof_end(ctx, ph);
+        ph = prof_begin(ctx, kProfIluBackward);
     }
     for (int l = 0; l < nb; ++l) {
         const int cnt = P.bwd_ptr[l + 1] - P.bwd_ptr[l];
@@ -1047,6 +1112,7 @@ int chidg::precon_apply_impl(chidg_gpu_precon* M, const TV* v, TV* z, int precis
             k_ilu_backward<double, double, TV, ACC><<<cnt, threads, smem_b, ctx->stream>>>(P.rows, (const double*)M->LD.ptr, (const double*)A->val.ptr, (const int32_t*)P.d_bwd_rows.ptr, P.bwd_ptr[l], zx);
         if ((st = check_launch(ctx, "k_ilu_backward"))) return st;
     }
+    prof_end(ctx, ph);
     if (zx != z) {
         const cudaError_t e = cudaMemcpyAsync(z, zx, sizeof(TV) * (size_t)n, cudaMemcpyDeviceToDevice, ctx->stream);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "precon output copy");
@@ -1059,10 +1125,18 @@ template int chidg::precon_apply_impl<float>(chidg_gpu_precon*, const float*, fl
 int chidg::precon_set_smem(chidg_gpu_precon* M) {
     IluProgram& P = M->P;
     const int threads = P.sweep_threads;
-    const size_t sf = sizeof(double) * ((size_t)P.max_lo_cols + threads) + 64;
-    const size_t sb = sizeof(double) * ((size_t)P.max_up_cols + P.max_b + threads) + 64;
-    if (sf > 48 * 1024) cudaFuncSetAttribute(k_ilu_forward<double, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sf);
-    if (sb > 48 * 1024) cudaFuncSetAttribute(k_ilu_backward<double, double, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
+    const size_t sf = sizeof(double) * ((size_t)P.max_lo_cols + threads) + 512;
+    const size_t sb = sizeof(double) * ((size_t)P.max_up_cols + P.max_b + threads) + 512;
+    if (sf > 48 * 1024) {
+        cudaFuncSetAttribute(k_ilu_forward<double, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sf);
+        cudaFuncSetAttribute(k_ilu_forward<float, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sf);
+        cudaFuncSetAttribute(k_ilu_forward<__nv_bfloat16, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sf);
+    }
+    if (sb > 48 * 1024) {
+        cudaFuncSetAttribute(k_ilu_backward<double, double, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
+        cudaFuncSetAttribute(k_ilu_backward<float, float, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
+        cudaFuncSetAttribute(k_ilu_backward<__nv_bfloat16, float, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
+    }
     return CHIDG_GPU_OK;
 }
 

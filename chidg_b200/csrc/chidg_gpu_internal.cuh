@@ -23,6 +23,7 @@ constexpr int kSlotWnorm = 2;      // ||w||^2 after orthogonalisation
 constexpr int kSlotR0 = 3;         // ||r0||^2
 constexpr int kSlotH = 16;         // h(1:j, j) of the current pass (up to 4000 entries)
 constexpr int kSlotY = 4096;       // y coefficients of the solution update
+constexpr int kMaxKrylov = 4000;   // restart length bound set by the slots above
 
 template <typename T> struct AccOf { using type = double; };
 template <> struct AccOf<float> { using type = float; };
@@ -56,6 +57,13 @@ struct IluProgram {
 
 }  // namespace chidg
 
+namespace chidg {
+// kernel classes timed with CUDA events when profiling is on
+enum { kProfMatvec = 0, kProfIluForward = 1, kProfIluBackward = 2, kProfFactor = 3, kProfMatvec32 = 4, kProfIlu32 = 5,
+       kProfClasses = 6 };
+struct EvPair { cudaEvent_t a, b; int cls; };
+}  // namespace chidg
+
 struct chidg_gpu_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -69,6 +77,11 @@ struct chidg_gpu_ctx {
     double* d_scal = nullptr;
     double* h_scal = nullptr;
     chidg::Buffer partial, partial2;
+    bool profiling = false;
+    std::vector<chidg::EvPair> prof_pending;
+    std::vector<cudaEvent_t> prof_pool;
+    double prof_ms[chidg::kProfClasses] = {};
+    int64_t prof_count[chidg::kProfClasses] = {};
 };
 
 struct chidg_gpu_matrix {
@@ -128,4 +141,7 @@ template <typename TV>
 int precon_apply_impl(chidg_gpu_precon* M, const TV* v, TV* z, int precision);
 int precon_set_smem(chidg_gpu_precon* M);
 void release_program(IluProgram& P);
+int prof_begin(chidg_gpu_ctx* ctx, int cls);        // -1 when profiling is off
+void prof_end(chidg_gpu_ctx* ctx, int handle);
+void prof_resolve(chidg_gpu_ctx* ctx);              // after a stream sync
 }  // namespace chidg

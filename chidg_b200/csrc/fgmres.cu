@@ -142,7 +142,7 @@ struct Solver {
         if (precon_update && (st = precon_update())) return st;
 
         const int m = nkrylov;
-        if (m < 1) return fail(ctx, CHIDG_GPU_EINVAL, "fgmres: nkrylov < 1");
+        if (m < 1 || m > kMaxKrylov) return fail(ctx, CHIDG_GPU_EINVAL, "fgmres: nkrylov outside [1, 4000]");
         if ((st = ensure(ctx, V, sizeof(T) * (size_t)(m + 1) * n)) || (st = ensure(ctx, Z, sizeof(T) * (size_t)(m + 1) * n)) ||
             (st = ensure(ctx, x0, sizeof(T) * (size_t)n)) || (st = ensure(ctx, tmp, sizeof(T) * (size_t)n)))
             return st;

@@ -1,0 +1,39 @@
+"""A mid-size case of the hot kernels for profiler captures.
+
+Runs `--reps` rounds of: ILU0 factorisation, one ILU0 apply (forward and
+backward sweeps) and one FP64 matvec, on an n^3 P2 box (5 fields, 135 x 135
+blocks).  n = 12 gives a 1.7 GB matrix: larger than L2 (126 MB), small enough
+for multi-pass profiler captures.
+
+  python -m chidg_b200.profile_case --n 12 --reps 2
+"""
+from __future__ import annotations
+
+import argparse
+
+from . import api, mesh
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=12)
+    ap.add_argument("--p", type=int, default=2)
+    ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--precon", default="ilu0")
+    args = ap.parse_args()
+    pat = mesh.box_pattern(args.n, args.n, args.n, 5, mesh.nterms_of_order(args.p))
+    A = api.ChidgMatrix(pat)
+    A.upload(mesh.synth_values(pat, seed=1))
+    v = api.ChidgVector(A, mesh.synth_vector(A.n, seed=2))
+    z = api.ChidgVector(A)
+    M = api.create_preconditioner(args.precon)
+    for _ in range(args.reps):
+        M.update(A)
+        M.apply(A, v, z)
+        api.chidg_mv(A, v, z)
+    A.ctx.sync()
+    print(f"profile_case n={args.n} p={args.p}: {A.ctx.launches()} launches")
+
+
+if __name__ == "__main__":
+    main()

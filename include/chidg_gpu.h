@@ -143,6 +143,13 @@ int chidg_gpu_last_error(chidg_gpu_ctx* ctx, char* buf, int32_t buflen);
 int chidg_gpu_error_element(chidg_gpu_ctx* ctx, int32_t* elem);
 /* Number of kernels this context has launched so far. */
 int chidg_gpu_launch_count(chidg_gpu_ctx* ctx, int64_t* count);
+/* Time kernel classes with CUDA events on the context's stream (off by
+ * default; switching resets the totals).  Classes: 0 FP64 matvec, 1 ILU
+ * forward sweep, 2 ILU backward sweep (FP64), 3 factorisation (whole
+ * precon update), 4 FP32 matvec, 5 low-precision ILU apply.  One count is
+ * one matvec launch, one full sweep, or one factorisation. */
+int chidg_gpu_ctx_set_profiling(chidg_gpu_ctx* ctx, int32_t on);
+int chidg_gpu_ctx_kernel_time(chidg_gpu_ctx* ctx, int32_t kernel_class, double* total_ms, int64_t* count);
 /* Page-locked host memory for the upload / download calls. */
 int chidg_gpu_host_alloc(size_t bytes, void** out);
 int chidg_gpu_host_free(void* p);

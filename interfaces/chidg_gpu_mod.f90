@@ -1,0 +1,157 @@
+!> iso_c_binding interface to the B200 linear-solve library (include/chidg_gpu.h).
+!!
+!! This module is the Fortran side of the drop-in: ChiDG's containers keep a
+!! type(c_ptr) handle (as they keep wrapped_petsc_matrix for backend='petsc',
+!! src/containers/type_chidg_matrix.f90:41) and forward init/store/solve calls
+!! here when mod_io::backend == 'cuda'.  No Fortran compiler exists in the
+!! build environment of this repository, so this file is not compiled here;
+!! the same entry points are exercised through ctypes by tests/.
+module chidg_gpu_mod
+    use iso_c_binding
+    implicit none
+
+    integer(c_int), parameter :: CHIDG_GPU_OK = 0, CHIDG_GPU_EINVAL = 1, CHIDG_GPU_ENOMEM = 2,  &
+                                 CHIDG_GPU_ESINGULAR = 3, CHIDG_GPU_ENONFINITE = 4,                &
+                                 CHIDG_GPU_ETIMEOUT = 5, CHIDG_GPU_ENOTCONVERGED = 6,              &
+                                 CHIDG_GPU_ECUDA = 7, CHIDG_GPU_ESTATE = 8
+    integer(c_int), parameter :: CHIDG_BLK_LOCAL = 0, CHIDG_BLK_CHIMERA = 1, CHIDG_BLK_BC = 2, CHIDG_BLK_HB = 3
+    integer(c_int), parameter :: CHIDG_PRECON_IDENTITY = 0, CHIDG_PRECON_JACOBI = 1, &
+                                 CHIDG_PRECON_ILU0 = 2, CHIDG_PRECON_RASILU0 = 3
+    integer(c_int), parameter :: CHIDG_GPU_FP64 = 0, CHIDG_GPU_MIXED_FP32 = 1, CHIDG_GPU_MIXED_BF16 = 2
+
+    type, bind(c) :: chidg_gpu_pattern
+        integer(c_int32_t) :: nelem, ntime
+        type(c_ptr)        :: elem_nvars, elem_nterms, elem_proc
+        integer(c_int64_t) :: nblocks
+        type(c_ptr)        :: blk_row_elem, blk_row_time, blk_col_elem, blk_col_time, blk_kind
+    end type chidg_gpu_pattern
+
+    type, bind(c) :: chidg_gpu_fgmres_opts
+        real(c_double)     :: tol, rtol
+        integer(c_int32_t) :: nmax, nkrylov, orthogonalization, inner_fgmres
+        real(c_double)     :: inner_tol, inner_rtol
+        integer(c_int32_t) :: inner_nmax, inner_nkrylov, inner_orthogonalization
+        integer(c_int32_t) :: use_controller, precision, mixed_inner_nkrylov
+        real(c_double)     :: mixed_inner_rtol
+        integer(c_int32_t) :: mixed_inner_nmax
+    end type chidg_gpu_fgmres_opts
+
+    type, bind(c) :: chidg_gpu_fgmres_result
+        integer(c_int32_t) :: niter, nrestart, inner_iters, nhist
+        real(c_double)     :: residual_norm, res_estimate, r0norm_initial, seconds
+    end type chidg_gpu_fgmres_result
+
+    interface
+        integer(c_int) function chidg_gpu_ctx_create(device, stream, ctx) bind(c, name='chidg_gpu_ctx_create')
+            import :: c_int, c_ptr
+            integer(c_int), value :: device
+            type(c_ptr),    value :: stream
+            type(c_ptr)           :: ctx
+        end function
+        integer(c_int) function chidg_gpu_ctx_destroy(ctx) bind(c, name='chidg_gpu_ctx_destroy')
+            import :: c_int, c_ptr
+            type(c_ptr), value :: ctx
+        end function
+        integer(c_int) function chidg_gpu_last_error(ctx, buf, buflen) bind(c, name='chidg_gpu_last_error')
+            import :: c_int, c_ptr, c_char, c_int32_t
+            type(c_ptr), value        :: ctx
+            character(kind=c_char)    :: buf(*)
+            integer(c_int32_t), value :: buflen
+        end function
+        integer(c_int) function chidg_gpu_error_element(ctx, elem) bind(c, name='chidg_gpu_error_element')
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr), value :: ctx
+            integer(c_int32_t) :: elem
+        end function
+        integer(c_int) function chidg_gpu_matrix_create(ctx, pat, mat) bind(c, name='chidg_gpu_matrix_create')
+            import :: c_int, c_ptr, chidg_gpu_pattern
+            type(c_ptr), value      :: ctx
+            type(chidg_gpu_pattern) :: pat
+            type(c_ptr)             :: mat
+        end function
+        integer(c_int) function chidg_gpu_matrix_destroy(mat) bind(c, name='chidg_gpu_matrix_destroy')
+            import :: c_int, c_ptr
+            type(c_ptr), value :: mat
+        end function
+        integer(c_int) function chidg_gpu_matrix_upload_blocks(mat, ptrs) bind(c, name='chidg_gpu_matrix_upload_blocks')
+            import :: c_int, c_ptr
+            type(c_ptr), value :: mat
+            type(c_ptr)        :: ptrs(*)
+        end function
+        integer(c_int) function chidg_gpu_matrix_upload(mat, vals) bind(c, name='chidg_gpu_matrix_upload')
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: mat
+            real(c_double)     :: vals(*)
+        end function
+        integer(c_int) function chidg_gpu_matrix_clear(mat) bind(c, name='chidg_gpu_matrix_clear')
+            import :: c_int, c_ptr
+            type(c_ptr), value :: mat
+        end function
+        integer(c_int) function chidg_gpu_matrix_scale_diagonal(mat, mass, scale) bind(c, name='chidg_gpu_matrix_scale_diagonal')
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: mat
+            real(c_double)     :: mass(*), scale(*)
+        end function
+        integer(c_int) function chidg_gpu_vector_create(mat, vec) bind(c, name='chidg_gpu_vector_create')
+            import :: c_int, c_ptr
+            type(c_ptr), value :: mat
+            type(c_ptr)        :: vec
+        end function
+        integer(c_int) function chidg_gpu_vector_destroy(vec) bind(c, name='chidg_gpu_vector_destroy')
+            import :: c_int, c_ptr
+            type(c_ptr), value :: vec
+        end function
+        integer(c_int) function chidg_gpu_vector_upload(vec, vals) bind(c, name='chidg_gpu_vector_upload')
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: vec
+            real(c_double)     :: vals(*)
+        end function
+        integer(c_int) function chidg_gpu_vector_download(vec, vals) bind(c, name='chidg_gpu_vector_download')
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: vec
+            real(c_double)     :: vals(*)
+        end function
+        integer(c_int) function chidg_gpu_matvec(mat, x, y) bind(c, name='chidg_gpu_matvec')
+            import :: c_int, c_ptr
+            type(c_ptr), value :: mat, x, y
+        end function
+        integer(c_int) function chidg_gpu_vector_norm(x, nrm) bind(c, name='chidg_gpu_vector_norm')
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: x
+            real(c_double)     :: nrm
+        end function
+        integer(c_int) function chidg_gpu_precon_create(mat, kind, M) bind(c, name='chidg_gpu_precon_create')
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr), value        :: mat
+            integer(c_int32_t), value :: kind
+            type(c_ptr)               :: M
+        end function
+        integer(c_int) function chidg_gpu_precon_update(M, mat, precision) bind(c, name='chidg_gpu_precon_update')
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr), value        :: M, mat
+            integer(c_int32_t), value :: precision
+        end function
+        integer(c_int) function chidg_gpu_precon_apply(M, mat, v, z) bind(c, name='chidg_gpu_precon_apply')
+            import :: c_int, c_ptr
+            type(c_ptr), value :: M, mat, v, z
+        end function
+        integer(c_int) function chidg_gpu_precon_destroy(M) bind(c, name='chidg_gpu_precon_destroy')
+            import :: c_int, c_ptr
+            type(c_ptr), value :: M
+        end function
+        integer(c_int) function chidg_gpu_fgmres_solve(mat, M, b, x, opts, res, hist, hist_cap) &
+                bind(c, name='chidg_gpu_fgmres_solve')
+            import :: c_int, c_ptr, c_double, c_int32_t, chidg_gpu_fgmres_opts, chidg_gpu_fgmres_result
+            type(c_ptr), value            :: mat, M, b, x
+            type(chidg_gpu_fgmres_opts)   :: opts
+            type(chidg_gpu_fgmres_result) :: res
+            real(c_double)                :: hist(*)
+            integer(c_int32_t), value     :: hist_cap
+        end function
+        integer(c_int) function chidg_gpu_fgmres_default_opts(opts) bind(c, name='chidg_gpu_fgmres_default_opts')
+            import :: c_int, chidg_gpu_fgmres_opts
+            type(chidg_gpu_fgmres_opts) :: opts
+        end function
+    end interface
+
+end module chidg_gpu_mod

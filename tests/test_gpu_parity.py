@@ -1,0 +1,232 @@
+"""GPU parity: every CUDA path against the CPU oracle on the same seeded inputs,
+through the C ABI (chidg_b200.api wraps include/chidg_gpu.h).
+
+Tolerances (FP64 mode): matvec and ILU sweeps 1e-12 relative to the vector
+norm (summation order differs from the oracle); factor blocks 1e-10 relative
+to the block norm (pivoted inverses of 135 x 135 blocks); FGMRES: same
+iteration count, residual history within 1e-8 relative, solution within
+1e-10 relative.
+"""
+import numpy as np
+import pytest
+
+from chidg_b200 import _lib, api, mesh
+from oracle import oracle as O
+from tests import kat_util
+
+pytestmark = pytest.mark.gpu
+
+
+def relerr(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def setup(shape, P, nt=1, sub=(1, 1, 1), seed=1, nvars=5):
+    pat = mesh.box_pattern(*shape, nvars, mesh.nterms_of_order(P), ntime=nt, subdomains=sub)
+    vals = mesh.synth_values(pat, seed=seed)
+    Ao = O.OracleMatrix(pat)
+    Ao.set_values(vals)
+    Ag = api.ChidgMatrix(pat)
+    Ag.upload(vals)
+    return pat, vals, Ao, Ag
+
+
+CASES = [((4, 3, 2), 1, 1), ((3, 3, 3), 2, 1), ((2, 2, 2), 1, 3), ((5, 1, 1), 0, 1)]
+
+
+@pytest.mark.parametrize("shape,P,nt", CASES)
+def test_matvec(shape, P, nt):
+    pat, vals, Ao, Ag = setup(shape, P, nt)
+    x = mesh.synth_vector(Ao.n, seed=2)
+    y = api.chidg_mv(Ag, api.ChidgVector(Ag, x)).download()
+    assert relerr(y, Ao.mv(x)) < 1e-13
+
+
+def test_dot_norm_axpy():
+    pat, vals, Ao, Ag = setup((3, 3, 3), 1)
+    x = mesh.synth_vector(Ao.n, seed=3)
+    y = mesh.synth_vector(Ao.n, seed=4)
+    xg, yg = api.ChidgVector(Ag, x), api.ChidgVector(Ag, y)
+    assert api.dot(xg, yg) == pytest.approx(float(x @ y), rel=1e-13)
+    assert xg.norm() == pytest.approx(float(np.linalg.norm(x)), rel=1e-13)
+    yg.axpy(-0.5, xg)
+    assert relerr(yg.download(), y - 0.5 * x) < 1e-15
+
+
+@pytest.mark.parametrize("kind", ["ilu0", "jacobi"])
+@pytest.mark.parametrize("shape,P,nt", CASES)
+def test_precon_factor_and_apply(kind, shape, P, nt):
+    pat, vals, Ao, Ag = setup(shape, P, nt, seed=5)
+    Mo = O.OraclePrecon(Ao, kind)
+    Mo.update()
+    Mg = api.create_preconditioner(kind)
+    Mg.update(Ag)
+    LDo, LDg = Mo.LD(), Mg.LD()
+    voff, _ = pat.value_offsets()
+    nr, nc = pat.block_dims()
+    worst = 0.0
+    for k in range(pat.nblocks):
+        a = LDo[voff[k]:voff[k] + nr[k] * nc[k]]
+        if not np.any(a):
+            continue
+        worst = max(worst, relerr(LDg[voff[k]:voff[k] + nr[k] * nc[k]], a))
+    assert worst < 1e-10
+    v = mesh.synth_vector(Ao.n, seed=6)
+    z = Mg.apply(Ag, api.ChidgVector(Ag, v)).download()
+    assert relerr(z, Mo.apply(v)) < 1e-11
+
+
+@pytest.mark.parametrize("shape,P,sub", [((4, 4, 2), 1, (2, 2, 1)), ((4, 4, 4), 0, (2, 2, 2)), ((6, 3, 3), 1, (3, 1, 1))])
+def test_rasilu0(shape, P, sub):
+    pat, vals, Ao, Ag = setup(shape, P, 1, sub=sub, seed=7)
+    Mo = O.OraclePrecon(Ao, "rasilu0")
+    Mo.update()
+    Mg = api.create_preconditioner("rasilu0")
+    Mg.update(Ag)
+    v = mesh.synth_vector(Ao.n, seed=8)
+    z = Mg.apply(Ag, api.ChidgVector(Ag, v)).download()
+    assert relerr(z, Mo.apply(v)) < 1e-11
+
+
+@pytest.mark.parametrize("prec,shape,P,nt,orth", [("ilu0", (4, 3, 3), 1, 1, "CGS"), ("ilu0", (3, 3, 3), 2, 1, "CGS"),
+                                                  ("ilu0", (3, 3, 2), 1, 1, "MGS"), ("jacobi", (3, 3, 3), 1, 1, "CGS"),
+                                                  ("ilu0", (2, 2, 2), 1, 3, "CGS"), ("rasilu0", (4, 4, 2), 1, 1, "CGS")])
+def test_fgmres_parity(prec, shape, P, nt, orth):
+    sub = (2, 2, 1) if prec == "rasilu0" else (1, 1, 1)
+    pat, vals, Ao, Ag = setup(shape, P, nt, sub=sub, seed=9)
+    b = mesh.synth_vector(Ao.n, seed=10)
+    opts = dict(tol=0.0, rtol=1e-8, nkrylov=12, inner_fgmres=0, nmax=400, orthogonalization=orth)
+    xo, ro = O.fgmres(Ao, O.OraclePrecon(Ao, prec), b, O.default_opts(**opts))
+    solver = api.create_linear_solver("fgmres", **opts)
+    xg = api.ChidgVector(Ag)
+    solver.solve(Ag, xg, api.ChidgVector(Ag, b), api.create_preconditioner(prec))
+    assert solver.niter == ro["niter"]
+    assert relerr(solver.hist, ro["hist"]) < 1e-8
+    assert relerr(xg.download(), xo) < 1e-10
+    assert solver.residual_norm == pytest.approx(ro["residual_norm"], rel=1e-6)
+
+
+def test_fgmres_inner_default_options():
+    """Reference defaults: inner FGMRES on, no controller (M refreshed per call)."""
+    pat, vals, Ao, Ag = setup((3, 3, 2), 1, 1, seed=11)
+    b = mesh.synth_vector(Ao.n, seed=12)
+    opts = dict(tol=1e-9, rtol=1e-10, nkrylov=20, nmax=200)
+    xo, ro = O.fgmres(Ao, O.OraclePrecon(Ao, "ilu0"), b, O.default_opts(**opts))
+    solver = api.create_linear_solver("fgmres", **opts)
+    xg = api.ChidgVector(Ag)
+    solver.solve(Ag, xg, api.ChidgVector(Ag, b), api.create_preconditioner("ilu0"))
+    assert solver.niter == ro["niter"]
+    assert relerr(solver.hist, ro["hist"]) < 1e-8
+    assert relerr(xg.download(), xo) < 1e-10
+
+
+@pytest.mark.parametrize("name", ["ilu0", "ilu0_hb", "fgmres", "fgmres_ref"])
+def test_reference_kats_on_gpu(name):
+    case = kat_util.load_cases()[name]
+    pat, vals, b = kat_util.build(case)
+    A = api.ChidgMatrix(pat)
+    A.upload(vals)
+    eo = pat.elem_offsets()
+    if name.startswith("ilu0"):
+        M = api.create_preconditioner("ilu0")
+        M.update(A)
+        LD = M.LD()
+        z = M.apply(A, api.ChidgVector(A, b)).download()
+        for kind, idx, expect in case["asserts"]:
+            if kind == "LD":
+                assert LD[kat_util.ld_index(pat, *idx)] == pytest.approx(expect, rel=1e-15)
+            else:
+                e, i = idx
+                assert abs(z[eo[e - 1] + i - 1] - expect) <= case["tol"]
+    else:
+        solver = api.create_linear_solver("fgmres", tol=case["solver_tol"], nmax=1000)
+        x = api.ChidgVector(A)
+        solver.solve(A, x, api.ChidgVector(A, b), api.create_preconditioner("identity"))
+        xv = x.download()
+        for kind, (e, i), expect in case["asserts"]:
+            assert abs(xv[eo[e - 1] + i - 1] - expect) <= case["tol"]
+
+
+@pytest.mark.parametrize("precision", ["mixed_fp32", "mixed_bf16"])
+def test_mixed_precision_reaches_fp64_accuracy(precision):
+    pat, vals, Ao, Ag = setup((4, 4, 4), 1, seed=13)
+    b = mesh.synth_vector(Ao.n, seed=14)
+    xo, ro = O.fgmres(Ao, O.OraclePrecon(Ao, "ilu0"), b,
+                      O.default_opts(tol=0.0, rtol=1e-12, nkrylov=40, inner_fgmres=0, nmax=400))
+    solver = api.create_linear_solver("fgmres", tol=0.0, rtol=1e-8, nkrylov=10, inner_fgmres=0, nmax=50,
+                                      precision=precision, mixed_inner_nkrylov=20, mixed_inner_rtol=1e-2,
+                                      mixed_inner_nmax=40)
+    xg = api.ChidgVector(Ag)
+    solver.solve(Ag, xg, api.ChidgVector(Ag, b), api.create_preconditioner("ilu0"))
+    assert solver.residual_norm <= 1.5e-8 * solver.r0norm_initial
+    assert relerr(xg.download(), xo) < 1e-6
+
+
+def test_singular_block_reports_element():
+    pat, vals, Ao, Ag = setup((3, 2, 2), 1, seed=15)
+    voff, _ = pat.value_offsets()
+    nr, nc = pat.block_dims()
+    k = int(np.nonzero((pat.blk_row_elem == 4) & (pat.blk_col_elem == 4))[0][0])
+    bad = vals.copy()
+    bad[voff[k]:voff[k] + nr[k] * nc[k]] = 0.0
+    Ag.upload(bad)
+    M = api.create_preconditioner("jacobi")
+    with pytest.raises(_lib.ChidgGpuError) as ei:
+        M.update(Ag)
+    assert ei.value.code == _lib.ESINGULAR and ei.value.element == 4
+
+
+def test_nonfinite_rhs_reported():
+    pat, vals, Ao, Ag = setup((3, 2, 2), 1, seed=16)
+    b = mesh.synth_vector(Ao.n, seed=17)
+    b[5] = np.nan
+    solver = api.create_linear_solver("fgmres", tol=0.0, rtol=1e-8, nkrylov=10, inner_fgmres=0, nmax=20)
+    with pytest.raises(_lib.ChidgGpuError) as ei:
+        solver.solve(Ag, api.ChidgVector(Ag), api.ChidgVector(Ag, b), api.create_preconditioner("ilu0"))
+    assert ei.value.code == _lib.ENONFINITE
+
+
+def test_controller_reuses_factorisation():
+    pat, vals, Ao, Ag = setup((3, 3, 2), 1, seed=18)
+    b = api.ChidgVector(Ag, mesh.synth_vector(Ao.n, seed=19))
+    M = api.create_preconditioner("ilu0")
+    solver = api.create_linear_solver("fgmres", tol=0.0, rtol=1e-8, nkrylov=20, inner_fgmres=0, nmax=100,
+                                      use_controller=True)
+    x = api.ChidgVector(Ag)
+    solver.solve(Ag, x, b, M)
+    s1 = M.stamp
+    solver.solve(Ag, x, b, M)
+    assert M.stamp == s1 == Ag.stamp
+    Ag.upload(vals * 1.0)     # a new assembly bumps the stamp -> refactor
+    solver.solve(Ag, x, b, M)
+    assert M.stamp == Ag.stamp and M.stamp != s1
+
+
+def test_upload_blocks_equals_packed():
+    pat, vals, Ao, Ag = setup((3, 2, 2), 1, seed=20)
+    voff, _ = pat.value_offsets()
+    nr, nc = pat.block_dims()
+    blocks = [vals[voff[k]:voff[k] + nr[k] * nc[k]].reshape(nc[k], nr[k]).T for k in range(pat.nblocks)]
+    A2 = api.ChidgMatrix(pat)
+    A2.upload_blocks(blocks)
+    assert np.array_equal(A2.download(), vals)
+
+
+def test_scale_diagonal():
+    pat, vals, Ao, Ag = setup((2, 2, 1), 1, seed=21)
+    nt = int(pat.elem_nterms[0])
+    nv = int(pat.elem_nvars[0])
+    rng = np.random.default_rng(0)
+    mass = rng.standard_normal((pat.nelem, nt, nt))
+    scale = rng.standard_normal((pat.nelem, nv))
+    Ag.scale_diagonal(np.ascontiguousarray(mass.transpose(0, 2, 1)).ravel(), scale.ravel())
+    got = Ag.download()
+    voff, _ = pat.value_offsets()
+    b = nt * nv
+    for k in range(pat.nblocks):
+        e = pat.blk_row_elem[k]
+        blk = vals[voff[k]:voff[k] + b * b].reshape(b, b).T.copy()
+        if pat.blk_col_elem[k] == e:
+            for f in range(nv):
+                blk[f * nt:(f + 1) * nt, f * nt:(f + 1) * nt] += scale[e, f] * mass[e]
+        assert np.allclose(got[voff[k]:voff[k] + b * b].reshape(b, b).T, blk, rtol=1e-15, atol=1e-15)
