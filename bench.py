@@ -144,41 +144,6 @@ def measured_peaks():
 
 
 # ---------------------------------------------------------------------------
-# distributed plumbing (replicas only: no data-path collective)
-# ---------------------------------------------------------------------------
-def dist_init(n_gpus):
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    pg = None
-    if world > 1:
-        import datetime
-
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-        pg = dist
-    return rank, world, local, pg
-
-
-def barrier(pg, local):
-    if pg is not None:
-        import torch
-        pg.barrier(device_ids=[local])
-        torch.cuda.synchronize()
-
-
-def allmax(pg, v, local):
-    if pg is None:
-        return v
-    import torch
-    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
-    pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    return float(t.item())
-
-
-# ---------------------------------------------------------------------------
 # CPU legs (oracle)
 # ---------------------------------------------------------------------------
 def cpu_sample_solve(seed_a=SEED_A, seed_b=SEED_B, n=SAMPLE_N):
@@ -246,8 +211,9 @@ def run_reference(args):
 def run_gpu(args):
     import torch
 
-    from chidg_b200 import _lib, api, mesh
-    rank, world, local, pg = dist_init(args.gpus)
+    from chidg_b200 import api, mesh
+    from chidg_b200.replicas import allmax, barrier, init_from_env
+    rank, world, local, pg = init_from_env("nccl")
     torch.cuda.set_device(local)
     stream = torch.cuda.current_stream()
     ctx = api.Context(local, stream=stream.cuda_stream)

@@ -238,8 +238,9 @@ PRECISIONS = {"fp64": _lib.FP64, "mixed_fp32": _lib.MIXED_FP32, "mixed_bf16": _l
 class Preconditioner:
     """preconditioner_t: init / update / apply / tear_down."""
 
-    def __init__(self, kind: str):
+    def __init__(self, kind: str, schedule: str = "dataflow"):
         self.kind = kind.lower()
+        self.schedule = schedule
         if self.kind not in PRECON_KINDS:
             raise ValueError(f"create_preconditioner: invalid preconditioner '{kind}'")
         self.h = None
@@ -251,7 +252,15 @@ class Preconditioner:
         h = C.c_void_p()
         A.ctx.check(A.ctx.L.chidg_gpu_precon_create(A.h, PRECON_KINDS[self.kind], C.byref(h)), f"{self.kind}%init")
         self.h = h
+        self.set_schedule(self.schedule)
         return self
+
+    def set_schedule(self, schedule: str):
+        """'levels' (one launch per wavefront) or 'dataflow' (one launch per sweep)."""
+        self.schedule = schedule
+        if self.h is not None:
+            code = {"levels": _lib.SCHED_LEVELS, "dataflow": _lib.SCHED_DATAFLOW}[schedule]
+            self.A.ctx.check(self.A.ctx.L.chidg_gpu_precon_set_schedule(self.h, code), "set_schedule")
 
     def update(self, A: ChidgMatrix, b=None, precision: str = "fp64"):
         if self.h is None or A is not self.A:
@@ -286,8 +295,8 @@ class Preconditioner:
             pass
 
 
-def create_preconditioner(name: str) -> Preconditioner:
-    return Preconditioner(name)
+def create_preconditioner(name: str, schedule: str = "dataflow") -> Preconditioner:
+    return Preconditioner(name, schedule)
 
 
 class FGMRES:

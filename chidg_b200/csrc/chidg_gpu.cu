@@ -104,6 +104,14 @@ extern "C" int chidg_gpu_ctx_kernel_time(chidg_gpu_ctx* ctx, int32_t cls, double
     return CHIDG_GPU_OK;
 }
 
+// Status word of the dataflow sweeps, read back as one double slot.
+int chidg::status_word(chidg_gpu_ctx* ctx, double slot_value) {
+    int w = 0;
+    std::memcpy(&w, &slot_value, sizeof(int));
+    if (w != 0) return fail(ctx, CHIDG_GPU_ETIMEOUT, "ILU sweep: a bounded wait for a parent row ran out");
+    return CHIDG_GPU_OK;
+}
+
 // Two-pass reductions into ctx->d_scal[slot..slot+nq).
 int chidg::reduce_partials(chidg_gpu_ctx* ctx, const double* partial, int ncta, int nq, int slot, bool do_sqrt) {
     k_reduce_partials<<<1, 1024, 0, ctx->stream>>>(partial, ncta, nq, ctx->d_scal + slot, do_sqrt ? 1 : 0);
@@ -230,6 +238,16 @@ static int upload_array(chidg_gpu_ctx* ctx, Buffer& buf, const std::vector<T>& v
     if (v.empty()) return CHIDG_GPU_OK;
     const cudaError_t e = cudaMemcpy(buf.ptr, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
     return e == cudaSuccess ? CHIDG_GPU_OK : cuda_fail(ctx, e, "pattern upload");
+}
+
+// Triangular sweeps: one row per CTA and a dependency chain through the
+// rows, so a row must stream its blocks as fast as one SM allows: use up to
+// 1024 threads (G = floor(1024 / b) column groups).
+static int sweep_dim_for(int bmax) {
+    const int G = std::max(1, 1024 / std::max(bmax, 1));
+    int t = G * bmax;
+    t = ((t + 31) / 32) * 32;
+    return std::min(std::max(t, 32), 1024);
 }
 
 static int block_dim_for(int bmax) {
@@ -926,7 +944,7 @@ static int finalize_program(chidg_gpu_ctx* ctx, const chidg_gpu_matrix* A, IluPr
     P.rows.up_U = (const int64_t*)P.d_up_U.ptr;
     P.rows.up_par = (const int32_t*)P.d_up_par.ptr;
     P.rows.up_nc = (const int32_t*)P.d_up_nc.ptr;
-    P.sweep_threads = block_dim_for(P.max_b);
+    P.sweep_threads = sweep_dim_for(P.max_b);
     (void)A;
     return CHIDG_GPU_OK;
 }
@@ -955,6 +973,9 @@ extern "C" int chidg_gpu_precon_create(chidg_gpu_matrix* A, int32_t kind, chidg_
         if (st) { delete M; return fail(ctx, st, err); }
         st = finalize_program(ctx, A, M->P);
         if (st) { release_program(M->P); delete M; return st; }
+        const size_t sync_bytes = sizeof(unsigned) * (2 + (size_t)M->P.nprow);
+        if ((st = ensure(ctx, M->sync, sync_bytes))) { release_program(M->P); delete M; return st; }
+        cudaMemsetAsync(M->sync.ptr, 0, sync_bytes, ctx->stream);
     }
     *out = M;
     return CHIDG_GPU_OK;
@@ -965,7 +986,7 @@ extern "C" int chidg_gpu_precon_destroy(chidg_gpu_precon* M) {
     cudaSetDevice(M->ctx->device);
     cudaStreamSynchronize(M->ctx->stream);
     release_program(M->P);
-    for (Buffer* b : {&M->LD, &M->LD32, &M->LD16, &M->zx, &M->zx32, &M->piv_scratch}) release(*b);
+    for (Buffer* b : {&M->LD, &M->LD32, &M->LD16, &M->zx, &M->zx32, &M->piv_scratch, &M->sync}) release(*b);
     delete M;
     return CHIDG_GPU_OK;
 }
@@ -980,6 +1001,11 @@ static int launch_inverse(chidg_gpu_precon* M, int row_begin, int count) {
     IluProgram& P = M->P;
     double* LD = (double*)M->LD.ptr;
     const int bmax = P.max_b;
+#define CHIDG_INV2(CL, RW)                                                                                       \
+    k_block_inverse2<CL, RW><<<count, 512, 0, ctx->stream>>>(LD, (const int64_t*)P.d_dinv_off.ptr,                  \
+                                                             (const int32_t*)P.d_prow_b.ptr,                        \
+                                                             (const int32_t*)P.d_prow_elem.ptr,                     \
+                                                             (const int32_t*)P.d_fwd_rows.ptr, row_begin, ctx->d_status)
     if (bmax <= 32)
         k_block_inverse<1, 1, 32><<<count, 1024, 0, ctx->stream>>>(LD, (const int64_t*)P.d_dinv_off.ptr, (const int32_t*)P.d_prow_b.ptr,
                                                                   (const int32_t*)P.d_prow_elem.ptr, (const int32_t*)P.d_fwd_rows.ptr, row_begin, ctx->d_status);
@@ -992,6 +1018,7 @@ static int launch_inverse(chidg_gpu_precon* M, int row_begin, int count) {
     else if (bmax <= 160)
         k_block_inverse<5, 10, 16><<<count, 512, 0, ctx->stream>>>(LD, (const int64_t*)P.d_dinv_off.ptr, (const int32_t*)P.d_prow_b.ptr,
                                                                   (const int32_t*)P.d_prow_elem.ptr, (const int32_t*)P.d_fwd_rows.ptr, row_begin, ctx->d_status);
+#undef CHIDG_INV2
     else {
         int st = ensure(ctx, M->piv_scratch, sizeof(int) * 1024 * (size_t)std::max(count, 1));
         if (st) return st;
@@ -1063,6 +1090,57 @@ extern "C" int chidg_gpu_precon_update(chidg_gpu_precon* M, chidg_gpu_matrix* A,
 
 // z = M^{-1} v in the given arithmetic.  TV is the vector type; factors come
 // from LD (FP64), LD32 or LD16 by precision; U blocks from A (FP64 or FP32).
+// Both sweeps as two dependency-driven launches (CHIDG_SCHED_DATAFLOW).
+template <typename TL, typename TU, typename TV>
+static int dataflow_sweeps(chidg_gpu_precon* M, const TL* LD, const TU* U, const TV* v, TV* zx, int variant) {
+    chidg_gpu_ctx* ctx = M->ctx;
+    IluProgram& P = M->P;
+    using ACC = typename AccOf<TV>::type;
+    const int threads = P.sweep_threads;
+    const size_t smem = sizeof(ACC) * ((size_t)std::max(P.max_lo_cols, P.max_up_cols) + P.max_b + threads) + 512;
+    auto kf = k_ilu_sweep_sf<TL, TU, TV, ACC, true>;
+    auto kb = k_ilu_sweep_sf<TL, TU, TV, ACC, false>;
+    if (M->sf_grid[variant] == 0) {
+        if (smem > 48 * 1024) {
+            cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        }
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kb, threads, smem) != cudaSuccess || per_sm < 1) {
+            cudaGetLastError();
+            per_sm = 1;
+        }
+        M->sf_grid[variant] = std::max(1, std::min(P.nprow, per_sm * ctx->nsm));
+    }
+    const int grid = M->sf_grid[variant];
+    unsigned* counters = (unsigned*)M->sync.ptr;
+    SweepSync S{counters, counters + 2, 0u, (int*)(ctx->d_scal + kSlotStatus), kSpinLimit};
+    int st;
+    cudaError_t e = cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned), ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "sweep counters");
+    int ph = prof_begin(ctx, sizeof(TV) == 8 ? kProfIluForward : kProfIlu32);
+    S.epoch = ++M->epoch;
+    S.counter = counters;
+    kf<<<grid, threads, smem, ctx->stream>>>(P.rows, LD, U, (const int32_t*)P.d_fwd_rows.ptr, P.nprow, v, zx, S);
+    if ((st = check_launch(ctx, "k_ilu_sweep_sf forward"))) return st;
+    if (sizeof(TV) == 8) {
+        prof_end(ctx, ph);
+        ph = prof_begin(ctx, kProfIluBackward);
+    }
+    S.epoch = ++M->epoch;
+    S.counter = counters + 1;
+    kb<<<grid, threads, smem, ctx->stream>>>(P.rows, LD, U, (const int32_t*)P.d_bwd_rows.ptr, P.nprow, v, zx, S);
+    if ((st = check_launch(ctx, "k_ilu_sweep_sf backward"))) return st;
+    prof_end(ctx, ph);
+    return CHIDG_GPU_OK;
+}
+
+extern "C" int chidg_gpu_precon_set_schedule(chidg_gpu_precon* M, int32_t schedule) {
+    if (!M || (schedule != CHIDG_SCHED_LEVELS && schedule != CHIDG_SCHED_DATAFLOW)) return CHIDG_GPU_EINVAL;
+    M->schedule = schedule;
+    return CHIDG_GPU_OK;
+}
+
 template <typename TV>
 int chidg::precon_apply_impl(chidg_gpu_precon* M, const TV* v, TV* z, int precision) {
     chidg_gpu_ctx* ctx = M->ctx;
@@ -1087,6 +1165,20 @@ int chidg::precon_apply_impl(chidg_gpu_precon* M, const TV* v, TV* z, int precis
     const size_t smem_b = sizeof(ACC) * ((size_t)P.max_up_cols + P.max_b + threads) + 512;
     const int nf = (int)P.fwd_ptr.size() - 1, nb = (int)P.bwd_ptr.size() - 1;
     int st;
+    if (M->schedule == CHIDG_SCHED_DATAFLOW) {
+        if (precision == CHIDG_GPU_MIXED_BF16 && sizeof(TV) == 4)
+            st = dataflow_sweeps(M, (const __nv_bfloat16*)M->LD16.ptr, (const float*)A->val32.ptr, v, zx, 2);
+        else if (sizeof(TV) == 4)
+            st = dataflow_sweeps(M, (const float*)M->LD32.ptr, (const float*)A->val32.ptr, v, zx, 1);
+        else
+            st = dataflow_sweeps(M, (const double*)M->LD.ptr, (const double*)A->val.ptr, v, zx, 0);
+        if (st) return st;
+        if (zx != z) {
+            const cudaError_t e = cudaMemcpyAsync(z, zx, sizeof(TV) * (size_t)n, cudaMemcpyDeviceToDevice, ctx->stream);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "precon output copy");
+        }
+        return CHIDG_GPU_OK;
+    }
     int ph = prof_begin(ctx, sizeof(TV) == 8 ? kProfIluForward : kProfIlu32);
     for (int l = 0; l < nf; ++l) {
         const int cnt = P.fwd_ptr[l + 1] - P.fwd_ptr[l];
@@ -1145,7 +1237,13 @@ extern "C" int chidg_gpu_precon_apply(chidg_gpu_precon* M, chidg_gpu_matrix* A, 
     cudaSetDevice(M->ctx->device);
     if (M->kind != CHIDG_PRECON_IDENTITY && M->stamp == 0) return fail(M->ctx, CHIDG_GPU_ESTATE, "precon_apply: preconditioner not updated");
     precon_set_smem(M);
-    return precon_apply_impl<double>(M, (const double*)v->buf.ptr, (double*)z->buf.ptr, CHIDG_GPU_FP64);
+    chidg_gpu_ctx* ctx = M->ctx;
+    cudaMemsetAsync(ctx->d_scal + kSlotStatus, 0, sizeof(double), ctx->stream);
+    int st = precon_apply_impl<double>(M, (const double*)v->buf.ptr, (double*)z->buf.ptr, CHIDG_GPU_FP64);
+    if (st) return st;
+    double w;
+    if ((st = fetch_scalars(ctx, kSlotStatus, 1, &w))) return st;
+    return status_word(ctx, w);
 }
 
 extern "C" int chidg_gpu_precon_download_LD(chidg_gpu_precon* M, double* host) {

@@ -21,6 +21,8 @@ constexpr int kSlotTmp = 0;        // one-off dots / norms
 constexpr int kSlotNormBefore = 1; // ||w||^2 before orthogonalisation
 constexpr int kSlotWnorm = 2;      // ||w||^2 after orthogonalisation
 constexpr int kSlotR0 = 3;         // ||r0||^2
+constexpr int kSlotStatus = 4;     // int status word of the dataflow sweeps (nonzero = a wait ran out)
+constexpr long long kSpinLimit = 2000000000LL;   // clock cycles a sweep waits for a parent (~1 s)
 constexpr int kSlotH = 16;         // h(1:j, j) of the current pass (up to 4000 entries)
 constexpr int kSlotY = 4096;       // y coefficients of the solution update
 constexpr int kMaxKrylov = 4000;   // restart length bound set by the slots above
@@ -119,6 +121,10 @@ struct chidg_gpu_precon {
     int64_t stamp = 0;
     chidg::IluProgram P;
     chidg::Buffer LD, LD32, LD16, zx, zx32, piv_scratch;
+    int schedule = CHIDG_SCHED_DATAFLOW;   // sweep schedule
+    chidg::Buffer sync;                    // [2 counters][flags per programme row]
+    unsigned epoch = 0;
+    int sf_grid[3] = {0, 0, 0};            // resident CTAs of the dataflow sweep per vector type
 };
 
 namespace chidg {
@@ -141,6 +147,7 @@ template <typename TV>
 int precon_apply_impl(chidg_gpu_precon* M, const TV* v, TV* z, int precision);
 int precon_set_smem(chidg_gpu_precon* M);
 void release_program(IluProgram& P);
+int status_word(chidg_gpu_ctx* ctx, double slot_value);
 int prof_begin(chidg_gpu_ctx* ctx, int cls);        // -1 when profiling is off
 void prof_end(chidg_gpu_ctx* ctx, int handle);
 void prof_resolve(chidg_gpu_ctx* ctx);              // after a stream sync

@@ -192,6 +192,7 @@ struct Solver {
                 if ((st = matvec(zj, w, nullptr, 1.0, 0.0, true, kSlotNormBefore))) return st;
                 if ((st = gs_pass(w, Vb, j))) return st;
                 if ((st = fetch_scalars(ctx, 0, kSlotH + j, sc.data()))) return st;
+                if ((st = status_word(ctx, sc[kSlotStatus]))) return st;
                 const double norm_before = std::sqrt(sc[kSlotNormBefore]);
                 if (!std::isfinite(norm_before)) return fail(ctx, CHIDG_GPU_ENONFINITE, "fgmres: non-finite A*z");
                 std::vector<double> hcol(sc.begin() + kSlotH, sc.begin() + kSlotH + j);
@@ -301,6 +302,7 @@ extern "C" int chidg_gpu_fgmres_solve(chidg_gpu_matrix* A, chidg_gpu_precon* M, 
     set_matvec_smem(A);
     if (M->kind != CHIDG_PRECON_IDENTITY) precon_set_smem(M);
     ctx->err_elem = -1;
+    cudaMemsetAsync(ctx->d_scal + kSlotStatus, 0, sizeof(double), ctx->stream);
 
     const int prec = o.precision;
     // M%update as solver_controller%update_preconditioner decides, or on every

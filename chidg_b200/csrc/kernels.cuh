@@ -49,6 +49,24 @@ template <> __device__ __forceinline__ __nv_bfloat16 ld_stream<__nv_bfloat16>(co
     return __ushort_as_bfloat16(u);
 }
 
+// acc + sum over the column stripe c = g, g+G, ... < nc of B[c*ld] * x[c],
+// summed in increasing c (the same order in every kernel that uses it), with
+// eight independent loads in flight per thread.
+template <typename T, typename ACC>
+__device__ __forceinline__ ACC stripe_dot(const T* __restrict__ B, int64_t ld, int nc, int g, int G,
+                                          const ACC* __restrict__ x, ACC acc) {
+    int c = g;
+    for (; c + 7 * G < nc; c += 8 * G) {
+        T a[8];
+        #pragma unroll
+        for (int u = 0; u < 8; ++u) a[u] = ld_stream(B + (int64_t)(c + u * G) * ld);
+        #pragma unroll
+        for (int u = 0; u < 8; ++u) acc += cvt<ACC>(a[u]) * x[c + u * G];
+    }
+    for (; c < nc; c += G) acc += cvt<ACC>(ld_stream(B + (int64_t)c * ld)) * x[c];
+    return acc;
+}
+
 // ---------------------------------------------------------------------------
 // block reductions (deterministic: fixed tree for a fixed blockDim)
 // ---------------------------------------------------------------------------
@@ -82,7 +100,7 @@ __device__ __forceinline__ double block_sum(double v, double* scratch) {
 // shared memory once.  Optionally writes the row's sum of squares of y.
 // ---------------------------------------------------------------------------
 template <typename TA, typename TX, typename TY, typename ACC>
-__global__ void k_matvec(const TA* __restrict__ val, const int64_t* __restrict__ row_ptr,
+__global__ void __launch_bounds__(1024) k_matvec(const TA* __restrict__ val, const int64_t* __restrict__ row_ptr,
                          const int64_t* __restrict__ blk_voff, const int64_t* __restrict__ blk_xoff,
                          const int32_t* __restrict__ blk_nc, const int64_t* __restrict__ row_yoff,
                          const int32_t* __restrict__ row_b, const TX* __restrict__ x,
@@ -112,18 +130,7 @@ __global__ void k_matvec(const TA* __restrict__ val, const int64_t* __restrict__
             const int nc = blk_nc[k];
             const TA* Ab = val + blk_voff[k] + r;
             const ACC* xb = xs + off;
-            int c = g;
-            for (; c + 3 * G < nc; c += 4 * G) {
-                const TA a0 = ld_stream(Ab + (int64_t)c * b);
-                const TA a1 = ld_stream(Ab + (int64_t)(c + G) * b);
-                const TA a2 = ld_stream(Ab + (int64_t)(c + 2 * G) * b);
-                const TA a3 = ld_stream(Ab + (int64_t)(c + 3 * G) * b);
-                acc += cvt<ACC>(a0) * xb[c];
-                acc += cvt<ACC>(a1) * xb[c + G];
-                acc += cvt<ACC>(a2) * xb[c + 2 * G];
-                acc += cvt<ACC>(a3) * xb[c + 3 * G];
-            }
-            for (; c < nc; c += G) acc += cvt<ACC>(ld_stream(Ab + (int64_t)c * b)) * xb[c];
+            acc = stripe_dot(Ab, (int64_t)b, nc, g, G, xb, acc);
             off += nc;
         }
     }
@@ -352,6 +359,91 @@ __global__ void __launch_bounds__(256) k_task_gemm(const GemmTask* __restrict__ 
     }
 }
 
+// FP64 tensor-core version of k_task_gemm for blocks up to 136 x 136: one CTA
+// computes a whole output block with mma.sync m8n8k4 (DMMA).  18 warps on a
+// 6 x 3 grid; warp (wm, wn) owns the 8x8 output tiles (wm + 6i, wn + 3j),
+// i < 3, j < 6, so each A fragment loaded from shared memory feeds six MMAs
+// and each B fragment three.  K is staged 32 at a time through shared memory
+// in the same k-major layout for both operands.
+constexpr int DM_MAX = 136, DM_KC = 32, DM_WM = 6, DM_WN = 3, DM_TI = 3, DM_TJ = 6;
+constexpr int DM_THREADS = 32 * DM_WM * DM_WN;
+constexpr size_t DM_SMEM = 2 * sizeof(double) * DM_KC * DM_MAX;
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
+}
+template <typename TA, typename TB, typename TC>
+__global__ void __launch_bounds__(DM_THREADS) k_task_gemm_dmma(const GemmTask* __restrict__ tasks, const GemmPair* __restrict__ pairs,
+                                                               const TA* Abase, const TB* Bbase,
+                                                               const double* Cinit, TC* Cbase, double sgn) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* As = reinterpret_cast<double*>(smem_raw);      // [DM_KC][DM_MAX]
+    double* Bs = As + DM_KC * DM_MAX;                        // [DM_KC][DM_MAX]
+    const GemmTask t = tasks[blockIdx.x];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int wm = w % DM_WM, wn = w / DM_WM;
+    const int g = lane >> 2, tq = lane & 3;
+    double acc[DM_TI][DM_TJ][2];
+    #pragma unroll
+    for (int i = 0; i < DM_TI; ++i)
+        #pragma unroll
+        for (int j = 0; j < DM_TJ; ++j) { acc[i][j][0] = 0.0; acc[i][j][1] = 0.0; }
+    const int tm = (t.m + 7) >> 3, tn = (t.n + 7) >> 3;
+    for (int q = t.q_begin; q < t.q_end; ++q) {
+        const GemmPair pr = pairs[q];
+        const TA* A = Abase + pr.a_off;   // m x k, column-major
+        const TB* B = Bbase + pr.b_off;   // k x n, column-major
+        for (int k0 = 0; k0 < pr.k; k0 += DM_KC) {
+            const int kc = min(DM_KC, pr.k - k0);
+            __syncthreads();
+            // A panel: As[kk][i] = A[i][k0+kk]; padded rows and columns are zero
+            for (int idx = threadIdx.x; idx < DM_KC * DM_MAX; idx += blockDim.x) {
+                const int i = idx % DM_MAX, kk = idx / DM_MAX;
+                As[idx] = (i < t.m && kk < kc) ? to_d(A[i + (int64_t)(k0 + kk) * t.m]) : 0.0;
+            }
+            // B panel: Bs[kk][j] = B[k0+kk][j] (coalesced along k in global memory)
+            for (int idx = threadIdx.x; idx < DM_KC * DM_MAX; idx += blockDim.x) {
+                const int kk = idx % DM_KC, j = idx / DM_KC;
+                Bs[kk * DM_MAX + j] = (j < t.n && kk < kc) ? to_d(B[(k0 + kk) + (int64_t)j * pr.k]) : 0.0;
+            }
+            __syncthreads();
+            for (int k4 = 0; k4 < kc; k4 += 4) {
+                double af[DM_TI], bf[DM_TJ];
+                #pragma unroll
+                for (int i = 0; i < DM_TI; ++i) af[i] = As[(k4 + tq) * DM_MAX + (wm + DM_WM * i) * 8 + g];
+                #pragma unroll
+                for (int j = 0; j < DM_TJ; ++j) bf[j] = Bs[(k4 + tq) * DM_MAX + (wn + DM_WN * j) * 8 + g];
+                #pragma unroll
+                for (int i = 0; i < DM_TI; ++i) {
+                    if (wm + DM_WM * i >= tm) continue;
+                    #pragma unroll
+                    for (int j = 0; j < DM_TJ; ++j) {
+                        if (wn + DM_WN * j >= tn) continue;
+                        dmma_8x8x4(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+                    }
+                }
+            }
+        }
+    }
+    #pragma unroll
+    for (int i = 0; i < DM_TI; ++i) {
+        const int row = (wm + DM_WM * i) * 8 + g;
+        if (row >= t.m) continue;
+        #pragma unroll
+        for (int j = 0; j < DM_TJ; ++j) {
+            #pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int col = (wn + DM_WN * j) * 8 + 2 * tq + e;
+                if (col >= t.n) continue;
+                const int64_t o = row + (int64_t)col * t.m;
+                double v = sgn * acc[i][j][e];
+                if (t.cinit_off >= 0) v = Cinit[t.cinit_off + o] + v;
+                Cbase[t.c_off + o] = from_d<TC>(v);
+            }
+        }
+    }
+}
+
 // In-place inverse of one diagonal block per CTA: Gauss-Jordan with partial
 // (row) pivoting, restated from the textbook algorithm.  The pivot of column
 // k is the entry of largest magnitude among rows not yet used as pivots
@@ -479,6 +571,125 @@ __global__ void __launch_bounds__(NW * 32) k_block_inverse(double* __restrict__ 
     if (singular && threadIdx.x == 0) atomicMin(status, prow_elem[prow]);
 }
 
+// In-place inverse, second layout: 16 warps, warp w owns rows w + 16*ri
+// (ri < RW), lane l owns columns l + 32*cl (cl < CL), so b <= min(32*CL, 16*RW).  The
+// pivot loop is split into a compile-time column slot ck and a runtime lane
+// lk (k = 32*ck + lk): every access to the pivot column is then a static
+// register index, and only the pivot row needs a runtime row select (done
+// by its owning warp alone).  Same pivoting rule and result as
+// k_block_inverse: Gauss-Jordan with implicit row pivoting, largest |a|
+// among unused rows (first on ties), permutation undone on the store.
+template <int CL, int RW>
+__global__ void __launch_bounds__(512) k_block_inverse2(double* __restrict__ LD, const int64_t* __restrict__ dinv_off,
+                                                       const int32_t* __restrict__ prow_b,
+                                                       const int32_t* __restrict__ prow_elem,
+                                                       const int32_t* __restrict__ rows, int row_begin,
+                                                       int* __restrict__ status) {
+    constexpr int NW = 16, NMAX = (32 * CL > NW * RW) ? 32 * CL : NW * RW;
+    __shared__ double colbuf[NMAX];
+    __shared__ double rowbuf[2][NMAX];
+    __shared__ double cand_v[NW];
+    __shared__ double cand_a[NW];
+    __shared__ int cand_i[NW];
+    __shared__ int pivrow[NMAX];
+    __shared__ int qinv[NMAX];
+    const int prow = rows[row_begin + blockIdx.x];
+    const int b = prow_b[prow];
+    double* D = LD + dinv_off[prow];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double a[RW][CL];
+    #pragma unroll
+    for (int ri = 0; ri < RW; ++ri)
+        #pragma unroll
+        for (int cl = 0; cl < CL; ++cl) {
+            const int i = w + NW * ri, j = lane + 32 * cl;
+            a[ri][cl] = (i < b && j < b) ? D[i + (int64_t)j * b] : 0.0;
+        }
+    unsigned used = 0;          // bit ri set: row w + NW*ri already used as a pivot
+    bool singular = false;
+    #pragma unroll
+    for (int ck = 0; ck < CL; ++ck) {
+        for (int lk = 0; lk < 32; ++lk) {
+            const int k = 32 * ck + lk;
+            if (k >= b) break;
+            const int buf = k & 1;
+            // (a) candidates of this warp's rows in column k; column k to colbuf
+            if (lane == lk) {
+                double best = -1.0, bestv = 0.0;
+                int bi = 0x7fffffff;
+                #pragma unroll
+                for (int ri = 0; ri < RW; ++ri) {
+                    const int i = w + NW * ri;
+                    if (i < b) {
+                        colbuf[i] = a[ri][ck];
+                        double m = fabs(a[ri][ck]);
+                        if (!(m == m)) m = INFINITY;   // a NaN pivot propagates
+                        if (!((used >> ri) & 1u) && (m > best || (m == best && i < bi))) { best = m; bi = i; bestv = a[ri][ck]; }
+                    }
+                }
+                cand_v[w] = best;
+                cand_a[w] = bestv;
+                cand_i[w] = bi;
+            }
+            __syncthreads();
+            // (b) every thread picks the pivot from the 16 candidates
+            double best = -1.0, piv = 0.0;
+            int p = 0x7fffffff;
+            #pragma unroll
+            for (int q = 0; q < NW; ++q) {
+                const double v = cand_v[q];
+                const int iq = cand_i[q];
+                if (v > best || (v == best && iq < p)) { best = v; p = iq; piv = cand_a[q]; }
+            }
+            if (piv == 0.0) { singular = true; piv = 1.0; }
+            const double rp = 1.0 / piv;
+            const int pw = p % NW, prr = p / NW;
+            if (w == pw) {
+                used |= 1u << prr;
+                #pragma unroll
+                for (int cl = 0; cl < CL; ++cl) {
+                    double v = 0.0;
+                    #pragma unroll
+                    for (int ri = 0; ri < RW; ++ri) if (ri == prr) v = a[ri][cl];
+                    if (cl == ck && lane == lk) v = 1.0;
+                    rowbuf[buf][lane + 32 * cl] = v * rp;
+                }
+            }
+            if (threadIdx.x == 0) pivrow[k] = p;
+            __syncthreads();
+            // (c) rank-1 update; row p becomes the scaled pivot row, column k
+            // becomes -a(i,k)/piv
+            double rv[CL];
+            #pragma unroll
+            for (int cl = 0; cl < CL; ++cl) rv[cl] = rowbuf[buf][lane + 32 * cl];
+            #pragma unroll
+            for (int ri = 0; ri < RW; ++ri) {
+                const int i = w + NW * ri;
+                if (i == p) {
+                    #pragma unroll
+                    for (int cl = 0; cl < CL; ++cl) a[ri][cl] = rv[cl];
+                } else {
+                    const double f = (i < b) ? colbuf[i] : 0.0;
+                    #pragma unroll
+                    for (int cl = 0; cl < CL; ++cl) a[ri][cl] = fma(-f, rv[cl], a[ri][cl]);
+                    if (lane == lk) a[ri][ck] = -f * rp;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < b; k += blockDim.x) qinv[pivrow[k]] = k;
+    __syncthreads();
+    #pragma unroll
+    for (int ri = 0; ri < RW; ++ri)
+        #pragma unroll
+        for (int cl = 0; cl < CL; ++cl) {
+            const int i = w + NW * ri, j = lane + 32 * cl;
+            if (i < b && j < b) D[qinv[i] + (int64_t)pivrow[j] * b] = a[ri][cl];
+        }
+    if (singular && threadIdx.x == 0) atomicMin(status, prow_elem[prow]);
+}
+
 // Same algorithm for blocks too large for the register tiles (b > 160):
 // one CTA, matrix kept in global memory (L2 resident), explicit row swaps.
 static __global__ void k_block_inverse_global(double* __restrict__ LD, const int64_t* __restrict__ dinv_off,
@@ -581,7 +792,7 @@ struct IluRows {
 };
 
 template <typename TL, typename TX, typename ACC>
-__global__ void k_ilu_forward(IluRows R, const TL* __restrict__ LD, const int32_t* __restrict__ rows, int row_begin,
+__global__ void __launch_bounds__(1024) k_ilu_forward(IluRows R, const TL* __restrict__ LD, const int32_t* __restrict__ rows, int row_begin,
                               const TX* __restrict__ v, TX* __restrict__ zx) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ACC* xs = reinterpret_cast<ACC*>(smem_raw);
@@ -607,18 +818,7 @@ __global__ void k_ilu_forward(IluRows R, const TL* __restrict__ LD, const int32_
             const int nc = R.lo_nc[q];
             const TL* Lb = LD + R.lo_L[q] + r;
             const ACC* xb = xs + off;
-            int c = g;
-            for (; c + 3 * G < nc; c += 4 * G) {
-                const TL a0 = ld_stream(Lb + (int64_t)c * b);
-                const TL a1 = ld_stream(Lb + (int64_t)(c + G) * b);
-                const TL a2 = ld_stream(Lb + (int64_t)(c + 2 * G) * b);
-                const TL a3 = ld_stream(Lb + (int64_t)(c + 3 * G) * b);
-                acc += cvt<ACC>(a0) * xb[c];
-                acc += cvt<ACC>(a1) * xb[c + G];
-                acc += cvt<ACC>(a2) * xb[c + 2 * G];
-                acc += cvt<ACC>(a3) * xb[c + 3 * G];
-            }
-            for (; c < nc; c += G) acc += cvt<ACC>(ld_stream(Lb + (int64_t)c * b)) * xb[c];
+            acc = stripe_dot(Lb, (int64_t)b, nc, g, G, xb, acc);
             off += nc;
         }
     }
@@ -634,7 +834,7 @@ __global__ void k_ilu_forward(IluRows R, const TL* __restrict__ LD, const int32_
 }
 
 template <typename TL, typename TU, typename TX, typename ACC>
-__global__ void k_ilu_backward(IluRows R, const TL* __restrict__ LD, const TU* __restrict__ Aval,
+__global__ void __launch_bounds__(1024) k_ilu_backward(IluRows R, const TL* __restrict__ LD, const TU* __restrict__ Aval,
                                const int32_t* __restrict__ rows, int row_begin, TX* __restrict__ zx) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ACC* xs = reinterpret_cast<ACC*>(smem_raw);
@@ -662,18 +862,7 @@ __global__ void k_ilu_backward(IluRows R, const TL* __restrict__ LD, const TU* _
             const int nc = R.up_nc[q];
             const TU* Ub = Aval + R.up_U[q] + r;
             const ACC* xb = xs + off;
-            int c = g;
-            for (; c + 3 * G < nc; c += 4 * G) {
-                const TU a0 = ld_stream(Ub + (int64_t)c * b);
-                const TU a1 = ld_stream(Ub + (int64_t)(c + G) * b);
-                const TU a2 = ld_stream(Ub + (int64_t)(c + 2 * G) * b);
-                const TU a3 = ld_stream(Ub + (int64_t)(c + 3 * G) * b);
-                acc += cvt<ACC>(a0) * xb[c];
-                acc += cvt<ACC>(a1) * xb[c + G];
-                acc += cvt<ACC>(a2) * xb[c + 2 * G];
-                acc += cvt<ACC>(a3) * xb[c + 3 * G];
-            }
-            for (; c < nc; c += G) acc += cvt<ACC>(ld_stream(Ub + (int64_t)c * b)) * xb[c];
+            acc = stripe_dot(Ub, (int64_t)b, nc, g, G, xb, acc);
             off += nc;
         }
         red[g * b + r] = acc;
@@ -689,18 +878,7 @@ __global__ void k_ilu_backward(IluRows R, const TL* __restrict__ LD, const TU* _
     acc = 0;
     if (g < G) {
         const TL* Db = LD + R.dinv_off[pr] + r;
-        int c = g;
-        for (; c + 3 * G < b; c += 4 * G) {
-            const TL a0 = ld_stream(Db + (int64_t)c * b);
-            const TL a1 = ld_stream(Db + (int64_t)(c + G) * b);
-            const TL a2 = ld_stream(Db + (int64_t)(c + 2 * G) * b);
-            const TL a3 = ld_stream(Db + (int64_t)(c + 3 * G) * b);
-            acc += cvt<ACC>(a0) * tvec[c];
-            acc += cvt<ACC>(a1) * tvec[c + G];
-            acc += cvt<ACC>(a2) * tvec[c + 2 * G];
-            acc += cvt<ACC>(a3) * tvec[c + 3 * G];
-        }
-        for (; c < b; c += G) acc += cvt<ACC>(ld_stream(Db + (int64_t)c * b)) * tvec[c];
+        acc = stripe_dot(Db, (int64_t)b, b, g, G, tvec, acc);
     }
     __syncthreads();
     if (g < G) red[g * b + r] = acc;
@@ -709,6 +887,139 @@ __global__ void k_ilu_backward(IluRows R, const TL* __restrict__ LD, const TU* _
         ACC s = 0;
         for (int gg = 0; gg < G; ++gg) s += red[gg * b + tid];
         zx[R.z_off[pr] + tid] = from_d<TX>((double)s);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// ILU programme: dependency-driven sweeps (one launch per sweep).
+// CTAs take programme rows from an atomic ticket counter in a topological
+// order (level-major).  A row waits, through per-row flags stamped with the
+// sweep's epoch, only for its own parents, so no grid-wide barrier separates
+// the levels.  Deadlock-free at any occupancy: a ticket holder only waits on
+// rows with smaller tickets, whose holders are already running.  Every wait
+// is bounded (about a second of clock cycles); when it runs out, status
+// records ETIMEOUT and the sweep carries on with whatever it has, so the
+// kernel always terminates.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
+}
+// wait (thread 0 only) until flags[row] == epoch; false on timeout
+__device__ __forceinline__ bool wait_flag(const unsigned* flags, int row, unsigned epoch, long long limit) {
+    if (ld_acquire(flags + row) == epoch) return true;
+    const long long t0 = clock64();
+    while (ld_acquire(flags + row) != epoch) {
+        if (clock64() - t0 > limit) return false;
+        __nanosleep(64);
+    }
+    return true;
+}
+template <typename T> __device__ __forceinline__ T ld_cg(const T* p) { return __ldcg(p); }
+
+struct SweepSync {
+    unsigned* counter;      // ticket counter, zero at launch
+    unsigned* flags;        // per programme row
+    unsigned epoch;
+    int* status;            // set to CHIDG_GPU_ETIMEOUT-like code on a timeout
+    long long spin_limit;   // clock cycles
+};
+
+template <typename TL, typename TU, typename TX, typename ACC, bool FORWARD>
+__global__ void __launch_bounds__(1024) k_ilu_sweep_sf(IluRows R, const TL* __restrict__ LD, const TU* __restrict__ Aval,
+                               const int32_t* __restrict__ order, int nrows, const TX* __restrict__ v,
+                               TX* __restrict__ zx, SweepSync S) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ACC* xs = reinterpret_cast<ACC*>(smem_raw);
+    __shared__ int s_row;
+    __shared__ int s_ok;
+    const int tid = threadIdx.x;
+    for (;;) {
+        if (tid == 0) {
+            const unsigned t = atomicAdd(S.counter, 1u);
+            s_row = (t < (unsigned)nrows) ? order[t] : -1;
+            s_ok = 1;
+        }
+        __syncthreads();
+        const int pr = s_row;
+        if (pr < 0) break;
+        const int b = R.prow_b[pr];
+        const int q0 = FORWARD ? R.lo_ptr[pr] : R.up_ptr[pr];
+        const int q1 = FORWARD ? R.lo_ptr[pr + 1] : R.up_ptr[pr + 1];
+        const int32_t* par = FORWARD ? R.lo_par : R.up_par;
+        const int32_t* ncs = FORWARD ? R.lo_nc : R.up_nc;
+        if (tid == 0)
+            for (int q = q0; q < q1; ++q)
+                if (!wait_flag(S.flags, par[q], S.epoch, S.spin_limit)) { s_ok = 0; atomicExch(S.status, 1); }
+        __syncthreads();
+        int off = 0;
+        for (int q = q0; q < q1; ++q) {
+            const int nc = ncs[q];
+            const TX* zp = zx + R.z_off[par[q]];
+            for (int c = tid; c < nc; c += blockDim.x) xs[off + c] = cvt<ACC>(ld_cg(zp + c));
+            off += nc;
+        }
+        const int ncols_total = off;
+        ACC* tvec = xs + ncols_total;
+        ACC* red = tvec + b;
+        __syncthreads();
+        const int G = blockDim.x / b;
+        const int r = tid % b, g = tid / b;
+        ACC acc = 0;
+        if (g < G) {
+            off = 0;
+            for (int q = q0; q < q1; ++q) {
+                const int nc = ncs[q];
+                const ACC* xb = xs + off;
+                int c = g;
+                if (FORWARD) {
+                    const TL* Bb = LD + R.lo_L[q] + r;
+                    acc = stripe_dot(Bb, (int64_t)b, nc, c, G, xb, acc);
+                } else {
+                    const TU* Bb = Aval + R.up_U[q] + r;
+                    acc = stripe_dot(Bb, (int64_t)b, nc, c, G, xb, acc);
+                }
+                off += nc;
+            }
+            red[g * b + r] = acc;
+        }
+        __syncthreads();
+        if (FORWARD) {
+            if (tid < b) {
+                ACC s = 0;
+                for (int gg = 0; gg < G; ++gg) s += red[gg * b + tid];
+                zx[R.z_off[pr] + tid] = from_d<TX>(to_d(v[R.v_off[pr] + tid]) - (double)s);
+            }
+        } else {
+            if (tid < b) {
+                ACC s = 0;
+                for (int gg = 0; gg < G; ++gg) s += red[gg * b + tid];
+                const double t = to_d(zx[R.z_off[pr] + tid]) - (double)s;
+                tvec[tid] = cvt<ACC>(from_d<TX>(t));
+            }
+            __syncthreads();
+            acc = 0;
+            if (g < G) {
+                const TL* Db = LD + R.dinv_off[pr] + r;
+                acc = stripe_dot(Db, (int64_t)b, b, g, G, tvec, acc);
+            }
+            __syncthreads();
+            if (g < G) red[g * b + r] = acc;
+            __syncthreads();
+            if (tid < b) {
+                ACC s = 0;
+                for (int gg = 0; gg < G; ++gg) s += red[gg * b + tid];
+                zx[R.z_off[pr] + tid] = from_d<TX>((double)s);
+            }
+        }
+        // publish: every writer fences its stores, then one thread stamps the flag
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) st_release(S.flags + pr, S.epoch);
     }
 }
 

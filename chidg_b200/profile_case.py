@@ -20,19 +20,27 @@ def main():
     ap.add_argument("--p", type=int, default=2)
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--precon", default="ilu0")
+    ap.add_argument("--schedule", default="dataflow", choices=["dataflow", "levels"])
+    ap.add_argument("--time", action="store_true", help="print CUDA-event times per kernel class")
     args = ap.parse_args()
     pat = mesh.box_pattern(args.n, args.n, args.n, 5, mesh.nterms_of_order(args.p))
     A = api.ChidgMatrix(pat)
     A.upload(mesh.synth_values(pat, seed=1))
     v = api.ChidgVector(A, mesh.synth_vector(A.n, seed=2))
     z = api.ChidgVector(A)
-    M = api.create_preconditioner(args.precon)
+    M = api.create_preconditioner(args.precon, schedule=args.schedule)
+    if args.time:
+        A.ctx.set_profiling(True)
     for _ in range(args.reps):
         M.update(A)
         M.apply(A, v, z)
         api.chidg_mv(A, v, z)
     A.ctx.sync()
-    print(f"profile_case n={args.n} p={args.p}: {A.ctx.launches()} launches")
+    print(f"profile_case n={args.n} p={args.p} schedule={args.schedule}: {A.ctx.launches()} launches")
+    if args.time:
+        for name, (ms, cnt) in A.ctx.kernel_times().items():
+            if cnt:
+                print(f"  {name:14s} {cnt:4d} x {ms / cnt:9.3f} ms")
 
 
 if __name__ == "__main__":

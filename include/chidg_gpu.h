@@ -215,6 +215,14 @@ int chidg_gpu_precon_update(chidg_gpu_precon* M, chidg_gpu_matrix* A, int32_t pr
 /* %apply(A,v) -> z: precon_ILU0.f90:286-411 / precon_RASILU0.f90:454-625. */
 int chidg_gpu_precon_apply(chidg_gpu_precon* M, chidg_gpu_matrix* A,
                            const chidg_gpu_vector* v, chidg_gpu_vector* z);
+/* Schedule of the triangular sweeps of precon%apply:
+ * CHIDG_SCHED_LEVELS   one kernel launch per dependency level (wavefront);
+ * CHIDG_SCHED_DATAFLOW one launch per sweep, rows taken in topological order,
+ *                      each waiting (bounded) only for its own parents.
+ * Both compute the same arithmetic; DATAFLOW is the default. */
+#define CHIDG_SCHED_LEVELS   0
+#define CHIDG_SCHED_DATAFLOW 1
+int chidg_gpu_precon_set_schedule(chidg_gpu_precon* M, int32_t schedule);
 /* Packed factor blocks (L blocks and inverted diagonals at the positions of
  * the matrix's LOCAL blocks, zero elsewhere), as precon_ILU0_t%LD holds them. */
 int chidg_gpu_precon_download_LD(chidg_gpu_precon* M, double* host);

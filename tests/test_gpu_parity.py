@@ -53,13 +53,14 @@ def test_dot_norm_axpy():
     assert relerr(yg.download(), y - 0.5 * x) < 1e-15
 
 
+@pytest.mark.parametrize("schedule", ["levels", "dataflow"])
 @pytest.mark.parametrize("kind", ["ilu0", "jacobi"])
 @pytest.mark.parametrize("shape,P,nt", CASES)
-def test_precon_factor_and_apply(kind, shape, P, nt):
+def test_precon_factor_and_apply(kind, shape, P, nt, schedule):
     pat, vals, Ao, Ag = setup(shape, P, nt, seed=5)
     Mo = O.OraclePrecon(Ao, kind)
     Mo.update()
-    Mg = api.create_preconditioner(kind)
+    Mg = api.create_preconditioner(kind, schedule=schedule)
     Mg.update(Ag)
     LDo, LDg = Mo.LD(), Mg.LD()
     voff, _ = pat.value_offsets()
@@ -76,12 +77,13 @@ def test_precon_factor_and_apply(kind, shape, P, nt):
     assert relerr(z, Mo.apply(v)) < 1e-11
 
 
+@pytest.mark.parametrize("schedule", ["levels", "dataflow"])
 @pytest.mark.parametrize("shape,P,sub", [((4, 4, 2), 1, (2, 2, 1)), ((4, 4, 4), 0, (2, 2, 2)), ((6, 3, 3), 1, (3, 1, 1))])
-def test_rasilu0(shape, P, sub):
+def test_rasilu0(shape, P, sub, schedule):
     pat, vals, Ao, Ag = setup(shape, P, 1, sub=sub, seed=7)
     Mo = O.OraclePrecon(Ao, "rasilu0")
     Mo.update()
-    Mg = api.create_preconditioner("rasilu0")
+    Mg = api.create_preconditioner("rasilu0", schedule=schedule)
     Mg.update(Ag)
     v = mesh.synth_vector(Ao.n, seed=8)
     z = Mg.apply(Ag, api.ChidgVector(Ag, v)).download()
@@ -104,6 +106,19 @@ def test_fgmres_parity(prec, shape, P, nt, orth):
     assert relerr(solver.hist, ro["hist"]) < 1e-8
     assert relerr(xg.download(), xo) < 1e-10
     assert solver.residual_norm == pytest.approx(ro["residual_norm"], rel=1e-6)
+
+
+@pytest.mark.parametrize("kind,sub", [("ilu0", (1, 1, 1)), ("rasilu0", (2, 2, 2))])
+def test_schedules_bitwise_identical(kind, sub):
+    """Both sweep schedules run the same per-row arithmetic."""
+    pat, vals, Ao, Ag = setup((6, 6, 4), 1, sub=sub, seed=22)
+    v = api.ChidgVector(Ag, mesh.synth_vector(Ao.n, seed=23))
+    out = []
+    for sched in ("levels", "dataflow"):
+        M = api.create_preconditioner(kind, schedule=sched)
+        M.update(Ag)
+        out.append(M.apply(Ag, v).download())
+    assert np.array_equal(out[0], out[1])
 
 
 def test_fgmres_inner_default_options():
