@@ -199,6 +199,20 @@ int chidg_gpu_vector_scale(chidg_gpu_vector* x, double a);                      
 int chidg_gpu_vector_dot(const chidg_gpu_vector* x, const chidg_gpu_vector* y, double* out);
 int chidg_gpu_vector_norm(const chidg_gpu_vector* x, double* out);
 
+/* Dot product of two device arrays that allocates no device memory.  It has
+ * no counterpart in the reference.  It is for callers that cannot call
+ * cudaMalloc at the point where they need a reduction: code running while a
+ * stream is captured into a CUDA graph, or frameworks that own all device
+ * memory through their own pool.  x, y (n doubles) and result (one double)
+ * are device pointers on `device`; the work is queued on `stream` (NULL = the
+ * default stream) and result is written asynchronously.  Partial sums live in
+ * a fixed 128 KiB array inside this library on every GPU that loads it, so
+ * n <= 67 108 864 (larger n returns CHIDG_GPU_EINVAL).  The first call on a
+ * device looks up that array's device address; make it before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race
+ * and must be serialised by the caller. */
+int chidg_gpu_dot_noalloc(int device, const double* x, const double* y, int64_t n, double* result, void* stream);
+
 /* ---- chidg_mv (src/containers/operator_chidg_mv.f90:46-645) --------------- */
 /* y = A x over lblks, chi_blks, bc_blks and hb_blks (hb at tparent). */
 int chidg_gpu_matvec(chidg_gpu_matrix* A, const chidg_gpu_vector* x, chidg_gpu_vector* y);
