@@ -468,13 +468,21 @@ extern "C" int chidg_gpu_matrix_scale_diagonal(chidg_gpu_matrix* A, const double
 int chidg::matrix_lowp(chidg_gpu_matrix* A, int precision) {
     chidg_gpu_ctx* ctx = A->ctx;
     if (precision == CHIDG_GPU_FP64) return CHIDG_GPU_OK;
-    if (A->val32_stamp == A->stamp) return CHIDG_GPU_OK;
-    int st = ensure(ctx, A->val32, sizeof(float) * (size_t)A->nval);
-    if (st) return st;
-    k_convert<double, float><<<grid_for(A->nval, 256, ctx->nsm * 8), 256, 0, ctx->stream>>>(A->nval, (const double*)A->val.ptr, (float*)A->val32.ptr);
-    st = check_launch(ctx, "k_convert A->fp32");
-    if (st) return st;
-    A->val32_stamp = A->stamp;
+    const int grid = grid_for(A->nval, 256, ctx->nsm * 8);
+    int st;
+    if (precision == CHIDG_GPU_MIXED_FP32) {
+        if (A->val32_stamp == A->stamp) return CHIDG_GPU_OK;
+        if ((st = ensure(ctx, A->val32, sizeof(float) * (size_t)A->nval))) return st;
+        k_convert<double, float><<<grid, 256, 0, ctx->stream>>>(A->nval, (const double*)A->val.ptr, (float*)A->val32.ptr);
+        if ((st = check_launch(ctx, "k_convert A->fp32"))) return st;
+        A->val32_stamp = A->stamp;
+    } else {
+        if (A->val16_stamp == A->stamp) return CHIDG_GPU_OK;
+        if ((st = ensure(ctx, A->val16, sizeof(__nv_bfloat16) * (size_t)A->nval))) return st;
+        k_convert<double, __nv_bfloat16><<<grid, 256, 0, ctx->stream>>>(A->nval, (const double*)A->val.ptr, (__nv_bfloat16*)A->val16.ptr);
+        if ((st = check_launch(ctx, "k_convert A->bf16"))) return st;
+        A->val16_stamp = A->stamp;
+    }
     return CHIDG_GPU_OK;
 }
 
@@ -493,6 +501,7 @@ int chidg::matvec_launch(chidg_gpu_matrix* A, const TA* val, const TV* x, TV* y,
 }
 template int chidg::matvec_launch<double, double>(chidg_gpu_matrix*, const double*, const double*, double*, const double*, double, double, double*);
 template int chidg::matvec_launch<float, float>(chidg_gpu_matrix*, const float*, const float*, float*, const float*, double, double, double*);
+template int chidg::matvec_launch<__nv_bfloat16, float>(chidg_gpu_matrix*, const __nv_bfloat16*, const float*, float*, const float*, double, double, double*);
 
 int chidg::set_matvec_smem(chidg_gpu_matrix* A) {
     // allow > 48 KB dynamic shared memory when a row has many wide blocks
@@ -500,6 +509,7 @@ int chidg::set_matvec_smem(chidg_gpu_matrix* A) {
     if (smem > 48 * 1024) {
         cudaFuncSetAttribute(k_matvec<double, double, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         cudaFuncSetAttribute(k_matvec<float, float, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_matvec<__nv_bfloat16, float, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     }
     return CHIDG_GPU_OK;
 }
@@ -1006,19 +1016,12 @@ static int launch_inverse(chidg_gpu_precon* M, int row_begin, int count) {
                                                              (const int32_t*)P.d_prow_b.ptr,                        \
                                                              (const int32_t*)P.d_prow_elem.ptr,                     \
                                                              (const int32_t*)P.d_fwd_rows.ptr, row_begin, ctx->d_status)
-    if (bmax <= 32)
-        k_block_inverse<1, 1, 32><<<count, 1024, 0, ctx->stream>>>(LD, (const int64_t*)P.d_dinv_off.ptr, (const int32_t*)P.d_prow_b.ptr,
-                                                                  (const int32_t*)P.d_prow_elem.ptr, (const int32_t*)P.d_fwd_rows.ptr, row_begin, ctx->d_status);
-    else if (bmax <= 64)
-        k_block_inverse<2, 2, 32><<<count, 1024, 0, ctx->stream>>>(LD, (const int64_t*)P.d_dinv_off.ptr, (const int32_t*)P.d_prow_b.ptr,
-                                                                  (const int32_t*)P.d_prow_elem.ptr, (const int32_t*)P.d_fwd_rows.ptr, row_begin, ctx->d_status);
-    else if (bmax <= 96)
-        k_block_inverse<3, 3, 32><<<count, 1024, 0, ctx->stream>>>(LD, (const int64_t*)P.d_dinv_off.ptr, (const int32_t*)P.d_prow_b.ptr,
-                                                                  (const int32_t*)P.d_prow_elem.ptr, (const int32_t*)P.d_fwd_rows.ptr, row_begin, ctx->d_status);
-    else if (bmax <= 160)
-        k_block_inverse<5, 10, 16><<<count, 512, 0, ctx->stream>>>(LD, (const int64_t*)P.d_dinv_off.ptr, (const int32_t*)P.d_prow_b.ptr,
-                                                                  (const int32_t*)P.d_prow_elem.ptr, (const int32_t*)P.d_fwd_rows.ptr, row_begin, ctx->d_status);
-#undef CHIDG_INV2
+    if (bmax <= 32) CHIDG_INV2(1, 2);
+    else if (bmax <= 64) CHIDG_INV2(2, 4);
+    else if (bmax <= 96) CHIDG_INV2(3, 6);
+    else if (bmax <= 128) CHIDG_INV2(4, 8);
+    else if (bmax <= 144) CHIDG_INV2(5, 9);
+    else if (bmax <= 160) CHIDG_INV2(5, 10);
     else {
         int st = ensure(ctx, M->piv_scratch, sizeof(int) * 1024 * (size_t)std::max(count, 1));
         if (st) return st;
@@ -1045,17 +1048,31 @@ extern "C" int chidg_gpu_precon_update(chidg_gpu_precon* M, chidg_gpu_matrix* A,
     cudaMemcpyAsync(ctx->d_status, &big, sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
     const int nlev = (int)P.fwd_ptr.size() - 1;
     const int tiles_1d = (P.max_b + GT_M - 1) / GT_M;
+    // one CTA per output block on the FP64 tensor cores when blocks fit 136 x 136
+    const bool use_dmma = P.max_b <= DM_MAX;
+    if (use_dmma)
+        cudaFuncSetAttribute(k_task_gemm_dmma<double, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DM_SMEM);
     const int ph = prof_begin(ctx, kProfFactor);
     for (int l = 0; l < nlev; ++l) {
         const int nl = P.ltask_ptr[l + 1] - P.ltask_ptr[l];
-        if (nl > 0) {
+        if (nl > 0 && use_dmma) {
+            k_task_gemm_dmma<double, double, double><<<nl, DM_THREADS, DM_SMEM, ctx->stream>>>(
+                (const GemmTask*)P.d_ltasks.ptr + P.ltask_ptr[l], (const GemmPair*)P.d_lpairs.ptr,
+                (const double*)A->val.ptr, (const double*)M->LD.ptr, nullptr, (double*)M->LD.ptr, 1.0);
+            if ((st = check_launch(ctx, "k_task_gemm_dmma L"))) return st;
+        } else if (nl > 0) {
             k_task_gemm<double, double, double><<<nl * tiles_1d * tiles_1d, 256, 0, ctx->stream>>>(
                 (const GemmTask*)P.d_ltasks.ptr + P.ltask_ptr[l], (const GemmPair*)P.d_lpairs.ptr, tiles_1d, tiles_1d,
                 (const double*)A->val.ptr, (const double*)M->LD.ptr, nullptr, (double*)M->LD.ptr, 1.0);
             if ((st = check_launch(ctx, "k_task_gemm L"))) return st;
         }
         const int ns = P.stask_ptr[l + 1] - P.stask_ptr[l];
-        if (ns > 0) {
+        if (ns > 0 && use_dmma) {
+            k_task_gemm_dmma<double, double, double><<<ns, DM_THREADS, DM_SMEM, ctx->stream>>>(
+                (const GemmTask*)P.d_stasks.ptr + P.stask_ptr[l], (const GemmPair*)P.d_spairs.ptr,
+                (const double*)M->LD.ptr, (const double*)A->val.ptr, (const double*)A->val.ptr, (double*)M->LD.ptr, -1.0);
+            if ((st = check_launch(ctx, "k_task_gemm_dmma S"))) return st;
+        } else if (ns > 0) {
             k_task_gemm<double, double, double><<<ns * tiles_1d * tiles_1d, 256, 0, ctx->stream>>>(
                 (const GemmTask*)P.d_stasks.ptr + P.stask_ptr[l], (const GemmPair*)P.d_spairs.ptr, tiles_1d, tiles_1d,
                 (const double*)M->LD.ptr, (const double*)A->val.ptr, (const double*)A->val.ptr, (double*)M->LD.ptr, -1.0);
@@ -1167,7 +1184,7 @@ int chidg::precon_apply_impl(chidg_gpu_precon* M, const TV* v, TV* z, int precis
     int st;
     if (M->schedule == CHIDG_SCHED_DATAFLOW) {
         if (precision == CHIDG_GPU_MIXED_BF16 && sizeof(TV) == 4)
-            st = dataflow_sweeps(M, (const __nv_bfloat16*)M->LD16.ptr, (const float*)A->val32.ptr, v, zx, 2);
+            st = dataflow_sweeps(M, (const __nv_bfloat16*)M->LD16.ptr, (const __nv_bfloat16*)A->val16.ptr, v, zx, 2);
         else if (sizeof(TV) == 4)
             st = dataflow_sweeps(M, (const float*)M->LD32.ptr, (const float*)A->val32.ptr, v, zx, 1);
         else
@@ -1197,7 +1214,7 @@ int chidg::precon_apply_impl(chidg_gpu_precon* M, const TV* v, TV* z, int precis
     for (int l = 0; l < nb; ++l) {
         const int cnt = P.bwd_ptr[l + 1] - P.bwd_ptr[l];
         if (precision == CHIDG_GPU_MIXED_BF16 && sizeof(TV) == 4)
-            k_ilu_backward<__nv_bfloat16, float, TV, ACC><<<cnt, threads, smem_b, ctx->stream>>>(P.rows, (const __nv_bfloat16*)M->LD16.ptr, (const float*)A->val32.ptr, (const int32_t*)P.d_bwd_rows.ptr, P.bwd_ptr[l], zx);
+            k_ilu_backward<__nv_bfloat16, __nv_bfloat16, TV, ACC><<<cnt, threads, smem_b, ctx->stream>>>(P.rows, (const __nv_bfloat16*)M->LD16.ptr, (const __nv_bfloat16*)A->val16.ptr, (const int32_t*)P.d_bwd_rows.ptr, P.bwd_ptr[l], zx);
         else if (sizeof(TV) == 4)
             k_ilu_backward<float, float, TV, ACC><<<cnt, threads, smem_b, ctx->stream>>>(P.rows, (const float*)M->LD32.ptr, (const float*)A->val32.ptr, (const int32_t*)P.d_bwd_rows.ptr, P.bwd_ptr[l], zx);
         else
@@ -1227,7 +1244,7 @@ int chidg::precon_set_smem(chidg_gpu_precon* M) {
     if (sb > 48 * 1024) {
         cudaFuncSetAttribute(k_ilu_backward<double, double, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
         cudaFuncSetAttribute(k_ilu_backward<float, float, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
-        cudaFuncSetAttribute(k_ilu_backward<__nv_bfloat16, float, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
+        cudaFuncSetAttribute(k_ilu_backward<__nv_bfloat16, __nv_bfloat16, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
     }
     return CHIDG_GPU_OK;
 }

@@ -96,7 +96,7 @@ struct chidg_gpu_matrix {
     std::vector<int32_t> diag;
     int max_row_cols = 0, max_b = 0, mv_threads = 32;
     chidg::Buffer val, val32, val16;
-    int64_t val32_stamp = -1;
+    int64_t val32_stamp = -1, val16_stamp = -1;
     chidg::Buffer d_row_ptr, d_blk_voff, d_blk_xoff, d_blk_nc, d_row_yoff, d_row_b, d_diag_voff, d_elem_nvars,
         d_elem_nterms, row_sq;
     int64_t stamp = 0;

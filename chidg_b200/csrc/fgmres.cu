@@ -75,6 +75,7 @@ struct Solver {
     double inner_tol = 0.1, inner_rtol = 0.1;
     int inner_nmax = 100, inner_nkrylov = 100, inner_orth = CHIDG_ORTH_CGS;
     bool true_residual = true;
+    int precision = CHIDG_GPU_FP64;     // float solvers: which low-precision copy of A
     // state
     int niter = 0, nrestart = 0;
     int64_t inner_iters = 0;
@@ -85,7 +86,6 @@ struct Solver {
     std::unique_ptr<Solver<T>> child;
     Buffer V, Z, x0, zr, dz, tmp, rowsq;
 
-    const T* aval() const;
     ~Solver() { for (Buffer* b : {&V, &Z, &x0, &zr, &dz, &tmp, &rowsq}) release(*b); }
 
     int matvec(const T* x, T* y, const T* z, double alpha, double beta, bool want_norm, int slot) {
@@ -95,11 +95,12 @@ struct Solver {
             if (st) return st;
             rs = (double*)rowsq.ptr;
         }
-        int st = matvec_launch<T, T>(A, aval(), x, y, z, alpha, beta, rs);
+        int st = launch_mv(x, y, z, alpha, beta, rs);
         if (st) return st;
         if (want_norm) return reduce_partials(ctx, rs, A->nrow, 1, slot, false);
         return CHIDG_GPU_OK;
     }
+    int launch_mv(const T* x, T* y, const T* z, double alpha, double beta, double* rs);
     int axpby(double a, const T* x, double b, T* y) {
         const int64_t n = A->n;
         k_axpby<T, T><<<grid_for(n, 256, ctx->nsm * 8), 256, 0, ctx->stream>>>(n, a, nullptr, x, b, y);
@@ -261,8 +262,17 @@ struct Solver {
         return CHIDG_GPU_OK;
     }
 };
-template <> const double* Solver<double>::aval() const { return (const double*)A->val.ptr; }
-template <> const float* Solver<float>::aval() const { return (const float*)A->val32.ptr; }
+
+template <>
+int Solver<double>::launch_mv(const double* x, double* y, const double* z, double alpha, double beta, double* rs) {
+    return matvec_launch<double, double>(A, (const double*)A->val.ptr, x, y, z, alpha, beta, rs);
+}
+template <>
+int Solver<float>::launch_mv(const float* x, float* y, const float* z, double alpha, double beta, double* rs) {
+    if (precision == CHIDG_GPU_MIXED_BF16)
+        return matvec_launch<__nv_bfloat16, float>(A, (const __nv_bfloat16*)A->val16.ptr, x, y, z, alpha, beta, rs);
+    return matvec_launch<float, float>(A, (const float*)A->val32.ptr, x, y, z, alpha, beta, rs);
+}
 
 }  // namespace
 
@@ -333,6 +343,7 @@ extern "C" int chidg_gpu_fgmres_solve(chidg_gpu_matrix* A, chidg_gpu_precon* M, 
         lo->tol = 0.0; lo->rtol = o.mixed_inner_rtol; lo->nmax = o.mixed_inner_nmax;
         lo->nkrylov = o.mixed_inner_nkrylov; lo->orth = CHIDG_ORTH_CGS; lo->inner = false;
         lo->true_residual = false;
+        lo->precision = prec;
         lo->precon = [M, prec](const float* v, float* z) { return precon_apply_impl<float>(M, v, z, prec); };
         if ((st = ensure(ctx, v32, sizeof(float) * (size_t)A->n)) || (st = ensure(ctx, z32, sizeof(float) * (size_t)A->n))) return st;
         Solver<float>* lp = lo.get();

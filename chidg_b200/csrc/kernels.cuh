@@ -50,20 +50,26 @@ template <> __device__ __forceinline__ __nv_bfloat16 ld_stream<__nv_bfloat16>(co
 }
 
 // acc + sum over the column stripe c = g, g+G, ... < nc of B[c*ld] * x[c],
-// summed in increasing c (the same order in every kernel that uses it), with
-// eight independent loads in flight per thread.
+// summed in increasing c (the same order in every kernel that uses it).  The
+// loads go out in predicated batches of 16, so a thread never waits on more
+// than ceil(stripe / 16) round trips to memory.
 template <typename T, typename ACC>
 __device__ __forceinline__ ACC stripe_dot(const T* __restrict__ B, int64_t ld, int nc, int g, int G,
                                           const ACC* __restrict__ x, ACC acc) {
-    int c = g;
-    for (; c + 7 * G < nc; c += 8 * G) {
-        T a[8];
+    constexpr int U = 16;
+    for (int c = g; c < nc; c += U * G) {
+        T a[U];
         #pragma unroll
-        for (int u = 0; u < 8; ++u) a[u] = ld_stream(B + (int64_t)(c + u * G) * ld);
+        for (int u = 0; u < U; ++u) {
+            const int cc = c + u * G;
+            a[u] = (cc < nc) ? ld_stream(B + (int64_t)cc * ld) : T(0);
+        }
         #pragma unroll
-        for (int u = 0; u < 8; ++u) acc += cvt<ACC>(a[u]) * x[c + u * G];
+        for (int u = 0; u < U; ++u) {
+            const int cc = c + u * G;
+            if (cc < nc) acc += cvt<ACC>(a[u]) * x[cc];
+        }
     }
-    for (; c < nc; c += G) acc += cvt<ACC>(ld_stream(B + (int64_t)c * ld)) * x[c];
     return acc;
 }
 
@@ -409,10 +415,14 @@ __global__ void __launch_bounds__(DM_THREADS) k_task_gemm_dmma(const GemmTask* _
             __syncthreads();
             for (int k4 = 0; k4 < kc; k4 += 4) {
                 double af[DM_TI], bf[DM_TJ];
+                // tiles past the 17th (rows/columns >= 136) exist only in the
+                // warp grid: never read them
                 #pragma unroll
-                for (int i = 0; i < DM_TI; ++i) af[i] = As[(k4 + tq) * DM_MAX + (wm + DM_WM * i) * 8 + g];
+                for (int i = 0; i < DM_TI; ++i)
+                    af[i] = (wm + DM_WM * i < tm) ? As[(k4 + tq) * DM_MAX + (wm + DM_WM * i) * 8 + g] : 0.0;
                 #pragma unroll
-                for (int j = 0; j < DM_TJ; ++j) bf[j] = Bs[(k4 + tq) * DM_MAX + (wn + DM_WN * j) * 8 + g];
+                for (int j = 0; j < DM_TJ; ++j)
+                    bf[j] = (wn + DM_WN * j < tn) ? Bs[(k4 + tq) * DM_MAX + (wn + DM_WN * j) * 8 + g] : 0.0;
                 #pragma unroll
                 for (int i = 0; i < DM_TI; ++i) {
                     if (wm + DM_WM * i >= tm) continue;
