@@ -58,7 +58,7 @@ class Context:
         return c.value
 
     PROFILE_CLASSES = {"matvec": 0, "ilu_forward": 1, "ilu_backward": 2, "factor": 3, "matvec_fp32": 4,
-                       "ilu_lowp": 5}
+                       "ilu_lowp": 5, "factor_gemm": 6, "factor_inverse": 7}
 
     def set_profiling(self, on: bool):
         self.check(self.L.chidg_gpu_ctx_set_profiling(self.h, int(bool(on))), "set_profiling")
@@ -238,7 +238,7 @@ PRECISIONS = {"fp64": _lib.FP64, "mixed_fp32": _lib.MIXED_FP32, "mixed_bf16": _l
 class Preconditioner:
     """preconditioner_t: init / update / apply / tear_down."""
 
-    def __init__(self, kind: str, schedule: str = "dataflow"):
+    def __init__(self, kind: str, schedule: str = "tasks"):
         self.kind = kind.lower()
         self.schedule = schedule
         if self.kind not in PRECON_KINDS:
@@ -256,10 +256,11 @@ class Preconditioner:
         return self
 
     def set_schedule(self, schedule: str):
-        """'levels' (one launch per wavefront) or 'dataflow' (one launch per sweep)."""
+        """'levels' (one launch per wavefront), 'dataflow' (one launch per sweep,
+        row granularity) or 'tasks' (one launch per sweep, block granularity)."""
         self.schedule = schedule
         if self.h is not None:
-            code = {"levels": _lib.SCHED_LEVELS, "dataflow": _lib.SCHED_DATAFLOW}[schedule]
+            code = {"levels": _lib.SCHED_LEVELS, "dataflow": _lib.SCHED_DATAFLOW, "tasks": _lib.SCHED_TASKS}[schedule]
             self.A.ctx.check(self.A.ctx.L.chidg_gpu_precon_set_schedule(self.h, code), "set_schedule")
 
     def update(self, A: ChidgMatrix, b=None, precision: str = "fp64"):
@@ -295,7 +296,7 @@ class Preconditioner:
             pass
 
 
-def create_preconditioner(name: str, schedule: str = "dataflow") -> Preconditioner:
+def create_preconditioner(name: str, schedule: str = "tasks") -> Preconditioner:
     return Preconditioner(name, schedule)
 
 
@@ -348,6 +349,28 @@ class FGMRES:
         self.hist = hist[:res.nhist].copy()
         A.ctx.check(st, "fgmres%solve")
         return x
+
+
+    def solve_batched(self, A: ChidgMatrix, x: ChidgVector, b: ChidgVector, M: Preconditioner, sys_elem,
+                      hist_cap: int = 1024):
+        """Independent systems packed block-diagonally in A (system s owns elements
+        sys_elem[s]:sys_elem[s+1]); returns one result dict per system."""
+        if M.h is None or M.A is not A:
+            M.init(A)
+        se = np.ascontiguousarray(sys_elem, dtype=np.int32)
+        ns = se.size - 1
+        res = (_lib.FgmresResult * ns)()
+        hist = np.zeros(ns * hist_cap)
+        st = A.ctx.L.chidg_gpu_fgmres_solve_batched(A.h, M.h, ns, se.ctypes.data_as(_lib.I32P), b.h, x.h,
+                                                    C.byref(self._o), res, hist.ctypes.data_as(_lib.DP), hist_cap)
+        A.ctx.check(st, "fgmres%solve (batched)")
+        out = []
+        for s in range(ns):
+            r = res[s]
+            out.append({"niter": r.niter, "nrestart": r.nrestart, "residual_norm": r.residual_norm,
+                        "res_estimate": r.res_estimate, "r0norm_initial": r.r0norm_initial, "seconds": r.seconds,
+                        "hist": hist[s * hist_cap:s * hist_cap + r.nhist].copy()})
+        return out
 
 
 def create_linear_solver(name: str, **options) -> FGMRES:

@@ -188,6 +188,8 @@ extern "C" int chidg_gpu_ctx_destroy(chidg_gpu_ctx* ctx) {
     for (cudaEvent_t e : ctx->prof_pool) cudaEventDestroy(e);
     release(ctx->partial);
     release(ctx->partial2);
+    for (Workspace* w : {&ctx->ws64, &ctx->ws32})
+        for (Buffer* b : {&w->V, &w->Z, &w->x0, &w->zr, &w->dz, &w->tmp, &w->rowsq}) release(*b);
     if (ctx->d_status) cudaFree(ctx->d_status);
     if (ctx->d_scal) cudaFree(ctx->d_scal);
     if (ctx->h_scal) cudaFreeHost(ctx->h_scal);
@@ -832,6 +834,11 @@ static int build_rasilu0(const chidg_gpu_matrix* A, IluProgram& P, std::string& 
     return CHIDG_GPU_OK;
 }
 
+// Register-tile class of the diagonal-block inverse for block size b.
+static int inv_class(int b) {
+    return b <= 32 ? 0 : b <= 64 ? 1 : b <= 96 ? 2 : b <= 128 ? 3 : b <= 144 ? 4 : b <= 160 ? 5 : 6;
+}
+
 // Levels, LD slots, GEMM tasks, device upload.
 static int finalize_program(chidg_gpu_ctx* ctx, const chidg_gpu_matrix* A, IluProgram& P) {
     const int np = (int)P.prow_b.size();
@@ -867,6 +874,47 @@ static int finalize_program(chidg_gpu_ctx* ctx, const chidg_gpu_matrix* A, IluPr
     };
     bucket(lf, P.fwd_rows, P.fwd_ptr);
     bucket(lb, P.bwd_rows, P.bwd_ptr);
+    // task-split sweeps: one task per entry, combine-only tasks for rows
+    // without entries; hand-out order by the level of the parent row
+    {
+        auto build_tasks = [&](bool fwd, std::vector<int32_t>& trow, std::vector<int32_t>& tent,
+                               std::vector<int64_t>& poff, int64_t& psize) {
+            const std::vector<int32_t>& order = fwd ? P.fwd_rows : P.bwd_rows;
+            const std::vector<int>& lev = fwd ? lf : lb;
+            std::vector<std::pair<int, std::pair<int32_t, int32_t>>> keyed;
+            int base = 0;
+            std::vector<int> first(np, 0);
+            for (int pr = 0; pr < np; ++pr) { first[pr] = base; base += (int)(fwd ? P.lo[pr].size() : P.up[pr].size()); }
+            poff.assign(base, 0);
+            psize = 0;
+            for (int pr = 0; pr < np; ++pr) {
+                const auto& ents = fwd ? P.lo[pr] : P.up[pr];
+                for (size_t e = 0; e < ents.size(); ++e) { poff[first[pr] + e] = psize; psize += P.prow_b[pr]; }
+            }
+            for (int32_t pr : order) {
+                const auto& ents = fwd ? P.lo[pr] : P.up[pr];
+                if (ents.empty()) keyed.push_back({-1, {pr, -1}});
+                for (size_t e = 0; e < ents.size(); ++e) keyed.push_back({lev[ents[e].parent], {pr, first[pr] + (int32_t)e}});
+            }
+            std::stable_sort(keyed.begin(), keyed.end(), [](const auto& a, const auto& c) { return a.first < c.first; });
+            trow.clear();
+            tent.clear();
+            for (auto& k : keyed) { trow.push_back(k.second.first); tent.push_back(k.second.second); }
+        };
+        std::vector<int32_t> tr, te;
+        std::vector<int64_t> po;
+        int st0;
+        build_tasks(true, tr, te, po, P.part_f);
+        P.ntask_f = (int)tr.size();
+        if ((st0 = upload_array(ctx, P.d_tf_row, tr)) || (st0 = upload_array(ctx, P.d_tf_ent, te)) ||
+            (st0 = upload_array(ctx, P.d_poff_f, po)))
+            return st0;
+        build_tasks(false, tr, te, po, P.part_b);
+        P.ntask_b = (int)tr.size();
+        if ((st0 = upload_array(ctx, P.d_tb_row, tr)) || (st0 = upload_array(ctx, P.d_tb_ent, te)) ||
+            (st0 = upload_array(ctx, P.d_poff_b, po)))
+            return st0;
+    }
     // LD slots: per programme row [inv(D)][L_1][L_2]...
     P.dinv_off.assign(np, 0);
     int64_t ld = 0;
@@ -898,34 +946,62 @@ static int finalize_program(chidg_gpu_ctx* ctx, const chidg_gpu_matrix* A, IluPr
         P.max_up_cols = std::max(P.max_up_cols, c);
         P.max_b = std::max(P.max_b, P.prow_b[pr]);
     }
-    // factorisation tasks per forward level
+    // factorisation schedule per forward level.  Rows of a level are ordered
+    // by block-size class so that each inverse launch uses the register tile
+    // that fits; GEMM tasks that fit one tensor-core CTA (<= 136 x 136) come
+    // first in each level.
     std::vector<GemmTask> ltasks, stasks;
     std::vector<GemmPair> lpairs, spairs;
     P.ltask_ptr.assign(P.fwd_ptr.size(), 0);
     P.stask_ptr.assign(P.fwd_ptr.size(), 0);
+    P.ltask_dmma.assign(P.fwd_ptr.size(), 0);
+    P.stask_dmma.assign(P.fwd_ptr.size(), 0);
+    P.inv_seg.clear();
+    P.inv_seg_ptr.assign(P.fwd_ptr.size(), 0);
     const int nlev = (int)P.fwd_ptr.size() - 1;
     for (int l = 0; l < nlev; ++l) {
-        for (int i = P.fwd_ptr[l]; i < P.fwd_ptr[l + 1]; ++i) {
-            const int pr = P.fwd_rows[i];
-            const int b = P.prow_b[pr];
-            for (auto& en : P.lo[pr]) {
-                // L = A_lower * inv(D_parent)      (precon_ILU0.f90:231)
+        std::stable_sort(P.fwd_rows.begin() + P.fwd_ptr[l], P.fwd_rows.begin() + P.fwd_ptr[l + 1],
+                         [&](int32_t a, int32_t b2) { return inv_class(P.prow_b[a]) < inv_class(P.prow_b[b2]); });
+        for (int i = P.fwd_ptr[l]; i < P.fwd_ptr[l + 1];) {
+            const int cls = inv_class(P.prow_b[P.fwd_rows[i]]);
+            int j = i;
+            while (j < P.fwd_ptr[l + 1] && inv_class(P.prow_b[P.fwd_rows[j]]) == cls) ++j;
+            P.inv_seg.push_back({i, j - i, cls});
+            i = j;
+        }
+        P.inv_seg_ptr[l + 1] = (int)P.inv_seg.size();
+        for (int pass = 0; pass < 2; ++pass) {      // pass 0: tensor-core sized, pass 1: the rest
+            for (int i = P.fwd_ptr[l]; i < P.fwd_ptr[l + 1]; ++i) {
+                const int pr = P.fwd_rows[i];
+                const int b = P.prow_b[pr];
+                for (auto& en : P.lo[pr]) {
+                    // L = A_lower * inv(D_parent)      (precon_ILU0.f90:231)
+                    const bool small = b <= DM_MAX && en.nc <= DM_MAX;
+                    if (small != (pass == 0)) continue;
+                    GemmTask t{};
+                    t.c_off = en.l_off; t.cinit_off = -1; t.m = b; t.n = en.nc;
+                    t.q_begin = (int32_t)lpairs.size();
+                    lpairs.push_back(GemmPair{en.a_off, P.dinv_off[en.parent], en.nc, 0});
+                    t.q_end = (int32_t)lpairs.size();
+                    t.elem = P.prow_elem[pr];
+                    ltasks.push_back(t);
+                }
+                // D = A_diag - sum L * A(parent, itranspose)   (:238-239)
+                bool small = b <= DM_MAX;
+                for (auto& en : P.lo[pr]) small = small && en.nc <= DM_MAX;
+                if (small != (pass == 0)) continue;
                 GemmTask t{};
-                t.c_off = en.l_off; t.cinit_off = -1; t.m = b; t.n = en.nc;
-                t.q_begin = (int32_t)lpairs.size();
-                lpairs.push_back(GemmPair{en.a_off, P.dinv_off[en.parent], en.nc, 0});
-                t.q_end = (int32_t)lpairs.size();
+                t.c_off = P.dinv_off[pr]; t.cinit_off = P.diagA_off[pr]; t.m = b; t.n = b;
+                t.q_begin = (int32_t)spairs.size();
+                for (auto& en : P.lo[pr]) spairs.push_back(GemmPair{en.l_off, en.t_off, en.nc, 0});
+                t.q_end = (int32_t)spairs.size();
                 t.elem = P.prow_elem[pr];
-                ltasks.push_back(t);
+                stasks.push_back(t);
             }
-            // D = A_diag - sum L * A(parent, itranspose)   (:238-239)
-            GemmTask t{};
-            t.c_off = P.dinv_off[pr]; t.cinit_off = P.diagA_off[pr]; t.m = b; t.n = b;
-            t.q_begin = (int32_t)spairs.size();
-            for (auto& en : P.lo[pr]) spairs.push_back(GemmPair{en.l_off, en.t_off, en.nc, 0});
-            t.q_end = (int32_t)spairs.size();
-            t.elem = P.prow_elem[pr];
-            stasks.push_back(t);
+            if (pass == 0) {
+                P.ltask_dmma[l + 1] = (int)ltasks.size() - P.ltask_ptr[l];
+                P.stask_dmma[l + 1] = (int)stasks.size() - P.stask_ptr[l];
+            }
         }
         P.ltask_ptr[l + 1] = (int)ltasks.size();
         P.stask_ptr[l + 1] = (int)stasks.size();
@@ -962,7 +1038,8 @@ static int finalize_program(chidg_gpu_ctx* ctx, const chidg_gpu_matrix* A, IluPr
 void chidg::release_program(IluProgram& P) {
     for (Buffer* b : {&P.d_prow_b, &P.d_prow_elem, &P.d_v_off, &P.d_z_off, &P.d_dinv_off, &P.d_lo_ptr, &P.d_lo_L,
                       &P.d_lo_par, &P.d_lo_nc, &P.d_up_ptr, &P.d_up_U, &P.d_up_par, &P.d_up_nc, &P.d_fwd_rows,
-                      &P.d_bwd_rows, &P.d_ltasks, &P.d_lpairs, &P.d_stasks, &P.d_spairs})
+                      &P.d_bwd_rows, &P.d_ltasks, &P.d_lpairs, &P.d_stasks, &P.d_spairs, &P.d_tf_row, &P.d_tf_ent,
+                      &P.d_tb_row, &P.d_tb_ent, &P.d_poff_f, &P.d_poff_b})
         release(*b);
 }
 
@@ -983,7 +1060,7 @@ extern "C" int chidg_gpu_precon_create(chidg_gpu_matrix* A, int32_t kind, chidg_
         if (st) { delete M; return fail(ctx, st, err); }
         st = finalize_program(ctx, A, M->P);
         if (st) { release_program(M->P); delete M; return st; }
-        const size_t sync_bytes = sizeof(unsigned) * (2 + (size_t)M->P.nprow);
+        const size_t sync_bytes = sizeof(unsigned) * (2 + 3 * (size_t)M->P.nprow);
         if ((st = ensure(ctx, M->sync, sync_bytes))) { release_program(M->P); delete M; return st; }
         cudaMemsetAsync(M->sync.ptr, 0, sync_bytes, ctx->stream);
     }
@@ -996,7 +1073,7 @@ extern "C" int chidg_gpu_precon_destroy(chidg_gpu_precon* M) {
     cudaSetDevice(M->ctx->device);
     cudaStreamSynchronize(M->ctx->stream);
     release_program(M->P);
-    for (Buffer* b : {&M->LD, &M->LD32, &M->LD16, &M->zx, &M->zx32, &M->piv_scratch, &M->sync}) release(*b);
+    for (Buffer* b : {&M->LD, &M->LD32, &M->LD16, &M->zx, &M->zx32, &M->piv_scratch, &M->sync, &M->part64, &M->part32}) release(*b);
     delete M;
     return CHIDG_GPU_OK;
 }
@@ -1006,29 +1083,31 @@ extern "C" int chidg_gpu_precon_stamp(chidg_gpu_precon* M, int64_t* s) {
     return CHIDG_GPU_OK;
 }
 
-static int launch_inverse(chidg_gpu_precon* M, int row_begin, int count) {
+static int launch_inverse(chidg_gpu_precon* M, int row_begin, int count, int cls) {
     chidg_gpu_ctx* ctx = M->ctx;
     IluProgram& P = M->P;
     double* LD = (double*)M->LD.ptr;
-    const int bmax = P.max_b;
 #define CHIDG_INV2(CL, RW)                                                                                       \
-    k_block_inverse2<CL, RW><<<count, 512, 0, ctx->stream>>>(LD, (const int64_t*)P.d_dinv_off.ptr,                  \
+    k_block_inverse3<CL, RW><<<count, 512, 0, ctx->stream>>>(LD, (const int64_t*)P.d_dinv_off.ptr,                  \
                                                              (const int32_t*)P.d_prow_b.ptr,                        \
                                                              (const int32_t*)P.d_prow_elem.ptr,                     \
                                                              (const int32_t*)P.d_fwd_rows.ptr, row_begin, ctx->d_status)
-    if (bmax <= 32) CHIDG_INV2(1, 2);
-    else if (bmax <= 64) CHIDG_INV2(2, 4);
-    else if (bmax <= 96) CHIDG_INV2(3, 6);
-    else if (bmax <= 128) CHIDG_INV2(4, 8);
-    else if (bmax <= 144) CHIDG_INV2(5, 9);
-    else if (bmax <= 160) CHIDG_INV2(5, 10);
-    else {
-        int st = ensure(ctx, M->piv_scratch, sizeof(int) * 1024 * (size_t)std::max(count, 1));
-        if (st) return st;
-        k_block_inverse_global<<<count, 512, 0, ctx->stream>>>(LD, (const int64_t*)P.d_dinv_off.ptr, (const int32_t*)P.d_prow_b.ptr,
-                                                             (const int32_t*)P.d_prow_elem.ptr, (const int32_t*)P.d_fwd_rows.ptr, row_begin,
-                                                             ctx->d_status, (int*)M->piv_scratch.ptr);
+    switch (cls) {
+        case 0: CHIDG_INV2(1, 2); break;
+        case 1: CHIDG_INV2(2, 4); break;
+        case 2: CHIDG_INV2(3, 6); break;
+        case 3: CHIDG_INV2(4, 8); break;
+        case 4: CHIDG_INV2(5, 9); break;
+        case 5: CHIDG_INV2(5, 10); break;
+        default: {
+            int st = ensure(ctx, M->piv_scratch, sizeof(int) * 1024 * (size_t)std::max(count, 1));
+            if (st) return st;
+            k_block_inverse_global<<<count, 512, 0, ctx->stream>>>(LD, (const int64_t*)P.d_dinv_off.ptr, (const int32_t*)P.d_prow_b.ptr,
+                                                                 (const int32_t*)P.d_prow_elem.ptr, (const int32_t*)P.d_fwd_rows.ptr, row_begin,
+                                                                 ctx->d_status, (int*)M->piv_scratch.ptr);
+        }
     }
+#undef CHIDG_INV2
     return check_launch(ctx, "k_block_inverse");
 }
 
@@ -1046,40 +1125,48 @@ extern "C" int chidg_gpu_precon_update(chidg_gpu_precon* M, chidg_gpu_matrix* A,
     if (st) return st;
     int big = INT_MAX;
     cudaMemcpyAsync(ctx->d_status, &big, sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
+    // fresh task counters for the task-split sweeps (a sweep cut short by an
+    // error would otherwise leave them out of step)
+    if (M->sync.ptr)
+        cudaMemsetAsync((unsigned*)M->sync.ptr + 2 + P.nprow, 0, sizeof(unsigned) * 2 * (size_t)P.nprow, ctx->stream);
     const int nlev = (int)P.fwd_ptr.size() - 1;
     const int tiles_1d = (P.max_b + GT_M - 1) / GT_M;
-    // one CTA per output block on the FP64 tensor cores when blocks fit 136 x 136
-    const bool use_dmma = P.max_b <= DM_MAX;
-    if (use_dmma)
-        cudaFuncSetAttribute(k_task_gemm_dmma<double, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DM_SMEM);
+    // one CTA per output block on the FP64 tensor cores for blocks up to 136 x 136
+    cudaFuncSetAttribute(k_task_gemm_dmma<double, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DM_SMEM);
     const int ph = prof_begin(ctx, kProfFactor);
     for (int l = 0; l < nlev; ++l) {
-        const int nl = P.ltask_ptr[l + 1] - P.ltask_ptr[l];
-        if (nl > 0 && use_dmma) {
-            k_task_gemm_dmma<double, double, double><<<nl, DM_THREADS, DM_SMEM, ctx->stream>>>(
+        const int pg = prof_begin(ctx, kProfFactorGemm);
+        const int nl = P.ltask_ptr[l + 1] - P.ltask_ptr[l], nld = P.ltask_dmma[l + 1];
+        if (nld > 0) {
+            k_task_gemm_dmma<double, double, double><<<nld, DM_THREADS, DM_SMEM, ctx->stream>>>(
                 (const GemmTask*)P.d_ltasks.ptr + P.ltask_ptr[l], (const GemmPair*)P.d_lpairs.ptr,
                 (const double*)A->val.ptr, (const double*)M->LD.ptr, nullptr, (double*)M->LD.ptr, 1.0);
             if ((st = check_launch(ctx, "k_task_gemm_dmma L"))) return st;
-        } else if (nl > 0) {
-            k_task_gemm<double, double, double><<<nl * tiles_1d * tiles_1d, 256, 0, ctx->stream>>>(
-                (const GemmTask*)P.d_ltasks.ptr + P.ltask_ptr[l], (const GemmPair*)P.d_lpairs.ptr, tiles_1d, tiles_1d,
+        }
+        if (nl > nld) {
+            k_task_gemm<double, double, double><<<(nl - nld) * tiles_1d * tiles_1d, 256, 0, ctx->stream>>>(
+                (const GemmTask*)P.d_ltasks.ptr + P.ltask_ptr[l] + nld, (const GemmPair*)P.d_lpairs.ptr, tiles_1d, tiles_1d,
                 (const double*)A->val.ptr, (const double*)M->LD.ptr, nullptr, (double*)M->LD.ptr, 1.0);
             if ((st = check_launch(ctx, "k_task_gemm L"))) return st;
         }
-        const int ns = P.stask_ptr[l + 1] - P.stask_ptr[l];
-        if (ns > 0 && use_dmma) {
-            k_task_gemm_dmma<double, double, double><<<ns, DM_THREADS, DM_SMEM, ctx->stream>>>(
+        const int ns = P.stask_ptr[l + 1] - P.stask_ptr[l], nsd = P.stask_dmma[l + 1];
+        if (nsd > 0) {
+            k_task_gemm_dmma<double, double, double><<<nsd, DM_THREADS, DM_SMEM, ctx->stream>>>(
                 (const GemmTask*)P.d_stasks.ptr + P.stask_ptr[l], (const GemmPair*)P.d_spairs.ptr,
                 (const double*)M->LD.ptr, (const double*)A->val.ptr, (const double*)A->val.ptr, (double*)M->LD.ptr, -1.0);
             if ((st = check_launch(ctx, "k_task_gemm_dmma S"))) return st;
-        } else if (ns > 0) {
-            k_task_gemm<double, double, double><<<ns * tiles_1d * tiles_1d, 256, 0, ctx->stream>>>(
-                (const GemmTask*)P.d_stasks.ptr + P.stask_ptr[l], (const GemmPair*)P.d_spairs.ptr, tiles_1d, tiles_1d,
+        }
+        if (ns > nsd) {
+            k_task_gemm<double, double, double><<<(ns - nsd) * tiles_1d * tiles_1d, 256, 0, ctx->stream>>>(
+                (const GemmTask*)P.d_stasks.ptr + P.stask_ptr[l] + nsd, (const GemmPair*)P.d_spairs.ptr, tiles_1d, tiles_1d,
                 (const double*)M->LD.ptr, (const double*)A->val.ptr, (const double*)A->val.ptr, (double*)M->LD.ptr, -1.0);
             if ((st = check_launch(ctx, "k_task_gemm S"))) return st;
         }
-        const int nr = P.fwd_ptr[l + 1] - P.fwd_ptr[l];
-        if ((st = launch_inverse(M, P.fwd_ptr[l], nr))) return st;
+        prof_end(ctx, pg);
+        const int pi = prof_begin(ctx, kProfFactorInv);
+        for (int q = P.inv_seg_ptr[l]; q < P.inv_seg_ptr[l + 1]; ++q)
+            if ((st = launch_inverse(M, P.inv_seg[q][0], P.inv_seg[q][1], P.inv_seg[q][2]))) return st;
+        prof_end(ctx, pi);
     }
     prof_end(ctx, ph);
     cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
@@ -1152,8 +1239,55 @@ static int dataflow_sweeps(chidg_gpu_precon* M, const TL* LD, const TU* U, const
     return CHIDG_GPU_OK;
 }
 
+// Both sweeps as two task-split launches (CHIDG_SCHED_TASKS).
+template <typename TL, typename TU, typename TV>
+static int task_sweeps(chidg_gpu_precon* M, const TL* LD, const TU* U, const TV* v, TV* zx, int variant) {
+    chidg_gpu_ctx* ctx = M->ctx;
+    IluProgram& P = M->P;
+    using ACC = typename AccOf<TV>::type;
+    const int threads = P.sweep_threads;
+    const size_t smem = sizeof(ACC) * 3 * 1024 + 512;
+    auto kf = k_ilu_tasks<TL, TU, TV, ACC, true>;
+    auto kb = k_ilu_tasks<TL, TU, TV, ACC, false>;
+    if (M->tk_grid[variant] == 0) {
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kb, threads, smem) != cudaSuccess || per_sm < 1) {
+            cudaGetLastError();
+            per_sm = 1;
+        }
+        M->tk_grid[variant] = std::max(1, per_sm * ctx->nsm);
+    }
+    Buffer& pb = (sizeof(ACC) == 8) ? M->part64 : M->part32;
+    int st = ensure(ctx, pb, sizeof(ACC) * (size_t)std::max<int64_t>(1, std::max(P.part_f, P.part_b)));
+    if (st) return st;
+    unsigned* sync = (unsigned*)M->sync.ptr;
+    unsigned* flags = sync + 2;
+    SweepSync S{sync, flags, 0u, (int*)(ctx->d_scal + kSlotStatus), kSpinLimit};
+    cudaError_t e = cudaMemsetAsync(sync, 0, 2 * sizeof(unsigned), ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "sweep counters");
+    int ph = prof_begin(ctx, sizeof(TV) == 8 ? kProfIluForward : kProfIlu32);
+    S.epoch = ++M->epoch;
+    S.counter = sync;
+    SweepTasks Tf{(const int32_t*)P.d_tf_row.ptr, (const int32_t*)P.d_tf_ent.ptr, (const int64_t*)P.d_poff_f.ptr,
+                  flags + P.nprow};
+    kf<<<std::min(M->tk_grid[variant], P.ntask_f), threads, smem, ctx->stream>>>(P.rows, LD, U, Tf, P.ntask_f, v, zx, (ACC*)pb.ptr, S);
+    if ((st = check_launch(ctx, "k_ilu_tasks forward"))) return st;
+    if (sizeof(TV) == 8) {
+        prof_end(ctx, ph);
+        ph = prof_begin(ctx, kProfIluBackward);
+    }
+    S.epoch = ++M->epoch;
+    S.counter = sync + 1;
+    SweepTasks Tb{(const int32_t*)P.d_tb_row.ptr, (const int32_t*)P.d_tb_ent.ptr, (const int64_t*)P.d_poff_b.ptr,
+                  flags + 2 * P.nprow};
+    kb<<<std::min(M->tk_grid[variant], P.ntask_b), threads, smem, ctx->stream>>>(P.rows, LD, U, Tb, P.ntask_b, v, zx, (ACC*)pb.ptr, S);
+    if ((st = check_launch(ctx, "k_ilu_tasks backward"))) return st;
+    prof_end(ctx, ph);
+    return CHIDG_GPU_OK;
+}
+
 extern "C" int chidg_gpu_precon_set_schedule(chidg_gpu_precon* M, int32_t schedule) {
-    if (!M || (schedule != CHIDG_SCHED_LEVELS && schedule != CHIDG_SCHED_DATAFLOW)) return CHIDG_GPU_EINVAL;
+    if (!M || schedule < CHIDG_SCHED_LEVELS || schedule > CHIDG_SCHED_TASKS) return CHIDG_GPU_EINVAL;
     M->schedule = schedule;
     return CHIDG_GPU_OK;
 }
@@ -1182,13 +1316,17 @@ int chidg::precon_apply_impl(chidg_gpu_precon* M, const TV* v, TV* z, int precis
     const size_t smem_b = sizeof(ACC) * ((size_t)P.max_up_cols + P.max_b + threads) + 512;
     const int nf = (int)P.fwd_ptr.size() - 1, nb = (int)P.bwd_ptr.size() - 1;
     int st;
-    if (M->schedule == CHIDG_SCHED_DATAFLOW) {
+    if (M->schedule == CHIDG_SCHED_DATAFLOW || M->schedule == CHIDG_SCHED_TASKS) {
+        const bool tk = M->schedule == CHIDG_SCHED_TASKS;
         if (precision == CHIDG_GPU_MIXED_BF16 && sizeof(TV) == 4)
-            st = dataflow_sweeps(M, (const __nv_bfloat16*)M->LD16.ptr, (const __nv_bfloat16*)A->val16.ptr, v, zx, 2);
+            st = tk ? task_sweeps(M, (const __nv_bfloat16*)M->LD16.ptr, (const __nv_bfloat16*)A->val16.ptr, v, zx, 2)
+                    : dataflow_sweeps(M, (const __nv_bfloat16*)M->LD16.ptr, (const __nv_bfloat16*)A->val16.ptr, v, zx, 2);
         else if (sizeof(TV) == 4)
-            st = dataflow_sweeps(M, (const float*)M->LD32.ptr, (const float*)A->val32.ptr, v, zx, 1);
+            st = tk ? task_sweeps(M, (const float*)M->LD32.ptr, (const float*)A->val32.ptr, v, zx, 1)
+                    : dataflow_sweeps(M, (const float*)M->LD32.ptr, (const float*)A->val32.ptr, v, zx, 1);
         else
-            st = dataflow_sweeps(M, (const double*)M->LD.ptr, (const double*)A->val.ptr, v, zx, 0);
+            st = tk ? task_sweeps(M, (const double*)M->LD.ptr, (const double*)A->val.ptr, v, zx, 0)
+                    : dataflow_sweeps(M, (const double*)M->LD.ptr, (const double*)A->val.ptr, v, zx, 0);
         if (st) return st;
         if (zx != z) {
             const cudaError_t e = cudaMemcpyAsync(z, zx, sizeof(TV) * (size_t)n, cudaMemcpyDeviceToDevice, ctx->stream);

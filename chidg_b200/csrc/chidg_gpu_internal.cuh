@@ -3,6 +3,7 @@
 #include "../../include/chidg_gpu.h"
 #include "kernels.cuh"
 
+#include <array>
 #include <cmath>
 #include <cstdint>
 #include <string>
@@ -51,7 +52,13 @@ struct IluProgram {
     std::vector<std::vector<IluEntry>> lo, up;
     std::vector<int32_t> fwd_rows, bwd_rows;
     std::vector<int> fwd_ptr, bwd_ptr;
-    std::vector<int> ltask_ptr, stask_ptr;
+    std::vector<int> ltask_ptr, stask_ptr, ltask_dmma, stask_dmma;
+    std::vector<std::array<int, 3>> inv_seg;   // per level: (row_begin, count, register-tile class)
+    // task-split sweeps: tasks in hand-out order, partial offsets per entry
+    int ntask_f = 0, ntask_b = 0;
+    int64_t part_f = 0, part_b = 0;            // scratch sizes (values)
+    Buffer d_tf_row, d_tf_ent, d_tb_row, d_tb_ent, d_poff_f, d_poff_b;
+    std::vector<int> inv_seg_ptr;
     Buffer d_prow_b, d_prow_elem, d_v_off, d_z_off, d_dinv_off, d_lo_ptr, d_lo_L, d_lo_par, d_lo_nc, d_up_ptr,
         d_up_U, d_up_par, d_up_nc, d_fwd_rows, d_bwd_rows, d_ltasks, d_lpairs, d_stasks, d_spairs;
     IluRows rows{};
@@ -62,8 +69,17 @@ struct IluProgram {
 namespace chidg {
 // kernel classes timed with CUDA events when profiling is on
 enum { kProfMatvec = 0, kProfIluForward = 1, kProfIluBackward = 2, kProfFactor = 3, kProfMatvec32 = 4, kProfIlu32 = 5,
-       kProfClasses = 6 };
+       kProfFactorGemm = 6, kProfFactorInv = 7, kProfClasses = 8 };
 struct EvPair { cudaEvent_t a, b; int cls; };
+}  // namespace chidg
+
+namespace chidg {
+// Krylov storage of one FGMRES instance; the context keeps one for the
+// top-level FP64 solver and one for the FP32 inner solver so that repeated
+// solves reuse their device memory
+struct Workspace {
+    Buffer V, Z, x0, zr, dz, tmp, rowsq;
+};
 }  // namespace chidg
 
 struct chidg_gpu_ctx {
@@ -79,6 +95,7 @@ struct chidg_gpu_ctx {
     double* d_scal = nullptr;
     double* h_scal = nullptr;
     chidg::Buffer partial, partial2;
+    chidg::Workspace ws64, ws32;
     bool profiling = false;
     std::vector<chidg::EvPair> prof_pending;
     std::vector<cudaEvent_t> prof_pool;
@@ -121,10 +138,12 @@ struct chidg_gpu_precon {
     int64_t stamp = 0;
     chidg::IluProgram P;
     chidg::Buffer LD, LD32, LD16, zx, zx32, piv_scratch;
-    int schedule = CHIDG_SCHED_DATAFLOW;   // sweep schedule
-    chidg::Buffer sync;                    // [2 counters][flags per programme row]
+    int schedule = CHIDG_SCHED_TASKS;      // sweep schedule
+    chidg::Buffer sync;                    // [2 counters][flags][forward row counts][backward row counts]
+    chidg::Buffer part64, part32;          // task-split sweep partials (FP64 / low precision)
     unsigned epoch = 0;
     int sf_grid[3] = {0, 0, 0};            // resident CTAs of the dataflow sweep per vector type
+    int tk_grid[3] = {0, 0, 0};            // resident CTAs of the task-split sweep per vector type
 };
 
 namespace chidg {

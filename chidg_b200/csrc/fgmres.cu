@@ -84,16 +84,17 @@ struct Solver {
     std::function<int(const T*, T*)> precon;        // z = M v
     std::function<int()> precon_update;              // M%update, or empty
     std::unique_ptr<Solver<T>> child;
-    Buffer V, Z, x0, zr, dz, tmp, rowsq;
+    Workspace own;
+    Workspace* ws = &own;          // Krylov storage (the context's, for top-level solvers)
 
-    ~Solver() { for (Buffer* b : {&V, &Z, &x0, &zr, &dz, &tmp, &rowsq}) release(*b); }
+    ~Solver() { for (Buffer* b : {&own.V, &own.Z, &own.x0, &own.zr, &own.dz, &own.tmp, &own.rowsq}) release(*b); }
 
     int matvec(const T* x, T* y, const T* z, double alpha, double beta, bool want_norm, int slot) {
         double* rs = nullptr;
         if (want_norm) {
-            int st = ensure(ctx, rowsq, sizeof(double) * (size_t)A->nrow);
+            int st = ensure(ctx, ws->rowsq, sizeof(double) * (size_t)A->nrow);
             if (st) return st;
-            rs = (double*)rowsq.ptr;
+            rs = (double*)ws->rowsq.ptr;
         }
         int st = launch_mv(x, y, z, alpha, beta, rs);
         if (st) return st;
@@ -144,13 +145,13 @@ struct Solver {
 
         const int m = nkrylov;
         if (m < 1 || m > kMaxKrylov) return fail(ctx, CHIDG_GPU_EINVAL, "fgmres: nkrylov outside [1, 4000]");
-        if ((st = ensure(ctx, V, sizeof(T) * (size_t)(m + 1) * n)) || (st = ensure(ctx, Z, sizeof(T) * (size_t)(m + 1) * n)) ||
-            (st = ensure(ctx, x0, sizeof(T) * (size_t)n)) || (st = ensure(ctx, tmp, sizeof(T) * (size_t)n)))
+        if ((st = ensure(ctx, ws->V, sizeof(T) * (size_t)(m + 1) * n)) || (st = ensure(ctx, ws->Z, sizeof(T) * (size_t)(m + 1) * n)) ||
+            (st = ensure(ctx, ws->x0, sizeof(T) * (size_t)n)) || (st = ensure(ctx, ws->tmp, sizeof(T) * (size_t)n)))
             return st;
-        if (inner && ((st = ensure(ctx, zr, sizeof(T) * (size_t)n)) || (st = ensure(ctx, dz, sizeof(T) * (size_t)n)))) return st;
-        T* Vb = (T*)V.ptr;
-        T* Zb = (T*)Z.ptr;
-        T* X0 = (T*)x0.ptr;
+        if (inner && ((st = ensure(ctx, ws->zr, sizeof(T) * (size_t)n)) || (st = ensure(ctx, ws->dz, sizeof(T) * (size_t)n)))) return st;
+        T* Vb = (T*)ws->V.ptr;
+        T* Zb = (T*)ws->Z.ptr;
+        T* X0 = (T*)ws->x0.ptr;
         cudaMemsetAsync(X0, 0, sizeof(T) * (size_t)n, ctx->stream);
         cudaMemsetAsync(x, 0, sizeof(T) * (size_t)n, ctx->stream);
 
@@ -182,8 +183,8 @@ struct Solver {
                 T* w = Vb + (int64_t)j * n;
                 if ((st = precon(vj, zj))) return st;
                 if (inner) {
-                    T* ZR = (T*)zr.ptr;
-                    T* DZ = (T*)dz.ptr;
+                    T* ZR = (T*)ws->zr.ptr;
+                    T* DZ = (T*)ws->dz.ptr;
                     if ((st = matvec(zj, ZR, vj, -1.0, 1.0, false, 0))) return st;   // zr = v - A z
                     if ((st = child->solve(ZR, DZ))) return st;
                     inner_iters += child->niter;
@@ -253,7 +254,7 @@ struct Solver {
             nrestart++;
         }
         if (true_residual) {   // print_report: ||b - A x|| (:512-520)
-            if ((st = matvec(x, (T*)tmp.ptr, b, -1.0, 1.0, true, kSlotTmp))) return st;
+            if ((st = matvec(x, (T*)ws->tmp.ptr, b, -1.0, 1.0, true, kSlotTmp))) return st;
             if ((st = fetch_scalars(ctx, kSlotTmp, 1, sc.data()))) return st;
             residual_norm = std::sqrt(sc[0]);
         } else {
@@ -324,6 +325,7 @@ extern "C" int chidg_gpu_fgmres_solve(chidg_gpu_matrix* A, chidg_gpu_precon* M, 
     std::vector<double> hv;
     Solver<double> S;
     S.ctx = ctx; S.A = A;
+    S.ws = &ctx->ws64;
     S.tol = o.tol; S.rtol = o.rtol; S.nmax = o.nmax; S.nkrylov = o.nkrylov; S.orth = o.orthogonalization;
     S.inner = o.inner_fgmres != 0; S.inner_tol = o.inner_tol; S.inner_rtol = o.inner_rtol;
     S.inner_nmax = o.inner_nmax; S.inner_nkrylov = o.inner_nkrylov; S.inner_orth = o.inner_orthogonalization;
@@ -340,6 +342,7 @@ extern "C" int chidg_gpu_fgmres_solve(chidg_gpu_matrix* A, chidg_gpu_precon* M, 
         S.inner = false;
         lo.reset(new Solver<float>());
         lo->ctx = ctx; lo->A = A;
+        lo->ws = &ctx->ws32;
         lo->tol = 0.0; lo->rtol = o.mixed_inner_rtol; lo->nmax = o.mixed_inner_nmax;
         lo->nkrylov = o.mixed_inner_nkrylov; lo->orth = CHIDG_ORTH_CGS; lo->inner = false;
         lo->true_residual = false;

@@ -373,7 +373,15 @@ __global__ void __launch_bounds__(256) k_task_gemm(const GemmTask* __restrict__ 
 // in the same k-major layout for both operands.
 constexpr int DM_MAX = 136, DM_KC = 32, DM_WM = 6, DM_WN = 3, DM_TI = 3, DM_TJ = 6;
 constexpr int DM_THREADS = 32 * DM_WM * DM_WN;
-constexpr size_t DM_SMEM = 2 * sizeof(double) * DM_KC * DM_MAX;
+constexpr size_t DM_SMEM = 4 * sizeof(double) * DM_KC * DM_MAX;   // two stages of (A, B) panels
+// 8-byte asynchronous global->shared copy; src_ok == false writes zeros
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool src_ok) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const int n = src_ok ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" :: "r"(s), "l"(gmem), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory"); }
 __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
                  : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
@@ -383,8 +391,8 @@ __global__ void __launch_bounds__(DM_THREADS) k_task_gemm_dmma(const GemmTask* _
                                                                const TA* Abase, const TB* Bbase,
                                                                const double* Cinit, TC* Cbase, double sgn) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double* As = reinterpret_cast<double*>(smem_raw);      // [DM_KC][DM_MAX]
-    double* Bs = As + DM_KC * DM_MAX;                        // [DM_KC][DM_MAX]
+    double* As = reinterpret_cast<double*>(smem_raw);      // 2 stages x {A [DM_KC][DM_MAX], B [DM_KC][DM_MAX]}
+    static_assert(sizeof(TA) == 8 && sizeof(TB) == 8, "FP64 operands");
     const GemmTask t = tasks[blockIdx.x];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int wm = w % DM_WM, wn = w / DM_WM;
@@ -395,45 +403,65 @@ __global__ void __launch_bounds__(DM_THREADS) k_task_gemm_dmma(const GemmTask* _
         #pragma unroll
         for (int j = 0; j < DM_TJ; ++j) { acc[i][j][0] = 0.0; acc[i][j][1] = 0.0; }
     const int tm = (t.m + 7) >> 3, tn = (t.n + 7) >> 3;
-    for (int q = t.q_begin; q < t.q_end; ++q) {
-        const GemmPair pr = pairs[q];
-        const TA* A = Abase + pr.a_off;   // m x k, column-major
-        const TB* B = Bbase + pr.b_off;   // k x n, column-major
-        for (int k0 = 0; k0 < pr.k; k0 += DM_KC) {
-            const int kc = min(DM_KC, pr.k - k0);
-            __syncthreads();
-            // A panel: As[kk][i] = A[i][k0+kk]; padded rows and columns are zero
-            for (int idx = threadIdx.x; idx < DM_KC * DM_MAX; idx += blockDim.x) {
-                const int i = idx % DM_MAX, kk = idx / DM_MAX;
-                As[idx] = (i < t.m && kk < kc) ? to_d(A[i + (int64_t)(k0 + kk) * t.m]) : 0.0;
-            }
-            // B panel: Bs[kk][j] = B[k0+kk][j] (coalesced along k in global memory)
-            for (int idx = threadIdx.x; idx < DM_KC * DM_MAX; idx += blockDim.x) {
-                const int kk = idx % DM_KC, j = idx / DM_KC;
-                Bs[kk * DM_MAX + j] = (j < t.n && kk < kc) ? to_d(B[(k0 + kk) + (int64_t)j * pr.k]) : 0.0;
-            }
-            __syncthreads();
-            for (int k4 = 0; k4 < kc; k4 += 4) {
-                double af[DM_TI], bf[DM_TJ];
-                // tiles past the 17th (rows/columns >= 136) exist only in the
-                // warp grid: never read them
+    // K is walked as one list of chunks over all pairs; chunk c+1 is copied
+    // into the other shared-memory stage (cp.async, zero-filled outside the
+    // operands) while chunk c feeds the tensor cores
+    int nchunk = 0;
+    for (int q = t.q_begin; q < t.q_end; ++q) nchunk += (pairs[q].k + DM_KC - 1) / DM_KC;
+    int lq = t.q_begin, lk0 = 0;                  // next chunk to load
+    auto issue = [&](int stage) {
+        const GemmPair pr = pairs[lq];
+        const TA* A = Abase + pr.a_off;           // m x k, column-major
+        const TB* B = Bbase + pr.b_off;           // k x n, column-major
+        const int kc = min(DM_KC, pr.k - lk0);
+        double* as = As + stage * 2 * DM_KC * DM_MAX;
+        double* bs = as + DM_KC * DM_MAX;
+        for (int idx = threadIdx.x; idx < DM_KC * DM_MAX; idx += blockDim.x) {
+            const int i = idx % DM_MAX, kk = idx / DM_MAX;
+            const bool ok = i < t.m && kk < kc;
+            cp_async8(as + idx, ok ? (const void*)(A + i + (int64_t)(lk0 + kk) * t.m) : (const void*)A, ok);
+        }
+        for (int idx = threadIdx.x; idx < DM_KC * DM_MAX; idx += blockDim.x) {
+            const int kk = idx % DM_KC, j = idx / DM_KC;
+            const bool ok = j < t.n && kk < kc;
+            cp_async8(bs + kk * DM_MAX + j, ok ? (const void*)(B + (lk0 + kk) + (int64_t)j * pr.k) : (const void*)B, ok);
+        }
+        cp_async_commit();
+        lk0 += DM_KC;
+        if (lk0 >= pr.k) { ++lq; lk0 = 0; }
+    };
+    int cq = t.q_begin, ck0 = 0;                  // chunk being computed
+    if (nchunk > 0) issue(0);
+    for (int c = 0; c < nchunk; ++c) {
+        if (c + 1 < nchunk) { issue((c + 1) & 1); cp_async_wait<1>(); }
+        else cp_async_wait<0>();
+        __syncthreads();
+        const int kc = min(DM_KC, pairs[cq].k - ck0);
+        const double* as = As + (c & 1) * 2 * DM_KC * DM_MAX;
+        const double* bs = as + DM_KC * DM_MAX;
+        for (int k4 = 0; k4 < kc; k4 += 4) {
+            double af[DM_TI], bf[DM_TJ];
+            // tiles past the 17th (rows/columns >= 136) exist only in the
+            // warp grid: never read them
+            #pragma unroll
+            for (int i = 0; i < DM_TI; ++i)
+                af[i] = (wm + DM_WM * i < tm) ? as[(k4 + tq) * DM_MAX + (wm + DM_WM * i) * 8 + g] : 0.0;
+            #pragma unroll
+            for (int j = 0; j < DM_TJ; ++j)
+                bf[j] = (wn + DM_WN * j < tn) ? bs[(k4 + tq) * DM_MAX + (wn + DM_WN * j) * 8 + g] : 0.0;
+            #pragma unroll
+            for (int i = 0; i < DM_TI; ++i) {
+                if (wm + DM_WM * i >= tm) continue;
                 #pragma unroll
-                for (int i = 0; i < DM_TI; ++i)
-                    af[i] = (wm + DM_WM * i < tm) ? As[(k4 + tq) * DM_MAX + (wm + DM_WM * i) * 8 + g] : 0.0;
-                #pragma unroll
-                for (int j = 0; j < DM_TJ; ++j)
-                    bf[j] = (wn + DM_WN * j < tn) ? Bs[(k4 + tq) * DM_MAX + (wn + DM_WN * j) * 8 + g] : 0.0;
-                #pragma unroll
-                for (int i = 0; i < DM_TI; ++i) {
-                    if (wm + DM_WM * i >= tm) continue;
-                    #pragma unroll
-                    for (int j = 0; j < DM_TJ; ++j) {
-                        if (wn + DM_WN * j >= tn) continue;
-                        dmma_8x8x4(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
-                    }
+                for (int j = 0; j < DM_TJ; ++j) {
+                    if (wn + DM_WN * j >= tn) continue;
+                    dmma_8x8x4(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
                 }
             }
         }
+        ck0 += DM_KC;
+        if (ck0 >= pairs[cq].k) { ++cq; ck0 = 0; }
+        __syncthreads();                          // stage (c & 1) is refilled two chunks later
     }
     #pragma unroll
     for (int i = 0; i < DM_TI; ++i) {
@@ -700,6 +728,135 @@ __global__ void __launch_bounds__(512) k_block_inverse2(double* __restrict__ LD,
     if (singular && threadIdx.x == 0) atomicMin(status, prow_elem[prow]);
 }
 
+// In-place inverse, third layout: the k_block_inverse2 tiles with one barrier
+// per pivot step.  Before the barrier every warp proposes the best unused row
+// of its own in column k, writes that candidate's value, reciprocal, index
+// and whole row (scaled later) into a double-buffered shared slot, and lane
+// lk writes the warp's part of column k.  After the barrier every warp picks
+// the winner with a 16-lane shuffle reduction (largest |a|, lowest row on
+// ties: the DGETRF choice) and reads the pivot row from the winner's slot, so
+// no warp has to wait for the owner of the pivot row.
+template <int CL, int RW>
+__global__ void __launch_bounds__(512) k_block_inverse3(double* __restrict__ LD, const int64_t* __restrict__ dinv_off,
+                                                       const int32_t* __restrict__ prow_b,
+                                                       const int32_t* __restrict__ prow_elem,
+                                                       const int32_t* __restrict__ rows, int row_begin,
+                                                       int* __restrict__ status) {
+    constexpr int NW = 16, NMAX = (32 * CL > NW * RW) ? 32 * CL : NW * RW;
+    __shared__ double colbuf[2][NMAX];
+    __shared__ double candrow[2][NW][32 * CL];
+    __shared__ double cand_v[2][NW];
+    __shared__ double cand_a[2][NW];
+    __shared__ int cand_i[2][NW];
+    __shared__ int pivrow[NMAX];
+    __shared__ int qinv[NMAX];
+    const int prow = rows[row_begin + blockIdx.x];
+    const int b = prow_b[prow];
+    double* D = LD + dinv_off[prow];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double a[RW][CL];
+    #pragma unroll
+    for (int ri = 0; ri < RW; ++ri)
+        #pragma unroll
+        for (int cl = 0; cl < CL; ++cl) {
+            const int i = w + NW * ri, j = lane + 32 * cl;
+            a[ri][cl] = (i < b && j < b) ? D[i + (int64_t)j * b] : 0.0;
+        }
+    unsigned used = 0;          // bit ri: row w + NW*ri already a pivot
+    bool singular = false;
+    #pragma unroll
+    for (int ck = 0; ck < CL; ++ck) {
+        for (int lk = 0; lk < 32; ++lk) {
+            const int k = 32 * ck + lk;
+            if (k >= b) break;
+            const int buf = k & 1;
+            // (a) this warp's candidate for column k
+            double best = -1.0, bestv = 0.0;
+            int bri = -1;
+            if (lane == lk) {
+                #pragma unroll
+                for (int ri = 0; ri < RW; ++ri) {
+                    const int i = w + NW * ri;
+                    if (i < b) {
+                        colbuf[buf][i] = a[ri][ck];
+                        double m = fabs(a[ri][ck]);
+                        if (!(m == m)) m = INFINITY;          // a NaN pivot propagates
+                        if (!((used >> ri) & 1u) && m > best) { best = m; bri = ri; bestv = a[ri][ck]; }
+                    }
+                }
+            }
+            best = __shfl_sync(0xffffffffu, best, lk);
+            bestv = __shfl_sync(0xffffffffu, bestv, lk);
+            bri = __shfl_sync(0xffffffffu, bri, lk);
+            if (bri >= 0) {
+                #pragma unroll
+                for (int cl = 0; cl < CL; ++cl) {
+                    double vsel = 0.0;
+                    #pragma unroll
+                    for (int ri = 0; ri < RW; ++ri) if (ri == bri) vsel = a[ri][cl];
+                    candrow[buf][w][lane + 32 * cl] = vsel;
+                }
+            }
+            if (lane == 0) {
+                cand_v[buf][w] = best;
+                cand_a[buf][w] = (bestv == 0.0) ? 1.0 : 1.0 / bestv;
+                cand_i[buf][w] = (bri >= 0) ? w + NW * bri : 0x7fffffff;
+            }
+            __syncthreads();
+            // (b) winner by shuffle reduction over the 16 candidates
+            double v = (lane < NW) ? cand_v[buf][lane] : -2.0;
+            int ii = (lane < NW) ? cand_i[buf][lane] : 0x7fffffff;
+            int src = lane;
+            #pragma unroll
+            for (int o = 8; o > 0; o >>= 1) {
+                const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, ii, o);
+                const int os = __shfl_xor_sync(0xffffffffu, src, o);
+                if (ov > v || (ov == v && oi < ii)) { v = ov; ii = oi; src = os; }
+            }
+            const int p = __shfl_sync(0xffffffffu, ii, 0);
+            const int ws = __shfl_sync(0xffffffffu, src, 0);
+            double rp = cand_a[buf][ws];
+            if (v == 0.0) singular = true;        // every candidate zero
+            if (w == (p % NW)) used |= 1u << (p / NW);
+            if (threadIdx.x == 0) pivrow[k] = p;
+            // (c) rank-1 update with the winner's row, scaled; row p becomes the
+            // scaled pivot row, column k becomes -a(i,k)/piv
+            double rv[CL];
+            #pragma unroll
+            for (int cl = 0; cl < CL; ++cl) {
+                const int j = lane + 32 * cl;
+                const double x = (cl == ck && lane == lk) ? 1.0 : candrow[buf][ws][j];
+                rv[cl] = x * rp;
+            }
+            #pragma unroll
+            for (int ri = 0; ri < RW; ++ri) {
+                const int i = w + NW * ri;
+                if (i == p) {
+                    #pragma unroll
+                    for (int cl = 0; cl < CL; ++cl) a[ri][cl] = rv[cl];
+                } else {
+                    const double f = (i < b) ? colbuf[buf][i] : 0.0;
+                    #pragma unroll
+                    for (int cl = 0; cl < CL; ++cl) a[ri][cl] = fma(-f, rv[cl], a[ri][cl]);
+                    if (lane == lk) a[ri][ck] = -f * rp;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < b; k += blockDim.x) qinv[pivrow[k]] = k;
+    __syncthreads();
+    #pragma unroll
+    for (int ri = 0; ri < RW; ++ri)
+        #pragma unroll
+        for (int cl = 0; cl < CL; ++cl) {
+            const int i = w + NW * ri, j = lane + 32 * cl;
+            if (i < b && j < b) D[qinv[i] + (int64_t)pivrow[j] * b] = a[ri][cl];
+        }
+    if (singular && threadIdx.x == 0) atomicMin(status, prow_elem[prow]);
+}
+
 // Same algorithm for blocks too large for the register tiles (b > 160):
 // one CTA, matrix kept in global memory (L2 resident), explicit row swaps.
 static __global__ void k_block_inverse_global(double* __restrict__ LD, const int64_t* __restrict__ dinv_off,
@@ -901,6 +1058,94 @@ __global__ void __launch_bounds__(1024) k_ilu_backward(IluRows R, const TL* __re
 }
 
 // ---------------------------------------------------------------------------
+// Segmented BLAS-1 for batches of independent systems packed one after the
+// other in one vector.  The vector is cut into chunks that never straddle two
+// systems; chunk c covers [cstart[c], cstart[c+1]) and belongs to csys[c].
+// All sums run in a fixed order (chunk order, then a fixed tree), so results
+// do not depend on the grid.
+// ---------------------------------------------------------------------------
+// partial[q * nchunk + c] = sum over chunk c of x * y_q
+template <typename T>
+__global__ void k_seg_mdot(const int64_t* __restrict__ cstart, int nchunk, const T* __restrict__ x,
+                           const T* __restrict__ y, int64_t ystride, int nq, double* __restrict__ partial) {
+    __shared__ double scratch[32];
+    const int c = blockIdx.x;
+    const int64_t i0 = cstart[c], i1 = cstart[c + 1];
+    for (int q = 0; q < nq; ++q) {
+        const T* yq = y + (int64_t)q * ystride;
+        double s = 0.0;
+        for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) s += to_d(x[i]) * to_d(yq[i]);
+        s = block_sum(s, scratch);
+        if (threadIdx.x == 0) partial[(int64_t)q * nchunk + c] = s;
+    }
+}
+// out[s * ostride + q] = sum over the chunks [sys_chunk[s], sys_chunk[s+1]) of partial[q * nchunk + c]
+static __global__ void k_seg_reduce(const double* __restrict__ partial, int nchunk, const int32_t* __restrict__ sys_chunk,
+                                    int nq, double* __restrict__ out, int ostride) {
+    const int s = blockIdx.x;
+    const int c0 = sys_chunk[s], c1 = sys_chunk[s + 1];
+    for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+        double acc = 0.0;
+        for (int c = c0; c < c1; ++c) acc += partial[(int64_t)q * nchunk + c];
+        out[(int64_t)s * ostride + q] = acc;
+    }
+}
+// w -= sum_q coef[sys * cstride + q] * v_q over each chunk; per-chunk sum of squares of w
+template <typename T>
+__global__ void k_seg_maxpy(const int64_t* __restrict__ cstart, const int32_t* __restrict__ csys, T* __restrict__ w,
+                            const T* __restrict__ v, int64_t vstride, int nq, const double* __restrict__ coef,
+                            int cstride, double* __restrict__ sumsq) {
+    __shared__ double scratch[32];
+    __shared__ double cs[256];
+    const int c = blockIdx.x;
+    const int64_t i0 = cstart[c], i1 = cstart[c + 1];
+    const double* cf = coef + (int64_t)csys[c] * cstride;
+    double sq = 0.0;
+    for (int q0 = 0; q0 < nq || q0 == 0; q0 += 256) {
+        const int qn = min(256, nq - q0);
+        __syncthreads();
+        for (int q = threadIdx.x; q < qn; q += blockDim.x) cs[q] = cf[q0 + q];
+        __syncthreads();
+        const bool last = (q0 + 256 >= nq);
+        for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+            double acc = to_d(w[i]);
+            for (int q = 0; q < qn; ++q) acc = acc - cs[q] * to_d(v[(int64_t)(q0 + q) * vstride + i]);
+            const T o = from_d<T>(acc);
+            w[i] = o;
+            if (last) { const double od = to_d(o); sq += od * od; }
+        }
+        if (nq <= 0) break;
+    }
+    if (sumsq != nullptr) {
+        sq = block_sum(sq, scratch);
+        if (threadIdx.x == 0) sumsq[c] = sq;
+    }
+}
+// x = x0 + sum_q coef[sys * cstride + q] * z_q   (x0 may be null)
+template <typename T>
+__global__ void k_seg_lincomb(const int64_t* __restrict__ cstart, const int32_t* __restrict__ csys, T* __restrict__ x,
+                              const T* __restrict__ x0, const T* __restrict__ z, int64_t zstride, int nq,
+                              const double* __restrict__ coef, int cstride) {
+    const int c = blockIdx.x;
+    const int64_t i0 = cstart[c], i1 = cstart[c + 1];
+    const double* cf = coef + (int64_t)csys[c] * cstride;
+    for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+        double acc = x0 ? to_d(x0[i]) : 0.0;
+        for (int q = 0; q < nq; ++q) acc = acc + cf[q] * to_d(z[(int64_t)q * zstride + i]);
+        x[i] = from_d<T>(acc);
+    }
+}
+// y = scale[sys] * x per chunk (in place allowed)
+template <typename T>
+__global__ void k_seg_scale(const int64_t* __restrict__ cstart, const int32_t* __restrict__ csys, const T* x, T* y,
+                            const double* __restrict__ scale) {
+    const int c = blockIdx.x;
+    const int64_t i0 = cstart[c], i1 = cstart[c + 1];
+    const double a = scale[csys[c]];
+    for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) y[i] = from_d<T>(a * to_d(x[i]));
+}
+
+// ---------------------------------------------------------------------------
 // ILU programme: dependency-driven sweeps (one launch per sweep).
 // CTAs take programme rows from an atomic ticket counter in a topological
 // order (level-major).  A row waits, through per-row flags stamped with the
@@ -1027,6 +1272,103 @@ __global__ void __launch_bounds__(1024) k_ilu_sweep_sf(IluRows R, const TL* __re
             }
         }
         // publish: every writer fences its stores, then one thread stamps the flag
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) st_release(S.flags + pr, S.epoch);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// ILU programme: task-split sweeps.  A task is one block product of one row,
+// partial = L_rq z_parent (forward) or U_rq z_parent (backward); the last task
+// of a row to finish adds the row's partials in entry order, completes the row
+// (z_r = v_r - sum, or z_r = inv(D_r) (z_r - sum)) and publishes it.  Rows
+// without entries are single combine tasks.  Tasks are handed out in
+// topological order of their parent rows, so a task only waits for rows whose
+// tasks were all handed out earlier: deadlock-free at any occupancy, and every
+// wait is bounded as in k_ilu_sweep_sf.
+// ---------------------------------------------------------------------------
+struct SweepTasks {
+    const int32_t* task_row;    // programme row of each task
+    const int32_t* task_ent;    // entry index (into lo_* / up_*) or -1 for a combine-only task
+    const int64_t* part_off;    // per entry: offset of its partial in the scratch vector
+    unsigned* row_count;        // per row: completed tasks, never reset (wraps by entry count)
+};
+
+template <typename TL, typename TU, typename TX, typename ACC, bool FORWARD>
+__global__ void __launch_bounds__(1024) k_ilu_tasks(IluRows R, const TL* __restrict__ LD, const TU* __restrict__ Aval,
+                                                    SweepTasks T, int ntasks, const TX* __restrict__ v,
+                                                    TX* __restrict__ zx, ACC* __restrict__ part, SweepSync S) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ACC* xs = reinterpret_cast<ACC*>(smem_raw);
+    __shared__ int s_task, s_last;
+    const int tid = threadIdx.x;
+    for (;;) {
+        if (tid == 0) {
+            const unsigned t = atomicAdd(S.counter, 1u);
+            s_task = (t < (unsigned)ntasks) ? (int)t : -1;
+        }
+        __syncthreads();
+        const int task = s_task;
+        if (task < 0) break;
+        const int pr = T.task_row[task];
+        const int q = T.task_ent[task];
+        const int b = R.prow_b[pr];
+        const int q0 = FORWARD ? R.lo_ptr[pr] : R.up_ptr[pr];
+        const int q1 = FORWARD ? R.lo_ptr[pr + 1] : R.up_ptr[pr + 1];
+        const int G = blockDim.x / b;
+        const int r = tid % b, g = tid / b;
+        ACC* red = xs + 1024;        // after the staged parent segment (<= 1024 values)
+        if (q >= 0) {
+            const int par = FORWARD ? R.lo_par[q] : R.up_par[q];
+            const int nc = FORWARD ? R.lo_nc[q] : R.up_nc[q];
+            if (tid == 0 && !wait_flag(S.flags, par, S.epoch, S.spin_limit)) atomicExch(S.status, 1);
+            __syncthreads();
+            const TX* zp = zx + R.z_off[par];
+            for (int c = tid; c < nc; c += blockDim.x) xs[c] = cvt<ACC>(ld_cg(zp + c));
+            __syncthreads();
+            ACC acc = 0;
+            if (g < G) {
+                if (FORWARD) acc = stripe_dot(LD + R.lo_L[q] + r, (int64_t)b, nc, g, G, xs, acc);
+                else acc = stripe_dot(Aval + R.up_U[q] + r, (int64_t)b, nc, g, G, xs, acc);
+                red[g * b + r] = acc;
+            }
+            __syncthreads();
+            if (tid < b) {
+                ACC s = 0;
+                for (int gg = 0; gg < G; ++gg) s += red[gg * b + tid];
+                part[T.part_off[q] + tid] = s;
+            }
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) {
+                const unsigned old = atomicAdd(T.row_count + pr, 1u);
+                s_last = ((old + 1u) % (unsigned)(q1 - q0)) == 0u;
+            }
+            __syncthreads();
+            if (!s_last) continue;
+            __threadfence();
+        }
+        // combine: sum the row's partials in entry order
+        ACC* tvec = xs + 1024 + 1024;
+        if (tid < b) {
+            ACC s = 0;
+            for (int qq = q0; qq < q1; ++qq) s += ld_cg(part + T.part_off[qq] + tid);
+            if (FORWARD) zx[R.z_off[pr] + tid] = from_d<TX>(to_d(v[R.v_off[pr] + tid]) - (double)s);
+            else tvec[tid] = cvt<ACC>(from_d<TX>(to_d(zx[R.z_off[pr] + tid]) - (double)s));
+        }
+        if (!FORWARD) {
+            __syncthreads();
+            ACC acc = 0;
+            if (g < G) acc = stripe_dot(LD + R.dinv_off[pr] + r, (int64_t)b, b, g, G, tvec, acc);
+            if (g < G) red[g * b + r] = acc;
+            __syncthreads();
+            if (tid < b) {
+                ACC s = 0;
+                for (int gg = 0; gg < G; ++gg) s += red[gg * b + tid];
+                zx[R.z_off[pr] + tid] = from_d<TX>((double)s);
+            }
+        }
         __threadfence();
         __syncthreads();
         if (tid == 0) st_release(S.flags + pr, S.epoch);

@@ -178,3 +178,26 @@ def synth_vector(n: int, seed: int = 0, out=None, nthreads=None) -> np.ndarray:
     nthreads = nthreads or max(1, len(os.sched_getaffinity(0)))
     _lib.synth().chidg_synth_vector(int(n), C.c_uint64(seed), out.ctypes.data_as(_lib.DP), int(nthreads))
     return out
+
+
+def concat_patterns(patterns):
+    """Pack independent systems block-diagonally into one pattern.
+
+    Returns (pattern, sys_elem) where system s owns elements
+    sys_elem[s]:sys_elem[s+1] of the union (the layout the batched solver
+    expects).  Element ranks (elem_proc) are kept per system."""
+    ntime = patterns[0].ntime
+    if any(p.ntime != ntime for p in patterns):
+        raise ValueError("all systems of a batch need the same number of time levels")
+    eoff = np.zeros(len(patterns) + 1, dtype=np.int64)
+    np.cumsum([p.nelem for p in patterns], out=eoff[1:])
+    cat = lambda name, shift=False: np.concatenate(
+        [getattr(p, name).astype(np.int64) + (eoff[i] if shift else 0) for i, p in enumerate(patterns)]).astype(np.int32)
+    union = BlockPattern(
+        nelem=int(eoff[-1]), ntime=ntime,
+        elem_nvars=cat("elem_nvars"), elem_nterms=cat("elem_nterms"), elem_proc=cat("elem_proc"),
+        blk_row_elem=cat("blk_row_elem", True), blk_row_time=cat("blk_row_time"),
+        blk_col_elem=cat("blk_col_elem", True), blk_col_time=cat("blk_col_time"),
+        blk_kind=cat("blk_kind"), blk_face=cat("blk_face"),
+        shape=(), extra={"systems": len(patterns)})
+    return union, eoff.astype(np.int32)

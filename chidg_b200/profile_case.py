@@ -20,8 +20,9 @@ def main():
     ap.add_argument("--p", type=int, default=2)
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--precon", default="ilu0")
-    ap.add_argument("--schedule", default="dataflow", choices=["dataflow", "levels"])
+    ap.add_argument("--schedule", default="tasks", choices=["tasks", "dataflow", "levels"])
     ap.add_argument("--time", action="store_true", help="print CUDA-event times per kernel class")
+    ap.add_argument("--solves", type=int, default=0, help="also time this many full solves per precision mode")
     args = ap.parse_args()
     pat = mesh.box_pattern(args.n, args.n, args.n, 5, mesh.nterms_of_order(args.p))
     A = api.ChidgMatrix(pat)
@@ -41,6 +42,35 @@ def main():
         for name, (ms, cnt) in A.ctx.kernel_times().items():
             if cnt:
                 print(f"  {name:14s} {cnt:4d} x {ms / cnt:9.3f} ms")
+    if args.solves:
+        solve_timings(args.n, args.p, args.solves, schedule=args.schedule)
+
+
+
+def solve_timings(n=24, p=2, reps=6, precisions=("fp64", "mixed_fp32", "mixed_bf16"), schedule="tasks"):
+    """Wall time of full solves (factorisation + FGMRES) per precision mode."""
+    import time
+    pat = mesh.box_pattern(n, n, n, 5, mesh.nterms_of_order(p))
+    A = api.ChidgMatrix(pat)
+    A.upload(mesh.synth_values(pat, seed=1))
+    b = api.ChidgVector(A, mesh.synth_vector(A.n, seed=2))
+    x = api.ChidgVector(A)
+    M = api.create_preconditioner("ilu0", schedule=schedule)
+    out = {}
+    for prec in precisions:
+        opts = dict(tol=0.0, rtol=1e-8, nkrylov=50, inner_fgmres=0, nmax=500, precision=prec)
+        if prec != "fp64":
+            opts.update(nkrylov=10, mixed_inner_nkrylov=30, mixed_inner_rtol=1e-2, mixed_inner_nmax=60)
+        s = api.create_linear_solver("fgmres", **opts)
+        times = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            s.solve(A, x, b, M)
+            A.ctx.sync()
+            times.append(time.perf_counter() - t0)
+        out[prec] = (times, s.niter, s.inner_iters)
+        print(f"  {prec:10s} iters {s.niter:3d}+{s.inner_iters:3d}  " + " ".join(f"{1e3 * t:7.1f}" for t in times) + " ms")
+    return out
 
 
 if __name__ == "__main__":

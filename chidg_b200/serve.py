@@ -1,0 +1,197 @@
+"""Continuous-batching solve server.
+
+Requests (one assembled Jacobian + right-hand side each) arrive at any time.
+A dispatcher packs the waiting requests into batches, first come first
+served, subject to a device-memory budget.  Each batch goes to a free worker
+slot.  A slot owns its own context and CUDA stream, so batches that are
+admitted while others are still on the GPU run concurrently with them.
+Inside a batch the systems are solved together by
+chidg_gpu_fgmres_solve_batched: one launch per matvec / ILU sweep /
+reduction for all of them, and an independent Arnoldi process per system.
+A system's arithmetic never depends on which other systems share its batch,
+so a request gets the same answer alone and in a mix.
+
+Latency is measured from arrival to the result being back on the host.
+"""
+from __future__ import annotations
+
+import collections
+import queue
+import threading
+import time
+from concurrent.futures import Future
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import api, mesh
+
+
+@dataclass
+class SolveRequest:
+    pattern: mesh.BlockPattern
+    values: np.ndarray
+    rhs: np.ndarray
+    tag: object = None
+    arrival: float = field(default_factory=time.perf_counter)
+
+
+@dataclass
+class SolveResult:
+    x: np.ndarray
+    niter: int
+    residual_norm: float
+    r0norm_initial: float
+    arrival: float
+    start: float
+    finish: float
+    batch_size: int
+    tag: object = None
+
+    @property
+    def latency(self) -> float:
+        return self.finish - self.arrival
+
+
+def request_bytes(pat: mesh.BlockPattern, nkrylov: int) -> int:
+    """Device bytes one request needs: A, factors (<= A), Krylov basis, vectors."""
+    _, nval = pat.value_offsets()
+    n = pat.vector_size()
+    return int(8 * nval * 2 + 8 * n * (2 * (nkrylov + 1) + 6))
+
+
+class Server:
+    """Continuous-batching server over `slots` concurrent GPU workers."""
+
+    def __init__(self, device: int = 0, slots: int = 2, mem_budget: int = 60 << 30, max_batch: int = 32,
+                 precon: str = "ilu0", **solver_options):
+        self.device = device
+        self.mem_budget = int(mem_budget)
+        self.max_batch = max_batch
+        self.precon = precon
+        self.options = dict(tol=0.0, rtol=1e-8, nkrylov=30, inner_fgmres=False, nmax=1000)
+        self.options.update(solver_options)
+        self._queue: "queue.Queue[tuple[SolveRequest, Future]]" = queue.Queue()
+        self._free = threading.Semaphore(slots)
+        self._mem_lock = threading.Condition()
+        self._mem_used = 0
+        self.peak_mem_used = 0
+        self.batches = 0
+        self._slot_ctx = queue.Queue()
+        for _ in range(slots):
+            self._slot_ctx.put(api.Context(device))
+        self._dispatcher = threading.Thread(target=self._dispatch, daemon=True)
+        self._dispatcher.start()
+
+    # -- public -------------------------------------------------------------
+    def submit(self, req: SolveRequest) -> Future:
+        fut: Future = Future()
+        self._queue.put((req, fut))
+        return fut
+
+    def close(self):
+        """Finish the queued requests, then stop the dispatcher."""
+        self._queue.put((None, None))
+        self._dispatcher.join(timeout=600)
+
+    # -- internals ----------------------------------------------------------
+    def _dispatch(self):
+        pending = collections.deque()
+        stopping = False
+
+        def drain(block):
+            nonlocal stopping
+            while not stopping:
+                try:
+                    item = self._queue.get() if (block and not pending) else self._queue.get_nowait()
+                except queue.Empty:
+                    return
+                if item[0] is None:
+                    stopping = True
+                    return
+                pending.append(item)
+                block = False
+
+        while True:
+            drain(block=True)
+            if not pending:
+                if stopping:
+                    break
+                continue
+            self._free.acquire()                       # a worker slot is free
+            drain(block=False)                         # requests that arrived meanwhile join
+            first = pending.popleft()
+            batch = [first]
+            nbytes = request_bytes(first[0].pattern, self.options["nkrylov"])
+            while pending and len(batch) < self.max_batch:
+                nxt = pending[0]
+                need = request_bytes(nxt[0].pattern, self.options["nkrylov"])
+                if nbytes + need > self.mem_budget or nxt[0].pattern.ntime != first[0].pattern.ntime:
+                    break
+                batch.append(pending.popleft())
+                nbytes += need
+            with self._mem_lock:                        # admission by device memory
+                while self._mem_used + nbytes > self.mem_budget and self._mem_used > 0:
+                    self._mem_lock.wait()
+                self._mem_used += nbytes
+                self.peak_mem_used = max(self.peak_mem_used, self._mem_used)
+                self.batches += 1
+            ctx = self._slot_ctx.get()
+            threading.Thread(target=self._run_batch, args=(ctx, batch, nbytes), daemon=True).start()
+
+    def _run_batch(self, ctx, batch, nbytes):
+        start = time.perf_counter()
+        try:
+            pats = [r.pattern for r, _ in batch]
+            union, sys_elem = mesh.concat_patterns(pats)
+            A = api.ChidgMatrix(union, ctx)
+            A.upload(np.concatenate([r.values for r, _ in batch]))
+            b = api.ChidgVector(A, np.concatenate([r.rhs for r, _ in batch]))
+            x = api.ChidgVector(A)
+            M = api.create_preconditioner(self.precon)
+            solver = api.create_linear_solver("fgmres", **self.options)
+            res = solver.solve_batched(A, x, b, M, sys_elem)
+            xh = x.download()
+            finish = time.perf_counter()
+            eo = union.elem_offsets()
+            for s, (req, fut) in enumerate(batch):
+                xs = xh[eo[sys_elem[s]]:eo[sys_elem[s + 1]]].copy()
+                fut.set_result(SolveResult(xs, res[s]["niter"], res[s]["residual_norm"], res[s]["r0norm_initial"],
+                                           req.arrival, start, finish, len(batch), req.tag))
+            M.tear_down()
+            for o in (x, b, A):
+                o.release()
+        except Exception as exc:  # surface the failure on every request of the batch
+            for _, fut in batch:
+                if not fut.done():
+                    fut.set_exception(exc)
+        finally:
+            with self._mem_lock:
+                self._mem_used -= nbytes
+                self._mem_lock.notify_all()
+            self._slot_ctx.put(ctx)
+            self._free.release()
+
+
+def poisson_arrivals(n: int, rate: float, seed: int = 0) -> np.ndarray:
+    """Arrival times (s) of n requests of a Poisson process with the given rate."""
+    rng = np.random.default_rng(seed)
+    return np.cumsum(rng.exponential(1.0 / rate, size=n))
+
+
+def run_stream(server: Server, requests, arrivals) -> dict:
+    """Submit requests at the given arrival times; return latency statistics."""
+    t0 = time.perf_counter()
+    futs = []
+    for req, ta in zip(requests, arrivals):
+        delay = t0 + ta - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        req.arrival = time.perf_counter()
+        futs.append(server.submit(req))
+    results = [f.result() for f in futs]
+    t1 = max(r.finish for r in results)
+    lat = np.array([r.latency for r in results])
+    return {"requests": len(results), "wall_s": t1 - t0, "solves_per_s": len(results) / (t1 - t0),
+            "p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+            "mean_batch": float(np.mean([r.batch_size for r in results])), "results": results}

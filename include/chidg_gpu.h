@@ -146,8 +146,9 @@ int chidg_gpu_launch_count(chidg_gpu_ctx* ctx, int64_t* count);
 /* Time kernel classes with CUDA events on the context's stream (off by
  * default; switching resets the totals).  Classes: 0 FP64 matvec, 1 ILU
  * forward sweep, 2 ILU backward sweep (FP64), 3 factorisation (whole
- * precon update), 4 FP32 matvec, 5 low-precision ILU apply.  One count is
- * one matvec launch, one full sweep, or one factorisation. */
+ * precon update), 4 FP32 matvec, 5 low-precision ILU apply, 6 and 7 the
+ * GEMM and inverse launches of one factorisation level.  One count is one
+ * matvec launch, one full sweep, one factorisation, or one level. */
 int chidg_gpu_ctx_set_profiling(chidg_gpu_ctx* ctx, int32_t on);
 int chidg_gpu_ctx_kernel_time(chidg_gpu_ctx* ctx, int32_t kernel_class, double* total_ms, int64_t* count);
 /* Page-locked host memory for the upload / download calls. */
@@ -232,10 +233,14 @@ int chidg_gpu_precon_apply(chidg_gpu_precon* M, chidg_gpu_matrix* A,
 /* Schedule of the triangular sweeps of precon%apply:
  * CHIDG_SCHED_LEVELS   one kernel launch per dependency level (wavefront);
  * CHIDG_SCHED_DATAFLOW one launch per sweep, rows taken in topological order,
- *                      each waiting (bounded) only for its own parents.
- * Both compute the same arithmetic; DATAFLOW is the default. */
+ *                      each waiting (bounded) only for its own parents;
+ * CHIDG_SCHED_TASKS    one launch per sweep, one task per block product, the
+ *                      last task of a row completes it (the default).
+ * LEVELS and DATAFLOW run identical per-row arithmetic; TASKS sums each
+ * block's product before adding the blocks (same values to rounding). */
 #define CHIDG_SCHED_LEVELS   0
 #define CHIDG_SCHED_DATAFLOW 1
+#define CHIDG_SCHED_TASKS    2
 int chidg_gpu_precon_set_schedule(chidg_gpu_precon* M, int32_t schedule);
 /* Packed factor blocks (L blocks and inverted diagonals at the positions of
  * the matrix's LOCAL blocks, zero elsewhere), as precon_ILU0_t%LD holds them. */
@@ -250,6 +255,17 @@ int chidg_gpu_fgmres_solve(chidg_gpu_matrix* A, chidg_gpu_precon* M,
                            const chidg_gpu_fgmres_opts* opts,
                            chidg_gpu_fgmres_result* result,
                            double* hist, int32_t hist_cap);
+/* Many independent solves in one: the systems are packed block-diagonally in
+ * A (system s owns elements [sys_elem[s], sys_elem[s+1]), sys_elem[0] = 0,
+ * sys_elem[nsys] = nelem, no block couples two systems).  Every system runs
+ * its own fgmres_t%solve Arnoldi process (dot products, re-orthogonalisation
+ * test, Givens rotations, convergence, restarts) while each matvec, ILU sweep
+ * and reduction is one launch for the whole batch.  results[s] and
+ * hist[s * hist_cap ...] are per system.  FP64, no inner FGMRES. */
+int chidg_gpu_fgmres_solve_batched(chidg_gpu_matrix* A, chidg_gpu_precon* M, int32_t nsys,
+                                   const int32_t* sys_elem, const chidg_gpu_vector* b,
+                                   chidg_gpu_vector* x, const chidg_gpu_fgmres_opts* opts,
+                                   chidg_gpu_fgmres_result* results, double* hist, int32_t hist_cap);
 /* Fill opts with the reference defaults (type_linear_solver.f90:23-40). */
 int chidg_gpu_fgmres_default_opts(chidg_gpu_fgmres_opts* opts);
 

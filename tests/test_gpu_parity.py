@@ -53,7 +53,7 @@ def test_dot_norm_axpy():
     assert relerr(yg.download(), y - 0.5 * x) < 1e-15
 
 
-@pytest.mark.parametrize("schedule", ["levels", "dataflow"])
+@pytest.mark.parametrize("schedule", ["levels", "dataflow", "tasks"])
 @pytest.mark.parametrize("kind", ["ilu0", "jacobi"])
 @pytest.mark.parametrize("shape,P,nt", CASES)
 def test_precon_factor_and_apply(kind, shape, P, nt, schedule):
@@ -77,7 +77,7 @@ def test_precon_factor_and_apply(kind, shape, P, nt, schedule):
     assert relerr(z, Mo.apply(v)) < 1e-11
 
 
-@pytest.mark.parametrize("schedule", ["levels", "dataflow"])
+@pytest.mark.parametrize("schedule", ["levels", "dataflow", "tasks"])
 @pytest.mark.parametrize("shape,P,sub", [((4, 4, 2), 1, (2, 2, 1)), ((4, 4, 4), 0, (2, 2, 2)), ((6, 3, 3), 1, (3, 1, 1))])
 def test_rasilu0(shape, P, sub, schedule):
     pat, vals, Ao, Ag = setup(shape, P, 1, sub=sub, seed=7)

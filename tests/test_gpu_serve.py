@@ -1,0 +1,59 @@
+"""Continuous-batching server: requests of different sizes arriving while
+others run are solved correctly, and each request's answer is the same
+alone and in a mix (the batched solver never mixes systems' arithmetic)."""
+import numpy as np
+import pytest
+
+from chidg_b200 import mesh, serve
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [((3, 3, 2), 1), ((2, 2, 2), 2), ((4, 2, 2), 1), ((2, 2, 1), 0), ((3, 2, 2), 2), ((2, 3, 2), 1), ((3, 3, 3), 1)]
+OPTS = dict(tol=0.0, rtol=1e-8, nkrylov=10, nmax=300)
+
+
+def make_requests():
+    reqs = []
+    for i, (shape, P) in enumerate(SIZES):
+        pat = mesh.box_pattern(*shape, 5, mesh.nterms_of_order(P))
+        reqs.append(serve.SolveRequest(pat, mesh.synth_values(pat, seed=40 + i),
+                                       mesh.synth_vector(pat.vector_size(), seed=80 + i), tag=i))
+    return reqs
+
+
+def test_server_results_match_oracle_and_are_mix_independent():
+    reqs = make_requests()
+    srv = serve.Server(slots=2, max_batch=3, **OPTS)
+    try:
+        stats = serve.run_stream(srv, reqs, serve.poisson_arrivals(len(reqs), rate=200.0, seed=1))
+        mixed = {r.tag: r for r in stats["results"]}
+        alone = {}
+        for req in make_requests():
+            alone[req.tag] = srv.submit(req).result()
+    finally:
+        srv.close()
+    assert stats["requests"] == len(reqs) and stats["p99_ms"] >= stats["p50_ms"] > 0
+    for i, req in enumerate(make_requests()):
+        Ao = O.OracleMatrix(req.pattern)
+        Ao.set_values(req.values)
+        xo, ro = O.fgmres(Ao, O.OraclePrecon(Ao, "ilu0"), req.rhs, O.default_opts(inner_fgmres=0, **OPTS))
+        assert mixed[i].niter == ro["niter"]
+        assert np.linalg.norm(mixed[i].x - xo) <= 1e-10 * np.linalg.norm(xo)
+        # same answer alone and in the mix
+        assert np.array_equal(mixed[i].x, alone[i].x)
+
+
+def test_server_admission_respects_memory_budget():
+    reqs = make_requests()
+    one = max(serve.request_bytes(r.pattern, OPTS["nkrylov"]) for r in reqs)
+    srv = serve.Server(slots=3, max_batch=8, mem_budget=one, **OPTS)   # room for about one request at a time
+    try:
+        futs = [srv.submit(r) for r in reqs]
+        res = [f.result(timeout=300) for f in futs]
+    finally:
+        srv.close()
+    # admitted work never exceeded the budget, except a single batch larger than it
+    assert srv.peak_mem_used <= one
+    assert srv.batches >= 2
+    assert all(r.residual_norm <= 2e-8 * r.r0norm_initial for r in res)
