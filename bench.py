@@ -144,6 +144,87 @@ def measured_peaks():
 
 
 # ---------------------------------------------------------------------------
+# batched and served solves (independent systems of uneven size and order)
+# ---------------------------------------------------------------------------
+BATCH_SYSTEMS = 48
+BATCH_OPTS = dict(tol=0.0, rtol=1e-8, nkrylov=30, inner_fgmres=0, nmax=1000, use_controller=0)
+
+
+def uneven_systems(count, seed, max_n=8):
+    """Boxes with each side uniform in {4..max_n} and P uniform in {1, 2} (40x40 or
+    135x135 blocks), seeded synthetic values and right-hand sides."""
+    from chidg_b200 import mesh
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        nx, ny, nz = (int(v) for v in rng.integers(4, max_n + 1, size=3))
+        P_ = int(rng.integers(1, 3))
+        pat = mesh.box_pattern(nx, ny, nz, NVARS, mesh.nterms_of_order(P_))
+        out.append((pat, mesh.synth_values(pat, seed=1000 + i), mesh.synth_vector(pat.vector_size(), seed=2000 + i)))
+    return out
+
+
+def run_batch_leg(ctx, schedule, reps=3):
+    from chidg_b200 import api, mesh
+    systems = uneven_systems(BATCH_SYSTEMS, seed=7)
+    union, sys_elem = mesh.concat_patterns([s[0] for s in systems])
+    A = api.ChidgMatrix(union, ctx)
+    A.upload(np.concatenate([s[1] for s in systems]))
+    b = api.ChidgVector(A, np.concatenate([s[2] for s in systems]))
+    x = api.ChidgVector(A)
+    M = api.create_preconditioner("ilu0", schedule=schedule)
+    solver = api.create_linear_solver("fgmres", **BATCH_OPTS)
+    solver.solve_batched(A, x, b, M, sys_elem)              # warm-up
+    ctx.sync()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        res = solver.solve_batched(A, x, b, M, sys_elem)
+    ctx.sync()
+    t_batch = (time.perf_counter() - t0) / reps
+    # the first 12 systems one solve at a time
+    singles = []
+    for pat, vals, rhs in systems[:12]:
+        As = api.ChidgMatrix(pat, ctx)
+        As.upload(vals)
+        bs, xs = api.ChidgVector(As, rhs), api.ChidgVector(As)
+        Ms = api.create_preconditioner("ilu0", schedule=schedule)
+        api.create_linear_solver("fgmres", **BATCH_OPTS).solve(As, xs, bs, Ms)   # warm-up
+        ctx.sync()
+        t0 = time.perf_counter()
+        api.create_linear_solver("fgmres", **BATCH_OPTS).solve(As, xs, bs, Ms)
+        ctx.sync()
+        singles.append(time.perf_counter() - t0)
+        Ms.tear_down()
+        for o in (xs, bs, As):
+            o.release()
+    M.tear_down()
+    for o in (x, b, A):
+        o.release()
+    return {"systems": BATCH_SYSTEMS,
+            "workload": "boxes 4..8 per side, P in {1,2}, FGMRES(30)+ILU0 to rtol 1e-8, FP64",
+            "solves_per_s_batched": BATCH_SYSTEMS / t_batch, "ms_per_batch": 1e3 * t_batch,
+            "solves_per_s_one_at_a_time": len(singles) / sum(singles),
+            "iterations": [r["niter"] for r in res],
+            "max_true_rel_residual": max(r["residual_norm"] / r["r0norm_initial"] for r in res)}
+
+
+def run_serve_leg(device, requests=64, rate=200.0):
+    from chidg_b200 import serve
+    systems = uneven_systems(requests, seed=11)
+    reqs = [serve.SolveRequest(p, v, r, tag=i) for i, (p, v, r) in enumerate(systems)]
+    srv = serve.Server(device=device, slots=2, max_batch=16, mem_budget=40 << 30, **BATCH_OPTS)
+    try:
+        srv.submit(serve.SolveRequest(*systems[0])).result()     # warm-up
+        st = serve.run_stream(srv, reqs, serve.poisson_arrivals(requests, rate, seed=5))
+    finally:
+        srv.close()
+    st.pop("results")
+    st.update({"arrival_rate_per_s": rate, "workload": "Poisson arrivals, boxes 4..8 per side, P in {1,2}, FP64",
+               "slots": 2, "max_batch": 16})
+    return st
+
+
+# ---------------------------------------------------------------------------
 # CPU legs (oracle)
 # ---------------------------------------------------------------------------
 def cpu_sample_solve(seed_a=SEED_A, seed_b=SEED_B, n=SAMPLE_N):
@@ -232,7 +313,7 @@ def run_gpu(args):
     A.upload(hv.numpy())
     b = api.ChidgVector(A, hb.numpy())
     x = api.ChidgVector(A)
-    M = api.create_preconditioner("ilu0")
+    M = api.create_preconditioner("ilu0", schedule=args.schedule)
     solver = api.create_linear_solver("fgmres", **SOLVER)
     L = ctx.L
 
@@ -319,7 +400,10 @@ def run_gpu(args):
                            "true_rel_residual": ms.residual_norm / ms.r0norm_initial,
                            "rel_err_vs_fp64_solution": float(np.linalg.norm(xm_h - x_h) / np.linalg.norm(x_h)),
                            "speedup_vs_fp64": (elapsed_ms / args.steps) / t, "phases": phases}
-        M = api.create_preconditioner("ilu0")   # drop low-precision factors
+        M = api.create_preconditioner("ilu0", schedule=args.schedule)   # drop low-precision factors
+
+    batch = run_batch_leg(ctx, args.schedule) if not args.no_batch else None
+    serving = run_serve_leg(local) if not args.no_serve else None
 
     if rank != 0:
         return 0
@@ -364,7 +448,7 @@ def run_gpu(args):
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload_config({"precision": "fp64", "fgmres_iterations": niters,
+        "config": workload_config({"precision": "fp64", "ilu_schedule": args.schedule, "fgmres_iterations": niters,
                                    "true_rel_residual": resid}),
         "latency_ms": {"p50": float(np.percentile(lat_sorted, 50)), "p99": float(np.percentile(lat_sorted, 99))},
         "clocks": clk,
@@ -376,6 +460,8 @@ def run_gpu(args):
                      "algorithmic_bytes_per_launch": dbytes},
         "kernels": kernels,
         "mixed": mixed,
+        "batch": batch,
+        "serving": serving,
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
@@ -390,6 +476,10 @@ def main():
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision legs")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-solve leg")
+    ap.add_argument("--schedule", default="stream", choices=["tasks", "stream", "dataflow", "levels"],
+                    help="schedule of the ILU sweeps")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

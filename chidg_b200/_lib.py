@@ -21,7 +21,7 @@ BLK_LOCAL, BLK_CHIMERA, BLK_BC, BLK_HB = 0, 1, 2, 3
 PRECON_IDENTITY, PRECON_JACOBI, PRECON_ILU0, PRECON_RASILU0 = 0, 1, 2, 3
 FP64, MIXED_FP32, MIXED_BF16 = 0, 1, 2
 ORTH_CGS, ORTH_MGS = 0, 1
-SCHED_LEVELS, SCHED_DATAFLOW, SCHED_TASKS = 0, 1, 2
+SCHED_LEVELS, SCHED_DATAFLOW, SCHED_TASKS, SCHED_STREAM = 0, 1, 2, 3
 
 I32P = C.POINTER(C.c_int32)
 I64P = C.POINTER(C.c_int64)

@@ -238,7 +238,7 @@ PRECISIONS = {"fp64": _lib.FP64, "mixed_fp32": _lib.MIXED_FP32, "mixed_bf16": _l
 class Preconditioner:
     """preconditioner_t: init / update / apply / tear_down."""
 
-    def __init__(self, kind: str, schedule: str = "tasks"):
+    def __init__(self, kind: str, schedule: str = "stream"):
         self.kind = kind.lower()
         self.schedule = schedule
         if self.kind not in PRECON_KINDS:
@@ -257,10 +257,12 @@ class Preconditioner:
 
     def set_schedule(self, schedule: str):
         """'levels' (one launch per wavefront), 'dataflow' (one launch per sweep,
-        row granularity) or 'tasks' (one launch per sweep, block granularity)."""
+        row granularity), 'tasks' (one launch per sweep, block granularity) or
+        'stream' (the tasks with blocks prefetched into shared memory)."""
         self.schedule = schedule
         if self.h is not None:
-            code = {"levels": _lib.SCHED_LEVELS, "dataflow": _lib.SCHED_DATAFLOW, "tasks": _lib.SCHED_TASKS}[schedule]
+            code = {"levels": _lib.SCHED_LEVELS, "dataflow": _lib.SCHED_DATAFLOW, "tasks": _lib.SCHED_TASKS,
+                    "stream": _lib.SCHED_STREAM}[schedule]
             self.A.ctx.check(self.A.ctx.L.chidg_gpu_precon_set_schedule(self.h, code), "set_schedule")
 
     def update(self, A: ChidgMatrix, b=None, precision: str = "fp64"):
@@ -296,7 +298,7 @@ class Preconditioner:
             pass
 
 
-def create_preconditioner(name: str, schedule: str = "tasks") -> Preconditioner:
+def create_preconditioner(name: str, schedule: str = "stream") -> Preconditioner:
     return Preconditioner(name, schedule)
 
 

@@ -8,6 +8,7 @@
 #include <chrono>
 #include <climits>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 
@@ -33,7 +34,9 @@ int chidg::ensure(chidg_gpu_ctx* ctx, Buffer& buf, size_t bytes) {
     if (buf.bytes >= bytes && buf.ptr) return CHIDG_GPU_OK;
     if (buf.ptr) { cudaFree(buf.ptr); buf.ptr = nullptr; buf.bytes = 0; }
     if (bytes == 0) return CHIDG_GPU_OK;
-    const cudaError_t e = cudaMalloc(&buf.ptr, bytes);
+    // 256 bytes of slack past the end: bulk copies rounded out to 16-byte
+    // boundaries may read up to 15 bytes beyond the last element
+    const cudaError_t e = cudaMalloc(&buf.ptr, bytes + 256);
     if (e != cudaSuccess) { cudaGetLastError(); return fail(ctx, CHIDG_GPU_ENOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed"); }
     buf.bytes = bytes;
     return CHIDG_GPU_OK;
@@ -245,19 +248,18 @@ static int upload_array(chidg_gpu_ctx* ctx, Buffer& buf, const std::vector<T>& v
 // Triangular sweeps: one row per CTA and a dependency chain through the
 // rows, so a row must stream its blocks as fast as one SM allows: use up to
 // 1024 threads (G = floor(1024 / b) column groups).
-static int sweep_dim_for(int bmax) {
-    const int G = std::max(1, 1024 / std::max(bmax, 1));
-    int t = G * bmax;
-    t = ((t + 31) / 32) * 32;
-    return std::min(std::max(t, 32), 1024);
-}
-
-static int block_dim_for(int bmax) {
-    // G = floor(512 / b) column groups of b threads, rounded up to whole warps
-    const int G = std::max(1, 512 / std::max(bmax, 1));
-    int t = G * bmax;
-    t = ((t + 31) / 32) * 32;
-    return std::min(std::max(t, 32), 1024);
+// Threads of a one-CTA-per-row launch: enough for G(b) = stripe_groups(cap, b)
+// column groups of b threads for every block size b present, in whole warps.
+static int launch_dim_for(int cap, const std::vector<int32_t>& sizes) {
+    int t = 32;
+    std::vector<char> seen(1025, 0);
+    for (int32_t b : sizes) {
+        const int bb = std::min(std::max((int)b, 1), 1024);
+        if (seen[bb]) continue;
+        seen[bb] = 1;
+        t = std::max(t, ((stripe_groups(cap, bb) * bb + 31) / 32) * 32);
+    }
+    return std::min(t, 1024);
 }
 
 extern "C" int chidg_gpu_matrix_create(chidg_gpu_ctx* ctx, const chidg_gpu_pattern* pat, chidg_gpu_matrix** out) {
@@ -356,7 +358,7 @@ extern "C" int chidg_gpu_matrix_create(chidg_gpu_ctx* ctx, const chidg_gpu_patte
     }
     if ((st = ensure(ctx, A->val, sizeof(double) * (size_t)A->nval))) { chidg_gpu_matrix_destroy(A); return st; }
     cudaMemsetAsync(A->val.ptr, 0, sizeof(double) * (size_t)A->nval, ctx->stream);
-    A->mv_threads = block_dim_for(A->max_b);
+    A->mv_threads = launch_dim_for(MV_GCAP, rb);
     A->stamp = 1;
     *out = A;
     return CHIDG_GPU_OK;
@@ -835,8 +837,11 @@ static int build_rasilu0(const chidg_gpu_matrix* A, IluProgram& P, std::string& 
 }
 
 // Register-tile class of the diagonal-block inverse for block size b.
+// inverse kernel by block size: 0..1 register-tiled Gauss-Jordan (b <= 64),
+// 2 tensor-core blocked Gauss-Jordan (b <= 136), 3..4 register-tiled
+// (b <= 160), 5 global-memory Gauss-Jordan
 static int inv_class(int b) {
-    return b <= 32 ? 0 : b <= 64 ? 1 : b <= 96 ? 2 : b <= 128 ? 3 : b <= 144 ? 4 : b <= 160 ? 5 : 6;
+    return b <= 32 ? 0 : b <= 64 ? 1 : b <= TCI_MAX ? 2 : b <= 144 ? 3 : b <= 160 ? 4 : 5;
 }
 
 // Levels, LD slots, GEMM tasks, device upload.
@@ -877,8 +882,11 @@ static int finalize_program(chidg_gpu_ctx* ctx, const chidg_gpu_matrix* A, IluPr
     // task-split sweeps: one task per entry, combine-only tasks for rows
     // without entries; hand-out order by the level of the parent row
     {
+        // with_diag: the streamed backward sweep's list, where each row also
+        // has an inv(D) task (entry -2) keyed between the U tasks it waits for
+        // (keys 2*level(parent) < 2*level(row)) and its children's U tasks
         auto build_tasks = [&](bool fwd, std::vector<int32_t>& trow, std::vector<int32_t>& tent,
-                               std::vector<int64_t>& poff, int64_t& psize) {
+                               std::vector<int64_t>& poff, int64_t& psize, bool with_diag = false) {
             const std::vector<int32_t>& order = fwd ? P.fwd_rows : P.bwd_rows;
             const std::vector<int>& lev = fwd ? lf : lb;
             std::vector<std::pair<int, std::pair<int32_t, int32_t>>> keyed;
@@ -893,8 +901,10 @@ static int finalize_program(chidg_gpu_ctx* ctx, const chidg_gpu_matrix* A, IluPr
             }
             for (int32_t pr : order) {
                 const auto& ents = fwd ? P.lo[pr] : P.up[pr];
-                if (ents.empty()) keyed.push_back({-1, {pr, -1}});
-                for (size_t e = 0; e < ents.size(); ++e) keyed.push_back({lev[ents[e].parent], {pr, first[pr] + (int32_t)e}});
+                const int sc = with_diag ? 2 : 1;
+                if (with_diag) keyed.push_back({2 * lev[pr] - 1, {pr, -2}});
+                else if (ents.empty()) keyed.push_back({-1, {pr, -1}});
+                for (size_t e = 0; e < ents.size(); ++e) keyed.push_back({sc * lev[ents[e].parent], {pr, first[pr] + (int32_t)e}});
             }
             std::stable_sort(keyed.begin(), keyed.end(), [](const auto& a, const auto& c) { return a.first < c.first; });
             trow.clear();
@@ -914,6 +924,10 @@ static int finalize_program(chidg_gpu_ctx* ctx, const chidg_gpu_matrix* A, IluPr
         if ((st0 = upload_array(ctx, P.d_tb_row, tr)) || (st0 = upload_array(ctx, P.d_tb_ent, te)) ||
             (st0 = upload_array(ctx, P.d_poff_b, po)))
             return st0;
+        int64_t psb = 0;
+        build_tasks(false, tr, te, po, psb, true);
+        P.ntask_sb = (int)tr.size();
+        if ((st0 = upload_array(ctx, P.d_sb_row, tr)) || (st0 = upload_array(ctx, P.d_sb_ent, te))) return st0;
     }
     // LD slots: per programme row [inv(D)][L_1][L_2]...
     P.dinv_off.assign(np, 0);
@@ -1030,7 +1044,7 @@ static int finalize_program(chidg_gpu_ctx* ctx, const chidg_gpu_matrix* A, IluPr
     P.rows.up_U = (const int64_t*)P.d_up_U.ptr;
     P.rows.up_par = (const int32_t*)P.d_up_par.ptr;
     P.rows.up_nc = (const int32_t*)P.d_up_nc.ptr;
-    P.sweep_threads = sweep_dim_for(P.max_b);
+    P.sweep_threads = launch_dim_for(SW_GCAP, P.prow_b);
     (void)A;
     return CHIDG_GPU_OK;
 }
@@ -1039,7 +1053,7 @@ void chidg::release_program(IluProgram& P) {
     for (Buffer* b : {&P.d_prow_b, &P.d_prow_elem, &P.d_v_off, &P.d_z_off, &P.d_dinv_off, &P.d_lo_ptr, &P.d_lo_L,
                       &P.d_lo_par, &P.d_lo_nc, &P.d_up_ptr, &P.d_up_U, &P.d_up_par, &P.d_up_nc, &P.d_fwd_rows,
                       &P.d_bwd_rows, &P.d_ltasks, &P.d_lpairs, &P.d_stasks, &P.d_spairs, &P.d_tf_row, &P.d_tf_ent,
-                      &P.d_tb_row, &P.d_tb_ent, &P.d_poff_f, &P.d_poff_b})
+                      &P.d_tb_row, &P.d_tb_ent, &P.d_poff_f, &P.d_poff_b, &P.d_sb_row, &P.d_sb_ent})
         release(*b);
 }
 
@@ -1060,7 +1074,7 @@ extern "C" int chidg_gpu_precon_create(chidg_gpu_matrix* A, int32_t kind, chidg_
         if (st) { delete M; return fail(ctx, st, err); }
         st = finalize_program(ctx, A, M->P);
         if (st) { release_program(M->P); delete M; return st; }
-        const size_t sync_bytes = sizeof(unsigned) * (2 + 3 * (size_t)M->P.nprow);
+        const size_t sync_bytes = sizeof(unsigned) * (2 + 4 * (size_t)M->P.nprow);
         if ((st = ensure(ctx, M->sync, sync_bytes))) { release_program(M->P); delete M; return st; }
         cudaMemsetAsync(M->sync.ptr, 0, sync_bytes, ctx->stream);
     }
@@ -1095,10 +1109,14 @@ static int launch_inverse(chidg_gpu_precon* M, int row_begin, int count, int cls
     switch (cls) {
         case 0: CHIDG_INV2(1, 2); break;
         case 1: CHIDG_INV2(2, 4); break;
-        case 2: CHIDG_INV2(3, 6); break;
-        case 3: CHIDG_INV2(4, 8); break;
-        case 4: CHIDG_INV2(5, 9); break;
-        case 5: CHIDG_INV2(5, 10); break;
+        case 2:
+            k_block_inverse_tc<<<count, TCI_THREADS, 0, ctx->stream>>>(LD, (const int64_t*)P.d_dinv_off.ptr,
+                                                                     (const int32_t*)P.d_prow_b.ptr,
+                                                                     (const int32_t*)P.d_prow_elem.ptr,
+                                                                     (const int32_t*)P.d_fwd_rows.ptr, row_begin, ctx->d_status);
+            break;
+        case 3: CHIDG_INV2(5, 9); break;
+        case 4: CHIDG_INV2(5, 10); break;
         default: {
             int st = ensure(ctx, M->piv_scratch, sizeof(int) * 1024 * (size_t)std::max(count, 1));
             if (st) return st;
@@ -1128,7 +1146,7 @@ extern "C" int chidg_gpu_precon_update(chidg_gpu_precon* M, chidg_gpu_matrix* A,
     // fresh task counters for the task-split sweeps (a sweep cut short by an
     // error would otherwise leave them out of step)
     if (M->sync.ptr)
-        cudaMemsetAsync((unsigned*)M->sync.ptr + 2 + P.nprow, 0, sizeof(unsigned) * 2 * (size_t)P.nprow, ctx->stream);
+        cudaMemsetAsync((unsigned*)M->sync.ptr + 2 + P.nprow, 0, sizeof(unsigned) * 3 * (size_t)P.nprow, ctx->stream);
     const int nlev = (int)P.fwd_ptr.size() - 1;
     const int tiles_1d = (P.max_b + GT_M - 1) / GT_M;
     // one CTA per output block on the FP64 tensor cores for blocks up to 136 x 136
@@ -1245,7 +1263,15 @@ static int task_sweeps(chidg_gpu_precon* M, const TL* LD, const TU* U, const TV*
     chidg_gpu_ctx* ctx = M->ctx;
     IluProgram& P = M->P;
     using ACC = typename AccOf<TV>::type;
-    const int threads = P.sweep_threads;
+    // column-group budget of one task CTA; CHIDG_TASK_THREADS (a multiple of 32
+    // up to 1024) narrows it for tuning
+    static const int tk_cap_env = [] {
+        const char* e = std::getenv("CHIDG_TASK_THREADS");
+        const int v = e ? std::atoi(e) : 0;
+        return (v >= 32 && v <= 1024 && v % 32 == 0) ? v : TK_GCAP;
+    }();
+    const int gcap = tk_cap_env;
+    const int threads = launch_dim_for(gcap, P.prow_b);
     const size_t smem = sizeof(ACC) * 3 * 1024 + 512;
     auto kf = k_ilu_tasks<TL, TU, TV, ACC, true>;
     auto kb = k_ilu_tasks<TL, TU, TV, ACC, false>;
@@ -1270,7 +1296,7 @@ static int task_sweeps(chidg_gpu_precon* M, const TL* LD, const TU* U, const TV*
     S.counter = sync;
     SweepTasks Tf{(const int32_t*)P.d_tf_row.ptr, (const int32_t*)P.d_tf_ent.ptr, (const int64_t*)P.d_poff_f.ptr,
                   flags + P.nprow};
-    kf<<<std::min(M->tk_grid[variant], P.ntask_f), threads, smem, ctx->stream>>>(P.rows, LD, U, Tf, P.ntask_f, v, zx, (ACC*)pb.ptr, S);
+    kf<<<std::min(M->tk_grid[variant], P.ntask_f), threads, smem, ctx->stream>>>(P.rows, LD, U, Tf, P.ntask_f, v, zx, (ACC*)pb.ptr, S, gcap);
     if ((st = check_launch(ctx, "k_ilu_tasks forward"))) return st;
     if (sizeof(TV) == 8) {
         prof_end(ctx, ph);
@@ -1280,14 +1306,98 @@ static int task_sweeps(chidg_gpu_precon* M, const TL* LD, const TU* U, const TV*
     S.counter = sync + 1;
     SweepTasks Tb{(const int32_t*)P.d_tb_row.ptr, (const int32_t*)P.d_tb_ent.ptr, (const int64_t*)P.d_poff_b.ptr,
                   flags + 2 * P.nprow};
-    kb<<<std::min(M->tk_grid[variant], P.ntask_b), threads, smem, ctx->stream>>>(P.rows, LD, U, Tb, P.ntask_b, v, zx, (ACC*)pb.ptr, S);
+    kb<<<std::min(M->tk_grid[variant], P.ntask_b), threads, smem, ctx->stream>>>(P.rows, LD, U, Tb, P.ntask_b, v, zx, (ACC*)pb.ptr, S, gcap);
     if ((st = check_launch(ctx, "k_ilu_tasks backward"))) return st;
     prof_end(ctx, ph);
     return CHIDG_GPU_OK;
 }
 
+// Shape of the streamed sweeps: consumer warps per CTA, ring stages and stage
+// size.  Read once from CHIDG_STREAM_SHAPE="warps,stages,kbytes" when set.
+struct StreamShape { int cw = 8, nstage = 2, stage_bytes = 48 * 1024; };
+static StreamShape stream_shape() {
+    static StreamShape sh = [] {
+        StreamShape d;
+        if (const char* e = std::getenv("CHIDG_STREAM_SHAPE")) {
+            int cw = 0, ns = 0, kb = 0;
+            if (std::sscanf(e, "%d,%d,%d", &cw, &ns, &kb) == 3 && (cw == 2 || cw == 4 || cw == 8) && ns >= 2 &&
+                ns <= SS_MAX_STAGES && kb >= 2 && kb <= 96)
+                d = StreamShape{cw, ns, kb * 1024};
+        }
+        return d;
+    }();
+    return sh;
+}
+
+template <typename TL, typename TU, typename TV, bool FWD, int CW>
+static int stream_launch(chidg_gpu_precon* M, const TL* LD, const TU* U, StreamTasks Tk, int ntask, const TV* v, TV* zx,
+                         void* part, SweepSync S, const StreamShape& sh, int variant) {
+    chidg_gpu_ctx* ctx = M->ctx;
+    using ACC = typename AccOf<TV>::type;
+    const size_t smem = stream_smem_bytes(sizeof(ACC), sh.nstage, sh.stage_bytes);
+    auto k = k_ilu_stream<TL, TU, TV, ACC, FWD, CW>;
+    int& grid = M->ss_grid[variant][FWD ? 0 : 1];
+    if (grid == 0) {
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 32 * CW + 32, smem) != cudaSuccess || per_sm < 1) {
+            cudaGetLastError();
+            per_sm = 1;
+        }
+        grid = per_sm * ctx->nsm;
+    }
+    k<<<std::max(1, std::min(grid, ntask)), 32 * CW + 32, smem, ctx->stream>>>(M->P.rows, LD, U, Tk, ntask, v, zx, (ACC*)part,
+                                                                              S, sh.nstage, sh.stage_bytes);
+    return check_launch(ctx, FWD ? "k_ilu_stream forward" : "k_ilu_stream backward");
+}
+
+// Both sweeps as two streamed launches (CHIDG_SCHED_STREAM): persistent CTAs,
+// blocks prefetched into shared memory by a producer lane.
+template <typename TL, typename TU, typename TV>
+static int stream_sweeps(chidg_gpu_precon* M, const TL* LD, const TU* U, const TV* v, TV* zx, int variant) {
+    chidg_gpu_ctx* ctx = M->ctx;
+    IluProgram& P = M->P;
+    using ACC = typename AccOf<TV>::type;
+    const StreamShape sh = stream_shape();
+    Buffer& pb = (sizeof(ACC) == 8) ? M->part64 : M->part32;
+    int st = ensure(ctx, pb, sizeof(ACC) * (size_t)std::max<int64_t>(1, std::max(P.part_f, P.part_b)));
+    if (st) return st;
+    unsigned* sync = (unsigned*)M->sync.ptr;
+    unsigned* flags = sync + 2;
+    SweepSync S{sync, flags, 0u, (int*)(ctx->d_scal + kSlotStatus), kSpinLimit};
+    cudaError_t e = cudaMemsetAsync(sync, 0, 2 * sizeof(unsigned), ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "sweep counters");
+    int ph = prof_begin(ctx, sizeof(TV) == 8 ? kProfIluForward : kProfIlu32);
+    S.epoch = ++M->epoch;
+    S.counter = sync;
+    StreamTasks Tf{(const int32_t*)P.d_tf_row.ptr, (const int32_t*)P.d_tf_ent.ptr, (const int64_t*)P.d_poff_f.ptr,
+                   flags + P.nprow, flags + 3 * P.nprow};
+    switch (sh.cw) {
+        case 2: st = stream_launch<TL, TU, TV, true, 2>(M, LD, U, Tf, P.ntask_f, v, zx, pb.ptr, S, sh, variant); break;
+        case 8: st = stream_launch<TL, TU, TV, true, 8>(M, LD, U, Tf, P.ntask_f, v, zx, pb.ptr, S, sh, variant); break;
+        default: st = stream_launch<TL, TU, TV, true, 4>(M, LD, U, Tf, P.ntask_f, v, zx, pb.ptr, S, sh, variant);
+    }
+    if (st) return st;
+    if (sizeof(TV) == 8) {
+        prof_end(ctx, ph);
+        ph = prof_begin(ctx, kProfIluBackward);
+    }
+    S.epoch = ++M->epoch;
+    S.counter = sync + 1;
+    StreamTasks Tb{(const int32_t*)P.d_sb_row.ptr, (const int32_t*)P.d_sb_ent.ptr, (const int64_t*)P.d_poff_b.ptr,
+                   flags + 2 * P.nprow, flags + 3 * P.nprow};
+    switch (sh.cw) {
+        case 2: st = stream_launch<TL, TU, TV, false, 2>(M, LD, U, Tb, P.ntask_sb, v, zx, pb.ptr, S, sh, variant); break;
+        case 8: st = stream_launch<TL, TU, TV, false, 8>(M, LD, U, Tb, P.ntask_sb, v, zx, pb.ptr, S, sh, variant); break;
+        default: st = stream_launch<TL, TU, TV, false, 4>(M, LD, U, Tb, P.ntask_sb, v, zx, pb.ptr, S, sh, variant);
+    }
+    if (st) return st;
+    prof_end(ctx, ph);
+    return CHIDG_GPU_OK;
+}
+
 extern "C" int chidg_gpu_precon_set_schedule(chidg_gpu_precon* M, int32_t schedule) {
-    if (!M || schedule < CHIDG_SCHED_LEVELS || schedule > CHIDG_SCHED_TASKS) return CHIDG_GPU_EINVAL;
+    if (!M || schedule < CHIDG_SCHED_LEVELS || schedule > CHIDG_SCHED_STREAM) return CHIDG_GPU_EINVAL;
     M->schedule = schedule;
     return CHIDG_GPU_OK;
 }
@@ -1316,8 +1426,25 @@ int chidg::precon_apply_impl(chidg_gpu_precon* M, const TV* v, TV* z, int precis
     const size_t smem_b = sizeof(ACC) * ((size_t)P.max_up_cols + P.max_b + threads) + 512;
     const int nf = (int)P.fwd_ptr.size() - 1, nb = (int)P.bwd_ptr.size() - 1;
     int st;
-    if (M->schedule == CHIDG_SCHED_DATAFLOW || M->schedule == CHIDG_SCHED_TASKS) {
-        const bool tk = M->schedule == CHIDG_SCHED_TASKS;
+    // blocks of more than 1024 rows: the streamed sweeps run as TASKS
+    const int sched = (M->schedule == CHIDG_SCHED_STREAM && P.max_b > SS_MAX_B) ? CHIDG_SCHED_TASKS : M->schedule;
+    if (sched == CHIDG_SCHED_STREAM) {
+        int st;
+        if (precision == CHIDG_GPU_MIXED_BF16 && sizeof(TV) == 4)
+            st = stream_sweeps(M, (const __nv_bfloat16*)M->LD16.ptr, (const __nv_bfloat16*)A->val16.ptr, v, zx, 2);
+        else if (sizeof(TV) == 4)
+            st = stream_sweeps(M, (const float*)M->LD32.ptr, (const float*)A->val32.ptr, v, zx, 1);
+        else
+            st = stream_sweeps(M, (const double*)M->LD.ptr, (const double*)A->val.ptr, v, zx, 0);
+        if (st) return st;
+        if (zx != z) {
+            const cudaError_t e = cudaMemcpyAsync(z, zx, sizeof(TV) * (size_t)n, cudaMemcpyDeviceToDevice, ctx->stream);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "precon output copy");
+        }
+        return CHIDG_GPU_OK;
+    }
+    if (sched == CHIDG_SCHED_DATAFLOW || sched == CHIDG_SCHED_TASKS) {
+        const bool tk = sched == CHIDG_SCHED_TASKS;
         if (precision == CHIDG_GPU_MIXED_BF16 && sizeof(TV) == 4)
             st = tk ? task_sweeps(M, (const __nv_bfloat16*)M->LD16.ptr, (const __nv_bfloat16*)A->val16.ptr, v, zx, 2)
                     : dataflow_sweeps(M, (const __nv_bfloat16*)M->LD16.ptr, (const __nv_bfloat16*)A->val16.ptr, v, zx, 2);

@@ -2,6 +2,8 @@
 #pragma once
 #include "../../include/chidg_gpu.h"
 #include "kernels.cuh"
+#include "stream_sweep.cuh"
+#include "inverse_tc.cuh"
 
 #include <array>
 #include <cmath>
@@ -58,6 +60,8 @@ struct IluProgram {
     int ntask_f = 0, ntask_b = 0;
     int64_t part_f = 0, part_b = 0;            // scratch sizes (values)
     Buffer d_tf_row, d_tf_ent, d_tb_row, d_tb_ent, d_poff_f, d_poff_b;
+    int ntask_sb = 0;                          // streamed backward sweep: U tasks + inv(D) tasks
+    Buffer d_sb_row, d_sb_ent;
     std::vector<int> inv_seg_ptr;
     Buffer d_prow_b, d_prow_elem, d_v_off, d_z_off, d_dinv_off, d_lo_ptr, d_lo_L, d_lo_par, d_lo_nc, d_up_ptr,
         d_up_U, d_up_par, d_up_nc, d_fwd_rows, d_bwd_rows, d_ltasks, d_lpairs, d_stasks, d_spairs;
@@ -138,12 +142,13 @@ struct chidg_gpu_precon {
     int64_t stamp = 0;
     chidg::IluProgram P;
     chidg::Buffer LD, LD32, LD16, zx, zx32, piv_scratch;
-    int schedule = CHIDG_SCHED_TASKS;      // sweep schedule
+    int schedule = CHIDG_SCHED_STREAM;     // sweep schedule (TASKS for blocks over 1024 rows)
     chidg::Buffer sync;                    // [2 counters][flags][forward row counts][backward row counts]
     chidg::Buffer part64, part32;          // task-split sweep partials (FP64 / low precision)
     unsigned epoch = 0;
     int sf_grid[3] = {0, 0, 0};            // resident CTAs of the dataflow sweep per vector type
     int tk_grid[3] = {0, 0, 0};            // resident CTAs of the task-split sweep per vector type
+    int ss_grid[3][2] = {{0, 0}, {0, 0}, {0, 0}};  // resident CTAs of the streamed sweeps (forward, backward)
 };
 
 namespace chidg {

@@ -18,6 +18,15 @@
 
 namespace chidg {
 
+// Column groups per row of b rows: G(b) = max(1, cap / b).  It depends on the
+// row's own block size only, never on the launch (which is sized for the
+// largest block present), so a row sums in the same order whatever it shares
+// a matrix or a batch with.
+constexpr int MV_GCAP = 512;     // matvec
+constexpr int SW_GCAP = 1024;    // triangular sweeps, one CTA per row
+constexpr int TK_GCAP = 512;     // task-split sweeps, one CTA per block product
+__host__ __device__ __forceinline__ int stripe_groups(int cap, int b) { return b >= cap ? 1 : cap / b; }
+
 // ---------------------------------------------------------------------------
 // conversions
 // ---------------------------------------------------------------------------
@@ -127,7 +136,7 @@ __global__ void __launch_bounds__(1024) k_matvec(const TA* __restrict__ val, con
     }
     const int ncols_total = off;
     __syncthreads();
-    const int G = blockDim.x / b;
+    const int G = stripe_groups(MV_GCAP, b);
     const int r = tid % b, g = tid / b;
     ACC acc = 0;
     if (g < G) {
@@ -366,14 +375,16 @@ __global__ void __launch_bounds__(256) k_task_gemm(const GemmTask* __restrict__ 
 }
 
 // FP64 tensor-core version of k_task_gemm for blocks up to 136 x 136: one CTA
-// computes a whole output block with mma.sync m8n8k4 (DMMA).  18 warps on a
-// 6 x 3 grid; warp (wm, wn) owns the 8x8 output tiles (wm + 6i, wn + 3j),
-// i < 3, j < 6, so each A fragment loaded from shared memory feeds six MMAs
-// and each B fragment three.  K is staged 32 at a time through shared memory
-// in the same k-major layout for both operands.
-constexpr int DM_MAX = 136, DM_KC = 32, DM_WM = 6, DM_WN = 3, DM_TI = 3, DM_TJ = 6;
+// computes a whole output block with mma.sync m8n8k4 (DMMA).  8 warps on a
+// 2 x 4 grid; warp (wm, wn) owns the 8x8 output tiles (wm + 2i, wn + 4j),
+// i < 9, j < 5 (45 accumulators, up to 255 registers a thread), so each A
+// fragment loaded from shared memory feeds five MMAs and each B fragment
+// nine.  K is staged 32 at a time through shared memory in the same k-major
+// layout for both operands, leading dimension 140 (= 12 mod 16 doubles: the
+// fragment loads of a half-warp hit 16 distinct bank pairs).
+constexpr int DM_MAX = 136, DM_LD = 140, DM_KC = 32, DM_WM = 2, DM_WN = 4, DM_TI = 9, DM_TJ = 5;
 constexpr int DM_THREADS = 32 * DM_WM * DM_WN;
-constexpr size_t DM_SMEM = 4 * sizeof(double) * DM_KC * DM_MAX;   // two stages of (A, B) panels
+constexpr size_t DM_SMEM = 4 * sizeof(double) * DM_KC * DM_LD;   // two stages of (A, B) panels
 // 8-byte asynchronous global->shared copy; src_ok == false writes zeros
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool src_ok) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -382,16 +393,24 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool src
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory"); }
+// D(16x8) += A(16x8) B(8x8): lane (g, t) holds A(g, t), A(g+8, t), A(g, t+4),
+// A(g+8, t+4); B(t, g), B(t+4, g); D(g, 2t), D(g, 2t+1), D(g+8, 2t), D(g+8, 2t+1)
+__device__ __forceinline__ void dmma_16x8x8(double& d0, double& d1, double& d2, double& d3, double a0, double a1,
+                                            double a2, double a3, double b0, double b1) {
+    asm volatile("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+                 : "+d"(d0), "+d"(d1), "+d"(d2), "+d"(d3)
+                 : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
+}
 __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
                  : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
 }
 template <typename TA, typename TB, typename TC>
-__global__ void __launch_bounds__(DM_THREADS) k_task_gemm_dmma(const GemmTask* __restrict__ tasks, const GemmPair* __restrict__ pairs,
+__global__ void __launch_bounds__(DM_THREADS, 1) k_task_gemm_dmma(const GemmTask* __restrict__ tasks, const GemmPair* __restrict__ pairs,
                                                                const TA* Abase, const TB* Bbase,
                                                                const double* Cinit, TC* Cbase, double sgn) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double* As = reinterpret_cast<double*>(smem_raw);      // 2 stages x {A [DM_KC][DM_MAX], B [DM_KC][DM_MAX]}
+    double* As = reinterpret_cast<double*>(smem_raw);      // 2 stages x {A [DM_KC][DM_LD], B [DM_KC][DM_LD]}
     static_assert(sizeof(TA) == 8 && sizeof(TB) == 8, "FP64 operands");
     const GemmTask t = tasks[blockIdx.x];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -414,17 +433,17 @@ __global__ void __launch_bounds__(DM_THREADS) k_task_gemm_dmma(const GemmTask* _
         const TA* A = Abase + pr.a_off;           // m x k, column-major
         const TB* B = Bbase + pr.b_off;           // k x n, column-major
         const int kc = min(DM_KC, pr.k - lk0);
-        double* as = As + stage * 2 * DM_KC * DM_MAX;
-        double* bs = as + DM_KC * DM_MAX;
+        double* as = As + stage * 2 * DM_KC * DM_LD;
+        double* bs = as + DM_KC * DM_LD;
         for (int idx = threadIdx.x; idx < DM_KC * DM_MAX; idx += blockDim.x) {
             const int i = idx % DM_MAX, kk = idx / DM_MAX;
             const bool ok = i < t.m && kk < kc;
-            cp_async8(as + idx, ok ? (const void*)(A + i + (int64_t)(lk0 + kk) * t.m) : (const void*)A, ok);
+            cp_async8(as + kk * DM_LD + i, ok ? (const void*)(A + i + (int64_t)(lk0 + kk) * t.m) : (const void*)A, ok);
         }
         for (int idx = threadIdx.x; idx < DM_KC * DM_MAX; idx += blockDim.x) {
             const int kk = idx % DM_KC, j = idx / DM_KC;
             const bool ok = j < t.n && kk < kc;
-            cp_async8(bs + kk * DM_MAX + j, ok ? (const void*)(B + (lk0 + kk) + (int64_t)j * pr.k) : (const void*)B, ok);
+            cp_async8(bs + kk * DM_LD + j, ok ? (const void*)(B + (lk0 + kk) + (int64_t)j * pr.k) : (const void*)B, ok);
         }
         cp_async_commit();
         lk0 += DM_KC;
@@ -437,18 +456,18 @@ __global__ void __launch_bounds__(DM_THREADS) k_task_gemm_dmma(const GemmTask* _
         else cp_async_wait<0>();
         __syncthreads();
         const int kc = min(DM_KC, pairs[cq].k - ck0);
-        const double* as = As + (c & 1) * 2 * DM_KC * DM_MAX;
-        const double* bs = as + DM_KC * DM_MAX;
+        const double* as = As + (c & 1) * 2 * DM_KC * DM_LD;
+        const double* bs = as + DM_KC * DM_LD;
         for (int k4 = 0; k4 < kc; k4 += 4) {
             double af[DM_TI], bf[DM_TJ];
             // tiles past the 17th (rows/columns >= 136) exist only in the
             // warp grid: never read them
             #pragma unroll
             for (int i = 0; i < DM_TI; ++i)
-                af[i] = (wm + DM_WM * i < tm) ? as[(k4 + tq) * DM_MAX + (wm + DM_WM * i) * 8 + g] : 0.0;
+                af[i] = (wm + DM_WM * i < tm) ? as[(k4 + tq) * DM_LD + (wm + DM_WM * i) * 8 + g] : 0.0;
             #pragma unroll
             for (int j = 0; j < DM_TJ; ++j)
-                bf[j] = (wn + DM_WN * j < tn) ? bs[(k4 + tq) * DM_MAX + (wn + DM_WN * j) * 8 + g] : 0.0;
+                bf[j] = (wn + DM_WN * j < tn) ? bs[(k4 + tq) * DM_LD + (wn + DM_WN * j) * 8 + g] : 0.0;
             #pragma unroll
             for (int i = 0; i < DM_TI; ++i) {
                 if (wm + DM_WM * i >= tm) continue;
@@ -976,7 +995,7 @@ __global__ void __launch_bounds__(1024) k_ilu_forward(IluRows R, const TL* __res
     }
     const int ncols_total = off;
     __syncthreads();
-    const int G = blockDim.x / b;
+    const int G = stripe_groups(SW_GCAP, b);
     const int r = tid % b, g = tid / b;
     ACC acc = 0;
     if (g < G) {
@@ -1020,7 +1039,7 @@ __global__ void __launch_bounds__(1024) k_ilu_backward(IluRows R, const TL* __re
     ACC* tvec = xs + ncols_total;          // b entries
     ACC* red = tvec + b;                   // G*b entries
     __syncthreads();
-    const int G = blockDim.x / b;
+    const int G = stripe_groups(SW_GCAP, b);
     const int r = tid % b, g = tid / b;
     ACC acc = 0;
     if (g < G) {
@@ -1222,7 +1241,7 @@ __global__ void __launch_bounds__(1024) k_ilu_sweep_sf(IluRows R, const TL* __re
         ACC* tvec = xs + ncols_total;
         ACC* red = tvec + b;
         __syncthreads();
-        const int G = blockDim.x / b;
+        const int G = stripe_groups(SW_GCAP, b);
         const int r = tid % b, g = tid / b;
         ACC acc = 0;
         if (g < G) {
@@ -1298,7 +1317,7 @@ struct SweepTasks {
 template <typename TL, typename TU, typename TX, typename ACC, bool FORWARD>
 __global__ void __launch_bounds__(1024) k_ilu_tasks(IluRows R, const TL* __restrict__ LD, const TU* __restrict__ Aval,
                                                     SweepTasks T, int ntasks, const TX* __restrict__ v,
-                                                    TX* __restrict__ zx, ACC* __restrict__ part, SweepSync S) {
+                                                    TX* __restrict__ zx, ACC* __restrict__ part, SweepSync S, int gcap) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ACC* xs = reinterpret_cast<ACC*>(smem_raw);
     __shared__ int s_task, s_last;
@@ -1316,7 +1335,7 @@ __global__ void __launch_bounds__(1024) k_ilu_tasks(IluRows R, const TL* __restr
         const int b = R.prow_b[pr];
         const int q0 = FORWARD ? R.lo_ptr[pr] : R.up_ptr[pr];
         const int q1 = FORWARD ? R.lo_ptr[pr + 1] : R.up_ptr[pr + 1];
-        const int G = blockDim.x / b;
+        const int G = stripe_groups(gcap, b);
         const int r = tid % b, g = tid / b;
         ACC* red = xs + 1024;        // after the staged parent segment (<= 1024 values)
         if (q >= 0) {

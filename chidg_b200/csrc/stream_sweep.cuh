@@ -1,0 +1,341 @@
+// ILU programme: streamed task sweeps (CHIDG_SCHED_STREAM).
+//
+// The work of one triangular sweep is the task list of the task-split sweep
+// (one block product per task, handed out in topological order of the parent
+// rows), executed by persistent CTAs (several per SM, so that several tasks
+// are in flight on each SM) with a producer/consumer split:
+//
+//   producer (one lane of the last warp)  takes a ticket, and copies the task's
+//       block column-chunk by column-chunk into a ring of shared-memory stages
+//       with cp.async.bulk (completion counted on the stage's mbarrier).  The
+//       copy does not depend on the sweep's values, so it runs ahead of the
+//       dependency waits: the block is in shared memory when the parent row is
+//       published.
+//   consumers (the other warps)  wait (bounded) for the parent row, stage its
+//       segment of z, multiply the chunks as they land, release each stage, and
+//       at the last chunk publish the block's partial product.  The last task of
+//       a row to finish completes it.
+//
+// Backward sweep: the product with inv(D_r) is a task of its own (entry -2),
+// ordered after the row's U tasks and before its children's; it waits for
+// the row's partials to be complete (the `ready` flag set by the last U task),
+// adds them to z_r in entry order and multiplies by inv(D_r) streamed through
+// the same ring, so inv(D_r) is prefetched like every other block.
+//
+// Deadlock freedom: a task waits only for tasks with smaller tickets.  Each
+// CTA consumes its tasks in ticket order, and a producer posts a task's chunks
+// as soon as stages free, so the unfinished task with the smallest ticket can
+// always proceed.  Every wait (flags, mbarriers) is bounded; on a timeout the
+// sweep records status 1 and finishes with wrong values instead of hanging.
+//
+// Bulk copies need 16-byte aligned source, destination and size: each chunk's
+// source is rounded down to 16 bytes (the element offset inside the stage is
+// carried with the chunk) and its length rounded up; device buffers carry 256
+// bytes of slack past their end, so the rounded copies stay inside them.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace chidg {
+
+constexpr int SS_MAX_B = 1024;                              // rows per block
+constexpr int SS_MAX_STAGES = 8;
+
+struct StreamMeta {
+    int task;      // ticket, -1 = end of the sweep for this CTA
+    int pr, q;     // programme row, entry (-1 combine-only, -2 backward diagonal)
+    int chunk, nchunk;
+    int col0, ncols;
+    int shift;     // element offset of the chunk inside the stage
+};
+
+struct StreamTasks {
+    const int32_t* task_row;
+    const int32_t* task_ent;
+    const int64_t* part_off;    // per entry: offset of its partial in the scratch vector
+    unsigned* row_count;        // per row: completed entry tasks, never reset (wraps by entry count)
+    unsigned* ready;            // backward: per row, epoch once all U partials are written
+};
+
+// ring of `stages` stages of `stage_bytes` (a multiple of 16), the parent
+// segment, the row-sum scratch, mbarriers and chunk descriptors
+__host__ __device__ constexpr size_t stream_smem_bytes(size_t acc_size, int stages, int stage_bytes) {
+    return (size_t)stages * stage_bytes + (SS_MAX_B + 256) * acc_size + 2 * SS_MAX_STAGES * sizeof(uint64_t) +
+           SS_MAX_STAGES * sizeof(StreamMeta) + 64;
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+// The waiting thread is suspended (up to the hint, 0.1 ms) until the phase
+// completes, so waiting warps do not take issue slots from working ones.
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity), "r"(100000u)
+        : "memory");
+    return ok != 0;
+}
+// wait until the phase with the given parity has completed; false on timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, long long limit) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity))
+        if (clock64() - t0 > limit) return false;
+    return true;
+}
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+template <int NC>
+__device__ __forceinline__ void consumers_sync() { asm volatile("bar.sync 1, %0;" ::"n"(NC) : "memory"); }
+
+// acc[rr] += sum over the chunk's columns of block(r, c) * x(c); rows r of this
+// thread as set up by the caller (b <= NC: one row, columns strided by the G
+// groups; otherwise rows r + NC*rr, all columns)
+template <int NC, int RPT, typename TB, typename ACC>
+__device__ __forceinline__ void stream_chunk(const TB* __restrict__ d, const ACC* __restrict__ xs, int b, int ncols, int r,
+                                             int g, int G, ACC (&acc)[RPT]) {
+    if (b <= NC) {
+        if (g >= G) return;
+        const TB* col = d + r;
+        ACC a0 = acc[0], a1 = 0;
+        int c = g;
+        for (; c + G < ncols; c += 2 * G) {
+            a0 += cvt<ACC>(col[(int64_t)c * b]) * xs[c];
+            a1 += cvt<ACC>(col[(int64_t)(c + G) * b]) * xs[c + G];
+        }
+        if (c < ncols) a0 += cvt<ACC>(col[(int64_t)c * b]) * xs[c];
+        acc[0] = a0 + a1;
+    } else {
+        for (int c = 0; c < ncols; ++c) {
+            const ACC x = xs[c];
+            #pragma unroll
+            for (int rr = 0; rr < RPT; ++rr) {
+                const int row = r + NC * rr;
+                if (row < b) acc[rr] += cvt<ACC>(d[(int64_t)c * b + row]) * x;
+            }
+        }
+    }
+}
+
+// the row sums of this task's product for rows ctid (+ NC*rr), as seen by
+// threads ctid < b (b <= NC) or all threads otherwise
+template <int NC, int RPT, typename ACC>
+__device__ __forceinline__ void stream_reduce(ACC* red, int b, int r, int g, int G, int ctid, ACC (&acc)[RPT]) {
+    if (b <= NC) {
+        if (g < G) red[g * b + r] = acc[0];
+        consumers_sync<NC>();
+        if (ctid < b) {
+            ACC s = 0;
+            for (int gg = 0; gg < G; ++gg) s += red[gg * b + ctid];
+            acc[0] = s;
+        }
+    }
+}
+
+// CW consumer warps; `stages` stages of `stage_bytes` bytes each
+template <typename TL, typename TU, typename TX, typename ACC, bool FORWARD, int CW>
+__global__ void __launch_bounds__(32 * CW + 32)
+    k_ilu_stream(IluRows R, const TL* __restrict__ LD, const TU* __restrict__ Aval, StreamTasks T, int ntasks,
+                 const TX* __restrict__ v, TX* __restrict__ zx, ACC* __restrict__ part, SweepSync S, int nstage,
+                 int stage_bytes) {
+    constexpr int NC = 32 * CW;                  // consumer threads
+    constexpr int RPT = (SS_MAX_B + NC - 1) / NC;
+    extern __shared__ __align__(128) unsigned char ss_smem[];
+    unsigned char* stages = ss_smem;
+    ACC* xs = reinterpret_cast<ACC*>(ss_smem + (size_t)nstage * stage_bytes);
+    ACC* red = xs + SS_MAX_B;                    // G*b <= NC <= 256 row sums
+    uint64_t* full = reinterpret_cast<uint64_t*>(red + 256);
+    uint64_t* empty = full + SS_MAX_STAGES;
+    StreamMeta* meta = reinterpret_cast<StreamMeta*>(empty + SS_MAX_STAGES);
+    __shared__ int s_last;
+    const int chunk_bytes = stage_bytes - 16;    // payload before rounding out to 16 bytes
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        for (int s = 0; s < nstage; ++s) {
+            mbar_init(full + s, 1);
+            mbar_init(empty + s, CW);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    if (warp == CW) {
+        // ------------------------------------------------------------ producer
+        if (lane != 0) return;
+        int stage = 0;
+        unsigned phase = 0;
+        for (;;) {
+            const unsigned t = atomicAdd(S.counter, 1u);
+            if (t >= (unsigned)ntasks) {
+                if (!mbar_wait(empty + stage, phase ^ 1u, S.spin_limit)) atomicExch(S.status, 1);
+                meta[stage].task = -1;
+                mbar_arrive(full + stage);
+                return;
+            }
+            const int pr = T.task_row[t], q = T.task_ent[t];
+            const int b = R.prow_b[pr];
+            const unsigned char* base = nullptr;
+            int cols = 0, esz = 1;
+            if (q >= 0) {
+                if (FORWARD) { base = reinterpret_cast<const unsigned char*>(LD + R.lo_L[q]); cols = R.lo_nc[q]; esz = sizeof(TL); }
+                else { base = reinterpret_cast<const unsigned char*>(Aval + R.up_U[q]); cols = R.up_nc[q]; esz = sizeof(TU); }
+            } else if (q == -2) {
+                base = reinterpret_cast<const unsigned char*>(LD + R.dinv_off[pr]);
+                cols = b;
+                esz = sizeof(TL);
+            }
+            const int kc = cols > 0 ? max(1, min(cols, chunk_bytes / (b * esz))) : 1;
+            const int nchunk = cols > 0 ? (cols + kc - 1) / kc : 1;
+            for (int ch = 0; ch < nchunk; ++ch) {
+                if (!mbar_wait(empty + stage, phase ^ 1u, S.spin_limit)) atomicExch(S.status, 1);
+                StreamMeta m;
+                m.task = (int)t; m.pr = pr; m.q = q; m.chunk = ch; m.nchunk = nchunk;
+                m.col0 = ch * kc;
+                m.ncols = cols > 0 ? min(kc, cols - ch * kc) : 0;
+                m.shift = 0;
+                if (cols > 0) {
+                    const uintptr_t src = reinterpret_cast<uintptr_t>(base + (size_t)m.col0 * b * esz);
+                    const uintptr_t a0 = src & ~(uintptr_t)15;
+                    const unsigned bytes = (unsigned)((size_t)m.ncols * b * esz);
+                    const unsigned len = (unsigned)(((src - a0) + bytes + 15) & ~(uintptr_t)15);
+                    m.shift = (int)((src - a0) / esz);
+                    meta[stage] = m;
+                    mbar_arrive_expect_tx(full + stage, len);
+                    bulk_copy_g2s(stages + (size_t)stage * stage_bytes, reinterpret_cast<const void*>(a0), len, full + stage);
+                } else {
+                    meta[stage] = m;
+                    mbar_arrive(full + stage);
+                }
+                if (++stage == nstage) { stage = 0; phase ^= 1u; }
+            }
+        }
+    }
+
+    // ---------------------------------------------------------------- consumers
+    const int ctid = tid;
+    int stage = 0;
+    unsigned phase = 0;
+    int pr = 0, q = 0, b = 0, G = 1, r = 0, g = 0;
+    ACC acc[RPT];
+    for (;;) {
+        if (!mbar_wait(full + stage, phase, S.spin_limit)) { if (ctid == 0) atomicExch(S.status, 1); }
+        const StreamMeta m = meta[stage];
+        if (m.task < 0) break;
+        if (m.chunk == 0) {
+            pr = m.pr;
+            q = m.q;
+            b = R.prow_b[pr];
+            if (b <= NC) { G = NC / b; r = ctid % b; g = ctid / b; }
+            else { G = 1; r = ctid; g = 0; }
+            #pragma unroll
+            for (int rr = 0; rr < RPT; ++rr) acc[rr] = 0;
+            if (q >= 0) {
+                const int par = FORWARD ? R.lo_par[q] : R.up_par[q];
+                const int nc = FORWARD ? R.lo_nc[q] : R.up_nc[q];
+                if (ctid == 0 && !wait_flag(S.flags, par, S.epoch, S.spin_limit)) atomicExch(S.status, 1);
+                consumers_sync<NC>();
+                const TX* zp = zx + R.z_off[par];
+                for (int c = ctid; c < nc; c += NC) xs[c] = cvt<ACC>(ld_cg(zp + c));
+                consumers_sync<NC>();
+            } else if (q == -2) {
+                // t_r = z_r - sum of the row's U partials, in entry order
+                const int q0 = R.up_ptr[pr], q1 = R.up_ptr[pr + 1];
+                if (q1 > q0 && ctid == 0 && !wait_flag(T.ready, pr, S.epoch, S.spin_limit)) atomicExch(S.status, 1);
+                consumers_sync<NC>();
+                for (int i = ctid; i < b; i += NC) {
+                    ACC s = 0;
+                    for (int qq = q0; qq < q1; ++qq) s += ld_cg(part + T.part_off[qq] + i);
+                    xs[i] = cvt<ACC>(from_d<TX>(to_d(ld_cg(zx + R.z_off[pr] + i)) - (double)s));
+                }
+                consumers_sync<NC>();
+            } else {
+                // forward row without lower entries: z_r = v_r
+                for (int i = ctid; i < b; i += NC) zx[R.z_off[pr] + i] = v[R.v_off[pr] + i];
+                consumers_sync<NC>();
+                if (ctid == 0) {
+                    __threadfence();
+                    st_release(S.flags + pr, S.epoch);
+                }
+            }
+        }
+        if (m.ncols > 0) {
+            const unsigned char* sb = stages + (size_t)stage * stage_bytes;
+            if (FORWARD || q == -2)
+                stream_chunk<NC, RPT, TL, ACC>(reinterpret_cast<const TL*>(sb) + m.shift, xs + m.col0, b, m.ncols, r, g, G, acc);
+            else
+                stream_chunk<NC, RPT, TU, ACC>(reinterpret_cast<const TU*>(sb) + m.shift, xs + m.col0, b, m.ncols, r, g, G, acc);
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(empty + stage);
+        if (++stage == nstage) { stage = 0; phase ^= 1u; }
+        if (m.chunk != m.nchunk - 1 || q == -1) continue;
+
+        // ------------------------------------------------ the task's last chunk
+        stream_reduce<NC, RPT>(red, b, r, g, G, ctid, acc);
+        if (q == -2) {
+            // x_r = inv(D_r) t_r: the row is complete
+            if (b <= NC) { if (ctid < b) zx[R.z_off[pr] + ctid] = from_d<TX>((double)acc[0]); }
+            else {
+                #pragma unroll
+                for (int rr = 0; rr < RPT; ++rr)
+                    if (ctid + NC * rr < b) zx[R.z_off[pr] + ctid + NC * rr] = from_d<TX>((double)acc[rr]);
+            }
+            consumers_sync<NC>();
+            if (ctid == 0) {
+                __threadfence();
+                st_release(S.flags + pr, S.epoch);
+            }
+            continue;
+        }
+        if (b <= NC) { if (ctid < b) part[T.part_off[q] + ctid] = acc[0]; }
+        else {
+            #pragma unroll
+            for (int rr = 0; rr < RPT; ++rr)
+                if (ctid + NC * rr < b) part[T.part_off[q] + ctid + NC * rr] = acc[rr];
+        }
+        consumers_sync<NC>();
+        const int q0 = FORWARD ? R.lo_ptr[pr] : R.up_ptr[pr];
+        const int q1 = FORWARD ? R.lo_ptr[pr + 1] : R.up_ptr[pr + 1];
+        if (ctid == 0) {
+            __threadfence();                          // the CTA's partial before the count
+            const unsigned old = atomicAdd(T.row_count + pr, 1u);
+            const bool last = ((old + 1u) % (unsigned)(q1 - q0)) == 0u;
+            if (last) __threadfence();                // the others' partials after the count
+            if (last && !FORWARD) st_release(T.ready + pr, S.epoch);
+            s_last = last;
+        }
+        consumers_sync<NC>();
+        if constexpr (FORWARD) {
+            if (!s_last) continue;
+            for (int i = ctid; i < b; i += NC) {
+                ACC s = 0;
+                for (int qq = q0; qq < q1; ++qq) s += ld_cg(part + T.part_off[qq] + i);
+                zx[R.z_off[pr] + i] = from_d<TX>(to_d(v[R.v_off[pr] + i]) - (double)s);
+            }
+            consumers_sync<NC>();
+            if (ctid == 0) {
+                __threadfence();
+                st_release(S.flags + pr, S.epoch);
+            }
+        }
+    }
+}
+
+}  // namespace chidg

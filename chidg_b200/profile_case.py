@@ -20,7 +20,7 @@ def main():
     ap.add_argument("--p", type=int, default=2)
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--precon", default="ilu0")
-    ap.add_argument("--schedule", default="tasks", choices=["tasks", "dataflow", "levels"])
+    ap.add_argument("--schedule", default="stream", choices=["tasks", "stream", "dataflow", "levels"])
     ap.add_argument("--time", action="store_true", help="print CUDA-event times per kernel class")
     ap.add_argument("--solves", type=int, default=0, help="also time this many full solves per precision mode")
     args = ap.parse_args()
@@ -47,7 +47,7 @@ def main():
 
 
 
-def solve_timings(n=24, p=2, reps=6, precisions=("fp64", "mixed_fp32", "mixed_bf16"), schedule="tasks"):
+def solve_timings(n=24, p=2, reps=6, precisions=("fp64", "mixed_fp32", "mixed_bf16"), schedule="stream"):
     """Wall time of full solves (factorisation + FGMRES) per precision mode."""
     import time
     pat = mesh.box_pattern(n, n, n, 5, mesh.nterms_of_order(p))

@@ -235,12 +235,17 @@ int chidg_gpu_precon_apply(chidg_gpu_precon* M, chidg_gpu_matrix* A,
  * CHIDG_SCHED_DATAFLOW one launch per sweep, rows taken in topological order,
  *                      each waiting (bounded) only for its own parents;
  * CHIDG_SCHED_TASKS    one launch per sweep, one task per block product, the
- *                      last task of a row completes it (the default).
- * LEVELS and DATAFLOW run identical per-row arithmetic; TASKS sums each
- * block's product before adding the blocks (same values to rounding). */
+ *                      last task of a row completes it;
+ * CHIDG_SCHED_STREAM   the TASKS work list run by persistent CTAs whose
+ *                      blocks are copied into shared memory ahead of the
+ *                      dependency waits (the default; blocks of more than
+ *                      1024 rows run the TASKS schedule).
+ * LEVELS and DATAFLOW run identical per-row arithmetic; TASKS and STREAM sum
+ * each block's product before adding the blocks (same values to rounding). */
 #define CHIDG_SCHED_LEVELS   0
 #define CHIDG_SCHED_DATAFLOW 1
 #define CHIDG_SCHED_TASKS    2
+#define CHIDG_SCHED_STREAM   3
 int chidg_gpu_precon_set_schedule(chidg_gpu_precon* M, int32_t schedule);
 /* Packed factor blocks (L blocks and inverted diagonals at the positions of
  * the matrix's LOCAL blocks, zero elsewhere), as precon_ILU0_t%LD holds them. */

@@ -53,7 +53,7 @@ def test_dot_norm_axpy():
     assert relerr(yg.download(), y - 0.5 * x) < 1e-15
 
 
-@pytest.mark.parametrize("schedule", ["levels", "dataflow", "tasks"])
+@pytest.mark.parametrize("schedule", ["levels", "dataflow", "tasks", "stream"])
 @pytest.mark.parametrize("kind", ["ilu0", "jacobi"])
 @pytest.mark.parametrize("shape,P,nt", CASES)
 def test_precon_factor_and_apply(kind, shape, P, nt, schedule):
@@ -77,7 +77,7 @@ def test_precon_factor_and_apply(kind, shape, P, nt, schedule):
     assert relerr(z, Mo.apply(v)) < 1e-11
 
 
-@pytest.mark.parametrize("schedule", ["levels", "dataflow", "tasks"])
+@pytest.mark.parametrize("schedule", ["levels", "dataflow", "tasks", "stream"])
 @pytest.mark.parametrize("shape,P,sub", [((4, 4, 2), 1, (2, 2, 1)), ((4, 4, 4), 0, (2, 2, 2)), ((6, 3, 3), 1, (3, 1, 1))])
 def test_rasilu0(shape, P, sub, schedule):
     pat, vals, Ao, Ag = setup(shape, P, 1, sub=sub, seed=7)
@@ -119,6 +119,82 @@ def test_schedules_bitwise_identical(kind, sub):
         M.update(Ag)
         out.append(M.apply(Ag, v).download())
     assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("shape,P", [((2, 2, 2), 3), ((3, 2, 2), 4), ((7, 7, 7), 1)])
+def test_stream_sweeps_block_sizes(shape, P):
+    """Streamed sweeps with 320- and 625-row blocks (several rows per consumer
+    thread, several column chunks per block) and with 343 small-block rows."""
+    pat, vals, Ao, Ag = setup(shape, P, seed=24)
+    Mo = O.OraclePrecon(Ao, "ilu0")
+    Mo.update()
+    Mg = api.create_preconditioner("ilu0", schedule="stream")
+    Mg.update(Ag)
+    v = mesh.synth_vector(Ao.n, seed=25)
+    z = Mg.apply(Ag, api.ChidgVector(Ag, v)).download()
+    assert relerr(z, Mo.apply(v)) < 1e-11
+
+
+def test_stream_sweeps_deterministic():
+    """The streamed sweeps' sums have a fixed order whichever CTA runs a task."""
+    pat, vals, Ao, Ag = setup((6, 6, 4), 2, seed=26)
+    v = api.ChidgVector(Ag, mesh.synth_vector(Ao.n, seed=27))
+    M = api.create_preconditioner("ilu0", schedule="stream")
+    M.update(Ag)
+    z1 = M.apply(Ag, v).download()
+    z2 = M.apply(Ag, v).download()
+    assert np.array_equal(z1, z2)
+    M.set_schedule("tasks")
+    assert relerr(M.apply(Ag, v).download(), z1) < 1e-13
+
+
+@pytest.mark.parametrize("precision", ["mixed_fp32", "mixed_bf16"])
+def test_stream_sweeps_mixed_precision(precision):
+    pat, vals, Ao, Ag = setup((4, 4, 4), 2, seed=28)
+    b = mesh.synth_vector(Ao.n, seed=29)
+    solver = api.create_linear_solver("fgmres", tol=0.0, rtol=1e-8, nkrylov=10, inner_fgmres=0, nmax=50,
+                                      precision=precision, mixed_inner_nkrylov=20, mixed_inner_rtol=1e-2,
+                                      mixed_inner_nmax=40)
+    xg = api.ChidgVector(Ag)
+    solver.solve(Ag, xg, api.ChidgVector(Ag, b), api.create_preconditioner("ilu0", schedule="stream"))
+    assert solver.residual_norm <= 1.5e-8 * solver.r0norm_initial
+    r = b - Ao.mv(xg.download())
+    assert np.linalg.norm(r) <= 2e-8 * np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("nvars,P", [(3, 2), (4, 2), (1, 4), (2, 3), (5, 2)])
+def test_factor_tensor_core_inverse_sizes(nvars, P):
+    """Diagonal inverses of 81..136-row blocks (blocked Gauss-Jordan on the FP64
+    tensor cores, partial tiles included) against the oracle's DGETRF/DGETRI."""
+    pat, vals, Ao, Ag = setup((3, 2, 2), P, seed=30, nvars=nvars)
+    Mo = O.OraclePrecon(Ao, "ilu0")
+    Mo.update()
+    Mg = api.create_preconditioner("ilu0")
+    Mg.update(Ag)
+    LDo, LDg = Mo.LD(), Mg.LD()
+    voff, _ = pat.value_offsets()
+    nr, nc = pat.block_dims()
+    worst = 0.0
+    for k in range(pat.nblocks):
+        a = LDo[voff[k]:voff[k] + nr[k] * nc[k]]
+        if np.any(a):
+            worst = max(worst, relerr(LDg[voff[k]:voff[k] + nr[k] * nc[k]], a))
+    assert worst < 1e-10
+
+
+def test_singular_block_reports_element_tensor_core_inverse():
+    pat, vals, Ao, Ag = setup((3, 2, 2), 2, seed=31)
+    voff, _ = pat.value_offsets()
+    nr, nc = pat.block_dims()
+    k = int(np.nonzero((pat.blk_row_elem == 7) & (pat.blk_col_elem == 7))[0][0])
+    bad = vals.copy()
+    blk = bad[voff[k]:voff[k] + nr[k] * nc[k]].reshape(nc[k], nr[k])
+    blk[:, 3] = 0.0                     # a zero row: singular
+    Ag.upload(bad)
+    M = api.create_preconditioner("jacobi")
+    with pytest.raises(_lib.ChidgGpuError) as ei:
+        M.update(Ag)
+    assert ei.value.code == _lib.ESINGULAR and ei.value.element == 7
 
 
 def test_fgmres_inner_default_options():
