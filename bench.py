@@ -79,6 +79,20 @@ def factor_flops(pat):
     return 4 * nL * b ** 3 + 2 * E * b ** 3
 
 
+# DRAM bytes of one launch (dram__bytes_read.sum + dram__bytes_write.sum)
+# from ncu captures of the 14^3 P2 case (2744 elements, 18 032 blocks; the
+# 24^3 workload is too large for a multi-pass capture), scaled to a launch of
+# the workload by its block count.  ilu_apply = both streamed sweeps.
+TRAFFIC_14CUBE_BLOCKS = 18032
+TRAFFIC_14CUBE = {"ilu_apply": 1.118791e9 + 13.724928e6 + 1.520100e9 + 18.709248e6}
+
+
+def measured_traffic(kind, pat):
+    if kind not in TRAFFIC_14CUBE:
+        return None
+    return TRAFFIC_14CUBE[kind] * pat.nblocks / TRAFFIC_14CUBE_BLOCKS
+
+
 # ---------------------------------------------------------------------------
 # clocks during the timed region
 # ---------------------------------------------------------------------------
@@ -424,19 +438,14 @@ def run_gpu(args):
                    "tflops": factor_flops(pat) / (fa_ms / max(fa_n, 1) / 1e3) / 1e12 if fa_n else None},
     }
     # dominant memory-bound kernel by total time: ILU sweeps or matvec
+    sweep = {"stream": "k_ilu_stream forward + backward", "tasks": "k_ilu_tasks forward + backward",
+             "dataflow": "k_ilu_sweep_sf forward + backward", "levels": "k_ilu_forward + k_ilu_backward, all levels"}
     if kernels["ilu_apply"]["total_ms"] >= kernels["matvec"]["total_ms"]:
-        dom, dbytes, dms = "ilu_apply (k_ilu_forward+k_ilu_backward, all levels)", ilub, kernels["ilu_apply"]["avg_ms"]
+        dom, dbytes, dms = f"ilu_apply ({sweep[args.schedule]})", ilub, kernels["ilu_apply"]["avg_ms"]
     else:
         dom, dbytes, dms = "matvec (k_matvec)", mvb, kernels["matvec"]["avg_ms"]
     achieved = dbytes / (dms / 1e3) / 1e9
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        try:
-            with open(tpath) as f:
-                traffic = json.load(f).get(dom.split()[0])
-        except (OSError, ValueError):
-            traffic = None
+    traffic = measured_traffic(dom.split()[0], pat) if args.schedule == "stream" else None
     cpu = None
     if not args.no_cpu and world == 1:
         dt, it = cpu_sample_solve()
