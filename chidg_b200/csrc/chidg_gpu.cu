@@ -11,6 +11,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 
 using namespace chidg;
 
@@ -507,14 +508,32 @@ template int chidg::matvec_launch<double, double>(chidg_gpu_matrix*, const doubl
 template int chidg::matvec_launch<float, float>(chidg_gpu_matrix*, const float*, const float*, float*, const float*, double, double, double*);
 template int chidg::matvec_launch<__nv_bfloat16, float>(chidg_gpu_matrix*, const __nv_bfloat16*, const float*, float*, const float*, double, double, double*);
 
+int chidg::raise_smem_limit(const void* func, size_t bytes) {
+    if (bytes <= 48 * 1024) return CHIDG_GPU_OK;
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, size_t> limit;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    size_t& cur = limit[{dev, func}];
+    if (bytes <= cur) return CHIDG_GPU_OK;
+    const cudaError_t e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return CHIDG_GPU_ECUDA;
+    }
+    cur = bytes;
+    return CHIDG_GPU_OK;
+}
+
 int chidg::set_matvec_smem(chidg_gpu_matrix* A) {
     // allow > 48 KB dynamic shared memory when a row has many wide blocks
     const size_t smem = sizeof(double) * ((size_t)A->max_row_cols + A->mv_threads) + 512;
-    if (smem > 48 * 1024) {
-        cudaFuncSetAttribute(k_matvec<double, double, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaFuncSetAttribute(k_matvec<float, float, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaFuncSetAttribute(k_matvec<__nv_bfloat16, float, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    }
+    int st;
+    if ((st = raise_smem_limit((const void*)k_matvec<double, double, double, double>, smem)) ||
+        (st = raise_smem_limit((const void*)k_matvec<float, float, float, float>, smem)) ||
+        (st = raise_smem_limit((const void*)k_matvec<__nv_bfloat16, float, float, float>, smem)))
+        return st;
     return CHIDG_GPU_OK;
 }
 
@@ -1150,7 +1169,7 @@ extern "C" int chidg_gpu_precon_update(chidg_gpu_precon* M, chidg_gpu_matrix* A,
     const int nlev = (int)P.fwd_ptr.size() - 1;
     const int tiles_1d = (P.max_b + GT_M - 1) / GT_M;
     // one CTA per output block on the FP64 tensor cores for blocks up to 136 x 136
-    cudaFuncSetAttribute(k_task_gemm_dmma<double, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DM_SMEM);
+    if ((st = raise_smem_limit((const void*)k_task_gemm_dmma<double, double, double>, DM_SMEM))) return fail(ctx, st, "factor GEMM shared memory");
     const int ph = prof_begin(ctx, kProfFactor);
     for (int l = 0; l < nlev; ++l) {
         const int pg = prof_begin(ctx, kProfFactorGemm);
@@ -1222,11 +1241,10 @@ static int dataflow_sweeps(chidg_gpu_precon* M, const TL* LD, const TU* U, const
     const size_t smem = sizeof(ACC) * ((size_t)std::max(P.max_lo_cols, P.max_up_cols) + P.max_b + threads) + 512;
     auto kf = k_ilu_sweep_sf<TL, TU, TV, ACC, true>;
     auto kb = k_ilu_sweep_sf<TL, TU, TV, ACC, false>;
+    int st;
+    if ((st = raise_smem_limit((const void*)kf, smem)) || (st = raise_smem_limit((const void*)kb, smem)))
+        return fail(ctx, st, "dataflow sweep shared memory");
     if (M->sf_grid[variant] == 0) {
-        if (smem > 48 * 1024) {
-            cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        }
         int per_sm = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kb, threads, smem) != cudaSuccess || per_sm < 1) {
             cudaGetLastError();
@@ -1237,7 +1255,6 @@ static int dataflow_sweeps(chidg_gpu_precon* M, const TL* LD, const TU* U, const
     const int grid = M->sf_grid[variant];
     unsigned* counters = (unsigned*)M->sync.ptr;
     SweepSync S{counters, counters + 2, 0u, (int*)(ctx->d_scal + kSlotStatus), kSpinLimit};
-    int st;
     cudaError_t e = cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned), ctx->stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "sweep counters");
     int ph = prof_begin(ctx, sizeof(TV) == 8 ? kProfIluForward : kProfIlu32);
@@ -1314,13 +1331,13 @@ static int task_sweeps(chidg_gpu_precon* M, const TL* LD, const TU* U, const TV*
 
 // Shape of the streamed sweeps: consumer warps per CTA, ring stages and stage
 // size.  Read once from CHIDG_STREAM_SHAPE="warps,stages,kbytes" when set.
-struct StreamShape { int cw = 8, nstage = 2, stage_bytes = 48 * 1024; };
+struct StreamShape { int cw = 8, nstage = 2, stage_bytes = 24 * 1024; };
 static StreamShape stream_shape() {
     static StreamShape sh = [] {
         StreamShape d;
         if (const char* e = std::getenv("CHIDG_STREAM_SHAPE")) {
             int cw = 0, ns = 0, kb = 0;
-            if (std::sscanf(e, "%d,%d,%d", &cw, &ns, &kb) == 3 && (cw == 2 || cw == 4 || cw == 8) && ns >= 2 &&
+            if (std::sscanf(e, "%d,%d,%d", &cw, &ns, &kb) == 3 && (cw == 4 || cw == 8 || cw == 16) && ns >= 2 &&
                 ns <= SS_MAX_STAGES && kb >= 2 && kb <= 96)
                 d = StreamShape{cw, ns, kb * 1024};
         }
@@ -1334,11 +1351,12 @@ static int stream_launch(chidg_gpu_precon* M, const TL* LD, const TU* U, StreamT
                          void* part, SweepSync S, const StreamShape& sh, int variant) {
     chidg_gpu_ctx* ctx = M->ctx;
     using ACC = typename AccOf<TV>::type;
-    const size_t smem = stream_smem_bytes(sizeof(ACC), sh.nstage, sh.stage_bytes);
+    const size_t smem = stream_smem_bytes(sizeof(ACC), sh.nstage, sh.stage_bytes, M->P.max_b, 32 * CW);
     auto k = k_ilu_stream<TL, TU, TV, ACC, FWD, CW>;
+    int st;
+    if ((st = raise_smem_limit((const void*)k, smem))) return fail(ctx, st, "streamed sweep shared memory");
     int& grid = M->ss_grid[variant][FWD ? 0 : 1];
     if (grid == 0) {
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         int per_sm = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 32 * CW + 32, smem) != cudaSuccess || per_sm < 1) {
             cudaGetLastError();
@@ -1347,7 +1365,7 @@ static int stream_launch(chidg_gpu_precon* M, const TL* LD, const TU* U, StreamT
         grid = per_sm * ctx->nsm;
     }
     k<<<std::max(1, std::min(grid, ntask)), 32 * CW + 32, smem, ctx->stream>>>(M->P.rows, LD, U, Tk, ntask, v, zx, (ACC*)part,
-                                                                              S, sh.nstage, sh.stage_bytes);
+                                                                              S, sh.nstage, sh.stage_bytes, M->P.max_b);
     return check_launch(ctx, FWD ? "k_ilu_stream forward" : "k_ilu_stream backward");
 }
 
@@ -1373,9 +1391,9 @@ static int stream_sweeps(chidg_gpu_precon* M, const TL* LD, const TU* U, const T
     StreamTasks Tf{(const int32_t*)P.d_tf_row.ptr, (const int32_t*)P.d_tf_ent.ptr, (const int64_t*)P.d_poff_f.ptr,
                    flags + P.nprow, flags + 3 * P.nprow};
     switch (sh.cw) {
-        case 2: st = stream_launch<TL, TU, TV, true, 2>(M, LD, U, Tf, P.ntask_f, v, zx, pb.ptr, S, sh, variant); break;
-        case 8: st = stream_launch<TL, TU, TV, true, 8>(M, LD, U, Tf, P.ntask_f, v, zx, pb.ptr, S, sh, variant); break;
-        default: st = stream_launch<TL, TU, TV, true, 4>(M, LD, U, Tf, P.ntask_f, v, zx, pb.ptr, S, sh, variant);
+        case 16: st = stream_launch<TL, TU, TV, true, 16>(M, LD, U, Tf, P.ntask_f, v, zx, pb.ptr, S, sh, variant); break;
+        case 4: st = stream_launch<TL, TU, TV, true, 4>(M, LD, U, Tf, P.ntask_f, v, zx, pb.ptr, S, sh, variant); break;
+        default: st = stream_launch<TL, TU, TV, true, 8>(M, LD, U, Tf, P.ntask_f, v, zx, pb.ptr, S, sh, variant);
     }
     if (st) return st;
     if (sizeof(TV) == 8) {
@@ -1387,9 +1405,9 @@ static int stream_sweeps(chidg_gpu_precon* M, const TL* LD, const TU* U, const T
     StreamTasks Tb{(const int32_t*)P.d_sb_row.ptr, (const int32_t*)P.d_sb_ent.ptr, (const int64_t*)P.d_poff_b.ptr,
                    flags + 2 * P.nprow, flags + 3 * P.nprow};
     switch (sh.cw) {
-        case 2: st = stream_launch<TL, TU, TV, false, 2>(M, LD, U, Tb, P.ntask_sb, v, zx, pb.ptr, S, sh, variant); break;
-        case 8: st = stream_launch<TL, TU, TV, false, 8>(M, LD, U, Tb, P.ntask_sb, v, zx, pb.ptr, S, sh, variant); break;
-        default: st = stream_launch<TL, TU, TV, false, 4>(M, LD, U, Tb, P.ntask_sb, v, zx, pb.ptr, S, sh, variant);
+        case 16: st = stream_launch<TL, TU, TV, false, 16>(M, LD, U, Tb, P.ntask_sb, v, zx, pb.ptr, S, sh, variant); break;
+        case 4: st = stream_launch<TL, TU, TV, false, 4>(M, LD, U, Tb, P.ntask_sb, v, zx, pb.ptr, S, sh, variant); break;
+        default: st = stream_launch<TL, TU, TV, false, 8>(M, LD, U, Tb, P.ntask_sb, v, zx, pb.ptr, S, sh, variant);
     }
     if (st) return st;
     prof_end(ctx, ph);
@@ -1501,16 +1519,14 @@ int chidg::precon_set_smem(chidg_gpu_precon* M) {
     const int threads = P.sweep_threads;
     const size_t sf = sizeof(double) * ((size_t)P.max_lo_cols + threads) + 512;
     const size_t sb = sizeof(double) * ((size_t)P.max_up_cols + P.max_b + threads) + 512;
-    if (sf > 48 * 1024) {
-        cudaFuncSetAttribute(k_ilu_forward<double, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sf);
-        cudaFuncSetAttribute(k_ilu_forward<float, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sf);
-        cudaFuncSetAttribute(k_ilu_forward<__nv_bfloat16, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sf);
-    }
-    if (sb > 48 * 1024) {
-        cudaFuncSetAttribute(k_ilu_backward<double, double, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
-        cudaFuncSetAttribute(k_ilu_backward<float, float, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
-        cudaFuncSetAttribute(k_ilu_backward<__nv_bfloat16, __nv_bfloat16, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
-    }
+    int st;
+    if ((st = raise_smem_limit((const void*)k_ilu_forward<double, double, double>, sf)) ||
+        (st = raise_smem_limit((const void*)k_ilu_forward<float, float, float>, sf)) ||
+        (st = raise_smem_limit((const void*)k_ilu_forward<__nv_bfloat16, float, float>, sf)) ||
+        (st = raise_smem_limit((const void*)k_ilu_backward<double, double, double, double>, sb)) ||
+        (st = raise_smem_limit((const void*)k_ilu_backward<float, float, float, float>, sb)) ||
+        (st = raise_smem_limit((const void*)k_ilu_backward<__nv_bfloat16, __nv_bfloat16, float, float>, sb)))
+        return st;
     return CHIDG_GPU_OK;
 }
 

@@ -167,6 +167,11 @@ int matrix_lowp(chidg_gpu_matrix* A, int precision);
 template <typename TA, typename TV>
 int matvec_launch(chidg_gpu_matrix* A, const TA* val, const TV* x, TV* y, const TV* z, double alpha, double beta, double* row_sq);
 int set_matvec_smem(chidg_gpu_matrix* A);
+// Let `func` launch with `bytes` of dynamic shared memory on the current
+// device.  The limit belongs to the kernel, not to one matrix or
+// preconditioner, so it is only ever raised: a smaller value set for one
+// object would make another object's launches fail.
+int raise_smem_limit(const void* func, size_t bytes);
 template <typename TV>
 int precon_apply_impl(chidg_gpu_precon* M, const TV* v, TV* z, int precision);
 int precon_set_smem(chidg_gpu_precon* M);

@@ -40,6 +40,7 @@ namespace chidg {
 
 constexpr int SS_MAX_B = 1024;                              // rows per block
 constexpr int SS_MAX_STAGES = 8;
+constexpr int SS_MAX_NC = 512;                              // consumer threads (16 warps)
 
 struct StreamMeta {
     int task;      // ticket, -1 = end of the sweep for this CTA
@@ -58,9 +59,11 @@ struct StreamTasks {
 };
 
 // ring of `stages` stages of `stage_bytes` (a multiple of 16), the parent
-// segment, the row-sum scratch, mbarriers and chunk descriptors
-__host__ __device__ constexpr size_t stream_smem_bytes(size_t acc_size, int stages, int stage_bytes) {
-    return (size_t)stages * stage_bytes + (SS_MAX_B + 256) * acc_size + 2 * SS_MAX_STAGES * sizeof(uint64_t) +
+// segment (xcap values: the largest block of the programme), the row-sum
+// scratch (nc values, one per consumer thread), mbarriers and descriptors
+__host__ __device__ constexpr size_t stream_xcap(int max_b) { return (size_t)((max_b + 31) / 32) * 32; }
+__host__ __device__ constexpr size_t stream_smem_bytes(size_t acc_size, int stages, int stage_bytes, int max_b, int nc) {
+    return (size_t)stages * stage_bytes + (stream_xcap(max_b) + nc) * acc_size + 2 * SS_MAX_STAGES * sizeof(uint64_t) +
            SS_MAX_STAGES * sizeof(StreamMeta) + 64;
 }
 
@@ -103,6 +106,14 @@ __device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsign
 }
 template <int NC>
 __device__ __forceinline__ void consumers_sync() { asm volatile("bar.sync 1, %0;" ::"n"(NC) : "memory"); }
+// counter increment that releases the writes ordered before it (this thread's
+// and, through the preceding barrier, the other consumers') and acquires the
+// writes the other CTAs released with their increments
+__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
 
 // acc[rr] += sum over the chunk's columns of block(r, c) * x(c); rows r of this
 // thread as set up by the caller (b <= NC: one row, columns strided by the G
@@ -153,14 +164,15 @@ template <typename TL, typename TU, typename TX, typename ACC, bool FORWARD, int
 __global__ void __launch_bounds__(32 * CW + 32)
     k_ilu_stream(IluRows R, const TL* __restrict__ LD, const TU* __restrict__ Aval, StreamTasks T, int ntasks,
                  const TX* __restrict__ v, TX* __restrict__ zx, ACC* __restrict__ part, SweepSync S, int nstage,
-                 int stage_bytes) {
+                 int stage_bytes, int max_b) {
     constexpr int NC = 32 * CW;                  // consumer threads
+    static_assert(NC <= SS_MAX_NC, "row-sum scratch");
     constexpr int RPT = (SS_MAX_B + NC - 1) / NC;
     extern __shared__ __align__(128) unsigned char ss_smem[];
     unsigned char* stages = ss_smem;
     ACC* xs = reinterpret_cast<ACC*>(ss_smem + (size_t)nstage * stage_bytes);
-    ACC* red = xs + SS_MAX_B;                    // G*b <= NC <= 256 row sums
-    uint64_t* full = reinterpret_cast<uint64_t*>(red + 256);
+    ACC* red = xs + stream_xcap(max_b);          // G*b <= NC row sums
+    uint64_t* full = reinterpret_cast<uint64_t*>(red + NC);
     uint64_t* empty = full + SS_MAX_STAGES;
     StreamMeta* meta = reinterpret_cast<StreamMeta*>(empty + SS_MAX_STAGES);
     __shared__ int s_last;
@@ -269,10 +281,7 @@ __global__ void __launch_bounds__(32 * CW + 32)
                 // forward row without lower entries: z_r = v_r
                 for (int i = ctid; i < b; i += NC) zx[R.z_off[pr] + i] = v[R.v_off[pr] + i];
                 consumers_sync<NC>();
-                if (ctid == 0) {
-                    __threadfence();
-                    st_release(S.flags + pr, S.epoch);
-                }
+                if (ctid == 0) st_release(S.flags + pr, S.epoch);
             }
         }
         if (m.ncols > 0) {
@@ -298,10 +307,7 @@ __global__ void __launch_bounds__(32 * CW + 32)
                     if (ctid + NC * rr < b) zx[R.z_off[pr] + ctid + NC * rr] = from_d<TX>((double)acc[rr]);
             }
             consumers_sync<NC>();
-            if (ctid == 0) {
-                __threadfence();
-                st_release(S.flags + pr, S.epoch);
-            }
+            if (ctid == 0) st_release(S.flags + pr, S.epoch);
             continue;
         }
         if (b <= NC) { if (ctid < b) part[T.part_off[q] + ctid] = acc[0]; }
@@ -314,10 +320,8 @@ __global__ void __launch_bounds__(32 * CW + 32)
         const int q0 = FORWARD ? R.lo_ptr[pr] : R.up_ptr[pr];
         const int q1 = FORWARD ? R.lo_ptr[pr + 1] : R.up_ptr[pr + 1];
         if (ctid == 0) {
-            __threadfence();                          // the CTA's partial before the count
-            const unsigned old = atomicAdd(T.row_count + pr, 1u);
+            const unsigned old = atom_add_acq_rel(T.row_count + pr, 1u);
             const bool last = ((old + 1u) % (unsigned)(q1 - q0)) == 0u;
-            if (last) __threadfence();                // the others' partials after the count
             if (last && !FORWARD) st_release(T.ready + pr, S.epoch);
             s_last = last;
         }
@@ -330,10 +334,7 @@ __global__ void __launch_bounds__(32 * CW + 32)
                 zx[R.z_off[pr] + i] = from_d<TX>(to_d(v[R.v_off[pr] + i]) - (double)s);
             }
             consumers_sync<NC>();
-            if (ctid == 0) {
-                __threadfence();
-                st_release(S.flags + pr, S.epoch);
-            }
+            if (ctid == 0) st_release(S.flags + pr, S.epoch);
         }
     }
 }

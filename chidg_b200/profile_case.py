@@ -31,6 +31,12 @@ def main():
     z = api.ChidgVector(A)
     M = api.create_preconditioner(args.precon, schedule=args.schedule)
     if args.time:
+        # one untimed round first: launch set-up (function attributes,
+        # occupancy queries) happens on the first call of each kernel
+        M.update(A)
+        M.apply(A, v, z)
+        api.chidg_mv(A, v, z)
+        A.ctx.sync()
         A.ctx.set_profiling(True)
     for _ in range(args.reps):
         M.update(A)

@@ -77,6 +77,7 @@ class Server:
         self._mem_used = 0
         self.peak_mem_used = 0
         self.batches = 0
+        self._workers: list[threading.Thread] = []
         self._slot_ctx = queue.Queue()
         for _ in range(slots):
             self._slot_ctx.put(api.Context(device))
@@ -90,9 +91,12 @@ class Server:
         return fut
 
     def close(self):
-        """Finish the queued requests, then stop the dispatcher."""
+        """Finish the queued requests, then stop the dispatcher and wait for the
+        batches still on the GPU (no library call may outlive the server)."""
         self._queue.put((None, None))
         self._dispatcher.join(timeout=600)
+        for t in list(self._workers):
+            t.join(timeout=600)
 
     # -- internals ----------------------------------------------------------
     def _dispatch(self):
@@ -137,7 +141,9 @@ class Server:
                 self.peak_mem_used = max(self.peak_mem_used, self._mem_used)
                 self.batches += 1
             ctx = self._slot_ctx.get()
-            threading.Thread(target=self._run_batch, args=(ctx, batch, nbytes), daemon=True).start()
+            worker = threading.Thread(target=self._run_batch, args=(ctx, batch, nbytes), daemon=True)
+            self._workers = [t for t in self._workers if t.is_alive()] + [worker]
+            worker.start()
 
     def _run_batch(self, ctx, batch, nbytes):
         start = time.perf_counter()
