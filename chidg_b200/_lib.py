@@ -19,7 +19,7 @@ STATUS_NAMES = {0: "OK", 1: "EINVAL", 2: "ENOMEM", 3: "ESINGULAR", 4: "ENONFINIT
 
 BLK_LOCAL, BLK_CHIMERA, BLK_BC, BLK_HB = 0, 1, 2, 3
 PRECON_IDENTITY, PRECON_JACOBI, PRECON_ILU0, PRECON_RASILU0 = 0, 1, 2, 3
-FP64, MIXED_FP32, MIXED_BF16 = 0, 1, 2
+FP64, MIXED_FP32, MIXED_BF16, MIXED_PRECON_FP32 = 0, 1, 2, 3
 ORTH_CGS, ORTH_MGS = 0, 1
 SCHED_LEVELS, SCHED_DATAFLOW, SCHED_TASKS, SCHED_STREAM = 0, 1, 2, 3
 

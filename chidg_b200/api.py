@@ -232,7 +232,8 @@ def chidg_mv(A: ChidgMatrix, x: ChidgVector, y: ChidgVector | None = None) -> Ch
 
 PRECON_KINDS = {"identity": _lib.PRECON_IDENTITY, "jacobi": _lib.PRECON_JACOBI, "ilu0": _lib.PRECON_ILU0,
                 "rasilu0": _lib.PRECON_RASILU0}
-PRECISIONS = {"fp64": _lib.FP64, "mixed_fp32": _lib.MIXED_FP32, "mixed_bf16": _lib.MIXED_BF16}
+PRECISIONS = {"fp64": _lib.FP64, "mixed_fp32": _lib.MIXED_FP32, "mixed_bf16": _lib.MIXED_BF16,
+              "mixed_precon_fp32": _lib.MIXED_PRECON_FP32}
 
 
 class Preconditioner:

@@ -473,6 +473,7 @@ extern "C" int chidg_gpu_matrix_scale_diagonal(chidg_gpu_matrix* A, const double
 int chidg::matrix_lowp(chidg_gpu_matrix* A, int precision) {
     chidg_gpu_ctx* ctx = A->ctx;
     if (precision == CHIDG_GPU_FP64) return CHIDG_GPU_OK;
+    if (precision == CHIDG_GPU_MIXED_PRECON_FP32) precision = CHIDG_GPU_MIXED_FP32;   // the same FP32 copy
     const int grid = grid_for(A->nval, 256, ctx->nsm * 8);
     int st;
     if (precision == CHIDG_GPU_MIXED_FP32) {
@@ -1154,7 +1155,7 @@ extern "C" int chidg_gpu_precon_update(chidg_gpu_precon* M, chidg_gpu_matrix* A,
     if (!M || !A || A != M->A) return CHIDG_GPU_EINVAL;
     chidg_gpu_ctx* ctx = M->ctx;
     cudaSetDevice(ctx->device);
-    if (precision < CHIDG_GPU_FP64 || precision > CHIDG_GPU_MIXED_BF16) return fail(ctx, CHIDG_GPU_EINVAL, "precon_update: bad precision");
+    if (precision < CHIDG_GPU_FP64 || precision > CHIDG_GPU_MIXED_PRECON_FP32) return fail(ctx, CHIDG_GPU_EINVAL, "precon_update: bad precision");
     ctx->err_elem = -1;
     if (M->kind == CHIDG_PRECON_IDENTITY) { M->stamp = A->stamp; M->precision = precision; return CHIDG_GPU_OK; }
     IluProgram& P = M->P;
@@ -1215,7 +1216,7 @@ extern "C" int chidg_gpu_precon_update(chidg_gpu_precon* M, chidg_gpu_matrix* A,
     }
     if (precision != CHIDG_GPU_FP64) {
         if ((st = matrix_lowp(A, precision))) return st;
-        if (precision == CHIDG_GPU_MIXED_FP32) {
+        if (precision == CHIDG_GPU_MIXED_FP32 || precision == CHIDG_GPU_MIXED_PRECON_FP32) {
             if ((st = ensure(ctx, M->LD32, sizeof(float) * (size_t)P.ld_size))) return st;
             k_convert<double, float><<<grid_for(P.ld_size, 256, ctx->nsm * 8), 256, 0, ctx->stream>>>(P.ld_size, (const double*)M->LD.ptr, (float*)M->LD32.ptr);
         } else {
@@ -1446,6 +1447,18 @@ int chidg::precon_apply_impl(chidg_gpu_precon* M, const TV* v, TV* z, int precis
     int st;
     // blocks of more than 1024 rows: the streamed sweeps run as TASKS
     const int sched = (M->schedule == CHIDG_SCHED_STREAM && P.max_b > SS_MAX_B) ? CHIDG_SCHED_TASKS : M->schedule;
+    if (sizeof(TV) == 8 && precision == CHIDG_GPU_MIXED_PRECON_FP32) {
+        // FP64 vectors and accumulation, FP32 blocks (streamed or task sweeps)
+        int st = (sched == CHIDG_SCHED_STREAM)
+                     ? stream_sweeps(M, (const float*)M->LD32.ptr, (const float*)A->val32.ptr, v, zx, 3)
+                     : task_sweeps(M, (const float*)M->LD32.ptr, (const float*)A->val32.ptr, v, zx, 3);
+        if (st) return st;
+        if (zx != z) {
+            const cudaError_t e = cudaMemcpyAsync(z, zx, sizeof(TV) * (size_t)n, cudaMemcpyDeviceToDevice, ctx->stream);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "precon output copy");
+        }
+        return CHIDG_GPU_OK;
+    }
     if (sched == CHIDG_SCHED_STREAM) {
         int st;
         if (precision == CHIDG_GPU_MIXED_BF16 && sizeof(TV) == 4)

@@ -147,8 +147,8 @@ struct chidg_gpu_precon {
     chidg::Buffer part64, part32;          // task-split sweep partials (FP64 / low precision)
     unsigned epoch = 0;
     int sf_grid[3] = {0, 0, 0};            // resident CTAs of the dataflow sweep per vector type
-    int tk_grid[3] = {0, 0, 0};            // resident CTAs of the task-split sweep per vector type
-    int ss_grid[3][2] = {{0, 0}, {0, 0}, {0, 0}};  // resident CTAs of the streamed sweeps (forward, backward)
+    int tk_grid[4] = {0, 0, 0, 0};         // resident CTAs of the task-split sweep per variant
+    int ss_grid[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};  // resident CTAs of the streamed sweeps (forward, backward)
 };
 
 namespace chidg {

@@ -309,7 +309,7 @@ extern "C" int chidg_gpu_fgmres_solve(chidg_gpu_matrix* A, chidg_gpu_precon* M, 
     chidg_gpu_fgmres_opts o;
     if (opts) o = *opts;
     else chidg_gpu_fgmres_default_opts(&o);
-    if (o.precision < CHIDG_GPU_FP64 || o.precision > CHIDG_GPU_MIXED_BF16) return fail(ctx, CHIDG_GPU_EINVAL, "fgmres: bad precision");
+    if (o.precision < CHIDG_GPU_FP64 || o.precision > CHIDG_GPU_MIXED_PRECON_FP32) return fail(ctx, CHIDG_GPU_EINVAL, "fgmres: bad precision");
     set_matvec_smem(A);
     if (M->kind != CHIDG_PRECON_IDENTITY) precon_set_smem(M);
     ctx->err_elem = -1;
@@ -335,8 +335,8 @@ extern "C" int chidg_gpu_fgmres_solve(chidg_gpu_matrix* A, chidg_gpu_precon* M, 
     Buffer v32, z32;
     int64_t lo_iters = 0;
     int st;
-    if (prec == CHIDG_GPU_FP64) {
-        S.precon = [M](const double* v, double* z) { return precon_apply_impl<double>(M, v, z, CHIDG_GPU_FP64); };
+    if (prec == CHIDG_GPU_FP64 || prec == CHIDG_GPU_MIXED_PRECON_FP32) {
+        S.precon = [M, prec](const double* v, double* z) { return precon_apply_impl<double>(M, v, z, prec); };
     } else {
         // FP32 inner FGMRES as the flexible preconditioner of the FP64 outer loop
         S.inner = false;

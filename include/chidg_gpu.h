@@ -65,6 +65,9 @@ extern "C" {
 #define CHIDG_GPU_MIXED_FP32  1   /* FP64 outer FGMRES; FP32 inner FGMRES, matvec and
                                      ILU factors with FP32 accumulation                 */
 #define CHIDG_GPU_MIXED_BF16  2   /* as MIXED_FP32 but the ILU factors stored in BF16   */
+#define CHIDG_GPU_MIXED_PRECON_FP32 3  /* FP64 FGMRES (vectors, matvec, residuals); the ILU0
+                                     apply reads FP32 factors and an FP32 copy of the
+                                     U blocks, with FP64 vectors and accumulation      */
 
 #define CHIDG_ORTH_CGS 0
 #define CHIDG_ORTH_MGS 1
@@ -112,7 +115,7 @@ typedef struct {
                                          (solver_controller%update_preconditioner);
                                          0 = refresh on every call, as without a
                                          controller (type_fgmres.f90:118-122)   */
-    int32_t precision;                /* CHIDG_GPU_FP64 / _MIXED_FP32 / _MIXED_BF16 */
+    int32_t precision;                /* CHIDG_GPU_FP64 / _MIXED_FP32 / _MIXED_BF16 / _MIXED_PRECON_FP32 */
     int32_t mixed_inner_nkrylov;      /* mixed: Krylov length of the FP32 inner solve */
     double  mixed_inner_rtol;         /* mixed: relative tolerance of the inner solve */
     int32_t mixed_inner_nmax;         /* mixed: iteration cap of the inner solve      */
@@ -225,7 +228,8 @@ int chidg_gpu_precon_create(chidg_gpu_matrix* A, int32_t kind, chidg_gpu_precon*
 int chidg_gpu_precon_destroy(chidg_gpu_precon* M);                  /* %tear_down */
 /* %update(A,b): ILU0 factorisation (precon_ILU0.f90:111-265) or RAS
  * factorisation with overlap rows (precon_RASILU0.f90:205-415).  `precision`
- * selects the factor storage: CHIDG_GPU_FP64, _MIXED_FP32 or _MIXED_BF16. */
+ * selects the factor storage: CHIDG_GPU_FP64, _MIXED_FP32 or _MIXED_PRECON_FP32
+ * (FP32 copies), or _MIXED_BF16 (BF16 copies); the factorisation itself is FP64. */
 int chidg_gpu_precon_update(chidg_gpu_precon* M, chidg_gpu_matrix* A, int32_t precision);
 /* %apply(A,v) -> z: precon_ILU0.f90:286-411 / precon_RASILU0.f90:454-625. */
 int chidg_gpu_precon_apply(chidg_gpu_precon* M, chidg_gpu_matrix* A,

@@ -148,7 +148,7 @@ def test_stream_sweeps_deterministic():
     assert relerr(M.apply(Ag, v).download(), z1) < 1e-13
 
 
-@pytest.mark.parametrize("precision", ["mixed_fp32", "mixed_bf16"])
+@pytest.mark.parametrize("precision", ["mixed_fp32", "mixed_bf16", "mixed_precon_fp32"])
 def test_stream_sweeps_mixed_precision(precision):
     pat, vals, Ao, Ag = setup((4, 4, 4), 2, seed=28)
     b = mesh.synth_vector(Ao.n, seed=29)
@@ -197,6 +197,47 @@ def test_singular_block_reports_element_tensor_core_inverse():
     assert ei.value.code == _lib.ESINGULAR and ei.value.element == 7
 
 
+@pytest.mark.parametrize("schedule", ["stream", "tasks"])
+def test_precon_fp32_factors_close_to_fp64(schedule):
+    """FP64 vectors through FP32 factors: the apply differs from the FP64 one by
+    the rounding of the blocks (about 1e-7 relative), not more."""
+    pat, vals, Ao, Ag = setup((4, 3, 3), 2, seed=32)
+    v = api.ChidgVector(Ag, mesh.synth_vector(Ao.n, seed=33))
+    M = api.create_preconditioner("ilu0", schedule=schedule)
+    M.update(Ag)
+    z64 = M.apply(Ag, v).download()
+    M.update(Ag, precision="mixed_precon_fp32")
+    assert relerr(M.apply(Ag, v).download(), z64) < 1e-12     # the plain apply stays FP64
+    solver = api.create_linear_solver("fgmres", tol=0.0, rtol=1e-10, nkrylov=20, inner_fgmres=0, nmax=200,
+                                      precision="mixed_precon_fp32")
+    x = api.ChidgVector(Ag)
+    b = mesh.synth_vector(Ao.n, seed=34)
+    solver.solve(Ag, x, api.ChidgVector(Ag, b), M)
+    xo, ro = O.fgmres(Ao, O.OraclePrecon(Ao, "ilu0"), b, O.default_opts(tol=0.0, rtol=1e-10, nkrylov=20,
+                                                                        inner_fgmres=0, nmax=200))
+    assert relerr(x.download(), xo) < 1e-8
+    assert abs(solver.niter - ro["niter"]) <= 1
+
+
+def test_precon_fp32_mode_uses_fp32_blocks():
+    """After one FGMRES iteration the FP32-preconditioner iterate differs from
+    the FP64 one by the rounding of the blocks: visible, and small."""
+    pat, vals, Ao, Ag = setup((4, 3, 3), 2, seed=35)
+    b = api.ChidgVector(Ag, mesh.synth_vector(Ao.n, seed=36))
+    out = {}
+    for prec in ("fp64", "mixed_precon_fp32"):
+        solver = api.create_linear_solver("fgmres", tol=0.0, rtol=1e-14, nkrylov=1, inner_fgmres=0, nmax=1,
+                                          precision=prec)
+        x = api.ChidgVector(Ag)
+        try:
+            solver.solve(Ag, x, b, api.create_preconditioner("ilu0"))
+        except _lib.ChidgGpuError as e:
+            assert e.code == _lib.ENOTCONVERGED
+        out[prec] = x.download()
+    d = relerr(out["mixed_precon_fp32"], out["fp64"])
+    assert 1e-12 < d < 1e-5, d
+
+
 def test_fgmres_inner_default_options():
     """Reference defaults: inner FGMRES on, no controller (M refreshed per call)."""
     pat, vals, Ao, Ag = setup((3, 3, 2), 1, 1, seed=11)
@@ -238,7 +279,7 @@ def test_reference_kats_on_gpu(name):
             assert abs(xv[eo[e - 1] + i - 1] - expect) <= case["tol"]
 
 
-@pytest.mark.parametrize("precision", ["mixed_fp32", "mixed_bf16"])
+@pytest.mark.parametrize("precision", ["mixed_fp32", "mixed_bf16", "mixed_precon_fp32"])
 def test_mixed_precision_reaches_fp64_accuracy(precision):
     pat, vals, Ao, Ag = setup((4, 4, 4), 1, seed=13)
     b = mesh.synth_vector(Ao.n, seed=14)
