@@ -194,6 +194,8 @@ extern "C" int chidg_gpu_ctx_destroy(chidg_gpu_ctx* ctx) {
     release(ctx->partial2);
     for (Workspace* w : {&ctx->ws64, &ctx->ws32})
         for (Buffer* b : {&w->V, &w->Z, &w->x0, &w->zr, &w->dz, &w->tmp, &w->rowsq}) release(*b);
+    release(ctx->mix_v32);
+    release(ctx->mix_z32);
     if (ctx->d_status) cudaFree(ctx->d_status);
     if (ctx->d_scal) cudaFree(ctx->d_scal);
     if (ctx->h_scal) cudaFreeHost(ctx->h_scal);
@@ -493,15 +495,46 @@ int chidg::matrix_lowp(chidg_gpu_matrix* A, int precision) {
 }
 
 // y = alpha * A x + beta * z, optional per-row sums of squares of y
+// CHIDG_MATVEC_ROWS=1 selects the one-CTA-per-row matvec (comparison runs)
+static bool matvec_rows_env() {
+    static const bool v = [] {
+        const char* e = std::getenv("CHIDG_MATVEC_ROWS");
+        return e && e[0] == '1';
+    }();
+    return v;
+}
+
 template <typename TA, typename TV>
 int chidg::matvec_launch(chidg_gpu_matrix* A, const TA* val, const TV* x, TV* y, const TV* z, double alpha, double beta, double* row_sq) {
     chidg_gpu_ctx* ctx = A->ctx;
     using ACC = typename AccOf<TV>::type;
-    const size_t smem = sizeof(ACC) * ((size_t)A->max_row_cols + A->mv_threads) + 512;
     const int ph = prof_begin(ctx, sizeof(TA) == 8 ? kProfMatvec : kProfMatvec32);
-    k_matvec<TA, TV, TV, ACC><<<A->nrow, A->mv_threads, smem, ctx->stream>>>(
-        val, (const int64_t*)A->d_row_ptr.ptr, (const int64_t*)A->d_blk_voff.ptr, (const int64_t*)A->d_blk_xoff.ptr,
-        (const int32_t*)A->d_blk_nc.ptr, (const int64_t*)A->d_row_yoff.ptr, (const int32_t*)A->d_row_b.ptr, x, y, z, alpha, beta, row_sq);
+    if (A->max_b <= SS_MAX_B && !matvec_rows_env()) {
+        // streamed: persistent CTAs, row values prefetched by bulk copies
+        constexpr int CW = 8, NST = 2, SB = 24 * 1024;
+        const size_t smem = matvec_stream_smem(sizeof(ACC), NST, SB, A->max_row_cols, 32 * CW);
+        auto k = k_matvec_stream<TA, TV, ACC, CW>;
+        int st;
+        if ((st = raise_smem_limit((const void*)k, smem))) return fail(ctx, st, "streamed matvec shared memory");
+        int& grid = A->mvs_grid[sizeof(TA) == 8 ? 0 : sizeof(TA) == 4 ? 1 : 2];
+        if (grid == 0) {
+            int per_sm = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 32 * CW + 32, smem) != cudaSuccess || per_sm < 1) {
+                cudaGetLastError();
+                per_sm = 1;
+            }
+            grid = std::max(1, std::min(A->nrow, per_sm * ctx->nsm));
+        }
+        MatvecRows R{(const int64_t*)A->d_row_ptr.ptr, (const int64_t*)A->d_blk_voff.ptr, (const int64_t*)A->d_blk_xoff.ptr,
+                     (const int32_t*)A->d_blk_nc.ptr, (const int64_t*)A->d_row_yoff.ptr, (const int32_t*)A->d_row_b.ptr};
+        k<<<grid, 32 * CW + 32, smem, ctx->stream>>>(R, A->nrow, val, x, y, z, alpha, beta, row_sq,
+                                                     (int*)(ctx->d_scal + kSlotStatus), kSpinLimit, NST, SB, A->max_row_cols);
+    } else {
+        const size_t smem = sizeof(ACC) * ((size_t)A->max_row_cols + A->mv_threads) + 512;
+        k_matvec<TA, TV, TV, ACC><<<A->nrow, A->mv_threads, smem, ctx->stream>>>(
+            val, (const int64_t*)A->d_row_ptr.ptr, (const int64_t*)A->d_blk_voff.ptr, (const int64_t*)A->d_blk_xoff.ptr,
+            (const int32_t*)A->d_blk_nc.ptr, (const int64_t*)A->d_row_yoff.ptr, (const int32_t*)A->d_row_b.ptr, x, y, z, alpha, beta, row_sq);
+    }
     prof_end(ctx, ph);
     return check_launch(ctx, "k_matvec");
 }

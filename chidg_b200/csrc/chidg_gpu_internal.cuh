@@ -4,6 +4,7 @@
 #include "kernels.cuh"
 #include "stream_sweep.cuh"
 #include "inverse_tc.cuh"
+#include "stream_matvec.cuh"
 
 #include <array>
 #include <cmath>
@@ -100,6 +101,7 @@ struct chidg_gpu_ctx {
     double* h_scal = nullptr;
     chidg::Buffer partial, partial2;
     chidg::Workspace ws64, ws32;
+    chidg::Buffer mix_v32, mix_z32;   // mixed precision: FP32 copies of the outer loop's v and z
     bool profiling = false;
     std::vector<chidg::EvPair> prof_pending;
     std::vector<cudaEvent_t> prof_pool;
@@ -116,6 +118,7 @@ struct chidg_gpu_matrix {
     std::vector<std::vector<int32_t>> rowblk, lblk;
     std::vector<int32_t> diag;
     int max_row_cols = 0, max_b = 0, mv_threads = 32;
+    int mvs_grid[3] = {0, 0, 0};             // resident CTAs of the streamed matvec per value type
     chidg::Buffer val, val32, val16;
     int64_t val32_stamp = -1, val16_stamp = -1;
     chidg::Buffer d_row_ptr, d_blk_voff, d_blk_xoff, d_blk_nc, d_row_yoff, d_row_b, d_diag_voff, d_elem_nvars,

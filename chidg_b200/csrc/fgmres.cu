@@ -332,7 +332,8 @@ extern "C" int chidg_gpu_fgmres_solve(chidg_gpu_matrix* A, chidg_gpu_precon* M, 
     S.hist = &hv;
     S.precon_update = do_update;
     std::unique_ptr<Solver<float>> lo;
-    Buffer v32, z32;
+    Buffer& v32 = ctx->mix_v32;       // kept by the context: no allocation per solve
+    Buffer& z32 = ctx->mix_z32;
     int64_t lo_iters = 0;
     int st;
     if (prec == CHIDG_GPU_FP64 || prec == CHIDG_GPU_MIXED_PRECON_FP32) {
@@ -364,8 +365,6 @@ extern "C" int chidg_gpu_fgmres_solve(chidg_gpu_matrix* A, chidg_gpu_precon* M, 
         };
     }
     st = S.solve((const double*)b->buf.ptr, (double*)x->buf.ptr);
-    release(v32);
-    release(z32);
     if (st == CHIDG_GPU_OK) {
         const cudaError_t e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) st = cuda_fail(ctx, e, "fgmres");
