@@ -179,6 +179,9 @@ def uneven_systems(count, seed, max_n=8):
 
 
 def run_batch_leg(ctx, schedule, reps=3):
+    """The same systems solved one at a time (the plain FP64 path, and the
+    FP32 inner solve) and batched (FP64, and FP64 Krylov with FP32
+    preconditioner blocks); every mode to the same FP64 rtol 1e-8."""
     from chidg_b200 import api, mesh
     systems = uneven_systems(BATCH_SYSTEMS, seed=7)
     union, sys_elem = mesh.concat_patterns([s[0] for s in systems])
@@ -187,55 +190,86 @@ def run_batch_leg(ctx, schedule, reps=3):
     b = api.ChidgVector(A, np.concatenate([s[2] for s in systems]))
     x = api.ChidgVector(A)
     M = api.create_preconditioner("ilu0", schedule=schedule)
-    solver = api.create_linear_solver("fgmres", **BATCH_OPTS)
-    solver.solve_batched(A, x, b, M, sys_elem)              # warm-up
-    ctx.sync()
-    t0 = time.perf_counter()
-    for _ in range(reps):
-        res = solver.solve_batched(A, x, b, M, sys_elem)
-    ctx.sync()
-    t_batch = (time.perf_counter() - t0) / reps
-    # the first 12 systems one solve at a time
-    singles = []
-    for pat, vals, rhs in systems[:12]:
+    batched = {}
+    for prec in ("fp64", "mixed_precon_fp32"):
+        solver = api.create_linear_solver("fgmres", **BATCH_OPTS, precision=prec)
+        solver.solve_batched(A, x, b, M, sys_elem)              # warm-up
+        ctx.sync()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            res = solver.solve_batched(A, x, b, M, sys_elem)
+        ctx.sync()
+        t = (time.perf_counter() - t0) / reps
+        batched[prec] = {"solves_per_s": BATCH_SYSTEMS / t, "ms_per_batch": 1e3 * t,
+                         "iterations": [r["niter"] for r in res],
+                         "max_true_rel_residual": max(r["residual_norm"] / r["r0norm_initial"] for r in res)}
+    M.tear_down()
+    for o in (x, b, A):
+        o.release()
+    single = {"fp64": 0.0, "mixed_fp32": 0.0}
+    for pat, vals, rhs in systems:
         As = api.ChidgMatrix(pat, ctx)
         As.upload(vals)
         bs, xs = api.ChidgVector(As, rhs), api.ChidgVector(As)
         Ms = api.create_preconditioner("ilu0", schedule=schedule)
-        api.create_linear_solver("fgmres", **BATCH_OPTS).solve(As, xs, bs, Ms)   # warm-up
-        ctx.sync()
-        t0 = time.perf_counter()
-        api.create_linear_solver("fgmres", **BATCH_OPTS).solve(As, xs, bs, Ms)
-        ctx.sync()
-        singles.append(time.perf_counter() - t0)
+        for prec in single:
+            extra = dict(precision=prec, nkrylov=10, mixed_inner_nkrylov=30, mixed_inner_rtol=1e-2,
+                         mixed_inner_nmax=60) if prec == "mixed_fp32" else {}
+            opts = {**BATCH_OPTS, **extra}
+            api.create_linear_solver("fgmres", **opts).solve(As, xs, bs, Ms)   # warm-up
+            ctx.sync()
+            t0 = time.perf_counter()
+            api.create_linear_solver("fgmres", **opts).solve(As, xs, bs, Ms)
+            ctx.sync()
+            single[prec] += time.perf_counter() - t0
         Ms.tear_down()
         for o in (xs, bs, As):
             o.release()
-    M.tear_down()
-    for o in (x, b, A):
-        o.release()
+    plain = BATCH_SYSTEMS / single["fp64"]
     return {"systems": BATCH_SYSTEMS,
-            "workload": "boxes 4..8 per side, P in {1,2}, FGMRES(30)+ILU0 to rtol 1e-8, FP64",
-            "solves_per_s_batched": BATCH_SYSTEMS / t_batch, "ms_per_batch": 1e3 * t_batch,
-            "solves_per_s_one_at_a_time": len(singles) / sum(singles),
-            "iterations": [r["niter"] for r in res],
-            "max_true_rel_residual": max(r["residual_norm"] / r["r0norm_initial"] for r in res)}
+            "workload": "boxes 4..8 per side, P in {1,2}, FGMRES(30)+ILU0 to rtol 1e-8 (FP64 residual)",
+            "solves_per_s_one_at_a_time_fp64": plain,
+            "solves_per_s_one_at_a_time_mixed_fp32": BATCH_SYSTEMS / single["mixed_fp32"],
+            "solves_per_s_batched_fp64": batched["fp64"]["solves_per_s"],
+            "solves_per_s_batched_mixed_precon_fp32": batched["mixed_precon_fp32"]["solves_per_s"],
+            "speedup_vs_plain_fp64": {"batched_fp64": batched["fp64"]["solves_per_s"] / plain,
+                                      "batched_mixed_precon_fp32": batched["mixed_precon_fp32"]["solves_per_s"] / plain,
+                                      "one_at_a_time_mixed_fp32": BATCH_SYSTEMS / single["mixed_fp32"] / plain},
+            "batched": batched}
+
+
+def serve_requests(count, seed):
+    """Requests of the batch leg's sizes, every 10th a harmonic-balance one
+    (8^3 box, P1, 7 coupled time levels: 3 harmonics)."""
+    from chidg_b200 import mesh, serve
+    out = []
+    for i, (p, v, r) in enumerate(uneven_systems(count, seed=seed)):
+        if i % 10 == 9:
+            p = mesh.box_pattern(8, 8, 8, NVARS, mesh.nterms_of_order(1), ntime=7)
+            v = mesh.synth_values(p, seed=3000 + i)
+            r = mesh.synth_vector(p.vector_size(), seed=4000 + i)
+        out.append(serve.SolveRequest(p, v, r, tag=i))
+    return out
 
 
 def run_serve_leg(device, requests=64, rate=200.0):
     from chidg_b200 import serve
-    systems = uneven_systems(requests, seed=11)
-    reqs = [serve.SolveRequest(p, v, r, tag=i) for i, (p, v, r) in enumerate(systems)]
-    srv = serve.Server(device=device, slots=2, max_batch=16, mem_budget=40 << 30, **BATCH_OPTS)
-    try:
-        srv.submit(serve.SolveRequest(*systems[0])).result()     # warm-up
-        st = serve.run_stream(srv, reqs, serve.poisson_arrivals(requests, rate, seed=5))
-    finally:
-        srv.close()
-    st.pop("results")
-    st.update({"arrival_rate_per_s": rate, "workload": "Poisson arrivals, boxes 4..8 per side, P in {1,2}, FP64",
-               "slots": 2, "max_batch": 16})
-    return st
+    out = {"arrival_rate_per_s": rate, "requests": requests, "slots": 2, "max_batch": 16,
+           "workload": "Poisson arrivals; boxes 4..8 per side, P in {1,2}; every 10th request harmonic balance "
+                       "(8^3, P1, 7 time levels); FGMRES(30)+ILU0 to rtol 1e-8 (FP64 residual)"}
+    for prec in ("fp64", "mixed_precon_fp32"):
+        reqs = serve_requests(requests, seed=11)
+        srv = serve.Server(device=device, slots=2, max_batch=16, mem_budget=40 << 30, **BATCH_OPTS, precision=prec)
+        try:
+            srv.submit(serve_requests(1, seed=11)[0]).result()    # warm-up
+            st = serve.run_stream(srv, reqs, serve.poisson_arrivals(requests, rate, seed=5))
+        finally:
+            srv.close()
+        res = st.pop("results")
+        st["max_true_rel_residual"] = max(r.residual_norm / r.r0norm_initial for r in res)
+        st.pop("requests", None)
+        out[prec] = st
+    return out
 
 
 # ---------------------------------------------------------------------------

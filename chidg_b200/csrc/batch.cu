@@ -22,11 +22,15 @@ namespace {
 
 constexpr int64_t kChunk = 2048;
 
+// the segment layout of one batched call; its device buffers belong to the
+// context and are reused by the next call
 struct Seg {
     int nsys = 0, nchunk = 0;
-    Buffer cstart, csys, sys_chunk, sys_row, d_out, d_coef, d_scale, partial, rowsq;
+    Buffer &cstart, &csys, &sys_chunk, &sys_row, &d_out, &d_coef, &d_scale, &partial, &rowsq;
     std::vector<int32_t> h_sys_chunk;
-    ~Seg() { for (Buffer* b : {&cstart, &csys, &sys_chunk, &sys_row, &d_out, &d_coef, &d_scale, &partial, &rowsq}) release(*b); }
+    explicit Seg(BatchBuffers& b)
+        : cstart(b.cstart), csys(b.csys), sys_chunk(b.sys_chunk), sys_row(b.sys_row), d_out(b.d_out), d_coef(b.d_coef),
+          d_scale(b.d_scale), partial(b.partial), rowsq(b.rowsq) {}
 };
 
 template <typename T>
@@ -102,7 +106,11 @@ extern "C" int chidg_gpu_fgmres_solve_batched(chidg_gpu_matrix* A, chidg_gpu_pre
     if (opts) o = *opts;
     else chidg_gpu_fgmres_default_opts(&o);
     if (o.inner_fgmres) return fail(ctx, CHIDG_GPU_EINVAL, "batched fgmres: inner FGMRES is not supported");
-    if (o.precision != CHIDG_GPU_FP64) return fail(ctx, CHIDG_GPU_EINVAL, "batched fgmres: FP64 only");
+    // FP64 Krylov vectors in every batched mode; MIXED_PRECON_FP32 applies the
+    // preconditioner with FP32 copies of its blocks
+    if (o.precision != CHIDG_GPU_FP64 && o.precision != CHIDG_GPU_MIXED_PRECON_FP32)
+        return fail(ctx, CHIDG_GPU_EINVAL, "batched fgmres: precision must be FP64 or MIXED_PRECON_FP32");
+    const int prec = o.precision;
     const int m = o.nkrylov;
     if (m < 1 || m > kMaxKrylov) return fail(ctx, CHIDG_GPU_EINVAL, "batched fgmres: nkrylov outside [1, 4000]");
     // segments: systems must tile the elements and not couple to each other
@@ -114,7 +122,7 @@ extern "C" int chidg_gpu_fgmres_solve_batched(chidg_gpu_matrix* A, chidg_gpu_pre
     }
     for (int64_t k = 0; k < A->nblk; ++k)
         if (elem_sys[A->re[k]] != elem_sys[A->ce[k]]) return fail(ctx, CHIDG_GPU_EINVAL, "batched fgmres: a block couples two systems");
-    Seg G;
+    Seg G(ctx->batch);
     G.nsys = nsys;
     std::vector<int64_t> cstart;
     std::vector<int32_t> csys, sys_chunk(nsys + 1), sys_row(nsys + 1);
@@ -151,15 +159,20 @@ extern "C" int chidg_gpu_fgmres_solve_batched(chidg_gpu_matrix* A, chidg_gpu_pre
     double* ROWSQ = (double*)G.rowsq.ptr;
 
     // M%update as the controller decides (type_fgmres.f90:118-122)
-    if (!(o.use_controller && M->stamp == A->stamp && M->precision == CHIDG_GPU_FP64))
-        if ((st = chidg_gpu_precon_update(M, A, CHIDG_GPU_FP64))) return st;
+    if (!(o.use_controller && M->stamp == A->stamp && M->precision == prec))
+        if ((st = chidg_gpu_precon_update(M, A, prec))) return st;
     set_matvec_smem(A);
     if (M->kind != CHIDG_PRECON_IDENTITY) precon_set_smem(M);
     cudaMemsetAsync(ctx->d_scal + kSlotStatus, 0, sizeof(double), ctx->stream);
 
     const int64_t n = A->n;
-    Buffer V, Z, X0, TMP;
-    auto cleanup = [&]() { for (Buffer* bb : {&V, &Z, &X0, &TMP}) release(*bb); };
+    // the Krylov basis and work vectors of the context's FP64 workspace (a
+    // context runs one solve at a time)
+    Buffer& V = ctx->ws64.V;
+    Buffer& Z = ctx->ws64.Z;
+    Buffer& X0 = ctx->ws64.x0;
+    Buffer& TMP = ctx->ws64.tmp;
+    auto cleanup = [&]() {};
     if ((st = ensure(ctx, V, sizeof(double) * (size_t)(m + 1) * n)) || (st = ensure(ctx, Z, sizeof(double) * (size_t)(m + 1) * n)) ||
         (st = ensure(ctx, X0, sizeof(double) * (size_t)n)) || (st = ensure(ctx, TMP, sizeof(double) * (size_t)n))) {
         cleanup();
@@ -246,7 +259,7 @@ extern "C" int chidg_gpu_fgmres_solve_batched(chidg_gpu_matrix* A, chidg_gpu_pre
             double* vj = Vb + (int64_t)(j - 1) * n;
             double* zj = Zb + (int64_t)(j - 1) * n;
             double* w = Vb + (int64_t)j * n;
-            if ((st = precon_apply_impl<double>(M, vj, zj, CHIDG_GPU_FP64))) { cleanup(); return st; }
+            if ((st = precon_apply_impl<double>(M, vj, zj, prec))) { cleanup(); return st; }
             if ((st = matvec_launch<double, double>(A, (const double*)A->val.ptr, zj, w, nullptr, 1.0, 0.0, ROWSQ)) ||
                 (st = rows_to_sys(OUT + (size_t)nsys * 0))) { cleanup(); return st; }
             std::vector<double> norm_before(nsys);

@@ -196,6 +196,9 @@ extern "C" int chidg_gpu_ctx_destroy(chidg_gpu_ctx* ctx) {
         for (Buffer* b : {&w->V, &w->Z, &w->x0, &w->zr, &w->dz, &w->tmp, &w->rowsq}) release(*b);
     release(ctx->mix_v32);
     release(ctx->mix_z32);
+    for (Buffer* b : {&ctx->batch.cstart, &ctx->batch.csys, &ctx->batch.sys_chunk, &ctx->batch.sys_row, &ctx->batch.d_out,
+                      &ctx->batch.d_coef, &ctx->batch.d_scale, &ctx->batch.partial, &ctx->batch.rowsq})
+        release(*b);
     if (ctx->d_status) cudaFree(ctx->d_status);
     if (ctx->d_scal) cudaFree(ctx->d_scal);
     if (ctx->h_scal) cudaFreeHost(ctx->h_scal);

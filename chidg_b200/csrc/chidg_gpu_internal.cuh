@@ -85,6 +85,11 @@ namespace chidg {
 struct Workspace {
     Buffer V, Z, x0, zr, dz, tmp, rowsq;
 };
+// device buffers of the batched solver's per-system segments, kept by the
+// context (they only grow) so that a batched solve allocates nothing
+struct BatchBuffers {
+    Buffer cstart, csys, sys_chunk, sys_row, d_out, d_coef, d_scale, partial, rowsq;
+};
 }  // namespace chidg
 
 struct chidg_gpu_ctx {
@@ -102,6 +107,7 @@ struct chidg_gpu_ctx {
     chidg::Buffer partial, partial2;
     chidg::Workspace ws64, ws32;
     chidg::Buffer mix_v32, mix_z32;   // mixed precision: FP32 copies of the outer loop's v and z
+    chidg::BatchBuffers batch;
     bool profiling = false;
     std::vector<chidg::EvPair> prof_pending;
     std::vector<cudaEvent_t> prof_pool;
