@@ -67,6 +67,7 @@ PROTOTYPES = {
     "chidg_gpu_matrix_nvalues": (C.c_int, [VP, I64P]),
     "chidg_gpu_matrix_nvec": (C.c_int, [VP, I64P]),
     "chidg_gpu_matrix_upload": (C.c_int, [VP, VP]),
+    "chidg_gpu_matrix_upload_range": (C.c_int, [VP, VP, C.c_int64, C.c_int64]),
     "chidg_gpu_matrix_upload_blocks": (C.c_int, [VP, C.POINTER(VP)]),
     "chidg_gpu_matrix_upload_device": (C.c_int, [VP, VP]),
     "chidg_gpu_matrix_download": (C.c_int, [VP, VP]),
@@ -76,6 +77,7 @@ PROTOTYPES = {
     "chidg_gpu_vector_create": (C.c_int, [VP, C.POINTER(VP)]),
     "chidg_gpu_vector_destroy": (C.c_int, [VP]),
     "chidg_gpu_vector_upload": (C.c_int, [VP, VP]),
+    "chidg_gpu_vector_upload_range": (C.c_int, [VP, VP, C.c_int64, C.c_int64]),
     "chidg_gpu_vector_download": (C.c_int, [VP, VP]),
     "chidg_gpu_vector_upload_device": (C.c_int, [VP, VP]),
     "chidg_gpu_vector_device_ptr": (C.c_int, [VP, C.POINTER(VP)]),

@@ -117,6 +117,18 @@ class ChidgMatrix:
         self.ctx.check(self.ctx.L.chidg_gpu_matrix_upload(self.h, _ptr(values)), "matrix_upload")
         self.ctx.sync()
 
+    def upload_parts(self, parts):
+        """Consecutive pieces of the packed values (e.g. one per system of a
+        batch), uploaded in place without first joining them on the host."""
+        parts = [np.ascontiguousarray(p, dtype=np.float64) for p in parts]
+        if sum(p.size for p in parts) != self.nvalues:
+            raise ValueError(f"expected {self.nvalues} values in total")
+        first = 0
+        for p in parts:
+            self.ctx.check(self.ctx.L.chidg_gpu_matrix_upload_range(self.h, _ptr(p), first, p.size), "matrix_upload_range")
+            first += p.size
+        self.ctx.sync()
+
     def upload_blocks(self, blocks):
         """One array per block (each densematrix_t%mat), in pattern order."""
         arrs = [np.asfortranarray(b, dtype=np.float64) for b in blocks]
@@ -177,6 +189,17 @@ class ChidgVector:
         if values.size != self.n:
             raise ValueError("vector size mismatch")
         self.ctx.check(self.ctx.L.chidg_gpu_vector_upload(self.h, _ptr(values)), "vector_upload")
+        self.ctx.sync()
+
+    def upload_parts(self, parts):
+        """Consecutive pieces of the vector, uploaded in place."""
+        parts = [np.ascontiguousarray(p, dtype=np.float64) for p in parts]
+        if sum(p.size for p in parts) != self.n:
+            raise ValueError("vector size mismatch")
+        first = 0
+        for p in parts:
+            self.ctx.check(self.ctx.L.chidg_gpu_vector_upload_range(self.h, _ptr(p), first, p.size), "vector_upload_range")
+            first += p.size
         self.ctx.sync()
 
     def download(self) -> np.ndarray:

@@ -151,8 +151,9 @@ class Server:
             pats = [r.pattern for r, _ in batch]
             union, sys_elem = mesh.concat_patterns(pats)
             A = api.ChidgMatrix(union, ctx)
-            A.upload(np.concatenate([r.values for r, _ in batch]))
-            b = api.ChidgVector(A, np.concatenate([r.rhs for r, _ in batch]))
+            A.upload_parts([r.values for r, _ in batch])      # each request in place, no host copy
+            b = api.ChidgVector(A)
+            b.upload_parts([r.rhs for r, _ in batch])
             x = api.ChidgVector(A)
             M = api.create_preconditioner(self.precon)
             solver = api.create_linear_solver("fgmres", **self.options)

@@ -175,6 +175,10 @@ int chidg_gpu_matrix_upload(chidg_gpu_matrix* A, const double* host);
 int chidg_gpu_matrix_upload_blocks(chidg_gpu_matrix* A, const double* const* block_ptrs);
 /* Same, from a packed device array already resident on this GPU. */
 int chidg_gpu_matrix_upload_device(chidg_gpu_matrix* A, const double* dev);
+/* Part of the packed values: host[0..count) into values first..first+count-1
+ * (no counterpart in the reference: a caller that packs several systems into
+ * one matrix uploads each from its own array).  Bumps the stamp. */
+int chidg_gpu_matrix_upload_range(chidg_gpu_matrix* A, const double* host, int64_t first, int64_t count);
 /* Download the packed blocks into host memory. */
 int chidg_gpu_matrix_download(chidg_gpu_matrix* A, double* host);
 /* chidg_matrix%clear (:841): zero all blocks, bump the stamp. */
@@ -191,6 +195,9 @@ int chidg_gpu_matrix_stamp(chidg_gpu_matrix* A, int64_t* stamp);
 int chidg_gpu_vector_create(chidg_gpu_matrix* A, chidg_gpu_vector** out);
 int chidg_gpu_vector_destroy(chidg_gpu_vector* x);
 int chidg_gpu_vector_upload(chidg_gpu_vector* x, const double* host);
+/* host[0..count) into entries first..first+count-1 (no counterpart in the
+ * reference; see chidg_gpu_matrix_upload_range). */
+int chidg_gpu_vector_upload_range(chidg_gpu_vector* x, const double* host, int64_t first, int64_t count);
 int chidg_gpu_vector_download(chidg_gpu_vector* x, double* host);
 /* Attach/read device memory directly (n doubles on this GPU). */
 int chidg_gpu_vector_upload_device(chidg_gpu_vector* x, const double* dev);

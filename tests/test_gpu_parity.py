@@ -238,6 +238,22 @@ def test_precon_fp32_mode_uses_fp32_blocks():
     assert 1e-12 < d < 1e-5, d
 
 
+def test_upload_in_parts_matches_whole_upload():
+    pat, vals, Ao, Ag = setup((3, 2, 2), 1, seed=37)
+    whole = Ag.download()
+    A2 = api.ChidgMatrix(pat)
+    cut = [0, 5, len(vals) // 3, len(vals) // 3 + 1, len(vals)]
+    A2.upload_parts([vals[a:b] for a, b in zip(cut[:-1], cut[1:])])
+    assert np.array_equal(A2.download(), whole)
+    v = mesh.synth_vector(Ao.n, seed=38)
+    x = api.ChidgVector(A2)
+    x.upload_parts([v[:7], v[7:]])
+    assert np.array_equal(x.download(), v)
+    with pytest.raises(_lib.ChidgGpuError) as ei:
+        Ag.ctx.check(Ag.ctx.L.chidg_gpu_matrix_upload_range(A2.h, vals.ctypes.data, len(vals) - 3, 4), "range")
+    assert ei.value.code == _lib.EINVAL
+
+
 def test_fgmres_inner_default_options():
     """Reference defaults: inner FGMRES on, no controller (M refreshed per call)."""
     pat, vals, Ao, Ag = setup((3, 3, 2), 1, 1, seed=11)
