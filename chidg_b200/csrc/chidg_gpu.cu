@@ -1205,6 +1205,67 @@ static int launch_inverse(chidg_gpu_precon* M, int row_begin, int count, int cls
     return check_launch(ctx, "k_block_inverse");
 }
 
+// precon%update for the mixed-precision inner solves (MIXED_FP32, MIXED_BF16):
+// the L and S products in FP32 (SIMT, from the FP32 copy of A), the diagonal
+// inverses in FP64 (the products' D blocks are written in FP64, inverted by the
+// tensor-core kernel and copied to FP32 per wavefront).  Only the FP32 (and
+// BF16) factors are produced; LD's FP64 L blocks are not.
+static int factor_fp32(chidg_gpu_precon* M, chidg_gpu_matrix* A, int precision) {
+    chidg_gpu_ctx* ctx = M->ctx;
+    IluProgram& P = M->P;
+    int st;
+    if ((st = matrix_lowp(A, CHIDG_GPU_MIXED_FP32))) return st;
+    if (precision == CHIDG_GPU_MIXED_BF16 && (st = matrix_lowp(A, CHIDG_GPU_MIXED_BF16))) return st;
+    if ((st = ensure(ctx, M->LD, sizeof(double) * (size_t)P.ld_size)) ||
+        (st = ensure(ctx, M->LD32, sizeof(float) * (size_t)P.ld_size)))
+        return st;
+    if ((st = raise_smem_limit((const void*)k_task_gemm_f32<float>, SF_SMEM)) ||
+        (st = raise_smem_limit((const void*)k_task_gemm_f32<double>, SF_SMEM)))
+        return fail(ctx, st, "FP32 factor GEMM shared memory");
+    const int nlev = (int)P.fwd_ptr.size() - 1;
+    const float* A32 = (const float*)A->val32.ptr;
+    float* L32 = (float*)M->LD32.ptr;
+    double* LD = (double*)M->LD.ptr;
+    const int ph = prof_begin(ctx, kProfFactor);
+    for (int l = 0; l < nlev; ++l) {
+        const int pg = prof_begin(ctx, kProfFactorGemm);
+        const int nl = P.ltask_ptr[l + 1] - P.ltask_ptr[l];
+        if (nl > 0) {
+            k_task_gemm_f32<float><<<nl, 256, SF_SMEM, ctx->stream>>>((const GemmTask*)P.d_ltasks.ptr + P.ltask_ptr[l],
+                                                                     (const GemmPair*)P.d_lpairs.ptr, A32, L32, nullptr,
+                                                                     L32, 1.0);
+            if ((st = check_launch(ctx, "k_task_gemm_f32 L"))) return st;
+        }
+        const int ns = P.stask_ptr[l + 1] - P.stask_ptr[l];
+        if (ns > 0) {
+            k_task_gemm_f32<double><<<ns, 256, SF_SMEM, ctx->stream>>>((const GemmTask*)P.d_stasks.ptr + P.stask_ptr[l],
+                                                                      (const GemmPair*)P.d_spairs.ptr, L32, A32,
+                                                                      (const double*)A->val.ptr, LD, -1.0);
+            if ((st = check_launch(ctx, "k_task_gemm_f32 S"))) return st;
+        }
+        prof_end(ctx, pg);
+        const int pi = prof_begin(ctx, kProfFactorInv);
+        for (int q = P.inv_seg_ptr[l]; q < P.inv_seg_ptr[l + 1]; ++q)
+            if ((st = launch_inverse(M, P.inv_seg[q][0], P.inv_seg[q][1], P.inv_seg[q][2]))) return st;
+        const int cnt = P.fwd_ptr[l + 1] - P.fwd_ptr[l];
+        if (cnt > 0) {
+            k_convert_dinv<<<cnt, 256, 0, ctx->stream>>>(LD, L32, (const int64_t*)P.d_dinv_off.ptr,
+                                                         (const int32_t*)P.d_prow_b.ptr, (const int32_t*)P.d_fwd_rows.ptr,
+                                                         P.fwd_ptr[l]);
+            if ((st = check_launch(ctx, "k_convert_dinv"))) return st;
+        }
+        prof_end(ctx, pi);
+    }
+    prof_end(ctx, ph);
+    if (precision == CHIDG_GPU_MIXED_BF16) {
+        if ((st = ensure(ctx, M->LD16, sizeof(__nv_bfloat16) * (size_t)P.ld_size))) return st;
+        k_convert<float, __nv_bfloat16><<<grid_for(P.ld_size, 256, ctx->nsm * 8), 256, 0, ctx->stream>>>(
+            P.ld_size, (const float*)M->LD32.ptr, (__nv_bfloat16*)M->LD16.ptr);
+        if ((st = check_launch(ctx, "k_convert LD32->LD16"))) return st;
+    }
+    return CHIDG_GPU_OK;
+}
+
 // precon%update: FP64 factorisation level by level, then the low-precision
 // copies of the factors when requested.
 extern "C" int chidg_gpu_precon_update(chidg_gpu_precon* M, chidg_gpu_matrix* A, int32_t precision) {
@@ -1223,6 +1284,21 @@ extern "C" int chidg_gpu_precon_update(chidg_gpu_precon* M, chidg_gpu_matrix* A,
     // error would otherwise leave them out of step)
     if (M->sync.ptr)
         cudaMemsetAsync((unsigned*)M->sync.ptr + 2 + P.nprow, 0, sizeof(unsigned) * 3 * (size_t)P.nprow, ctx->stream);
+    if ((precision == CHIDG_GPU_MIXED_FP32 || precision == CHIDG_GPU_MIXED_BF16) && P.max_b <= SF_MAX) {
+        // the inner solves only read FP32 / BF16 factors: compute them in FP32
+        if ((st = factor_fp32(M, A, precision))) return st;
+        cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+        const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "precon update");
+        if (ctx->h_status[0] != INT_MAX) {
+            ctx->err_elem = ctx->h_status[0];
+            return fail(ctx, CHIDG_GPU_ESINGULAR, "inv: Matrix is numerically singular! (element " + std::to_string(ctx->h_status[0]) + ")");
+        }
+        M->ld64_valid = false;
+        M->precision = precision;
+        M->stamp = A->stamp;
+        return CHIDG_GPU_OK;
+    }
     const int nlev = (int)P.fwd_ptr.size() - 1;
     const int tiles_1d = (P.max_b + GT_M - 1) / GT_M;
     // one CTA per output block on the FP64 tensor cores for blocks up to 136 x 136
@@ -1281,6 +1357,7 @@ extern "C" int chidg_gpu_precon_update(chidg_gpu_precon* M, chidg_gpu_matrix* A,
         }
         if ((st = check_launch(ctx, "k_convert LD"))) return st;
     }
+    M->ld64_valid = true;
     M->precision = precision;
     M->stamp = A->stamp;
     return CHIDG_GPU_OK;
@@ -1603,6 +1680,8 @@ extern "C" int chidg_gpu_precon_apply(chidg_gpu_precon* M, chidg_gpu_matrix* A, 
     if (!M || !A || !v || !z || A != M->A || v->n != A->n || z->n != A->n || v == z) return CHIDG_GPU_EINVAL;
     cudaSetDevice(M->ctx->device);
     if (M->kind != CHIDG_PRECON_IDENTITY && M->stamp == 0) return fail(M->ctx, CHIDG_GPU_ESTATE, "precon_apply: preconditioner not updated");
+    if (M->kind != CHIDG_PRECON_IDENTITY && !M->ld64_valid)
+        return fail(M->ctx, CHIDG_GPU_ESTATE, "precon_apply: the factors were computed in FP32 (mixed precision); update in FP64 first");
     precon_set_smem(M);
     chidg_gpu_ctx* ctx = M->ctx;
     cudaMemsetAsync(ctx->d_scal + kSlotStatus, 0, sizeof(double), ctx->stream);
@@ -1619,6 +1698,7 @@ extern "C" int chidg_gpu_precon_download_LD(chidg_gpu_precon* M, double* host) {
     cudaSetDevice(ctx->device);
     chidg_gpu_matrix* A = M->A;
     if (M->kind == CHIDG_PRECON_IDENTITY || M->stamp == 0) return fail(ctx, CHIDG_GPU_ESTATE, "download_LD: no factors");
+    if (!M->ld64_valid) return fail(ctx, CHIDG_GPU_ESTATE, "download_LD: the factors were computed in FP32 (mixed precision)");
     std::vector<double> ld((size_t)M->P.ld_size);
     cudaError_t e = cudaMemcpyAsync(ld.data(), M->LD.ptr, sizeof(double) * ld.size(), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);

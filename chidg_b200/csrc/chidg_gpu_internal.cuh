@@ -149,6 +149,7 @@ struct chidg_gpu_precon {
     int kind = 0;
     int precision = 0;
     int64_t stamp = 0;
+    bool ld64_valid = false;               // LD holds the FP64 factors (false after an FP32 factorisation)
     chidg::IluProgram P;
     chidg::Buffer LD, LD32, LD16, zx, zx32, piv_scratch;
     int schedule = CHIDG_SCHED_STREAM;     // sweep schedule (TASKS for blocks over 1024 rows)

@@ -501,6 +501,107 @@ __global__ void __launch_bounds__(DM_THREADS, 1) k_task_gemm_dmma(const GemmTask
     }
 }
 
+// FP32 SIMT version of the factor products for blocks up to 144 x 144, used
+// when the factors are only needed in FP32 (the mixed-precision inner solves):
+// one CTA per output block, 256 threads on a 16 x 16 grid, thread (tx, ty)
+// accumulating rows ty + 16i and columns tx + 16j (i, j < 9) in FP32.  K is
+// staged 32 at a time (cp.async, zero-filled outside the operands, two
+// stages).  A (m x k) and B (k x n) column-major FP32; the output is TC
+// (FP32 L blocks, or FP64 D blocks for the FP64 diagonal inverse), with an
+// optional FP64 Cinit.
+constexpr int SF_MAX = 144, SF_KC = 32, SF_LDA = 144, SF_LDB = 145;
+constexpr size_t SF_SMEM = 2 * sizeof(float) * SF_KC * (SF_LDA + SF_LDB);
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem, bool src_ok) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const int n = src_ok ? 4 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" :: "r"(s), "l"(gmem), "r"(n) : "memory");
+}
+template <typename TC>
+__global__ void __launch_bounds__(256, 1) k_task_gemm_f32(const GemmTask* __restrict__ tasks, const GemmPair* __restrict__ pairs,
+                                                          const float* Abase, const float* Bbase, const double* Cinit,
+                                                          TC* Cbase, double sgn) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float* As = reinterpret_cast<float*>(smem_raw);        // 2 stages x {A [SF_KC][SF_LDA], B [SF_KC][SF_LDB]}
+    const GemmTask t = tasks[blockIdx.x];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float acc[9][9];
+    #pragma unroll
+    for (int i = 0; i < 9; ++i)
+        #pragma unroll
+        for (int j = 0; j < 9; ++j) acc[i][j] = 0.0f;
+    int nchunk = 0;
+    for (int q = t.q_begin; q < t.q_end; ++q) nchunk += (pairs[q].k + SF_KC - 1) / SF_KC;
+    int lq = t.q_begin, lk0 = 0;
+    auto issue = [&](int stage) {
+        const GemmPair pr = pairs[lq];
+        const float* A = Abase + pr.a_off;        // m x k
+        const float* B = Bbase + pr.b_off;        // k x n
+        const int kc = min(SF_KC, pr.k - lk0);
+        float* as = As + stage * SF_KC * (SF_LDA + SF_LDB);
+        float* bs = as + SF_KC * SF_LDA;
+        for (int kk = warp; kk < SF_KC; kk += 8)              // A: coalesced along the rows
+            for (int i = lane; i < SF_MAX; i += 32) {
+                const bool ok = i < t.m && kk < kc;
+                cp_async4(as + kk * SF_LDA + i, ok ? (const void*)(A + i + (int64_t)(lk0 + kk) * t.m) : (const void*)A, ok);
+            }
+        for (int j = warp; j < SF_MAX; j += 8) {               // B: coalesced along k
+            const bool ok = j < t.n && lane < kc;
+            cp_async4(bs + lane * SF_LDB + j, ok ? (const void*)(B + (lk0 + lane) + (int64_t)j * pr.k) : (const void*)B, ok);
+        }
+        cp_async_commit();
+        lk0 += SF_KC;
+        if (lk0 >= pr.k) { ++lq; lk0 = 0; }
+    };
+    if (nchunk > 0) issue(0);
+    for (int c = 0; c < nchunk; ++c) {
+        if (c + 1 < nchunk) { issue((c + 1) & 1); cp_async_wait<1>(); }
+        else cp_async_wait<0>();
+        __syncthreads();
+        const float* as = As + (c & 1) * SF_KC * (SF_LDA + SF_LDB);
+        const float* bs = as + SF_KC * SF_LDA;
+        #pragma unroll 4
+        for (int kk = 0; kk < SF_KC; ++kk) {          // a short last chunk is zero-filled
+            float a[9], b[9];
+            #pragma unroll
+            for (int i = 0; i < 9; ++i) a[i] = as[kk * SF_LDA + ty + 16 * i];
+            #pragma unroll
+            for (int j = 0; j < 9; ++j) b[j] = bs[kk * SF_LDB + tx + 16 * j];
+            #pragma unroll
+            for (int i = 0; i < 9; ++i)
+                #pragma unroll
+                for (int j = 0; j < 9; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+        }
+        __syncthreads();                          // stage (c & 1) is refilled two chunks later
+    }
+    #pragma unroll
+    for (int j = 0; j < 9; ++j) {
+        const int col = tx + 16 * j;
+        if (col >= t.n) continue;
+        #pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            const int row = ty + 16 * i;
+            if (row >= t.m) continue;
+            const int64_t o = row + (int64_t)col * t.m;
+            double v = sgn * (double)acc[i][j];
+            if (t.cinit_off >= 0) v = Cinit[t.cinit_off + o] + v;
+            Cbase[t.c_off + o] = from_d<TC>(v);
+        }
+    }
+}
+
+// FP32 copies of the inverted diagonal blocks of some programme rows (one CTA
+// per row): the inverses of a wavefront, for the next wavefront's FP32 products
+// and the FP32 sweeps
+static __global__ void k_convert_dinv(const double* __restrict__ LD, float* __restrict__ LD32,
+                                      const int64_t* __restrict__ dinv_off, const int32_t* __restrict__ prow_b,
+                                      const int32_t* __restrict__ rows, int row_begin) {
+    const int pr = rows[row_begin + blockIdx.x];
+    const int64_t o = dinv_off[pr];
+    const int n = prow_b[pr] * prow_b[pr];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) LD32[o + i] = (float)LD[o + i];
+}
+
 // In-place inverse of one diagonal block per CTA: Gauss-Jordan with partial
 // (row) pivoting, restated from the textbook algorithm.  The pivot of column
 // k is the entry of largest magnitude among rows not yet used as pivots

@@ -254,6 +254,22 @@ def test_upload_in_parts_matches_whole_upload():
     assert ei.value.code == _lib.EINVAL
 
 
+def test_fp32_factorisation_guards_the_fp64_apply():
+    """MIXED_FP32 computes only FP32 factors: the FP64 apply and the factor
+    download refuse until the next FP64 update, which then matches the oracle."""
+    pat, vals, Ao, Ag = setup((3, 3, 2), 2, seed=39)
+    M = api.create_preconditioner("ilu0")
+    M.update(Ag, precision="mixed_fp32")
+    v = api.ChidgVector(Ag, mesh.synth_vector(Ao.n, seed=40))
+    with pytest.raises(_lib.ChidgGpuError) as ei:
+        M.apply(Ag, v)
+    assert ei.value.code == _lib.ESTATE
+    M.update(Ag)
+    Mo = O.OraclePrecon(Ao, "ilu0")
+    Mo.update()
+    assert relerr(M.apply(Ag, v).download(), Mo.apply(v.download())) < 1e-11
+
+
 def test_fgmres_inner_default_options():
     """Reference defaults: inner FGMRES on, no controller (M refreshed per call)."""
     pat, vals, Ao, Ag = setup((3, 3, 2), 1, 1, seed=11)
