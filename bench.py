@@ -275,6 +275,77 @@ def run_serve_leg(device, requests=64, rate=200.0):
 # ---------------------------------------------------------------------------
 # CPU legs (oracle)
 # ---------------------------------------------------------------------------
+CFG3 = (32, 32, 32)
+CFG3_SUB = (4, 4, 4)
+CFG3_SOLVER = dict(tol=0.0, rtol=1e-8, nkrylov=30, inner_fgmres=0, nmax=600, orthogonalization="CGS",
+                   use_controller=0)
+
+
+def run_cfg3_leg(ctx, stream, schedule, reps=2):
+    """32^3 P2 (223 232 blocks of 135 x 135, 32.5 GB FP64): FGMRES(30) to rtol
+    1e-8 with block-ILU0 in FP64, with FP32 factors and FP32 Krylov, with BF16
+    factors and FP32 Krylov, and RAS+ILU0 over 4 x 4 x 4 box subdomains of 8^3
+    elements (each subdomain plays one MPI rank) in FP64 and with FP32 inner
+    solves.  Every mode reaches the same FP64 true residual."""
+    import torch
+
+    from chidg_b200 import api, mesh
+    pat = mesh.box_pattern(*CFG3, NVARS, mesh.nterms_of_order(P), subdomains=CFG3_SUB)
+    A = api.ChidgMatrix(pat, ctx)
+    t0 = time.perf_counter()
+    vals = mesh.synth_values(pat, seed=SEED_A + 3)
+    A.upload(vals)
+    del vals
+    b = api.ChidgVector(A, mesh.synth_vector(pat.vector_size(), seed=SEED_B + 3))
+    setup_s = time.perf_counter() - t0
+    x_ref = None
+    out = {}
+    for kind, prec in (("ilu0", "fp64"), ("ilu0", "mixed_fp32"), ("ilu0", "mixed_bf16"),
+                       ("rasilu0", "fp64"), ("rasilu0", "mixed_fp32")):
+        M = api.create_preconditioner(kind, schedule=schedule)
+        opts = {**CFG3_SOLVER, "precision": prec}
+        if prec != "fp64":
+            opts.update(MIXED)
+        solver = api.create_linear_solver("fgmres", **opts)
+        x = api.ChidgVector(A)
+        solver.solve(A, x, b, M)                       # warm-up (builds the programme)
+        torch.cuda.synchronize()
+        ctx.set_profiling(True)
+        ev = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            solver.solve(A, x, b, M)
+            e1.record(stream)
+            ev.append((e0, e1))
+        torch.cuda.synchronize()
+        kt = ctx.kernel_times()
+        ctx.set_profiling(False)
+        lat = [a.elapsed_time(bb) for a, bb in ev]
+        xh = x.download()
+        if x_ref is None:
+            x_ref = xh
+        fa_ms, fa_n = kt.get("factor", (0.0, 0))
+        out[f"{kind}_{prec}"] = {
+            "solves_per_s": 1000.0 * reps / sum(lat), "ms_per_solve": sum(lat) / reps,
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "outer_iters": solver.niter, "inner_iters": solver.inner_iters,
+            "true_rel_residual": solver.residual_norm / solver.r0norm_initial,
+            "rel_err_vs_ilu0_fp64_solution": float(np.linalg.norm(xh - x_ref) / np.linalg.norm(x_ref)),
+            "factor_ms": fa_ms / fa_n if fa_n else None}
+        M.tear_down()
+        x.release()
+    base = out["ilu0_fp64"]["ms_per_solve"]
+    for v in out.values():
+        v["speedup_vs_ilu0_fp64"] = base / v["ms_per_solve"]
+    free, total = torch.cuda.mem_get_info()
+    b.release()
+    A.release()
+    return {"workload": "32^3 hex box, 5 fields, P2 (223232 blocks of 135x135, 32.5 GB FP64), FGMRES(30) "
+                        "to rtol 1e-8 (FP64 true residual); RAS over 4x4x4 subdomains of 8^3, 1-element overlap",
+            "setup_s": setup_s, "device_bytes_in_use_at_end": int(total - free), "modes": out}
+
+
 def cpu_sample_solve(seed_a=SEED_A, seed_b=SEED_B, n=SAMPLE_N):
     """One full FGMRES(50)+ILU0 FP64 solve of an n^3 P2 box on one host core."""
     from chidg_b200 import mesh
@@ -454,6 +525,13 @@ def run_gpu(args):
 
     batch = run_batch_leg(ctx, args.schedule) if not args.no_batch else None
     serving = run_serve_leg(local) if not args.no_serve else None
+    cfg3 = None
+    if not args.no_cfg3 and world == 1:
+        # the 24^3 objects leave the device first: the 32^3 legs hold ~120 GB
+        M.tear_down()
+        for o in (x, b, A):
+            o.release()
+        cfg3 = run_cfg3_leg(ctx, stream, args.schedule)
 
     if rank != 0:
         return 0
@@ -507,6 +585,7 @@ def run_gpu(args):
         "mixed": mixed,
         "batch": batch,
         "serving": serving,
+        "cfg3": cfg3,
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
@@ -525,6 +604,7 @@ def main():
     ap.add_argument("--schedule", default="stream", choices=["tasks", "stream", "dataflow", "levels"],
                     help="schedule of the ILU sweeps")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
+    ap.add_argument("--no-cfg3", action="store_true", help="skip the 32^3 P2 legs (ILU0 and RAS, FP64 and mixed)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

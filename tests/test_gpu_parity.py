@@ -311,9 +311,14 @@ def test_reference_kats_on_gpu(name):
             assert abs(xv[eo[e - 1] + i - 1] - expect) <= case["tol"]
 
 
-@pytest.mark.parametrize("precision", ["mixed_fp32", "mixed_bf16", "mixed_precon_fp32"])
-def test_mixed_precision_reaches_fp64_accuracy(precision):
-    pat, vals, Ao, Ag = setup((4, 4, 4), 1, seed=13)
+@pytest.mark.parametrize("precision,kind", [("mixed_fp32", "ilu0"), ("mixed_bf16", "ilu0"),
+                                            ("mixed_precon_fp32", "ilu0"), ("mixed_fp32", "rasilu0"),
+                                            ("mixed_bf16", "rasilu0")])
+def test_mixed_precision_reaches_fp64_accuracy(precision, kind):
+    """Every mixed mode, with ILU0 and with RAS+ILU0 (2 x 2 x 2 subdomains,
+    FP32 factorisation of the overlap rows), reaches the FP64 residual."""
+    sub = (2, 2, 2) if kind == "rasilu0" else (1, 1, 1)
+    pat, vals, Ao, Ag = setup((4, 4, 4), 1, sub=sub, seed=13)
     b = mesh.synth_vector(Ao.n, seed=14)
     xo, ro = O.fgmres(Ao, O.OraclePrecon(Ao, "ilu0"), b,
                       O.default_opts(tol=0.0, rtol=1e-12, nkrylov=40, inner_fgmres=0, nmax=400))
@@ -321,7 +326,7 @@ def test_mixed_precision_reaches_fp64_accuracy(precision):
                                       precision=precision, mixed_inner_nkrylov=20, mixed_inner_rtol=1e-2,
                                       mixed_inner_nmax=40)
     xg = api.ChidgVector(Ag)
-    solver.solve(Ag, xg, api.ChidgVector(Ag, b), api.create_preconditioner("ilu0"))
+    solver.solve(Ag, xg, api.ChidgVector(Ag, b), api.create_preconditioner(kind))
     assert solver.residual_norm <= 1.5e-8 * solver.r0norm_initial
     assert relerr(xg.download(), xo) < 1e-6
 
