@@ -9,6 +9,7 @@
 //   chidg_mv                                src/containers/operator_chidg_mv.f90:117-645
 //   dot / norm                              src/containers/operator_chidg_dot.f90:30-97,
 //                                           src/containers/type_chidg_vector.f90:1237-1305
+//   chidg_mv, transposed (A%transposed)     src/containers/operator_chidg_mv.f90:46-60,692-1049
 //   inv (getrf + getri semantics)           src/numerical_methods/mod_inv.f90:97-150
 //   precon_jacobi update/apply              src/preconditioners/precon_jacobi.f90:95-215
 //   precon_ILU0 update/apply                src/preconditioners/precon_ILU0.f90:111-411
@@ -45,6 +46,7 @@ struct Mat {
     vector<vector<int>> lblk;     // per row: LOCAL blocks in storage order
     vector<int> diag;             // per row: DIAG block id
     long stamp = 1;
+    bool transposed = false;      // chidg_matrix_t%transposed (type_chidg_matrix.f90:49)
 
     int bsize(int e) const { return nvars[e] * nterms[e]; }
     int64_t seg(int e, int t) const { return eoff[e] + (int64_t)t * bsize(e); }
@@ -68,6 +70,43 @@ inline void gemv_sub(int nr, int nc, const double* A, const double* x, double* y
         const double* col = A + (int64_t)c * nr;
         for (int r = 0; r < nr; ++r) y[r] -= col[r] * xc;
     }
+}
+// y(0:nc) += A(nr x nc)^T * x(0:nr)
+inline void gemv_t_acc(int nr, int nc, const double* A, const double* x, double* y) {
+    for (int c = 0; c < nc; ++c) {
+        const double* col = A + (int64_t)c * nr;
+        double s = 0.0;
+        for (int r = 0; r < nr; ++r) s += col[r] * x[r];
+        y[c] += s;
+    }
+}
+// y(0:nc) -= A(nr x nc)^T * x(0:nr)
+inline void gemv_t_sub(int nr, int nc, const double* A, const double* x, double* y) {
+    for (int c = 0; c < nc; ++c) {
+        const double* col = A + (int64_t)c * nr;
+        double s = 0.0;
+        for (int r = 0; r < nr; ++r) s += col[r] * x[r];
+        y[c] -= s;
+    }
+}
+// C(m x n) = A(k x m)^T * B(k x n)
+void gemm_tn(int m, int n, int k, const double* A, const double* B, double* C) {
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < m; ++i) {
+            double s = 0.0;
+            for (int p = 0; p < k; ++p) s += A[p + (int64_t)i * k] * B[p + (int64_t)j * k];
+            C[i + (int64_t)j * m] = s;
+        }
+}
+// C(m x n) -= A(m x k) * B(n x k)^T
+void gemm_sub_nt(int m, int n, int k, const double* A, const double* B, double* C) {
+    for (int j = 0; j < n; ++j)
+        for (int p = 0; p < k; ++p) {
+            const double b = B[j + (int64_t)p * n];
+            const double* a = A + (int64_t)p * m;
+            double* c = C + (int64_t)j * m;
+            for (int i = 0; i < m; ++i) c[i] -= a[i] * b;
+        }
 }
 // C(m x n) = A(m x k) * B(k x n), all column-major
 void gemm(int m, int n, int k, const double* A, const double* B, double* C) {
@@ -207,14 +246,23 @@ struct PreconILU0 : Precon {
                 }
             }
     }
-    // precon_ILU0.f90:111-265 (non-transposed branch)
+    // precon_ILU0.f90:111-265; with A%transposed (:148-207) the factors are
+    // those of A^T: D = A(e,e)^T, L = A(parent, itranspose)^T inv(D_parent),
+    // D -= L A_lower^T.  precon_jacobi.f90:121-125 likewise inverts A(e,e)^T.
     int update(Mat& A) override {
         LD.assign(A.nval, 0.0);
         err_elem = -1;
         for (int t = 0; t < A.ntime; ++t) {
             for (int e = 0; e < A.nelem; ++e) {
                 const int k = A.diag[A.row(e, t)];
-                std::memcpy(LD.data() + A.voff[k], A.blk(k), sizeof(double) * A.nr[k] * A.nc[k]);
+                const int b = A.nr[k];
+                double* D = LD.data() + A.voff[k];
+                if (A.transposed) {
+                    for (int j = 0; j < b; ++j)
+                        for (int i = 0; i < b; ++i) D[i + (int64_t)j * b] = A.blk(k)[j + (int64_t)i * b];
+                } else {
+                    std::memcpy(D, A.blk(k), sizeof(double) * A.nr[k] * A.nc[k]);
+                }
             }
             for (int e = 0; e < A.nelem; ++e) {
                 const int r = A.row(e, t);
@@ -225,11 +273,16 @@ struct PreconILU0 : Precon {
                     const int p = A.ce[kl];
                     const int kpd = A.diag[A.row(p, t)];
                     double* L = LD.data() + A.voff[kl];
-                    // L = A_lower * inv(D_parent)
-                    gemm(A.nr[kl], A.nc[kl], A.nc[kl], A.blk(kl), LD.data() + A.voff[kpd], L);
-                    // D -= L * A(parent, itranspose)
                     const int kt = itrans[kl];
-                    gemm_sub(b, A.nc[kt], A.nc[kl], L, A.blk(kt), D);
+                    if (A.transposed) {
+                        // L = A(parent, itranspose)^T * inv(D_parent); D -= L * A_lower^T
+                        gemm_tn(A.nr[kl], A.nc[kl], A.nr[kt], A.blk(kt), LD.data() + A.voff[kpd], L);
+                        gemm_sub_nt(b, A.nc[kl], A.nc[kl], L, A.blk(kl), D);
+                    } else {
+                        // L = A_lower * inv(D_parent); D -= L * A(parent, itranspose)
+                        gemm(A.nr[kl], A.nc[kl], A.nc[kl], A.blk(kl), LD.data() + A.voff[kpd], L);
+                        gemm_sub(b, A.nc[kt], A.nc[kl], L, A.blk(kt), D);
+                    }
                 }
                 if (inv_inplace(b, D) != 0) { err_elem = e; return ORC_ESINGULAR; }
             }
@@ -237,7 +290,8 @@ struct PreconILU0 : Precon {
         stamp = A.stamp;
         return ORC_OK;
     }
-    // precon_ILU0.f90:286-411 (non-transposed branch)
+    // precon_ILU0.f90:286-411; with A%transposed the backward solve uses
+    // A(parent, itranspose)^T in place of the upper block (:378-383)
     int apply(Mat& A, const double* v, double* z) override {
         std::memcpy(z, v, sizeof(double) * A.n);
         vector<double> tmp;
@@ -251,8 +305,14 @@ struct PreconILU0 : Precon {
             for (int e = A.nelem - 1; e >= 0; --e) {
                 const int r = A.row(e, t);
                 double* ze = z + A.seg(e, t);
-                for (int ku : upper[r])
-                    gemv_sub(A.nr[ku], A.nc[ku], A.blk(ku), z + A.seg(A.ce[ku], t), ze);
+                for (int ku : upper[r]) {
+                    if (A.transposed) {
+                        const int kt = itrans[ku];
+                        gemv_t_sub(A.nr[kt], A.nc[kt], A.blk(kt), z + A.seg(A.ce[ku], t), ze);
+                    } else {
+                        gemv_sub(A.nr[ku], A.nc[ku], A.blk(ku), z + A.seg(A.ce[ku], t), ze);
+                    }
+                }
                 const int kd = A.diag[r];
                 const int b = A.nr[kd];
                 tmp.assign(b, 0.0);
@@ -398,6 +458,7 @@ struct PreconRAS : Precon {
     // precon_RASILU0.f90:205-415 (native branch)
     int update(Mat& A) override {
         if (A.ntime != 1) return ORC_EINVAL;   // single time level only (recv_dom_comm.f90:83)
+        if (A.transposed) return ORC_EINVAL;   // "transpose not implemented for 'native' containers" (:254)
         err_elem = -1;
         LD.assign(A.nval, 0.0);
         for (int s = 0; s < nsub; ++s) {
@@ -459,6 +520,7 @@ struct PreconRAS : Precon {
 
     // precon_RASILU0.f90:454-625 (native branch)
     int apply(Mat& A, const double* v, double* z) override {
+        if (A.transposed) return ORC_EINVAL;   // "not implemented for transposed matrices" (:494)
         vector<double> zl(A.n), tmp;
         std::memcpy(zl.data(), v, sizeof(double) * A.n);  // each subdomain only touches its own rows
         for (int s = 0; s < nsub; ++s) {
@@ -528,8 +590,34 @@ struct PreconRAS : Precon {
 // ---------------------------------------------------------------------------
 // Vector kernels
 // ---------------------------------------------------------------------------
-// chidg_mv, non-transposed, local part (operator_chidg_mv.f90:117-410)
+// transposed_matrix_vector_product, local part (operator_chidg_mv.f90:692-1049):
+// per time level, each lblks / chi_blks / bc_blks block of row (e,t) adds its
+// transpose times x(e,t) into its parent's segment; then the harmonic-balance
+// term y(e,t) += D(t',t) mass^T x(e,t') for t' /= t.  The hb_blks block of row
+// (e,t') and column (e,t) holds D(t',t) mass per field
+// (type_harmonic_balance.f90:127-229), so that term is its transpose times x(e,t').
+void mtv(const Mat& A, const double* x, double* y) {
+    std::fill(y, y + A.n, 0.0);
+    for (int t = 0; t < A.ntime; ++t) {
+        for (int e = 0; e < A.nelem; ++e) {
+            const double* xe = x + A.seg(e, t);
+            for (int k : A.rowblk[A.row(e, t)])
+                if (A.kind[k] != ORC_BLK_HB) gemv_t_acc(A.nr[k], A.nc[k], A.blk(k), xe, y + A.seg(A.ce[k], A.ct[k]));
+        }
+        for (int e = 0; e < A.nelem; ++e)
+            for (int ti = 0; ti < A.ntime; ++ti) {
+                if (ti == t) continue;
+                for (int k : A.rowblk[A.row(e, ti)])
+                    if (A.kind[k] == ORC_BLK_HB && A.ce[k] == e && A.ct[k] == t)
+                        gemv_t_acc(A.nr[k], A.nc[k], A.blk(k), x + A.seg(e, ti), y + A.seg(e, t));
+            }
+    }
+}
+
+// chidg_mv (operator_chidg_mv.f90:46-60 selects the transposed product when
+// A%transposed), non-transposed local part :117-410
 void mv(const Mat& A, const double* x, double* y) {
+    if (A.transposed) { mtv(A, x, y); return; }
     std::fill(y, y + A.n, 0.0);
     for (int t = 0; t < A.ntime; ++t)
         for (int e = 0; e < A.nelem; ++e) {
@@ -777,6 +865,7 @@ int orc_matrix_block_offsets(const orc_matrix* h, int64_t* offsets) {
     return ORC_OK;
 }
 void orc_matrix_touch(orc_matrix* h) { h->m.stamp++; }
+int orc_matrix_set_transposed(orc_matrix* h, int32_t transposed) { h->m.transposed = transposed != 0; return ORC_OK; }
 int orc_mv(orc_matrix* h, const double* x, double* y) { mv(h->m, x, y); return ORC_OK; }
 double orc_dot(const orc_matrix* h, const double* x, const double* y) { return dotv(h->m.n, x, y); }
 double orc_norm(const orc_matrix* h, const double* x) { return std::sqrt(dotv(h->m.n, x, x)); }

@@ -86,6 +86,9 @@ int     orc_precon_get_LD(const orc_precon*, double* packed);
 int     orc_fgmres_solve(orc_matrix*, orc_precon*, const double* b, double* x,
                          const orc_fgmres_opts*, orc_fgmres_result*, double* hist, int32_t hist_cap);
 void    orc_matrix_touch(orc_matrix*);   /* bump the stamp, as chidg_matrix%store does */
+/* chidg_matrix_t%transposed: orc_mv then computes A^T x, ILU0 / Jacobi factor
+ * A^T and RASILU0 refuses (ORC_EINVAL), as the reference does. */
+int     orc_matrix_set_transposed(orc_matrix*, int32_t transposed);
 
 #ifdef __cplusplus
 }

@@ -59,6 +59,7 @@ def lib():
         for f in ("orc_matrix_set_values", "orc_matrix_get_values"):
             getattr(L, f).argtypes = [VP, DP]
         L.orc_matrix_touch.argtypes = [VP]
+        L.orc_matrix_set_transposed.argtypes = [VP, C.c_int32]
         L.orc_mv.argtypes = [VP, DP, DP]
         L.orc_dot.restype = C.c_double
         L.orc_dot.argtypes = [VP, DP, DP]
@@ -124,6 +125,10 @@ class OracleMatrix:
         out = np.empty(self.nval)
         lib().orc_matrix_get_values(self.h, _dp(out))
         return out
+
+    def set_transposed(self, transposed: bool = True):
+        """chidg_matrix_t%transposed: mv computes A^T x, ILU0 / Jacobi factor A^T."""
+        lib().orc_matrix_set_transposed(self.h, int(bool(transposed)))
 
     def mv(self, x):
         x = np.ascontiguousarray(x, dtype=np.float64)

@@ -104,6 +104,91 @@ def parse(path: str):
     return blocks, rhs, asserts, tol, solver_tol
 
 
+# Operator known-answer tests: two 2x2x2 domains, one field, P1 (8 modes).
+# Each test sets some blocks to a constant (or to M(i,j) = i), sets x per
+# element, multiplies and asserts whole element segments of the result.
+OPERATOR_TESTS = {
+    # name: (file, subroutine)
+    "mv": ("test/unit_testing/containers/test_chidg_matrix_operator_mv.pf", "test_chidg_matrix_operator_mv"),
+    "mtv": ("test/unit_testing/containers/test_chidg_matrix_operator_mtv.pf", "test_chidg_matrix_operator_mtv"),
+    "mtv_2": ("test/unit_testing/containers/test_chidg_matrix_operator_mtv.pf", "test_chidg_matrix_operator_mtv_2"),
+}
+OP_ELEMS_PER_DOMAIN, OP_NTERMS = 8, 8
+# Chimera donors of the "D2 E8 M1 : Overlapping : NonMatching" mesh, used by
+# the tests that address blocks through chi_blks(...)%dparent_g/eparent_g(k)
+# instead of loc(dom, elem).  The mesh's hole cutting is not reproducible
+# here; the donors follow from test_chidg_matrix_operator_mtv's own asserts
+# (b(2,1) = 2*0.1*nterms and b(2,3) = 3*0.1*nterms: the two donors of domain 1
+# element 2 are domain 2 elements 1 and 3; b(1,2) = 4*0.2*nterms: the donor of
+# domain 2 element 1 is domain 1 element 2).  (domain, element) -> donors.
+CHIMERA_DONORS = {(1, 2): [(2, 1), (2, 3)], (2, 1): [(1, 2)]}
+
+
+def op_value(expr: str) -> float:
+    """bref_* expressions: products and sums of literals, named constants and nterms_s."""
+    e = expr.replace("_rk", "")
+    e = re.sub(r"\bnterms_s\b", str(OP_NTERMS), e)
+    for k, v in CONST.items():
+        e = re.sub(rf"\b{k}\b", repr(v), e)
+    if not re.fullmatch(r"[\d.+*/() \-]+", e):
+        raise ValueError(f"unsupported expression {expr!r}")
+    return float(eval(e, {"__builtins__": {}}))   # arithmetic on literals only
+
+
+def parse_operator(path: str, subroutine: str):
+    text = open(path).read()
+    m = re.search(rf"subroutine {subroutine}\(\)(.*?)end subroutine {subroutine}", text, re.S)
+    body = m.group(1)
+    state = {"idom": None, "ielem": None, "itime": 1}
+    locvar, blocks, x, bref, asserts = {}, {}, {}, {}, []
+    mode, tol, rowindex = None, None, False
+    gid = lambda d, e: (d - 1) * OP_ELEMS_PER_DOMAIN + (e - 1)     # 0-based global element
+    res = lambda tok: state[tok] if tok in state else int(tok)
+    for raw in body.splitlines():
+        line = raw.split("!")[0].strip()
+        if not line:
+            continue
+        if (m := re.fullmatch(r"(idom|ielem|itime)\s*=\s*(\d+)", line)):
+            state[m.group(1)] = int(m.group(2))
+        elif (m := re.fullmatch(r"tol\s*=\s*([\d.eE+-]+)_rk", line)):
+            tol = float(m.group(1))
+        elif (m := re.fullmatch(r"(\w+)\s*=\s*A%dom\((\w+)\)%(lblks|chi_blks)\(ielem,\s*itime\)%loc\((\d+),\s*(\d+),\s*itime\)", line)):
+            kind = 0 if m.group(3) == "lblks" else 1
+            locvar[m.group(1)] = (kind, gid(res(m.group(2)), state["ielem"]), gid(int(m.group(4)), int(m.group(5))))
+        elif (m := re.fullmatch(r"(idom_d|ielem_d)\s*=\s*A%dom\((\w+)\)%chi_blks\(ielem,\s*itime\)%(dparent_g|eparent_g)\((\d+)\)", line)):
+            donor = CHIMERA_DONORS[(res(m.group(2)), state["ielem"])][int(m.group(4)) - 1]
+            state[m.group(1)] = donor[0] if m.group(3) == "dparent_g" else donor[1]
+        elif (m := re.fullmatch(r"M\(i,j\)\s*=\s*real\(i,\s*rk\)", line)):
+            rowindex = True
+        elif (m := re.fullmatch(r"A%dom\((\w+)\)%(lblks|chi_blks)\(ielem,\s*itime\)%data_\((\w+)\)%mat\s*=\s*(\w+)", line)):
+            dom = res(m.group(1))
+            if m.group(3) in locvar:
+                key = locvar[m.group(3)]
+            else:                                   # chi_blks%data_(k): the k-th donor
+                d, e = CHIMERA_DONORS[(dom, state["ielem"])][int(m.group(3)) - 1]
+                key = (1, gid(dom, state["ielem"]), gid(d, e))
+            if m.group(4) == "M":
+                assert rowindex
+                blocks[key] = "rowindex"
+            else:
+                blocks[key] = CONST[m.group(4)]
+        elif (m := re.fullmatch(r"x%dom\((\w+)\)%vecs\((\w+)\)%vec\s*=\s*([\d.]+)_rk", line)):
+            x[gid(res(m.group(1)), res(m.group(2)))] = float(m.group(3))
+        elif (m := re.fullmatch(r"b\s*=\s*(chidg_mv|transposed_matrix_vector_product)\(A,\s*x\)", line)):
+            mode = "mv" if m.group(1) == "chidg_mv" else "mtv"
+        elif (m := re.fullmatch(r"(bref_\w+)\s*=\s*(.+)", line)):
+            bref[m.group(1)] = op_value(m.group(2))
+        elif (m := re.fullmatch(r"@assertEqual\((bref_\w+),\s*b%dom\((\d+)\)%vecs\((\d+)\)%vec,\s*tol\)", line)):
+            asserts.append([gid(int(m.group(2)), int(m.group(3))), bref[m.group(1)]])
+    assert mode and asserts and tol
+    return {"subroutine": subroutine, "mode": mode, "nelem": 2 * OP_ELEMS_PER_DOMAIN, "nvars": 1,
+            "nterms": OP_NTERMS, "tol": tol,
+            # [row element, column element, kind (0 LOCAL, 1 CHIMERA), value or "rowindex" (M(i,j) = i)]
+            "blocks": [[r, c, k, v] for (k, r, c), v in sorted(blocks.items())],
+            "x": [[e, v] for e, v in sorted(x.items())],
+            "asserts": asserts}
+
+
 def main(root: str):
     out = {"source": "ChiDG unit tests (read as text by tests/golden/make_golden.py)", "cases": {}}
     for name, (rel, nx, ntime) in TESTS.items():
@@ -116,6 +201,8 @@ def main(root: str):
             "asserts": [[k, idx, v] for k, idx, v in asserts],
             "tol": tol, "solver_tol": solver_tol,
         }
+    for name, (rel, sub) in OPERATOR_TESTS.items():
+        out["cases"][name] = {"file": rel, **parse_operator(os.path.join(root, rel), sub)}
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_kat.json")
     with open(dst, "w") as f:
         json.dump(out, f, indent=1)

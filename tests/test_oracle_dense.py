@@ -141,3 +141,74 @@ def test_rasilu0_reduces_residual():
     _, res1 = O.fgmres(A, O.OraclePrecon(A, "jacobi"), b,
                        O.default_opts(tol=0.0, rtol=1e-8, nkrylov=30, inner_fgmres=0, nmax=300))
     assert res["niter"] <= res1["niter"]
+
+
+def transposed_values(pat, vals):
+    """Values of A^T on A's own pattern: block (r, c) holds the transpose of
+    block (c, r) (box patterns are structurally symmetric, HB blocks included)."""
+    voff, _ = pat.value_offsets()
+    nr, nc = pat.block_dims()
+    where = {(int(pat.blk_row_elem[k]), int(pat.blk_row_time[k]), int(pat.blk_col_elem[k]),
+              int(pat.blk_col_time[k]), int(pat.blk_kind[k])): k for k in range(pat.nblocks)}
+    out = np.empty_like(vals)
+    for (re_, rt, ce, ct, kd), k in where.items():
+        kt = where[(ce, ct, re_, rt, kd)]
+        src = vals[voff[kt]:voff[kt] + nr[kt] * nc[kt]].reshape(nc[kt], nr[kt]).T   # block kt, (nr x nc)
+        out[voff[k]:voff[k] + nr[k] * nc[k]] = src.T.ravel(order="F")
+    return out
+
+
+@pytest.mark.parametrize("shape,P,nt", [((3, 2, 2), 1, 1), ((2, 2, 2), 0, 3)])
+def test_mtv_matches_dense(shape, P, nt):
+    """transposed_matrix_vector_product (operator_chidg_mv.f90:692-1049), HB term included."""
+    pat = mesh.box_pattern(*shape, 5, mesh.nterms_of_order(P), ntime=nt)
+    vals = mesh.synth_values(pat, seed=31)
+    A = O.OracleMatrix(pat)
+    A.set_values(vals)
+    A.set_transposed(True)
+    x = mesh.synth_vector(A.n, seed=32)
+    assert np.allclose(A.mv(x), dense(pat, vals).T @ x, rtol=1e-13, atol=1e-13)
+
+
+@pytest.mark.parametrize("kind,nt", [("ilu0", 1), ("ilu0", 2), ("jacobi", 1)])
+def test_transposed_factors_are_those_of_the_transpose(kind, nt):
+    """precon_ILU0.f90:148-207 / precon_jacobi.f90:121-125: the transposed
+    branch factors A^T, so it matches the plain branch run on A^T's values."""
+    pat = mesh.box_pattern(3, 2, 2, 5, mesh.nterms_of_order(1), ntime=nt)
+    vals = mesh.synth_values(pat, seed=33)
+    A = O.OracleMatrix(pat)
+    A.set_values(vals)
+    A.set_transposed(True)
+    M = O.OraclePrecon(A, kind)
+    M.update()
+    B = O.OracleMatrix(pat)
+    B.set_values(transposed_values(pat, vals))
+    MB = O.OraclePrecon(B, kind)
+    MB.update()
+    assert np.allclose(M.LD(), MB.LD(), rtol=1e-12, atol=1e-13)
+    v = mesh.synth_vector(A.n, seed=34)
+    assert np.allclose(M.apply(v), MB.apply(v), rtol=1e-12, atol=1e-13)
+
+
+def test_transposed_fgmres_solves_the_adjoint_system():
+    pat = mesh.box_pattern(3, 3, 2, 5, mesh.nterms_of_order(1))
+    vals = mesh.synth_values(pat, seed=35)
+    A = O.OracleMatrix(pat)
+    A.set_values(vals)
+    A.set_transposed(True)
+    b = mesh.synth_vector(A.n, seed=36)
+    x, res = O.fgmres(A, O.OraclePrecon(A, "ilu0"), b,
+                      O.default_opts(tol=0.0, rtol=1e-12, nkrylov=30, inner_fgmres=0, nmax=500))
+    xd = np.linalg.solve(dense(pat, vals).T, b)
+    assert np.linalg.norm(x - xd) <= 1e-9 * np.linalg.norm(xd)
+
+
+def test_rasilu0_refuses_transposed_matrix():
+    """precon_RASILU0.f90:254: transpose not implemented for native containers."""
+    pat = mesh.box_pattern(4, 2, 2, 5, mesh.nterms_of_order(0), subdomains=(2, 1, 1))
+    A = O.OracleMatrix(pat)
+    A.set_values(mesh.synth_values(pat, seed=37))
+    A.set_transposed(True)
+    M = O.OraclePrecon(A, "rasilu0")
+    with pytest.raises(ArithmeticError):
+        M.update()

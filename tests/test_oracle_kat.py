@@ -51,6 +51,23 @@ def test_fgmres_kat(name):
     assert res["residual_norm"] < 1e-12
 
 
+@pytest.mark.parametrize("name", ["mv", "mtv", "mtv_2"])
+def test_operator_kat(name):
+    """test_chidg_matrix_operator_mv.pf / _mtv.pf: chidg_mv and the
+    transposed product (chidg_matrix_t%transposed) on LOCAL and CHIMERA blocks."""
+    case = CASES[name]
+    pat, vals, x = kat_util.build_operator(case)
+    A = O.OracleMatrix(pat)
+    A.set_values(vals)
+    if case["mode"] == "mtv":
+        A.set_transposed(True)
+    y = A.mv(x)
+    eo = pat.elem_offsets()
+    for e, expect in case["asserts"]:
+        assert np.all(np.abs(y[eo[e]:eo[e + 1]] - expect) <= case["tol"]), (e, expect, y[eo[e]:eo[e + 1]])
+    assert len(case["asserts"]) >= 2
+
+
 def test_inv_matches_numpy():
     rng = np.random.default_rng(0)
     for n in (1, 2, 5, 40, 135):
