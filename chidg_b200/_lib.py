@@ -74,6 +74,8 @@ PROTOTYPES = {
     "chidg_gpu_matrix_clear": (C.c_int, [VP]),
     "chidg_gpu_matrix_scale_diagonal": (C.c_int, [VP, DP, DP]),
     "chidg_gpu_matrix_stamp": (C.c_int, [VP, I64P]),
+    "chidg_gpu_matrix_set_transposed": (C.c_int, [VP, C.c_int32]),
+    "chidg_gpu_matrix_get_transposed": (C.c_int, [VP, C.POINTER(C.c_int32)]),
     "chidg_gpu_vector_create": (C.c_int, [VP, C.POINTER(VP)]),
     "chidg_gpu_vector_destroy": (C.c_int, [VP]),
     "chidg_gpu_vector_upload": (C.c_int, [VP, VP]),

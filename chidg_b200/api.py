@@ -159,6 +159,17 @@ class ChidgMatrix:
         self.ctx.L.chidg_gpu_matrix_stamp(self.h, C.byref(s))
         return s.value
 
+    @property
+    def transposed(self) -> bool:
+        """chidg_matrix_t%transposed: products, ILU0 and Jacobi act on A^T."""
+        t = C.c_int32()
+        self.ctx.check(self.ctx.L.chidg_gpu_matrix_get_transposed(self.h, C.byref(t)), "get_transposed")
+        return bool(t.value)
+
+    @transposed.setter
+    def transposed(self, value: bool):
+        self.ctx.check(self.ctx.L.chidg_gpu_matrix_set_transposed(self.h, int(bool(value))), "set_transposed")
+
     def release(self):
         if getattr(self, "h", None):
             self.ctx.L.chidg_gpu_matrix_destroy(self.h)

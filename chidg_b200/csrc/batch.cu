@@ -161,6 +161,8 @@ extern "C" int chidg_gpu_fgmres_solve_batched(chidg_gpu_matrix* A, chidg_gpu_pre
     // M%update as the controller decides (type_fgmres.f90:118-122)
     if (!(o.use_controller && M->stamp == A->stamp && M->precision == prec))
         if ((st = chidg_gpu_precon_update(M, A, prec))) return st;
+    // from here on A is the operator: A, or A^T when A->transposed (same rows and segments)
+    if ((st = matrix_op(A, &A))) return st;
     set_matvec_smem(A);
     if (M->kind != CHIDG_PRECON_IDENTITY) precon_set_smem(M);
     cudaMemsetAsync(ctx->d_scal + kSlotStatus, 0, sizeof(double), ctx->stream);

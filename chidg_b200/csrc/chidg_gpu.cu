@@ -12,6 +12,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <unordered_map>
 
 using namespace chidg;
 
@@ -331,6 +332,13 @@ extern "C" int chidg_gpu_matrix_create(chidg_gpu_ctx* ctx, const chidg_gpu_patte
         }
     for (int r = 0; r < A->nrow; ++r)
         if (A->diag[r] < 0) { delete A; return fail(ctx, CHIDG_GPU_EINVAL, "matrix_create: row without DIAG block"); }
+    // a pattern listed in the reference's order (per row: lblks, chi_blks,
+    // bc_blks, hb_blks) stores each row's blocks one after another
+    for (int r = 0; r < A->nrow && A->rows_contiguous; ++r)
+        for (size_t q = 1; q < A->rowblk[r].size(); ++q) {
+            const int32_t kp = A->rowblk[r][q - 1], k = A->rowblk[r][q];
+            if (A->voff[k] != A->voff[kp] + (int64_t)A->bsize(A->re[kp]) * A->bsize(A->ce[kp])) { A->rows_contiguous = false; break; }
+        }
     // CSR in row order for the matvec
     std::vector<int64_t> row_ptr(A->nrow + 1), bvoff, bxoff, yoff(A->nrow), dvoff(A->nrow);
     std::vector<int32_t> bnc, rb(A->nrow);
@@ -375,8 +383,10 @@ extern "C" int chidg_gpu_matrix_destroy(chidg_gpu_matrix* A) {
     cudaSetDevice(A->ctx->device);
     cudaStreamSynchronize(A->ctx->stream);
     for (Buffer* b : {&A->val, &A->val32, &A->val16, &A->d_row_ptr, &A->d_blk_voff, &A->d_blk_xoff, &A->d_blk_nc,
-                      &A->d_row_yoff, &A->d_row_b, &A->d_diag_voff, &A->d_elem_nvars, &A->d_elem_nterms, &A->row_sq})
+                      &A->d_row_yoff, &A->d_row_b, &A->d_diag_voff, &A->d_elem_nvars, &A->d_elem_nterms, &A->row_sq,
+                      &A->d_tr_src, &A->d_tr_dst, &A->d_tr_nr, &A->d_tr_nc})
         release(*b);
+    if (A->T) chidg_gpu_matrix_destroy(A->T);
     delete A;
     return CHIDG_GPU_OK;
 }
@@ -486,6 +496,100 @@ extern "C" int chidg_gpu_matrix_scale_diagonal(chidg_gpu_matrix* A, const double
     return CHIDG_GPU_OK;
 }
 
+// ---------------------------------------------------------------------------
+// chidg_matrix_t%transposed
+// ---------------------------------------------------------------------------
+// A^T as a matrix of its own: block (c, r) of the same kind for every block
+// (r, c) of A.  Row r of A^T lists, per kind, the blocks whose transposed
+// partner sits in row r of A, in A's order, then the others by block id; so a
+// structurally symmetric pattern (every box mesh, harmonic-balance blocks
+// included) gives A^T the block order and value offsets of A.
+static int build_transposed(chidg_gpu_matrix* A) {
+    chidg_gpu_ctx* ctx = A->ctx;
+    const int64_t nb = A->nblk;
+    const uint64_t nrow = (uint64_t)A->nrow;
+    auto key = [nrow](int r, int c, int kd) { return ((uint64_t)r * nrow + (uint64_t)c) * 4u + (uint64_t)kd; };
+    std::unordered_map<uint64_t, int> pos;          // (row, column row, kind) -> position in A's row
+    pos.reserve((size_t)nb * 2);
+    for (int r = 0; r < A->nrow; ++r)
+        for (size_t q = 0; q < A->rowblk[r].size(); ++q) {
+            const int32_t k = A->rowblk[r][q];
+            pos[key(r, A->row(A->ce[k], A->ct[k]), A->kind[k])] = (int)q;
+        }
+    struct TB { int row, kind; int64_t order, src; };
+    std::vector<TB> tb((size_t)nb);
+    for (int64_t k = 0; k < nb; ++k) {
+        const int r = A->row(A->ce[k], A->ct[k]);
+        const auto it = pos.find(key(r, A->row(A->re[k], A->rt[k]), A->kind[k]));
+        tb[k] = {r, A->kind[k], it != pos.end() ? (int64_t)it->second : (int64_t)A->rowblk[r].size() + k, k};
+    }
+    std::sort(tb.begin(), tb.end(), [](const TB& a, const TB& b) {
+        return a.row != b.row ? a.row < b.row : a.kind != b.kind ? a.kind < b.kind : a.order < b.order;
+    });
+    std::vector<int32_t> bre(nb), brt(nb), bce(nb), bct(nb), bk(nb);
+    std::vector<int64_t> src(nb);
+    for (int64_t i = 0; i < nb; ++i) {
+        const int64_t k = tb[i].src;
+        bre[i] = A->ce[k]; brt[i] = A->ct[k]; bce[i] = A->re[k]; bct[i] = A->rt[k]; bk[i] = A->kind[k];
+        src[i] = A->voff[k];
+    }
+    chidg_gpu_pattern pt{};
+    pt.nelem = A->nelem; pt.ntime = A->ntime;
+    pt.elem_nvars = A->nvars.data(); pt.elem_nterms = A->nterms.data(); pt.elem_proc = A->proc.data();
+    pt.nblocks = nb;
+    pt.blk_row_elem = bre.data(); pt.blk_row_time = brt.data();
+    pt.blk_col_elem = bce.data(); pt.blk_col_time = bct.data(); pt.blk_kind = bk.data();
+    chidg_gpu_matrix* T = nullptr;
+    int st = chidg_gpu_matrix_create(ctx, &pt, &T);
+    if (st) return st;
+    std::vector<int64_t> dst(nb);
+    std::vector<int32_t> tnr(nb), tnc(nb);
+    for (int64_t i = 0; i < nb; ++i) { dst[i] = T->voff[i]; tnr[i] = T->bsize(T->re[i]); tnc[i] = T->bsize(T->ce[i]); }
+    if ((st = upload_array(ctx, A->d_tr_src, src)) || (st = upload_array(ctx, A->d_tr_dst, dst)) ||
+        (st = upload_array(ctx, A->d_tr_nr, tnr)) || (st = upload_array(ctx, A->d_tr_nc, tnc))) {
+        chidg_gpu_matrix_destroy(T);
+        return st;
+    }
+    A->T = T;
+    A->T_src_stamp = -1;
+    return CHIDG_GPU_OK;
+}
+
+extern "C" int chidg_gpu_matrix_set_transposed(chidg_gpu_matrix* A, int32_t transposed) {
+    if (!A) return CHIDG_GPU_EINVAL;
+    cudaSetDevice(A->ctx->device);
+    if (transposed && !A->T) {
+        const int st = build_transposed(A);
+        if (st) return st;
+    }
+    A->transposed = transposed != 0;
+    return CHIDG_GPU_OK;
+}
+extern "C" int chidg_gpu_matrix_get_transposed(chidg_gpu_matrix* A, int32_t* transposed) {
+    if (!A || !transposed) return CHIDG_GPU_EINVAL;
+    *transposed = A->transposed ? 1 : 0;
+    return CHIDG_GPU_OK;
+}
+
+int chidg::matrix_op(chidg_gpu_matrix* A, chidg_gpu_matrix** out) {
+    if (!A->transposed) { *out = A; return CHIDG_GPU_OK; }
+    chidg_gpu_matrix* T = A->T;
+    if (A->T_src_stamp != A->stamp) {
+        chidg_gpu_ctx* ctx = A->ctx;
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(T->nblk, (int64_t)ctx->nsm * 16));
+        k_block_transpose<<<grid, dim3(32, 8), 0, ctx->stream>>>((const double*)A->val.ptr, (double*)T->val.ptr,
+                                                                (const int64_t*)A->d_tr_src.ptr, (const int64_t*)A->d_tr_dst.ptr,
+                                                                (const int32_t*)A->d_tr_nr.ptr, (const int32_t*)A->d_tr_nc.ptr,
+                                                                T->nblk);
+        const int st = check_launch(ctx, "k_block_transpose");
+        if (st) return st;
+        A->T_src_stamp = A->stamp;
+        T->stamp = A->stamp;           // the FP32 / BF16 copies of T follow A's stamp
+    }
+    *out = T;
+    return CHIDG_GPU_OK;
+}
+
 // Low-precision copies of A for the mixed-precision inner solves.
 int chidg::matrix_lowp(chidg_gpu_matrix* A, int precision) {
     chidg_gpu_ctx* ctx = A->ctx;
@@ -509,7 +613,10 @@ int chidg::matrix_lowp(chidg_gpu_matrix* A, int precision) {
     return CHIDG_GPU_OK;
 }
 
-// y = alpha * A x + beta * z, optional per-row sums of squares of y
+// y = alpha * A x + beta * z, optional per-row sums of squares of y.  The
+// streamed kernel reads each row as one strip of values; rows whose blocks are
+// not stored one after another, and blocks over 1024 rows, take the
+// one-CTA-per-row kernel, which addresses every block by its own offset.
 // CHIDG_MATVEC_ROWS=1 selects the one-CTA-per-row matvec (comparison runs)
 static bool matvec_rows_env() {
     static const bool v = [] {
@@ -524,7 +631,7 @@ int chidg::matvec_launch(chidg_gpu_matrix* A, const TA* val, const TV* x, TV* y,
     chidg_gpu_ctx* ctx = A->ctx;
     using ACC = typename AccOf<TV>::type;
     const int ph = prof_begin(ctx, sizeof(TA) == 8 ? kProfMatvec : kProfMatvec32);
-    if (A->max_b <= SS_MAX_B && !matvec_rows_env()) {
+    if (A->max_b <= SS_MAX_B && A->rows_contiguous && !matvec_rows_env()) {
         // streamed: persistent CTAs, row values prefetched by bulk copies
         constexpr int CW = 8, NST = 2, SB = 24 * 1024;
         const size_t smem = matvec_stream_smem(sizeof(ACC), NST, SB, A->max_row_cols, 32 * CW);
@@ -689,8 +796,11 @@ extern "C" int chidg_gpu_vector_norm(const chidg_gpu_vector* x, double* out) {
 extern "C" int chidg_gpu_matvec(chidg_gpu_matrix* A, const chidg_gpu_vector* x, chidg_gpu_vector* y) {
     if (!A || !x || !y || x->n != A->n || y->n != A->n || x == y) return CHIDG_GPU_EINVAL;
     cudaSetDevice(A->ctx->device);
-    set_matvec_smem(A);
-    return matvec_launch<double, double>(A, (const double*)A->val.ptr, (const double*)x->buf.ptr, (double*)y->buf.ptr,
+    chidg_gpu_matrix* S;                 // A, or A^T when A->transposed (operator_chidg_mv.f90:46-60)
+    int st = matrix_op(A, &S);
+    if (st) return st;
+    set_matvec_smem(S);
+    return matvec_launch<double, double>(S, (const double*)S->val.ptr, (const double*)x->buf.ptr, (double*)y->buf.ptr,
                                          nullptr, 1.0, 0.0, nullptr);
 }
 
@@ -1133,6 +1243,37 @@ void chidg::release_program(IluProgram& P) {
         release(*b);
 }
 
+// The ILU programme of M from A's pattern, or from A^T's when A->transposed
+// (ILU0 and Jacobi of A^T, precon_ILU0.f90:148-207, precon_jacobi.f90:121-125).
+// RASILU0 always uses A: the reference refuses transposed matrices there.
+static int build_programme(chidg_gpu_precon* M, chidg_gpu_matrix* A) {
+    chidg_gpu_ctx* ctx = M->ctx;
+    chidg_gpu_matrix* S = A;
+    int st;
+    if (M->kind != CHIDG_PRECON_RASILU0 && (st = matrix_op(A, &S))) return st;
+    std::string err;
+    st = (M->kind == CHIDG_PRECON_RASILU0) ? build_rasilu0(S, M->P, err)
+                                           : build_ilu0(S, M->kind == CHIDG_PRECON_JACOBI, M->P, err);
+    if (st) { release_program(M->P); return fail(ctx, st, err); }
+    if ((st = finalize_program(ctx, S, M->P))) { release_program(M->P); return st; }
+    const size_t sync_bytes = sizeof(unsigned) * (2 + 4 * (size_t)M->P.nprow);
+    if ((st = ensure(ctx, M->sync, sync_bytes))) { release_program(M->P); return st; }
+    cudaMemsetAsync(M->sync.ptr, 0, sync_bytes, ctx->stream);
+    M->built_transposed = A->transposed && M->kind != CHIDG_PRECON_RASILU0;
+    return CHIDG_GPU_OK;
+}
+
+// The matrix whose blocks M factors and applies: A, or A^T for ILU0 / Jacobi
+// of a transposed A.  RASILU0 with a transposed A is an error, as in the
+// reference ("transpose not implemented for 'native' containers",
+// precon_RASILU0.f90:254,494).
+static int precon_source(chidg_gpu_precon* M, chidg_gpu_matrix** S) {
+    chidg_gpu_matrix* A = M->A;
+    if (A->transposed && M->kind == CHIDG_PRECON_RASILU0)
+        return fail(M->ctx, CHIDG_GPU_EINVAL, "RASILU0: transpose not implemented for 'native' containers");
+    return matrix_op(A, S);
+}
+
 extern "C" int chidg_gpu_precon_create(chidg_gpu_matrix* A, int32_t kind, chidg_gpu_precon** out) {
     if (!A || !out) return CHIDG_GPU_EINVAL;
     *out = nullptr;
@@ -1144,15 +1285,8 @@ extern "C" int chidg_gpu_precon_create(chidg_gpu_matrix* A, int32_t kind, chidg_
     M->A = A;
     M->kind = kind;
     if (kind != CHIDG_PRECON_IDENTITY) {
-        std::string err;
-        int st = (kind == CHIDG_PRECON_RASILU0) ? build_rasilu0(A, M->P, err)
-                                                : build_ilu0(A, kind == CHIDG_PRECON_JACOBI, M->P, err);
-        if (st) { delete M; return fail(ctx, st, err); }
-        st = finalize_program(ctx, A, M->P);
-        if (st) { release_program(M->P); delete M; return st; }
-        const size_t sync_bytes = sizeof(unsigned) * (2 + 4 * (size_t)M->P.nprow);
-        if ((st = ensure(ctx, M->sync, sync_bytes))) { release_program(M->P); delete M; return st; }
-        cudaMemsetAsync(M->sync.ptr, 0, sync_bytes, ctx->stream);
+        const int st = build_programme(M, A);
+        if (st) { release(M->sync); delete M; return st; }
     }
     *out = M;
     return CHIDG_GPU_OK;
@@ -1275,9 +1409,18 @@ extern "C" int chidg_gpu_precon_update(chidg_gpu_precon* M, chidg_gpu_matrix* A,
     if (precision < CHIDG_GPU_FP64 || precision > CHIDG_GPU_MIXED_PRECON_FP32) return fail(ctx, CHIDG_GPU_EINVAL, "precon_update: bad precision");
     ctx->err_elem = -1;
     if (M->kind == CHIDG_PRECON_IDENTITY) { M->stamp = A->stamp; M->precision = precision; return CHIDG_GPU_OK; }
+    int st;
+    chidg_gpu_matrix* user = A;
+    if ((st = precon_source(M, &A))) return st;          // from here on A is the matrix factored (A or A^T)
+    if (M->kind != CHIDG_PRECON_RASILU0 && M->built_transposed != user->transposed) {
+        // the transposed flag changed since the programme was built
+        cudaStreamSynchronize(ctx->stream);
+        release_program(M->P);
+        M->stamp = 0;
+        if ((st = build_programme(M, user))) return st;
+    }
     IluProgram& P = M->P;
-    int st = ensure(ctx, M->LD, sizeof(double) * (size_t)P.ld_size);
-    if (st) return st;
+    if ((st = ensure(ctx, M->LD, sizeof(double) * (size_t)P.ld_size))) return st;
     int big = INT_MAX;
     cudaMemcpyAsync(ctx->d_status, &big, sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
     // fresh task counters for the task-split sweeps (a sweep cut short by an
@@ -1296,7 +1439,7 @@ extern "C" int chidg_gpu_precon_update(chidg_gpu_precon* M, chidg_gpu_matrix* A,
         }
         M->ld64_valid = false;
         M->precision = precision;
-        M->stamp = A->stamp;
+        M->stamp = user->stamp;
         return CHIDG_GPU_OK;
     }
     const int nlev = (int)P.fwd_ptr.size() - 1;
@@ -1359,7 +1502,7 @@ extern "C" int chidg_gpu_precon_update(chidg_gpu_precon* M, chidg_gpu_matrix* A,
     }
     M->ld64_valid = true;
     M->precision = precision;
-    M->stamp = A->stamp;
+    M->stamp = user->stamp;
     return CHIDG_GPU_OK;
 }
 
@@ -1563,6 +1706,8 @@ int chidg::precon_apply_impl(chidg_gpu_precon* M, const TV* v, TV* z, int precis
         const cudaError_t e = cudaMemcpyAsync(z, v, sizeof(TV) * (size_t)n, cudaMemcpyDeviceToDevice, ctx->stream);
         return e == cudaSuccess ? CHIDG_GPU_OK : cuda_fail(ctx, e, "identity apply");
     }
+    int st0;
+    if ((st0 = precon_source(M, &A))) return st0;     // the U blocks come from A^T for a transposed A
     IluProgram& P = M->P;
     using ACC = typename AccOf<TV>::type;
     // work buffer: the output itself when there are no overlap rows
@@ -1699,6 +1844,7 @@ extern "C" int chidg_gpu_precon_download_LD(chidg_gpu_precon* M, double* host) {
     chidg_gpu_matrix* A = M->A;
     if (M->kind == CHIDG_PRECON_IDENTITY || M->stamp == 0) return fail(ctx, CHIDG_GPU_ESTATE, "download_LD: no factors");
     if (!M->ld64_valid) return fail(ctx, CHIDG_GPU_ESTATE, "download_LD: the factors were computed in FP32 (mixed precision)");
+    if (M->kind != CHIDG_PRECON_RASILU0 && M->built_transposed) A = A->T;   // factors of A^T, in A^T's block order
     std::vector<double> ld((size_t)M->P.ld_size);
     cudaError_t e = cudaMemcpyAsync(ld.data(), M->LD.ptr, sizeof(double) * ld.size(), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);

@@ -124,12 +124,19 @@ struct chidg_gpu_matrix {
     std::vector<std::vector<int32_t>> rowblk, lblk;
     std::vector<int32_t> diag;
     int max_row_cols = 0, max_b = 0, mv_threads = 32;
+    bool rows_contiguous = true;             // each row's blocks follow one another in val (the streamed matvec's layout)
     int mvs_grid[3] = {0, 0, 0};             // resident CTAs of the streamed matvec per value type
     chidg::Buffer val, val32, val16;
     int64_t val32_stamp = -1, val16_stamp = -1;
     chidg::Buffer d_row_ptr, d_blk_voff, d_blk_xoff, d_blk_nc, d_row_yoff, d_row_b, d_diag_voff, d_elem_nvars,
         d_elem_nterms, row_sq;
     int64_t stamp = 0;
+    // chidg_matrix_t%transposed (type_chidg_matrix.f90:49): products, ILU0 and
+    // Jacobi then act on A^T, kept as a second matrix T in block-row storage
+    bool transposed = false;
+    chidg_gpu_matrix* T = nullptr;
+    int64_t T_src_stamp = -1;                // stamp of A that T's values were transposed from
+    chidg::Buffer d_tr_src, d_tr_dst, d_tr_nr, d_tr_nc;   // per block of T: source / target offsets, T's block dims
 
     int bsize(int e) const { return nvars[e] * nterms[e]; }
     int64_t seg(int e, int t) const { return eoff[e] + (int64_t)t * bsize(e); }
@@ -150,6 +157,7 @@ struct chidg_gpu_precon {
     int precision = 0;
     int64_t stamp = 0;
     bool ld64_valid = false;               // LD holds the FP64 factors (false after an FP32 factorisation)
+    bool built_transposed = false;         // the programme was built from A^T (A->transposed at build time)
     chidg::IluProgram P;
     chidg::Buffer LD, LD32, LD16, zx, zx32, piv_scratch;
     int schedule = CHIDG_SCHED_STREAM;     // sweep schedule (TASKS for blocks over 1024 rows)
@@ -174,6 +182,9 @@ int push_scalars(chidg_gpu_ctx* ctx, int slot, int count, const double* in);
 template <typename T>
 int mdot(chidg_gpu_ctx* ctx, int64_t n, const T* x, const T* y, int64_t ystride, int nq, int slot);
 int matrix_lowp(chidg_gpu_matrix* A, int precision);
+// The matrix the operators act on: A itself, or A^T (A->T, its values
+// re-transposed when A's stamp changed) when A->transposed is set.
+int matrix_op(chidg_gpu_matrix* A, chidg_gpu_matrix** out);
 template <typename TA, typename TV>
 int matvec_launch(chidg_gpu_matrix* A, const TA* val, const TV* x, TV* y, const TV* z, double alpha, double beta, double* row_sq);
 int set_matvec_smem(chidg_gpu_matrix* A);

@@ -310,7 +310,16 @@ extern "C" int chidg_gpu_fgmres_solve(chidg_gpu_matrix* A, chidg_gpu_precon* M, 
     if (opts) o = *opts;
     else chidg_gpu_fgmres_default_opts(&o);
     if (o.precision < CHIDG_GPU_FP64 || o.precision > CHIDG_GPU_MIXED_PRECON_FP32) return fail(ctx, CHIDG_GPU_EINVAL, "fgmres: bad precision");
-    set_matvec_smem(A);
+    int st;
+    // the operator: A, or A^T when A->transposed (chidg_mv, operator_chidg_mv.f90:46-60)
+    chidg_gpu_matrix* Aop;
+    if ((st = matrix_op(A, &Aop))) return st;
+    // the FP32 / BF16 copy read by the inner solves' products (M%update makes it
+    // too, but not for the identity preconditioner)
+    if ((o.precision == CHIDG_GPU_MIXED_FP32 || o.precision == CHIDG_GPU_MIXED_BF16) &&
+        (st = matrix_lowp(Aop, o.precision)))
+        return st;
+    set_matvec_smem(Aop);
     if (M->kind != CHIDG_PRECON_IDENTITY) precon_set_smem(M);
     ctx->err_elem = -1;
     cudaMemsetAsync(ctx->d_scal + kSlotStatus, 0, sizeof(double), ctx->stream);
@@ -324,7 +333,7 @@ extern "C" int chidg_gpu_fgmres_solve(chidg_gpu_matrix* A, chidg_gpu_precon* M, 
     };
     std::vector<double> hv;
     Solver<double> S;
-    S.ctx = ctx; S.A = A;
+    S.ctx = ctx; S.A = Aop;
     S.ws = &ctx->ws64;
     S.tol = o.tol; S.rtol = o.rtol; S.nmax = o.nmax; S.nkrylov = o.nkrylov; S.orth = o.orthogonalization;
     S.inner = o.inner_fgmres != 0; S.inner_tol = o.inner_tol; S.inner_rtol = o.inner_rtol;
@@ -335,14 +344,13 @@ extern "C" int chidg_gpu_fgmres_solve(chidg_gpu_matrix* A, chidg_gpu_precon* M, 
     Buffer& v32 = ctx->mix_v32;       // kept by the context: no allocation per solve
     Buffer& z32 = ctx->mix_z32;
     int64_t lo_iters = 0;
-    int st;
     if (prec == CHIDG_GPU_FP64 || prec == CHIDG_GPU_MIXED_PRECON_FP32) {
         S.precon = [M, prec](const double* v, double* z) { return precon_apply_impl<double>(M, v, z, prec); };
     } else {
         // FP32 inner FGMRES as the flexible preconditioner of the FP64 outer loop
         S.inner = false;
         lo.reset(new Solver<float>());
-        lo->ctx = ctx; lo->A = A;
+        lo->ctx = ctx; lo->A = Aop;
         lo->ws = &ctx->ws32;
         lo->tol = 0.0; lo->rtol = o.mixed_inner_rtol; lo->nmax = o.mixed_inner_nmax;
         lo->nkrylov = o.mixed_inner_nkrylov; lo->orth = CHIDG_ORTH_CGS; lo->inner = false;

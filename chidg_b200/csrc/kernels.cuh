@@ -287,6 +287,38 @@ static __global__ void k_scale_diagonal(double* __restrict__ val, const int64_t*
 }
 
 // ---------------------------------------------------------------------------
+// A^T in block-row storage: block k of A^T (nr x nc, column-major) is the
+// transpose of its source block of A (nc x nr).  32 x 32 tiles pass through
+// shared memory so that the reads and the writes are both coalesced; CTAs of
+// 32 x 8 threads stride over the blocks.
+// ---------------------------------------------------------------------------
+static __global__ void __launch_bounds__(256)
+    k_block_transpose(const double* __restrict__ src, double* __restrict__ dst, const int64_t* __restrict__ src_off,
+                      const int64_t* __restrict__ dst_off, const int32_t* __restrict__ blk_nr,
+                      const int32_t* __restrict__ blk_nc, int64_t nblk) {
+    __shared__ double tile[32][33];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    for (int64_t k = blockIdx.x; k < nblk; k += gridDim.x) {
+        const int nr = blk_nr[k], nc = blk_nc[k];
+        const double* S = src + src_off[k];
+        double* D = dst + dst_off[k];
+        for (int i0 = 0; i0 < nr; i0 += 32)
+            for (int j0 = 0; j0 < nc; j0 += 32) {
+                for (int ii = ty; ii < 32; ii += 8) {        // tile[ii][tx] = S(j0+tx, i0+ii) = T(i0+ii, j0+tx)
+                    const int i = i0 + ii, j = j0 + tx;
+                    if (i < nr && j < nc) tile[ii][tx] = S[j + (int64_t)i * nc];
+                }
+                __syncthreads();
+                for (int jj = ty; jj < 32; jj += 8) {        // T(i0+tx, j0+jj)
+                    const int i = i0 + tx, j = j0 + jj;
+                    if (i < nr && j < nc) D[i + (int64_t)j * nr] = tile[tx][jj];
+                }
+                __syncthreads();
+            }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // ILU programme: factorisation
 // ---------------------------------------------------------------------------
 struct GemmTask {            // C(m x n) = [Cinit] + sgn * sum_q A_q(m x k_q) B_q(k_q x n)

@@ -190,6 +190,18 @@ int chidg_gpu_matrix_clear(chidg_gpu_matrix* A);
 int chidg_gpu_matrix_scale_diagonal(chidg_gpu_matrix* A, const double* mass,
                                     const double* scale);
 int chidg_gpu_matrix_stamp(chidg_gpu_matrix* A, int64_t* stamp);
+/* chidg_matrix_t%transposed (:49; set by solverdata%init for the adjoint,
+ * type_solverdata.f90:242).  While set, chidg_gpu_matvec computes A^T x
+ * (operator_chidg_mv.f90:46-60, 692-1049), ILU0 and Jacobi factor A^T
+ * (precon_ILU0.f90:148-207, precon_jacobi.f90:121-125), the FGMRES entry
+ * points solve A^T x = b, and RASILU0 update/apply return CHIDG_GPU_EINVAL
+ * (precon_RASILU0.f90:254,494).  The first set builds A^T in block-row
+ * storage on the device (as much memory again as A's values); its values are
+ * re-transposed from A when A's stamp has changed.  The packed values of A
+ * (upload, download) stay in A's own layout.  A preconditioner built before the
+ * flag changed rebuilds its programme at its next update. */
+int chidg_gpu_matrix_set_transposed(chidg_gpu_matrix* A, int32_t transposed);
+int chidg_gpu_matrix_get_transposed(chidg_gpu_matrix* A, int32_t* transposed);
 
 /* ---- chidg_vector_t (src/containers/type_chidg_vector.f90) --------------- */
 int chidg_gpu_vector_create(chidg_gpu_matrix* A, chidg_gpu_vector** out);
@@ -259,7 +271,9 @@ int chidg_gpu_precon_apply(chidg_gpu_precon* M, chidg_gpu_matrix* A,
 #define CHIDG_SCHED_STREAM   3
 int chidg_gpu_precon_set_schedule(chidg_gpu_precon* M, int32_t schedule);
 /* Packed factor blocks (L blocks and inverted diagonals at the positions of
- * the matrix's LOCAL blocks, zero elsewhere), as precon_ILU0_t%LD holds them. */
+ * the matrix's LOCAL blocks, zero elsewhere), as precon_ILU0_t%LD holds them.
+ * For a transposed matrix the positions are those of A^T's blocks (the same
+ * as A's for a structurally symmetric pattern). */
 int chidg_gpu_precon_download_LD(chidg_gpu_precon* M, double* host);
 int chidg_gpu_precon_stamp(chidg_gpu_precon* M, int64_t* stamp);
 

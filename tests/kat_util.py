@@ -42,14 +42,19 @@ def ld_index(pat, e, t, c):
     raise KeyError((e, t, c))
 
 
-def build_operator(case):
+def build_operator(case, order="reference"):
     """Pattern, packed values and x of an operator KAT (mv / mtv): one field,
     `nterms` modes, a DIAG block on every element plus the blocks the test sets;
-    a block is a constant or M(i,j) = i (1-based row index)."""
+    a block is a constant or M(i,j) = i (1-based row index).  Blocks are listed
+    per row in the reference's storage order (lblks, then chi_blks), or with
+    order="by_column" by column element whatever their kind."""
     E, nt = case["nelem"], case["nterms"]
     listed = {(r, c, k): v for r, c, k, v in case["blocks"]}
     blocks = [(e, e, 0) for e in range(E) if (e, e, 0) not in listed] + list(listed)
-    blocks.sort()
+    if order == "reference":
+        blocks.sort(key=lambda t: (t[0], t[2], t[1]))
+    else:
+        blocks.sort()
     i32 = lambda a: np.asarray(a, dtype=np.int32)
     pat = mesh.BlockPattern(
         nelem=E, ntime=1, elem_nvars=i32([case["nvars"]] * E), elem_nterms=i32([nt] * E), elem_proc=i32([0] * E),
