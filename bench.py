@@ -275,6 +275,56 @@ def run_serve_leg(device, requests=64, rate=200.0):
 # ---------------------------------------------------------------------------
 # CPU legs (oracle)
 # ---------------------------------------------------------------------------
+def run_adjoint_leg(ctx, stream, A, b, schedule, reps=3):
+    """The adjoint solve on the same 24^3 P2 system: A%transposed set, FGMRES(50)
+    + ILU0 of A^T to rtol 1e-8 in FP64.  Each timed solve starts from a fresh
+    A^T (A's stamp bumped, so its values are transposed again), as a Newton
+    step's adjoint would."""
+    import torch
+
+    from chidg_b200 import api
+    L = ctx.L
+    A.transposed = True
+    x = api.ChidgVector(A)
+    y = api.ChidgVector(A)
+    M = api.create_preconditioner("ilu0", schedule=schedule)
+    solver = api.create_linear_solver("fgmres", **SOLVER)
+    solver.solve(A, x, b, M)                       # warm-up: builds A^T and its programme
+    bump = lambda: ctx.check(L.chidg_gpu_matrix_upload_range(A.h, None, 0, 0), "stamp")
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    api.chidg_mv(A, b, y)
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    api.chidg_mv(A, b, y)                          # A^T current: product only
+    ev[1].record(stream)
+    bump()
+    ev[2].record(stream)
+    api.chidg_mv(A, b, y)                          # transposition + product
+    ev[3].record(stream)
+    torch.cuda.synchronize()
+    transpose_ms = ev[2].elapsed_time(ev[3]) - ev[0].elapsed_time(ev[1])
+    lat = []
+    for _ in range(reps):
+        bump()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        solver.solve(A, x, b, M)
+        e1.record(stream)
+        lat.append((e0, e1))
+    torch.cuda.synchronize()
+    ms = [a.elapsed_time(bb) for a, bb in lat]
+    out = {"workload": "adjoint of the 24^3 P2 system: A^T x = b, FGMRES(50) + ILU0 of A^T to rtol 1e-8, FP64, "
+                       "A^T re-transposed before every solve",
+           "solves_per_s": 1000.0 * reps / sum(ms), "ms_per_solve": sum(ms) / reps,
+           "transpose_ms": transpose_ms, "transpose_gbs": 2 * 8 * A.nvalues / (transpose_ms / 1e3) / 1e9,
+           "iterations": solver.niter, "true_rel_residual": solver.residual_norm / solver.r0norm_initial}
+    M.tear_down()
+    for o in (x, y):
+        o.release()
+    A.transposed = False
+    return out
+
+
 CFG3 = (32, 32, 32)
 CFG3_SUB = (4, 4, 4)
 CFG3_SOLVER = dict(tol=0.0, rtol=1e-8, nkrylov=30, inner_fgmres=0, nmax=600, orthogonalization="CGS",
@@ -415,7 +465,11 @@ def run_gpu(args):
     from chidg_b200.replicas import allmax, barrier, init_from_env
     rank, world, local, pg = init_from_env("nccl")
     torch.cuda.set_device(local)
-    stream = torch.cuda.current_stream()
+    # the library launches on this stream and every CUDA event below is recorded
+    # on it (torch's default stream has handle 0, for which the library would
+    # create a stream of its own)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     ctx = api.Context(local, stream=stream.cuda_stream)
     pat = mesh.box_pattern(NX, NY, NZ, NVARS, mesh.nterms_of_order(P))
     nval = pat.value_offsets()[1]
@@ -523,6 +577,7 @@ def run_gpu(args):
                            "speedup_vs_fp64": (elapsed_ms / args.steps) / t, "phases": phases}
         M = api.create_preconditioner("ilu0", schedule=args.schedule)   # drop low-precision factors
 
+    adjoint = run_adjoint_leg(ctx, stream, A, b, args.schedule) if not args.no_adjoint else None
     batch = run_batch_leg(ctx, args.schedule) if not args.no_batch else None
     serving = run_serve_leg(local) if not args.no_serve else None
     cfg3 = None
@@ -585,6 +640,7 @@ def run_gpu(args):
         "mixed": mixed,
         "batch": batch,
         "serving": serving,
+        "adjoint": adjoint,
         "cfg3": cfg3,
         "cpu_baseline": cpu,
     }
@@ -604,6 +660,7 @@ def main():
     ap.add_argument("--schedule", default="stream", choices=["tasks", "stream", "dataflow", "levels"],
                     help="schedule of the ILU sweeps")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (A^T) solve leg")
     ap.add_argument("--no-cfg3", action="store_true", help="skip the 32^3 P2 legs (ILU0 and RAS, FP64 and mixed)")
     args = ap.parse_args()
     if args.impl == "reference":
