@@ -92,6 +92,17 @@ module chidg_gpu_mod
             type(c_ptr), value :: mat
             real(c_double)     :: mass(*), scale(*)
         end function
+        ! chidg_matrix_t%transposed (type_chidg_matrix.f90:49)
+        integer(c_int) function chidg_gpu_matrix_set_transposed(mat, transposed) bind(c, name='chidg_gpu_matrix_set_transposed')
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr),        value :: mat
+            integer(c_int32_t), value :: transposed
+        end function
+        integer(c_int) function chidg_gpu_matrix_get_transposed(mat, transposed) bind(c, name='chidg_gpu_matrix_get_transposed')
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr), value :: mat
+            integer(c_int32_t) :: transposed
+        end function
         integer(c_int) function chidg_gpu_vector_create(mat, vec) bind(c, name='chidg_gpu_vector_create')
             import :: c_int, c_ptr
             type(c_ptr), value :: mat
