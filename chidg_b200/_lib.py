@@ -18,7 +18,7 @@ STATUS_NAMES = {0: "OK", 1: "EINVAL", 2: "ENOMEM", 3: "ESINGULAR", 4: "ENONFINIT
                 6: "ENOTCONVERGED", 7: "ECUDA", 8: "ESTATE"}
 
 BLK_LOCAL, BLK_CHIMERA, BLK_BC, BLK_HB = 0, 1, 2, 3
-PRECON_IDENTITY, PRECON_JACOBI, PRECON_ILU0, PRECON_RASILU0 = 0, 1, 2, 3
+PRECON_IDENTITY, PRECON_JACOBI, PRECON_ILU0, PRECON_RASILU0, PRECON_HB = 0, 1, 2, 3, 4
 FP64, MIXED_FP32, MIXED_BF16, MIXED_PRECON_FP32 = 0, 1, 2, 3
 ORTH_CGS, ORTH_MGS = 0, 1
 SCHED_LEVELS, SCHED_DATAFLOW, SCHED_TASKS, SCHED_STREAM = 0, 1, 2, 3
@@ -76,6 +76,11 @@ PROTOTYPES = {
     "chidg_gpu_matrix_stamp": (C.c_int, [VP, I64P]),
     "chidg_gpu_matrix_set_transposed": (C.c_int, [VP, C.c_int32]),
     "chidg_gpu_matrix_get_transposed": (C.c_int, [VP, C.POINTER(C.c_int32)]),
+    "chidg_gpu_matrix_to_file": (C.c_int, [VP, C.c_char_p]),
+    "chidg_gpu_matrix_save": (C.c_int, [VP, C.c_char_p]),
+    "chidg_gpu_matrix_load": (C.c_int, [VP, C.c_char_p, C.POINTER(VP)]),
+    "chidg_gpu_matrix_get_pattern": (C.c_int, [VP, C.POINTER(C.c_int32), C.POINTER(C.c_int32), I64P, I32P, I32P, I32P,
+                                               I32P, I32P, I32P, I32P, I32P]),
     "chidg_gpu_vector_create": (C.c_int, [VP, C.POINTER(VP)]),
     "chidg_gpu_vector_destroy": (C.c_int, [VP]),
     "chidg_gpu_vector_upload": (C.c_int, [VP, VP]),

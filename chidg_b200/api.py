@@ -17,10 +17,11 @@ reference's chidg_signal(FATAL, ...).
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
-from . import _lib
+from . import _lib, mesh
 from ._lib import ChidgGpuError
 
 _ctx_default = {}
@@ -170,6 +171,40 @@ class ChidgMatrix:
     def transposed(self, value: bool):
         self.ctx.check(self.ctx.L.chidg_gpu_matrix_set_transposed(self.h, int(bool(value))), "set_transposed")
 
+    def to_file(self, path: str):
+        """chidg_matrix%to_file: the LOCAL blocks as ChiDG's text listing."""
+        self.ctx.check(self.ctx.L.chidg_gpu_matrix_to_file(self.h, os.fsencode(path)), "to_file")
+
+    def save(self, path: str):
+        """Binary image (pattern, transposed flag, values) for ChidgMatrix.load."""
+        self.ctx.check(self.ctx.L.chidg_gpu_matrix_save(self.h, os.fsencode(path)), "save")
+
+    @classmethod
+    def load(cls, path: str, ctx: Context | None = None) -> "ChidgMatrix":
+        ctx = ctx or default_context()
+        h = C.c_void_p()
+        ctx.check(ctx.L.chidg_gpu_matrix_load(ctx.h, os.fsencode(path), C.byref(h)), "load")
+        self = cls.__new__(cls)
+        self.ctx, self.h = ctx, h
+        ne, nt, nb = C.c_int32(), C.c_int32(), C.c_int64()
+        ctx.check(ctx.L.chidg_gpu_matrix_get_pattern(h, C.byref(ne), C.byref(nt), C.byref(nb), *([None] * 8)), "get_pattern")
+        el = [np.empty(ne.value, dtype=np.int32) for _ in range(3)]
+        bl = [np.empty(nb.value, dtype=np.int32) for _ in range(5)]
+        ctx.check(ctx.L.chidg_gpu_matrix_get_pattern(h, None, None, None, *[a.ctypes.data_as(_lib.I32P) for a in el + bl]),
+                  "get_pattern")
+        diag = (bl[0] == bl[2]) & (bl[1] == bl[3]) & (bl[4] == _lib.BLK_LOCAL)
+        self.pattern = mesh.BlockPattern(nelem=ne.value, ntime=nt.value, elem_nvars=el[0], elem_nterms=el[1],
+                                         elem_proc=el[2], blk_row_elem=bl[0], blk_row_time=bl[1], blk_col_elem=bl[2],
+                                         blk_col_time=bl[3], blk_kind=bl[4],
+                                         blk_face=np.where(diag, mesh.DIAG, mesh.OTHER).astype(np.int32))
+        self._pat = self.pattern.as_struct()
+        n = C.c_int64()
+        ctx.L.chidg_gpu_matrix_nvalues(h, C.byref(n))
+        self.nvalues = n.value
+        ctx.L.chidg_gpu_matrix_nvec(h, C.byref(n))
+        self.n = n.value
+        return self
+
     def release(self):
         if getattr(self, "h", None):
             self.ctx.L.chidg_gpu_matrix_destroy(self.h)
@@ -265,7 +300,7 @@ def chidg_mv(A: ChidgMatrix, x: ChidgVector, y: ChidgVector | None = None) -> Ch
 
 
 PRECON_KINDS = {"identity": _lib.PRECON_IDENTITY, "jacobi": _lib.PRECON_JACOBI, "ilu0": _lib.PRECON_ILU0,
-                "rasilu0": _lib.PRECON_RASILU0}
+                "rasilu0": _lib.PRECON_RASILU0, "hb": _lib.PRECON_HB}
 PRECISIONS = {"fp64": _lib.FP64, "mixed_fp32": _lib.MIXED_FP32, "mixed_bf16": _lib.MIXED_BF16,
               "mixed_precon_fp32": _lib.MIXED_PRECON_FP32}
 

@@ -864,6 +864,47 @@ static int build_ilu0(const chidg_gpu_matrix* A, bool jacobi, IluProgram& P, std
     return CHIDG_GPU_OK;
 }
 
+// precon_HB (precon_HB.f90:169-310): one programme row per element over all
+// its time levels (the element's segment is contiguous: time-major inside the
+// element).  Its D is assembled, not factored: the DIAG block of level t at
+// (t, t), the hb_blks block of row (e, ta) and column (e, tb) at (ta, tb) (it
+// holds D(ta,tb) mass per field, what the reference places there), zero
+// elsewhere; then inverted.  No lower or upper entries.
+static int build_hb(const chidg_gpu_matrix* A, IluProgram& P, std::string& err) {
+    P = IluProgram();
+    P.n_ext = A->n;
+    P.nlocal_rows = A->nelem;
+    P.assembled = true;
+    P.asm_ptr.assign(1, 0);
+    for (int e = 0; e < A->nelem; ++e) {
+        const int b = A->bsize(e), B = b * A->ntime;
+        if (B > 1024) { err = "precon_HB: element block over all time levels above 1024 rows"; return CHIDG_GPU_EINVAL; }
+        P.prow_b.push_back(B);
+        P.prow_elem.push_back(e);
+        P.v_off.push_back(A->eoff[e]);
+        P.z_off.push_back(A->eoff[e]);
+        P.diagA_off.push_back(-1);
+        P.diag_blk.push_back(-1);
+        P.lo.emplace_back();
+        P.up.emplace_back();
+        auto piece = [&](int32_t k, int ta, int tb) {
+            P.asm_src.push_back(A->voff[k]);
+            P.asm_r0.push_back(ta * b);
+            P.asm_c0.push_back(tb * b);
+            P.asm_nr.push_back(b);
+            P.asm_nc.push_back(b);
+        };
+        for (int ta = 0; ta < A->ntime; ++ta) {
+            const int r = A->row(e, ta);
+            piece(A->diag[r], ta, ta);
+            for (int32_t k : A->rowblk[r])
+                if (A->kind[k] == CHIDG_BLK_HB && A->ce[k] == e && A->ct[k] != ta) piece(k, ta, A->ct[k]);
+        }
+        P.asm_ptr.push_back((int32_t)P.asm_src.size());
+    }
+    return CHIDG_GPU_OK;
+}
+
 // RAS+ILU0: subdomain s plays MPI rank s.  Local rows in local element order,
 // then the overlap rows received from each neighbour rank, as the reference
 // builds them (RASILU0/type_RASILU0_send_comm.f90:66-275 selects the sent
@@ -1186,7 +1227,9 @@ static int finalize_program(chidg_gpu_ctx* ctx, const chidg_gpu_matrix* A, IluPr
                     t.elem = P.prow_elem[pr];
                     ltasks.push_back(t);
                 }
-                // D = A_diag - sum L * A(parent, itranspose)   (:238-239)
+                // D = A_diag - sum L * A(parent, itranspose)   (:238-239);
+                // assembled rows get their D from k_assemble_rows instead
+                if (P.assembled) continue;
                 bool small = b <= DM_MAX;
                 for (auto& en : P.lo[pr]) small = small && en.nc <= DM_MAX;
                 if (small != (pass == 0)) continue;
@@ -1231,6 +1274,11 @@ static int finalize_program(chidg_gpu_ctx* ctx, const chidg_gpu_matrix* A, IluPr
     P.rows.up_par = (const int32_t*)P.d_up_par.ptr;
     P.rows.up_nc = (const int32_t*)P.d_up_nc.ptr;
     P.sweep_threads = launch_dim_for(SW_GCAP, P.prow_b);
+    if (P.assembled &&
+        ((st = upload_array(ctx, P.d_asm_ptr, P.asm_ptr)) || (st = upload_array(ctx, P.d_asm_src, P.asm_src)) ||
+         (st = upload_array(ctx, P.d_asm_r0, P.asm_r0)) || (st = upload_array(ctx, P.d_asm_c0, P.asm_c0)) ||
+         (st = upload_array(ctx, P.d_asm_nr, P.asm_nr)) || (st = upload_array(ctx, P.d_asm_nc, P.asm_nc))))
+        return st;
     (void)A;
     return CHIDG_GPU_OK;
 }
@@ -1239,7 +1287,8 @@ void chidg::release_program(IluProgram& P) {
     for (Buffer* b : {&P.d_prow_b, &P.d_prow_elem, &P.d_v_off, &P.d_z_off, &P.d_dinv_off, &P.d_lo_ptr, &P.d_lo_L,
                       &P.d_lo_par, &P.d_lo_nc, &P.d_up_ptr, &P.d_up_U, &P.d_up_par, &P.d_up_nc, &P.d_fwd_rows,
                       &P.d_bwd_rows, &P.d_ltasks, &P.d_lpairs, &P.d_stasks, &P.d_spairs, &P.d_tf_row, &P.d_tf_ent,
-                      &P.d_tb_row, &P.d_tb_ent, &P.d_poff_f, &P.d_poff_b, &P.d_sb_row, &P.d_sb_ent})
+                      &P.d_tb_row, &P.d_tb_ent, &P.d_poff_f, &P.d_poff_b, &P.d_sb_row, &P.d_sb_ent, &P.d_asm_ptr,
+                      &P.d_asm_src, &P.d_asm_r0, &P.d_asm_c0, &P.d_asm_nr, &P.d_asm_nc})
         release(*b);
 }
 
@@ -1250,16 +1299,18 @@ static int build_programme(chidg_gpu_precon* M, chidg_gpu_matrix* A) {
     chidg_gpu_ctx* ctx = M->ctx;
     chidg_gpu_matrix* S = A;
     int st;
-    if (M->kind != CHIDG_PRECON_RASILU0 && (st = matrix_op(A, &S))) return st;
+    const bool own = M->kind == CHIDG_PRECON_RASILU0 || M->kind == CHIDG_PRECON_HB;   // built from A itself
+    if (!own && (st = matrix_op(A, &S))) return st;
     std::string err;
     st = (M->kind == CHIDG_PRECON_RASILU0) ? build_rasilu0(S, M->P, err)
+         : (M->kind == CHIDG_PRECON_HB)    ? build_hb(S, M->P, err)
                                            : build_ilu0(S, M->kind == CHIDG_PRECON_JACOBI, M->P, err);
     if (st) { release_program(M->P); return fail(ctx, st, err); }
     if ((st = finalize_program(ctx, S, M->P))) { release_program(M->P); return st; }
     const size_t sync_bytes = sizeof(unsigned) * (2 + 4 * (size_t)M->P.nprow);
     if ((st = ensure(ctx, M->sync, sync_bytes))) { release_program(M->P); return st; }
     cudaMemsetAsync(M->sync.ptr, 0, sync_bytes, ctx->stream);
-    M->built_transposed = A->transposed && M->kind != CHIDG_PRECON_RASILU0;
+    M->built_transposed = A->transposed && !own;
     return CHIDG_GPU_OK;
 }
 
@@ -1267,10 +1318,13 @@ static int build_programme(chidg_gpu_precon* M, chidg_gpu_matrix* A) {
 // of a transposed A.  RASILU0 with a transposed A is an error, as in the
 // reference ("transpose not implemented for 'native' containers",
 // precon_RASILU0.f90:254,494).
+// precon_HB reads A's own blocks whether or not A is transposed, as the
+// reference does (precon_HB.f90:169-310 does not consult A%transposed).
 static int precon_source(chidg_gpu_precon* M, chidg_gpu_matrix** S) {
     chidg_gpu_matrix* A = M->A;
     if (A->transposed && M->kind == CHIDG_PRECON_RASILU0)
         return fail(M->ctx, CHIDG_GPU_EINVAL, "RASILU0: transpose not implemented for 'native' containers");
+    if (M->kind == CHIDG_PRECON_HB) { *S = A; return CHIDG_GPU_OK; }
     return matrix_op(A, S);
 }
 
@@ -1279,7 +1333,7 @@ extern "C" int chidg_gpu_precon_create(chidg_gpu_matrix* A, int32_t kind, chidg_
     *out = nullptr;
     chidg_gpu_ctx* ctx = A->ctx;
     cudaSetDevice(ctx->device);
-    if (kind < CHIDG_PRECON_IDENTITY || kind > CHIDG_PRECON_RASILU0) return fail(ctx, CHIDG_GPU_EINVAL, "precon_create: unknown kind");
+    if (kind < CHIDG_PRECON_IDENTITY || kind > CHIDG_PRECON_HB) return fail(ctx, CHIDG_GPU_EINVAL, "precon_create: unknown kind");
     auto* M = new chidg_gpu_precon();
     M->ctx = ctx;
     M->A = A;
@@ -1412,7 +1466,7 @@ extern "C" int chidg_gpu_precon_update(chidg_gpu_precon* M, chidg_gpu_matrix* A,
     int st;
     chidg_gpu_matrix* user = A;
     if ((st = precon_source(M, &A))) return st;          // from here on A is the matrix factored (A or A^T)
-    if (M->kind != CHIDG_PRECON_RASILU0 && M->built_transposed != user->transposed) {
+    if (M->kind != CHIDG_PRECON_RASILU0 && M->kind != CHIDG_PRECON_HB && M->built_transposed != user->transposed) {
         // the transposed flag changed since the programme was built
         cudaStreamSynchronize(ctx->stream);
         release_program(M->P);
@@ -1427,7 +1481,7 @@ extern "C" int chidg_gpu_precon_update(chidg_gpu_precon* M, chidg_gpu_matrix* A,
     // error would otherwise leave them out of step)
     if (M->sync.ptr)
         cudaMemsetAsync((unsigned*)M->sync.ptr + 2 + P.nprow, 0, sizeof(unsigned) * 3 * (size_t)P.nprow, ctx->stream);
-    if ((precision == CHIDG_GPU_MIXED_FP32 || precision == CHIDG_GPU_MIXED_BF16) && P.max_b <= SF_MAX) {
+    if ((precision == CHIDG_GPU_MIXED_FP32 || precision == CHIDG_GPU_MIXED_BF16) && P.max_b <= SF_MAX && !P.assembled) {
         // the inner solves only read FP32 / BF16 factors: compute them in FP32
         if ((st = factor_fp32(M, A, precision))) return st;
         cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
@@ -1447,6 +1501,14 @@ extern "C" int chidg_gpu_precon_update(chidg_gpu_precon* M, chidg_gpu_matrix* A,
     // one CTA per output block on the FP64 tensor cores for blocks up to 136 x 136
     if ((st = raise_smem_limit((const void*)k_task_gemm_dmma<double, double, double>, DM_SMEM))) return fail(ctx, st, "factor GEMM shared memory");
     const int ph = prof_begin(ctx, kProfFactor);
+    if (P.assembled) {
+        k_assemble_rows<<<P.nprow, 256, 0, ctx->stream>>>((double*)M->LD.ptr, (const int64_t*)P.d_dinv_off.ptr,
+                                                         (const int32_t*)P.d_prow_b.ptr, (const double*)A->val.ptr,
+                                                         (const int32_t*)P.d_asm_ptr.ptr, (const int64_t*)P.d_asm_src.ptr,
+                                                         (const int32_t*)P.d_asm_r0.ptr, (const int32_t*)P.d_asm_c0.ptr,
+                                                         (const int32_t*)P.d_asm_nr.ptr, (const int32_t*)P.d_asm_nc.ptr);
+        if ((st = check_launch(ctx, "k_assemble_rows"))) return st;
+    }
     for (int l = 0; l < nlev; ++l) {
         const int pg = prof_begin(ctx, kProfFactorGemm);
         const int nl = P.ltask_ptr[l + 1] - P.ltask_ptr[l], nld = P.ltask_dmma[l + 1];
@@ -1844,6 +1906,8 @@ extern "C" int chidg_gpu_precon_download_LD(chidg_gpu_precon* M, double* host) {
     chidg_gpu_matrix* A = M->A;
     if (M->kind == CHIDG_PRECON_IDENTITY || M->stamp == 0) return fail(ctx, CHIDG_GPU_ESTATE, "download_LD: no factors");
     if (!M->ld64_valid) return fail(ctx, CHIDG_GPU_ESTATE, "download_LD: the factors were computed in FP32 (mixed precision)");
+    if (M->kind == CHIDG_PRECON_HB)
+        return fail(ctx, CHIDG_GPU_EINVAL, "download_LD: the HB preconditioner's element blocks span time levels");
     if (M->kind != CHIDG_PRECON_RASILU0 && M->built_transposed) A = A->T;   // factors of A^T, in A^T's block order
     std::vector<double> ld((size_t)M->P.ld_size);
     cudaError_t e = cudaMemcpyAsync(ld.data(), M->LD.ptr, sizeof(double) * ld.size(), cudaMemcpyDeviceToHost, ctx->stream);

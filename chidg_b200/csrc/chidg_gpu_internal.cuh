@@ -63,6 +63,12 @@ struct IluProgram {
     Buffer d_tf_row, d_tf_ent, d_tb_row, d_tb_ent, d_poff_f, d_poff_b;
     int ntask_sb = 0;                          // streamed backward sweep: U tasks + inv(D) tasks
     Buffer d_sb_row, d_sb_ent;
+    // rows whose D is assembled from several blocks of A (precon_HB) instead
+    // of starting from one diagonal block: pieces per row, placed at (r0, c0)
+    bool assembled = false;
+    std::vector<int32_t> asm_ptr, asm_r0, asm_c0, asm_nr, asm_nc;
+    std::vector<int64_t> asm_src;
+    Buffer d_asm_ptr, d_asm_src, d_asm_r0, d_asm_c0, d_asm_nr, d_asm_nc;
     std::vector<int> inv_seg_ptr;
     Buffer d_prow_b, d_prow_elem, d_v_off, d_z_off, d_dinv_off, d_lo_ptr, d_lo_L, d_lo_par, d_lo_nc, d_up_ptr,
         d_up_U, d_up_par, d_up_nc, d_fwd_rows, d_bwd_rows, d_ltasks, d_lpairs, d_stasks, d_spairs;

@@ -319,6 +319,33 @@ static __global__ void __launch_bounds__(256)
 }
 
 // ---------------------------------------------------------------------------
+// D blocks assembled from several blocks of A (precon_HB): one CTA per
+// programme row zeroes its B x B slot in LD and copies each piece (a block of
+// A, nr x nc, column-major) to rows r0.., columns c0.. of it.
+// ---------------------------------------------------------------------------
+static __global__ void __launch_bounds__(256)
+    k_assemble_rows(double* __restrict__ LD, const int64_t* __restrict__ dinv_off, const int32_t* __restrict__ prow_b,
+                    const double* __restrict__ Aval, const int32_t* __restrict__ piece_ptr,
+                    const int64_t* __restrict__ piece_src, const int32_t* __restrict__ piece_r0,
+                    const int32_t* __restrict__ piece_c0, const int32_t* __restrict__ piece_nr,
+                    const int32_t* __restrict__ piece_nc) {
+    const int pr = blockIdx.x;
+    const int B = prow_b[pr];
+    double* D = LD + dinv_off[pr];
+    for (int64_t i = threadIdx.x; i < (int64_t)B * B; i += blockDim.x) D[i] = 0.0;
+    __syncthreads();
+    for (int q = piece_ptr[pr]; q < piece_ptr[pr + 1]; ++q) {
+        const int nr = piece_nr[q], r0 = piece_r0[q], c0 = piece_c0[q];
+        const int64_t cnt = (int64_t)nr * piece_nc[q];
+        const double* S = Aval + piece_src[q];
+        for (int64_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+            const int r = (int)(i % nr), c = (int)(i / nr);
+            D[(int64_t)(r0 + r) + (int64_t)(c0 + c) * B] = S[i];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // ILU programme: factorisation
 // ---------------------------------------------------------------------------
 struct GemmTask {            // C(m x n) = [Cinit] + sgn * sum_q A_q(m x k_q) B_q(k_q x n)

@@ -59,6 +59,8 @@ extern "C" {
 #define CHIDG_PRECON_JACOBI   1   /* 'jacobi'   */
 #define CHIDG_PRECON_ILU0     2   /* 'ilu0'     */
 #define CHIDG_PRECON_RASILU0  3   /* 'rasilu0'  */
+#define CHIDG_PRECON_HB       4   /* 'HB' (precon_HB.f90): per element the inverse of its block over all time
+                                     levels (DIAG blocks and hb_blks); element blocks up to 1024 rows */
 
 /* ---- precision modes ----------------------------------------------------- */
 #define CHIDG_GPU_FP64        0   /* everything FP64 (the plain GPU path)               */
@@ -202,6 +204,26 @@ int chidg_gpu_matrix_stamp(chidg_gpu_matrix* A, int64_t* stamp);
  * flag changed rebuilds its programme at its next update. */
 int chidg_gpu_matrix_set_transposed(chidg_gpu_matrix* A, int32_t transposed);
 int chidg_gpu_matrix_get_transposed(chidg_gpu_matrix* A, int32_t* transposed);
+/* chidg_matrix%to_file (:1451-1507): the LOCAL blocks as text, one line per
+ * entry, " irow,icol,nblk,value" with each field centred in 25 columns as
+ * messenger%write_line writes them (integers in I10, values in F24.14 for
+ * 0.1 < |v| < 1e9 and in E24.14 otherwise), 1-based irow = b (ielem-1) + i,
+ * icol = b (ielement_g-1) + j with b the block's row count, nblk the row's
+ * LOCAL block count; time levels, elements and blocks in storage order, each
+ * block column by column.  Like the reference it assumes one block size for
+ * all elements and writes no time offset. */
+int chidg_gpu_matrix_to_file(chidg_gpu_matrix* A, const char* path);
+/* No counterpart in the reference: a binary image of the matrix (pattern,
+ * transposed flag and packed FP64 values, little-endian) that
+ * chidg_gpu_matrix_load reads back without loss into a new matrix. */
+int chidg_gpu_matrix_save(chidg_gpu_matrix* A, const char* path);
+int chidg_gpu_matrix_load(chidg_gpu_ctx* ctx, const char* path, chidg_gpu_matrix** out);
+/* The pattern the matrix was created with (arrays sized nelem / nblocks;
+ * any output may be NULL). */
+int chidg_gpu_matrix_get_pattern(chidg_gpu_matrix* A, int32_t* nelem, int32_t* ntime, int64_t* nblocks,
+                                 int32_t* elem_nvars, int32_t* elem_nterms, int32_t* elem_proc,
+                                 int32_t* blk_row_elem, int32_t* blk_row_time, int32_t* blk_col_elem,
+                                 int32_t* blk_col_time, int32_t* blk_kind);
 
 /* ---- chidg_vector_t (src/containers/type_chidg_vector.f90) --------------- */
 int chidg_gpu_vector_create(chidg_gpu_matrix* A, chidg_gpu_vector** out);

@@ -14,6 +14,7 @@
 //   precon_jacobi update/apply              src/preconditioners/precon_jacobi.f90:95-215
 //   precon_ILU0 update/apply                src/preconditioners/precon_ILU0.f90:111-411
 //   precon_RASILU0 update/apply             src/preconditioners/RASILU0/precon_RASILU0.f90:205-625
+//   precon_HB update/apply                  src/preconditioners/precon_HB.f90:169-310
 //     overlap set / ordering / transposes   .../RASILU0/type_RASILU0_send_comm.f90:66-275,
 //                                           .../RASILU0/type_RASILU0_recv_dom_comm.f90:59-305
 //   fgmres_t%solve, CGS, MGS                src/linear_solvers/type_fgmres.f90:81-442
@@ -587,6 +588,48 @@ struct PreconRAS : Precon {
     }
 };
 
+// precon_HB (precon_HB.f90:169-310): per element one matrix over all its time
+// levels, the DIAG block of level t at (t, t) and D(ta,tb) mass per field at
+// (ta, tb), inverted (inv) and applied to the element's whole segment.  The
+// hb_blks block of row (e,ta) and column (e,tb) holds D(ta,tb) mass per field
+// (type_harmonic_balance.f90:127-229), so it is the (ta, tb) entry here.  Like
+// the reference, A's own blocks are used whether or not A is transposed.
+struct PreconHB : Precon {
+    vector<vector<double>> inv;        // per element, (nt*b)^2 column-major
+    int update(Mat& A) override {
+        err_elem = -1;
+        inv.assign(A.nelem, {});
+        for (int e = 0; e < A.nelem; ++e) {
+            const int b = A.bsize(e), B = b * A.ntime;
+            vector<double>& M = inv[e];
+            M.assign((size_t)B * B, 0.0);
+            auto put = [&](int k, int ta, int tb) {
+                const double* src = A.blk(k);
+                for (int j = 0; j < b; ++j)
+                    for (int i = 0; i < b; ++i) M[(size_t)(ta * b + i) + (size_t)(tb * b + j) * B] = src[i + (size_t)j * b];
+            };
+            for (int ta = 0; ta < A.ntime; ++ta) {
+                put(A.diag[A.row(e, ta)], ta, ta);
+                for (int k : A.rowblk[A.row(e, ta)])
+                    if (A.kind[k] == ORC_BLK_HB && A.ce[k] == e && A.ct[k] != ta) put(k, ta, A.ct[k]);
+            }
+            if (inv_inplace(B, M.data()) != 0) { err_elem = e; return ORC_ESINGULAR; }
+        }
+        stamp = A.stamp;
+        return ORC_OK;
+    }
+    int apply(Mat& A, const double* v, double* z) override {
+        for (int e = 0; e < A.nelem; ++e) {
+            const int B = A.bsize(e) * A.ntime;
+            const double* ve = v + A.eoff[e];
+            double* ze = z + A.eoff[e];
+            std::fill(ze, ze + B, 0.0);
+            gemv_acc(B, B, inv[e].data(), ve, ze);
+        }
+        return ORC_OK;
+    }
+};
+
 // ---------------------------------------------------------------------------
 // Vector kernels
 // ---------------------------------------------------------------------------
@@ -880,6 +923,7 @@ orc_precon* orc_precon_create(orc_matrix* h, int32_t kind) {
         case ORC_PRECON_IDENTITY: pc->p.reset(new PreconIdentity()); break;
         case ORC_PRECON_JACOBI: { auto* q = new PreconILU0(); q->jacobi = true; q->build(h->m); pc->p.reset(q); break; }
         case ORC_PRECON_ILU0: { auto* q = new PreconILU0(); q->build(h->m); pc->p.reset(q); break; }
+        case ORC_PRECON_HB: pc->p.reset(new PreconHB()); break;
         case ORC_PRECON_RASILU0: {
             if (h->m.ntime != 1) { delete pc; return nullptr; }
             auto* q = new PreconRAS(); q->build(h->m); pc->p.reset(q); break;

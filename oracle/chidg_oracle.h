@@ -34,7 +34,7 @@ typedef struct orc_matrix orc_matrix;
 typedef struct orc_precon orc_precon;
 
 enum { ORC_BLK_LOCAL = 0, ORC_BLK_CHIMERA = 1, ORC_BLK_BC = 2, ORC_BLK_HB = 3 };
-enum { ORC_PRECON_IDENTITY = 0, ORC_PRECON_JACOBI = 1, ORC_PRECON_ILU0 = 2, ORC_PRECON_RASILU0 = 3 };
+enum { ORC_PRECON_IDENTITY = 0, ORC_PRECON_JACOBI = 1, ORC_PRECON_ILU0 = 2, ORC_PRECON_RASILU0 = 3, ORC_PRECON_HB = 4 };
 enum { ORC_OK = 0, ORC_EINVAL = 1, ORC_ESINGULAR = 3 };
 
 typedef struct {

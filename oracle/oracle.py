@@ -20,8 +20,8 @@ I64P = C.POINTER(C.c_int64)
 DP = C.POINTER(C.c_double)
 VP = C.c_void_p
 
-IDENTITY, JACOBI, ILU0, RASILU0 = 0, 1, 2, 3
-PRECON_NAMES = {"identity": IDENTITY, "jacobi": JACOBI, "ilu0": ILU0, "rasilu0": RASILU0}
+IDENTITY, JACOBI, ILU0, RASILU0, HB = 0, 1, 2, 3, 4
+PRECON_NAMES = {"identity": IDENTITY, "jacobi": JACOBI, "ilu0": ILU0, "rasilu0": RASILU0, "hb": HB}
 
 
 class Opts(C.Structure):
@@ -197,3 +197,73 @@ def inv(a):
     if st:
         raise ArithmeticError("inv: Matrix is numerically singular!")
     return out
+
+
+# ---------------------------------------------------------------------------
+# chidg_matrix%to_file (src/containers/type_chidg_matrix.f90:1451-1507) with
+# messenger%write_line's formatting (src/tools/messenger.f90:505-640, 695-790)
+# ---------------------------------------------------------------------------
+def _fortran_fixed(s: str, w: int = 24) -> str:
+    return "*" * w if len(s) > w else s.rjust(w)
+
+
+def fortran_F(v: float, w: int = 24, d: int = 14) -> str:
+    """Fw.d: [-]digits.d-digits, right-justified, asterisks when too wide."""
+    return _fortran_fixed(f"{v:.{d}f}", w)
+
+
+def fortran_E(v: float, w: int = 24, d: int = 14) -> str:
+    """Ew.d: [-]0.d-digits then E+dd (|exp| <= 99) or +ddd (<= 999)."""
+    if v != v:
+        return _fortran_fixed("NaN", w)
+    if v in (float("inf"), float("-inf")):
+        return _fortran_fixed("Infinity" if v > 0 else "-Infinity", w)
+    if v == 0.0:
+        mant, exp10 = "0" * d, 0
+    else:
+        m, e = f"{abs(v):.{d - 1}e}".split("e")
+        mant, exp10 = m.replace(".", ""), int(e) + 1
+    sign = "-" if v < 0 else ""
+    ex = f"E{'-' if exp10 < 0 else '+'}{abs(exp10):02d}" if abs(exp10) <= 99 else f"{'-' if exp10 < 0 else '+'}{abs(exp10):03d}"
+    return _fortran_fixed(f"{sign}0.{mant}{ex}", w)
+
+
+def _column(s: str, width: int = 25) -> str:
+    s = s.strip()
+    while len(s) < width:
+        s = " " + s + " "
+    return s[:width]
+
+
+def _real_field(v: float) -> str:
+    a = abs(v)
+    if a < 0.1:
+        s = fortran_E(v)
+    elif 0.1 < a < 1.e9:
+        s = fortran_F(v)
+    else:
+        s = fortran_E(v)
+    return _column(s)
+
+
+def to_file_text(pat, vals) -> str:
+    """The file chidg_matrix%to_file writes for this pattern and these values:
+    per time level, element and LOCAL block (storage order) the entries column
+    by column, list-directed (one leading blank), fields joined by ','."""
+    voff, _ = pat.value_offsets()
+    nr, nc = pat.block_dims()
+    out = []
+    for t in range(pat.ntime):
+        for e in range(pat.nelem):
+            ks = [k for k in range(pat.nblocks) if pat.blk_kind[k] == 0 and pat.blk_row_elem[k] == e
+                  and pat.blk_row_time[k] == t]
+            nblk = _column(str(len(ks)))
+            for k in ks:
+                b, c = int(nr[k]), int(nc[k])
+                r0, c0 = 1 + b * e, 1 + b * int(pat.blk_col_elem[k])
+                blk = vals[voff[k]:voff[k] + b * c]
+                for j in range(c):
+                    for i in range(b):
+                        out.append(" " + ",".join([_column(str(r0 + i)), _column(str(c0 + j)), nblk,
+                                                    _real_field(float(blk[i + j * b]))]) + "\n")
+    return "".join(out)
