@@ -325,6 +325,42 @@ def run_adjoint_leg(ctx, stream, A, b, schedule, reps=3):
     return out
 
 
+def run_hb_leg(ctx, stream, schedule, reps=3):
+    """The harmonic-balance system of the serving requests (8^3 P1, 7 time
+    levels, hb_blks coupling every pair of levels): FGMRES(30) to rtol 1e-8,
+    FP64, with ILU0 per time level and with precon_HB (per-element inverse
+    over all levels)."""
+    import torch
+
+    from chidg_b200 import api, mesh
+    pat = mesh.box_pattern(8, 8, 8, NVARS, mesh.nterms_of_order(1), ntime=7)
+    A = api.ChidgMatrix(pat, ctx)
+    A.upload(mesh.synth_values(pat, seed=SEED_A + 7))
+    b = api.ChidgVector(A, mesh.synth_vector(pat.vector_size(), seed=SEED_B + 7))
+    out = {"workload": "8^3 hex box, 5 fields, P1, 7 time levels (40x40 blocks, 280x280 element blocks over the "
+                       "levels), FGMRES(30) to rtol 1e-8, FP64"}
+    for kind in ("ilu0", "hb"):
+        M = api.create_preconditioner(kind, schedule=schedule)
+        solver = api.create_linear_solver("fgmres", **{**SOLVER, "nkrylov": 30})
+        x = api.ChidgVector(A)
+        solver.solve(A, x, b, M)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            solver.solve(A, x, b, M)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        out[kind] = {"solves_per_s": 1000.0 / ms, "ms_per_solve": ms, "iterations": solver.niter,
+                     "true_rel_residual": solver.residual_norm / solver.r0norm_initial}
+        M.tear_down()
+        x.release()
+    b.release()
+    A.release()
+    return out
+
+
 CFG3 = (32, 32, 32)
 CFG3_SUB = (4, 4, 4)
 CFG3_SOLVER = dict(tol=0.0, rtol=1e-8, nkrylov=30, inner_fgmres=0, nmax=600, orthogonalization="CGS",
@@ -578,6 +614,7 @@ def run_gpu(args):
         M = api.create_preconditioner("ilu0", schedule=args.schedule)   # drop low-precision factors
 
     adjoint = run_adjoint_leg(ctx, stream, A, b, args.schedule) if not args.no_adjoint else None
+    hb = run_hb_leg(ctx, stream, args.schedule) if not args.no_hb else None
     batch = run_batch_leg(ctx, args.schedule) if not args.no_batch else None
     serving = run_serve_leg(local) if not args.no_serve else None
     cfg3 = None
@@ -641,6 +678,7 @@ def run_gpu(args):
         "batch": batch,
         "serving": serving,
         "adjoint": adjoint,
+        "harmonic_balance": hb,
         "cfg3": cfg3,
         "cpu_baseline": cpu,
     }
@@ -661,6 +699,7 @@ def main():
                     help="schedule of the ILU sweeps")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (A^T) solve leg")
+    ap.add_argument("--no-hb", action="store_true", help="skip the harmonic-balance preconditioner leg")
     ap.add_argument("--no-cfg3", action="store_true", help="skip the 32^3 P2 legs (ILU0 and RAS, FP64 and mixed)")
     args = ap.parse_args()
     if args.impl == "reference":
