@@ -16,7 +16,7 @@ module chidg_gpu_mod
                                  CHIDG_GPU_ECUDA = 7, CHIDG_GPU_ESTATE = 8
     integer(c_int), parameter :: CHIDG_BLK_LOCAL = 0, CHIDG_BLK_CHIMERA = 1, CHIDG_BLK_BC = 2, CHIDG_BLK_HB = 3
     integer(c_int), parameter :: CHIDG_PRECON_IDENTITY = 0, CHIDG_PRECON_JACOBI = 1, &
-                                 CHIDG_PRECON_ILU0 = 2, CHIDG_PRECON_RASILU0 = 3
+                                 CHIDG_PRECON_ILU0 = 2, CHIDG_PRECON_RASILU0 = 3, CHIDG_PRECON_HB = 4
     integer(c_int), parameter :: CHIDG_GPU_FP64 = 0, CHIDG_GPU_MIXED_FP32 = 1, CHIDG_GPU_MIXED_BF16 = 2
 
     type, bind(c) :: chidg_gpu_pattern
@@ -102,6 +102,23 @@ module chidg_gpu_mod
             import :: c_int, c_ptr, c_int32_t
             type(c_ptr), value :: mat
             integer(c_int32_t) :: transposed
+        end function
+        ! chidg_matrix%to_file (type_chidg_matrix.f90:1451-1507); path NUL-terminated
+        integer(c_int) function chidg_gpu_matrix_to_file(mat, path) bind(c, name='chidg_gpu_matrix_to_file')
+            import :: c_int, c_ptr, c_char
+            type(c_ptr), value     :: mat
+            character(kind=c_char) :: path(*)
+        end function
+        integer(c_int) function chidg_gpu_matrix_save(mat, path) bind(c, name='chidg_gpu_matrix_save')
+            import :: c_int, c_ptr, c_char
+            type(c_ptr), value     :: mat
+            character(kind=c_char) :: path(*)
+        end function
+        integer(c_int) function chidg_gpu_matrix_load(ctx, path, mat) bind(c, name='chidg_gpu_matrix_load')
+            import :: c_int, c_ptr, c_char
+            type(c_ptr), value     :: ctx
+            character(kind=c_char) :: path(*)
+            type(c_ptr)            :: mat
         end function
         integer(c_int) function chidg_gpu_vector_create(mat, vec) bind(c, name='chidg_gpu_vector_create')
             import :: c_int, c_ptr
