@@ -38,7 +38,7 @@ int upload_vec(chidg_gpu_ctx* ctx, Buffer& b, const std::vector<T>& v) {
     int st = ensure(ctx, b, std::max<size_t>(sizeof(T) * v.size(), sizeof(T)));
     if (st) return st;
     if (!v.empty()) {
-        const cudaError_t e = cudaMemcpy(b.ptr, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
+        const cudaError_t e = cudaMemcpyAsync(b.ptr, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, ctx->stream);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "batch set-up");
     }
     return CHIDG_GPU_OK;

@@ -32,19 +32,52 @@ int chidg::check_launch(chidg_gpu_ctx* ctx, const char* what) {
     if (e != cudaSuccess) return cuda_fail(ctx, e, what);
     return CHIDG_GPU_OK;
 }
+// One stream-ordered memory pool per device for every buffer of the library.
+// Allocation and free are ordered on the owning context's stream, so neither
+// waits for the device (cudaMalloc / cudaFree synchronise it, which made
+// concurrent contexts, e.g. the worker slots of a server, wait for each
+// other).  Up to 4 GB of freed memory stays in the pool for the next
+// allocations; a stream does not wait on another stream's frees to reuse memory.
+static cudaMemPool_t device_pool(int dev) {
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = pools.find(dev);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+    uint64_t keep = (uint64_t)4 << 30;          // the attribute is a 64-bit unsigned value
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    int no = 0;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no);
+    pools[dev] = pool;
+    return pool;
+}
+
 int chidg::ensure(chidg_gpu_ctx* ctx, Buffer& buf, size_t bytes) {
     if (buf.bytes >= bytes && buf.ptr) return CHIDG_GPU_OK;
-    if (buf.ptr) { cudaFree(buf.ptr); buf.ptr = nullptr; buf.bytes = 0; }
+    if (buf.ptr) { cudaFreeAsync(buf.ptr, buf.stream); buf.ptr = nullptr; buf.bytes = 0; }
     if (bytes == 0) return CHIDG_GPU_OK;
+    cudaMemPool_t pool = device_pool(ctx->device);
+    if (!pool) return fail(ctx, CHIDG_GPU_ECUDA, "no stream-ordered memory pool on this device");
     // 256 bytes of slack past the end: bulk copies rounded out to 16-byte
     // boundaries may read up to 15 bytes beyond the last element
-    const cudaError_t e = cudaMalloc(&buf.ptr, bytes + 256);
-    if (e != cudaSuccess) { cudaGetLastError(); return fail(ctx, CHIDG_GPU_ENOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed"); }
+    const cudaError_t e = cudaMallocFromPoolAsync(&buf.ptr, bytes + 256, pool, ctx->stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        buf.ptr = nullptr;
+        return fail(ctx, CHIDG_GPU_ENOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed");
+    }
     buf.bytes = bytes;
+    buf.stream = ctx->stream;
     return CHIDG_GPU_OK;
 }
 void chidg::release(Buffer& buf) {
-    if (buf.ptr) cudaFree(buf.ptr);
+    if (buf.ptr) cudaFreeAsync(buf.ptr, buf.stream);
     buf.ptr = nullptr;
     buf.bytes = 0;
 }
@@ -200,6 +233,7 @@ extern "C" int chidg_gpu_ctx_destroy(chidg_gpu_ctx* ctx) {
     for (Buffer* b : {&ctx->batch.cstart, &ctx->batch.csys, &ctx->batch.sys_chunk, &ctx->batch.sys_row, &ctx->batch.d_out,
                       &ctx->batch.d_coef, &ctx->batch.d_scale, &ctx->batch.partial, &ctx->batch.rowsq})
         release(*b);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);   // the frees above are ordered on this stream
     if (ctx->d_status) cudaFree(ctx->d_status);
     if (ctx->d_scal) cudaFree(ctx->d_scal);
     if (ctx->h_scal) cudaFreeHost(ctx->h_scal);
@@ -248,7 +282,8 @@ static int upload_array(chidg_gpu_ctx* ctx, Buffer& buf, const std::vector<T>& v
     int st = ensure(ctx, buf, std::max<size_t>(sizeof(T) * v.size(), sizeof(T)));
     if (st) return st;
     if (v.empty()) return CHIDG_GPU_OK;
-    const cudaError_t e = cudaMemcpy(buf.ptr, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
+    // from pageable memory: staged before the call returns, so v may go
+    const cudaError_t e = cudaMemcpyAsync(buf.ptr, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, ctx->stream);
     return e == cudaSuccess ? CHIDG_GPU_OK : cuda_fail(ctx, e, "pattern upload");
 }
 
@@ -482,8 +517,8 @@ extern "C" int chidg_gpu_matrix_scale_diagonal(chidg_gpu_matrix* A, const double
         release(dm); release(ds); release(dmo); release(dso);
         return st;
     }
-    cudaMemcpy(dm.ptr, mass, sizeof(double) * m, cudaMemcpyHostToDevice);
-    cudaMemcpy(ds.ptr, scale, sizeof(double) * s, cudaMemcpyHostToDevice);
+    cudaMemcpyAsync(dm.ptr, mass, sizeof(double) * m, cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(ds.ptr, scale, sizeof(double) * s, cudaMemcpyHostToDevice, ctx->stream);
     k_scale_diagonal<<<A->nrow, 256, 0, ctx->stream>>>((double*)A->val.ptr, (const int64_t*)A->d_diag_voff.ptr,
                                                       (const int32_t*)A->d_elem_nvars.ptr, (const int32_t*)A->d_elem_nterms.ptr,
                                                       (const int64_t*)dmo.ptr, (const double*)dm.ptr, (const double*)ds.ptr,
@@ -708,6 +743,9 @@ extern "C" int chidg_gpu_vector_create(chidg_gpu_matrix* A, chidg_gpu_vector** o
     int st = ensure(ctx, x->buf, sizeof(double) * (size_t)x->n);
     if (st) { delete x; return st; }
     cudaMemsetAsync(x->buf.ptr, 0, sizeof(double) * (size_t)x->n, ctx->stream);
+    // the buffer is stream-ordered on ctx->stream; callers may use its device
+    // pointer (chidg_gpu_vector_device_ptr) on streams of their own
+    cudaStreamSynchronize(ctx->stream);
     *out = x;
     return CHIDG_GPU_OK;
 }

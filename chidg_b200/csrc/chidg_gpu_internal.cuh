@@ -14,9 +14,12 @@
 
 namespace chidg {
 
+// Device memory from the stream-ordered pool of its device, allocated and
+// freed on the stream of the context that owns it (the only stream that uses it).
 struct Buffer {
     void* ptr = nullptr;
     size_t bytes = 0;
+    cudaStream_t stream = nullptr;
 };
 
 // device scalar slots (ctx->d_scal): results of reductions read by the host

@@ -92,11 +92,16 @@ class Server:
 
     def close(self):
         """Finish the queued requests, then stop the dispatcher and wait for the
-        batches still on the GPU (no library call may outlive the server)."""
+        batches still on the GPU (no library call may outlive the server).  The
+        slot contexts are released here: left to the garbage collector, their
+        release (which frees device and page-locked memory, a device-wide
+        synchronisation) could land in the middle of another server's work."""
         self._queue.put((None, None))
         self._dispatcher.join(timeout=600)
         for t in list(self._workers):
             t.join(timeout=600)
+        while not self._slot_ctx.empty():
+            self._slot_ctx.get_nowait().close()
 
     # -- internals ----------------------------------------------------------
     def _dispatch(self):
