@@ -23,25 +23,35 @@ def main():
     ap.add_argument("--schedule", default="stream", choices=["tasks", "stream", "dataflow", "levels"])
     ap.add_argument("--time", action="store_true", help="print CUDA-event times per kernel class")
     ap.add_argument("--solves", type=int, default=0, help="also time this many full solves per precision mode")
+    ap.add_argument("--transposed", action="store_true", help="set A%%transposed (products and factors of A^T)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed_fp32", "mixed_bf16", "mixed_precon_fp32"],
+                    help="precision of the preconditioner update (mixed_fp32 / mixed_bf16 factor in FP32 and skip "
+                         "the FP64 apply)")
     args = ap.parse_args()
     pat = mesh.box_pattern(args.n, args.n, args.n, 5, mesh.nterms_of_order(args.p))
     A = api.ChidgMatrix(pat)
     A.upload(mesh.synth_values(pat, seed=1))
+    if args.transposed:
+        A.transposed = True
     v = api.ChidgVector(A, mesh.synth_vector(A.n, seed=2))
     z = api.ChidgVector(A)
     M = api.create_preconditioner(args.precon, schedule=args.schedule)
+    fp64_apply = args.precision in ("fp64", "mixed_precon_fp32")
+
+    def round_():
+        M.update(A, precision=args.precision)
+        if fp64_apply:
+            M.apply(A, v, z)
+        api.chidg_mv(A, v, z)
+
     if args.time:
         # one untimed round first: launch set-up (function attributes,
         # occupancy queries) happens on the first call of each kernel
-        M.update(A)
-        M.apply(A, v, z)
-        api.chidg_mv(A, v, z)
+        round_()
         A.ctx.sync()
         A.ctx.set_profiling(True)
     for _ in range(args.reps):
-        M.update(A)
-        M.apply(A, v, z)
-        api.chidg_mv(A, v, z)
+        round_()
     A.ctx.sync()
     print(f"profile_case n={args.n} p={args.p} schedule={args.schedule}: {A.ctx.launches()} launches")
     if args.time:
