@@ -84,7 +84,7 @@ def factor_flops(pat):
 # 24^3 workload is too large for a multi-pass capture), scaled to a launch of
 # the workload by its block count.  ilu_apply = both streamed sweeps.
 TRAFFIC_14CUBE_BLOCKS = 18032
-TRAFFIC_14CUBE = {"ilu_apply": 1.118791e9 + 13.724928e6 + 1.520100e9 + 18.709248e6}
+TRAFFIC_14CUBE = {"ilu_apply": 1.119160e9 + 14.508288e6 + 1.520102e9 + 14.406656e6}
 
 
 def measured_traffic(kind, pat):
