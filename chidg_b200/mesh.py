@@ -147,6 +147,19 @@ def box_pattern(nx: int, ny: int, nz: int, nvars: int, nterms: int, ntime: int =
         shape=(nx, ny, nz), extra={"subdomains": tuple(subdomains)})
 
 
+def with_element_orders(pat: BlockPattern, orders) -> BlockPattern:
+    """The same block pattern with a polynomial order per element (ragged
+    blocks: a block coupling orders p and q is nterms(p)*nvars rows by
+    nterms(q)*nvars columns)."""
+    orders = np.asarray(orders)
+    nterms = np.array([nterms_of_order(int(o)) for o in orders], dtype=np.int32)
+    return BlockPattern(nelem=pat.nelem, ntime=pat.ntime, elem_nvars=pat.elem_nvars.copy(), elem_nterms=nterms,
+                        elem_proc=pat.elem_proc.copy(), blk_row_elem=pat.blk_row_elem.copy(),
+                        blk_row_time=pat.blk_row_time.copy(), blk_col_elem=pat.blk_col_elem.copy(),
+                        blk_col_time=pat.blk_col_time.copy(), blk_kind=pat.blk_kind.copy(), blk_face=pat.blk_face.copy(),
+                        shape=pat.shape, extra=dict(pat.extra))
+
+
 def nterms_of_order(p: int) -> int:
     """Legendre tensor basis size (P+1)^3 (src/chidg/type_chidg.f90:572)."""
     return (p + 1) ** 3

@@ -267,3 +267,38 @@ def test_hb_precon_reduces_hb_residual():
     x, res = O.fgmres(A, O.OraclePrecon(A, "hb"), b, O.default_opts(tol=0.0, rtol=1e-10, nkrylov=40, inner_fgmres=0,
                                                                      nmax=400))
     assert res["residual_norm"] <= 1e-9 * res["r0norm_initial"]
+
+
+def test_ragged_orders_match_dense():
+    """Elements of orders 0, 1 and 2 in one matrix (non-square coupling
+    blocks): matvec, block ILU0 (dense restatement on element slices) and FGMRES."""
+    base = mesh.box_pattern(3, 3, 2, 5, mesh.nterms_of_order(1))
+    pat = mesh.with_element_orders(base, [(e * 7) % 3 for e in range(base.nelem)])
+    vals = mesh.synth_values(pat, seed=85)
+    A = O.OracleMatrix(pat)
+    A.set_values(vals)
+    D = dense(pat, vals)
+    x = mesh.synth_vector(A.n, seed=86)
+    assert np.allclose(A.mv(x), D @ x, rtol=1e-13, atol=1e-13)
+    eo = pat.elem_offsets()
+    sl = [slice(eo[e], eo[e + 1]) for e in range(pat.nelem)]
+    local = {(int(pat.blk_row_elem[k]), int(pat.blk_col_elem[k])) for k in range(pat.nblocks) if pat.blk_kind[k] == 0}
+    Dinv, L = {}, {}
+    for r in range(pat.nelem):
+        Dr = D[sl[r], sl[r]].copy()
+        for c in sorted(c for (rr, c) in local if rr == r and c < r):
+            L[(r, c)] = D[sl[r], sl[c]] @ Dinv[c]
+            Dr -= L[(r, c)] @ D[sl[c], sl[r]]
+        Dinv[r] = np.linalg.inv(Dr)
+    z = mesh.synth_vector(A.n, seed=87)
+    v = z.copy()
+    for r in range(pat.nelem):
+        for c in sorted(c for (rr, c) in local if rr == r and c < r):
+            z[sl[r]] -= L[(r, c)] @ z[sl[c]]
+    for r in reversed(range(pat.nelem)):
+        for c in sorted(c for (rr, c) in local if rr == r and c > r):
+            z[sl[r]] -= D[sl[r], sl[c]] @ z[sl[c]]
+        z[sl[r]] = Dinv[r] @ z[sl[r]]
+    M = O.OraclePrecon(A, "ilu0")
+    M.update()
+    assert np.allclose(M.apply(v), z, rtol=1e-11, atol=1e-12)
