@@ -1436,6 +1436,15 @@ static int launch_inverse(chidg_gpu_precon* M, int row_begin, int count, int cls
 // inverses in FP64 (the products' D blocks are written in FP64, inverted by the
 // tensor-core kernel and copied to FP32 per wavefront).  Only the FP32 (and
 // BF16) factors are produced; LD's FP64 L blocks are not.
+// CHIDG_FACTOR32_SIMT=1 selects the FP32 SIMT products (comparison runs)
+static bool factor32_simt_env() {
+    static const bool v = [] {
+        const char* e = std::getenv("CHIDG_FACTOR32_SIMT");
+        return e && e[0] == '1';
+    }();
+    return v;
+}
+
 static int factor_fp32(chidg_gpu_precon* M, chidg_gpu_matrix* A, int precision) {
     chidg_gpu_ctx* ctx = M->ctx;
     IluProgram& P = M->P;
@@ -1445,8 +1454,11 @@ static int factor_fp32(chidg_gpu_precon* M, chidg_gpu_matrix* A, int precision) 
     if ((st = ensure(ctx, M->LD, sizeof(double) * (size_t)P.ld_size)) ||
         (st = ensure(ctx, M->LD32, sizeof(float) * (size_t)P.ld_size)))
         return st;
+    const bool simt = factor32_simt_env();
     if ((st = raise_smem_limit((const void*)k_task_gemm_f32<float>, SF_SMEM)) ||
-        (st = raise_smem_limit((const void*)k_task_gemm_f32<double>, SF_SMEM)))
+        (st = raise_smem_limit((const void*)k_task_gemm_f32<double>, SF_SMEM)) ||
+        (st = raise_smem_limit((const void*)k_task_gemm_tf32<float>, ST_SMEM)) ||
+        (st = raise_smem_limit((const void*)k_task_gemm_tf32<double>, ST_SMEM)))
         return fail(ctx, st, "FP32 factor GEMM shared memory");
     const int nlev = (int)P.fwd_ptr.size() - 1;
     const float* A32 = (const float*)A->val32.ptr;
@@ -1456,18 +1468,26 @@ static int factor_fp32(chidg_gpu_precon* M, chidg_gpu_matrix* A, int precision) 
     for (int l = 0; l < nlev; ++l) {
         const int pg = prof_begin(ctx, kProfFactorGemm);
         const int nl = P.ltask_ptr[l + 1] - P.ltask_ptr[l];
+        const GemmTask* lt = (const GemmTask*)P.d_ltasks.ptr + P.ltask_ptr[l];
+        const GemmTask* stt = (const GemmTask*)P.d_stasks.ptr + P.stask_ptr[l];
         if (nl > 0) {
-            k_task_gemm_f32<float><<<nl, 256, SF_SMEM, ctx->stream>>>((const GemmTask*)P.d_ltasks.ptr + P.ltask_ptr[l],
-                                                                     (const GemmPair*)P.d_lpairs.ptr, A32, L32, nullptr,
-                                                                     L32, 1.0);
-            if ((st = check_launch(ctx, "k_task_gemm_f32 L"))) return st;
+            if (simt)
+                k_task_gemm_f32<float><<<nl, 256, SF_SMEM, ctx->stream>>>(lt, (const GemmPair*)P.d_lpairs.ptr, A32, L32,
+                                                                         nullptr, L32, 1.0);
+            else
+                k_task_gemm_tf32<float><<<nl, ST_THREADS, ST_SMEM, ctx->stream>>>(lt, (const GemmPair*)P.d_lpairs.ptr, A32,
+                                                                                 L32, nullptr, L32, 1.0);
+            if ((st = check_launch(ctx, "factor L products (FP32 / TF32)"))) return st;
         }
         const int ns = P.stask_ptr[l + 1] - P.stask_ptr[l];
         if (ns > 0) {
-            k_task_gemm_f32<double><<<ns, 256, SF_SMEM, ctx->stream>>>((const GemmTask*)P.d_stasks.ptr + P.stask_ptr[l],
-                                                                      (const GemmPair*)P.d_spairs.ptr, L32, A32,
-                                                                      (const double*)A->val.ptr, LD, -1.0);
-            if ((st = check_launch(ctx, "k_task_gemm_f32 S"))) return st;
+            if (simt)
+                k_task_gemm_f32<double><<<ns, 256, SF_SMEM, ctx->stream>>>(stt, (const GemmPair*)P.d_spairs.ptr, L32, A32,
+                                                                          (const double*)A->val.ptr, LD, -1.0);
+            else
+                k_task_gemm_tf32<double><<<ns, ST_THREADS, ST_SMEM, ctx->stream>>>(stt, (const GemmPair*)P.d_spairs.ptr, L32,
+                                                                                  A32, (const double*)A->val.ptr, LD, -1.0);
+            if ((st = check_launch(ctx, "factor S products (FP32 / TF32)"))) return st;
         }
         prof_end(ctx, pg);
         const int pi = prof_begin(ctx, kProfFactorInv);

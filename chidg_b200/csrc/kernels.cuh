@@ -649,6 +649,114 @@ __global__ void __launch_bounds__(256, 1) k_task_gemm_f32(const GemmTask* __rest
     }
 }
 
+// The same products on the tensor cores: mma.sync m16n8k8 with TF32 operands
+// (rounded to nearest from the FP32 blocks) and FP32 accumulation.  One
+// 144 x 144 output tile per CTA, 9 warps in a 3 x 3 grid of 48 x 48 regions
+// (3 x 6 MMA tiles each).  K chunks of 32 in two cp.async stages: A stored
+// [k][m] (leading dimension 152) and B stored [n][k] (leading dimension 36),
+// so that the staging writes and the fragment reads are both free of bank
+// conflicts.  Bounds: loads past m, n or k are zero-filled, stores are guarded.
+constexpr int ST_LDA = 152, ST_LDB = 36, ST_THREADS = 288;
+constexpr size_t ST_STAGE = (size_t)SF_KC * ST_LDA + (size_t)SF_MAX * ST_LDB;   // floats per stage
+constexpr size_t ST_SMEM = 2 * sizeof(float) * ST_STAGE;
+__device__ __forceinline__ unsigned to_tf32(float x) {
+    unsigned r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ void mma_tf32_16x8x8(float (&d)[4], const unsigned (&a)[4], const unsigned (&b)[2]) {
+    asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+template <typename TC>
+__global__ void __launch_bounds__(ST_THREADS, 1) k_task_gemm_tf32(const GemmTask* __restrict__ tasks, const GemmPair* __restrict__ pairs,
+                                                                  const float* Abase, const float* Bbase, const double* Cinit,
+                                                                  TC* Cbase, double sgn) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float* S = reinterpret_cast<float*>(smem_raw);          // 2 stages x {A [SF_KC][ST_LDA], B [SF_MAX][ST_LDB]}
+    const GemmTask t = tasks[blockIdx.x];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, tig = lane & 3;
+    const int wm = (warp / 3) * 48, wn = (warp % 3) * 48;    // this warp's region
+    float acc[3][6][4];
+    #pragma unroll
+    for (int i = 0; i < 3; ++i)
+        #pragma unroll
+        for (int j = 0; j < 6; ++j)
+            #pragma unroll
+            for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0f;
+    int nchunk = 0;
+    for (int q = t.q_begin; q < t.q_end; ++q) nchunk += (pairs[q].k + SF_KC - 1) / SF_KC;
+    int lq = t.q_begin, lk0 = 0;
+    auto issue = [&](int stage) {
+        const GemmPair pr = pairs[lq];
+        const float* A = Abase + pr.a_off;        // m x k, column-major
+        const float* B = Bbase + pr.b_off;        // k x n, column-major
+        const int kc = min(SF_KC, pr.k - lk0);
+        float* as = S + stage * ST_STAGE;
+        float* bs = as + SF_KC * ST_LDA;
+        for (int idx = tid; idx < SF_KC * SF_MAX; idx += ST_THREADS) {   // A: consecutive m, coalesced
+            const int kk = idx / SF_MAX, i = idx % SF_MAX;
+            const bool ok = i < t.m && kk < kc;
+            cp_async4(as + kk * ST_LDA + i, ok ? (const void*)(A + i + (int64_t)(lk0 + kk) * t.m) : (const void*)A, ok);
+        }
+        for (int idx = tid; idx < SF_MAX * SF_KC; idx += ST_THREADS) {   // B: consecutive k, coalesced
+            const int j = idx / SF_KC, kk = idx % SF_KC;
+            const bool ok = j < t.n && kk < kc;
+            cp_async4(bs + j * ST_LDB + kk, ok ? (const void*)(B + (lk0 + kk) + (int64_t)j * pr.k) : (const void*)B, ok);
+        }
+        cp_async_commit();
+        lk0 += SF_KC;
+        if (lk0 >= pr.k) { ++lq; lk0 = 0; }
+    };
+    if (nchunk > 0) issue(0);
+    for (int c = 0; c < nchunk; ++c) {
+        if (c + 1 < nchunk) { issue((c + 1) & 1); cp_async_wait<1>(); }
+        else cp_async_wait<0>();
+        __syncthreads();
+        const float* as = S + (c & 1) * ST_STAGE;
+        const float* bs = as + SF_KC * ST_LDA;
+        #pragma unroll
+        for (int k0 = 0; k0 < SF_KC; k0 += 8) {   // a short last chunk is zero-filled
+            unsigned af[3][4], bf[6][2];
+            #pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const float* ap = as + (k0 + tig) * ST_LDA + wm + 16 * i + g;
+                af[i][0] = to_tf32(ap[0]);
+                af[i][1] = to_tf32(ap[8]);
+                af[i][2] = to_tf32(ap[4 * ST_LDA]);
+                af[i][3] = to_tf32(ap[4 * ST_LDA + 8]);
+            }
+            #pragma unroll
+            for (int j = 0; j < 6; ++j) {
+                const float* bp = bs + (wn + 8 * j + g) * ST_LDB + k0 + tig;
+                bf[j][0] = to_tf32(bp[0]);
+                bf[j][1] = to_tf32(bp[4]);
+            }
+            #pragma unroll
+            for (int i = 0; i < 3; ++i)
+                #pragma unroll
+                for (int j = 0; j < 6; ++j) mma_tf32_16x8x8(acc[i][j], af[i], bf[j]);
+        }
+        __syncthreads();                          // stage (c & 1) is refilled two chunks later
+    }
+    #pragma unroll
+    for (int i = 0; i < 3; ++i)
+        #pragma unroll
+        for (int j = 0; j < 6; ++j)
+            #pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int row = wm + 16 * i + g + ((r & 2) ? 8 : 0);
+                const int col = wn + 8 * j + 2 * tig + (r & 1);
+                if (row >= t.m || col >= t.n) continue;
+                const int64_t o = row + (int64_t)col * t.m;
+                double v = sgn * (double)acc[i][j][r];
+                if (t.cinit_off >= 0) v = Cinit[t.cinit_off + o] + v;
+                Cbase[t.c_off + o] = from_d<TC>(v);
+            }
+}
+
 // FP32 copies of the inverted diagonal blocks of some programme rows (one CTA
 // per row): the inverses of a wavefront, for the next wavefront's FP32 products
 // and the FP32 sweeps
