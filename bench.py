@@ -374,6 +374,33 @@ def run_hb_leg(ctx, stream, schedule, reps=3):
     return out
 
 
+def run_newton_leg(ctx):
+    """Whole Newton solve of five steps on the 8^3 P1 box (cfg1's size): the
+    Newton driver (pseudo-transient continuation, backtracking) over a
+    synthetic nonlinear system with the ChiDG block layout, R(q) = A0 (q - q*)
+    + c (q - q*)^2, assembled on the host; each step's linear solve is
+    FGMRES(30) + ILU0 to rtol 1e-8 in FP64."""
+    from chidg_b200 import api, mesh
+    from chidg_b200.newton import Newton, SyntheticSystem
+    pat = mesh.box_pattern(8, 8, 8, NVARS, mesh.nterms_of_order(1))
+    sysm = SyntheticSystem(pat, seed=SEED_A + 11, root_seed=SEED_B + 11)
+    A = api.ChidgMatrix(pat, ctx)
+    out = {"workload": "8^3 hex box, 5 fields, P1 (40x40 blocks): 5 Newton steps on a synthetic nonlinear system "
+                       "(host assembly), PTC cfl0 10, backtracking, FGMRES(30)+ILU0 to rtol 1e-8 per step, FP64"}
+    for rep in range(2):                              # the first run warms up
+        q = api.ChidgVector(A)
+        solver = api.create_linear_solver("fgmres", **{**SOLVER, "nkrylov": 30})
+        res = Newton(nmax=5, tol=0.0, rtol=0.0, cfl0=10.0).solve(sysm, q, A, solver,
+                                                                api.create_preconditioner("ilu0"))
+        q.release()
+    out.update({"seconds_whole_newton": res.seconds, "steps": res.niter,
+                "seconds_linear_solves": float(sum(res.linear_seconds)),
+                "residual_history": [float(r) for r in res.residual_norm],
+                "linear_iterations": res.matrix_iterations, "alphas": res.alphas})
+    A.release()
+    return out
+
+
 CFG3 = (32, 32, 32)
 CFG3_SUB = (4, 4, 4)
 CFG3_SOLVER = dict(tol=0.0, rtol=1e-8, nkrylov=30, inner_fgmres=0, nmax=600, orthogonalization="CGS",
@@ -628,6 +655,7 @@ def run_gpu(args):
 
     adjoint = run_adjoint_leg(ctx, stream, A, b, args.schedule) if not args.no_adjoint else None
     hb = run_hb_leg(ctx, stream, args.schedule) if not args.no_hb else None
+    newton = run_newton_leg(ctx) if not args.no_newton else None
     batch = run_batch_leg(ctx, args.schedule) if not args.no_batch else None
     serving = run_serve_leg(local) if not args.no_serve else None
     cfg3 = None
@@ -692,6 +720,7 @@ def run_gpu(args):
         "serving": serving,
         "adjoint": adjoint,
         "harmonic_balance": hb,
+        "newton": newton,
         "cfg3": cfg3,
         "cpu_baseline": cpu,
     }
@@ -713,6 +742,7 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (A^T) solve leg")
     ap.add_argument("--no-hb", action="store_true", help="skip the harmonic-balance preconditioner leg")
+    ap.add_argument("--no-newton", action="store_true", help="skip the whole-Newton leg (8^3 P1, 5 steps)")
     ap.add_argument("--no-cfg3", action="store_true", help="skip the 32^3 P2 legs (ILU0 and RAS, FP64 and mixed)")
     args = ap.parse_args()
     if args.impl == "reference":

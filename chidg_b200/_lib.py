@@ -96,6 +96,7 @@ PROTOTYPES = {
     "chidg_gpu_vector_norm": (C.c_int, [VP, DP]),
     "chidg_gpu_dot_noalloc": (C.c_int, [C.c_int, VP, VP, C.c_int64, VP, VP]),
     "chidg_gpu_matvec": (C.c_int, [VP, VP, VP]),
+    "chidg_gpu_vector_norm_fields": (C.c_int, [VP, VP, C.c_int32]),
     "chidg_gpu_precon_create": (C.c_int, [VP, C.c_int32, C.POINTER(VP)]),
     "chidg_gpu_precon_destroy": (C.c_int, [VP]),
     "chidg_gpu_precon_update": (C.c_int, [VP, VP, C.c_int32]),

@@ -275,6 +275,48 @@ class ChidgVector:
         self.ctx.check(self.ctx.L.chidg_gpu_vector_norm(self.h, C.byref(out)), "vector_norm")
         return out.value
 
+    def norm_fields(self, nfields: int | None = None) -> np.ndarray:
+        """chidg_vector%norm_fields: the L2 norm of each field over all elements,
+        time levels and modes (every element with the same field count)."""
+        nf = int(self.A.pattern.elem_nvars[0]) if nfields is None else int(nfields)
+        out = np.empty(nf)
+        self.ctx.check(self.ctx.L.chidg_gpu_vector_norm_fields(self.h, _ptr(out), nf), "vector_norm_fields")
+        return out
+
+    # chidg_vector_t's overloaded operators (type_chidg_vector.f90:1740-2084):
+    # each returns a new vector
+    def _new_copy(self) -> "ChidgVector":
+        out = ChidgVector(self.A)
+        out.copy_from(self)
+        return out
+
+    def __add__(self, other: "ChidgVector") -> "ChidgVector":
+        out = self._new_copy()
+        out.axpy(1.0, other)
+        return out
+
+    def __sub__(self, other: "ChidgVector") -> "ChidgVector":
+        out = self._new_copy()
+        out.axpy(-1.0, other)
+        return out
+
+    def __neg__(self) -> "ChidgVector":
+        out = self._new_copy()
+        out.scale(-1.0)
+        return out
+
+    def __mul__(self, a: float) -> "ChidgVector":
+        out = self._new_copy()
+        out.scale(float(a))
+        return out
+
+    __rmul__ = __mul__
+
+    def __truediv__(self, a: float) -> "ChidgVector":
+        out = self._new_copy()
+        out.scale(1.0 / float(a))
+        return out
+
     def release(self):
         if getattr(self, "h", None):
             self.ctx.L.chidg_gpu_vector_destroy(self.h)

@@ -831,6 +831,27 @@ extern "C" int chidg_gpu_vector_norm(const chidg_gpu_vector* x, double* out) {
     *out = std::sqrt(s);
     return CHIDG_GPU_OK;
 }
+// chidg_vector%norm_fields (type_chidg_vector.f90:1319-1352): per field the
+// L2 norm over all elements, time levels and modes.  Every element must have
+// nfields fields.
+extern "C" int chidg_gpu_vector_norm_fields(const chidg_gpu_vector* x, double* out, int32_t nfields) {
+    if (!x || !out || nfields <= 0 || nfields > 32) return CHIDG_GPU_EINVAL;
+    chidg_gpu_matrix* A = x->A;
+    chidg_gpu_ctx* ctx = x->ctx;
+    cudaSetDevice(ctx->device);
+    for (int e = 0; e < A->nelem; ++e)
+        if (A->nvars[e] != nfields) return fail(ctx, CHIDG_GPU_EINVAL, "norm_fields: an element with another field count");
+    const int grid = std::max(1, std::min(A->nrow, ctx->nsm * 4));
+    int st = ensure(ctx, ctx->partial2, sizeof(double) * (size_t)grid * nfields);
+    if (st) return st;
+    k_field_sumsq<<<grid, 256, 0, ctx->stream>>>((const double*)x->buf.ptr, (const int64_t*)A->d_row_yoff.ptr,
+                                                (const int32_t*)A->d_elem_nterms.ptr, A->nrow, A->ntime, nfields,
+                                                (double*)ctx->partial2.ptr);
+    if ((st = check_launch(ctx, "k_field_sumsq"))) return st;
+    if ((st = reduce_partials(ctx, (const double*)ctx->partial2.ptr, grid, nfields, kSlotFields, true))) return st;
+    return fetch_scalars(ctx, kSlotFields, nfields, out);
+}
+
 extern "C" int chidg_gpu_matvec(chidg_gpu_matrix* A, const chidg_gpu_vector* x, chidg_gpu_vector* y) {
     if (!A || !x || !y || x->n != A->n || y->n != A->n || x == y) return CHIDG_GPU_EINVAL;
     cudaSetDevice(A->ctx->device);

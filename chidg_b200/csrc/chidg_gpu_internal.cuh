@@ -31,7 +31,8 @@ constexpr int kSlotR0 = 3;         // ||r0||^2
 constexpr int kSlotStatus = 4;     // int status word of the dataflow sweeps (nonzero = a wait ran out)
 constexpr long long kSpinLimit = 2000000000LL;   // clock cycles a sweep waits for a parent (~1 s)
 constexpr int kSlotH = 16;         // h(1:j, j) of the current pass (up to 4000 entries)
-constexpr int kSlotY = 4096;       // y coefficients of the solution update
+constexpr int kSlotY = 4096;       // y coefficients of the solution update (up to 4000 entries)
+constexpr int kSlotFields = 8160;  // per-field norms (up to 32 fields)
 constexpr int kMaxKrylov = 4000;   // restart length bound set by the slots above
 
 template <typename T> struct AccOf { using type = double; };

@@ -202,6 +202,26 @@ static __global__ void k_reduce_partials(const double* __restrict__ partial, int
         __syncthreads();
     }
 }
+// sumsqr_fields (type_densevector.f90:806-830) summed over the elements
+// (type_domain_vector.f90:495-511): CTA c adds, for every field, the squares
+// of the modes of rows c, c + gridDim.x, ... (row = element and time level)
+// and writes partial[f * gridDim.x + c]; every sum runs in a fixed order.
+static __global__ void k_field_sumsq(const double* __restrict__ x, const int64_t* __restrict__ row_yoff,
+                                     const int32_t* __restrict__ elem_nterms, int nrow, int ntime, int nfields,
+                                     double* __restrict__ partial) {
+    __shared__ double scratch[32];
+    for (int f = 0; f < nfields; ++f) {
+        double s = 0.0;
+        for (int r = blockIdx.x; r < nrow; r += gridDim.x) {
+            const int nt = elem_nterms[r / ntime];
+            const double* seg = x + row_yoff[r] + (int64_t)f * nt;
+            for (int m = threadIdx.x; m < nt; m += blockDim.x) s += seg[m] * seg[m];
+        }
+        s = block_sum(s, scratch);
+        if (threadIdx.x == 0) partial[(int64_t)f * gridDim.x + blockIdx.x] = s;
+        __syncthreads();
+    }
+}
 // w[i] = w[i] - sum_q h[q] * v_q[i]  (CGS update, h on device), with sum of squares partials
 template <typename T>
 __global__ void k_maxpy_sub_norm(int64_t n, T* __restrict__ w, const T* __restrict__ v, int64_t vstride,

@@ -186,9 +186,10 @@ int chidg_gpu_matrix_download(chidg_gpu_matrix* A, double* host);
 /* chidg_matrix%clear (:841): zero all blocks, bump the stamp. */
 int chidg_gpu_matrix_clear(chidg_gpu_matrix* A);
 /* chidg_matrix%scale_diagonal (:769-792), the pseudo-transient term: for
- * every element e and time t, add scale[e] * mass_e to each field's
+ * every element e, field f and time t, add scale[e,f] * mass_e to field f's
  * nterms x nterms diagonal sub-block of the DIAG block.  mass is packed per
- * element, nterms*nterms column-major; bump the stamp. */
+ * element, nterms*nterms column-major; scale holds nvars(e) entries per
+ * element, elements in order; bump the stamp. */
 int chidg_gpu_matrix_scale_diagonal(chidg_gpu_matrix* A, const double* mass,
                                     const double* scale);
 int chidg_gpu_matrix_stamp(chidg_gpu_matrix* A, int64_t* stamp);
@@ -243,6 +244,10 @@ int chidg_gpu_vector_scale(chidg_gpu_vector* x, double a);                      
 /* operator_chidg_dot.f90:30-97 (dot) and type_chidg_vector.f90:1237-1305 (norm) */
 int chidg_gpu_vector_dot(const chidg_gpu_vector* x, const chidg_gpu_vector* y, double* out);
 int chidg_gpu_vector_norm(const chidg_gpu_vector* x, double* out);
+/* chidg_vector%norm_fields (:1319-1352, sumsqr_fields of type_densevector.f90:
+ * 806-830): out[f] = sqrt(sum over elements, time levels and modes of field f
+ * squared), f < nfields <= 32; every element must have nfields fields. */
+int chidg_gpu_vector_norm_fields(const chidg_gpu_vector* x, double* out, int32_t nfields);
 
 /* Dot product of two device arrays that allocates no device memory.  It has
  * no counterpart in the reference.  It is for callers that cannot call

@@ -399,3 +399,24 @@ def test_scale_diagonal():
             for f in range(nv):
                 blk[f * nt:(f + 1) * nt, f * nt:(f + 1) * nt] += scale[e, f] * mass[e]
         assert np.allclose(got[voff[k]:voff[k] + b * b].reshape(b, b).T, blk, rtol=1e-15, atol=1e-15)
+
+
+@pytest.mark.parametrize("shape,P,nt", [((3, 2, 2), 1, 1), ((2, 2, 2), 2, 3)])
+def test_norm_fields_and_operators(shape, P, nt):
+    """chidg_vector%norm_fields (per-field L2 norms over elements, time levels
+    and modes) and the overloaded + - * / against numpy."""
+    pat, vals, Ao, Ag = setup(shape, P, nt=nt, seed=111)
+    x = mesh.synth_vector(Ao.n, seed=112)
+    y = mesh.synth_vector(Ao.n, seed=113)
+    xv, yv = api.ChidgVector(Ag, x), api.ChidgVector(Ag, y)
+    nv, nterms = int(pat.elem_nvars[0]), int(pat.elem_nterms[0])
+    per = x.reshape(pat.nelem, nt, nv, nterms)
+    expect = np.sqrt((per ** 2).sum(axis=(0, 1, 3)))
+    assert np.allclose(xv.norm_fields(), expect, rtol=1e-13)
+    assert np.allclose((xv + yv).download(), x + y, rtol=0, atol=0)
+    assert np.allclose((xv - yv).download(), x - y, rtol=0, atol=0)
+    assert np.allclose((2.5 * xv).download(), 2.5 * x, rtol=0, atol=0)
+    assert np.allclose((xv / 4.0).download(), x * 0.25, rtol=0, atol=0)
+    assert np.allclose((-xv).download(), -x, rtol=0, atol=0)
+    with pytest.raises(_lib.ChidgGpuError):
+        xv.norm_fields(nv + 1)
