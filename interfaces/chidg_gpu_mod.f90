@@ -143,6 +143,13 @@ module chidg_gpu_mod
             import :: c_int, c_ptr
             type(c_ptr), value :: mat, x, y
         end function
+        ! chidg_vector%norm_fields (type_chidg_vector.f90:1319-1352)
+        integer(c_int) function chidg_gpu_vector_norm_fields(x, nrm, nfields) bind(c, name='chidg_gpu_vector_norm_fields')
+            import :: c_int, c_ptr, c_double, c_int32_t
+            type(c_ptr),        value :: x
+            real(c_double)            :: nrm(*)
+            integer(c_int32_t), value :: nfields
+        end function
         integer(c_int) function chidg_gpu_vector_norm(x, nrm) bind(c, name='chidg_gpu_vector_norm')
             import :: c_int, c_ptr, c_double
             type(c_ptr), value :: x
