@@ -264,12 +264,27 @@ def serve_requests(count, seed, pinned=True):
     return out
 
 
+def run_serve_subprocess(device, timeout=900):
+    """The serving leg in a fresh process on the same GPU: a request server is
+    a process of its own, and its latencies must not depend on what the earlier
+    legs left in this one (page-locked buffers, cached allocations, garbage)."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--serve-only", "--serve-device", str(device)]
+    try:
+        p = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+    except subprocess.TimeoutExpired:
+        return {"error": "serving leg timed out"}
+    lines = [l for l in p.stdout.splitlines() if l.startswith("{")]
+    if p.returncode != 0 or not lines:
+        return {"error": f"serving leg failed (exit {p.returncode}): {p.stderr.strip().splitlines()[-1:] }"}
+    return json.loads(lines[-1])["serving"]
+
+
 def run_serve_leg(device, requests=64, rate=200.0):
     from chidg_b200 import serve
     out = {"arrival_rate_per_s": rate, "requests": requests, "slots": 2, "max_batch": 16,
            "workload": "Poisson arrivals; boxes 4..8 per side, P in {1,2}; every 10th request harmonic balance "
                        "(8^3, P1, 7 time levels); FGMRES(30)+ILU0 to rtol 1e-8 (FP64 residual); request values "
-                       "in page-locked host memory"}
+                       "in page-locked host memory; the server in a process of its own"}
     for prec in ("fp64", "mixed_precon_fp32"):
         reqs = serve_requests(requests, seed=11)
         srv = serve.Server(device=device, slots=2, max_batch=16, mem_budget=40 << 30, **BATCH_OPTS, precision=prec)
@@ -657,7 +672,7 @@ def run_gpu(args):
     hb = run_hb_leg(ctx, stream, args.schedule) if not args.no_hb else None
     newton = run_newton_leg(ctx) if not args.no_newton else None
     batch = run_batch_leg(ctx, args.schedule) if not args.no_batch else None
-    serving = run_serve_leg(local) if not args.no_serve else None
+    serving = run_serve_subprocess(local) if not args.no_serve else None
     cfg3 = None
     if not args.no_cfg3 and world == 1:
         # the 24^3 objects leave the device first: the 32^3 legs hold ~120 GB
@@ -744,7 +759,14 @@ def main():
     ap.add_argument("--no-hb", action="store_true", help="skip the harmonic-balance preconditioner leg")
     ap.add_argument("--no-newton", action="store_true", help="skip the whole-Newton leg (8^3 P1, 5 steps)")
     ap.add_argument("--no-cfg3", action="store_true", help="skip the 32^3 P2 legs (ILU0 and RAS, FP64 and mixed)")
+    ap.add_argument("--serve-only", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--serve-device", type=int, default=0, help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.serve_only:
+        import torch
+        torch.cuda.set_device(args.serve_device)
+        print(json.dumps({"serving": run_serve_leg(args.serve_device)}), flush=True)
+        return 0
     if args.impl == "reference":
         return run_reference(args)
     return run_gpu(args)
