@@ -269,8 +269,10 @@ def run_serve_subprocess(device, timeout=900):
     a process of its own, and its latencies must not depend on what the earlier
     legs left in this one (page-locked buffers, cached allocations, garbage)."""
     cmd = [sys.executable, os.path.abspath(__file__), "--serve-only", "--serve-device", str(device)]
+    # a server loads its kernels when it starts, not at a request's first use
+    env = dict(os.environ, CUDA_MODULE_LOADING="EAGER")
     try:
-        p = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+        p = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout, env=env)
     except subprocess.TimeoutExpired:
         return {"error": "serving leg timed out"}
     lines = [l for l in p.stdout.splitlines() if l.startswith("{")]
@@ -285,18 +287,23 @@ def run_serve_leg(device, requests=64, rate=200.0):
            "workload": "Poisson arrivals; boxes 4..8 per side, P in {1,2}; every 10th request harmonic balance "
                        "(8^3, P1, 7 time levels); FGMRES(30)+ILU0 to rtol 1e-8 (FP64 residual); request values "
                        "in page-locked host memory; the server in a process of its own"}
-    for prec in ("fp64", "mixed_precon_fp32"):
+    out["server"] = "native (chidg_gpu_serve_*: dispatcher and worker slots as native threads)"
+    for key, cls, prec in (("fp64", serve.NativeServer, "fp64"),
+                           ("mixed_precon_fp32", serve.NativeServer, "mixed_precon_fp32"),
+                           ("python_server_fp64", serve.Server, "fp64")):
         reqs = serve_requests(requests, seed=11)
-        srv = serve.Server(device=device, slots=2, max_batch=16, mem_budget=40 << 30, **BATCH_OPTS, precision=prec)
+        srv = cls(device=device, slots=2, max_batch=16, mem_budget=40 << 30, **BATCH_OPTS, precision=prec)
         try:
-            srv.submit(serve_requests(1, seed=11)[0]).result()    # warm-up
+            # warm-up: a batch of the stream's kinds (P1 and P2 boxes, one harmonic-balance system)
+            for f in [srv.submit(r) for r in serve_requests(10, seed=12)]:
+                f.result()
             st = serve.run_stream(srv, reqs, serve.poisson_arrivals(requests, rate, seed=5))
         finally:
             srv.close()
         res = st.pop("results")
         st["max_true_rel_residual"] = max(r.residual_norm / r.r0norm_initial for r in res)
         st.pop("requests", None)
-        out[prec] = st
+        out[key] = st
     return out
 
 

@@ -50,7 +50,10 @@ static cudaMemPool_t device_pool(int dev) {
     props.location.id = dev;
     cudaMemPool_t pool = nullptr;
     if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) { cudaGetLastError(); return nullptr; }
-    uint64_t keep = (uint64_t)4 << 30;          // the attribute is a 64-bit unsigned value
+    // CHIDG_POOL_KEEP_GB: freed memory the pool keeps for reuse (default 4)
+    double keep_gb = 4.0;
+    if (const char* e = std::getenv("CHIDG_POOL_KEEP_GB")) keep_gb = std::max(0.0, std::atof(e));
+    uint64_t keep = (uint64_t)(keep_gb * (double)(1ull << 30));   // the attribute is a 64-bit unsigned value
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     int no = 0;
     cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no);

@@ -1,0 +1,319 @@
+// serve.cu -- a continuous-batching solve server behind the C ABI.
+//
+// Requests (one assembled system each: pattern, packed block values, right-
+// hand side) are submitted at any time and wait in arrival order.  A
+// dispatcher thread forms a batch whenever a worker slot is free: the oldest
+// request and the ones after it that share its number of time levels, up to
+// max_batch systems and the device-memory budget (a batch of one may exceed
+// it).  Admission waits while the batches on the device already hold the
+// budget.  Each slot is a worker thread with a context (and stream) of its
+// own, so batches run concurrently; a batch is solved by
+// chidg_gpu_fgmres_solve_batched, whose
+// per-system arithmetic does not depend on the other systems of the batch.
+// Host code only: no kernel of its own.
+#include "../../include/chidg_gpu.h"
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace {
+
+struct Request {
+    int64_t ticket = 0;
+    chidg_gpu_pattern pat{};
+    std::vector<int32_t> nvars, nterms, proc, re, rt, ce, ct, kind;
+    const double* values = nullptr;      // caller-owned until the request's wait returns
+    const double* rhs = nullptr;
+    int64_t nval = 0, n = 0, bytes = 0;
+    double arrival = 0, start = 0, finish = 0;
+    int32_t batch_size = 0;
+    std::vector<double> x;
+    chidg_gpu_fgmres_result result{};
+    int status = CHIDG_GPU_OK;
+    std::string error;
+    bool done = false;
+};
+
+struct Job {
+    std::vector<std::shared_ptr<Request>> batch;
+    int64_t bytes = 0;
+};
+
+}  // namespace
+
+struct chidg_gpu_server {
+    int device = 0;
+    int32_t max_batch = 16, precon_kind = CHIDG_PRECON_ILU0;
+    int64_t budget = 0;
+    chidg_gpu_fgmres_opts opts{};
+    std::chrono::steady_clock::time_point t0;
+    std::mutex mu;
+    std::condition_variable cv;              // queue, slots, memory and completion changes
+    std::deque<std::shared_ptr<Request>> pending;
+    std::map<int64_t, std::shared_ptr<Request>> live;   // submitted, not yet waited for
+    std::deque<Job> jobs;                    // formed batches not yet taken by a worker
+    int64_t next_ticket = 0;
+    bool stopping = false;                   // no more submissions; the dispatcher drains the queue
+    bool workers_stop = false;               // the workers exit once the job queue is empty
+    int idle = 0;                            // workers without a batch
+    int64_t mem_used = 0, peak_mem = 0, batches = 0;
+    std::vector<chidg_gpu_ctx*> all_ctx;
+    std::thread dispatcher;
+    std::vector<std::thread> workers;
+
+    double now() const {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+};
+
+namespace {
+
+// device bytes one request needs: A, the factors (at most A), the Krylov
+// basis (V and Z) and a few vectors
+int64_t request_bytes(int64_t nval, int64_t n, int32_t nkrylov) {
+    return 8 * nval * 2 + 8 * n * (2 * ((int64_t)nkrylov + 1) + 6);
+}
+
+void run_batch(chidg_gpu_server* S, chidg_gpu_ctx* ctx, std::vector<std::shared_ptr<Request>> batch, int64_t bytes) {
+    const double start = S->now();
+    const int nsys = (int)batch.size();
+    // the packed pattern: system s owns elements sys_elem[s] .. sys_elem[s+1]-1
+    std::vector<int32_t> nv, nt, pr, re, rt, ce, ct, kd, sys_elem(nsys + 1, 0);
+    int64_t nval = 0, n = 0;
+    for (int s = 0; s < nsys; ++s) {
+        const Request& q = *batch[s];
+        const int32_t e0 = sys_elem[s];
+        nv.insert(nv.end(), q.nvars.begin(), q.nvars.end());
+        nt.insert(nt.end(), q.nterms.begin(), q.nterms.end());
+        pr.insert(pr.end(), q.proc.begin(), q.proc.end());
+        for (size_t k = 0; k < q.re.size(); ++k) {
+            re.push_back(q.re[k] + e0); ce.push_back(q.ce[k] + e0);
+            rt.push_back(q.rt[k]); ct.push_back(q.ct[k]); kd.push_back(q.kind[k]);
+        }
+        sys_elem[s + 1] = e0 + q.pat.nelem;
+        nval += q.nval;
+        n += q.n;
+    }
+    chidg_gpu_pattern pat{};
+    pat.nelem = sys_elem[nsys]; pat.ntime = batch[0]->pat.ntime; pat.nblocks = (int64_t)re.size();
+    pat.elem_nvars = nv.data(); pat.elem_nterms = nt.data(); pat.elem_proc = pr.data();
+    pat.blk_row_elem = re.data(); pat.blk_row_time = rt.data(); pat.blk_col_elem = ce.data();
+    pat.blk_col_time = ct.data(); pat.blk_kind = kd.data();
+
+    chidg_gpu_matrix* A = nullptr;
+    chidg_gpu_vector *b = nullptr, *x = nullptr;
+    chidg_gpu_precon* M = nullptr;
+    std::vector<chidg_gpu_fgmres_result> res(nsys);
+    std::vector<double> xh;
+    int st = chidg_gpu_matrix_create(ctx, &pat, &A);
+    if (!st) {
+        int64_t v0 = 0;
+        for (int s = 0; s < nsys && !st; ++s) { st = chidg_gpu_matrix_upload_range(A, batch[s]->values, v0, batch[s]->nval); v0 += batch[s]->nval; }
+    }
+    if (!st) st = chidg_gpu_vector_create(A, &b);
+    if (!st) st = chidg_gpu_vector_create(A, &x);
+    if (!st) {
+        int64_t o = 0;
+        for (int s = 0; s < nsys && !st; ++s) { st = chidg_gpu_vector_upload_range(b, batch[s]->rhs, o, batch[s]->n); o += batch[s]->n; }
+    }
+    if (!st) st = chidg_gpu_precon_create(A, S->precon_kind, &M);
+    if (!st) st = chidg_gpu_fgmres_solve_batched(A, M, nsys, sys_elem.data(), b, x, &S->opts, res.data(), nullptr, 0);
+    if (!st) { xh.resize((size_t)n); st = chidg_gpu_vector_download(x, xh.data()); }
+    std::string err;
+    if (st) {
+        char buf[512] = {0};
+        chidg_gpu_last_error(ctx, buf, (int32_t)sizeof(buf));
+        err = buf;
+    }
+    const double finish = S->now();
+    if (M) chidg_gpu_precon_destroy(M);
+    if (x) chidg_gpu_vector_destroy(x);
+    if (b) chidg_gpu_vector_destroy(b);
+    if (A) chidg_gpu_matrix_destroy(A);
+
+    std::lock_guard<std::mutex> lk(S->mu);
+    int64_t o = 0;
+    for (int s = 0; s < nsys; ++s) {
+        Request& q = *batch[s];
+        q.status = st;
+        q.error = err;
+        q.start = start;
+        q.finish = finish;
+        q.batch_size = nsys;
+        if (!st) {
+            q.result = res[s];
+            q.x.assign(xh.begin() + o, xh.begin() + o + q.n);
+        }
+        o += q.n;
+        q.done = true;
+    }
+    S->mem_used -= bytes;
+    ++S->idle;
+    S->cv.notify_all();
+}
+
+void work(chidg_gpu_server* S, chidg_gpu_ctx* ctx) {
+    std::unique_lock<std::mutex> lk(S->mu);
+    for (;;) {
+        S->cv.wait(lk, [S] { return !S->jobs.empty() || S->workers_stop; });
+        if (S->jobs.empty()) return;         // workers_stop and nothing left
+        Job job = std::move(S->jobs.front());
+        S->jobs.pop_front();
+        lk.unlock();
+        run_batch(S, ctx, std::move(job.batch), job.bytes);
+        lk.lock();
+    }
+}
+
+void dispatch(chidg_gpu_server* S) {
+    std::unique_lock<std::mutex> lk(S->mu);
+    for (;;) {
+        S->cv.wait(lk, [S] { return (!S->pending.empty() && S->idle > 0) || (S->stopping && S->pending.empty()); });
+        if (S->pending.empty()) break;       // stopping, queue drained
+        std::vector<std::shared_ptr<Request>> batch{S->pending.front()};
+        S->pending.pop_front();
+        int64_t bytes = batch[0]->bytes;
+        while (!S->pending.empty() && (int32_t)batch.size() < S->max_batch) {
+            const auto& nxt = S->pending.front();
+            if (bytes + nxt->bytes > S->budget || nxt->pat.ntime != batch[0]->pat.ntime) break;
+            bytes += nxt->bytes;
+            batch.push_back(nxt);
+            S->pending.pop_front();
+        }
+        // admission by device memory: wait for running batches to finish
+        S->cv.wait(lk, [S, bytes] { return S->mem_used + bytes <= S->budget || S->mem_used == 0; });
+        S->mem_used += bytes;
+        S->peak_mem = std::max(S->peak_mem, S->mem_used);
+        ++S->batches;
+        --S->idle;
+        S->jobs.push_back(Job{std::move(batch), bytes});
+        S->cv.notify_all();
+    }
+}
+
+}  // namespace
+
+extern "C" int chidg_gpu_serve_create(int device, int32_t slots, int64_t mem_budget, int32_t max_batch,
+                                      int32_t precon_kind, const chidg_gpu_fgmres_opts* opts, chidg_gpu_server** out) {
+    if (!out || slots < 1 || mem_budget <= 0 || max_batch < 1 || precon_kind < CHIDG_PRECON_IDENTITY ||
+        precon_kind > CHIDG_PRECON_HB)
+        return CHIDG_GPU_EINVAL;
+    *out = nullptr;
+    auto* S = new chidg_gpu_server();
+    S->device = device;
+    S->budget = mem_budget;
+    S->max_batch = max_batch;
+    S->precon_kind = precon_kind;
+    if (opts) S->opts = *opts;
+    else chidg_gpu_fgmres_default_opts(&S->opts);
+    S->t0 = std::chrono::steady_clock::now();
+    for (int i = 0; i < slots; ++i) {
+        chidg_gpu_ctx* c = nullptr;
+        const int st = chidg_gpu_ctx_create(device, nullptr, &c);
+        if (st) {
+            for (chidg_gpu_ctx* d : S->all_ctx) chidg_gpu_ctx_destroy(d);
+            delete S;
+            return st;
+        }
+        S->all_ctx.push_back(c);
+    }
+    S->idle = slots;
+    for (chidg_gpu_ctx* c : S->all_ctx) S->workers.emplace_back(work, S, c);
+    S->dispatcher = std::thread(dispatch, S);
+    *out = S;
+    return CHIDG_GPU_OK;
+}
+
+extern "C" int chidg_gpu_serve_submit(chidg_gpu_server* S, const chidg_gpu_pattern* pat, const double* values,
+                                      const double* rhs, int64_t* ticket) {
+    if (!S || !pat || !values || !rhs || !ticket || pat->nelem <= 0 || pat->ntime <= 0 || pat->nblocks <= 0 ||
+        !pat->elem_nvars || !pat->elem_nterms || !pat->blk_row_elem || !pat->blk_row_time || !pat->blk_col_elem ||
+        !pat->blk_col_time || !pat->blk_kind)
+        return CHIDG_GPU_EINVAL;
+    auto q = std::make_shared<Request>();
+    const int32_t ne = pat->nelem;
+    const int64_t nb = pat->nblocks;
+    q->nvars.assign(pat->elem_nvars, pat->elem_nvars + ne);
+    q->nterms.assign(pat->elem_nterms, pat->elem_nterms + ne);
+    q->proc.assign(ne, 0);
+    if (pat->elem_proc) q->proc.assign(pat->elem_proc, pat->elem_proc + ne);
+    q->re.assign(pat->blk_row_elem, pat->blk_row_elem + nb);
+    q->rt.assign(pat->blk_row_time, pat->blk_row_time + nb);
+    q->ce.assign(pat->blk_col_elem, pat->blk_col_elem + nb);
+    q->ct.assign(pat->blk_col_time, pat->blk_col_time + nb);
+    q->kind.assign(pat->blk_kind, pat->blk_kind + nb);
+    for (int32_t e = 0; e < ne; ++e) {
+        if (q->nvars[e] <= 0 || q->nterms[e] <= 0) return CHIDG_GPU_EINVAL;
+        q->n += (int64_t)pat->ntime * q->nvars[e] * q->nterms[e];
+    }
+    for (int64_t k = 0; k < nb; ++k) {
+        if (q->re[k] < 0 || q->re[k] >= ne || q->ce[k] < 0 || q->ce[k] >= ne) return CHIDG_GPU_EINVAL;
+        q->nval += (int64_t)q->nvars[q->re[k]] * q->nterms[q->re[k]] * q->nvars[q->ce[k]] * q->nterms[q->ce[k]];
+    }
+    q->pat.nelem = pat->nelem;               // the arrays are copied above; keep only the sizes
+    q->pat.ntime = pat->ntime;
+    q->pat.nblocks = pat->nblocks;
+    q->values = values;
+    q->rhs = rhs;
+    q->bytes = request_bytes(q->nval, q->n, S->opts.nkrylov);
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (S->stopping) return CHIDG_GPU_ESTATE;
+    q->arrival = S->now();
+    q->ticket = S->next_ticket++;
+    *ticket = q->ticket;
+    S->live[q->ticket] = q;
+    S->pending.push_back(q);
+    S->cv.notify_all();
+    return CHIDG_GPU_OK;
+}
+
+extern "C" int chidg_gpu_serve_wait(chidg_gpu_server* S, int64_t ticket, double* x, chidg_gpu_fgmres_result* result,
+                                    double* timing) {
+    if (!S) return CHIDG_GPU_EINVAL;
+    std::unique_lock<std::mutex> lk(S->mu);
+    const auto it = S->live.find(ticket);
+    if (it == S->live.end()) return CHIDG_GPU_EINVAL;
+    const std::shared_ptr<Request> q = it->second;
+    S->cv.wait(lk, [&q] { return q->done; });
+    S->live.erase(ticket);
+    if (x && !q->status) std::memcpy(x, q->x.data(), sizeof(double) * q->x.size());
+    if (result) *result = q->result;
+    if (timing) { timing[0] = q->arrival; timing[1] = q->start; timing[2] = q->finish; timing[3] = q->batch_size; }
+    return q->status;
+}
+
+extern "C" int chidg_gpu_serve_stats(chidg_gpu_server* S, int64_t* batches, int64_t* peak_mem_bytes) {
+    if (!S) return CHIDG_GPU_EINVAL;
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (batches) *batches = S->batches;
+    if (peak_mem_bytes) *peak_mem_bytes = S->peak_mem;
+    return CHIDG_GPU_OK;
+}
+
+extern "C" int chidg_gpu_serve_destroy(chidg_gpu_server* S) {
+    if (!S) return CHIDG_GPU_OK;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stopping = true;
+        S->cv.notify_all();
+    }
+    S->dispatcher.join();                    // forms batches for every queued request, then stops
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->workers_stop = true;
+        S->cv.notify_all();
+    }
+    for (std::thread& t : S->workers) t.join();   // each finishes the queued batches first
+    for (chidg_gpu_ctx* c : S->all_ctx) chidg_gpu_ctx_destroy(c);
+    delete S;
+    return CHIDG_GPU_OK;
+}

@@ -24,7 +24,9 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import api, mesh
+import ctypes as C
+
+from . import _lib, api, mesh
 
 
 @dataclass
@@ -183,6 +185,81 @@ class Server:
                 self._mem_lock.notify_all()
             self._slot_ctx.put(ctx)
             self._free.release()
+
+
+class NativeServer:
+    """The same continuous batching with the dispatcher and the worker slots as
+    native threads behind the C ABI (chidg_gpu_serve_*), with the interface of
+    Server.  A request's arrays are handed over by pointer: the returned
+    future keeps them alive until its result has been taken."""
+
+    def __init__(self, device: int = 0, slots: int = 2, mem_budget: int = 60 << 30, max_batch: int = 32,
+                 precon: str = "ilu0", **solver_options):
+        self.L = _lib.lib()
+        self.options = dict(tol=0.0, rtol=1e-8, nkrylov=30, inner_fgmres=False, nmax=1000)
+        self.options.update(solver_options)
+        self._solver = api.FGMRES(**self.options)       # the options struct of the batched solves
+        h = C.c_void_p()
+        self._t0 = time.perf_counter()                 # server timestamps count from its creation
+        st = self.L.chidg_gpu_serve_create(int(device), int(slots), int(mem_budget), int(max_batch),
+                                           api.PRECON_KINDS[precon.lower()], C.byref(self._solver._o), C.byref(h))
+        if st:
+            raise _lib.ChidgGpuError(st, "serve_create")
+        self.h = h
+
+    def submit(self, req: SolveRequest) -> "NativeFuture":
+        values = np.ascontiguousarray(req.values, dtype=np.float64)
+        rhs = np.ascontiguousarray(req.rhs, dtype=np.float64)
+        pat = req.pattern.as_struct()
+        ticket = C.c_int64()
+        st = self.L.chidg_gpu_serve_submit(self.h, C.byref(pat), C.c_void_p(values.ctypes.data),
+                                           C.c_void_p(rhs.ctypes.data), C.byref(ticket))
+        if st:
+            raise _lib.ChidgGpuError(st, "serve_submit")
+        return NativeFuture(self, req, ticket.value, (values, rhs))
+
+    def _stats(self):
+        if getattr(self, "h", None) is None:
+            return self._final_stats                   # recorded by close()
+        b, p = C.c_int64(), C.c_int64()
+        self.L.chidg_gpu_serve_stats(self.h, C.byref(b), C.byref(p))
+        return b.value, p.value
+
+    @property
+    def batches(self) -> int:
+        return self._stats()[0]
+
+    @property
+    def peak_mem_used(self) -> int:
+        return self._stats()[1]
+
+    def close(self):
+        """Solve everything queued, then stop the native threads."""
+        if getattr(self, "h", None):
+            self._final_stats = self._stats()
+            self.L.chidg_gpu_serve_destroy(self.h)
+            self.h = None
+
+
+class NativeFuture:
+    def __init__(self, server: NativeServer, req: SolveRequest, ticket: int, keep):
+        self.server, self.req, self.ticket, self._keep = server, req, ticket, keep
+        self._result = None
+
+    def result(self, timeout=None) -> SolveResult:
+        if self._result is None:
+            x = np.empty(self.req.pattern.vector_size())
+            res = _lib.FgmresResult()
+            timing = (C.c_double * 4)()
+            st = self.server.L.chidg_gpu_serve_wait(self.server.h, self.ticket, C.c_void_p(x.ctypes.data),
+                                                    C.byref(res), timing)
+            self._keep = None                          # the server no longer reads the request's arrays
+            if st:
+                raise _lib.ChidgGpuError(st, "serve_wait")
+            t0 = self.server._t0
+            self._result = SolveResult(x, res.niter, res.residual_norm, res.r0norm_initial, t0 + timing[0],
+                                       t0 + timing[1], t0 + timing[2], int(timing[3]), self.req.tag)
+        return self._result
 
 
 def poisson_arrivals(n: int, rate: float, seed: int = 0) -> np.ndarray:

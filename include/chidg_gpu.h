@@ -328,6 +328,32 @@ int chidg_gpu_fgmres_solve_batched(chidg_gpu_matrix* A, chidg_gpu_precon* M, int
 /* Fill opts with the reference defaults (type_linear_solver.f90:23-40). */
 int chidg_gpu_fgmres_default_opts(chidg_gpu_fgmres_opts* opts);
 
+/* ---- serving (no counterpart in the reference) ----------------------------
+ * A continuous-batching server: requests (pattern, packed block values,
+ * right-hand side) are submitted at any time; a dispatcher batches waiting
+ * requests first come first served (same number of time levels, up to
+ * max_batch systems, admission by a device-memory budget estimate of
+ * 16 nval + 8 n (2 nkrylov + 8) bytes per request) onto `slots` worker
+ * threads, each with its own context and stream, and solves each batch with
+ * chidg_gpu_fgmres_solve_batched (opts; precon_kind a CHIDG_PRECON_*).  A
+ * request's answer does not depend on the other requests of its batch.
+ * submit copies the pattern; values and rhs are read from the caller's
+ * memory until wait returns for that ticket, so they must stay valid and
+ * unchanged until then.  wait blocks until the request is solved, copies x
+ * (the request's vector length) and its result, and timing[0..3] = arrival,
+ * batch start, batch finish (seconds since the server's creation) and the
+ * batch size; it returns the batch's status.  destroy solves everything
+ * queued, then stops. */
+typedef struct chidg_gpu_server chidg_gpu_server;
+int chidg_gpu_serve_create(int device, int32_t slots, int64_t mem_budget, int32_t max_batch,
+                           int32_t precon_kind, const chidg_gpu_fgmres_opts* opts, chidg_gpu_server** out);
+int chidg_gpu_serve_submit(chidg_gpu_server* s, const chidg_gpu_pattern* pat, const double* values,
+                           const double* rhs, int64_t* ticket);
+int chidg_gpu_serve_wait(chidg_gpu_server* s, int64_t ticket, double* x, chidg_gpu_fgmres_result* result,
+                         double* timing);
+int chidg_gpu_serve_stats(chidg_gpu_server* s, int64_t* batches, int64_t* peak_mem_bytes);
+int chidg_gpu_serve_destroy(chidg_gpu_server* s);
+
 #ifdef __cplusplus
 }
 #endif

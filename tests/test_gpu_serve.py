@@ -22,9 +22,13 @@ def make_requests():
     return reqs
 
 
-def test_server_results_match_oracle_and_are_mix_independent():
+SERVERS = [serve.Server, serve.NativeServer]
+
+
+@pytest.mark.parametrize("server", SERVERS)
+def test_server_results_match_oracle_and_are_mix_independent(server):
     reqs = make_requests()
-    srv = serve.Server(slots=2, max_batch=3, **OPTS)
+    srv = server(slots=2, max_batch=3, **OPTS)
     try:
         stats = serve.run_stream(srv, reqs, serve.poisson_arrivals(len(reqs), rate=200.0, seed=1))
         mixed = {r.tag: r for r in stats["results"]}
@@ -44,10 +48,11 @@ def test_server_results_match_oracle_and_are_mix_independent():
         assert np.array_equal(mixed[i].x, alone[i].x)
 
 
-def test_server_admission_respects_memory_budget():
+@pytest.mark.parametrize("server", SERVERS)
+def test_server_admission_respects_memory_budget(server):
     reqs = make_requests()
     one = max(serve.request_bytes(r.pattern, OPTS["nkrylov"]) for r in reqs)
-    srv = serve.Server(slots=3, max_batch=8, mem_budget=one, **OPTS)   # room for about one request at a time
+    srv = server(slots=3, max_batch=8, mem_budget=one, **OPTS)   # room for about one request at a time
     try:
         futs = [srv.submit(r) for r in reqs]
         res = [f.result(timeout=300) for f in futs]
