@@ -97,6 +97,7 @@ PROTOTYPES = {
     "chidg_gpu_dot_noalloc": (C.c_int, [C.c_int, VP, VP, C.c_int64, VP, VP]),
     "chidg_gpu_matvec": (C.c_int, [VP, VP, VP]),
     "chidg_gpu_vector_norm_fields": (C.c_int, [VP, VP, C.c_int32]),
+    "chidg_gpu_selftest_bounded_waits": (C.c_int, [VP, C.c_int64, C.POINTER(C.c_int32)]),
     "chidg_gpu_serve_create": (C.c_int, [C.c_int, C.c_int32, C.c_int64, C.c_int32, C.c_int32, VP, C.POINTER(VP)]),
     "chidg_gpu_serve_submit": (C.c_int, [VP, VP, VP, VP, C.POINTER(C.c_int64)]),
     "chidg_gpu_serve_wait": (C.c_int, [VP, C.c_int64, VP, VP, VP]),

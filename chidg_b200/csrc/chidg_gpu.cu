@@ -834,6 +834,46 @@ extern "C" int chidg_gpu_vector_norm(const chidg_gpu_vector* x, double* out) {
     *out = std::sqrt(s);
     return CHIDG_GPU_OK;
 }
+// Failure detection without a fault: the bounded waits of the streamed
+// kernels (a flag another CTA sets, an mbarrier the producer completes) are
+// made to run out on a flag that nothing sets and an mbarrier that nobody
+// arrives at.  Each gives up after `limit` clock cycles and reports it:
+// bit 0 the flag wait, bit 1 the mbarrier wait.  One thread, one CTA.
+static __global__ void k_bounded_wait_selftest(const unsigned* flag, long long limit, int* bits) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    int b = 0;
+    if (!wait_flag(flag, 0, 1u, limit)) b |= 1;
+    if (!mbar_wait(&bar, 0u, limit)) b |= 2;
+    *bits = b;
+}
+
+extern "C" int chidg_gpu_selftest_bounded_waits(chidg_gpu_ctx* ctx, int64_t limit_cycles, int32_t* bits) {
+    if (!ctx || !bits || limit_cycles <= 0 || limit_cycles > 4000000000LL) return CHIDG_GPU_EINVAL;
+    cudaSetDevice(ctx->device);
+    Buffer flag, out;
+    int st;
+    if ((st = ensure(ctx, flag, 64)) || (st = ensure(ctx, out, sizeof(int)))) { release(flag); release(out); return st; }
+    cudaMemsetAsync(flag.ptr, 0, 64, ctx->stream);
+    k_bounded_wait_selftest<<<1, 32, 0, ctx->stream>>>((const unsigned*)flag.ptr, (long long)limit_cycles, (int*)out.ptr);
+    st = check_launch(ctx, "k_bounded_wait_selftest");
+    int h = 0;
+    if (!st) {
+        cudaError_t e = cudaMemcpyAsync(&h, out.ptr, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) st = cuda_fail(ctx, e, "bounded wait self-test");
+    }
+    release(flag);
+    release(out);
+    *bits = h;
+    return st;
+}
+
 // chidg_vector%norm_fields (type_chidg_vector.f90:1319-1352): per field the
 // L2 norm over all elements, time levels and modes.  Every element must have
 // nfields fields.

@@ -344,6 +344,14 @@ int chidg_gpu_fgmres_default_opts(chidg_gpu_fgmres_opts* opts);
  * batch start, batch finish (seconds since the server's creation) and the
  * batch size; it returns the batch's status.  destroy solves everything
  * queued, then stops. */
+/* Failure detection without a fault (no counterpart in the reference): the
+ * bounded waits the streamed kernels use (on another CTA's flag, on an
+ * mbarrier) are run on a flag that nothing sets and an mbarrier that nobody
+ * arrives at, each with a limit of limit_cycles clock cycles (<= 4e9).
+ * *bits: bit 0 set when the flag wait gave up, bit 1 when the mbarrier wait
+ * did (3: both detected).  The context stays usable. */
+int chidg_gpu_selftest_bounded_waits(chidg_gpu_ctx* ctx, int64_t limit_cycles, int32_t* bits);
+
 typedef struct chidg_gpu_server chidg_gpu_server;
 int chidg_gpu_serve_create(int device, int32_t slots, int64_t mem_budget, int32_t max_batch,
                            int32_t precon_kind, const chidg_gpu_fgmres_opts* opts, chidg_gpu_server** out);

@@ -64,3 +64,12 @@ def test_synth_is_deterministic_and_thread_independent():
     b = mesh.synth_values(pat, seed=1, nthreads=4)
     c = mesh.synth_values(pat, seed=2, nthreads=4)
     assert np.array_equal(a, b) and not np.array_equal(a, c)
+
+
+def test_selftest_argument_checks_need_no_gpu():
+    """The self-test entry refuses bad arguments before touching the device."""
+    import ctypes as C
+    from chidg_b200 import _lib
+    L = _lib.lib()
+    bits = C.c_int32(0)
+    assert L.chidg_gpu_selftest_bounded_waits(None, 1000, C.byref(bits)) == _lib.EINVAL
