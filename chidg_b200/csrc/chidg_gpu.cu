@@ -447,7 +447,8 @@ extern "C" int chidg_gpu_matrix_upload(chidg_gpu_matrix* A, const double* host) 
     if (!A || !host) return CHIDG_GPU_EINVAL;
     chidg_gpu_ctx* ctx = A->ctx;
     cudaSetDevice(ctx->device);
-    const cudaError_t e = cudaMemcpyAsync(A->val.ptr, host, sizeof(double) * (size_t)A->nval, cudaMemcpyHostToDevice, ctx->stream);
+    cudaError_t e = cudaMemcpyAsync(A->val.ptr, host, sizeof(double) * (size_t)A->nval, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);   // host arrays are only read during the call
     if (e != cudaSuccess) return cuda_fail(ctx, e, "matrix upload");
     A->stamp++;
     return CHIDG_GPU_OK;
@@ -457,8 +458,9 @@ extern "C" int chidg_gpu_matrix_upload_range(chidg_gpu_matrix* A, const double* 
     chidg_gpu_ctx* ctx = A->ctx;
     cudaSetDevice(ctx->device);
     if (count > 0) {
-        const cudaError_t e = cudaMemcpyAsync((double*)A->val.ptr + first, host, sizeof(double) * (size_t)count,
-                                              cudaMemcpyHostToDevice, ctx->stream);
+        cudaError_t e = cudaMemcpyAsync((double*)A->val.ptr + first, host, sizeof(double) * (size_t)count,
+                                        cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "matrix upload_range");
     }
     A->stamp++;
@@ -475,6 +477,8 @@ extern "C" int chidg_gpu_matrix_upload_blocks(chidg_gpu_matrix* A, const double*
         const cudaError_t e = cudaMemcpyAsync(d + A->voff[k], ptrs[k], bytes, cudaMemcpyHostToDevice, ctx->stream);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "block upload");
     }
+    const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "block upload");
     A->stamp++;
     return CHIDG_GPU_OK;
 }
@@ -763,15 +767,17 @@ extern "C" int chidg_gpu_vector_destroy(chidg_gpu_vector* x) {
 extern "C" int chidg_gpu_vector_upload(chidg_gpu_vector* x, const double* host) {
     if (!x || !host) return CHIDG_GPU_EINVAL;
     cudaSetDevice(x->ctx->device);
-    const cudaError_t e = cudaMemcpyAsync(x->buf.ptr, host, sizeof(double) * (size_t)x->n, cudaMemcpyHostToDevice, x->ctx->stream);
+    cudaError_t e = cudaMemcpyAsync(x->buf.ptr, host, sizeof(double) * (size_t)x->n, cudaMemcpyHostToDevice, x->ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(x->ctx->stream);
     return e == cudaSuccess ? CHIDG_GPU_OK : cuda_fail(x->ctx, e, "vector upload");
 }
 extern "C" int chidg_gpu_vector_upload_range(chidg_gpu_vector* x, const double* host, int64_t first, int64_t count) {
     if (!x || (!host && count > 0) || first < 0 || count < 0 || first + count > x->n) return CHIDG_GPU_EINVAL;
     cudaSetDevice(x->ctx->device);
     if (count == 0) return CHIDG_GPU_OK;
-    const cudaError_t e = cudaMemcpyAsync((double*)x->buf.ptr + first, host, sizeof(double) * (size_t)count,
-                                          cudaMemcpyHostToDevice, x->ctx->stream);
+    cudaError_t e = cudaMemcpyAsync((double*)x->buf.ptr + first, host, sizeof(double) * (size_t)count,
+                                    cudaMemcpyHostToDevice, x->ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(x->ctx->stream);
     return e == cudaSuccess ? CHIDG_GPU_OK : cuda_fail(x->ctx, e, "vector upload_range");
 }
 extern "C" int chidg_gpu_vector_download(chidg_gpu_vector* x, double* host) {

@@ -13,11 +13,13 @@
  *    chidg_signal(FATAL, ...) exactly where the reference would stop
  *    (src/tools/messenger.f90:968-977).
  *  - Host arrays are owned by the caller and only read (or written, for
- *    outputs) during the call.  Device objects are opaque library handles,
+ *    outputs) during the call: uploads return once the copy has left the host
+ *    array, whether it is pageable or page-locked.  Device objects are opaque library handles,
  *    released by the matching _destroy call (the reference's tear_down/release).
  *  - Handles are not thread safe.  A context owns one CUDA stream (the caller
- *    may pass its own); all work of objects made from that context is ordered
- *    on it.  Concurrency comes from several contexts.
+ *    may pass its own, which must then outlive the context and everything
+ *    made from it); all work of objects made from that context is ordered on
+ *    it.  Concurrency comes from several contexts.
  *  - Element numbering is 0-based over all domains of the mesh (flattened
  *    reference element order).  The vector of an element holds ntime levels
  *    of nvars fields x nterms modes: time-major, then field, then mode
