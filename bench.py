@@ -397,28 +397,37 @@ def run_hb_leg(ctx, stream, schedule, reps=3):
 
 
 def run_newton_leg(ctx):
-    """Whole Newton solve of five steps on the 8^3 P1 box (cfg1's size): the
-    Newton driver (pseudo-transient continuation, backtracking) over a
-    synthetic nonlinear system with the ChiDG block layout, R(q) = A0 (q - q*)
-    + c (q - q*)^2, assembled on the host; each step's linear solve is
+    """Whole Newton solve of five steps on cfg1: the 8^3 P1 box of the Euler
+    equations (farfield on every face, freestream M = 0.3, rho = 1, p = 1/gamma,
+    a Gaussian density bump of amplitude 1e-2 and width 0.1 at a seeded centre
+    in [0.3, 0.7]^3), residual and Jacobian assembled on the host by the DG
+    restatement, the Newton driver (pseudo-transient continuation from cfl 10,
+    backtracking) over the device containers, each step's linear solve
     FGMRES(30) + ILU0 to rtol 1e-8 in FP64."""
-    from chidg_b200 import api, mesh
-    from chidg_b200.newton import Newton, SyntheticSystem
-    pat = mesh.box_pattern(8, 8, 8, NVARS, mesh.nterms_of_order(1))
-    sysm = SyntheticSystem(pat, seed=SEED_A + 11, root_seed=SEED_B + 11)
-    A = api.ChidgMatrix(pat, ctx)
-    out = {"workload": "8^3 hex box, 5 fields, P1 (40x40 blocks): 5 Newton steps on a synthetic nonlinear system "
-                       "(host assembly), PTC cfl0 10, backtracking, FGMRES(30)+ILU0 to rtol 1e-8 per step, FP64"}
+    from chidg_b200 import api, euler
+    from chidg_b200.newton import Newton
+    rng = np.random.default_rng(SEED_A + 11)
+    centre = tuple(float(c) for c in rng.uniform(0.3, 0.7, 3))
+    box = euler.EulerBox(8, 8, 8, 1)
+    A = api.ChidgMatrix(box.pattern, ctx)
+    out = {"workload": "cfg1: 8^3 hex box, Euler, P1 (40x40 blocks), farfield, M 0.3 with a Gaussian density bump "
+                       "(amplitude 1e-2, width 0.1): 5 Newton steps, host DG assembly, PTC cfl0 10, backtracking, "
+                       "FGMRES(30)+ILU0 to rtol 1e-8 per step, FP64",
+           "bump_centre": centre}
+    q0 = box.density_bump(amplitude=1e-2, width=0.1, centre=centre)
     for rep in range(2):                              # the first run warms up
-        q = api.ChidgVector(A)
+        sysm = euler.EulerSystem(box)
+        q = api.ChidgVector(A, q0)
         solver = api.create_linear_solver("fgmres", **{**SOLVER, "nkrylov": 30})
         res = Newton(nmax=5, tol=0.0, rtol=0.0, cfl0=10.0).solve(sysm, q, A, solver,
                                                                 api.create_preconditioner("ilu0"))
         q.release()
     out.update({"seconds_whole_newton": res.seconds, "steps": res.niter,
                 "seconds_linear_solves": float(sum(res.linear_seconds)),
+                "seconds_host_assembly": sysm.assemble_seconds, "assemblies": sysm.nassemble,
                 "residual_history": [float(r) for r in res.residual_norm],
-                "linear_iterations": res.matrix_iterations, "alphas": res.alphas})
+                "linear_iterations": res.matrix_iterations,
+                "linear_true_rel_residual": [float(r) for r in res.linear_rel_residual], "alphas": res.alphas})
     A.release()
     return out
 

@@ -10,9 +10,10 @@ Assembly of the residual and its Jacobian stays with the caller, through a
 
     system.assemble(q, A, rhs, differentiate)   fill rhs = R(q), and A = dR/dq
                                                 when differentiate is true
-    system.pseudo_timestep(q, cfl) -> dtau      one pseudo time step per element
-                                                (the reference's minval over the
-                                                element's fields), cfl per field
+    system.pseudo_timestep(q, cfl) -> dtau      pseudo time steps, cfl per field:
+                                                one per element, or one per element
+                                                and field (nelem x nfields, as
+                                                elems(:)%dtau(ieqn))
     system.mass -> packed per-element mass matrices (nterms x nterms,
                    column-major), as chidg_gpu_matrix_scale_diagonal takes them
 
@@ -98,7 +99,10 @@ class Newton:
             b.scale(-1.0)
             if o.ptc:                                        # contribute_pseudo_temporal (:320-352)
                 dtau = np.asarray(system.pseudo_timestep(q, cfln), dtype=np.float64)
-                scale = np.repeat(1.0 / dtau, A.pattern.elem_nvars)
+                if dtau.ndim == 1:                           # one pseudo time step per element
+                    scale = np.repeat(1.0 / dtau, A.pattern.elem_nvars)
+                else:                                        # per element and field (elems(:)%dtau(ieqn))
+                    scale = (1.0 / dtau).reshape(-1)
                 A.scale_diagonal(system.mass, scale)
             if niter == 1:
                 res.residual_norm.append(resid)

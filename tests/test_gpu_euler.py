@@ -1,0 +1,128 @@
+"""The path on Euler DG Jacobians (chidg_b200.euler) instead of synthetic
+values: the linear systems of a pseudo-transient Newton step solved by FGMRES +
+ILU0 on the GPU against the oracle (pseudo-transient term added on the device
+by scale_diagonal, on the host for the oracle), and whole Newton solves over
+the device containers against a dense numpy Newton on the same host assembly.
+
+Tolerances: FGMRES as the synthetic parity cases (same iteration count,
+residual history within 1e-8 relative, solution within 1e-10 relative);
+Newton residual history within 1e-6 relative while the iteration contracts
+(the linear solves stop at rtol 1e-12, the dense one is exact)."""
+import numpy as np
+import pytest
+
+from chidg_b200 import api, euler
+from chidg_b200.newton import Newton, NewtonOptions
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def relerr(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def add_ptc(box, vals, dtau):
+    """vals + mass / dtau on every field's diagonal sub-block of DIAG (host)."""
+    nb, b, nt = box.pattern.nblocks, 5 * box.nterms, box.nterms
+    out = vals.copy()
+    blk = out.reshape(nb, b, b)                           # [block, column, row]
+    for e in range(box.nelem):
+        k = box._diag_k[e]
+        for f in range(5):
+            s = slice(f * nt, (f + 1) * nt)
+            blk[k][s, s] += box.mass_block.T / dtau[e, f]
+    return out
+
+
+def dense(pat, vals):
+    n = pat.vector_size()
+    J = np.zeros((n, n))
+    voff, _ = pat.value_offsets()
+    nr, nc = pat.block_dims()
+    eo = pat.elem_offsets()
+    for k in range(pat.nblocks):
+        r0, c0 = eo[pat.blk_row_elem[k]], eo[pat.blk_col_elem[k]]
+        J[r0:r0 + nr[k], c0:c0 + nc[k]] += vals[voff[k]:voff[k] + nr[k] * nc[k]].reshape(nc[k], nr[k]).T
+    return J
+
+
+@pytest.mark.parametrize("shape,P,bcs", [((4, 3, 3), 1, "farfield"), ((3, 3, 2), 2, "farfield"),
+                                         ((5, 2, 2), 1, ["farfield", "extrapolate"] * 3)])
+@pytest.mark.parametrize("orth", ["CGS", "MGS"])
+def test_newton_step_solve_parity(shape, P, bcs, orth):
+    box = euler.EulerBox(*shape, P, bcs=bcs)
+    q = box.density_bump(amplitude=1e-2, width=0.15, centre=(0.45, 0.55, 0.5))
+    R, vals = box.residual(q, jacobian=True)
+    dtau = box.pseudo_timestep(q, 10.0)
+    Ao = O.OracleMatrix(box.pattern)
+    Ao.set_values(add_ptc(box, vals, dtau))
+    Ag = api.ChidgMatrix(box.pattern)
+    Ag.upload(vals)
+    Ag.scale_diagonal(box.mass, (1.0 / dtau).reshape(-1))
+    assert relerr(Ag.download(), Ao.get_values()) < 1e-14
+    opts = dict(tol=0.0, rtol=1e-8, nkrylov=30, inner_fgmres=0, nmax=400, orthogonalization=orth)
+    xo, ro = O.fgmres(Ao, O.OraclePrecon(Ao, "ilu0"), -R, O.default_opts(**opts))
+    solver = api.create_linear_solver("fgmres", **opts)
+    xg = api.ChidgVector(Ag)
+    solver.solve(Ag, xg, api.ChidgVector(Ag, -R), api.create_preconditioner("ilu0"))
+    assert solver.niter == ro["niter"]
+    assert relerr(solver.hist, ro["hist"]) < 1e-8
+    assert relerr(xg.download(), xo) < 1e-10
+
+
+def newton_dense(box, q0, opts: NewtonOptions):
+    """The driver's loop with dense matrices and exact solves, on the same
+    host assembly."""
+    M = np.zeros((q0.size, q0.size))
+    nt = box.nterms
+    for e in range(box.nelem):
+        for f in range(5):
+            s = (e * 5 + f) * nt
+            M[s:s + nt, s:s + nt] = box.mass_block
+    q, hist, alphas = q0.copy(), [], []
+    cfl = np.full(5, opts.cfl0)
+    resid0 = np.linalg.norm(box.residual(q))
+    hist.append(resid0)
+    for niter in range(1, 100):
+        R, vals = box.residual(q, jacobian=True)
+        resid = np.linalg.norm(R)
+        J = dense(box.pattern, vals)
+        if opts.ptc:
+            J += M * (1.0 / box.pseudo_timestep(q, cfl)).reshape(-1).repeat(nt)[:, None]
+        dq = np.linalg.solve(J, -R)
+        step = 0
+        while True:
+            alpha = 2.0 ** -step
+            fn = np.linalg.norm(box.residual(q + alpha * dq))
+            step += 1
+            if not ((fn > 1e-3 and fn > 2 * resid) or (fn < 1e-3 and fn > resid)):
+                break
+        q = q + alpha * dq
+        alphas.append(alpha)
+        cfl = cfl * (opts.cfl_up if alpha > 0.75 else (opts.cfl_down if alpha < 0.2 else 1.0))
+        hist.append(fn)
+        if not (fn > opts.tol and fn / resid0 > opts.rtol and (niter < opts.nmax or opts.nmax <= 0)):
+            break
+    return q, hist, alphas
+
+
+@pytest.mark.parametrize("shape,P,amp", [((4, 3, 3), 1, 1e-2), ((3, 3, 2), 2, 5e-2)])
+def test_newton_on_euler_matches_dense(shape, P, amp):
+    box = euler.EulerBox(*shape, P)
+    sysm = euler.EulerSystem(box)
+    q0 = box.density_bump(amplitude=amp, width=0.2, centre=(0.45, 0.55, 0.5))
+    A = api.ChidgMatrix(box.pattern)
+    q = api.ChidgVector(A, q0)
+    opts = dict(tol=1e-12, rtol=1e-8, nmax=8, ptc=True, cfl0=10.0)
+    solver = api.create_linear_solver("fgmres", tol=0.0, rtol=1e-12, nkrylov=40, inner_fgmres=0, nmax=400)
+    res = Newton(**opts).solve(sysm, q, A, solver, api.create_preconditioner("ilu0"))
+    qd, hist, alphas = newton_dense(box, q0, NewtonOptions(**opts))
+    note = (res.residual_norm, hist)
+    assert max(res.linear_rel_residual) <= 1e-11, note
+    assert len(res.residual_norm) == len(hist), note
+    for a, b in zip(res.residual_norm, hist):
+        assert abs(a - b) <= 1e-6 * b + 1e-15, note
+    assert res.alphas == alphas
+    assert hist[-1] < 1e-3 * hist[0]
+    assert relerr(q.download(), qd) < 1e-8
