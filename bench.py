@@ -415,20 +415,83 @@ def run_newton_leg(ctx):
                        "FGMRES(30)+ILU0 to rtol 1e-8 per step, FP64",
            "bump_centre": centre}
     q0 = box.density_bump(amplitude=1e-2, width=0.1, centre=centre)
-    for rep in range(2):                              # the first run warms up
-        sysm = euler.EulerSystem(box)
-        q = api.ChidgVector(A, q0)
-        solver = api.create_linear_solver("fgmres", **{**SOLVER, "nkrylov": 30})
-        res = Newton(nmax=5, tol=0.0, rtol=0.0, cfl0=10.0).solve(sysm, q, A, solver,
-                                                                api.create_preconditioner("ilu0"))
-        q.release()
-    out.update({"seconds_whole_newton": res.seconds, "steps": res.niter,
-                "seconds_linear_solves": float(sum(res.linear_seconds)),
-                "seconds_host_assembly": sysm.assemble_seconds, "assemblies": sysm.nassemble,
-                "residual_history": [float(r) for r in res.residual_norm],
-                "linear_iterations": res.matrix_iterations,
-                "linear_true_rel_residual": [float(r) for r in res.linear_rel_residual], "alphas": res.alphas})
+    dev = euler.EulerDeviceSystem(box, ctx)
+    for name, make in (("host_assembly", lambda: euler.EulerSystem(box)), ("device_assembly", lambda: dev)):
+        for rep in range(2):                          # the first run warms up
+            sysm = make()
+            sysm.assemble_seconds, sysm.nassemble = 0.0, 0
+            q = api.ChidgVector(A, q0)
+            solver = api.create_linear_solver("fgmres", **{**SOLVER, "nkrylov": 30})
+            res = Newton(nmax=5, tol=0.0, rtol=0.0, cfl0=10.0).solve(sysm, q, A, solver,
+                                                                    api.create_preconditioner("ilu0"))
+            q.release()
+        out[name] = {"seconds_whole_newton": res.seconds, "steps": res.niter,
+                     "seconds_linear_solves": float(sum(res.linear_seconds)),
+                     "seconds_assembly": sysm.assemble_seconds, "assemblies": sysm.nassemble,
+                     "residual_history": [float(r) for r in res.residual_norm],
+                     "linear_iterations": res.matrix_iterations,
+                     "linear_true_rel_residual": [float(r) for r in res.linear_rel_residual], "alphas": res.alphas}
+    dev.device.release()
     A.release()
+    return out
+
+
+def run_assembly_leg(ctx, stream, A, reps=3):
+    """The Euler DG residual and Jacobian of the 24^3 P2 box assembled on the
+    device (k_euler_assemble) into the 24^3 P2 matrix (its synthetic values are
+    overwritten: the leg runs after every leg that reads them), then one whole
+    Newton step on it: assembly, pseudo-transient term, FGMRES(50) + ILU0 to
+    rtol 1e-8, backtracking.  Farfield on every face, M 0.3 with a Gaussian
+    density bump (amplitude 1e-2, width 0.1).  Algorithmic work per element:
+    the DIAG block 25 nt rows x [qv (3 + nt) + 6 qf (1 + nt)] FMAs, each
+    interior-face block 25 nt x qf (1 + nt) FMAs; bytes: the blocks and rhs
+    written once, q read once."""
+    import torch
+
+    from chidg_b200 import api, euler
+    from chidg_b200.newton import Newton
+    box = euler.EulerBox(24, 24, 24, 2)
+    dev = euler.EulerDevice(box, ctx)
+    q0 = box.density_bump(amplitude=1e-2, width=0.1, centre=(0.45, 0.55, 0.5))
+    q, r = api.ChidgVector(A, q0), api.ChidgVector(A)
+    dev.assemble(q, r, A)                            # warm-up
+    dev.assemble(q, r)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * reps + 2)]
+    for i in range(reps):
+        ev[2 * i].record(stream)
+        dev.assemble(q, r, A)
+        ev[2 * i + 1].record(stream)
+    ev[-2].record(stream)
+    dev.assemble(q, r)
+    ev[-1].record(stream)
+    torch.cuda.synchronize()
+    jac_ms = sum(ev[2 * i].elapsed_time(ev[2 * i + 1]) for i in range(reps)) / reps
+    res_ms = ev[-2].elapsed_time(ev[-1])
+    nt, n1 = box.nterms, euler.nnodes_1d(box.order)
+    qv, qf = n1 ** 3, n1 ** 2
+    nface = sum(box._interior_pairs(d)[0].size for d in range(3)) * 2
+    fma = box.nelem * 25 * nt * (qv * (3 + nt) + 6 * qf * (1 + nt)) + nface * 25 * nt * qf * (1 + nt)
+    nbytes = 8 * (A.nvalues + 2 * A.n)
+    out = {"workload": "Euler DG residual + Jacobian of the 24^3 P2 box on the device (93312 blocks of 135x135, "
+                       "13.6 GB written), farfield, M 0.3 with a density bump",
+           "jacobian_ms": jac_ms, "residual_only_ms": res_ms,
+           "gflops": 2.0 * fma / (jac_ms / 1e3) / 1e9, "flops_per_call": 2.0 * fma,
+           "gbs_written": nbytes / (jac_ms / 1e3) / 1e9, "bytes_per_call": nbytes}
+    sysm = euler.EulerDeviceSystem(box, ctx)
+    sysm.device = dev
+    solver = api.create_linear_solver("fgmres", **SOLVER)
+    t0 = time.perf_counter()
+    res = Newton(nmax=1, tol=0.0, rtol=0.0, cfl0=10.0).solve(sysm, q, A, solver,
+                                                             api.create_preconditioner("ilu0"))
+    out["newton_step"] = {"seconds": time.perf_counter() - t0, "seconds_linear_solve": res.linear_seconds[0],
+                          "seconds_assembly": sysm.assemble_seconds, "assemblies": sysm.nassemble,
+                          "linear_iterations": res.matrix_iterations[0],
+                          "linear_true_rel_residual": res.linear_rel_residual[0],
+                          "residual_history": [float(v) for v in res.residual_norm], "alpha": res.alphas[0]}
+    for o in (q, r):
+        o.release()
+    dev.release()
     return out
 
 
@@ -689,6 +752,7 @@ def run_gpu(args):
     newton = run_newton_leg(ctx) if not args.no_newton else None
     batch = run_batch_leg(ctx, args.schedule) if not args.no_batch else None
     serving = run_serve_subprocess(local) if not args.no_serve else None
+    assembly = run_assembly_leg(ctx, stream, A) if not args.no_assembly else None
     cfg3 = None
     if not args.no_cfg3 and world == 1:
         # the 24^3 objects leave the device first: the 32^3 legs hold ~120 GB
@@ -752,6 +816,7 @@ def run_gpu(args):
         "adjoint": adjoint,
         "harmonic_balance": hb,
         "newton": newton,
+        "euler_assembly": assembly,
         "cfg3": cfg3,
         "cpu_baseline": cpu,
     }
@@ -774,6 +839,8 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (A^T) solve leg")
     ap.add_argument("--no-hb", action="store_true", help="skip the harmonic-balance preconditioner leg")
     ap.add_argument("--no-newton", action="store_true", help="skip the whole-Newton leg (8^3 P1, 5 steps)")
+    ap.add_argument("--no-assembly", action="store_true",
+                    help="skip the device Euler assembly leg (24^3 P2, overwrites the 24^3 matrix)")
     ap.add_argument("--no-cfg3", action="store_true", help="skip the 32^3 P2 legs (ILU0 and RAS, FP64 and mixed)")
     ap.add_argument("--serve-only", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--serve-device", type=int, default=0, help=argparse.SUPPRESS)

@@ -29,6 +29,16 @@ DP = C.POINTER(C.c_double)
 VP = C.c_void_p
 
 
+class EulerBoxDesc(C.Structure):
+    """chidg_gpu_euler_box"""
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("order", C.c_int32),
+                ("lo", C.c_double * 3), ("hi", C.c_double * 3), ("bc", C.c_int32 * 6),
+                ("rho_inf", C.c_double), ("p_inf", C.c_double), ("vel_inf", C.c_double * 3)]
+
+
+EULER_FARFIELD, EULER_EXTRAPOLATE = 0, 1
+
+
 class Pattern(C.Structure):
     _fields_ = [("nelem", C.c_int32), ("ntime", C.c_int32), ("elem_nvars", I32P), ("elem_nterms", I32P),
                 ("elem_proc", I32P), ("nblocks", C.c_int64), ("blk_row_elem", I32P), ("blk_row_time", I32P),
@@ -98,6 +108,10 @@ PROTOTYPES = {
     "chidg_gpu_matvec": (C.c_int, [VP, VP, VP]),
     "chidg_gpu_vector_norm_fields": (C.c_int, [VP, VP, C.c_int32]),
     "chidg_gpu_selftest_bounded_waits": (C.c_int, [VP, C.c_int64, C.POINTER(C.c_int32)]),
+    "chidg_gpu_euler_create": (C.c_int, [VP, VP, C.POINTER(VP)]),
+    "chidg_gpu_euler_destroy": (C.c_int, [VP]),
+    "chidg_gpu_euler_assemble": (C.c_int, [VP, VP, VP, VP]),
+    "chidg_gpu_euler_pseudo_timestep": (C.c_int, [VP, VP, DP, DP]),
     "chidg_gpu_serve_create": (C.c_int, [C.c_int, C.c_int32, C.c_int64, C.c_int32, C.c_int32, VP, C.POINTER(VP)]),
     "chidg_gpu_serve_submit": (C.c_int, [VP, VP, VP, VP, C.POINTER(C.c_int64)]),
     "chidg_gpu_serve_wait": (C.c_int, [VP, C.c_int64, VP, VP, VP]),

@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["chidg_gpu.cu", "fgmres.cu", "batch.cu", "noalloc.cu", "matrix_io.cu", "serve.cu"]
+CU_SOURCES = ["chidg_gpu.cu", "fgmres.cu", "batch.cu", "noalloc.cu", "matrix_io.cu", "serve.cu", "euler.cu"]
 
 
 def _run(cmd):

@@ -4,6 +4,8 @@
 // level-scheduled GPU sweeps.  The FGMRES driver lives in fgmres.cu.
 #include "chidg_gpu_internal.cuh"
 
+#include <atomic>
+
 #include <algorithm>
 #include <chrono>
 #include <climits>
@@ -315,6 +317,8 @@ extern "C" int chidg_gpu_matrix_create(chidg_gpu_ctx* ctx, const chidg_gpu_patte
         !pat->blk_row_elem || !pat->blk_row_time || !pat->blk_col_elem || !pat->blk_col_time || !pat->blk_kind)
         return fail(ctx, CHIDG_GPU_EINVAL, "matrix_create: incomplete pattern");
     auto* A = new chidg_gpu_matrix();
+    static std::atomic<int64_t> next_uid{1};
+    A->uid = next_uid++;
     A->ctx = ctx;
     A->nelem = pat->nelem;
     A->ntime = pat->ntime;

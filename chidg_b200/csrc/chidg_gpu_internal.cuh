@@ -127,6 +127,7 @@ struct chidg_gpu_ctx {
 
 struct chidg_gpu_matrix {
     chidg_gpu_ctx* ctx = nullptr;
+    int64_t uid = 0;                         // unique over the process (caches keyed on a matrix use it, not the address)
     int nelem = 0, ntime = 0, nrow = 0;
     int64_t n = 0, nval = 0, nblk = 0;
     std::vector<int32_t> nvars, nterms, proc, re, rt, ce, ct, kind;

@@ -1,0 +1,749 @@
+// euler.cu -- Euler DG residual and Jacobian on hex boxes, assembled on the
+// device straight into the vector and the block matrix of the linear solves.
+//
+// The discretisation is ChiDG's (mod_spatial.f90:40-197 driving the Euler
+// operators of src/equations/fluid/euler/): modal tensor Legendre basis in the
+// reference's mode order (mod_legendre.f90, mod_ordering.f90), Gauss-Legendre
+// quadrature with ceil(3 (P+1) / 2) nodes per direction (gq_rule = 2,
+// mod_quadrature.f90:68-80), R = -int grad(phi).F dV (euler_volume_operator,
+// stored negated by store_volume_integrals, mod_integrate.f90:652-779) +
+// int phi Fhat.n dA with Fhat the central average plus Roe's upwind term with
+// Harten's entropy fix (euler_boundary_average_operator, euler_roe_operator)
+// on interior faces and F(Q_bc).n on boundary faces (euler_bc_operator) with
+// the farfield (bc_state_farfield.f90) or extrapolation
+// (bc_state_fluid_extrapolate.f90) state.  The Jacobian is exact: forward-mode
+// dual numbers through the pointwise functions, as the reference's DNAD types
+// (AD_D) carry derivatives, and the chain rule through the basis.
+//
+// One CTA per element.  Shared memory holds the modes of the element and of
+// its face neighbours and the weighted pointwise data (flux and its 5x5
+// derivatives at every volume node; face integrand and its derivatives with
+// respect to both states at every face node).  The residual, the DIAG block and
+// the face blocks are then contractions over the nodes, each output written by
+// one thread: no atomics, one writer per value.  Each element integrates its
+// own faces (the reference evaluates a shared face once and negates it for the
+// neighbour, integrate_boundary_scalar_flux, mod_integrate.f90:219-346; the
+// two agree to rounding since the numerical flux is antisymmetric).
+#include "chidg_gpu_internal.cuh"
+
+#include <cmath>
+#include <vector>
+
+using namespace chidg;
+
+namespace {
+
+constexpr double kGamma = 1.4;          // mod_fluid.f90:10
+constexpr double kRgas = 287.15;        // mod_fluid.f90:9
+constexpr double kRkTol = 20.0 * 2.220446049250313e-16;   // RKTOL, mod_constants.f90:241
+constexpr double kFixEps = 0.01;        // entropy-fix width, euler_roe_operator.f90
+constexpr int kMaxOrder = 2;
+constexpr int kThreads = 256;
+
+// Legendre degrees (xi, eta, zeta) of the first 27 modes in the reference's
+// order (mod_ordering.f90, xi/eta/zeta_order_3d, 0-based); each prefix of
+// (P+1)^3 modes is the full order-P set.
+constexpr int kModes[27][3] = {
+    {0, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 0}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}, {0, 2, 0},
+    {0, 0, 2}, {2, 0, 0}, {0, 2, 1}, {0, 1, 2}, {1, 2, 0}, {1, 0, 2}, {2, 1, 0}, {2, 0, 1}, {0, 2, 2},
+    {1, 2, 1}, {1, 1, 2}, {2, 2, 0}, {2, 0, 2}, {2, 1, 1}, {1, 2, 2}, {2, 2, 1}, {2, 1, 2}, {2, 2, 2}};
+
+// ---- forward-mode dual numbers ------------------------------------------------
+template <int N>
+struct Dual {
+    double v;
+    double d[N];
+};
+template <int N> __device__ __forceinline__ Dual<N> mk(double v) {
+    Dual<N> r; r.v = v;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = 0.0;
+    return r;
+}
+template <int N> __device__ __forceinline__ Dual<N> operator+(const Dual<N>& a, const Dual<N>& b) {
+    Dual<N> r; r.v = a.v + b.v;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = a.d[i] + b.d[i];
+    return r;
+}
+template <int N> __device__ __forceinline__ Dual<N> operator-(const Dual<N>& a, const Dual<N>& b) {
+    Dual<N> r; r.v = a.v - b.v;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = a.d[i] - b.d[i];
+    return r;
+}
+template <int N> __device__ __forceinline__ Dual<N> operator-(const Dual<N>& a) {
+    Dual<N> r; r.v = -a.v;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = -a.d[i];
+    return r;
+}
+template <int N> __device__ __forceinline__ Dual<N> operator*(const Dual<N>& a, const Dual<N>& b) {
+    Dual<N> r; r.v = a.v * b.v;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * b.v + a.v * b.d[i];
+    return r;
+}
+template <int N> __device__ __forceinline__ Dual<N> operator/(const Dual<N>& a, const Dual<N>& b) {
+    Dual<N> r; r.v = a.v / b.v;
+    const double ib = 1.0 / b.v;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = (a.d[i] - r.v * b.d[i]) * ib;
+    return r;
+}
+template <int N> __device__ __forceinline__ Dual<N> operator+(const Dual<N>& a, double b) { Dual<N> r = a; r.v += b; return r; }
+template <int N> __device__ __forceinline__ Dual<N> operator+(double b, const Dual<N>& a) { return a + b; }
+template <int N> __device__ __forceinline__ Dual<N> operator-(const Dual<N>& a, double b) { Dual<N> r = a; r.v -= b; return r; }
+template <int N> __device__ __forceinline__ Dual<N> operator-(double b, const Dual<N>& a) { return (-a) + b; }
+template <int N> __device__ __forceinline__ Dual<N> operator*(const Dual<N>& a, double b) {
+    Dual<N> r; r.v = a.v * b;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * b;
+    return r;
+}
+template <int N> __device__ __forceinline__ Dual<N> operator*(double b, const Dual<N>& a) { return a * b; }
+template <int N> __device__ __forceinline__ Dual<N> operator/(const Dual<N>& a, double b) { return a * (1.0 / b); }
+template <int N> __device__ __forceinline__ Dual<N> operator/(double a, const Dual<N>& b) { return mk<N>(a) / b; }
+template <int N> __device__ __forceinline__ Dual<N> dsqrt(const Dual<N>& a) {
+    Dual<N> r; r.v = sqrt(a.v);
+    const double h = 0.5 / r.v;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * h;
+    return r;
+}
+template <int N> __device__ __forceinline__ Dual<N> dpow(const Dual<N>& a, double e) {
+    Dual<N> r; r.v = pow(a.v, e);
+    const double s = e * pow(a.v, e - 1.0);
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * s;
+    return r;
+}
+template <int N> __device__ __forceinline__ Dual<N> dabs(const Dual<N>& a) { return a.v < 0.0 ? -a : a; }
+// select by a condition evaluated on values (the branch the AD type takes)
+template <int N> __device__ __forceinline__ Dual<N> dsel(bool c, const Dual<N>& a, const Dual<N>& b) { return c ? a : b; }
+
+// ---- pointwise Euler functions --------------------------------------------------
+template <int N> __device__ __forceinline__ Dual<N> pressure(const Dual<N>* Q) {
+    return (kGamma - 1.0) * (Q[4] - 0.5 * (Q[1] * Q[1] + Q[2] * Q[2] + Q[3] * Q[3]) / Q[0]);
+}
+
+// F_d(Q): the physical flux in direction d (euler_volume_operator.f90:112-181)
+template <int N> __device__ __forceinline__ void flux_dir(const Dual<N>* Q, int d, Dual<N>* F) {
+    const Dual<N> inv = 1.0 / Q[0];
+    const Dual<N> vel = Q[1 + d] * inv;
+    const Dual<N> p = pressure(Q);
+    const Dual<N> H = (Q[4] + p) * inv;
+    F[0] = Q[0] * vel;
+    F[1] = Q[1] * vel;
+    F[2] = Q[2] * vel;
+    F[3] = Q[3] * vel;
+    F[1 + d] = F[1 + d] + p;
+    F[4] = Q[0] * H * vel;
+}
+
+// Roe's upwind term per unit area with the entropy fix (euler_roe_operator.f90)
+template <int N> __device__ void roe_upwind(const Dual<N>* Qm, const Dual<N>* Qp, const double* n, Dual<N>* up) {
+    const Dual<N> inv_m = 1.0 / Qm[0], inv_p = 1.0 / Qp[0];
+    const Dual<N> p_m = pressure(Qm), p_p = pressure(Qp);
+    const Dual<N> H_m = (Qm[4] + p_m) * inv_m, H_p = (Qp[4] + p_p) * inv_p;
+    const Dual<N> u_m = Qm[1] * inv_m, v_m = Qm[2] * inv_m, w_m = Qm[3] * inv_m;
+    const Dual<N> u_p = Qp[1] * inv_p, v_p = Qp[2] * inv_p, w_p = Qp[3] * inv_p;
+    const Dual<N> vmag_m = u_m * n[0] + v_m * n[1] + w_m * n[2];
+    const Dual<N> vmag_p = u_p * n[0] + v_p * n[1] + w_p * n[2];
+    const Dual<N> sm = dsqrt(Qm[0]), sp = dsqrt(Qp[0]);
+    const Dual<N> ssum = sm + sp;
+    const Dual<N> rtil = dsqrt(Qp[0] * Qm[0]);
+    const Dual<N> util = (sm * u_m + sp * u_p) / ssum;
+    const Dual<N> vtil = (sm * v_m + sp * v_p) / ssum;
+    const Dual<N> wtil = (sm * w_m + sp * w_p) / ssum;
+    const Dual<N> Htil = (sm * H_m + sp * H_p) / ssum;
+    const Dual<N> vmagtil = util * n[0] + vtil * n[1] + wtil * n[2];
+    const Dual<N> qtil2 = util * util + vtil * vtil + wtil * wtil;
+    const Dual<N> ctil = dsqrt((kGamma - 1.0) * (Htil - 0.5 * qtil2));
+    const Dual<N> ctil2 = ctil * ctil;
+    const Dual<N> delr = Qm[0] - Qp[0];
+    const Dual<N> delu = u_m - u_p, delv = v_m - v_p, delw = w_m - w_p;
+    const Dual<N> delvmag = vmag_m - vmag_p;
+    const Dual<N> delp = p_m - p_p;
+    Dual<N> lam[3] = {dabs(vmagtil - ctil), dabs(vmagtil), dabs(vmagtil + ctil)};
+    const Dual<N> ec = kFixEps * ctil;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const bool small = (-ec.v < lam[i].v) && (lam[i].v < ec.v);
+        lam[i] = dsel(small, 0.5 * (ec + lam[i] * lam[i] / ec), dabs(lam[i]));
+    }
+    const Dual<N> C1 = dabs(lam[0]) * (delp - rtil * ctil * delvmag) / (2.0 * ctil2);
+    const Dual<N> C2a = dabs(lam[1]) * (delr - delp / ctil2);
+    const Dual<N> C2b = dabs(lam[1]) * rtil;
+    const Dual<N> C3 = dabs(lam[2]) * (delp + rtil * ctil * delvmag) / (2.0 * ctil2);
+    up[0] = 0.5 * (C1 + C2a + C3);
+    up[1] = 0.5 * (C1 * (util - ctil * n[0]) + C2a * util + C2b * (delu - delvmag * n[0]) + C3 * (util + ctil * n[0]));
+    up[2] = 0.5 * (C1 * (vtil - ctil * n[1]) + C2a * vtil + C2b * (delv - delvmag * n[1]) + C3 * (vtil + ctil * n[1]));
+    up[3] = 0.5 * (C1 * (wtil - ctil * n[2]) + C2a * wtil + C2b * (delw - delvmag * n[2]) + C3 * (wtil + ctil * n[2]));
+    up[4] = 0.5 * (C1 * (Htil - ctil * vmagtil) + C2a * (qtil2 / 2.0)
+                   + C2b * (util * delu + vtil * delv + wtil * delw - vmagtil * delvmag) + C3 * (Htil + ctil * vmagtil));
+}
+
+struct Freestream {
+    double rho, p, u[3];
+};
+
+// exterior state of the farfield condition (bc_state_farfield.f90, compute_bc_state)
+template <int N> __device__ void farfield_state(const Dual<N>* Qm, const double* n, const Freestream& fs, Dual<N>* Qb) {
+    const double T_in = fs.p / (fs.rho * kRgas);
+    const double c_in = sqrt(kGamma * kRgas * T_in);
+    const Dual<N> p_m = pressure(Qm);
+    const Dual<N> T_m = p_m / (Qm[0] * kRgas);
+    const Dual<N> c_m = dsqrt(kGamma * kRgas * T_m);
+    const Dual<N> nmom = Qm[1] * n[0] + Qm[2] * n[1] + Qm[3] * n[2];
+    const bool inflow = nmom.v <= kRkTol;
+    const Dual<N> u_m = Qm[1] / Qm[0], v_m = Qm[2] / Qm[0], w_m = Qm[3] / Qm[0];
+    const double un_in = fs.u[0] * n[0] + fs.u[1] * n[1] + fs.u[2] * n[2];
+    const double R_inf = un_in - 2.0 * c_in / (kGamma - 1.0);
+    const Dual<N> un_m = u_m * n[0] + v_m * n[1] + w_m * n[2];
+    const Dual<N> R_ext = un_m + 2.0 * c_m / (kGamma - 1.0);
+    const Dual<N> c_bc = ((kGamma - 1.0) / 4.0) * (R_ext - R_inf);
+    const Dual<N> half = 0.5 * (R_ext + R_inf);
+    Dual<N> ut, vt, wt, entropy;
+    if (inflow) {
+        ut = mk<N>(fs.u[0] - un_in * n[0]);
+        vt = mk<N>(fs.u[1] - un_in * n[1]);
+        wt = mk<N>(fs.u[2] - un_in * n[2]);
+        entropy = mk<N>(fs.p / pow(fs.rho, kGamma));
+    } else {
+        ut = u_m - un_m * n[0];
+        vt = v_m - un_m * n[1];
+        wt = w_m - un_m * n[2];
+        entropy = p_m / dpow(Qm[0], kGamma);
+    }
+    const Dual<N> rho_bc = dpow(c_bc * c_bc / (entropy * kGamma), 1.0 / (kGamma - 1.0));
+    Qb[0] = rho_bc;
+    Qb[1] = (half * n[0] + ut) * rho_bc;
+    Qb[2] = (half * n[1] + vt) * rho_bc;
+    Qb[3] = (half * n[2] + wt) * rho_bc;
+    const Dual<N> p_bc = dpow(rho_bc, kGamma) * entropy;
+    Qb[4] = p_bc / (kGamma - 1.0) + 0.5 * (Qb[1] * Qb[1] + Qb[2] * Qb[2] + Qb[3] * Qb[3]) / rho_bc;
+}
+
+// ---- kernel --------------------------------------------------------------------
+struct BoxGeom {
+    int nx, ny, nz;
+    int nt, qv, qf;             // modes, volume nodes, face nodes
+    double area[3];             // |scaled normal| on xi, eta, zeta faces
+    int bc[6];
+    Freestream fs;
+};
+
+struct Tables {
+    const double* phi;          // [qv][nt]
+    const double* grad;         // [3][qv][nt] physical gradients
+    const double* wv;           // [qv] weights * jinv
+    const double* phif;         // [6][qf][nt]
+    const double* wf;           // [qf] face weights (reference)
+};
+
+__device__ __forceinline__ int neighbour(const BoxGeom& g, int e, int face) {
+    const int i = e % g.nx, j = (e / g.nx) % g.ny, k = e / (g.nx * g.ny);
+    switch (face) {
+        case 0: return i > 0 ? e - 1 : -1;
+        case 1: return i < g.nx - 1 ? e + 1 : -1;
+        case 2: return j > 0 ? e - g.nx : -1;
+        case 3: return j < g.ny - 1 ? e + g.nx : -1;
+        case 4: return k > 0 ? e - g.nx * g.ny : -1;
+        default: return k < g.nz - 1 ? e + g.nx * g.ny : -1;
+    }
+}
+
+// Shared memory (doubles): U[7][5 nt] | WF[qv][3][5] | WdF[qv][3][5][5] |
+// FI[6][qf][5] | Fs[6][qf][5][5] | Fn[6][qf][5][5]
+__host__ __device__ inline size_t smem_doubles(int nt, int qv, int qf) {
+    return (size_t)7 * 5 * nt + (size_t)qv * 15 + (size_t)qv * 75 + (size_t)6 * qf * 5 + (size_t)12 * qf * 25;
+}
+
+template <int NT>
+__global__ void __launch_bounds__(kThreads) k_euler_assemble(BoxGeom g, Tables tb, const double* __restrict__ q,
+                                                            double* __restrict__ rhs, double* __restrict__ val,
+                                                            const int64_t* __restrict__ blk_off) {
+    extern __shared__ double sm[];
+    const int e = blockIdx.x;
+    const int nt = NT, b = 5 * NT, qv = g.qv, qf = g.qf;
+    double* sU = sm;                            // [7][5 nt]: own (slot 6) and face neighbours (slots 0..5)
+    double* sWF = sU + 7 * 5 * nt;              // [qv][3][5]
+    double* sWdF = sWF + (size_t)qv * 15;       // [qv][3][5][5]
+    double* sFI = sWdF + (size_t)qv * 75;       // [6][qf][5]
+    double* sFs = sFI + (size_t)6 * qf * 5;     // [6][qf][5][5]  d integrand / d own state
+    double* sFn = sFs + (size_t)6 * qf * 25;    // [6][qf][5][5]  d integrand / d neighbour state
+    int nbr[6];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) nbr[f] = neighbour(g, e, f);
+
+    // 1. modes of the element and its neighbours
+    for (int t = threadIdx.x; t < 7 * b; t += blockDim.x) {
+        const int slot = t / b, i = t - slot * b;
+        const int src = slot == 6 ? e : nbr[slot];
+        sU[t] = src >= 0 ? q[(int64_t)src * b + i] : 0.0;
+    }
+    __syncthreads();
+
+    // 2. pointwise data at volume nodes and face nodes
+    for (int t = threadIdx.x; t < qv + 6 * qf; t += blockDim.x) {
+        if (t < qv) {
+            Dual<5> Q[5];
+#pragma unroll
+            for (int f = 0; f < 5; ++f) {
+                double s = 0.0;
+                for (int m = 0; m < nt; ++m) s += tb.phi[t * nt + m] * sU[6 * b + f * nt + m];
+                Q[f] = mk<5>(s);
+                Q[f].d[f] = 1.0;
+            }
+            const double w = tb.wv[t];
+            for (int d = 0; d < 3; ++d) {
+                Dual<5> F[5];
+                flux_dir(Q, d, F);
+#pragma unroll
+                for (int f = 0; f < 5; ++f) {
+                    sWF[(t * 3 + d) * 5 + f] = w * F[f].v;
+#pragma unroll
+                    for (int gg = 0; gg < 5; ++gg) sWdF[((t * 3 + d) * 5 + f) * 5 + gg] = w * F[f].d[gg];
+                }
+            }
+        } else {
+            const int u = t - qv, face = u / qf, qq = u - face * qf;
+            const int d = face >> 1;
+            const double s = (face & 1) ? 1.0 : -1.0;
+            const double a = g.area[d];
+            double n[3] = {0.0, 0.0, 0.0};
+            n[d] = s;
+            const double w = tb.wf[qq];
+            const double* pm = tb.phif + ((size_t)face * qf + qq) * nt;
+            double Qm0[5], Qp0[5];
+#pragma unroll
+            for (int f = 0; f < 5; ++f) {
+                double sm_ = 0.0;
+                for (int m = 0; m < nt; ++m) sm_ += pm[m] * sU[6 * b + f * nt + m];
+                Qm0[f] = sm_;
+            }
+            double* FI = sFI + ((size_t)face * qf + qq) * 5;
+            double* Fs = sFs + ((size_t)face * qf + qq) * 25;
+            double* Fn = sFn + ((size_t)face * qf + qq) * 25;
+            if (nbr[face] >= 0) {
+                const double* pp = tb.phif + ((size_t)(face ^ 1) * qf + qq) * nt;
+#pragma unroll
+                for (int f = 0; f < 5; ++f) {
+                    double sp_ = 0.0;
+                    for (int m = 0; m < nt; ++m) sp_ += pp[m] * sU[face * b + f * nt + m];
+                    Qp0[f] = sp_;
+                }
+                // two passes: derivatives with respect to the own state, then the neighbour's
+                for (int side = 0; side < 2; ++side) {
+                    Dual<5> Qm[5], Qp[5];
+#pragma unroll
+                    for (int f = 0; f < 5; ++f) {
+                        Qm[f] = mk<5>(Qm0[f]);
+                        Qp[f] = mk<5>(Qp0[f]);
+                        if (side == 0) Qm[f].d[f] = 1.0; else Qp[f].d[f] = 1.0;
+                    }
+                    Dual<5> Fm[5], Fp[5], up[5];
+                    flux_dir(Qm, d, Fm);
+                    flux_dir(Qp, d, Fp);
+                    roe_upwind(Qm, Qp, n, up);
+                    double* dst = side == 0 ? Fs : Fn;
+#pragma unroll
+                    for (int f = 0; f < 5; ++f) {
+                        const Dual<5> I = (0.5 * s * a) * (Fm[f] + Fp[f]) + a * up[f];
+                        if (side == 0) FI[f] = w * I.v;
+#pragma unroll
+                        for (int gg = 0; gg < 5; ++gg) dst[f * 5 + gg] = w * I.d[gg];
+                    }
+                }
+            } else {
+                Dual<5> Qm[5], Qb[5];
+#pragma unroll
+                for (int f = 0; f < 5; ++f) {
+                    Qm[f] = mk<5>(Qm0[f]);
+                    Qm[f].d[f] = 1.0;
+                }
+                if (g.bc[face] == CHIDG_EULER_FARFIELD) {
+                    farfield_state(Qm, n, g.fs, Qb);
+                } else {
+#pragma unroll
+                    for (int f = 0; f < 5; ++f) Qb[f] = Qm[f];
+                }
+                Dual<5> F[5];
+                flux_dir(Qb, d, F);
+#pragma unroll
+                for (int f = 0; f < 5; ++f) {
+                    FI[f] = w * s * a * F[f].v;
+#pragma unroll
+                    for (int gg = 0; gg < 5; ++gg) {
+                        Fs[f * 5 + gg] = w * s * a * F[f].d[gg];
+                        Fn[f * 5 + gg] = 0.0;
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+
+    // 3. residual: R[f, m] = -sum_q sum_d grad_d[q, m] WF[q, d, f] + sum_faces sum_q phif[q, m] FI[q, f]
+    for (int t = threadIdx.x; t < b; t += blockDim.x) {
+        const int f = t / nt, m = t - f * nt;
+        double r = 0.0;
+        for (int qq = 0; qq < qv; ++qq)
+            r -= tb.grad[(0 * qv + qq) * nt + m] * sWF[(qq * 3 + 0) * 5 + f]
+               + tb.grad[(1 * qv + qq) * nt + m] * sWF[(qq * 3 + 1) * 5 + f]
+               + tb.grad[(2 * qv + qq) * nt + m] * sWF[(qq * 3 + 2) * 5 + f];
+        for (int face = 0; face < 6; ++face)
+            for (int qq = 0; qq < qf; ++qq)
+                r += tb.phif[((size_t)face * qf + qq) * nt + m] * sFI[((size_t)face * qf + qq) * 5 + f];
+        rhs[(int64_t)e * b + t] = r;
+    }
+
+    // 4. DIAG block and 5. face blocks (skipped for a residual-only call): one
+    // thread per (f, m, g) row of outputs, all nt columns n in registers; block
+    // entry (f nt + m, g nt + n) stored column-major.  Lanes of a warp take
+    // consecutive m: coalesced stores.
+    if (val == nullptr) return;
+    for (int blk = 6; blk >= 0; --blk) {
+        if (blk < 6 && nbr[blk] < 0) continue;
+        double* out = val + blk_off[(int64_t)e * 7 + blk];
+        for (int rid = threadIdx.x; rid < 25 * nt; rid += blockDim.x) {
+            const int m = rid % nt, fg = rid / nt, f = fg % 5, gg = fg / 5;
+            double acc[NT];
+#pragma unroll
+            for (int n = 0; n < NT; ++n) acc[n] = 0.0;
+            if (blk == 6) {
+                for (int qq = 0; qq < qv; ++qq) {
+                    const double tcoef = -(tb.grad[(0 * qv + qq) * nt + m] * sWdF[((qq * 3 + 0) * 5 + f) * 5 + gg]
+                                         + tb.grad[(1 * qv + qq) * nt + m] * sWdF[((qq * 3 + 1) * 5 + f) * 5 + gg]
+                                         + tb.grad[(2 * qv + qq) * nt + m] * sWdF[((qq * 3 + 2) * 5 + f) * 5 + gg]);
+                    const double* ph = tb.phi + (size_t)qq * nt;
+#pragma unroll
+                    for (int n = 0; n < NT; ++n) acc[n] += tcoef * ph[n];
+                }
+                for (int face = 0; face < 6; ++face) {
+                    for (int qq = 0; qq < qf; ++qq) {
+                        const double* pf = tb.phif + ((size_t)face * qf + qq) * nt;
+                        const double tcoef = pf[m] * sFs[((size_t)face * qf + qq) * 25 + f * 5 + gg];
+#pragma unroll
+                        for (int n = 0; n < NT; ++n) acc[n] += tcoef * pf[n];
+                    }
+                }
+            } else {
+                for (int qq = 0; qq < qf; ++qq) {
+                    const double* pf = tb.phif + ((size_t)blk * qf + qq) * nt;
+                    const double* pn = tb.phif + ((size_t)(blk ^ 1) * qf + qq) * nt;
+                    const double tcoef = pf[m] * sFn[((size_t)blk * qf + qq) * 25 + f * 5 + gg];
+#pragma unroll
+                    for (int n = 0; n < NT; ++n) acc[n] += tcoef * pn[n];
+                }
+            }
+            const int row = f * nt + m;
+#pragma unroll
+            for (int n = 0; n < NT; ++n) out[(int64_t)(gg * nt + n) * b + row] = acc[n];
+        }
+    }
+}
+
+// dtau[e, f] = cfl[f] h / (mean |u| + mean c) over the volume nodes
+// (type_fluid_pseudo_timestep.f90, compute)
+template <int NT>
+__global__ void __launch_bounds__(kThreads) k_euler_dtau(BoxGeom g, Tables tb, const double* __restrict__ q,
+                                                        double h, double c0, double c1, double c2, double c3, double c4,
+                                                        double* __restrict__ dtau) {
+    __shared__ double red[2][kThreads / 32];
+    const int e = blockIdx.x, nt = NT, b = 5 * NT;
+    double sv = 0.0, sc = 0.0;
+    for (int qq = threadIdx.x; qq < g.qv; qq += blockDim.x) {
+        double Q[5];
+        for (int f = 0; f < 5; ++f) {
+            double s = 0.0;
+            for (int m = 0; m < nt; ++m) s += tb.phi[qq * nt + m] * q[(int64_t)e * b + f * nt + m];
+            Q[f] = s;
+        }
+        const double p = (kGamma - 1.0) * (Q[4] - 0.5 * (Q[1] * Q[1] + Q[2] * Q[2] + Q[3] * Q[3]) / Q[0]);
+        sc += sqrt(kGamma * p / Q[0]);
+        sv += sqrt((Q[1] * Q[1] + Q[2] * Q[2] + Q[3] * Q[3]) / (Q[0] * Q[0]));
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        sv += __shfl_down_sync(0xffffffffu, sv, o);
+        sc += __shfl_down_sync(0xffffffffu, sc, o);
+    }
+    if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = sv; red[1][threadIdx.x >> 5] = sc; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, c = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { a += red[0][w]; c += red[1][w]; }
+        const double lam = a / g.qv + c / g.qv;
+        const double cfl[5] = {c0, c1, c2, c3, c4};
+        for (int f = 0; f < 5; ++f) dtau[(int64_t)e * 5 + f] = cfl[f] * h / lam;
+    }
+}
+
+// ---- host tables ----------------------------------------------------------------
+void legendre(int order, double x, double* L, double* D) {
+    L[0] = 1.0;
+    D[0] = 0.0;
+    if (order >= 1) { L[1] = x; D[1] = 1.0; }
+    for (int n = 2; n <= order; ++n) {
+        L[n] = ((2.0 * n - 1.0) * x * L[n - 1] - (n - 1.0) * L[n - 2]) / n;
+        D[n] = D[n - 2] + (2.0 * n - 1.0) * L[n - 1];
+    }
+}
+
+// Gauss-Legendre nodes and weights on [-1, 1] by Newton's iteration on P_n
+// from the asymptotic guesses cos(pi (i + 3/4) / (n + 1/2)); w = 2 / ((1 - x^2) P_n'(x)^2).
+void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {
+    x.assign(n, 0.0);
+    w.assign(n, 0.0);
+    std::vector<double> L(n + 1), D(n + 1);
+    for (int i = 0; i < n; ++i) {
+        double z = std::cos(M_PI * (i + 0.75) / (n + 0.5));
+        for (int it = 0; it < 100; ++it) {
+            legendre(n, z, L.data(), D.data());
+            const double dz = L[n] / D[n];
+            z -= dz;
+            if (std::fabs(dz) < 1e-16) break;
+        }
+        legendre(n, z, L.data(), D.data());
+        x[n - 1 - i] = z;
+        w[n - 1 - i] = 2.0 / ((1.0 - z * z) * D[n] * D[n]);
+    }
+}
+
+}  // namespace
+
+struct chidg_gpu_euler {
+    chidg_gpu_ctx* ctx = nullptr;
+    chidg_gpu_euler_box box{};
+    BoxGeom g{};
+    int order = 0, nelem = 0;
+    double h = 0.0;
+    Buffer phi, grad, wv, phif, wf, dtau;
+    Buffer blk_off;
+    int64_t off_uid = 0;                           // matrix (uid) the block-offset table was built for
+};
+
+extern "C" int chidg_gpu_euler_create(chidg_gpu_ctx* ctx, const chidg_gpu_euler_box* box, chidg_gpu_euler** out) {
+    if (!ctx || !box || !out) return CHIDG_GPU_EINVAL;
+    *out = nullptr;
+    if (box->nx < 1 || box->ny < 1 || box->nz < 1 || box->order < 0 || box->order > kMaxOrder)
+        return fail(ctx, CHIDG_GPU_EINVAL, "euler_create: box sizes must be >= 1 and order 0..2");
+    for (int d = 0; d < 3; ++d)
+        if (!(box->hi[d] > box->lo[d])) return fail(ctx, CHIDG_GPU_EINVAL, "euler_create: empty extent");
+    for (int f = 0; f < 6; ++f)
+        if (box->bc[f] != CHIDG_EULER_FARFIELD && box->bc[f] != CHIDG_EULER_EXTRAPOLATE)
+            return fail(ctx, CHIDG_GPU_EINVAL, "euler_create: unknown boundary condition");
+    if (!(box->rho_inf > 0.0) || !(box->p_inf > 0.0)) return fail(ctx, CHIDG_GPU_EINVAL, "euler_create: freestream");
+    const int64_t nelem = (int64_t)box->nx * box->ny * box->nz;
+    if (nelem > (int64_t)INT32_MAX) return fail(ctx, CHIDG_GPU_EINVAL, "euler_create: too many elements");
+    auto* E = new chidg_gpu_euler;
+    E->ctx = ctx;
+    E->box = *box;
+    E->order = box->order;
+    E->nelem = (int)nelem;
+    const int P = box->order, n1 = (3 * (P + 1) + 1) / 2, nt = (P + 1) * (P + 1) * (P + 1);
+    const int qv = n1 * n1 * n1, qf = n1 * n1;
+    double hx[3];
+    const int ne[3] = {box->nx, box->ny, box->nz};
+    for (int d = 0; d < 3; ++d) hx[d] = (box->hi[d] - box->lo[d]) / ne[d];
+    const double jinv = hx[0] * hx[1] * hx[2] / 8.0;
+    E->h = std::cbrt(hx[0] * hx[1] * hx[2]);
+    BoxGeom& g = E->g;
+    g.nx = box->nx; g.ny = box->ny; g.nz = box->nz;
+    g.nt = nt; g.qv = qv; g.qf = qf;
+    g.area[0] = hx[1] * hx[2] / 4.0; g.area[1] = hx[0] * hx[2] / 4.0; g.area[2] = hx[0] * hx[1] / 4.0;
+    for (int f = 0; f < 6; ++f) g.bc[f] = box->bc[f];
+    g.fs.rho = box->rho_inf; g.fs.p = box->p_inf;
+    for (int d = 0; d < 3; ++d) g.fs.u[d] = box->vel_inf[d];
+
+    std::vector<double> xg, wg;
+    gauss_legendre(n1, xg, wg);
+    std::vector<double> Lv((P + 1) * n1), Ld((P + 1) * n1), Lend_lo(P + 1), Lend_hi(P + 1), tmpL(P + 1), tmpD(P + 1);
+    for (int i = 0; i < n1; ++i) {
+        legendre(P, xg[i], tmpL.data(), tmpD.data());
+        for (int n = 0; n <= P; ++n) { Lv[n * n1 + i] = tmpL[n]; Ld[n * n1 + i] = tmpD[n]; }
+    }
+    for (int n = 0; n <= P; ++n) { Lend_hi[n] = 1.0; Lend_lo[n] = (n % 2) ? -1.0 : 1.0; }
+    std::vector<double> phi((size_t)qv * nt), grad((size_t)3 * qv * nt), wv(qv), phif((size_t)6 * qf * nt), wf(qf);
+    for (int k = 0; k < n1; ++k)
+        for (int j = 0; j < n1; ++j)
+            for (int i = 0; i < n1; ++i) {
+                const int qq = (k * n1 + j) * n1 + i;                       // xi fastest
+                wv[qq] = wg[i] * wg[j] * wg[k] * jinv;
+                for (int m = 0; m < nt; ++m) {
+                    const int a = kModes[m][0], bb = kModes[m][1], c = kModes[m][2];
+                    const double la = Lv[a * n1 + i], lb = Lv[bb * n1 + j], lc = Lv[c * n1 + k];
+                    phi[(size_t)qq * nt + m] = la * lb * lc;
+                    grad[((size_t)0 * qv + qq) * nt + m] = Ld[a * n1 + i] * lb * lc * (2.0 / hx[0]);
+                    grad[((size_t)1 * qv + qq) * nt + m] = la * Ld[bb * n1 + j] * lc * (2.0 / hx[1]);
+                    grad[((size_t)2 * qv + qq) * nt + m] = la * lb * Ld[c * n1 + k] * (2.0 / hx[2]);
+                }
+            }
+    for (int t0 = 0; t0 < n1; ++t0)
+        for (int t1 = 0; t1 < n1; ++t1) wf[t0 * n1 + t1] = wg[t0] * wg[t1];
+    for (int face = 0; face < 6; ++face) {
+        const int d = face >> 1;
+        const int ta = d == 0 ? 1 : 0, tb_ = d == 2 ? 1 : 2;                // tangential directions, ta < tb_
+        const std::vector<double>& Lend = (face & 1) ? Lend_hi : Lend_lo;
+        for (int t0 = 0; t0 < n1; ++t0)
+            for (int t1 = 0; t1 < n1; ++t1) {
+                const int qq = t0 * n1 + t1;
+                for (int m = 0; m < nt; ++m) {
+                    double v = 1.0;
+                    for (int dd = 0; dd < 3; ++dd) {
+                        const int deg = kModes[m][dd];
+                        if (dd == d) v *= Lend[deg];
+                        else if (dd == ta) v *= Lv[deg * n1 + t0];
+                        else v *= Lv[deg * n1 + t1];
+                    }
+                    phif[((size_t)face * qf + qq) * nt + m] = v;
+                }
+            }
+        (void)tb_;
+    }
+    auto up = [&](Buffer& buf, const std::vector<double>& v) {
+        int st = ensure(ctx, buf, v.size() * sizeof(double));
+        if (st) return st;
+        const cudaError_t ce = cudaMemcpyAsync(buf.ptr, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice,
+                                               ctx->stream);
+        return ce == cudaSuccess ? CHIDG_GPU_OK : cuda_fail(ctx, ce, "euler tables");
+    };
+    int st = up(E->phi, phi);
+    if (!st) st = up(E->grad, grad);
+    if (!st) st = up(E->wv, wv);
+    if (!st) st = up(E->phif, phif);
+    if (!st) st = up(E->wf, wf);
+    if (!st) st = ensure(ctx, E->dtau, (size_t)nelem * 5 * sizeof(double));
+    if (!st) {
+        const cudaError_t ce = cudaStreamSynchronize(ctx->stream);     // the host tables go out of scope
+        if (ce != cudaSuccess) st = cuda_fail(ctx, ce, "euler tables");
+    }
+    const size_t smem = smem_doubles(nt, qv, qf) * sizeof(double);
+    if (!st) {
+        const void* fn = P == 0 ? (const void*)k_euler_assemble<1> : P == 1 ? (const void*)k_euler_assemble<8>
+                                                                            : (const void*)k_euler_assemble<27>;
+        st = raise_smem_limit(fn, smem);
+    }
+    if (st) {
+        chidg_gpu_euler_destroy(E);
+        return st;
+    }
+    *out = E;
+    return CHIDG_GPU_OK;
+}
+
+extern "C" int chidg_gpu_euler_destroy(chidg_gpu_euler* E) {
+    if (!E) return CHIDG_GPU_OK;
+    for (Buffer* b : {&E->phi, &E->grad, &E->wv, &E->phif, &E->wf, &E->dtau, &E->blk_off}) release(*b);
+    delete E;
+    return CHIDG_GPU_OK;
+}
+
+namespace {
+Tables tables_of(const chidg_gpu_euler* E) {
+    return Tables{(const double*)E->phi.ptr, (const double*)E->grad.ptr, (const double*)E->wv.ptr,
+                  (const double*)E->phif.ptr, (const double*)E->wf.ptr};
+}
+
+int check_vector(chidg_gpu_euler* E, const chidg_gpu_vector* v, const char* what) {
+    if (!v || v->ctx != E->ctx) return fail(E->ctx, CHIDG_GPU_EINVAL, std::string("euler: ") + what + " of another context");
+    if (v->n != (int64_t)E->nelem * 5 * E->g.nt)
+        return fail(E->ctx, CHIDG_GPU_EINVAL, std::string("euler: ") + what + " length does not match the box");
+    return CHIDG_GPU_OK;
+}
+
+// Offsets of each element's blocks in A's values: [e][face 0..5, DIAG], -1 on
+// boundary faces.  A must hold exactly the box pattern: one time level, 5
+// fields and (P+1)^3 modes per element, and in every row the DIAG block and
+// one block per interior face.
+int block_offsets(chidg_gpu_euler* E, chidg_gpu_matrix* A) {
+    if (E->off_uid == A->uid) return CHIDG_GPU_OK;
+    const int nt = E->g.nt;
+    if (A->nelem != E->nelem || A->ntime != 1)
+        return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble: matrix is not this box's (elements or time levels)");
+    std::vector<int64_t> off((size_t)E->nelem * 7, -1);
+    BoxGeom g = E->g;
+    for (int e = 0; e < E->nelem; ++e) {
+        if (A->nvars[e] != 5 || A->nterms[e] != nt)
+            return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble: element fields or modes differ from the box");
+        const int i = e % g.nx, j = (e / g.nx) % g.ny, k = e / (g.nx * g.ny);
+        const int nb[6] = {i > 0 ? e - 1 : -1, i < g.nx - 1 ? e + 1 : -1, j > 0 ? e - g.nx : -1,
+                           j < g.ny - 1 ? e + g.nx : -1, k > 0 ? e - g.nx * g.ny : -1,
+                           k < g.nz - 1 ? e + g.nx * g.ny : -1};
+        int expect = 1;
+        for (int f = 0; f < 6; ++f) expect += nb[f] >= 0;
+        const std::vector<int32_t>& row = A->rowblk[A->row(e, 0)];
+        if ((int)row.size() != expect)
+            return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble: matrix row is not the box pattern");
+        for (int32_t kb : row) {
+            if (A->kind[kb] != CHIDG_BLK_LOCAL)
+                return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble: matrix has non-local blocks");
+            int slot = -1;
+            if (A->ce[kb] == e) slot = 6;
+            for (int f = 0; f < 6 && slot < 0; ++f)
+                if (nb[f] == A->ce[kb]) slot = f;
+            if (slot < 0 || off[(size_t)e * 7 + slot] >= 0)
+                return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble: matrix row is not the box pattern");
+            off[(size_t)e * 7 + slot] = A->voff[kb];
+        }
+    }
+    int st = ensure(E->ctx, E->blk_off, off.size() * sizeof(int64_t));
+    if (st) return st;
+    cudaError_t ce = cudaMemcpyAsync(E->blk_off.ptr, off.data(), off.size() * sizeof(int64_t), cudaMemcpyHostToDevice,
+                                     E->ctx->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(E->ctx->stream);
+    if (ce != cudaSuccess) return cuda_fail(E->ctx, ce, "euler block offsets");
+    E->off_uid = A->uid;
+    return CHIDG_GPU_OK;
+}
+}  // namespace
+
+extern "C" int chidg_gpu_euler_assemble(chidg_gpu_euler* E, chidg_gpu_vector* q, chidg_gpu_vector* rhs,
+                                        chidg_gpu_matrix* A) {
+    if (!E) return CHIDG_GPU_EINVAL;
+    int st = check_vector(E, q, "q");
+    if (!st) st = check_vector(E, rhs, "rhs");
+    if (st) return st;
+    if (q == rhs) return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble: q and rhs must differ");
+    const bool jac = A != nullptr;
+    if (jac) {
+        if (A->ctx != E->ctx) return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble: matrix of another context");
+        st = block_offsets(E, A);
+        if (st) return st;
+    }
+    const int P = E->order, nt = E->g.nt;
+    const size_t smem = smem_doubles(nt, E->g.qv, E->g.qf) * sizeof(double);
+    const Tables tb = tables_of(E);
+    double* val = jac ? (double*)A->val.ptr : nullptr;
+    const int64_t* off = jac ? (const int64_t*)E->blk_off.ptr : nullptr;
+    const dim3 grid(E->nelem), block(kThreads);
+    if (P == 0) k_euler_assemble<1><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, (const double*)q->buf.ptr, (double*)rhs->buf.ptr, val, off);
+    else if (P == 1) k_euler_assemble<8><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, (const double*)q->buf.ptr, (double*)rhs->buf.ptr, val, off);
+    else k_euler_assemble<27><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, (const double*)q->buf.ptr, (double*)rhs->buf.ptr, val, off);
+    st = check_launch(E->ctx, "k_euler_assemble");
+    if (st) return st;
+    if (jac) A->stamp++;
+    return CHIDG_GPU_OK;
+}
+
+extern "C" int chidg_gpu_euler_pseudo_timestep(chidg_gpu_euler* E, chidg_gpu_vector* q, const double* cfl,
+                                               double* dtau) {
+    if (!E || !cfl || !dtau) return E ? fail(E->ctx, CHIDG_GPU_EINVAL, "euler_pseudo_timestep: null argument")
+                                      : CHIDG_GPU_EINVAL;
+    int st = check_vector(E, q, "q");
+    if (st) return st;
+    const dim3 grid(E->nelem), block(kThreads);
+    const Tables tb = tables_of(E);
+    const double* qp = (const double*)q->buf.ptr;
+    double* out = (double*)E->dtau.ptr;
+    if (E->order == 0) k_euler_dtau<1><<<grid, block, 0, E->ctx->stream>>>(E->g, tb, qp, E->h, cfl[0], cfl[1], cfl[2], cfl[3], cfl[4], out);
+    else if (E->order == 1) k_euler_dtau<8><<<grid, block, 0, E->ctx->stream>>>(E->g, tb, qp, E->h, cfl[0], cfl[1], cfl[2], cfl[3], cfl[4], out);
+    else k_euler_dtau<27><<<grid, block, 0, E->ctx->stream>>>(E->g, tb, qp, E->h, cfl[0], cfl[1], cfl[2], cfl[3], cfl[4], out);
+    st = check_launch(E->ctx, "k_euler_dtau");
+    if (st) return st;
+    cudaError_t ce = cudaMemcpyAsync(dtau, out, (size_t)E->nelem * 5 * sizeof(double), cudaMemcpyDeviceToHost,
+                                     E->ctx->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(E->ctx->stream);
+    return ce == cudaSuccess ? CHIDG_GPU_OK : cuda_fail(E->ctx, ce, "euler_pseudo_timestep");
+}

@@ -463,3 +463,82 @@ class EulerSystem:
 
     def pseudo_timestep(self, q, cfl):
         return self.box.pseudo_timestep(q.download(), cfl)
+
+
+class EulerDevice:
+    """The same discretisation assembled on the GPU (chidg_gpu_euler_*): the
+    residual into a device vector and the Jacobian straight into the device
+    matrix's blocks, orders 0..2.  The extent, boundary conditions and
+    freestream are the EulerBox's."""
+
+    def __init__(self, box: EulerBox, ctx: api.Context | None = None):
+        import ctypes as C
+
+        from . import _lib
+        if box.order > 2:
+            raise ValueError("EulerDevice: orders 0..2")
+        self.box = box
+        self.ctx = ctx or api.default_context()
+        d = _lib.EulerBoxDesc()
+        d.nx, d.ny, d.nz = box.shape
+        d.order = box.order
+        for i in range(3):
+            d.lo[i] = float(box.lo[i])
+            d.hi[i] = float(box.lo[i] + box.h[i] * box.shape[i])
+            d.vel_inf[i] = box.vel_inf[i]
+        for f in range(6):
+            d.bc[f] = _lib.EULER_FARFIELD if box.bcs[f] == "farfield" else _lib.EULER_EXTRAPOLATE
+        d.rho_inf, d.p_inf = box.rho_inf, box.p_inf
+        self._desc = d
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.L.chidg_gpu_euler_create(self.ctx.h, C.byref(d), C.byref(h)), "euler_create")
+        self.h = h
+
+    def assemble(self, q: api.ChidgVector, rhs: api.ChidgVector, A: api.ChidgMatrix | None = None):
+        """rhs = R(q); with A also A = dR/dq (every block of A overwritten)."""
+        self.ctx.check(self.ctx.L.chidg_gpu_euler_assemble(self.h, q.h, rhs.h, A.h if A is not None else None),
+                       "euler_assemble")
+
+    def pseudo_timestep(self, q: api.ChidgVector, cfl) -> np.ndarray:
+        cfl = np.ascontiguousarray(np.broadcast_to(np.asarray(cfl, dtype=np.float64), (NFIELDS,)))
+        out = np.empty((self.box.nelem, NFIELDS))
+        from . import _lib
+        self.ctx.check(self.ctx.L.chidg_gpu_euler_pseudo_timestep(self.h, q.h, cfl.ctypes.data_as(_lib.DP),
+                                                                  out.ctypes.data_as(_lib.DP)), "euler_pseudo_timestep")
+        return out
+
+    def release(self):
+        if getattr(self, "h", None):
+            self.ctx.L.chidg_gpu_euler_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
+class EulerDeviceSystem:
+    """The Newton driver's `system` with the assembly on the GPU: q, rhs and
+    the Jacobian never leave the device; only the pseudo time steps (nelem x 5)
+    come back to the host for chidg_gpu_matrix_scale_diagonal."""
+
+    def __init__(self, box: EulerBox, ctx: api.Context | None = None):
+        self.box = box
+        self.pattern = box.pattern
+        self.mass = box.mass
+        self.device = EulerDevice(box, ctx)
+        self.assemble_seconds = 0.0
+        self.nassemble = 0
+
+    def assemble(self, q, A, rhs, differentiate):
+        import time
+        t0 = time.perf_counter()
+        self.device.assemble(q, rhs, A if differentiate else None)
+        self.device.ctx.sync()
+        self.assemble_seconds += time.perf_counter() - t0
+        self.nassemble += 1
+
+    def pseudo_timestep(self, q, cfl):
+        return self.device.pseudo_timestep(q, cfl)

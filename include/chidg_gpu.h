@@ -364,6 +364,44 @@ int chidg_gpu_serve_wait(chidg_gpu_server* s, int64_t ticket, double* x, chidg_g
 int chidg_gpu_serve_stats(chidg_gpu_server* s, int64_t* batches, int64_t* peak_mem_bytes);
 int chidg_gpu_serve_destroy(chidg_gpu_server* s);
 
+/* ---- Euler DG assembly on hex boxes (the caller side of the solves) ------- */
+/* The residual and Jacobian of ChiDG's Euler discretisation
+ * (src/spatial/mod_spatial.f90:40-197 over the operators of
+ * src/equations/fluid/euler/: euler_volume_operator, euler_boundary_average_
+ * operator, euler_roe_operator, euler_bc_operator; boundary states
+ * bc_state_farfield.f90 and bc_state_fluid_extrapolate.f90) on an
+ * nx x ny x nz box of affine hexes, elements i-fastest, assembled on the
+ * device: rhs = R(q) as the reference stores it (volume integrals negated,
+ * face integrals added, mod_integrate.f90:652-1022), and the Jacobian dR/dq
+ * into the DIAG and interior-face blocks of a matrix holding exactly the box
+ * pattern (one time level, 5 fields, (P+1)^3 modes).  Orders 0..2; modal
+ * Legendre basis in the reference's mode order (mod_ordering.f90),
+ * Gauss-Legendre quadrature with ceil(3 (P+1) / 2) nodes per direction
+ * (gq_rule = 2).  Not in the reference's C-callable surface: its assembly is
+ * Fortran on the CPU ranks (replaces the call of update_space,
+ * mod_spatial.f90:40, for such boxes). */
+#define CHIDG_EULER_FARFIELD    0   /* bc_state_farfield: Riemann invariants, inflow by normal momentum <= RKTOL */
+#define CHIDG_EULER_EXTRAPOLATE 1   /* bc_state_fluid_extrapolate: exterior state = interior state               */
+typedef struct chidg_gpu_euler_box {
+    int32_t nx, ny, nz;        /* elements per direction                                          */
+    int32_t order;             /* polynomial order P, 0..2                                        */
+    double lo[3], hi[3];       /* box extent                                                      */
+    int32_t bc[6];             /* CHIDG_EULER_* on faces XI_MIN, XI_MAX, ETA_MIN, ..., ZETA_MAX     */
+    double rho_inf, p_inf;     /* farfield density and pressure                                   */
+    double vel_inf[3];         /* farfield velocity                                               */
+} chidg_gpu_euler_box;
+typedef struct chidg_gpu_euler chidg_gpu_euler;
+int chidg_gpu_euler_create(chidg_gpu_ctx* ctx, const chidg_gpu_euler_box* box, chidg_gpu_euler** out);
+int chidg_gpu_euler_destroy(chidg_gpu_euler* E);
+/* rhs = R(q); with A non-NULL also A's blocks = dR/dq (every block of A is
+ * overwritten; bumps A's stamp).  q and rhs: vectors of the box's length, on
+ * E's context; q is read only. */
+int chidg_gpu_euler_assemble(chidg_gpu_euler* E, chidg_gpu_vector* q, chidg_gpu_vector* rhs, chidg_gpu_matrix* A);
+/* dtau[e * 5 + f] = cfl[f] h / (mean |u| + mean c) over the element's volume
+ * nodes, h = vol^(1/3) (src/equations/fluid/type_fluid_pseudo_timestep.f90);
+ * cfl holds 5 values, dtau nelem * 5 (host). */
+int chidg_gpu_euler_pseudo_timestep(chidg_gpu_euler* E, chidg_gpu_vector* q, const double* cfl, double* dtau);
+
 #ifdef __cplusplus
 }
 #endif
