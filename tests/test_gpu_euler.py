@@ -152,11 +152,11 @@ def test_device_assembly_matches_host(shape, P, bcs):
     assert np.abs(got - vals).max() <= 1e-12 * scale
     assert np.abs(got - vals).reshape(-1, b * b).max(axis=1).max() <= 1e-12 * scale
     # residual only: same rhs, the matrix untouched
-    stamp = A.stamp()
+    stamp = A.stamp
     rg2 = api.ChidgVector(A)
     dev.assemble(qg, rg2)
     assert np.array_equal(rg2.download(), rg.download())
-    assert A.stamp() == stamp
+    assert A.stamp == stamp
     dtau = dev.pseudo_timestep(qg, [1.0, 2.0, 3.0, 4.0, 5.0])
     assert relerr(dtau, box.pseudo_timestep(q, [1.0, 2.0, 3.0, 4.0, 5.0])) < 1e-13
 
