@@ -36,6 +36,15 @@ module chidg_gpu_mod
         integer(c_int32_t) :: mixed_inner_nmax
     end type chidg_gpu_fgmres_opts
 
+    ! chidg_gpu_euler_box: the Euler box of chidg_gpu_euler_create
+    type, bind(c) :: chidg_gpu_euler_box
+        integer(c_int32_t) :: nx, ny, nz, order
+        real(c_double)     :: lo(3), hi(3)
+        integer(c_int32_t) :: bc(6)
+        real(c_double)     :: rho_inf, p_inf
+        real(c_double)     :: vel_inf(3)
+    end type chidg_gpu_euler_box
+
     type, bind(c) :: chidg_gpu_fgmres_result
         integer(c_int32_t) :: niter, nrestart, inner_iters, nhist
         real(c_double)     :: residual_norm, res_estimate, r0norm_initial, seconds
@@ -186,6 +195,27 @@ module chidg_gpu_mod
         integer(c_int) function chidg_gpu_fgmres_default_opts(opts) bind(c, name='chidg_gpu_fgmres_default_opts')
             import :: c_int, chidg_gpu_fgmres_opts
             type(chidg_gpu_fgmres_opts) :: opts
+        end function
+        integer(c_int) function chidg_gpu_euler_create(ctx, box, E) bind(c, name='chidg_gpu_euler_create')
+            import :: c_int, c_ptr, chidg_gpu_euler_box
+            type(c_ptr), value        :: ctx
+            type(chidg_gpu_euler_box) :: box
+            type(c_ptr)               :: E
+        end function
+        integer(c_int) function chidg_gpu_euler_destroy(E) bind(c, name='chidg_gpu_euler_destroy')
+            import :: c_int, c_ptr
+            type(c_ptr), value :: E
+        end function
+        ! pass c_null_ptr as mat for the residual alone (the line search)
+        integer(c_int) function chidg_gpu_euler_assemble(E, q, rhs, mat) bind(c, name='chidg_gpu_euler_assemble')
+            import :: c_int, c_ptr
+            type(c_ptr), value :: E, q, rhs, mat
+        end function
+        integer(c_int) function chidg_gpu_euler_pseudo_timestep(E, q, cfl, dtau) &
+                bind(c, name='chidg_gpu_euler_pseudo_timestep')
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: E, q
+            real(c_double)     :: cfl(5), dtau(*)
         end function
     end interface
 

@@ -175,7 +175,7 @@ def test_device_assembly_rejects_other_patterns():
 
 def test_newton_device_assembly_matches_host_assembly():
     """The Newton driver with the assembly on the device against the same
-    driver with the host assembly: identical steps to 1e-9."""
+    driver with the host assembly: the same steps, residuals within 1e-9."""
     box = euler.EulerBox(4, 3, 3, 1)
     q0 = box.density_bump(amplitude=1e-2, width=0.2, centre=(0.45, 0.55, 0.5))
     opts = dict(tol=1e-12, rtol=1e-8, nmax=6, ptc=True, cfl0=10.0)
@@ -189,6 +189,8 @@ def test_newton_device_assembly_matches_host_assembly():
     (rh, qh), (rd, qd) = out
     assert len(rh.residual_norm) == len(rd.residual_norm)
     for a, b in zip(rd.residual_norm, rh.residual_norm):
-        assert abs(a - b) <= 1e-9 * b
+        # relative 1e-9, with a floor of 1e-14 for the rounding of the O(1)
+        # fluxes that sum to the last, small residuals (~1e-11 of |R0| here)
+        assert abs(a - b) <= 1e-9 * b + 1e-14
     assert rd.alphas == rh.alphas
     assert relerr(qd, qh) < 1e-10
