@@ -440,8 +440,9 @@ def run_assembly_leg(ctx, stream, A, reps=3):
     """The Euler DG residual and Jacobian of the 24^3 P2 box assembled on the
     device (k_euler_assemble) into the 24^3 P2 matrix (its synthetic values are
     overwritten: the leg runs after every leg that reads them), then one whole
-    Newton step on it: assembly, pseudo-transient term, FGMRES(50) + ILU0 to
-    rtol 1e-8, backtracking.  Farfield on every face, M 0.3 with a Gaussian
+    Newton step on it (the second of two, the first builds the ILU programme):
+    assembly, pseudo-transient term, FGMRES(50) + ILU0 to rtol 1e-8,
+    backtracking.  Farfield on every face, M 0.3 with a Gaussian
     density bump (amplitude 1e-2, width 0.1).  Algorithmic work per element:
     the DIAG block 25 nt rows x [qv (3 + nt) + 6 qf (1 + nt)] FMAs, each
     interior-face block 25 nt x qf (1 + nt) FMAs; bytes: the blocks and rhs
@@ -479,16 +480,20 @@ def run_assembly_leg(ctx, stream, A, reps=3):
            "gflops": 2.0 * fma / (jac_ms / 1e3) / 1e9, "flops_per_call": 2.0 * fma,
            "gbs_written": nbytes / (jac_ms / 1e3) / 1e9, "bytes_per_call": nbytes}
     sysm = euler.EulerDeviceSystem(box, ctx)
+    sysm.device.release()
     sysm.device = dev
     solver = api.create_linear_solver("fgmres", **SOLVER)
-    t0 = time.perf_counter()
-    res = Newton(nmax=1, tol=0.0, rtol=0.0, cfl0=10.0).solve(sysm, q, A, solver,
-                                                             api.create_preconditioner("ilu0"))
+    M = api.create_preconditioner("ilu0")
+    for rep in range(2):                             # the first step builds the ILU programme
+        sysm.assemble_seconds, sysm.nassemble = 0.0, 0
+        t0 = time.perf_counter()
+        res = Newton(nmax=1, tol=0.0, rtol=0.0, cfl0=10.0).solve(sysm, q, A, solver, M)
     out["newton_step"] = {"seconds": time.perf_counter() - t0, "seconds_linear_solve": res.linear_seconds[0],
                           "seconds_assembly": sysm.assemble_seconds, "assemblies": sysm.nassemble,
                           "linear_iterations": res.matrix_iterations[0],
                           "linear_true_rel_residual": res.linear_rel_residual[0],
                           "residual_history": [float(v) for v in res.residual_norm], "alpha": res.alphas[0]}
+    M.tear_down()
     for o in (q, r):
         o.release()
     dev.release()

@@ -6,6 +6,10 @@ blocks).  n = 12 gives a 1.7 GB matrix: larger than L2 (126 MB), small enough
 for multi-pass profiler captures.
 
   python -m chidg_b200.profile_case --n 12 --reps 2
+
+With --euler: `--reps` device assemblies of the Euler DG residual and
+Jacobian of the n^3 box at order p (farfield, M 0.3, a density bump) into the
+box's matrix (k_euler_assemble).
 """
 from __future__ import annotations
 
@@ -27,7 +31,11 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed_fp32", "mixed_bf16", "mixed_precon_fp32"],
                     help="precision of the preconditioner update (mixed_fp32 / mixed_bf16 factor in FP32 and skip "
                          "the FP64 apply)")
+    ap.add_argument("--euler", action="store_true",
+                    help="run the device Euler DG assembly (residual + Jacobian) instead of the solver kernels")
     args = ap.parse_args()
+    if args.euler:
+        return euler_case(args)
     pat = mesh.box_pattern(args.n, args.n, args.n, 5, mesh.nterms_of_order(args.p))
     A = api.ChidgMatrix(pat)
     A.upload(mesh.synth_values(pat, seed=1))
@@ -87,6 +95,26 @@ def solve_timings(n=24, p=2, reps=6, precisions=("fp64", "mixed_fp32", "mixed_bf
         out[prec] = (times, s.niter, s.inner_iters)
         print(f"  {prec:10s} iters {s.niter:3d}+{s.inner_iters:3d}  " + " ".join(f"{1e3 * t:7.1f}" for t in times) + " ms")
     return out
+
+
+def euler_case(args):
+    import time
+
+    from . import euler
+    box = euler.EulerBox(args.n, args.n, args.n, args.p)
+    A = api.ChidgMatrix(box.pattern)
+    dev = euler.EulerDevice(box, A.ctx)
+    q = api.ChidgVector(A, box.density_bump(amplitude=1e-2, width=0.1, centre=(0.45, 0.55, 0.5)))
+    r = api.ChidgVector(A)
+    dev.assemble(q, r, A)
+    A.ctx.sync()
+    t0 = time.perf_counter()
+    for _ in range(args.reps):
+        dev.assemble(q, r, A)
+    A.ctx.sync()
+    ms = (time.perf_counter() - t0) * 1e3 / max(args.reps, 1)
+    print(f"profile_case euler n={args.n} p={args.p}: {args.reps} assemblies, {ms:.3f} ms each (host clock), "
+          f"{A.ctx.launches()} launches")
 
 
 if __name__ == "__main__":
