@@ -430,7 +430,8 @@ def run_newton_leg(ctx):
                      "seconds_assembly": sysm.assemble_seconds, "assemblies": sysm.nassemble,
                      "residual_history": [float(r) for r in res.residual_norm],
                      "linear_iterations": res.matrix_iterations,
-                     "linear_true_rel_residual": [float(r) for r in res.linear_rel_residual], "alphas": res.alphas}
+                     "linear_true_rel_residual": [float(r) for r in res.linear_rel_residual], "alphas": res.alphas,
+                     "phase_seconds": res.phase_seconds}
     dev.device.release()
     A.release()
     return out
@@ -492,7 +493,8 @@ def run_assembly_leg(ctx, stream, A, reps=3):
                           "seconds_assembly": sysm.assemble_seconds, "assemblies": sysm.nassemble,
                           "linear_iterations": res.matrix_iterations[0],
                           "linear_true_rel_residual": res.linear_rel_residual[0],
-                          "residual_history": [float(v) for v in res.residual_norm], "alpha": res.alphas[0]}
+                          "residual_history": [float(v) for v in res.residual_norm], "alpha": res.alphas[0],
+                          "phase_seconds": res.phase_seconds}
     M.tear_down()
     for o in (q, r):
         o.release()

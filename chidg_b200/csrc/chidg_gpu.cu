@@ -426,7 +426,7 @@ extern "C" int chidg_gpu_matrix_destroy(chidg_gpu_matrix* A) {
     cudaStreamSynchronize(A->ctx->stream);
     for (Buffer* b : {&A->val, &A->val32, &A->val16, &A->d_row_ptr, &A->d_blk_voff, &A->d_blk_xoff, &A->d_blk_nc,
                       &A->d_row_yoff, &A->d_row_b, &A->d_diag_voff, &A->d_elem_nvars, &A->d_elem_nterms, &A->row_sq,
-                      &A->d_tr_src, &A->d_tr_dst, &A->d_tr_nr, &A->d_tr_nc})
+                      &A->d_tr_src, &A->d_tr_dst, &A->d_tr_nr, &A->d_tr_nc, &A->d_mass_off, &A->d_scale_off})
         release(*b);
     if (A->T) chidg_gpu_matrix_destroy(A->T);
     delete A;
@@ -515,17 +515,29 @@ extern "C" int chidg_gpu_matrix_scale_diagonal(chidg_gpu_matrix* A, const double
     if (!A || !mass || !scale) return CHIDG_GPU_EINVAL;
     chidg_gpu_ctx* ctx = A->ctx;
     cudaSetDevice(ctx->device);
-    std::vector<int64_t> moff(A->nelem), soff(A->nelem);
     int64_t m = 0, s = 0;
     for (int e = 0; e < A->nelem; ++e) {
-        moff[e] = m; m += (int64_t)A->nterms[e] * A->nterms[e];
-        soff[e] = s; s += A->nvars[e];
+        m += (int64_t)A->nterms[e] * A->nterms[e];
+        s += A->nvars[e];
     }
-    Buffer dm, ds, dmo, dso;
     int st;
-    if ((st = ensure(ctx, dm, sizeof(double) * m)) || (st = ensure(ctx, ds, sizeof(double) * s)) ||
-        (st = upload_array(ctx, dmo, moff)) || (st = upload_array(ctx, dso, soff))) {
-        release(dm); release(ds); release(dmo); release(dso);
+    if (!A->d_mass_off.ptr) {                // per-element offsets of mass and scale: fixed by the pattern
+        std::vector<int64_t> moff(A->nelem), soff(A->nelem);
+        int64_t mm = 0, ss = 0;
+        for (int e = 0; e < A->nelem; ++e) {
+            moff[e] = mm; mm += (int64_t)A->nterms[e] * A->nterms[e];
+            soff[e] = ss; ss += A->nvars[e];
+        }
+        if ((st = upload_array(ctx, A->d_mass_off, moff)) || (st = upload_array(ctx, A->d_scale_off, soff))) {
+            release(A->d_mass_off); release(A->d_scale_off);
+            return st;
+        }
+    }
+    const Buffer& dmo = A->d_mass_off;
+    const Buffer& dso = A->d_scale_off;
+    Buffer dm, ds;
+    if ((st = ensure(ctx, dm, sizeof(double) * m)) || (st = ensure(ctx, ds, sizeof(double) * s))) {
+        release(dm); release(ds);
         return st;
     }
     cudaMemcpyAsync(dm.ptr, mass, sizeof(double) * m, cudaMemcpyHostToDevice, ctx->stream);
@@ -536,7 +548,7 @@ extern "C" int chidg_gpu_matrix_scale_diagonal(chidg_gpu_matrix* A, const double
                                                       (const int64_t*)dso.ptr, A->ntime);
     st = check_launch(ctx, "k_scale_diagonal");
     cudaStreamSynchronize(ctx->stream);
-    release(dm); release(ds); release(dmo); release(dso);
+    release(dm); release(ds);
     if (st) return st;
     A->stamp++;
     return CHIDG_GPU_OK;

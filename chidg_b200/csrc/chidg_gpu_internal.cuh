@@ -148,6 +148,7 @@ struct chidg_gpu_matrix {
     chidg_gpu_matrix* T = nullptr;
     int64_t T_src_stamp = -1;                // stamp of A that T's values were transposed from
     chidg::Buffer d_tr_src, d_tr_dst, d_tr_nr, d_tr_nc;   // per block of T: source / target offsets, T's block dims
+    chidg::Buffer d_mass_off, d_scale_off;   // scale_diagonal: per-element offsets into mass and scale
 
     int bsize(int e) const { return nvars[e] * nterms[e]; }
     int64_t seg(int e, int t) const { return eoff[e] + (int64_t)t * bsize(e); }

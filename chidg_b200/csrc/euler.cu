@@ -400,47 +400,75 @@ __global__ void __launch_bounds__(kThreads) k_euler_assemble(BoxGeom g, Tables t
     }
 
     // 4. DIAG block and 5. face blocks (skipped for a residual-only call): one
-    // thread per (f, m, g) row of outputs, all nt columns n in registers; block
-    // entry (f nt + m, g nt + n) stored column-major.  Lanes of a warp take
-    // consecutive m: coalesced stores.
+    // thread per pair of (f, m, g) rows with the same f and g and modes m0,
+    // m0 + 1, all nt columns n of both in registers, so each basis value
+    // loaded feeds two FMAs; block entry (f nt + m, g nt + n) stored
+    // column-major.  Lanes of a warp take consecutive mode pairs.
     if (val == nullptr) return;
+    const int npair = (nt + 1) >> 1;
     for (int blk = 6; blk >= 0; --blk) {
         if (blk < 6 && nbr[blk] < 0) continue;
         double* out = val + blk_off[(int64_t)e * 7 + blk];
-        for (int rid = threadIdx.x; rid < 25 * nt; rid += blockDim.x) {
-            const int m = rid % nt, fg = rid / nt, f = fg % 5, gg = fg / 5;
-            double acc[NT];
+        for (int item = threadIdx.x; item < 25 * npair; item += blockDim.x) {
+            const int mp = item % npair, fg = item / npair, f = fg % 5, gg = fg / 5;
+            const int m0 = 2 * mp;
+            const bool two = m0 + 1 < nt;
+            const int m1 = two ? m0 + 1 : m0;
+            double a0[NT], a1[NT];
 #pragma unroll
-            for (int n = 0; n < NT; ++n) acc[n] = 0.0;
+            for (int n = 0; n < NT; ++n) { a0[n] = 0.0; a1[n] = 0.0; }
             if (blk == 6) {
                 for (int qq = 0; qq < qv; ++qq) {
-                    const double tcoef = -(tb.grad[(0 * qv + qq) * nt + m] * sWdF[((qq * 3 + 0) * 5 + f) * 5 + gg]
-                                         + tb.grad[(1 * qv + qq) * nt + m] * sWdF[((qq * 3 + 1) * 5 + f) * 5 + gg]
-                                         + tb.grad[(2 * qv + qq) * nt + m] * sWdF[((qq * 3 + 2) * 5 + f) * 5 + gg]);
+                    const double w0 = sWdF[((qq * 3 + 0) * 5 + f) * 5 + gg];
+                    const double w1 = sWdF[((qq * 3 + 1) * 5 + f) * 5 + gg];
+                    const double w2 = sWdF[((qq * 3 + 2) * 5 + f) * 5 + gg];
+                    const double* g0 = tb.grad + (size_t)(0 * qv + qq) * nt;
+                    const double* g1 = tb.grad + (size_t)(1 * qv + qq) * nt;
+                    const double* g2 = tb.grad + (size_t)(2 * qv + qq) * nt;
+                    const double t0 = -(g0[m0] * w0 + g1[m0] * w1 + g2[m0] * w2);
+                    const double t1 = -(g0[m1] * w0 + g1[m1] * w1 + g2[m1] * w2);
                     const double* ph = tb.phi + (size_t)qq * nt;
 #pragma unroll
-                    for (int n = 0; n < NT; ++n) acc[n] += tcoef * ph[n];
+                    for (int n = 0; n < NT; ++n) {
+                        const double p = ph[n];
+                        a0[n] += t0 * p;
+                        a1[n] += t1 * p;
+                    }
                 }
                 for (int face = 0; face < 6; ++face) {
                     for (int qq = 0; qq < qf; ++qq) {
                         const double* pf = tb.phif + ((size_t)face * qf + qq) * nt;
-                        const double tcoef = pf[m] * sFs[((size_t)face * qf + qq) * 25 + f * 5 + gg];
+                        const double w = sFs[((size_t)face * qf + qq) * 25 + f * 5 + gg];
+                        const double t0 = pf[m0] * w, t1 = pf[m1] * w;
 #pragma unroll
-                        for (int n = 0; n < NT; ++n) acc[n] += tcoef * pf[n];
+                        for (int n = 0; n < NT; ++n) {
+                            const double p = pf[n];
+                            a0[n] += t0 * p;
+                            a1[n] += t1 * p;
+                        }
                     }
                 }
             } else {
                 for (int qq = 0; qq < qf; ++qq) {
                     const double* pf = tb.phif + ((size_t)blk * qf + qq) * nt;
                     const double* pn = tb.phif + ((size_t)(blk ^ 1) * qf + qq) * nt;
-                    const double tcoef = pf[m] * sFn[((size_t)blk * qf + qq) * 25 + f * 5 + gg];
+                    const double w = sFn[((size_t)blk * qf + qq) * 25 + f * 5 + gg];
+                    const double t0 = pf[m0] * w, t1 = pf[m1] * w;
 #pragma unroll
-                    for (int n = 0; n < NT; ++n) acc[n] += tcoef * pn[n];
+                    for (int n = 0; n < NT; ++n) {
+                        const double p = pn[n];
+                        a0[n] += t0 * p;
+                        a1[n] += t1 * p;
+                    }
                 }
             }
-            const int row = f * nt + m;
+            const int row = f * nt + m0;
 #pragma unroll
-            for (int n = 0; n < NT; ++n) out[(int64_t)(gg * nt + n) * b + row] = acc[n];
+            for (int n = 0; n < NT; ++n) {
+                double* col = out + (int64_t)(gg * nt + n) * b + row;
+                col[0] = a0[n];
+                if (two) col[1] = a1[n];
+            }
         }
     }
 }

@@ -58,6 +58,7 @@ class NewtonResult:
     alphas: list = field(default_factory=list)
     cfl: list = field(default_factory=list)
     seconds: float = 0.0
+    phase_seconds: dict = field(default_factory=dict)    # wall time by phase: assembly, ptc, linear, search, other
     converged: bool = False
 
 
@@ -76,6 +77,7 @@ class Newton:
         o = self.options
         res = NewtonResult()
         t_start = time.perf_counter()
+        ph = {"assembly": 0.0, "ptc": 0.0, "linear": 0.0, "search": 0.0}
         nfields = int(A.pattern.elem_nvars[0])
         rhs = api.ChidgVector(A)
         dq = api.ChidgVector(A)
@@ -90,7 +92,9 @@ class Newton:
             niter += 1
             qold.copy_from(q)
             # residual and linearisation (:140-146)
+            t0 = time.perf_counter()
             system.assemble(q, A, rhs, differentiate=True)
+            ph["assembly"] += time.perf_counter() - t0
             if niter == 1:
                 resid0 = rhs.norm()
                 cfln = np.full(nfields, o.cfl0)
@@ -98,12 +102,14 @@ class Newton:
             b.copy_from(rhs)                                 # b = -rhs (:180)
             b.scale(-1.0)
             if o.ptc:                                        # contribute_pseudo_temporal (:320-352)
+                t0 = time.perf_counter()
                 dtau = np.asarray(system.pseudo_timestep(q, cfln), dtype=np.float64)
                 if dtau.ndim == 1:                           # one pseudo time step per element
                     scale = np.repeat(1.0 / dtau, A.pattern.elem_nvars)
                 else:                                        # per element and field (elems(:)%dtau(ieqn))
                     scale = (1.0 / dtau).reshape(-1)
                 A.scale_diagonal(system.mass, scale)
+                ph["ptc"] += time.perf_counter() - t0
             if niter == 1:
                 res.residual_norm.append(resid)
             if resid < o.tol:
@@ -115,6 +121,8 @@ class Newton:
             t0 = time.perf_counter()
             linear_solver.solve(A, dq, b, preconditioner)
             res.linear_seconds.append(time.perf_counter() - t0)
+            ph["linear"] += res.linear_seconds[-1]
+            t0 = time.perf_counter()
             res.linear_rel_residual.append(linear_solver.residual_norm / max(linear_solver.r0norm_initial, 1e-300))
             # line search (:219-240, backtracking :466-549)
             f0 = resid
@@ -154,6 +162,7 @@ class Newton:
                 system.assemble(q, A, rhs, differentiate=False)
                 fn = rhs.norm()
             q.copy_from(qn)
+            ph["search"] += time.perf_counter() - t0
             res.matrix_iterations.append(linear_solver.niter)
             res.residual_norm.append(fn)
             res.alphas.append(alpha)
@@ -163,6 +172,8 @@ class Newton:
                 break
         res.niter = niter
         res.seconds = time.perf_counter() - t_start
+        ph["other"] = res.seconds - sum(ph.values())
+        res.phase_seconds = ph
         for v in (rhs, dq, b, qold, qn):
             v.release()
         return res
