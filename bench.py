@@ -4,8 +4,10 @@ One step = one Newton linear solve: the block-ILU0 factorisation of a freshly
 assembled Jacobian followed by FGMRES(50) to a relative residual of 1e-8 and
 the true-residual check, all in FP64 (the plain GPU path).  Workload: 24x24x24
 hex box, 5 fields, P2 (27 modes) -> 13 824 elements, 93 312 blocks of
-135 x 135, 13.6 GB of FP64 blocks, seeded synthetic values with the ChiDG
-block layout (no reference-assembled Jacobians exist in this environment).
+135 x 135, 13.6 GB of FP64 blocks: the first Newton step's system of the
+Euler equations on that box (freestream M 0.3 with a seeded Gaussian density
+bump, farfield boundaries), its Jacobian assembled on the device by the DG
+restatement, the pseudo-transient term at cfl 10 added, b = -R(q0).
 
 Prints one JSON line (rank 0).  `value` times the solves with A and b resident
 in HBM; `e2e` times the same solves through the C ABI from pinned host
@@ -45,7 +47,10 @@ def workload_config(extra=None):
                        "block-ILU0 factorisation + FGMRES(50) to rtol 1e-8, CGS, no inner FGMRES",
            "elements": NX * NY * NZ, "block": NVARS * (P + 1) ** 3, "blocks": 93312,
            "matrix_bytes_fp64": 13604889600, "l2_flush": "inputs larger than L2 (13.6 GB matrix)",
-           "parallelism": "replicas", "values": "seeded synthetic Jacobian (ChiDG block layout)"}
+           "parallelism": "replicas",
+           "values": "Euler DG Newton system at the initial state: Jacobian (assembled on the device) + the "
+                     "pseudo-transient term at cfl 10, b = -R(q0); freestream M 0.3, rho 1, p 1/gamma, Gaussian "
+                     "density bump (amplitude 1e-2, width 0.1, seeded centre in [0.3, 0.7]^3), farfield on every face"}
     if extra:
         cfg.update(extra)
     return cfg
@@ -164,17 +169,35 @@ BATCH_SYSTEMS = 48
 BATCH_OPTS = dict(tol=0.0, rtol=1e-8, nkrylov=30, inner_fgmres=0, nmax=1000, use_controller=0)
 
 
-def uneven_systems(count, seed, max_n=8):
-    """Boxes with each side uniform in {4..max_n} and P uniform in {1, 2} (40x40 or
-    135x135 blocks), seeded synthetic values and right-hand sides."""
-    from chidg_b200 import mesh
+_SYSTEMS = {}
+
+
+def uneven_systems(count, seed, max_n=8, device=0):
+    """Euler boxes with each side uniform in {4..max_n}, P uniform in {1, 2}
+    (40x40 or 135x135 blocks), freestream Mach uniform in [0.2, 0.6] and bump
+    amplitude uniform in [1e-3, 1e-2] (the scope table's draws for many solves,
+    with smaller boxes): the first Newton step's system of each, assembled on
+    the device and returned as host arrays (pattern, values, right-hand side)."""
+    key = (count, seed, max_n)
+    if key in _SYSTEMS:
+        return _SYSTEMS[key]
+    from chidg_b200 import api, euler
+    ctx = api.default_context(device)
     rng = np.random.default_rng(seed)
     out = []
     for i in range(count):
         nx, ny, nz = (int(v) for v in rng.integers(4, max_n + 1, size=3))
         P_ = int(rng.integers(1, 3))
-        pat = mesh.box_pattern(nx, ny, nz, NVARS, mesh.nterms_of_order(P_))
-        out.append((pat, mesh.synth_values(pat, seed=1000 + i), mesh.synth_vector(pat.vector_size(), seed=2000 + i)))
+        mach, amp = float(rng.uniform(0.2, 0.6)), float(rng.uniform(1e-3, 1e-2))
+        centre = tuple(float(c) for c in rng.uniform(0.3, 0.7, 3))
+        box = euler.EulerBox(nx, ny, nz, P_, vel_inf=(mach, 0.0, 0.0))
+        q0 = box.density_bump(amplitude=amp, width=0.1, centre=centre)
+        A = api.ChidgMatrix(box.pattern, ctx)
+        b, _ = device_newton_system(ctx, A, box, q0)
+        out.append((box.pattern, A.download(), b.download()))
+        b.release()
+        A.release()
+    _SYSTEMS[key] = out
     return out
 
 
@@ -238,7 +261,7 @@ def run_batch_leg(ctx, schedule, reps=3):
             "batched": batched}
 
 
-def serve_requests(count, seed, pinned=True):
+def serve_requests(count, seed, pinned=True, device=0):
     """Requests of the batch leg's sizes, every 10th a harmonic-balance one
     (8^3 box, P1, 7 coupled time levels: 3 harmonics).  The values and
     right-hand sides arrive in page-locked host memory, as a front end's
@@ -255,7 +278,7 @@ def serve_requests(count, seed, pinned=True):
         return t
 
     out = []
-    for i, (p, v, r) in enumerate(uneven_systems(count, seed=seed)):
+    for i, (p, v, r) in enumerate(uneven_systems(count, seed=seed, device=device)):
         if i % 10 == 9:
             p = mesh.box_pattern(8, 8, 8, NVARS, mesh.nterms_of_order(1), ntime=7)
             v = mesh.synth_values(p, seed=3000 + i)
@@ -284,18 +307,19 @@ def run_serve_subprocess(device, timeout=900):
 def run_serve_leg(device, requests=64, rate=200.0):
     from chidg_b200 import serve
     out = {"arrival_rate_per_s": rate, "requests": requests, "slots": 2, "max_batch": 16,
-           "workload": "Poisson arrivals; boxes 4..8 per side, P in {1,2}; every 10th request harmonic balance "
-                       "(8^3, P1, 7 time levels); FGMRES(30)+ILU0 to rtol 1e-8 (FP64 residual); request values "
-                       "in page-locked host memory; the server in a process of its own"}
+           "workload": "Poisson arrivals; Euler Newton systems of boxes 4..8 per side, P in {1,2}, Mach in "
+                       "[0.2, 0.6]; every 10th request harmonic balance (8^3, P1, 7 time levels, synthetic values); "
+                       "FGMRES(30)+ILU0 to rtol 1e-8 (FP64 residual); request values in page-locked host memory; "
+                       "the server in a process of its own"}
     out["server"] = "native (chidg_gpu_serve_*: dispatcher and worker slots as native threads)"
     for key, cls, prec in (("fp64", serve.NativeServer, "fp64"),
                            ("mixed_precon_fp32", serve.NativeServer, "mixed_precon_fp32"),
                            ("python_server_fp64", serve.Server, "fp64")):
-        reqs = serve_requests(requests, seed=11)
+        reqs = serve_requests(requests, seed=11, device=device)
         srv = cls(device=device, slots=2, max_batch=16, mem_budget=40 << 30, **BATCH_OPTS, precision=prec)
         try:
             # warm-up: a batch of the stream's kinds (P1 and P2 boxes, one harmonic-balance system)
-            for f in [srv.submit(r) for r in serve_requests(10, seed=12)]:
+            for f in [srv.submit(r) for r in serve_requests(10, seed=12, device=device)]:
                 f.result()
             st = serve.run_stream(srv, reqs, serve.poisson_arrivals(requests, rate, seed=5))
         finally:
@@ -439,7 +463,7 @@ def run_newton_leg(ctx):
 
 def run_assembly_leg(ctx, stream, A, reps=3):
     """The Euler DG residual and Jacobian of the 24^3 P2 box assembled on the
-    device (k_euler_assemble) into the 24^3 P2 matrix (its synthetic values are
+    device (k_euler_assemble) into the 24^3 P2 matrix (its values are
     overwritten: the leg runs after every leg that reads them), then one whole
     Newton step on it (the second of two, the first builds the ILU programme):
     assembly, pseudo-transient term, FGMRES(50) + ILU0 to rtol 1e-8,
@@ -509,21 +533,20 @@ CFG3_SOLVER = dict(tol=0.0, rtol=1e-8, nkrylov=30, inner_fgmres=0, nmax=600, ort
 
 
 def run_cfg3_leg(ctx, stream, schedule, reps=2):
-    """32^3 P2 (223 232 blocks of 135 x 135, 32.5 GB FP64): FGMRES(30) to rtol
-    1e-8 with block-ILU0 in FP64, with FP32 factors and FP32 Krylov, with BF16
+    """32^3 P2 Euler (223 232 blocks of 135 x 135, 32.5 GB FP64; freestream Mach
+    drawn from a seeded U[0.2, 0.6]), the first Newton step's system:
+    FGMRES(30) to rtol 1e-8 with block-ILU0 in FP64, with FP32 factors and FP32 Krylov, with BF16
     factors and FP32 Krylov, and RAS+ILU0 over 4 x 4 x 4 box subdomains of 8^3
     elements (each subdomain plays one MPI rank) in FP64 and with FP32 inner
     solves.  Every mode reaches the same FP64 true residual."""
     import torch
 
     from chidg_b200 import api, mesh
-    pat = mesh.box_pattern(*CFG3, NVARS, mesh.nterms_of_order(P), subdomains=CFG3_SUB)
-    A = api.ChidgMatrix(pat, ctx)
+    mach = float(np.random.default_rng(SEED_B + 3).uniform(0.2, 0.6))
     t0 = time.perf_counter()
-    vals = mesh.synth_values(pat, seed=SEED_A + 3)
-    A.upload(vals)
-    del vals
-    b = api.ChidgVector(A, mesh.synth_vector(pat.vector_size(), seed=SEED_B + 3))
+    box, q0, centre = euler_box(CFG3[0], SEED_A + 3, mach=mach, subdomains=CFG3_SUB)
+    A = api.ChidgMatrix(box.pattern, ctx)
+    b, assembly_s = device_newton_system(ctx, A, box, q0)
     setup_s = time.perf_counter() - t0
     x_ref = None
     out = {}
@@ -568,19 +591,64 @@ def run_cfg3_leg(ctx, stream, schedule, reps=2):
     free, total = torch.cuda.mem_get_info()
     b.release()
     A.release()
-    return {"workload": "32^3 hex box, 5 fields, P2 (223232 blocks of 135x135, 32.5 GB FP64), FGMRES(30) "
+    return {"workload": "32^3 hex box, Euler, P2 (223232 blocks of 135x135, 32.5 GB FP64): the first Newton step's "
+                        "system (device-assembled Jacobian + pseudo-transient term at cfl 10, b = -R(q0)), FGMRES(30) "
                         "to rtol 1e-8 (FP64 true residual); RAS over 4x4x4 subdomains of 8^3, 1-element overlap",
+            "mach": mach, "bump_centre": [float(c) for c in centre], "device_assembly_s": assembly_s,
             "setup_s": setup_s, "device_bytes_in_use_at_end": int(total - free), "modes": out}
 
 
-def cpu_sample_solve(seed_a=SEED_A, seed_b=SEED_B, n=SAMPLE_N):
-    """One full FGMRES(50)+ILU0 FP64 solve of an n^3 P2 box on one host core."""
-    from chidg_b200 import mesh
+CFL_PTC = 10.0          # pseudo-transient cfl of the Newton systems solved
+
+
+def euler_box(n, seed, order=P, mach=0.3, subdomains=(1, 1, 1)):
+    """The Euler box of the scope table's configurations: n^3 elements on
+    [0,1]^3, freestream Mach `mach` (rho 1, p 1/gamma, so c = 1), a Gaussian
+    density bump of amplitude 1e-2 and width 0.1 at a seeded centre in
+    [0.3, 0.7]^3, farfield on every face; returns the box and q0."""
+    from chidg_b200 import euler
+    centre = np.random.default_rng(seed).uniform(0.3, 0.7, 3)
+    box = euler.EulerBox(n, n, n, order, vel_inf=(mach, 0.0, 0.0), subdomains=subdomains)
+    return box, box.density_bump(amplitude=1e-2, width=0.1, centre=tuple(centre)), centre
+
+
+def device_newton_system(ctx, A, box, q0):
+    """The first Newton step's linear system, on the device: A = dR/dq(q0) +
+    mass / dtau (cfl CFL_PTC), returns b = -R(q0) and the assembly time."""
+    from chidg_b200 import api, euler
+    dev = euler.EulerDevice(box, ctx)
+    q = api.ChidgVector(A, q0)
+    b = api.ChidgVector(A)
+    t0 = time.perf_counter()
+    dev.assemble(q, b, A)
+    dtau = dev.pseudo_timestep(q, CFL_PTC)
+    A.scale_diagonal(box.mass, (1.0 / dtau).reshape(-1))
+    b.scale(-1.0)
+    ctx.sync()
+    dt = time.perf_counter() - t0
+    q.release()
+    dev.release()
+    return b, dt
+
+
+def cpu_sample_system(n=SAMPLE_N, seed=SEED_A):
+    """The same Newton system on an n^3 P2 box, assembled on the host."""
+    from chidg_b200 import euler
+    box, q0, _ = euler_box(n, seed)
+    R, vals = box.residual(q0, jacobian=True)
+    vals = euler.add_pseudo_time(box, vals, box.pseudo_timestep(q0, CFL_PTC))
+    return box.pattern, vals, -R
+
+
+def cpu_sample_solve(sample, A=None):
+    """One full FGMRES(50)+ILU0 FP64 solve (factorisation included) of a
+    sample system on one host core; A: an oracle matrix already holding its
+    values (set up outside the timed region)."""
     from oracle import oracle as O
-    pat = mesh.box_pattern(n, n, n, NVARS, mesh.nterms_of_order(P))
-    A = O.OracleMatrix(pat)
-    A.set_values(mesh.synth_values(pat, seed=seed_a, nthreads=1))
-    b = mesh.synth_vector(A.n, seed=seed_b, nthreads=1)
+    pat, vals, b = sample
+    if A is None:
+        A = O.OracleMatrix(pat)
+        A.set_values(vals)
     opts = {k: v for k, v in SOLVER.items() if k != "orthogonalization"}
     t0 = time.perf_counter()
     x, res = O.fgmres(A, O.OraclePrecon(A, "ilu0"), b, O.default_opts(**opts))
@@ -598,11 +666,18 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    from oracle import oracle as O
     cores = max(1, len(os.sched_getaffinity(0)))
     threads = min(cores, 16)
+    sample = cpu_sample_system()
+    mats = []
+    for _ in range(threads):                         # set-up outside the timed steps
+        m = O.OracleMatrix(sample[0])
+        m.set_values(sample[1])
+        mats.append(m)
 
     def one(results, i):
-        results[i] = cpu_sample_solve()
+        results[i] = cpu_sample_solve(sample, mats[i])
 
     times = []
     for step in range(args.warmup + args.steps):
@@ -620,8 +695,8 @@ def run_reference(args):
     niter = results[0][1]
     # `threads` independent sample solves per step, each 1/27 of the workload
     value = threads * cpu_solves_per_s(per_step)
-    sample = (f"{threads} concurrent {SAMPLE_N}^3 P2 FGMRES(50)+ILU0 FP64 solves ({niter} iterations each) per step, "
-              f"scaled by element count to 24^3")
+    sample = (f"{threads} concurrent {SAMPLE_N}^3 P2 Euler Newton-system FGMRES(50)+ILU0 FP64 solves ({niter} "
+              f"iterations each) per step, scaled by element count to 24^3")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -648,6 +723,7 @@ def run_gpu(args):
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     ctx = api.Context(local, stream=stream.cuda_stream)
+    L0 = ctx.L
     pat = mesh.box_pattern(NX, NY, NZ, NVARS, mesh.nterms_of_order(P))
     nval = pat.value_offsets()[1]
     n = pat.vector_size()
@@ -656,12 +732,13 @@ def run_gpu(args):
     hv = torch.empty(nval, dtype=torch.float64, pin_memory=True)
     hb = torch.empty(n, dtype=torch.float64, pin_memory=True)
     hx = torch.empty(n, dtype=torch.float64, pin_memory=True)
-    mesh.synth_values(pat, seed=SEED_A + 1000 * rank, out=hv.numpy())
-    mesh.synth_vector(n, seed=SEED_B + 1000 * rank, out=hb.numpy())
-
-    A = api.ChidgMatrix(pat, ctx)
-    A.upload(hv.numpy())
-    b = api.ChidgVector(A, hb.numpy())
+    # the first Newton step's system of the Euler box, assembled on the device
+    # (each rank its own seeded bump); the host copies are what e2e uploads
+    box, q0, centre = euler_box(NX, SEED_A + 1000 * rank)
+    A = api.ChidgMatrix(box.pattern, ctx)
+    b, assembly_s = device_newton_system(ctx, A, box, q0)
+    ctx.check(L0.chidg_gpu_matrix_download(A.h, api._ptr(hv.numpy())), "download A")
+    ctx.check(L0.chidg_gpu_vector_download(b.h, api._ptr(hb.numpy())), "download b")
     x = api.ChidgVector(A)
     M = api.create_preconditioner("ilu0", schedule=args.schedule)
     solver = api.create_linear_solver("fgmres", **SOLVER)
@@ -797,16 +874,17 @@ def run_gpu(args):
     traffic = measured_traffic(dom.split()[0], pat) if args.schedule == "stream" else None
     cpu = None
     if not args.no_cpu and world == 1:
-        dt, it = cpu_sample_solve()
+        dt, it = cpu_sample_solve(cpu_sample_system())
         cpu = {"value": cpu_solves_per_s(dt), "unit": "solves/s", "cores": 1, "kind": "port",
-               "sample": f"one {SAMPLE_N}^3 P2 FGMRES(50)+ILU0 FP64 solve on 1 core ({it} iterations, {dt:.1f} s), "
-                         f"scaled by element count to 24^3"}
+               "sample": f"one {SAMPLE_N}^3 P2 Euler Newton-system FGMRES(50)+ILU0 FP64 solve on 1 core ({it} "
+                         f"iterations, {dt:.1f} s), scaled by element count to 24^3"}
     lat_sorted = sorted(lat_ms)
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_config({"precision": "fp64", "ilu_schedule": args.schedule, "fgmres_iterations": niters,
+                                   "bump_centre": [float(c) for c in centre], "device_assembly_s": assembly_s,
                                    "true_rel_residual": resid}),
         "latency_ms": {"p50": float(np.percentile(lat_sorted, 50)), "p99": float(np.percentile(lat_sorted, 99))},
         "clocks": clk,

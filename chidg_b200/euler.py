@@ -224,17 +224,18 @@ class EulerBox:
     Jacobian in the block layout of mesh.box_pattern.
 
     bcs: one of 'farfield' or 'extrapolate' for each face XI_MIN..ZETA_MAX (or a
-    single name for all).  The farfield state is (rho_inf, p_inf, vel_inf)."""
+    single name for all).  The farfield state is (rho_inf, p_inf, vel_inf).
+    subdomains: box subdomains of the pattern's elem_proc (the RAS "ranks")."""
 
     def __init__(self, nx: int, ny: int, nz: int, order: int, extent=((0.0, 1.0),) * 3, bcs="farfield",
-                 rho_inf: float = 1.0, p_inf: float = 1.0 / GAMMA, vel_inf=(0.3, 0.0, 0.0)):
+                 rho_inf: float = 1.0, p_inf: float = 1.0 / GAMMA, vel_inf=(0.3, 0.0, 0.0), subdomains=(1, 1, 1)):
         if not 0 <= order <= MAX_ORDER:
             raise ValueError(f"EulerBox: order must be 0..{MAX_ORDER}")
         self.shape = (nx, ny, nz)
         self.order = order
         self.nterms = (order + 1) ** 3
         self.nelem = nx * ny * nz
-        self.pattern = mesh.box_pattern(nx, ny, nz, NFIELDS, self.nterms)
+        self.pattern = mesh.box_pattern(nx, ny, nz, NFIELDS, self.nterms, subdomains=tuple(subdomains))
         self.bcs = [bcs] * 6 if isinstance(bcs, str) else list(bcs)
         if len(self.bcs) != 6 or any(b not in ("farfield", "extrapolate") for b in self.bcs):
             raise ValueError("EulerBox: bcs must name 'farfield' or 'extrapolate' for each of the 6 faces")
@@ -434,6 +435,22 @@ class EulerBox:
         h = self.vol ** (1.0 / 3.0)
         cfl = np.broadcast_to(np.asarray(cfl, dtype=np.float64), (NFIELDS,))
         return cfl[None, :] * (h / lam)[:, None]
+
+
+def add_pseudo_time(box: EulerBox, vals: np.ndarray, dtau: np.ndarray) -> np.ndarray:
+    """Host counterpart of chidg_gpu_matrix_scale_diagonal for a host-assembled
+    Jacobian: vals + mass / dtau[e, f] on every field's diagonal sub-block of
+    the DIAG blocks (type_newton.f90:320-352)."""
+    nb, b, nt = box.pattern.nblocks, NFIELDS * box.nterms, box.nterms
+    out = np.array(vals, dtype=np.float64, copy=True)
+    blk = out.reshape(nb, b, b)                            # [block, column, row]
+    dtau = np.asarray(dtau, dtype=np.float64).reshape(box.nelem, -1)
+    dtau = np.broadcast_to(dtau, (box.nelem, NFIELDS))
+    Mt = box.mass_block.T
+    for f in range(NFIELDS):
+        s = slice(f * nt, (f + 1) * nt)
+        blk[box._diag_k, s, s] += Mt[None, :, :] / dtau[:, f, None, None]
+    return out
 
 
 class EulerSystem:
