@@ -387,6 +387,37 @@ inline std::unique_ptr<LinearSolver> create_linear_solver(std::string name) {
     return std::make_unique<LinearSolver>();
 }
 
+// The Euler DG residual and Jacobian of a hex box on the device
+// (chidg_gpu_euler_*; the reference's update_space for the Euler equation set,
+// src/spatial/mod_spatial.f90:40-197).  The matrix must hold the box's
+// pattern: Pattern::box(nx, ny, nz, 5, (order + 1)^3).
+class EulerAssembly {
+public:
+    EulerAssembly(Context& ctx, const chidg_gpu_euler_box& box) : ctx_(&ctx) {
+        detail::check(ctx.handle(), chidg_gpu_euler_create(ctx.handle(), &box, &h_), "euler_create");
+    }
+    ~EulerAssembly() { if (h_) chidg_gpu_euler_destroy(h_); }
+    EulerAssembly(const EulerAssembly&) = delete;
+    EulerAssembly& operator=(const EulerAssembly&) = delete;
+
+    // rhs = R(q); with A also A = dR/dq (every block overwritten)
+    void assemble(const ChidgVector& q, ChidgVector& rhs, ChidgMatrix* A = nullptr) {
+        detail::check(ctx_->handle(), chidg_gpu_euler_assemble(h_, q.handle(), rhs.handle(), A ? A->handle() : nullptr),
+                      "euler_assemble");
+    }
+    // dtau[e * 5 + f] (type_fluid_pseudo_timestep.f90)
+    std::vector<double> pseudo_timestep(const ChidgVector& q, const std::array<double, 5>& cfl, int nelem) {
+        std::vector<double> dtau((size_t)nelem * 5);
+        detail::check(ctx_->handle(), chidg_gpu_euler_pseudo_timestep(h_, q.handle(), cfl.data(), dtau.data()),
+                      "euler_pseudo_timestep");
+        return dtau;
+    }
+
+private:
+    Context* ctx_ = nullptr;
+    chidg_gpu_euler* h_ = nullptr;
+};
+
 }  // namespace chidg_gpu
 
 #endif

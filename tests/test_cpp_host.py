@@ -12,11 +12,14 @@ LIB_DIR = os.path.join(ROOT, "chidg_b200")
 SRC = os.path.join(ROOT, "tests", "cpp", "test_reference_kats.cpp")
 
 
-def build(tmp_path):
+EULER_SRC = os.path.join(ROOT, "tests", "cpp", "test_euler_freestream.cpp")
+
+
+def build(tmp_path, src=SRC):
     if not os.path.exists(os.path.join(LIB_DIR, "libchidg_gpu.so")):
         pytest.skip("libchidg_gpu.so is not built")
-    exe = str(tmp_path / "test_reference_kats")
-    subprocess.check_call(["g++", "-std=c++17", "-O1", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"), SRC,
+    exe = str(tmp_path / os.path.splitext(os.path.basename(src))[0])
+    subprocess.check_call(["g++", "-std=c++17", "-O1", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"), src,
                            "-o", exe, "-L", LIB_DIR, "-lchidg_gpu", "-Wl,-rpath," + LIB_DIR])
     return exe
 
@@ -36,6 +39,7 @@ def cases_text():
 
 def test_host_layer_compiles_and_links(tmp_path):
     assert os.path.exists(build(tmp_path))
+    assert os.path.exists(build(tmp_path, EULER_SRC))
 
 
 @pytest.mark.gpu
@@ -46,3 +50,10 @@ def test_reference_kats_through_cpp_host_layer(tmp_path):
     p = subprocess.run([exe, str(cases)], capture_output=True, text=True, timeout=300)
     assert p.returncode == 0, p.stdout + p.stderr
     assert "4 cases, 0 failures" in p.stdout
+
+
+@pytest.mark.gpu
+def test_euler_assembly_through_cpp_host_layer(tmp_path):
+    exe = build(tmp_path, EULER_SRC)
+    p = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stdout + p.stderr
