@@ -792,9 +792,12 @@ def run_gpu(args):
     # solve still follows its own upload, and every copy is inside the timed
     # region, which opens with an event both streams wait on and closes after
     # both.
+    link = threading.Lock()          # the host link: one lane uploads while the other solves
+
     def e2e_step(c, Am, bm, xm, Mm, sm, hxm):
-        c.check(L.chidg_gpu_matrix_upload(Am.h, api._ptr(hv.numpy())), "upload A")
-        c.check(L.chidg_gpu_vector_upload(bm.h, api._ptr(hb.numpy())), "upload b")
+        with link:
+            c.check(L.chidg_gpu_matrix_upload(Am.h, api._ptr(hv.numpy())), "upload A")
+            c.check(L.chidg_gpu_vector_upload(bm.h, api._ptr(hb.numpy())), "upload b")
         sm.solve(Am, xm, bm, Mm)
         c.check(L.chidg_gpu_vector_download(xm.h, api._ptr(hxm.numpy())), "download x")
 
