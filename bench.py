@@ -791,7 +791,9 @@ def run_gpu(args):
     # alternate steps, so one lane's upload overlaps the other's solve; each
     # solve still follows its own upload, and every copy is inside the timed
     # region, which opens with an event both streams wait on and closes after
-    # both.
+    # both.  Uploads take the host link in turn: started together, the two
+    # lanes' uploads would share it and finish together, and the lanes would
+    # then run in lock-step with nothing overlapped.
     link = threading.Lock()          # the host link: one lane uploads while the other solves
 
     def e2e_step(c, Am, bm, xm, Mm, sm, hxm):
@@ -823,7 +825,7 @@ def run_gpu(args):
     hx2 = torch.empty(n, dtype=torch.float64, pin_memory=True)
     lanes = [(ctx, A, b, x, M, solver, hx), (ctx2, A2, b2, x2, M2, solver2, hx2)]
     e2e_step(*lanes[1])                                # the second lane's warm-up (its ILU programme)
-    nb_e2e = 2 * max(1, min(args.steps, 2))
+    nb_e2e = 2 * max(1, min(args.steps, 4))
     errors = []
 
     def run_lane(i):
