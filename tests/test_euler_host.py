@@ -167,3 +167,20 @@ def test_bad_arguments():
         euler.EulerBox(2, 2, 2, 4)
     with pytest.raises(ValueError):
         euler.EulerBox(2, 2, 2, 1, bcs="wall")
+
+
+def test_add_pseudo_time_matches_dense():
+    """euler.add_pseudo_time (the host counterpart of scale_diagonal) adds
+    mass / dtau[e, f] to each field's diagonal sub-block of DIAG, nothing else."""
+    b = euler.EulerBox(3, 2, 2, 1)
+    q = b.density_bump(amplitude=0.05, width=0.3)
+    _, vals = b.residual(q, jacobian=True)
+    dtau = b.pseudo_timestep(q, [1.0, 2.0, 3.0, 4.0, 5.0])
+    got = dense(b.pattern, euler.add_pseudo_time(b, vals, dtau))
+    want = dense(b.pattern, vals)
+    nt = b.nterms
+    for e in range(b.nelem):
+        for f in range(5):
+            s = (e * 5 + f) * nt
+            want[s:s + nt, s:s + nt] += b.mass_block / dtau[e, f]
+    assert np.allclose(got, want, rtol=0, atol=1e-15 * np.abs(want).max())
