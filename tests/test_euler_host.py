@@ -5,12 +5,10 @@ Fortran compiler, HDF5 and MPI), so it is held to the properties a correct DG
 discretisation has: the mode order and basis of the reference, freestream
 preservation, consistency and conservation of the face fluxes, a Jacobian equal
 to the derivative of the residual, and exact projection of polynomials."""
-import math
-
 import numpy as np
 import pytest
 
-from chidg_b200 import euler, mesh
+from chidg_b200 import euler
 
 
 def test_mode_order_shells():
