@@ -15,14 +15,12 @@
 // dual numbers through the pointwise functions, as the reference's DNAD types
 // (AD_D) carry derivatives, and the chain rule through the basis.
 //
-// k_euler_assemble: one CTA per element.  Shared memory holds the modes of the
-// element and of its face neighbours and the weighted pointwise data (flux and
-// its 5x5 derivatives at every volume node; face integrand and its derivatives
-// with respect to both states at every face node); the residual is a
-// contraction over the nodes, and for the Jacobian the pointwise derivatives
-// go to a scratch buffer.  k_euler_contract: one CTA per (element, block)
-// contracts them into the DIAG block and the face blocks.  Every output is
-// written by one thread: no atomics, one writer per value.  Each element integrates its
+// One CTA per element.  Shared memory holds the modes of the element and of
+// its face neighbours and the weighted pointwise data (flux and its 5x5
+// derivatives at every volume node; face integrand and its derivatives with
+// respect to both states at every face node).  The residual, the DIAG block and
+// the face blocks are then contractions over the nodes, each output written by
+// one thread: no atomics, one writer per value.  Each element integrates its
 // own faces (the reference evaluates a shared face once and negates it for the
 // neighbour, integrate_boundary_scalar_flux, mod_integrate.f90:219-346; the
 // two agree to rounding since the numerical flux is antisymmetric).
@@ -264,7 +262,8 @@ __host__ __device__ inline size_t smem_doubles(int nt, int qv, int qf) {
 
 template <int NT>
 __global__ void __launch_bounds__(kThreads) k_euler_assemble(BoxGeom g, Tables tb, const double* __restrict__ q,
-                                                            double* __restrict__ rhs, double* __restrict__ pts) {
+                                                            double* __restrict__ rhs, double* __restrict__ val,
+                                                            const int64_t* __restrict__ blk_off) {
     extern __shared__ double sm[];
     const int e = blockIdx.x;
     const int nt = NT, b = 5 * NT, qv = g.qv, qf = g.qf;
@@ -400,96 +399,76 @@ __global__ void __launch_bounds__(kThreads) k_euler_assemble(BoxGeom g, Tables t
         rhs[(int64_t)e * b + t] = r;
     }
 
-    // 4. for the Jacobian (skipped for a residual-only call): the weighted
-    // derivatives (WdF, FI, Fs, Fn: one contiguous run of shared memory) go
-    // to the element's slot of the scratch that k_euler_contract reads
-    if (pts == nullptr) return;
-    __syncthreads();
-    const size_t pw = (size_t)qv * 75 + (size_t)qf * 330;
-    double* dst = pts + (size_t)e * pw;
-    for (size_t t = threadIdx.x; t < pw; t += blockDim.x) dst[t] = sWdF[t];
-}
-
-// The Jacobian blocks of element blockIdx.x: blockIdx.y = 6 its DIAG block
-// (volume and the six faces), 0..5 the block of that face's neighbour (none
-// on a boundary face), from the pointwise derivatives k_euler_assemble left
-// in `pts`.  One thread per pair of (f, m, g) rows with the same f and g and
-// modes m0, m0 + 1, all nt columns n of both in registers, so each basis value
-// loaded feeds two FMAs; block entry (f nt + m, g nt + n) stored
-// column-major.  Lanes of a warp take consecutive mode pairs (the derivative
-// they read is the same: a broadcast).  No shared memory: two CTAs share an SM.
-template <int NT>
-__global__ void __launch_bounds__(kThreads, 2) k_euler_contract(BoxGeom g, Tables tb, const double* __restrict__ pts,
-                                                               double* __restrict__ val,
-                                                               const int64_t* __restrict__ blk_off) {
-    const int e = blockIdx.x, blk = blockIdx.y;
-    if (blk < 6 && neighbour(g, e, blk) < 0) return;
-    const int nt = NT, b = 5 * NT, qv = g.qv, qf = g.qf;
-    const size_t pw = (size_t)qv * 75 + (size_t)qf * 330;
-    const double* sWdF = pts + (size_t)e * pw;                     // [qv][3][5][5]
-    const double* sFs = sWdF + (size_t)qv * 75 + (size_t)qf * 30;  // [6][qf][5][5]
-    const double* sFn = sFs + (size_t)qf * 150;                    // [6][qf][5][5]
-    double* out = val + blk_off[(int64_t)e * 7 + blk];
+    // 4. DIAG block and 5. face blocks (skipped for a residual-only call): one
+    // thread per pair of (f, m, g) rows with the same f and g and modes m0,
+    // m0 + 1, all nt columns n of both in registers, so each basis value
+    // loaded feeds two FMAs; block entry (f nt + m, g nt + n) stored
+    // column-major.  Lanes of a warp take consecutive mode pairs.
+    if (val == nullptr) return;
     const int npair = (nt + 1) >> 1;
-    for (int item = threadIdx.x; item < 25 * npair; item += blockDim.x) {
-        const int mp = item % npair, fg = item / npair, f = fg % 5, gg = fg / 5;
-        const int m0 = 2 * mp;
-        const bool two = m0 + 1 < nt;
-        const int m1 = two ? m0 + 1 : m0;
-        double a0[NT], a1[NT];
+    for (int blk = 6; blk >= 0; --blk) {
+        if (blk < 6 && nbr[blk] < 0) continue;
+        double* out = val + blk_off[(int64_t)e * 7 + blk];
+        for (int item = threadIdx.x; item < 25 * npair; item += blockDim.x) {
+            const int mp = item % npair, fg = item / npair, f = fg % 5, gg = fg / 5;
+            const int m0 = 2 * mp;
+            const bool two = m0 + 1 < nt;
+            const int m1 = two ? m0 + 1 : m0;
+            double a0[NT], a1[NT];
 #pragma unroll
-        for (int n = 0; n < NT; ++n) { a0[n] = 0.0; a1[n] = 0.0; }
-        if (blk == 6) {
-            for (int qq = 0; qq < qv; ++qq) {
-                const double w0 = __ldg(sWdF + ((qq * 3 + 0) * 5 + f) * 5 + gg);
-                const double w1 = __ldg(sWdF + ((qq * 3 + 1) * 5 + f) * 5 + gg);
-                const double w2 = __ldg(sWdF + ((qq * 3 + 2) * 5 + f) * 5 + gg);
-                const double* g0 = tb.grad + (size_t)(0 * qv + qq) * nt;
-                const double* g1 = tb.grad + (size_t)(1 * qv + qq) * nt;
-                const double* g2 = tb.grad + (size_t)(2 * qv + qq) * nt;
-                const double t0 = -(g0[m0] * w0 + g1[m0] * w1 + g2[m0] * w2);
-                const double t1 = -(g0[m1] * w0 + g1[m1] * w1 + g2[m1] * w2);
-                const double* ph = tb.phi + (size_t)qq * nt;
+            for (int n = 0; n < NT; ++n) { a0[n] = 0.0; a1[n] = 0.0; }
+            if (blk == 6) {
+                for (int qq = 0; qq < qv; ++qq) {
+                    const double w0 = sWdF[((qq * 3 + 0) * 5 + f) * 5 + gg];
+                    const double w1 = sWdF[((qq * 3 + 1) * 5 + f) * 5 + gg];
+                    const double w2 = sWdF[((qq * 3 + 2) * 5 + f) * 5 + gg];
+                    const double* g0 = tb.grad + (size_t)(0 * qv + qq) * nt;
+                    const double* g1 = tb.grad + (size_t)(1 * qv + qq) * nt;
+                    const double* g2 = tb.grad + (size_t)(2 * qv + qq) * nt;
+                    const double t0 = -(g0[m0] * w0 + g1[m0] * w1 + g2[m0] * w2);
+                    const double t1 = -(g0[m1] * w0 + g1[m1] * w1 + g2[m1] * w2);
+                    const double* ph = tb.phi + (size_t)qq * nt;
 #pragma unroll
-                for (int n = 0; n < NT; ++n) {
-                    const double p = ph[n];
-                    a0[n] += t0 * p;
-                    a1[n] += t1 * p;
+                    for (int n = 0; n < NT; ++n) {
+                        const double p = ph[n];
+                        a0[n] += t0 * p;
+                        a1[n] += t1 * p;
+                    }
                 }
-            }
-            for (int face = 0; face < 6; ++face) {
+                for (int face = 0; face < 6; ++face) {
+                    for (int qq = 0; qq < qf; ++qq) {
+                        const double* pf = tb.phif + ((size_t)face * qf + qq) * nt;
+                        const double w = sFs[((size_t)face * qf + qq) * 25 + f * 5 + gg];
+                        const double t0 = pf[m0] * w, t1 = pf[m1] * w;
+#pragma unroll
+                        for (int n = 0; n < NT; ++n) {
+                            const double p = pf[n];
+                            a0[n] += t0 * p;
+                            a1[n] += t1 * p;
+                        }
+                    }
+                }
+            } else {
                 for (int qq = 0; qq < qf; ++qq) {
-                    const double* pf = tb.phif + ((size_t)face * qf + qq) * nt;
-                    const double w = __ldg(sFs + ((size_t)face * qf + qq) * 25 + f * 5 + gg);
+                    const double* pf = tb.phif + ((size_t)blk * qf + qq) * nt;
+                    const double* pn = tb.phif + ((size_t)(blk ^ 1) * qf + qq) * nt;
+                    const double w = sFn[((size_t)blk * qf + qq) * 25 + f * 5 + gg];
                     const double t0 = pf[m0] * w, t1 = pf[m1] * w;
 #pragma unroll
                     for (int n = 0; n < NT; ++n) {
-                        const double p = pf[n];
+                        const double p = pn[n];
                         a0[n] += t0 * p;
                         a1[n] += t1 * p;
                     }
                 }
             }
-        } else {
-            for (int qq = 0; qq < qf; ++qq) {
-                const double* pf = tb.phif + ((size_t)blk * qf + qq) * nt;
-                const double* pn = tb.phif + ((size_t)(blk ^ 1) * qf + qq) * nt;
-                const double w = __ldg(sFn + ((size_t)blk * qf + qq) * 25 + f * 5 + gg);
-                const double t0 = pf[m0] * w, t1 = pf[m1] * w;
+            const int row = f * nt + m0;
 #pragma unroll
-                for (int n = 0; n < NT; ++n) {
-                    const double p = pn[n];
-                    a0[n] += t0 * p;
-                    a1[n] += t1 * p;
-                }
+            for (int n = 0; n < NT; ++n) {
+                double* col = out + (int64_t)(gg * nt + n) * b + row;
+                col[0] = a0[n];
+                if (two) col[1] = a1[n];
             }
-        }
-        const int row = f * nt + m0;
-#pragma unroll
-        for (int n = 0; n < NT; ++n) {
-            double* col = out + (int64_t)(gg * nt + n) * b + row;
-            col[0] = a0[n];
-            if (two) col[1] = a1[n];
         }
     }
 }
@@ -569,7 +548,6 @@ struct chidg_gpu_euler {
     int order = 0, nelem = 0;
     double h = 0.0;
     Buffer phi, grad, wv, phif, wf, dtau;
-    Buffer pts;                                    // pointwise derivatives, nelem x (75 qv + 330 qf)
     Buffer blk_off;
     int64_t off_uid = 0;                           // matrix (uid) the block-offset table was built for
 };
@@ -685,7 +663,7 @@ extern "C" int chidg_gpu_euler_create(chidg_gpu_ctx* ctx, const chidg_gpu_euler_
 
 extern "C" int chidg_gpu_euler_destroy(chidg_gpu_euler* E) {
     if (!E) return CHIDG_GPU_OK;
-    for (Buffer* b : {&E->phi, &E->grad, &E->wv, &E->phif, &E->wf, &E->dtau, &E->blk_off, &E->pts}) release(*b);
+    for (Buffer* b : {&E->phi, &E->grad, &E->wv, &E->phif, &E->wf, &E->dtau, &E->blk_off}) release(*b);
     delete E;
     return CHIDG_GPU_OK;
 }
@@ -764,28 +742,16 @@ extern "C" int chidg_gpu_euler_assemble(chidg_gpu_euler* E, chidg_gpu_vector* q,
     }
     const int P = E->order, nt = E->g.nt;
     const size_t smem = smem_doubles(nt, E->g.qv, E->g.qf) * sizeof(double);
-    const size_t pw = (size_t)E->g.qv * 75 + (size_t)E->g.qf * 330;      // pointwise derivatives per element
-    if (jac && (st = ensure(E->ctx, E->pts, (size_t)E->nelem * pw * sizeof(double)))) return st;
     const Tables tb = tables_of(E);
-    double* pts = jac ? (double*)E->pts.ptr : nullptr;
-    const double* qp = (const double*)q->buf.ptr;
-    double* rp = (double*)rhs->buf.ptr;
+    double* val = jac ? (double*)A->val.ptr : nullptr;
+    const int64_t* off = jac ? (const int64_t*)E->blk_off.ptr : nullptr;
     const dim3 grid(E->nelem), block(kThreads);
-    cudaStream_t s = E->ctx->stream;
-    if (P == 0) k_euler_assemble<1><<<grid, block, smem, s>>>(E->g, tb, qp, rp, pts);
-    else if (P == 1) k_euler_assemble<8><<<grid, block, smem, s>>>(E->g, tb, qp, rp, pts);
-    else k_euler_assemble<27><<<grid, block, smem, s>>>(E->g, tb, qp, rp, pts);
+    if (P == 0) k_euler_assemble<1><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, (const double*)q->buf.ptr, (double*)rhs->buf.ptr, val, off);
+    else if (P == 1) k_euler_assemble<8><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, (const double*)q->buf.ptr, (double*)rhs->buf.ptr, val, off);
+    else k_euler_assemble<27><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, (const double*)q->buf.ptr, (double*)rhs->buf.ptr, val, off);
     st = check_launch(E->ctx, "k_euler_assemble");
-    if (st || !jac) return st;
-    double* val = (double*)A->val.ptr;
-    const int64_t* off = (const int64_t*)E->blk_off.ptr;
-    const dim3 cgrid(E->nelem, 7);
-    if (P == 0) k_euler_contract<1><<<cgrid, block, 0, s>>>(E->g, tb, pts, val, off);
-    else if (P == 1) k_euler_contract<8><<<cgrid, block, 0, s>>>(E->g, tb, pts, val, off);
-    else k_euler_contract<27><<<cgrid, block, 0, s>>>(E->g, tb, pts, val, off);
-    st = check_launch(E->ctx, "k_euler_contract");
     if (st) return st;
-    A->stamp++;
+    if (jac) A->stamp++;
     return CHIDG_GPU_OK;
 }
 
