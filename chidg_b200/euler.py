@@ -293,12 +293,13 @@ class EulerBox:
         p = self.pattern
         diag = np.full(self.nelem, -1, dtype=np.int64)
         face = np.full((self.nelem, 6), -1, dtype=np.int64)
-        for k in range(p.nblocks):
-            f = int(p.blk_face[k])
-            if f == mesh.DIAG:
-                diag[p.blk_row_elem[k]] = k
-            elif f < 6:
-                face[p.blk_row_elem[k], f] = k
+        k = np.arange(p.nblocks, dtype=np.int64)
+        f = np.asarray(p.blk_face)
+        row = np.asarray(p.blk_row_elem)
+        d = f == mesh.DIAG
+        diag[row[d]] = k[d]
+        o = f < 6
+        face[row[o], f[o]] = k[o]
         return diag, face
 
     def modes(self, q: np.ndarray) -> np.ndarray:
