@@ -624,7 +624,7 @@ def device_newton_system(ctx, A, box, q0):
     t0 = time.perf_counter()
     dev.assemble(q, b, A)
     dtau = dev.pseudo_timestep(q, CFL_PTC)
-    A.scale_diagonal(box.mass, (1.0 / dtau).reshape(-1))
+    A.scale_diagonal(box.mass, np.repeat(1.0 / dtau.min(axis=1), NVARS))   # minval over the fields
     b.scale(-1.0)
     ctx.sync()
     dt = time.perf_counter() - t0

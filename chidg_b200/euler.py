@@ -440,13 +440,14 @@ class EulerBox:
 
 def add_pseudo_time(box: EulerBox, vals: np.ndarray, dtau: np.ndarray) -> np.ndarray:
     """Host counterpart of chidg_gpu_matrix_scale_diagonal for a host-assembled
-    Jacobian: vals + mass / dtau[e, f] on every field's diagonal sub-block of
-    the DIAG blocks (type_newton.f90:320-352)."""
+    Jacobian: vals + mass / dtau_e on every field's diagonal sub-block of the
+    DIAG blocks, dtau_e the minimum of the element's pseudo time steps over its
+    fields (contribute_pseudo_temporal, type_newton.f90:320-352)."""
     nb, b, nt = box.pattern.nblocks, NFIELDS * box.nterms, box.nterms
     out = np.array(vals, dtype=np.float64, copy=True)
     blk = out.reshape(nb, b, b)                            # [block, column, row]
-    dtau = np.asarray(dtau, dtype=np.float64).reshape(box.nelem, -1)
-    dtau = np.broadcast_to(dtau, (box.nelem, NFIELDS))
+    dtau = np.asarray(dtau, dtype=np.float64).reshape(box.nelem, -1).min(axis=1)
+    dtau = np.broadcast_to(dtau[:, None], (box.nelem, NFIELDS))
     Mt = box.mass_block.T
     for f in range(NFIELDS):
         s = slice(f * nt, (f + 1) * nt)

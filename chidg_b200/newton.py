@@ -13,7 +13,9 @@ Assembly of the residual and its Jacobian stays with the caller, through a
     system.pseudo_timestep(q, cfl) -> dtau      pseudo time steps, cfl per field:
                                                 one per element, or one per element
                                                 and field (nelem x nfields, as
-                                                elems(:)%dtau(ieqn))
+                                                elems(:)%dtau(ieqn)), of which the
+                                                element's minimum is applied to
+                                                every field and time level
     system.mass -> packed per-element mass matrices (nterms x nterms,
                    column-major), as chidg_gpu_matrix_scale_diagonal takes them
 
@@ -104,10 +106,9 @@ class Newton:
             if o.ptc:                                        # contribute_pseudo_temporal (:320-352)
                 t0 = time.perf_counter()
                 dtau = np.asarray(system.pseudo_timestep(q, cfln), dtype=np.float64)
-                if dtau.ndim == 1:                           # one pseudo time step per element
-                    scale = np.repeat(1.0 / dtau, A.pattern.elem_nvars)
-                else:                                        # per element and field (elems(:)%dtau(ieqn))
-                    scale = (1.0 / dtau).reshape(-1)
+                if dtau.ndim == 2:                           # minval(elems(ielem)%dtau) over the fields
+                    dtau = dtau.min(axis=1)
+                scale = np.repeat(1.0 / dtau, A.pattern.elem_nvars)
                 A.scale_diagonal(system.mass, scale)
                 ph["ptc"] += time.perf_counter() - t0
             if niter == 1:
