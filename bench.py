@@ -282,9 +282,7 @@ def serve_requests(count, seed, pinned=True, device=0):
     out = []
     for i, (p, v, r) in enumerate(uneven_systems(count, seed=seed, device=device)):
         if i % 10 == 9:
-            p = mesh.box_pattern(8, 8, 8, NVARS, mesh.nterms_of_order(1), ntime=7)
-            v = mesh.synth_values(p, seed=3000 + i)
-            r = mesh.synth_vector(p.vector_size(), seed=4000 + i)
+            p, v, r = hb_system(i)
         out.append(serve.SolveRequest(p, pin(v), pin(r), tag=i))
     return out
 
@@ -310,7 +308,7 @@ def run_serve_leg(device, requests=64, rate=200.0):
     from chidg_b200 import serve
     out = {"arrival_rate_per_s": rate, "requests": requests, "slots": 2, "max_batch": 16,
            "workload": "Poisson arrivals; Euler Newton systems of boxes 4..8 per side, P in {1,2}, Mach in "
-                       "[0.2, 0.6]; every 10th request harmonic balance (8^3, P1, 7 time levels, synthetic values); "
+                       "[0.2, 0.6]; every 10th request an Euler harmonic-balance system (8^3, P1, 7 time levels); "
                        "FGMRES(30)+ILU0 to rtol 1e-8 (FP64 residual); request values in page-locked host memory; "
                        "the server in a process of its own"}
     out["server"] = "native (chidg_gpu_serve_*: dispatcher and worker slots as native threads)"
@@ -387,19 +385,20 @@ def run_adjoint_leg(ctx, stream, A, b, schedule, reps=3):
 
 
 def run_hb_leg(ctx, stream, schedule, reps=3):
-    """The harmonic-balance system of the serving requests (8^3 P1, 7 time
-    levels, hb_blks coupling every pair of levels): FGMRES(30) to rtol 1e-8,
-    FP64, with ILU0 per time level and with precon_HB (per-element inverse
-    over all levels)."""
+    """A harmonic-balance request of the serving leg (the Euler box of
+    hb_system: 8^3 P1, 7 time levels, hb_blks coupling every pair of levels):
+    FGMRES(30) to rtol 1e-8, FP64, with ILU0 per time level and with
+    precon_HB (per-element inverse over all levels)."""
     import torch
 
-    from chidg_b200 import api, mesh
-    pat = mesh.box_pattern(8, 8, 8, NVARS, mesh.nterms_of_order(1), ntime=7)
+    from chidg_b200 import api
+    pat, vals, rhs = hb_system(9)
     A = api.ChidgMatrix(pat, ctx)
-    A.upload(mesh.synth_values(pat, seed=SEED_A + 7))
-    b = api.ChidgVector(A, mesh.synth_vector(pat.vector_size(), seed=SEED_B + 7))
-    out = {"workload": "8^3 hex box, 5 fields, P1, 7 time levels (40x40 blocks, 280x280 element blocks over the "
-                       "levels), FGMRES(30) to rtol 1e-8, FP64"}
+    A.upload(vals)
+    b = api.ChidgVector(A, rhs)
+    out = {"workload": "8^3 hex box, Euler under harmonic balance, P1, 3 harmonics = 7 time levels (40x40 blocks, "
+                       "280x280 element blocks over the levels), sinusoidal inflow amplitude 1e-2, the first Newton "
+                       "step's system; FGMRES(30) to rtol 1e-8, FP64"}
     for kind in ("ilu0", "hb"):
         M = api.create_preconditioner(kind, schedule=schedule)
         solver = api.create_linear_solver("fgmres", **{**SOLVER, "nkrylov": 30})
@@ -631,6 +630,26 @@ def device_newton_system(ctx, A, box, q0):
     q.release()
     dev.release()
     return b, dt
+
+
+_HB_SYSTEMS = {}
+
+
+def hb_system(i):
+    """The harmonic-balance request of the scope table's serving workload: the
+    8^3 P1 Euler box under harmonic balance with 3 harmonics (7 time levels,
+    280 x 280 element blocks over the levels), a sinusoidal inflow of amplitude
+    1e-2, a Gaussian density bump at a centre seeded by i; the first Newton
+    step's system (pseudo-transient term at cfl 10), assembled on the host and
+    cached: (pattern, values, right-hand side)."""
+    if i not in _HB_SYSTEMS:
+        from chidg_b200 import euler
+        centre = tuple(float(c) for c in np.random.default_rng(5000 + i).uniform(0.3, 0.7, 3))
+        hb = euler.EulerHB(8, 8, 8, 1, [1.0, 2.0, 3.0], amplitude=1e-2)
+        q0 = hb.density_bump(amplitude=1e-2, width=0.1, centre=centre)
+        R, vals = hb.residual(q0, jacobian=True)
+        _HB_SYSTEMS[i] = (hb.pattern, hb.add_pseudo_time(vals, hb.pseudo_timestep(q0, CFL_PTC)), -R)
+    return _HB_SYSTEMS[i]
 
 
 def cpu_sample_system(n=SAMPLE_N, seed=SEED_A):

@@ -43,7 +43,7 @@ import math
 
 import numpy as np
 
-from . import api, mesh
+from . import _lib, api, mesh
 
 GAMMA = 1.4                      # src/equations/fluid/mod_fluid.f90:10
 RGAS = 287.15                    # src/equations/fluid/mod_fluid.f90:9
@@ -436,6 +436,122 @@ class EulerBox:
         h = self.vol ** (1.0 / 3.0)
         cfl = np.broadcast_to(np.asarray(cfl, dtype=np.float64), (NFIELDS,))
         return cfl[None, :] * (h / lam)[:, None]
+
+
+def hb_times(freqs) -> np.ndarray:
+    """Harmonic-balance time levels t_i = (2 pi / min |omega|) i / ntime,
+    i = 1..ntime, ntime = 2 nfreq + 1 (type_time_manager.f90:153-187)."""
+    w = np.asarray(freqs, dtype=np.float64)
+    ntime = 2 * w.size + 1
+    return (2.0 * np.pi / np.min(np.abs(w))) * (np.arange(1, ntime + 1) / ntime)
+
+
+def hb_operator(freqs, times) -> np.ndarray:
+    """The pseudo-spectral time-derivative operator D = dE^-1 E with E^-1 the
+    samples of (1, sin w_k t, cos w_k t) at the time levels and dE^-1 their time
+    derivatives (mod_HB_matrices.f90: calc_inv_E, calc_diff_inv_E,
+    calc_pseudo_spectral_operator)."""
+    w = np.asarray(freqs, dtype=np.float64)
+    t = np.asarray(times, dtype=np.float64)
+    nf, nt = w.size, t.size
+    invE = np.empty((nt, nt))
+    dinvE = np.empty((nt, nt))
+    invE[:, 0], dinvE[:, 0] = 1.0, 0.0
+    for k in range(nf):
+        invE[:, 1 + k] = np.sin(w[k] * t)
+        dinvE[:, 1 + k] = w[k] * np.cos(w[k] * t)
+        invE[:, 1 + nf + k] = np.cos(w[k] * t)
+        dinvE[:, 1 + nf + k] = -w[k] * np.sin(w[k] * t)
+    return dinvE @ np.linalg.inv(invE)
+
+
+class EulerHB:
+    """The Euler box under harmonic balance (assemble_harmonic_balance_t%assemble,
+    type_harmonic_balance.f90:127-229): at every time level t the spatial
+    residual and Jacobian of that level's state, with the farfield velocity
+    vel_inf (1 + amplitude sin(w_1 t)) (a sinusoidal inflow), plus
+    sum_t' D(t, t') M q_t' in the residual and D(t, t') M on each field's
+    diagonal in the hb block coupling t to t' != t (the reference stores the
+    t' = t term in the residual only).  The pattern is mesh.box_pattern with
+    ntime levels; vectors are element-major, then time level, field, mode."""
+
+    def __init__(self, nx, ny, nz, order, freqs, amplitude=1e-2, **box_args):
+        self.freqs = np.atleast_1d(np.asarray(freqs, dtype=np.float64))
+        self.times = hb_times(self.freqs)
+        self.D = hb_operator(self.freqs, self.times)
+        self.ntime = self.times.size
+        base = EulerBox(nx, ny, nz, order, **box_args)
+        u0 = np.asarray(base.vel_inf)
+        self.levels = []
+        for t in self.times:
+            args = dict(box_args)
+            args["vel_inf"] = tuple(u0 * (1.0 + amplitude * np.sin(self.freqs[0] * t)))
+            self.levels.append(EulerBox(nx, ny, nz, order, **args))
+        self.base = base
+        self.nelem, self.nterms = base.nelem, base.nterms
+        self.mass = base.mass
+        self.pattern = mesh.box_pattern(nx, ny, nz, NFIELDS, base.nterms, ntime=self.ntime)
+        p = self.pattern
+        local = np.asarray(p.blk_kind) == _lib.BLK_LOCAL
+        e, f = np.asarray(p.blk_row_elem), np.asarray(p.blk_face)
+        ks = np.where(f == mesh.DIAG, base._diag_k[e], base._face_k[e, np.minimum(f, 5)])
+        self._local_k = np.nonzero(local)[0]                  # hb-pattern blocks from the spatial Jacobians
+        self._local_src = ks[local]                           # their block in the level's pattern
+        self._local_t = np.asarray(p.blk_row_time)[local]
+        self._hb_k = np.nonzero(~local)[0]
+        self._hb_to = np.asarray(p.blk_row_time)[~local]
+        self._hb_from = np.asarray(p.blk_col_time)[~local]
+
+    def freestream(self) -> np.ndarray:
+        """Every level at its own farfield state."""
+        return np.stack([lv.freestream().reshape(self.nelem, -1) for lv in self.levels], axis=1).reshape(-1)
+
+    def density_bump(self, **kw) -> np.ndarray:
+        return np.stack([lv.density_bump(**kw).reshape(self.nelem, -1) for lv in self.levels], axis=1).reshape(-1)
+
+    def residual(self, q: np.ndarray, jacobian: bool = False):
+        nt, b, T = self.nterms, NFIELDS * self.nterms, self.ntime
+        U = np.asarray(q, dtype=np.float64).reshape(self.nelem, T, b)
+        R = np.empty_like(U)
+        if jacobian:
+            vals = np.empty((self.pattern.nblocks, b, b))           # [block, column, row]
+        for t, lv in enumerate(self.levels):
+            if jacobian:
+                Rt, vt = lv.residual(U[:, t].reshape(-1), jacobian=True)
+                sel = self._local_t == t
+                vals[self._local_k[sel]] = vt.reshape(-1, b, b)[self._local_src[sel]]
+            else:
+                Rt = lv.residual(U[:, t].reshape(-1))
+            R[:, t] = Rt.reshape(self.nelem, b)
+        Mq = np.einsum("mn,etfn->etfm", self.base.mass_block, U.reshape(self.nelem, T, NFIELDS, nt))
+        R += np.einsum("ab,ebfm->eafm", self.D, Mq).reshape(self.nelem, T, b)
+        if not jacobian:
+            return R.reshape(-1)
+        blk = np.kron(np.eye(NFIELDS), self.base.mass_block.T)
+        vals[self._hb_k] = self.D[self._hb_to, self._hb_from][:, None, None] * blk[None]
+        return R.reshape(-1), vals.reshape(-1)
+
+    def pseudo_timestep(self, q: np.ndarray, cfl) -> np.ndarray:
+        """The pseudo time steps of time level 1, as compute_pseudo_timestep
+        takes them (type_newton.f90:294-306, itime = 1)."""
+        U = np.asarray(q, dtype=np.float64).reshape(self.nelem, self.ntime, -1)
+        return self.levels[0].pseudo_timestep(U[:, 0].reshape(-1), cfl)
+
+    def add_pseudo_time(self, vals: np.ndarray, dtau: np.ndarray) -> np.ndarray:
+        """vals + mass / dtau_e on every field's diagonal sub-block of the DIAG
+        block of every time level, dtau_e the element's smallest pseudo time
+        step over its fields (contribute_pseudo_temporal)."""
+        nt, b = self.nterms, NFIELDS * self.nterms
+        out = np.array(vals, dtype=np.float64, copy=True)
+        blk = out.reshape(self.pattern.nblocks, b, b)                # [block, column, row]
+        diag = np.nonzero(np.asarray(self.pattern.blk_face) == mesh.DIAG)[0]
+        dmin = np.asarray(dtau, dtype=np.float64).reshape(self.nelem, -1).min(axis=1)
+        scale = 1.0 / dmin[np.asarray(self.pattern.blk_row_elem)[diag]]
+        Mt = self.base.mass_block.T
+        for f in range(NFIELDS):
+            s = slice(f * nt, (f + 1) * nt)
+            blk[diag, s, s] += scale[:, None, None] * Mt[None]
+        return out
 
 
 def add_pseudo_time(box: EulerBox, vals: np.ndarray, dtau: np.ndarray) -> np.ndarray:

@@ -183,3 +183,59 @@ def test_add_pseudo_time_matches_dense():
             s = (e * 5 + f) * nt
             want[s:s + nt, s:s + nt] += b.mass_block / dtau[e].min()
     assert np.allclose(got, want, rtol=0, atol=1e-15 * np.abs(want).max())
+
+
+def dense_levels(pat, vals):
+    """dense() with time levels: element-major, then time level, field, mode."""
+    n = pat.vector_size()
+    J = np.zeros((n, n))
+    voff, _ = pat.value_offsets()
+    nr, nc = pat.block_dims()
+    eo, b = pat.elem_offsets(), pat.bsize()
+    for k in range(pat.nblocks):
+        r0 = eo[pat.blk_row_elem[k]] + pat.blk_row_time[k] * b[pat.blk_row_elem[k]]
+        c0 = eo[pat.blk_col_elem[k]] + pat.blk_col_time[k] * b[pat.blk_col_elem[k]]
+        J[r0:r0 + nr[k], c0:c0 + nc[k]] += vals[voff[k]:voff[k] + nr[k] * nc[k]].reshape(nc[k], nr[k]).T
+    return J
+
+
+def test_hb_operator_differentiates_its_harmonics():
+    """D (mod_HB_matrices.f90) maps samples of 1, sin w t, cos w t at the time
+    levels (type_time_manager.f90) to the samples of their derivatives."""
+    w = np.array([1.3, 2.6])
+    t = euler.hb_times(w)
+    assert t.size == 5 and np.isclose(t[-1], 2 * np.pi / 1.3)
+    D = euler.hb_operator(w, t)
+    for wk in w:
+        assert np.allclose(D @ np.sin(wk * t), wk * np.cos(wk * t), atol=1e-13)
+        assert np.allclose(D @ np.cos(wk * t), -wk * np.sin(wk * t), atol=1e-13)
+    assert np.allclose(D @ np.ones(5), 0.0, atol=1e-13)
+
+
+def test_hb_freestream_and_jacobian():
+    """Steady farfield: every level at freestream has a zero residual.  With a
+    sinusoidal inflow, dR/dq (spatial blocks per level + D(t, t') mass in the
+    hb blocks) against central differences of R."""
+    hb = euler.EulerHB(3, 2, 2, 1, [1.0], amplitude=0.0, vel_inf=(0.3, 0.1, -0.05))
+    assert np.abs(hb.residual(hb.freestream())).max() < 1e-13
+    hb = euler.EulerHB(3, 2, 2, 1, [1.0, 2.0], amplitude=0.05, vel_inf=(0.3, 0.1, -0.07))
+    assert hb.ntime == 5 and hb.pattern.ntime == 5
+    q = hb.density_bump(amplitude=0.05, width=0.3, centre=(0.4, 0.5, 0.5))
+    R, vals = hb.residual(q, jacobian=True)
+    assert np.allclose(R, hb.residual(q), atol=1e-15)
+    J = dense_levels(hb.pattern, vals)
+    v = np.random.default_rng(7).standard_normal(q.size)
+    eps = 1e-6
+    fd = (hb.residual(q + eps * v) - hb.residual(q - eps * v)) / (2 * eps)
+    assert np.linalg.norm(J @ v - fd) <= 1e-8 * np.linalg.norm(fd)
+    # the pseudo-transient term reaches the DIAG block of every level
+    d = hb.pseudo_timestep(q, 10.0)
+    added = dense_levels(hb.pattern, hb.add_pseudo_time(vals, d)) - J
+    nt, T = hb.nterms, hb.ntime
+    want = np.zeros_like(added)
+    for e in range(hb.nelem):
+        for t in range(T):
+            for f in range(5):
+                s = ((e * T + t) * 5 + f) * nt
+                want[s:s + nt, s:s + nt] = hb.base.mass_block / d[e].min()
+    assert np.allclose(added, want, atol=1e-15 * np.abs(want).max())

@@ -194,3 +194,28 @@ def test_newton_device_assembly_matches_host_assembly():
         assert abs(a - b) <= 1e-9 * b + 1e-14
     assert rd.alphas == rh.alphas
     assert relerr(qd, qh) < 1e-10
+
+
+@pytest.mark.parametrize("kind", ["ilu0", "hb"])
+def test_hb_newton_system_solve_parity(kind):
+    """The harmonic-balance Euler system (euler.EulerHB: one harmonic, 3 time
+    levels, a sinusoidal inflow; spatial blocks per level and D(t, t') mass
+    hb blocks) with the pseudo-transient term: FGMRES with ILU0 per time level
+    or precon_HB on the GPU against the oracle, the same bar as the steady
+    systems."""
+    hb = euler.EulerHB(3, 3, 2, 1, [1.0], amplitude=1e-2)
+    q = hb.density_bump(amplitude=1e-2, width=0.15, centre=(0.45, 0.55, 0.5))
+    R, vals = hb.residual(q, jacobian=True)
+    vals = hb.add_pseudo_time(vals, hb.pseudo_timestep(q, 10.0))
+    Ao = O.OracleMatrix(hb.pattern)
+    Ao.set_values(vals)
+    Ag = api.ChidgMatrix(hb.pattern)
+    Ag.upload(vals)
+    opts = dict(tol=0.0, rtol=1e-8, nkrylov=30, inner_fgmres=0, nmax=400)
+    xo, ro = O.fgmres(Ao, O.OraclePrecon(Ao, kind), -R, O.default_opts(**opts))
+    solver = api.create_linear_solver("fgmres", **opts)
+    xg = api.ChidgVector(Ag)
+    solver.solve(Ag, xg, api.ChidgVector(Ag, -R), api.create_preconditioner(kind))
+    assert solver.niter == ro["niter"]
+    assert relerr(solver.hist, ro["hist"]) < 1e-8
+    assert relerr(xg.download(), xo) < 1e-10
