@@ -15,8 +15,10 @@ buffers, host->device upload of A and b and download of x included in every
 step, with two pipelines taking alternate steps so that one step's upload
 overlaps the other's solve (`e2e.sequential`: one pipeline, no overlap).
 `--impl reference` times the CPU FP64 oracle (the restatement of the
-reference solver; the Fortran original cannot be built here) on the host
-cores with bounded samples of the same workload.
+reference solver; the Fortran original cannot be built here) solving the same
+24^3 system, one whole solve per step, on every host thread.  The GPU arm's
+`cpu_baseline` is one such solve of its own headline system, which also gives
+the GPU solution's relative error against the oracle (`rel_err_vs_oracle`).
 """
 from __future__ import annotations
 
@@ -41,7 +43,6 @@ SEED_A, SEED_B = 1, 2
 SOLVER = dict(tol=0.0, rtol=1e-8, nkrylov=50, inner_fgmres=0, nmax=500, orthogonalization="CGS",
               use_controller=0)
 MIXED = dict(nkrylov=10, mixed_inner_nkrylov=30, mixed_inner_rtol=1e-2, mixed_inner_nmax=60)
-SAMPLE_N = 8            # cpu sample: 8^3 box with the same block size
 
 
 def workload_config(extra=None):
@@ -282,7 +283,7 @@ def serve_requests(count, seed, pinned=True, device=0):
     out = []
     for i, (p, v, r) in enumerate(uneven_systems(count, seed=seed, device=device)):
         if i % 10 == 9:
-            p, v, r = hb_system(i)
+            p, v, r = hb_system(i, seed)
         out.append(serve.SolveRequest(p, pin(v), pin(r), tag=i))
     return out
 
@@ -392,7 +393,7 @@ def run_hb_leg(ctx, stream, schedule, reps=3):
     import torch
 
     from chidg_b200 import api
-    pat, vals, rhs = hb_system(9)
+    pat, vals, rhs = hb_system(9, 11)
     A = api.ChidgMatrix(pat, ctx)
     A.upload(vals)
     b = api.ChidgVector(A, rhs)
@@ -635,97 +636,133 @@ def device_newton_system(ctx, A, box, q0):
 _HB_SYSTEMS = {}
 
 
-def hb_system(i):
+def hb_system(i, seed):
     """The harmonic-balance request of the scope table's serving workload: the
     8^3 P1 Euler box under harmonic balance with 3 harmonics (7 time levels,
     280 x 280 element blocks over the levels), a sinusoidal inflow of amplitude
-    1e-2, a Gaussian density bump at a centre seeded by i; the first Newton
-    step's system (pseudo-transient term at cfl 10), assembled on the host and
-    cached: (pattern, values, right-hand side)."""
-    if i not in _HB_SYSTEMS:
+    1e-2, a Gaussian density bump at a centre seeded by (request index, stream
+    seed), so that streams of different seeds hold different systems; the
+    first Newton step's system (pseudo-transient term at cfl 10), assembled on
+    the host and cached: (pattern, values, right-hand side)."""
+    key = (i, seed)
+    if key not in _HB_SYSTEMS:
         from chidg_b200 import euler
-        centre = tuple(float(c) for c in np.random.default_rng(5000 + i).uniform(0.3, 0.7, 3))
+        centre = tuple(float(c) for c in np.random.default_rng((5000 + i, seed)).uniform(0.3, 0.7, 3))
         hb = euler.EulerHB(8, 8, 8, 1, [1.0, 2.0, 3.0], amplitude=1e-2)
         q0 = hb.density_bump(amplitude=1e-2, width=0.1, centre=centre)
         R, vals = hb.residual(q0, jacobian=True)
-        _HB_SYSTEMS[i] = (hb.pattern, hb.add_pseudo_time(vals, hb.pseudo_timestep(q0, CFL_PTC)), -R)
-    return _HB_SYSTEMS[i]
+        _HB_SYSTEMS[key] = (hb.pattern, hb.add_pseudo_time(vals, hb.pseudo_timestep(q0, CFL_PTC)), -R)
+    return _HB_SYSTEMS[key]
 
 
-def cpu_sample_system(n=SAMPLE_N, seed=SEED_A):
-    """The same Newton system on an n^3 P2 box, assembled on the host."""
+def host_newton_system(n=NX, seed=SEED_A, order=P):
+    """The workload's Newton system assembled on the host (the DG restatement
+    in numpy): A = dR/dq(q0) + mass / dtau (cfl CFL_PTC, the element's smallest
+    pseudo time step over its fields), b = -R(q0).  The same system as
+    device_newton_system builds on the GPU."""
     from chidg_b200 import euler
-    box, q0, _ = euler_box(n, seed)
+    box, q0, _ = euler_box(n, seed, order=order)
     R, vals = box.residual(q0, jacobian=True)
     vals = euler.add_pseudo_time(box, vals, box.pseudo_timestep(q0, CFL_PTC))
     return box.pattern, vals, -R
 
 
-def cpu_sample_solve(sample, A=None):
-    """One full FGMRES(50)+ILU0 FP64 solve (factorisation included) of a
-    sample system on one host core; A: an oracle matrix already holding its
-    values (set up outside the timed region)."""
+def host_threads():
+    return max(1, len(os.sched_getaffinity(0)))
+
+
+def oracle_matrix(pat, vals):
     from oracle import oracle as O
-    pat, vals, b = sample
-    if A is None:
-        A = O.OracleMatrix(pat)
-        A.set_values(vals)
-    opts = {k: v for k, v in SOLVER.items() if k != "orthogonalization"}
+    A = O.OracleMatrix(pat)
+    A.set_values(vals)
+    return A
+
+
+def oracle_solve(A, b, opts=None):
+    """One full FGMRES(50)+ILU0 FP64 solve with the oracle (the restated
+    reference solver), its ILU0 factorisation included (fgmres refreshes the
+    preconditioner on every call without a controller, type_fgmres.f90:118-122),
+    on the oracle's current host threads; returns (wall seconds, x, result)."""
+    from oracle import oracle as O
+    opts = {k: v for k, v in (opts or SOLVER).items() if k != "orthogonalization"}
+    M = O.OraclePrecon(A, "ilu0")
     t0 = time.perf_counter()
-    x, res = O.fgmres(A, O.OraclePrecon(A, "ilu0"), b, O.default_opts(**opts))
-    dt = time.perf_counter() - t0
-    return dt, res["niter"]
-
-
-def cpu_solves_per_s(dt_sample, n_sample=SAMPLE_N):
-    """Scale a sample solve to the 24^3 workload: time grows with the element
-    count at equal iteration count (every kernel is linear in the elements)."""
-    return 1.0 / (dt_sample * (NX * NY * NZ) / n_sample ** 3)
+    x, res = O.fgmres(A, M, b, O.default_opts(**opts))
+    return time.perf_counter() - t0, x, res
 
 
 def run_reference(args):
+    """The reference's CPU solver on this host: the oracle's FGMRES(50) + block
+    ILU0 (the restatement of type_fgmres.f90 and precon_ILU0.f90) solving the
+    24^3 P2 Newton system itself, factorisation included, one whole solve per
+    step, on every host thread (rows of one dependency level, matrix rows and
+    independent Gram-Schmidt dots run in parallel; each row's arithmetic is the
+    serial reference's, so x is bitwise the one-thread x)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     from oracle import oracle as O
-    cores = max(1, len(os.sched_getaffinity(0)))
-    threads = min(cores, 16)
-    sample = cpu_sample_system()
-    mats = []
-    for _ in range(threads):                         # set-up outside the timed steps
-        m = O.OracleMatrix(sample[0])
-        m.set_values(sample[1])
-        mats.append(m)
-
-    def one(results, i):
-        results[i] = cpu_sample_solve(sample, mats[i])
-
-    times = []
+    threads = host_threads()
+    O.set_threads(threads)
+    t0 = time.perf_counter()
+    pat, vals, b = host_newton_system()
+    A = oracle_matrix(pat, vals)
+    del vals
+    setup_s = time.perf_counter() - t0
+    walls, niters = [], []
     for step in range(args.warmup + args.steps):
-        results = [None] * threads
-        th = [threading.Thread(target=one, args=(results, i)) for i in range(threads)]
-        t0 = time.perf_counter()
-        for t in th:
-            t.start()
-        for t in th:
-            t.join()
-        wall = time.perf_counter() - t0
+        dt, x, res = oracle_solve(A, b)
         if step >= args.warmup:
-            times.append(wall)
-    per_step = float(np.mean(times))
-    niter = results[0][1]
-    # `threads` independent sample solves per step, each 1/27 of the workload
-    value = threads * cpu_solves_per_s(per_step)
-    sample = (f"{threads} concurrent {SAMPLE_N}^3 P2 Euler Newton-system FGMRES(50)+ILU0 FP64 solves ({niter} "
-              f"iterations each) per step, scaled by element count to 24^3")
+            walls.append(dt)
+            niters.append(res["niter"])
+    total = float(sum(walls))
+    value = args.steps / total
+    sample = (f"the 24^3 P2 Euler Newton system itself (host-assembled), one whole FGMRES(50)+ILU0 FP64 solve per step "
+              f"(factorisation included, {niters[-1]} iterations, true relative residual "
+              f"{res['residual_norm'] / res['r0norm_initial']:.2e}) on {threads} host threads")
+    lat = sorted(1000.0 * w for w in walls)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config({"precision": "fp64", "implementation": "CPU FP64 oracle (restated reference solver)"}),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config({"precision": "fp64", "fgmres_iterations": niters,
+                                       "implementation": "CPU FP64 oracle (the restated reference solver), "
+                                                         f"{threads} host threads",
+                                       "host_setup_s": setup_s}),
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def run_oracle_check(pat, vals, rhs, x_gpu, solver, mixed_x):
+    """The headline system solved by the oracle on every host thread (one whole
+    FGMRES(50)+ILU0 FP64 solve, factorisation included): the GPU solution's
+    relative error against it, the iteration counts and residual histories of
+    both, each mixed mode's error against it, and the solve's wall time as the
+    CPU baseline."""
+    from oracle import oracle as O
+    threads = host_threads()
+    O.set_threads(threads)
+    t0 = time.perf_counter()
+    A = oracle_matrix(pat, vals)
+    setup_s = time.perf_counter() - t0
+    dt, xo, res = oracle_solve(A, np.array(rhs, copy=True))
+    nx = float(np.linalg.norm(xo))
+    hist_g, hist_o = np.asarray(solver.hist), np.asarray(res["hist"])
+    m = min(hist_g.size, hist_o.size)
+    check = {"oracle": f"CPU FP64 oracle, FGMRES(50)+ILU0, {threads} host threads",
+             "rel_err_vs_oracle": float(np.linalg.norm(x_gpu - xo) / nx),
+             "gpu_iterations": int(solver.niter), "oracle_iterations": int(res["niter"]),
+             "max_rel_history_diff": float(np.max(np.abs(hist_g[:m] - hist_o[:m]) / hist_o[:m])) if m else None,
+             "oracle_true_rel_residual": res["residual_norm"] / res["r0norm_initial"],
+             "oracle_solve_s": dt, "oracle_setup_s": setup_s,
+             "mixed_rel_err_vs_oracle": {k: float(np.linalg.norm(v - xo) / nx) for k, v in mixed_x.items()}}
+    cpu = {"value": 1.0 / dt, "unit": "solves/s", "cores": threads, "kind": "port",
+           "sample": f"one whole FGMRES(50)+ILU0 FP64 solve of this 24^3 P2 system itself (factorisation included, "
+                     f"{res['niter']} iterations) by the oracle on {threads} host threads, {dt:.1f} s"}
+    del A
+    return check, cpu
 
 
 # ---------------------------------------------------------------------------
@@ -880,6 +917,7 @@ def run_gpu(args):
 
     # ---- mixed precision (same workload, same 1e-8 target) ----
     mixed = {}
+    mixed_x = {}
     if not args.no_mixed:
         for prec in ("mixed_precon_fp32", "mixed_fp32", "mixed_bf16"):
             # FP64 FGMRES(50) with FP32 preconditioner blocks; or an FP32 inner FGMRES
@@ -904,12 +942,20 @@ def run_gpu(args):
                       for k, (v, c) in mkt.items() if c}
             xm_h = xm.download()
             x_h = x.download()
+            mixed_x[prec] = xm_h
             mixed[prec] = {"solves_per_s": 1000.0 / t, "ms_per_solve": t, "outer_iters": ms.niter,
                            "inner_iters": ms.inner_iters,
                            "true_rel_residual": ms.residual_norm / ms.r0norm_initial,
                            "rel_err_vs_fp64_solution": float(np.linalg.norm(xm_h - x_h) / np.linalg.norm(x_h)),
                            "speedup_vs_fp64": (elapsed_ms / args.steps) / t, "phases": phases}
         M = api.create_preconditioner("ilu0", schedule=args.schedule)   # drop low-precision factors
+
+    # ---- the oracle on the same system: parity of the headline solve and the CPU baseline ----
+    oracle_check, cpu = None, None
+    if not args.no_cpu and world == 1:
+        oracle_check, cpu = run_oracle_check(box.pattern, hv.numpy(), hb.numpy(), x.download(), solver, mixed_x)
+        for prec, err in oracle_check.pop("mixed_rel_err_vs_oracle").items():
+            mixed[prec]["rel_err_vs_oracle"] = err
 
     adjoint = run_adjoint_leg(ctx, stream, A, b, args.schedule) if not args.no_adjoint else None
     hb = run_hb_leg(ctx, stream, args.schedule) if not args.no_hb else None
@@ -952,12 +998,6 @@ def run_gpu(args):
         dom, dbytes, dms = "matvec (k_matvec)", mvb, kernels["matvec"]["avg_ms"]
     achieved = dbytes / (dms / 1e3) / 1e9
     traffic = measured_traffic(dom.split()[0], pat) if args.schedule == "stream" else None
-    cpu = None
-    if not args.no_cpu and world == 1:
-        dt, it = cpu_sample_solve(cpu_sample_system())
-        cpu = {"value": cpu_solves_per_s(dt), "unit": "solves/s", "cores": 1, "kind": "port",
-               "sample": f"one {SAMPLE_N}^3 P2 Euler Newton-system FGMRES(50)+ILU0 FP64 solve on 1 core ({it} "
-                         f"iterations, {dt:.1f} s), scaled by element count to 24^3"}
     lat_sorted = sorted(lat_ms)
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
@@ -965,7 +1005,9 @@ def run_gpu(args):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_config({"precision": "fp64", "ilu_schedule": args.schedule, "fgmres_iterations": niters,
                                    "bump_centre": [float(c) for c in centre], "device_assembly_s": assembly_s,
-                                   "true_rel_residual": resid}),
+                                   "true_rel_residual": resid,
+                                   "rel_err_vs_oracle": oracle_check["rel_err_vs_oracle"] if oracle_check else None}),
+        "oracle_check": oracle_check,
         "latency_ms": {"p50": float(np.percentile(lat_sorted, 50)), "p99": float(np.percentile(lat_sorted, 99))},
         "clocks": clk,
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(nval * 8 + n * 8),
@@ -996,7 +1038,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
-    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
+    ap.add_argument("--no-cpu", action="store_true",
+                    help="skip the oracle solve of the headline system (cpu_baseline and rel_err_vs_oracle)")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision legs")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-solve leg")
     ap.add_argument("--schedule", default="stream", choices=["tasks", "stream", "dataflow", "levels"],

@@ -1,20 +1,22 @@
 // noalloc.cu -- a dot product that allocates no device memory.
 //
-// Some callers cannot call cudaMalloc when they need a reduction: code that
-// runs while a CUDA stream is being captured into a graph (a device allocation
-// is not a capturable operation), and host frameworks that own all device
-// memory through their own pool and forbid allocations behind their back.
-// cudaMalloc may also synchronise the whole device, which a latency-bound
-// Krylov loop cannot afford.  chidg_gpu_dot_noalloc serves them: the caller
-// passes device pointers for the inputs and the output, and the per-chunk
-// partial sums go to a fixed-size array in this library's own device memory.
+// Some callers cannot call cudaMalloc when they need a reduction: host
+// frameworks that own all device memory through their own pool and forbid
+// allocations behind their back, and latency-bound loops that cannot afford
+// the device-wide synchronisation cudaMalloc may bring.
+// chidg_gpu_dot_noalloc serves them: the caller passes device pointers for
+// the inputs and the output, and the per-chunk partial sums go to a
+// fixed-size array in this library's own device memory.
 //
 // Scratch: one FP64 partial per 4096-element chunk, at most 16384 chunks
 // (128 KiB on every GPU that loads this library, held until the process
 // exits), so n is limited to 67 108 864 elements.  All calls share that
-// array: calls that overlap on the GPU (two streams, or two host threads)
-// race on it and must be serialised by the caller.  Each call overwrites
-// every partial it reads, so nothing needs clearing between calls.
+// array and it keeps the last call's contents: calls that overlap on the GPU
+// (two streams, or two host threads) race on it and must be serialised by
+// the caller.  Each call writes every partial it reads before reading it, so
+// nothing needs clearing between calls.  The first call on a device looks up
+// the array's device address (cudaGetSymbolAddress with that device
+// current); make that first call before any stream capture.
 #include "chidg_gpu_internal.cuh"
 
 #include <mutex>

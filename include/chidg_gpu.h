@@ -253,9 +253,9 @@ int chidg_gpu_vector_norm_fields(const chidg_gpu_vector* x, double* out, int32_t
 
 /* Dot product of two device arrays that allocates no device memory.  It has
  * no counterpart in the reference.  It is for callers that cannot call
- * cudaMalloc at the point where they need a reduction: code running while a
- * stream is captured into a CUDA graph, or frameworks that own all device
- * memory through their own pool.  x, y (n doubles) and result (one double)
+ * cudaMalloc at the point where they need a reduction: frameworks that own
+ * all device memory through their own pool, and loops that cannot afford the
+ * device-wide synchronisation an allocation may bring.  x, y (n doubles) and result (one double)
  * are device pointers on `device`; the work is queued on `stream` (NULL = the
  * default stream) and result is written asynchronously.  Partial sums live in
  * a fixed 128 KiB array inside this library on every GPU that loads it, so

@@ -17,7 +17,12 @@ module chidg_gpu_mod
     integer(c_int), parameter :: CHIDG_BLK_LOCAL = 0, CHIDG_BLK_CHIMERA = 1, CHIDG_BLK_BC = 2, CHIDG_BLK_HB = 3
     integer(c_int), parameter :: CHIDG_PRECON_IDENTITY = 0, CHIDG_PRECON_JACOBI = 1, &
                                  CHIDG_PRECON_ILU0 = 2, CHIDG_PRECON_RASILU0 = 3, CHIDG_PRECON_HB = 4
-    integer(c_int), parameter :: CHIDG_GPU_FP64 = 0, CHIDG_GPU_MIXED_FP32 = 1, CHIDG_GPU_MIXED_BF16 = 2
+    integer(c_int), parameter :: CHIDG_GPU_FP64 = 0, CHIDG_GPU_MIXED_FP32 = 1, CHIDG_GPU_MIXED_BF16 = 2, &
+                                 CHIDG_GPU_MIXED_PRECON_FP32 = 3
+    integer(c_int), parameter :: CHIDG_ORTH_CGS = 0, CHIDG_ORTH_MGS = 1
+    integer(c_int), parameter :: CHIDG_SCHED_LEVELS = 0, CHIDG_SCHED_DATAFLOW = 1, CHIDG_SCHED_TASKS = 2, &
+                                 CHIDG_SCHED_STREAM = 3
+    integer(c_int), parameter :: CHIDG_EULER_FARFIELD = 0, CHIDG_EULER_EXTRAPOLATE = 1
 
     type, bind(c) :: chidg_gpu_pattern
         integer(c_int32_t) :: nelem, ntime
@@ -216,6 +221,206 @@ module chidg_gpu_mod
             import :: c_int, c_ptr, c_double
             type(c_ptr), value :: E, q
             real(c_double)     :: cfl(5), dtau(*)
+        end function
+        ! ---- context utilities --------------------------------------------
+        integer(c_int) function chidg_gpu_ctx_sync(ctx) bind(c, name='chidg_gpu_ctx_sync')
+            import :: c_int, c_ptr
+            type(c_ptr), value :: ctx
+        end function
+        integer(c_int) function chidg_gpu_launch_count(ctx, count) bind(c, name='chidg_gpu_launch_count')
+            import :: c_int, c_ptr, c_int64_t
+            type(c_ptr), value :: ctx
+            integer(c_int64_t) :: count
+        end function
+        integer(c_int) function chidg_gpu_ctx_set_profiling(ctx, on) bind(c, name='chidg_gpu_ctx_set_profiling')
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr),        value :: ctx
+            integer(c_int32_t), value :: on
+        end function
+        integer(c_int) function chidg_gpu_ctx_kernel_time(ctx, kernel_class, total_ms, count) &
+                bind(c, name='chidg_gpu_ctx_kernel_time')
+            import :: c_int, c_ptr, c_int32_t, c_int64_t, c_double
+            type(c_ptr),        value :: ctx
+            integer(c_int32_t), value :: kernel_class
+            real(c_double)            :: total_ms
+            integer(c_int64_t)        :: count
+        end function
+        integer(c_int) function chidg_gpu_host_alloc(bytes, p) bind(c, name='chidg_gpu_host_alloc')
+            import :: c_int, c_ptr, c_size_t
+            integer(c_size_t), value :: bytes
+            type(c_ptr)              :: p
+        end function
+        integer(c_int) function chidg_gpu_host_free(p) bind(c, name='chidg_gpu_host_free')
+            import :: c_int, c_ptr
+            type(c_ptr), value :: p
+        end function
+        integer(c_int) function chidg_gpu_selftest_bounded_waits(ctx, limit_cycles, bits) &
+                bind(c, name='chidg_gpu_selftest_bounded_waits')
+            import :: c_int, c_ptr, c_int32_t, c_int64_t
+            type(c_ptr),        value :: ctx
+            integer(c_int64_t), value :: limit_cycles
+            integer(c_int32_t)        :: bits
+        end function
+        ! ---- chidg_matrix_t accessors and partial stores --------------------
+        integer(c_int) function chidg_gpu_matrix_nvalues(mat, nvalues) bind(c, name='chidg_gpu_matrix_nvalues')
+            import :: c_int, c_ptr, c_int64_t
+            type(c_ptr), value :: mat
+            integer(c_int64_t) :: nvalues
+        end function
+        integer(c_int) function chidg_gpu_matrix_nvec(mat, n) bind(c, name='chidg_gpu_matrix_nvec')
+            import :: c_int, c_ptr, c_int64_t
+            type(c_ptr), value :: mat
+            integer(c_int64_t) :: n
+        end function
+        ! values already on the device (a device pointer passed by value)
+        integer(c_int) function chidg_gpu_matrix_upload_device(mat, dev) bind(c, name='chidg_gpu_matrix_upload_device')
+            import :: c_int, c_ptr
+            type(c_ptr), value :: mat, dev
+        end function
+        ! chidg_matrix%store of a range of the packed values (bumps the stamp)
+        integer(c_int) function chidg_gpu_matrix_upload_range(mat, vals, first, count) &
+                bind(c, name='chidg_gpu_matrix_upload_range')
+            import :: c_int, c_ptr, c_double, c_int64_t
+            type(c_ptr),        value :: mat
+            real(c_double)            :: vals(*)
+            integer(c_int64_t), value :: first, count
+        end function
+        integer(c_int) function chidg_gpu_matrix_download(mat, vals) bind(c, name='chidg_gpu_matrix_download')
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: mat
+            real(c_double)     :: vals(*)
+        end function
+        ! chidg_matrix_t%stamp (type_chidg_matrix.f90:575-747): a counter bumped by every store
+        integer(c_int) function chidg_gpu_matrix_stamp(mat, stamp) bind(c, name='chidg_gpu_matrix_stamp')
+            import :: c_int, c_ptr, c_int64_t
+            type(c_ptr), value :: mat
+            integer(c_int64_t) :: stamp
+        end function
+        integer(c_int) function chidg_gpu_matrix_get_pattern(mat, nelem, ntime, nblocks, elem_nvars, elem_nterms, &
+                elem_proc, blk_row_elem, blk_row_time, blk_col_elem, blk_col_time, blk_kind) &
+                bind(c, name='chidg_gpu_matrix_get_pattern')
+            import :: c_int, c_ptr, c_int32_t, c_int64_t
+            type(c_ptr), value :: mat
+            integer(c_int32_t) :: nelem, ntime
+            integer(c_int64_t) :: nblocks
+            integer(c_int32_t) :: elem_nvars(*), elem_nterms(*), elem_proc(*)
+            integer(c_int32_t) :: blk_row_elem(*), blk_row_time(*), blk_col_elem(*), blk_col_time(*), blk_kind(*)
+        end function
+        ! ---- chidg_vector_t operators (type_chidg_vector.f90) ----------------
+        integer(c_int) function chidg_gpu_vector_upload_range(vec, vals, first, count) &
+                bind(c, name='chidg_gpu_vector_upload_range')
+            import :: c_int, c_ptr, c_double, c_int64_t
+            type(c_ptr),        value :: vec
+            real(c_double)            :: vals(*)
+            integer(c_int64_t), value :: first, count
+        end function
+        integer(c_int) function chidg_gpu_vector_upload_device(vec, dev) bind(c, name='chidg_gpu_vector_upload_device')
+            import :: c_int, c_ptr
+            type(c_ptr), value :: vec, dev
+        end function
+        integer(c_int) function chidg_gpu_vector_device_ptr(vec, dev) bind(c, name='chidg_gpu_vector_device_ptr')
+            import :: c_int, c_ptr
+            type(c_ptr), value :: vec
+            type(c_ptr)        :: dev
+        end function
+        integer(c_int) function chidg_gpu_vector_clear(vec) bind(c, name='chidg_gpu_vector_clear')
+            import :: c_int, c_ptr
+            type(c_ptr), value :: vec
+        end function
+        integer(c_int) function chidg_gpu_vector_copy(dst, src) bind(c, name='chidg_gpu_vector_copy')
+            import :: c_int, c_ptr
+            type(c_ptr), value :: dst, src
+        end function
+        ! y = y + a x
+        integer(c_int) function chidg_gpu_vector_axpy(y, a, x) bind(c, name='chidg_gpu_vector_axpy')
+            import :: c_int, c_ptr, c_double
+            type(c_ptr),    value :: y
+            real(c_double), value :: a
+            type(c_ptr),    value :: x
+        end function
+        integer(c_int) function chidg_gpu_vector_scale(x, a) bind(c, name='chidg_gpu_vector_scale')
+            import :: c_int, c_ptr, c_double
+            type(c_ptr),    value :: x
+            real(c_double), value :: a
+        end function
+        ! dot (operator_chidg_dot.f90:30-97)
+        integer(c_int) function chidg_gpu_vector_dot(x, y, res) bind(c, name='chidg_gpu_vector_dot')
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: x, y
+            real(c_double)     :: res
+        end function
+        ! dot of two device arrays with no device allocation (no counterpart in the reference)
+        integer(c_int) function chidg_gpu_dot_noalloc(device, x, y, n, res, stream) bind(c, name='chidg_gpu_dot_noalloc')
+            import :: c_int, c_ptr, c_int64_t
+            integer(c_int),     value :: device
+            type(c_ptr),        value :: x, y
+            integer(c_int64_t), value :: n
+            type(c_ptr),        value :: res, stream
+        end function
+        ! ---- preconditioner_t extras -----------------------------------------
+        integer(c_int) function chidg_gpu_precon_set_schedule(M, schedule) bind(c, name='chidg_gpu_precon_set_schedule')
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr),        value :: M
+            integer(c_int32_t), value :: schedule
+        end function
+        integer(c_int) function chidg_gpu_precon_download_LD(M, vals) bind(c, name='chidg_gpu_precon_download_LD')
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: M
+            real(c_double)     :: vals(*)
+        end function
+        ! preconditioner_t%stamp (type_preconditioner.f90:21-121)
+        integer(c_int) function chidg_gpu_precon_stamp(M, stamp) bind(c, name='chidg_gpu_precon_stamp')
+            import :: c_int, c_ptr, c_int64_t
+            type(c_ptr), value :: M
+            integer(c_int64_t) :: stamp
+        end function
+        ! ---- many independent systems in one call ------------------------------
+        integer(c_int) function chidg_gpu_fgmres_solve_batched(mat, M, nsys, sys_elem, b, x, opts, results, hist, &
+                hist_cap) bind(c, name='chidg_gpu_fgmres_solve_batched')
+            import :: c_int, c_ptr, c_double, c_int32_t, chidg_gpu_fgmres_opts, chidg_gpu_fgmres_result
+            type(c_ptr),        value     :: mat, M
+            integer(c_int32_t), value     :: nsys
+            integer(c_int32_t)            :: sys_elem(*)
+            type(c_ptr),        value     :: b, x
+            type(chidg_gpu_fgmres_opts)   :: opts
+            type(chidg_gpu_fgmres_result) :: results(*)
+            real(c_double)                :: hist(*)
+            integer(c_int32_t), value     :: hist_cap
+        end function
+        ! ---- request server ----------------------------------------------------
+        integer(c_int) function chidg_gpu_serve_create(device, slots, mem_budget, max_batch, precon_kind, opts, srv) &
+                bind(c, name='chidg_gpu_serve_create')
+            import :: c_int, c_ptr, c_int32_t, c_int64_t, chidg_gpu_fgmres_opts
+            integer(c_int),     value   :: device
+            integer(c_int32_t), value   :: slots
+            integer(c_int64_t), value   :: mem_budget
+            integer(c_int32_t), value   :: max_batch, precon_kind
+            type(chidg_gpu_fgmres_opts) :: opts
+            type(c_ptr)                 :: srv
+        end function
+        integer(c_int) function chidg_gpu_serve_submit(srv, pat, vals, rhs, ticket) bind(c, name='chidg_gpu_serve_submit')
+            import :: c_int, c_ptr, c_double, c_int64_t, chidg_gpu_pattern
+            type(c_ptr), value      :: srv
+            type(chidg_gpu_pattern) :: pat
+            real(c_double)          :: vals(*), rhs(*)
+            integer(c_int64_t)      :: ticket
+        end function
+        integer(c_int) function chidg_gpu_serve_wait(srv, ticket, x, res, timing) bind(c, name='chidg_gpu_serve_wait')
+            import :: c_int, c_ptr, c_double, c_int64_t, chidg_gpu_fgmres_result
+            type(c_ptr),        value     :: srv
+            integer(c_int64_t), value     :: ticket
+            real(c_double)                :: x(*)
+            type(chidg_gpu_fgmres_result) :: res
+            real(c_double)                :: timing(*)
+        end function
+        integer(c_int) function chidg_gpu_serve_stats(srv, batches, peak_mem_bytes) bind(c, name='chidg_gpu_serve_stats')
+            import :: c_int, c_ptr, c_int64_t
+            type(c_ptr), value :: srv
+            integer(c_int64_t) :: batches, peak_mem_bytes
+        end function
+        integer(c_int) function chidg_gpu_serve_destroy(srv) bind(c, name='chidg_gpu_serve_destroy')
+            import :: c_int, c_ptr
+            type(c_ptr), value :: srv
         end function
     end interface
 

@@ -22,16 +22,153 @@
 #include "chidg_oracle.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cfloat>
 #include <cmath>
+#include <condition_variable>
 #include <cstdint>
 #include <cstring>
+#include <functional>
+#include <immintrin.h>
 #include <memory>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 namespace {
 
 using std::vector;
+
+// Host threads for the oracle's data-parallel loops.  A loop run through the
+// pool hands each index to exactly one thread, and the work of an index is
+// the serial loop's work for that index in the serial loop's order, so every
+// result is bitwise the one-thread result whatever the thread count.  Loops
+// whose serial order couples indices (a dot product's running sum, an ILU row
+// that needs its parents) are either kept serial or split only where the
+// serial order allows it (independent dots, rows of one dependency level).
+// Calls made while the pool is busy on another caller's loop run serially.
+class Pool {
+  public:
+    static Pool& get() {
+        static Pool p;
+        return p;
+    }
+    int threads() const { return nthreads_; }
+    void set_threads(int n) {
+        n = std::max(1, std::min(n, 1024));
+        std::lock_guard<std::mutex> busy(run_mu_);
+        stop_workers();
+        nthreads_ = n;
+        // workers start at the current generation: run() cannot advance it
+        // while this call holds run_mu_
+        for (int i = 1; i < n; ++i) workers_.emplace_back([this, g0 = gen_] { worker(g0); });
+    }
+    template <class F>
+    void run(int64_t n, F&& f) {
+        if (n <= 0) return;
+        std::unique_lock<std::mutex> busy(run_mu_, std::try_to_lock);
+        if (!busy.owns_lock() || nthreads_ == 1 || n == 1) {
+            for (int64_t i = 0; i < n; ++i) f(i);
+            return;
+        }
+        std::function<void(int64_t)> job = std::forward<F>(f);
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            job_ = &job;
+            n_ = n;
+            next_.store(0);
+            pending_ = nthreads_ - 1;
+            ++gen_;
+        }
+        cv_.notify_all();
+        work();
+        std::unique_lock<std::mutex> g(mu_);
+        done_.wait(g, [this] { return pending_ == 0; });
+        job_ = nullptr;
+    }
+    // f(begin, end) over [0, n) in chunks of `grain`
+    template <class F>
+    void run_chunks(int64_t n, int64_t grain, F&& f) {
+        const int64_t nc = (n + grain - 1) / grain;
+        run(nc, [&](int64_t c) { f(c * grain, std::min(n, (c + 1) * grain)); });
+    }
+    ~Pool() {
+        std::lock_guard<std::mutex> busy(run_mu_);
+        stop_workers();
+    }
+
+  private:
+    void work() {
+        for (;;) {
+            const int64_t i = next_.fetch_add(1);
+            if (i >= n_) break;
+            (*job_)(i);
+        }
+    }
+    void worker(uint64_t seen) {
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> g(mu_);
+                cv_.wait(g, [&] { return stop_ || gen_ != seen; });
+                if (stop_) return;
+                seen = gen_;
+            }
+            work();
+            std::lock_guard<std::mutex> g(mu_);
+            if (--pending_ == 0) done_.notify_one();
+        }
+    }
+    void stop_workers() {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : workers_) t.join();
+        workers_.clear();
+        stop_ = false;
+    }
+    int nthreads_ = 1;
+    std::vector<std::thread> workers_;
+    std::mutex run_mu_, mu_;
+    std::condition_variable cv_, done_;
+    const std::function<void(int64_t)>* job_ = nullptr;
+    int64_t n_ = 0;
+    std::atomic<int64_t> next_{0};
+    int pending_ = 0;
+    uint64_t gen_ = 0;
+    bool stop_ = false;
+};
+constexpr int64_t kGrain = 1 << 14;   // vector entries per chunk of an elementwise loop
+
+// A large FP64 array filled on the pool (zeroed, or copied) instead of by one
+// thread: at the workload sizes these arrays hold up to tens of GB.
+struct DBuf {
+    std::unique_ptr<double[]> p;
+    int64_t n = 0;
+    double* data() { return p.get(); }
+    const double* data() const { return p.get(); }
+    int64_t size() const { return n; }
+    void resize(int64_t n_) {
+        if (n_ != n) {
+            p.reset(n_ > 0 ? new double[n_] : nullptr);
+            n = n_;
+        }
+    }
+    void zeros(int64_t n_) {
+        resize(n_);
+        double* d = p.get();
+        Pool::get().run_chunks(n, 1 << 20, [d](int64_t a, int64_t b) { std::memset(d + a, 0, sizeof(double) * (b - a)); });
+    }
+    void copy_from(const double* src) {
+        double* d = p.get();
+        Pool::get().run_chunks(n, 1 << 20, [d, src](int64_t a, int64_t b) { std::memcpy(d + a, src + a, sizeof(double) * (b - a)); });
+    }
+    void copy_to(double* dst) const {
+        const double* d = p.get();
+        Pool::get().run_chunks(n, 1 << 20, [d, dst](int64_t a, int64_t b) { std::memcpy(dst + a, d + a, sizeof(double) * (b - a)); });
+    }
+};
 
 struct Mat {
     int nelem = 0, ntime = 0;
@@ -42,7 +179,7 @@ struct Mat {
     vector<int> re, rt, ce, ct, kind, nr, nc;
     vector<int64_t> voff;   // packed value offset of each block
     int64_t nval = 0;
-    vector<double> val;
+    DBuf val;
     vector<vector<int>> rowblk;   // per row (e*ntime+t): all blocks, lblks first then chi/bc/hb
     vector<vector<int>> lblk;     // per row: LOCAL blocks in storage order
     vector<int> diag;             // per row: DIAG block id
@@ -109,26 +246,118 @@ void gemm_sub_nt(int m, int n, int k, const double* A, const double* B, double* 
             for (int i = 0; i < m; ++i) c[i] -= a[i] * b;
         }
 }
+// C(m x n) +=/-= A(m x k) * B(k x n), all column-major.  Every entry is
+// updated as c = fma(+-a(i,p), b(p,j), c) for p = 0 .. k-1 in order (the
+// fused multiply-add the compiler makes of `c += a * b`), so the register
+// tiles below give the same bits as the plain triple loop: they only keep a
+// tile of C in registers across p instead of reloading it.  An AVX-512 tile
+// (up to 24 rows x 8 columns, the last row vector masked) is used where the
+// host has AVX-512, an AVX2 tile (12 x 4) otherwise.
+template <bool SUB, int NV, int NJ>
+__attribute__((target("avx512f"))) void tile512(int m, int k, const double* A, const double* B, double* C, int i,
+                                                int j, __mmask8 last) {
+    __m512d c[NV][NJ];
+    for (int jj = 0; jj < NJ; ++jj)
+        for (int ii = 0; ii < NV; ++ii)
+            c[ii][jj] = _mm512_maskz_loadu_pd(ii == NV - 1 ? last : (__mmask8)0xFF, C + i + 8 * ii + (int64_t)(j + jj) * m);
+    for (int p = 0; p < k; ++p) {
+        const double* ap = A + i + (int64_t)p * m;
+        __m512d a[NV];
+        for (int ii = 0; ii < NV; ++ii) a[ii] = _mm512_maskz_loadu_pd(ii == NV - 1 ? last : (__mmask8)0xFF, ap + 8 * ii);
+        for (int jj = 0; jj < NJ; ++jj) {
+            const __m512d b = _mm512_set1_pd(B[p + (int64_t)(j + jj) * k]);
+            for (int ii = 0; ii < NV; ++ii)
+                c[ii][jj] = SUB ? _mm512_fnmadd_pd(a[ii], b, c[ii][jj]) : _mm512_fmadd_pd(a[ii], b, c[ii][jj]);
+        }
+    }
+    for (int jj = 0; jj < NJ; ++jj)
+        for (int ii = 0; ii < NV; ++ii)
+            _mm512_mask_storeu_pd(C + i + 8 * ii + (int64_t)(j + jj) * m, ii == NV - 1 ? last : (__mmask8)0xFF, c[ii][jj]);
+}
+template <bool SUB, int NV>
+void tile512_nj(int nj, int m, int k, const double* A, const double* B, double* C, int i, int j, __mmask8 last) {
+    switch (nj) {
+        case 8: tile512<SUB, NV, 8>(m, k, A, B, C, i, j, last); break;
+        case 7: tile512<SUB, NV, 7>(m, k, A, B, C, i, j, last); break;
+        case 6: tile512<SUB, NV, 6>(m, k, A, B, C, i, j, last); break;
+        case 5: tile512<SUB, NV, 5>(m, k, A, B, C, i, j, last); break;
+        case 4: tile512<SUB, NV, 4>(m, k, A, B, C, i, j, last); break;
+        case 3: tile512<SUB, NV, 3>(m, k, A, B, C, i, j, last); break;
+        case 2: tile512<SUB, NV, 2>(m, k, A, B, C, i, j, last); break;
+        default: tile512<SUB, NV, 1>(m, k, A, B, C, i, j, last); break;
+    }
+}
+template <bool SUB>
+void gemm_update_avx512(int m, int n, int k, const double* A, const double* B, double* C) {
+    for (int j = 0; j < n; j += 8) {
+        const int nj = std::min(8, n - j);
+        for (int i = 0; i < m; i += 24) {
+            const int rows = std::min(24, m - i);
+            const int nv = (rows + 7) / 8;
+            const __mmask8 last = (rows % 8) ? (__mmask8)((1u << (rows % 8)) - 1u) : (__mmask8)0xFF;
+            if (nv == 3) tile512_nj<SUB, 3>(nj, m, k, A, B, C, i, j, last);
+            else if (nv == 2) tile512_nj<SUB, 2>(nj, m, k, A, B, C, i, j, last);
+            else tile512_nj<SUB, 1>(nj, m, k, A, B, C, i, j, last);
+        }
+    }
+}
+template <bool SUB>
+void gemm_update_avx2(int m, int n, int k, const double* A, const double* B, double* C) {
+    auto upd = [](double a, double b, double c) { return SUB ? std::fma(-a, b, c) : std::fma(a, b, c); };
+    int j = 0;
+    for (; j + 4 <= n; j += 4) {
+        int i = 0;
+        for (; i + 12 <= m; i += 12) {
+            __m256d c[3][4];
+            for (int jj = 0; jj < 4; ++jj)
+                for (int ii = 0; ii < 3; ++ii) c[ii][jj] = _mm256_loadu_pd(C + i + 4 * ii + (int64_t)(j + jj) * m);
+            for (int p = 0; p < k; ++p) {
+                const double* ap = A + i + (int64_t)p * m;
+                const __m256d a0 = _mm256_loadu_pd(ap), a1 = _mm256_loadu_pd(ap + 4), a2 = _mm256_loadu_pd(ap + 8);
+                for (int jj = 0; jj < 4; ++jj) {
+                    const __m256d b = _mm256_broadcast_sd(B + p + (int64_t)(j + jj) * k);
+                    if (SUB) {
+                        c[0][jj] = _mm256_fnmadd_pd(a0, b, c[0][jj]);
+                        c[1][jj] = _mm256_fnmadd_pd(a1, b, c[1][jj]);
+                        c[2][jj] = _mm256_fnmadd_pd(a2, b, c[2][jj]);
+                    } else {
+                        c[0][jj] = _mm256_fmadd_pd(a0, b, c[0][jj]);
+                        c[1][jj] = _mm256_fmadd_pd(a1, b, c[1][jj]);
+                        c[2][jj] = _mm256_fmadd_pd(a2, b, c[2][jj]);
+                    }
+                }
+            }
+            for (int jj = 0; jj < 4; ++jj)
+                for (int ii = 0; ii < 3; ++ii) _mm256_storeu_pd(C + i + 4 * ii + (int64_t)(j + jj) * m, c[ii][jj]);
+        }
+        for (; i < m; ++i)
+            for (int jj = 0; jj < 4; ++jj) {
+                double c = C[i + (int64_t)(j + jj) * m];
+                for (int p = 0; p < k; ++p) c = upd(A[i + (int64_t)p * m], B[p + (int64_t)(j + jj) * k], c);
+                C[i + (int64_t)(j + jj) * m] = c;
+            }
+    }
+    for (; j < n; ++j)
+        for (int i = 0; i < m; ++i) {
+            double c = C[i + (int64_t)j * m];
+            for (int p = 0; p < k; ++p) c = upd(A[i + (int64_t)p * m], B[p + (int64_t)j * k], c);
+            C[i + (int64_t)j * m] = c;
+        }
+}
+const bool kHostAvx512 = __builtin_cpu_supports("avx512f");
+template <bool SUB>
+void gemm_update(int m, int n, int k, const double* A, const double* B, double* C) {
+    if (kHostAvx512) gemm_update_avx512<SUB>(m, n, k, A, B, C);
+    else gemm_update_avx2<SUB>(m, n, k, A, B, C);
+}
 // C(m x n) = A(m x k) * B(k x n), all column-major
 void gemm(int m, int n, int k, const double* A, const double* B, double* C) {
     std::fill(C, C + (int64_t)m * n, 0.0);
-    for (int j = 0; j < n; ++j)
-        for (int p = 0; p < k; ++p) {
-            const double b = B[p + (int64_t)j * k];
-            const double* a = A + (int64_t)p * m;
-            double* c = C + (int64_t)j * m;
-            for (int i = 0; i < m; ++i) c[i] += a[i] * b;
-        }
+    gemm_update<false>(m, n, k, A, B, C);
 }
 // C -= A * B
 void gemm_sub(int m, int n, int k, const double* A, const double* B, double* C) {
-    for (int j = 0; j < n; ++j)
-        for (int p = 0; p < k; ++p) {
-            const double b = B[p + (int64_t)j * k];
-            const double* a = A + (int64_t)p * m;
-            double* c = C + (int64_t)j * m;
-            for (int i = 0; i < m; ++i) c[i] -= a[i] * b;
-        }
+    gemm_update<true>(m, n, k, A, B, C);
 }
 
 // Explicit inverse with partial pivoting, following the semantics of
@@ -225,37 +454,64 @@ struct PreconIdentity : Precon {
 // Jacobi (precon_jacobi.f90:95-215 stores inv(diag) and applies it).
 struct PreconILU0 : Precon {
     bool jacobi = false;
-    vector<double> LD;                       // same packing as A: L blocks and inv(D)
+    DBuf LD;                                 // same packing as A: L blocks and inv(D)
     vector<vector<int>> lower, upper;        // per row, block ids (local_lower/upper_blocks)
     vector<int> itrans;                      // per block: transposed block in parent row
+    // Rows of one time level grouped by dependency level: a row's factor and
+    // forward-sweep work needs its lower parents finished (flev), its
+    // backward-sweep work its upper parents (blev).  Rows of a level are
+    // independent, so they run on the pool; each row's own arithmetic is the
+    // serial loop's.
+    vector<vector<vector<int>>> flev, blev;  // [t][level] -> elements, increasing
     void build(Mat& A) {
         lower.assign((size_t)A.nelem * A.ntime, {});
         upper.assign((size_t)A.nelem * A.ntime, {});
         itrans.assign(A.nblk, -1);
-        if (jacobi) return;
-        // type_domain_matrix.f90:295-302 with a single rank: lower iff eparent < ielem
-        for (int e = 0; e < A.nelem; ++e)
-            for (int t = 0; t < A.ntime; ++t) {
-                const int r = A.row(e, t);
-                for (int k : A.lblk[r]) {
-                    if (A.ce[k] < e) lower[r].push_back(k);
-                    else if (A.ce[k] > e) upper[r].push_back(k);
-                    // transposed block (type_domain_matrix.f90:592-627)
-                    const int p = A.ce[k];
-                    for (int kk : A.lblk[A.row(p, t)])
-                        if (A.ce[kk] == e) { itrans[k] = kk; break; }
+        if (!jacobi) {
+            // type_domain_matrix.f90:295-302 with a single rank: lower iff eparent < ielem
+            for (int e = 0; e < A.nelem; ++e)
+                for (int t = 0; t < A.ntime; ++t) {
+                    const int r = A.row(e, t);
+                    for (int k : A.lblk[r]) {
+                        if (A.ce[k] < e) lower[r].push_back(k);
+                        else if (A.ce[k] > e) upper[r].push_back(k);
+                        // transposed block (type_domain_matrix.f90:592-627)
+                        const int p = A.ce[k];
+                        for (int kk : A.lblk[A.row(p, t)])
+                            if (A.ce[kk] == e) { itrans[k] = kk; break; }
+                    }
                 }
+        }
+        flev.assign(A.ntime, {});
+        blev.assign(A.ntime, {});
+        vector<int> lv(A.nelem);
+        for (int t = 0; t < A.ntime; ++t) {
+            for (int e = 0; e < A.nelem; ++e) {
+                int l = 0;
+                for (int k : lower[A.row(e, t)]) l = std::max(l, lv[A.ce[k]] + 1);
+                lv[e] = l;
+                if ((int)flev[t].size() <= l) flev[t].resize(l + 1);
+                flev[t][l].push_back(e);
             }
+            for (int e = A.nelem - 1; e >= 0; --e) {
+                int l = 0;
+                for (int k : upper[A.row(e, t)]) l = std::max(l, lv[A.ce[k]] + 1);
+                lv[e] = l;
+                if ((int)blev[t].size() <= l) blev[t].resize(l + 1);
+                blev[t][l].push_back(e);
+            }
+        }
     }
     // precon_ILU0.f90:111-265; with A%transposed (:148-207) the factors are
     // those of A^T: D = A(e,e)^T, L = A(parent, itranspose)^T inv(D_parent),
     // D -= L A_lower^T.  precon_jacobi.f90:121-125 likewise inverts A(e,e)^T.
     int update(Mat& A) override {
-        LD.assign(A.nval, 0.0);
+        LD.zeros(A.nval);
         err_elem = -1;
+        Pool& pool = Pool::get();
         for (int t = 0; t < A.ntime; ++t) {
-            for (int e = 0; e < A.nelem; ++e) {
-                const int k = A.diag[A.row(e, t)];
+            pool.run(A.nelem, [&](int64_t e) {
+                const int k = A.diag[A.row((int)e, t)];
                 const int b = A.nr[k];
                 double* D = LD.data() + A.voff[k];
                 if (A.transposed) {
@@ -264,29 +520,42 @@ struct PreconILU0 : Precon {
                 } else {
                     std::memcpy(D, A.blk(k), sizeof(double) * A.nr[k] * A.nc[k]);
                 }
-            }
-            for (int e = 0; e < A.nelem; ++e) {
-                const int r = A.row(e, t);
-                const int kd = A.diag[r];
-                const int b = A.nr[kd];
-                double* D = LD.data() + A.voff[kd];
-                for (int kl : lower[r]) {
-                    const int p = A.ce[kl];
-                    const int kpd = A.diag[A.row(p, t)];
-                    double* L = LD.data() + A.voff[kl];
-                    const int kt = itrans[kl];
-                    if (A.transposed) {
-                        // L = A(parent, itranspose)^T * inv(D_parent); D -= L * A_lower^T
-                        gemm_tn(A.nr[kl], A.nc[kl], A.nr[kt], A.blk(kt), LD.data() + A.voff[kpd], L);
-                        gemm_sub_nt(b, A.nc[kl], A.nc[kl], L, A.blk(kl), D);
-                    } else {
-                        // L = A_lower * inv(D_parent); D -= L * A(parent, itranspose)
-                        gemm(A.nr[kl], A.nc[kl], A.nc[kl], A.blk(kl), LD.data() + A.voff[kpd], L);
-                        gemm_sub(b, A.nc[kt], A.nc[kl], L, A.blk(kt), D);
+            });
+            // The serial loop stops at the first singular element in natural
+            // order.  Once a level finds a singular element e_bad, later levels
+            // only factor rows below e_bad (their parents are below them, so
+            // all factored): the element reported is the serial loop's.
+            int e_bad = A.nelem;
+            vector<char> bad(A.nelem, 0);
+            for (const vector<int>& level : flev[t]) {
+                pool.run((int64_t)level.size(), [&](int64_t i) {
+                    const int e = level[i];
+                    if (e >= e_bad) return;
+                    const int r = A.row(e, t);
+                    const int kd = A.diag[r];
+                    const int b = A.nr[kd];
+                    double* D = LD.data() + A.voff[kd];
+                    for (int kl : lower[r]) {
+                        const int p = A.ce[kl];
+                        const int kpd = A.diag[A.row(p, t)];
+                        double* L = LD.data() + A.voff[kl];
+                        const int kt = itrans[kl];
+                        if (A.transposed) {
+                            // L = A(parent, itranspose)^T * inv(D_parent); D -= L * A_lower^T
+                            gemm_tn(A.nr[kl], A.nc[kl], A.nr[kt], A.blk(kt), LD.data() + A.voff[kpd], L);
+                            gemm_sub_nt(b, A.nc[kl], A.nc[kl], L, A.blk(kl), D);
+                        } else {
+                            // L = A_lower * inv(D_parent); D -= L * A(parent, itranspose)
+                            gemm(A.nr[kl], A.nc[kl], A.nc[kl], A.blk(kl), LD.data() + A.voff[kpd], L);
+                            gemm_sub(b, A.nc[kt], A.nc[kl], L, A.blk(kt), D);
+                        }
                     }
-                }
-                if (inv_inplace(b, D) != 0) { err_elem = e; return ORC_ESINGULAR; }
+                    if (inv_inplace(b, D) != 0) bad[e] = 1;
+                });
+                for (int e : level)
+                    if (bad[e]) e_bad = std::min(e_bad, e);
             }
+            if (e_bad < A.nelem) { err_elem = e_bad; return ORC_ESINGULAR; }
         }
         stamp = A.stamp;
         return ORC_OK;
@@ -294,32 +563,38 @@ struct PreconILU0 : Precon {
     // precon_ILU0.f90:286-411; with A%transposed the backward solve uses
     // A(parent, itranspose)^T in place of the upper block (:378-383)
     int apply(Mat& A, const double* v, double* z) override {
-        std::memcpy(z, v, sizeof(double) * A.n);
-        vector<double> tmp;
+        Pool& pool = Pool::get();
+        pool.run_chunks(A.n, kGrain, [&](int64_t q0, int64_t q1) {
+            std::memcpy(z + q0, v + q0, sizeof(double) * (q1 - q0));
+        });
         for (int t = 0; t < A.ntime; ++t) {
-            for (int e = 0; e < A.nelem; ++e) {
-                const int r = A.row(e, t);
-                double* ze = z + A.seg(e, t);
-                for (int kl : lower[r])
-                    gemv_sub(A.nr[kl], A.nc[kl], LD.data() + A.voff[kl], z + A.seg(A.ce[kl], t), ze);
-            }
-            for (int e = A.nelem - 1; e >= 0; --e) {
-                const int r = A.row(e, t);
-                double* ze = z + A.seg(e, t);
-                for (int ku : upper[r]) {
-                    if (A.transposed) {
-                        const int kt = itrans[ku];
-                        gemv_t_sub(A.nr[kt], A.nc[kt], A.blk(kt), z + A.seg(A.ce[ku], t), ze);
-                    } else {
-                        gemv_sub(A.nr[ku], A.nc[ku], A.blk(ku), z + A.seg(A.ce[ku], t), ze);
+            for (const vector<int>& level : flev[t])
+                pool.run((int64_t)level.size(), [&](int64_t i) {
+                    const int e = level[i];
+                    const int r = A.row(e, t);
+                    double* ze = z + A.seg(e, t);
+                    for (int kl : lower[r])
+                        gemv_sub(A.nr[kl], A.nc[kl], LD.data() + A.voff[kl], z + A.seg(A.ce[kl], t), ze);
+                });
+            for (const vector<int>& level : blev[t])
+                pool.run((int64_t)level.size(), [&](int64_t i) {
+                    const int e = level[i];
+                    const int r = A.row(e, t);
+                    double* ze = z + A.seg(e, t);
+                    for (int ku : upper[r]) {
+                        if (A.transposed) {
+                            const int kt = itrans[ku];
+                            gemv_t_sub(A.nr[kt], A.nc[kt], A.blk(kt), z + A.seg(A.ce[ku], t), ze);
+                        } else {
+                            gemv_sub(A.nr[ku], A.nc[ku], A.blk(ku), z + A.seg(A.ce[ku], t), ze);
+                        }
                     }
-                }
-                const int kd = A.diag[r];
-                const int b = A.nr[kd];
-                tmp.assign(b, 0.0);
-                gemv_acc(b, b, LD.data() + A.voff[kd], ze, tmp.data());
-                std::memcpy(ze, tmp.data(), sizeof(double) * b);
-            }
+                    const int kd = A.diag[r];
+                    const int b = A.nr[kd];
+                    vector<double> tmp(b, 0.0);
+                    gemv_acc(b, b, LD.data() + A.voff[kd], ze, tmp.data());
+                    std::memcpy(ze, tmp.data(), sizeof(double) * b);
+                });
         }
         return ORC_OK;
     }
@@ -354,7 +629,7 @@ struct PreconRAS : Precon {
     vector<int> lidx;                      // element -> local index on its owner
     vector<Sub> subs;
     vector<int> itrans;
-    vector<double> LD;                     // local L blocks and inv(D), packed as A
+    DBuf LD;                               // local L blocks and inv(D), packed as A
     int nsub = 0;
 
     void build(Mat& A) {
@@ -461,8 +736,20 @@ struct PreconRAS : Precon {
         if (A.ntime != 1) return ORC_EINVAL;   // single time level only (recv_dom_comm.f90:83)
         if (A.transposed) return ORC_EINVAL;   // "transpose not implemented for 'native' containers" (:254)
         err_elem = -1;
-        LD.assign(A.nval, 0.0);
-        for (int s = 0; s < nsub; ++s) {
+        LD.zeros(A.nval);
+        // Subdomains share nothing they write (each plays its own rank), so
+        // they factor on the pool; the failure reported is the one of the
+        // first failing subdomain in order, as the serial loop reports it.
+        vector<int> fail_elem(nsub, -1);
+        Pool::get().run(nsub, [&](int64_t si) { fail_elem[si] = update_sub(A, (int)si); });
+        for (int s = 0; s < nsub; ++s)
+            if (fail_elem[s] >= 0) { err_elem = fail_elem[s]; return ORC_ESINGULAR; }
+        stamp = A.stamp;
+        return ORC_OK;
+    }
+    // one subdomain's factorisation; the element whose inverse failed, or -1
+    int update_sub(Mat& A, int s) {
+        {
             Sub& S = subs[s];
             for (int e : S.elems) {
                 const int k = A.diag[A.row(e, 0)];
@@ -482,7 +769,7 @@ struct PreconRAS : Precon {
                         const int kt = itrans[kl];
                         gemm_sub(b, A.nc[kt], A.nc[kl], L, A.blk(kt), D);
                     }
-                if (inv_inplace(b, D) != 0) { err_elem = e; return ORC_ESINGULAR; }
+                if (inv_inplace(b, D) != 0) return e;
             }
             // overlap rows (received copies)
             for (auto& O : S.ov)
@@ -512,19 +799,21 @@ struct PreconRAS : Precon {
                             gemm_sub(b, A.nc[bk.trans_src], nn, bk.mat.data(), A.blk(bk.trans_src), dg.mat.data());
                         }
                     }
-                    if (inv_inplace(b, dg.mat.data()) != 0) { err_elem = oe.elem; return ORC_ESINGULAR; }
+                    if (inv_inplace(b, dg.mat.data()) != 0) return oe.elem;
                 }
         }
-        stamp = A.stamp;
-        return ORC_OK;
+        return -1;
     }
 
     // precon_RASILU0.f90:454-625 (native branch)
     int apply(Mat& A, const double* v, double* z) override {
         if (A.transposed) return ORC_EINVAL;   // "not implemented for transposed matrices" (:494)
-        vector<double> zl(A.n), tmp;
+        vector<double> zl(A.n);
         std::memcpy(zl.data(), v, sizeof(double) * A.n);  // each subdomain only touches its own rows
-        for (int s = 0; s < nsub; ++s) {
+        // subdomains write disjoint rows of zl and their own overlap copies
+        Pool::get().run(nsub, [&](int64_t si) {
+            const int s = (int)si;
+            vector<double> tmp;
             Sub& S = subs[s];
             // halo of v for the overlap elements (z%comm_send/recv)
             for (auto& O : S.ov)
@@ -582,7 +871,7 @@ struct PreconRAS : Precon {
                 gemv_acc(b, b, LD.data() + A.voff[kd], ze, tmp.data());
                 std::memcpy(ze, tmp.data(), sizeof(double) * b);
             }
-        }
+        });
         std::memcpy(z, zl.data(), sizeof(double) * A.n);
         return ORC_OK;
     }
@@ -661,13 +950,14 @@ void mtv(const Mat& A, const double* x, double* y) {
 // A%transposed), non-transposed local part :117-410
 void mv(const Mat& A, const double* x, double* y) {
     if (A.transposed) { mtv(A, x, y); return; }
-    std::fill(y, y + A.n, 0.0);
-    for (int t = 0; t < A.ntime; ++t)
-        for (int e = 0; e < A.nelem; ++e) {
-            double* ye = y + A.seg(e, t);
-            for (int k : A.rowblk[A.row(e, t)])
-                gemv_acc(A.nr[k], A.nc[k], A.blk(k), x + A.seg(A.ce[k], A.ct[k]), ye);
-        }
+    // rows are independent: each row's sum runs in the serial order on one thread
+    Pool::get().run((int64_t)A.nelem * A.ntime, [&](int64_t r) {
+        const int e = (int)(r / A.ntime), t = (int)(r % A.ntime);
+        double* ye = y + A.seg(e, t);
+        std::fill(ye, ye + A.bsize(e), 0.0);
+        for (int k : A.rowblk[A.row(e, t)])
+            gemv_acc(A.nr[k], A.nc[k], A.blk(k), x + A.seg(A.ce[k], A.ct[k]), ye);
+    });
 }
 double dotv(int64_t n, const double* x, const double* y) {
     double s = 0.0;
@@ -703,19 +993,26 @@ struct Fgmres {
     void orthogonalize(const Mat& A, vector<double>& w, const vector<vector<double>>& v, int j,
                        vector<double>& hcol, vector<double>& htmp) {
         const int64_t n = A.n;
+        Pool& pool = Pool::get();
         if (orth == 0) {            // CGS (:331-396)
-            for (int i = 0; i < j; ++i) htmp[i] = dotv(n, w.data(), v[i].data());
-            for (int i = 0; i < j; ++i) {
-                const double hi = htmp[i];
-                const double* vi = v[i].data();
-                for (int64_t q = 0; q < n; ++q) w[q] = w[q] - hi * vi[q];
-            }
+            // the j dots are independent (each a serial sum); every entry of w
+            // takes its j updates in order
+            pool.run(j, [&](int64_t i) { htmp[i] = dotv(n, w.data(), v[i].data()); });
+            pool.run_chunks(n, kGrain, [&](int64_t q0, int64_t q1) {
+                for (int i = 0; i < j; ++i) {
+                    const double hi = htmp[i];
+                    const double* vi = v[i].data();
+                    for (int64_t q = q0; q < q1; ++q) w[q] = w[q] - hi * vi[q];
+                }
+            });
         } else {                    // MGS (:417-442)
             for (int i = 0; i < j; ++i) {
                 htmp[i] = dotv(n, w.data(), v[i].data());
                 const double hi = htmp[i];
                 const double* vi = v[i].data();
-                for (int64_t q = 0; q < n; ++q) w[q] = w[q] - hi * vi[q];
+                pool.run_chunks(n, kGrain, [&](int64_t q0, int64_t q1) {
+                    for (int64_t q = q0; q < q1; ++q) w[q] = w[q] - hi * vi[q];
+                });
             }
         }
         for (int i = 0; i < j; ++i) hcol[i] += htmp[i];
@@ -816,11 +1113,13 @@ struct Fgmres {
                 y[ii] = sacc;
             }
             x = x0;
-            for (int iv = 0; iv < nvecs; ++iv) {
-                const double yi = y[iv];
-                const double* zi = z[iv].data();
-                for (int64_t q = 0; q < n; ++q) x[q] = x[q] + yi * zi[q];
-            }
+            Pool::get().run_chunks(n, kGrain, [&](int64_t q0, int64_t q1) {
+                for (int iv = 0; iv < nvecs; ++iv) {
+                    const double yi = y[iv];
+                    const double* zi = z[iv].data();
+                    for (int64_t q = q0; q < q1; ++q) x[q] = x[q] + yi * zi[q];
+                }
+            });
             res_est = res;
             if (cabs || crel || cmax) break;
             x0 = x;
@@ -876,7 +1175,7 @@ orc_matrix* orc_matrix_create(int32_t nelem, int32_t ntime, const int32_t* elem_
         v += (int64_t)A.nr[k] * A.nc[k];
     }
     A.nval = v;
-    A.val.assign(v, 0.0);
+    A.val.zeros(v);
     for (int kind = 0; kind < 4; ++kind)
         for (int64_t k = 0; k < nblocks; ++k) {
             if (A.kind[k] != kind) continue;
@@ -895,12 +1194,12 @@ void orc_matrix_destroy(orc_matrix* h) { delete h; }
 int64_t orc_matrix_nvalues(const orc_matrix* h) { return h->m.nval; }
 int64_t orc_matrix_nvec(const orc_matrix* h) { return h->m.n; }
 int orc_matrix_set_values(orc_matrix* h, const double* packed) {
-    std::memcpy(h->m.val.data(), packed, sizeof(double) * h->m.nval);
+    h->m.val.copy_from(packed);
     h->m.stamp++;
     return ORC_OK;
 }
 int orc_matrix_get_values(const orc_matrix* h, double* packed) {
-    std::memcpy(packed, h->m.val.data(), sizeof(double) * h->m.nval);
+    h->m.val.copy_to(packed);
     return ORC_OK;
 }
 int orc_matrix_block_offsets(const orc_matrix* h, int64_t* offsets) {
@@ -912,6 +1211,12 @@ int orc_matrix_set_transposed(orc_matrix* h, int32_t transposed) { h->m.transpos
 int orc_mv(orc_matrix* h, const double* x, double* y) { mv(h->m, x, y); return ORC_OK; }
 double orc_dot(const orc_matrix* h, const double* x, const double* y) { return dotv(h->m.n, x, y); }
 double orc_norm(const orc_matrix* h, const double* x) { return std::sqrt(dotv(h->m.n, x, x)); }
+int orc_set_threads(int32_t n) {
+    if (n < 1) return ORC_EINVAL;
+    Pool::get().set_threads(n);
+    return ORC_OK;
+}
+int32_t orc_get_threads(void) { return Pool::get().threads(); }
 int orc_inv(int32_t n, const double* a, double* ainv) {
     std::memcpy(ainv, a, sizeof(double) * n * n);
     return inv_inplace(n, ainv) ? ORC_ESINGULAR : ORC_OK;
@@ -939,9 +1244,9 @@ int orc_precon_apply(orc_precon* pc, orc_matrix* h, const double* v, double* z) 
 int orc_precon_error_elem(const orc_precon* pc) { return pc->p->err_elem; }
 int orc_precon_get_LD(const orc_precon* pc, double* packed) {
     auto* q = dynamic_cast<PreconILU0*>(pc->p.get());
-    if (q) { std::memcpy(packed, q->LD.data(), sizeof(double) * q->LD.size()); return ORC_OK; }
+    if (q) { q->LD.copy_to(packed); return ORC_OK; }
     auto* r = dynamic_cast<PreconRAS*>(pc->p.get());
-    if (r) { std::memcpy(packed, r->LD.data(), sizeof(double) * r->LD.size()); return ORC_OK; }
+    if (r) { r->LD.copy_to(packed); return ORC_OK; }
     return ORC_EINVAL;
 }
 

@@ -72,6 +72,12 @@ int     orc_mv(orc_matrix*, const double* x, double* y);
 double  orc_dot(const orc_matrix*, const double* x, const double* y);
 double  orc_norm(const orc_matrix*, const double* x);
 int     orc_inv(int32_t n, const double* a, double* ainv);
+/* Host threads for the data-parallel loops (matrix rows, ILU rows of one
+ * dependency level, RAS subdomains, independent Gram-Schmidt dots).  Results
+ * are bitwise the same for every thread count: each row, dot or vector entry
+ * is computed on one thread in the serial order.  Default 1. */
+int     orc_set_threads(int32_t n);
+int32_t orc_get_threads(void);
 
 orc_precon* orc_precon_create(orc_matrix*, int32_t kind);
 void    orc_precon_destroy(orc_precon*);

@@ -66,6 +66,8 @@ def lib():
         L.orc_norm.restype = C.c_double
         L.orc_norm.argtypes = [VP, DP]
         L.orc_inv.argtypes = [C.c_int32, DP, DP]
+        L.orc_set_threads.argtypes = [C.c_int32]
+        L.orc_get_threads.restype = C.c_int32
         L.orc_precon_create.restype = VP
         L.orc_precon_create.argtypes = [VP, C.c_int32]
         L.orc_precon_destroy.argtypes = [VP]
@@ -76,6 +78,17 @@ def lib():
         L.orc_fgmres_solve.argtypes = [VP, VP, DP, DP, C.POINTER(Opts), C.POINTER(Result), DP, C.c_int32]
         _L = L
     return _L
+
+
+def set_threads(n: int) -> None:
+    """Host threads of the oracle's data-parallel loops (results are bitwise
+    the same for every count)."""
+    if lib().orc_set_threads(int(n)):
+        raise ValueError("oracle: thread count must be >= 1")
+
+
+def get_threads() -> int:
+    return int(lib().orc_get_threads())
 
 
 def _dp(a):

@@ -5,7 +5,8 @@ compiler).  Each known-answer test poke-sets matrix blocks with
 right-hand side per element, and asserts values; this script replays that
 bookkeeping and records the matrices, right-hand sides and expected values.
 
-Usage: python tests/golden/make_golden.py [/path/to/ChiDG]   (default /root/reference)
+Usage: python tests/golden/make_golden.py /path/to/ChiDG
+(the root of the ChiDG source tree; required)
 """
 from __future__ import annotations
 
@@ -210,4 +211,6 @@ def main(root: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py /path/to/ChiDG")
+    main(sys.argv[1])

@@ -1,6 +1,6 @@
 """Host-side pieces of bench.py (no GPU): the seeded Euler box of the
-configurations and the host-assembled Newton system that the CPU baseline and
-the reference arm solve with the oracle."""
+configurations and the host-assembled Newton system that the reference arm
+solves with the oracle."""
 import numpy as np
 
 import bench
@@ -16,13 +16,24 @@ def test_euler_box_seeding():
     assert np.array_equal(centre, centre2)                  # the centre depends on the seed only
 
 
-def test_cpu_sample_system_is_solved_by_the_oracle():
-    pat, vals, b = bench.cpu_sample_system(n=3)
+def test_host_newton_system_is_solved_by_the_oracle():
+    pat, vals, b = bench.host_newton_system(n=3)
     assert vals.size == pat.value_offsets()[1] and b.size == pat.vector_size()
-    A = O.OracleMatrix(pat)
-    A.set_values(vals)
-    dt, niter = bench.cpu_sample_solve((pat, vals, b), A)
-    assert dt > 0.0 and 0 < niter < bench.SOLVER["nmax"]
-    opts = {k: v for k, v in bench.SOLVER.items() if k != "orthogonalization"}
-    x, res = O.fgmres(A, O.OraclePrecon(A, "ilu0"), b, O.default_opts(**opts))
+    A = bench.oracle_matrix(pat, vals)
+    dt, x, res = bench.oracle_solve(A, b)
+    assert dt > 0.0 and 0 < res["niter"] < bench.SOLVER["nmax"]
     assert np.linalg.norm(A.mv(x) - b) <= 1e-8 * np.linalg.norm(b) * 1.0001
+
+
+def test_oracle_threads_give_the_one_thread_solution():
+    """The reference arm runs the oracle on every host thread; its solution is
+    bitwise the one-thread solution."""
+    pat, vals, b = bench.host_newton_system(n=4, order=1)
+    out = []
+    for threads in (1, 3):
+        O.set_threads(threads)
+        A = bench.oracle_matrix(pat, vals)
+        out.append(bench.oracle_solve(A, b)[1:])
+    O.set_threads(1)
+    (x1, r1), (x3, r3) = out
+    assert np.array_equal(x1, x3) and np.array_equal(r1["hist"], r3["hist"])
