@@ -59,7 +59,7 @@ class Context:
         return c.value
 
     PROFILE_CLASSES = {"matvec": 0, "ilu_forward": 1, "ilu_backward": 2, "factor": 3, "matvec_fp32": 4,
-                       "ilu_lowp": 5, "factor_gemm": 6, "factor_inverse": 7}
+                       "ilu_lowp": 5, "factor_gemm": 6, "factor_inverse": 7, "ilu_backward_matvec": 8}
 
     def set_profiling(self, on: bool):
         self.check(self.L.chidg_gpu_ctx_set_profiling(self.h, int(bool(on))), "set_profiling")

@@ -4,6 +4,8 @@
 // level-scheduled GPU sweeps.  The FGMRES driver lives in fgmres.cu.
 #include "chidg_gpu_internal.cuh"
 
+#include <type_traits>
+
 #include <atomic>
 
 #include <algorithm>
@@ -1230,6 +1232,8 @@ static int finalize_program(chidg_gpu_ctx* ctx, const chidg_gpu_matrix* A, IluPr
     };
     bucket(lf, P.fwd_rows, P.fwd_ptr);
     bucket(lb, P.bwd_rows, P.bwd_ptr);
+    P.lb = lb;
+    P.bmv_uid = -1;
     // task-split sweeps: one task per entry, combine-only tasks for rows
     // without entries; hand-out order by the level of the parent row
     {
@@ -1412,8 +1416,10 @@ void chidg::release_program(IluProgram& P) {
                       &P.d_lo_par, &P.d_lo_nc, &P.d_up_ptr, &P.d_up_U, &P.d_up_par, &P.d_up_nc, &P.d_fwd_rows,
                       &P.d_bwd_rows, &P.d_ltasks, &P.d_lpairs, &P.d_stasks, &P.d_spairs, &P.d_tf_row, &P.d_tf_ent,
                       &P.d_tb_row, &P.d_tb_ent, &P.d_poff_f, &P.d_poff_b, &P.d_sb_row, &P.d_sb_ent, &P.d_asm_ptr,
-                      &P.d_asm_src, &P.d_asm_r0, &P.d_asm_c0, &P.d_asm_nr, &P.d_asm_nc})
+                      &P.d_asm_src, &P.d_asm_r0, &P.d_asm_c0, &P.d_asm_nr, &P.d_asm_nc, &P.d_bmv_row, &P.d_bmv_ent,
+                      &P.d_col_prow})
         release(*b);
+    P.bmv_uid = -1;
 }
 
 // The ILU programme of M from A's pattern, or from A^T's when A->transposed
@@ -1829,16 +1835,18 @@ static StreamShape stream_shape() {
     return sh;
 }
 
-template <typename TL, typename TU, typename TV, bool FWD, int CW>
+template <typename TL, typename TU, typename TV, bool FWD, int CW, typename TA = double, bool MV = false>
 static int stream_launch(chidg_gpu_precon* M, const TL* LD, const TU* U, StreamTasks Tk, int ntask, const TV* v, TV* zx,
-                         void* part, SweepSync S, const StreamShape& sh, int variant) {
+                         void* part, SweepSync S, const StreamShape& sh, int variant, FusedMv<TA, TV> F = {},
+                         int mv_cols = 0) {
     chidg_gpu_ctx* ctx = M->ctx;
     using ACC = typename AccOf<TV>::type;
-    const size_t smem = stream_smem_bytes(sizeof(ACC), sh.nstage, sh.stage_bytes, M->P.max_b, 32 * CW);
-    auto k = k_ilu_stream<TL, TU, TV, ACC, FWD, CW>;
+    const int xcols = std::max(M->P.max_b, mv_cols);    // the widest segment staged in shared memory
+    const size_t smem = stream_smem_bytes(sizeof(ACC), sh.nstage, sh.stage_bytes, xcols, 32 * CW);
+    auto k = k_ilu_stream<TL, TU, TV, ACC, FWD, CW, TA, MV>;
     int st;
     if ((st = raise_smem_limit((const void*)k, smem))) return fail(ctx, st, "streamed sweep shared memory");
-    int& grid = M->ss_grid[variant][FWD ? 0 : 1];
+    int& grid = M->ss_grid[variant][MV ? 2 : FWD ? 0 : 1];
     if (grid == 0) {
         int per_sm = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 32 * CW + 32, smem) != cudaSuccess || per_sm < 1) {
@@ -1848,14 +1856,80 @@ static int stream_launch(chidg_gpu_precon* M, const TL* LD, const TU* U, StreamT
         grid = per_sm * ctx->nsm;
     }
     k<<<std::max(1, std::min(grid, ntask)), 32 * CW + 32, smem, ctx->stream>>>(M->P.rows, LD, U, Tk, ntask, v, zx, (ACC*)part,
-                                                                              S, sh.nstage, sh.stage_bytes, M->P.max_b);
-    return check_launch(ctx, FWD ? "k_ilu_stream forward" : "k_ilu_stream backward");
+                                                                              S, sh.nstage, sh.stage_bytes, xcols, F);
+    return check_launch(ctx, MV ? "k_ilu_stream backward + matvec" : FWD ? "k_ilu_stream forward" : "k_ilu_stream backward");
+}
+
+// Task list of the backward sweep with the matvec rows of A in it: the
+// streamed backward sweep's tasks in their order (the keys of finalize_program,
+// scaled by 4), and for every matrix row r a task (r, -3) keyed after the
+// inv(D) task of the last row its columns read, `lag` levels later, so that
+// when a CTA takes it the rows it waits for are most likely published.  A
+// matvec task waits only for tasks with smaller tickets (deadlock freedom as
+// for the sweep).  Needs programme rows == matrix rows (ILU0, Jacobi).
+static int build_bwd_mv_tasks(chidg_gpu_precon* M, const chidg_gpu_matrix* A, int lag) {
+    IluProgram& P = M->P;
+    if (P.bmv_uid == A->uid && P.bmv_lag == lag) return CHIDG_GPU_OK;
+    const int np = P.nprow;
+    std::vector<int> first(np + 1, 0);
+    for (int pr = 0; pr < np; ++pr) first[pr + 1] = first[pr] + (int)P.up[pr].size();
+    std::vector<std::pair<int64_t, std::pair<int32_t, int32_t>>> keyed;
+    for (int32_t pr : P.bwd_rows) {
+        keyed.push_back({4LL * (2 * P.lb[pr] - 1), {pr, -2}});
+        for (size_t e = 0; e < P.up[pr].size(); ++e)
+            keyed.push_back({4LL * (2 * P.lb[P.up[pr][e].parent]), {pr, first[pr] + (int32_t)e}});
+    }
+    std::vector<int32_t> col_prow;
+    col_prow.reserve(A->nblk);
+    for (int r = 0; r < A->nrow; ++r) {
+        int last = -1;
+        for (int32_t k : A->rowblk[r]) {
+            const int c = A->row(A->ce[k], A->ct[k]);
+            col_prow.push_back(c);
+            last = std::max(last, 2 * P.lb[c] - 1);
+        }
+        keyed.push_back({4LL * (last + 2 * lag) + 2, {r, -3}});
+    }
+    std::stable_sort(keyed.begin(), keyed.end(), [](const auto& a, const auto& c) { return a.first < c.first; });
+    std::vector<int32_t> tr, te;
+    tr.reserve(keyed.size());
+    te.reserve(keyed.size());
+    for (auto& k : keyed) { tr.push_back(k.second.first); te.push_back(k.second.second); }
+    int st;
+    if ((st = upload_array(M->ctx, P.d_bmv_row, tr)) || (st = upload_array(M->ctx, P.d_bmv_ent, te)) ||
+        (st = upload_array(M->ctx, P.d_col_prow, col_prow)))
+        return st;
+    P.ntask_bmv = (int)tr.size();
+    P.bmv_uid = A->uid;
+    P.bmv_lag = lag;
+    return CHIDG_GPU_OK;
+}
+
+// Levels by which a matvec row trails the last row it reads in the fused
+// backward sweep; CHIDG_FUSED_MV=0 turns the fusion off (comparison runs),
+// CHIDG_FUSED_LAG=<n> sets the lag.
+static bool fused_mv_enabled() {
+    static const bool v = [] {
+        const char* e = std::getenv("CHIDG_FUSED_MV");
+        return !(e && e[0] == '0');
+    }();
+    return v;
+}
+static int fused_mv_lag() {
+    static const int v = [] {
+        int lag = 1;
+        if (const char* e = std::getenv("CHIDG_FUSED_LAG")) lag = std::max(0, std::min(8, std::atoi(e)));
+        return lag;
+    }();
+    return v;
 }
 
 // Both sweeps as two streamed launches (CHIDG_SCHED_STREAM): persistent CTAs,
-// blocks prefetched into shared memory by a producer lane.
-template <typename TL, typename TU, typename TV>
-static int stream_sweeps(chidg_gpu_precon* M, const TL* LD, const TU* U, const TV* v, TV* zx, int variant) {
+// blocks prefetched into shared memory by a producer lane.  With F, the
+// backward launch also runs the matvec rows of F (task list d_bmv_*).
+template <typename TL, typename TU, typename TV, typename TA = double>
+static int stream_sweeps(chidg_gpu_precon* M, const TL* LD, const TU* U, const TV* v, TV* zx, int variant,
+                         const FusedMv<TA, TV>* F = nullptr, int mv_cols = 0) {
     chidg_gpu_ctx* ctx = M->ctx;
     IluProgram& P = M->P;
     using ACC = typename AccOf<TV>::type;
@@ -1881,10 +1955,22 @@ static int stream_sweeps(chidg_gpu_precon* M, const TL* LD, const TU* U, const T
     if (st) return st;
     if (sizeof(TV) == 8) {
         prof_end(ctx, ph);
-        ph = prof_begin(ctx, kProfIluBackward);
+        ph = prof_begin(ctx, F ? kProfIluBackwardMv : kProfIluBackward);
     }
     S.epoch = ++M->epoch;
     S.counter = sync + 1;
+    if (F) {
+        StreamTasks Tm{(const int32_t*)P.d_bmv_row.ptr, (const int32_t*)P.d_bmv_ent.ptr, (const int64_t*)P.d_poff_b.ptr,
+                       flags + 2 * P.nprow, flags + 3 * P.nprow};
+        switch (sh.cw) {
+            case 16: st = stream_launch<TL, TU, TV, false, 16, TA, true>(M, LD, U, Tm, P.ntask_bmv, v, zx, pb.ptr, S, sh, variant, *F, mv_cols); break;
+            case 4: st = stream_launch<TL, TU, TV, false, 4, TA, true>(M, LD, U, Tm, P.ntask_bmv, v, zx, pb.ptr, S, sh, variant, *F, mv_cols); break;
+            default: st = stream_launch<TL, TU, TV, false, 8, TA, true>(M, LD, U, Tm, P.ntask_bmv, v, zx, pb.ptr, S, sh, variant, *F, mv_cols);
+        }
+        if (st) return st;
+        prof_end(ctx, ph);
+        return CHIDG_GPU_OK;
+    }
     StreamTasks Tb{(const int32_t*)P.d_sb_row.ptr, (const int32_t*)P.d_sb_ent.ptr, (const int64_t*)P.d_poff_b.ptr,
                    flags + 2 * P.nprow, flags + 3 * P.nprow};
     switch (sh.cw) {
@@ -2010,6 +2096,44 @@ int chidg::precon_apply_impl(chidg_gpu_precon* M, const TV* v, TV* z, int precis
 }
 template int chidg::precon_apply_impl<double>(chidg_gpu_precon*, const double*, double*, int);
 template int chidg::precon_apply_impl<float>(chidg_gpu_precon*, const float*, float*, int);
+
+template <typename TV, typename TA>
+int chidg::precon_apply_mv(chidg_gpu_precon* M, const TV* v, TV* z, int precision, chidg_gpu_matrix* Aop, const TA* val,
+                           TV* w, double* row_sq) {
+    constexpr int kNotFused = 1;
+    if (!fused_mv_enabled() || !(M->kind == CHIDG_PRECON_ILU0 || M->kind == CHIDG_PRECON_JACOBI)) return kNotFused;
+    // the matvec's value type must be the one the solver's product reads
+    constexpr bool ta_bf16 = std::is_same<TA, __nv_bfloat16>::value;
+    if (sizeof(TV) == 4 && ta_bf16 != (precision == CHIDG_GPU_MIXED_BF16)) return kNotFused;
+    chidg_gpu_matrix* S = nullptr;
+    int st;
+    if ((st = precon_source(M, &S))) return st;
+    IluProgram& P = M->P;
+    if (S != Aop || M->schedule != CHIDG_SCHED_STREAM || P.max_b > SS_MAX_B || P.n_ext != Aop->n ||
+        P.nprow != Aop->nrow || !Aop->rows_contiguous || Aop->max_b > SS_MAX_B || matvec_rows_env())
+        return kNotFused;
+    if ((st = build_bwd_mv_tasks(M, Aop, fused_mv_lag()))) return st;
+    MatvecRowsView R{(const int64_t*)Aop->d_row_ptr.ptr, (const int64_t*)Aop->d_blk_voff.ptr,
+                     (const int64_t*)Aop->d_blk_xoff.ptr, (const int32_t*)Aop->d_blk_nc.ptr,
+                     (const int64_t*)Aop->d_row_yoff.ptr, (const int32_t*)Aop->d_row_b.ptr};
+    const FusedMv<TA, TV> F{R, val, w, row_sq, (const int32_t*)P.d_col_prow.ptr};
+    if constexpr (sizeof(TV) == 8) {
+        if (precision == CHIDG_GPU_MIXED_PRECON_FP32)
+            return stream_sweeps(M, (const float*)M->LD32.ptr, (const float*)S->val32.ptr, v, z, 3, &F, Aop->max_row_cols);
+        return stream_sweeps(M, (const double*)M->LD.ptr, (const double*)S->val.ptr, v, z, 0, &F, Aop->max_row_cols);
+    } else {
+        if (precision == CHIDG_GPU_MIXED_BF16)
+            return stream_sweeps(M, (const __nv_bfloat16*)M->LD16.ptr, (const __nv_bfloat16*)S->val16.ptr, v, z, 2, &F,
+                                 Aop->max_row_cols);
+        return stream_sweeps(M, (const float*)M->LD32.ptr, (const float*)S->val32.ptr, v, z, 1, &F, Aop->max_row_cols);
+    }
+}
+template int chidg::precon_apply_mv<double, double>(chidg_gpu_precon*, const double*, double*, int, chidg_gpu_matrix*,
+                                                    const double*, double*, double*);
+template int chidg::precon_apply_mv<float, float>(chidg_gpu_precon*, const float*, float*, int, chidg_gpu_matrix*,
+                                                  const float*, float*, double*);
+template int chidg::precon_apply_mv<float, __nv_bfloat16>(chidg_gpu_precon*, const float*, float*, int, chidg_gpu_matrix*,
+                                                          const __nv_bfloat16*, float*, double*);
 
 int chidg::precon_set_smem(chidg_gpu_precon* M) {
     IluProgram& P = M->P;

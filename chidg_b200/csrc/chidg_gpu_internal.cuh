@@ -67,6 +67,12 @@ struct IluProgram {
     Buffer d_tf_row, d_tf_ent, d_tb_row, d_tb_ent, d_poff_f, d_poff_b;
     int ntask_sb = 0;                          // streamed backward sweep: U tasks + inv(D) tasks
     Buffer d_sb_row, d_sb_ent;
+    std::vector<int> lb;                       // backward dependency level of every programme row
+    // streamed backward sweep with the following matvec's rows (entry -3),
+    // built for one matrix structure (bmv_uid) on first use
+    int ntask_bmv = 0, bmv_lag = -1;
+    int64_t bmv_uid = -1;
+    Buffer d_bmv_row, d_bmv_ent, d_col_prow;
     // rows whose D is assembled from several blocks of A (precon_HB) instead
     // of starting from one diagonal block: pieces per row, placed at (r0, c0)
     bool assembled = false;
@@ -84,7 +90,7 @@ struct IluProgram {
 namespace chidg {
 // kernel classes timed with CUDA events when profiling is on
 enum { kProfMatvec = 0, kProfIluForward = 1, kProfIluBackward = 2, kProfFactor = 3, kProfMatvec32 = 4, kProfIlu32 = 5,
-       kProfFactorGemm = 6, kProfFactorInv = 7, kProfClasses = 8 };
+       kProfFactorGemm = 6, kProfFactorInv = 7, kProfIluBackwardMv = 8, kProfClasses = 9 };
 struct EvPair { cudaEvent_t a, b; int cls; };
 }  // namespace chidg
 
@@ -178,7 +184,7 @@ struct chidg_gpu_precon {
     unsigned epoch = 0;
     int sf_grid[3] = {0, 0, 0};            // resident CTAs of the dataflow sweep per vector type
     int tk_grid[4] = {0, 0, 0, 0};         // resident CTAs of the task-split sweep per variant
-    int ss_grid[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};  // resident CTAs of the streamed sweeps (forward, backward)
+    int ss_grid[4][3] = {};                // resident CTAs of the streamed sweeps (forward, backward, backward + matvec)
 };
 
 namespace chidg {
@@ -207,6 +213,13 @@ int set_matvec_smem(chidg_gpu_matrix* A);
 int raise_smem_limit(const void* func, size_t bytes);
 template <typename TV>
 int precon_apply_impl(chidg_gpu_precon* M, const TV* v, TV* z, int precision);
+// z = M v followed by w = Aop z (with w's row sums of squares) when both can
+// run as one streamed backward sweep with the matvec rows in it: returns
+// CHIDG_GPU_OK having done both, 1 (+ nothing done) when this M / Aop / type
+// combination does not take the fused path, or an error code.
+template <typename TV, typename TA>
+int precon_apply_mv(chidg_gpu_precon* M, const TV* v, TV* z, int precision, chidg_gpu_matrix* Aop, const TA* val,
+                    TV* w, double* row_sq);
 int precon_set_smem(chidg_gpu_precon* M);
 void release_program(IluProgram& P);
 int status_word(chidg_gpu_ctx* ctx, double slot_value);

@@ -82,6 +82,9 @@ struct Solver {
     double residual_norm = 0.0, res_est = 0.0, r0norm_initial = 0.0;
     std::vector<double>* hist = nullptr;
     std::function<int(const T*, T*)> precon;        // z = M v
+    // z = M v and w = A z with w's row sums of squares in one streamed pass;
+    // returns 1 (nothing done) when the preconditioner cannot fuse them
+    std::function<int(const T*, T*, T*, double*)> precon_mv;
     std::function<int()> precon_update;              // M%update, or empty
     std::unique_ptr<Solver<T>> child;
     Workspace own;
@@ -138,7 +141,7 @@ struct Solver {
             c.ctx = ctx; c.A = A;
             c.nkrylov = inner_nkrylov; c.tol = inner_tol; c.rtol = inner_rtol; c.nmax = inner_nmax;
             c.orth = inner_orth; c.inner = false;
-            c.precon = precon; c.precon_update = precon_update;
+            c.precon = precon; c.precon_mv = precon_mv; c.precon_update = precon_update;
             c.true_residual = true_residual;
         }
         if (precon_update && (st = precon_update())) return st;
@@ -181,17 +184,32 @@ struct Solver {
                 T* vj = Vb + (int64_t)(j - 1) * n;
                 T* zj = Zb + (int64_t)(j - 1) * n;
                 T* w = Vb + (int64_t)j * n;
-                if ((st = precon(vj, zj))) return st;
-                if (inner) {
-                    T* ZR = (T*)ws->zr.ptr;
-                    T* DZ = (T*)ws->dz.ptr;
-                    if ((st = matvec(zj, ZR, vj, -1.0, 1.0, false, 0))) return st;   // zr = v - A z
-                    if ((st = child->solve(ZR, DZ))) return st;
-                    inner_iters += child->niter;
-                    if ((st = axpby(1.0, DZ, 1.0, zj))) return st;                     // z = z + dz
+                // z_j = M v_j, then w = A z_j and ||w|| before orthogonalisation;
+                // without an inner solve both can run as one streamed pass
+                bool fused = false;
+                if (precon_mv && !inner) {
+                    if ((st = ensure(ctx, ws->rowsq, sizeof(double) * (size_t)A->nrow))) return st;
+                    st = precon_mv(vj, zj, w, (double*)ws->rowsq.ptr);
+                    if (st == CHIDG_GPU_OK) {
+                        fused = true;
+                        if ((st = reduce_partials(ctx, (const double*)ws->rowsq.ptr, A->nrow, 1, kSlotNormBefore, false)))
+                            return st;
+                    } else if (st != 1) {
+                        return st;
+                    }
                 }
-                // w = A z_j and ||w|| before orthogonalisation
-                if ((st = matvec(zj, w, nullptr, 1.0, 0.0, true, kSlotNormBefore))) return st;
+                if (!fused) {
+                    if ((st = precon(vj, zj))) return st;
+                    if (inner) {
+                        T* ZR = (T*)ws->zr.ptr;
+                        T* DZ = (T*)ws->dz.ptr;
+                        if ((st = matvec(zj, ZR, vj, -1.0, 1.0, false, 0))) return st;   // zr = v - A z
+                        if ((st = child->solve(ZR, DZ))) return st;
+                        inner_iters += child->niter;
+                        if ((st = axpby(1.0, DZ, 1.0, zj))) return st;                     // z = z + dz
+                    }
+                    if ((st = matvec(zj, w, nullptr, 1.0, 0.0, true, kSlotNormBefore))) return st;
+                }
                 if ((st = gs_pass(w, Vb, j))) return st;
                 if ((st = fetch_scalars(ctx, 0, kSlotH + j, sc.data()))) return st;
                 if ((st = status_word(ctx, sc[kSlotStatus]))) return st;
@@ -346,6 +364,9 @@ extern "C" int chidg_gpu_fgmres_solve(chidg_gpu_matrix* A, chidg_gpu_precon* M, 
     int64_t lo_iters = 0;
     if (prec == CHIDG_GPU_FP64 || prec == CHIDG_GPU_MIXED_PRECON_FP32) {
         S.precon = [M, prec](const double* v, double* z) { return precon_apply_impl<double>(M, v, z, prec); };
+        S.precon_mv = [M, prec, Aop](const double* v, double* z, double* w, double* rs) {
+            return precon_apply_mv<double, double>(M, v, z, prec, Aop, (const double*)Aop->val.ptr, w, rs);
+        };
     } else {
         // FP32 inner FGMRES as the flexible preconditioner of the FP64 outer loop
         S.inner = false;
@@ -357,6 +378,14 @@ extern "C" int chidg_gpu_fgmres_solve(chidg_gpu_matrix* A, chidg_gpu_precon* M, 
         lo->true_residual = false;
         lo->precision = prec;
         lo->precon = [M, prec](const float* v, float* z) { return precon_apply_impl<float>(M, v, z, prec); };
+        if (prec == CHIDG_GPU_MIXED_BF16)
+            lo->precon_mv = [M, prec, Aop](const float* v, float* z, float* w, double* rs) {
+                return precon_apply_mv<float, __nv_bfloat16>(M, v, z, prec, Aop, (const __nv_bfloat16*)Aop->val16.ptr, w, rs);
+            };
+        else
+            lo->precon_mv = [M, prec, Aop](const float* v, float* z, float* w, double* rs) {
+                return precon_apply_mv<float, float>(M, v, z, prec, Aop, (const float*)Aop->val32.ptr, w, rs);
+            };
         if ((st = ensure(ctx, v32, sizeof(float) * (size_t)A->n)) || (st = ensure(ctx, z32, sizeof(float) * (size_t)A->n))) return st;
         Solver<float>* lp = lo.get();
         float* V32 = (float*)v32.ptr;

@@ -22,28 +22,7 @@
 
 namespace chidg {
 
-// the sum over the consumer threads (result in consumer thread 0)
-template <int NC>
-__device__ __forceinline__ double consumers_sum(double v, double* scratch, int ctid) {
-    v = warp_sum(v);
-    if ((ctid & 31) == 0) scratch[ctid >> 5] = v;
-    consumers_sync<NC>();
-    double s = 0.0;
-    if (ctid < 32) {
-        s = (ctid < NC / 32) ? scratch[ctid] : 0.0;
-        s = warp_sum(s);
-    }
-    return s;
-}
-
-struct MatvecRows {
-    const int64_t* row_ptr;     // blocks of row i: row_ptr[i] .. row_ptr[i+1]-1
-    const int64_t* blk_voff;
-    const int64_t* blk_xoff;
-    const int32_t* blk_nc;
-    const int64_t* row_yoff;
-    const int32_t* row_b;
-};
+using MatvecRows = MatvecRowsView;
 
 __host__ __device__ constexpr size_t matvec_stream_smem(size_t acc_size, int stages, int stage_bytes, int max_cols,
                                                          int nc) {

@@ -58,14 +58,43 @@ struct StreamTasks {
     unsigned* ready;            // backward: per row, epoch once all U partials are written
 };
 
+// the row structure of a matrix whose rows' blocks are stored one after
+// another (the streamed matvec's view)
+struct MatvecRowsView {
+    const int64_t* row_ptr;     // blocks of row i: row_ptr[i] .. row_ptr[i+1]-1
+    const int64_t* blk_voff;
+    const int64_t* blk_xoff;
+    const int32_t* blk_nc;
+    const int64_t* row_yoff;
+    const int32_t* row_b;
+};
+
 // ring of `stages` stages of `stage_bytes` (a multiple of 16), the parent
 // segment (xcap values: the largest block of the programme), the row-sum
 // scratch (nc values, one per consumer thread), mbarriers and descriptors
 __host__ __device__ constexpr size_t stream_xcap(int max_b) { return (size_t)((max_b + 31) / 32) * 32; }
+// (max_b: the largest segment staged at once -- a block's columns, or with
+// fused matvec rows also a matrix row's columns; a 32-double scratch follows
+// the row sums for the fused rows' sums of squares)
 __host__ __device__ constexpr size_t stream_smem_bytes(size_t acc_size, int stages, int stage_bytes, int max_b, int nc) {
-    return (size_t)stages * stage_bytes + (stream_xcap(max_b) + nc) * acc_size + 2 * SS_MAX_STAGES * sizeof(uint64_t) +
-           SS_MAX_STAGES * sizeof(StreamMeta) + 64;
+    return (size_t)stages * stage_bytes + (stream_xcap(max_b) + nc) * acc_size + 32 * sizeof(double) +
+           2 * SS_MAX_STAGES * sizeof(uint64_t) + SS_MAX_STAGES * sizeof(StreamMeta) + 64;
 }
+
+// The matvec that follows the backward sweep in FGMRES (w = A z_j,
+// type_fgmres.f90:175-189), run inside the backward sweep's launch: one task
+// per matrix row (entry -3), handed out after the sweep tasks that publish
+// the rows its columns read, so the rows' values stream while the sweep's
+// dependency chain waits.  Row r computes y_r = A_r z and its sum of squares
+// exactly as k_matvec_stream does (same chunks, same per-thread order).
+template <typename TA, typename TX>
+struct FusedMv {
+    MatvecRowsView rows;         // the matrix rows (contiguous values per row)
+    const TA* val;
+    TX* y;
+    double* row_sumsq;
+    const int32_t* col_prow;     // per block of the matrix: the programme row publishing its column segment
+};
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
@@ -115,6 +144,20 @@ __device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v) {
     return old;
 }
 
+// the sum over the consumer threads (result in consumer thread 0)
+template <int NC>
+__device__ __forceinline__ double consumers_sum(double v, double* scratch, int ctid) {
+    v = warp_sum(v);
+    if ((ctid & 31) == 0) scratch[ctid >> 5] = v;
+    consumers_sync<NC>();
+    double s = 0.0;
+    if (ctid < 32) {
+        s = (ctid < NC / 32) ? scratch[ctid] : 0.0;
+        s = warp_sum(s);
+    }
+    return s;
+}
+
 // acc[rr] += sum over the chunk's columns of block(r, c) * x(c); rows r of this
 // thread as set up by the caller (b <= NC: one row, columns strided by the G
 // groups; otherwise rows r + NC*rr, all columns)
@@ -159,20 +202,23 @@ __device__ __forceinline__ void stream_reduce(ACC* red, int b, int r, int g, int
     }
 }
 
-// CW consumer warps; `stages` stages of `stage_bytes` bytes each
-template <typename TL, typename TU, typename TX, typename ACC, bool FORWARD, int CW>
+// CW consumer warps; `stages` stages of `stage_bytes` bytes each.  MV: the
+// backward sweep also runs the matvec rows of F (tasks with entry -3).
+template <typename TL, typename TU, typename TX, typename ACC, bool FORWARD, int CW, typename TA = double, bool MV = false>
 __global__ void __launch_bounds__(32 * CW + 32)
     k_ilu_stream(IluRows R, const TL* __restrict__ LD, const TU* __restrict__ Aval, StreamTasks T, int ntasks,
                  const TX* __restrict__ v, TX* __restrict__ zx, ACC* __restrict__ part, SweepSync S, int nstage,
-                 int stage_bytes, int max_b) {
+                 int stage_bytes, int max_b, FusedMv<TA, TX> F) {
     constexpr int NC = 32 * CW;                  // consumer threads
     static_assert(NC <= SS_MAX_NC, "row-sum scratch");
+    static_assert(!(MV && FORWARD), "matvec rows run in the backward sweep");
     constexpr int RPT = (SS_MAX_B + NC - 1) / NC;
     extern __shared__ __align__(128) unsigned char ss_smem[];
     unsigned char* stages = ss_smem;
     ACC* xs = reinterpret_cast<ACC*>(ss_smem + (size_t)nstage * stage_bytes);
     ACC* red = xs + stream_xcap(max_b);          // G*b <= NC row sums
-    uint64_t* full = reinterpret_cast<uint64_t*>(red + NC);
+    double* scratch = reinterpret_cast<double*>(red + NC);   // 32 doubles
+    uint64_t* full = reinterpret_cast<uint64_t*>(scratch + 32);
     uint64_t* empty = full + SS_MAX_STAGES;
     StreamMeta* meta = reinterpret_cast<StreamMeta*>(empty + SS_MAX_STAGES);
     __shared__ int s_last;
@@ -202,10 +248,17 @@ __global__ void __launch_bounds__(32 * CW + 32)
                 return;
             }
             const int pr = T.task_row[t], q = T.task_ent[t];
-            const int b = R.prow_b[pr];
+            int b = R.prow_b[pr];
             const unsigned char* base = nullptr;
             int cols = 0, esz = 1;
-            if (q >= 0) {
+            if (MV && q == -3) {
+                // matvec row pr: the row's blocks, one b x cols strip
+                const int64_t k0 = F.rows.row_ptr[pr], k1 = F.rows.row_ptr[pr + 1];
+                b = F.rows.row_b[pr];
+                for (int64_t k = k0; k < k1; ++k) cols += F.rows.blk_nc[k];
+                base = reinterpret_cast<const unsigned char*>(F.val + (k1 > k0 ? F.rows.blk_voff[k0] : 0));
+                esz = sizeof(TA);
+            } else if (q >= 0) {
                 if (FORWARD) { base = reinterpret_cast<const unsigned char*>(LD + R.lo_L[q]); cols = R.lo_nc[q]; esz = sizeof(TL); }
                 else { base = reinterpret_cast<const unsigned char*>(Aval + R.up_U[q]); cols = R.up_nc[q]; esz = sizeof(TU); }
             } else if (q == -2) {
@@ -253,12 +306,27 @@ __global__ void __launch_bounds__(32 * CW + 32)
         if (m.chunk == 0) {
             pr = m.pr;
             q = m.q;
-            b = R.prow_b[pr];
+            b = (MV && q == -3) ? F.rows.row_b[pr] : R.prow_b[pr];
             if (b <= NC) { G = NC / b; r = ctid % b; g = ctid / b; }
             else { G = 1; r = ctid; g = 0; }
             #pragma unroll
             for (int rr = 0; rr < RPT; ++rr) acc[rr] = 0;
-            if (q >= 0) {
+            if (MV && q == -3) {
+                // every column segment of the row published by the sweep, then staged
+                const int64_t k0 = F.rows.row_ptr[pr], k1 = F.rows.row_ptr[pr + 1];
+                if (ctid == 0)
+                    for (int64_t k = k0; k < k1; ++k)
+                        if (!wait_flag(S.flags, F.col_prow[k], S.epoch, S.spin_limit)) atomicExch(S.status, 1);
+                consumers_sync<NC>();
+                int off = 0;
+                for (int64_t k = k0; k < k1; ++k) {
+                    const int nc = F.rows.blk_nc[k];
+                    const TX* xp = zx + F.rows.blk_xoff[k];
+                    for (int c = ctid; c < nc; c += NC) xs[off + c] = cvt<ACC>(ld_cg(xp + c));
+                    off += nc;
+                }
+                consumers_sync<NC>();
+            } else if (q >= 0) {
                 const int par = FORWARD ? R.lo_par[q] : R.up_par[q];
                 const int nc = FORWARD ? R.lo_nc[q] : R.up_nc[q];
                 if (ctid == 0 && !wait_flag(S.flags, par, S.epoch, S.spin_limit)) atomicExch(S.status, 1);
@@ -286,7 +354,9 @@ __global__ void __launch_bounds__(32 * CW + 32)
         }
         if (m.ncols > 0) {
             const unsigned char* sb = stages + (size_t)stage * stage_bytes;
-            if (FORWARD || q == -2)
+            if (MV && q == -3)
+                stream_chunk<NC, RPT, TA, ACC>(reinterpret_cast<const TA*>(sb) + m.shift, xs + m.col0, b, m.ncols, r, g, G, acc);
+            else if (FORWARD || q == -2)
                 stream_chunk<NC, RPT, TL, ACC>(reinterpret_cast<const TL*>(sb) + m.shift, xs + m.col0, b, m.ncols, r, g, G, acc);
             else
                 stream_chunk<NC, RPT, TU, ACC>(reinterpret_cast<const TU*>(sb) + m.shift, xs + m.col0, b, m.ncols, r, g, G, acc);
@@ -298,6 +368,27 @@ __global__ void __launch_bounds__(32 * CW + 32)
 
         // ------------------------------------------------ the task's last chunk
         stream_reduce<NC, RPT>(red, b, r, g, G, ctid, acc);
+        if (MV && q == -3) {
+            // y_r = A_r z and its sum of squares, as the streamed matvec writes them
+            double sq = 0.0;
+            const int64_t yo = F.rows.row_yoff[pr];
+            #pragma unroll
+            for (int rr = 0; rr < RPT; ++rr) {
+                const int i = (b <= NC) ? (rr == 0 ? ctid : b) : ctid + NC * rr;
+                if (i < b) {
+                    const TX o = from_d<TX>((double)acc[rr]);
+                    F.y[yo + i] = o;
+                    const double od = to_d(o);
+                    sq += od * od;
+                }
+            }
+            if (F.row_sumsq != nullptr) {
+                const double s2 = consumers_sum<NC>(sq, scratch, ctid);
+                if (ctid == 0) F.row_sumsq[pr] = s2;
+            }
+            consumers_sync<NC>();        // xs, red and scratch are reused by the next task
+            continue;
+        }
         if (q == -2) {
             // x_r = inv(D_r) t_r: the row is complete
             if (b <= NC) { if (ctid < b) zx[R.z_off[pr] + ctid] = from_d<TX>((double)acc[0]); }

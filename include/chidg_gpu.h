@@ -154,8 +154,10 @@ int chidg_gpu_launch_count(chidg_gpu_ctx* ctx, int64_t* count);
  * default; switching resets the totals).  Classes: 0 FP64 matvec, 1 ILU
  * forward sweep, 2 ILU backward sweep (FP64), 3 factorisation (whole
  * precon update), 4 FP32 matvec, 5 low-precision ILU apply, 6 and 7 the
- * GEMM and inverse launches of one factorisation level.  One count is one
- * matvec launch, one full sweep, one factorisation, or one level. */
+ * GEMM and inverse launches of one factorisation level, 8 the FP64 backward
+ * sweep with FGMRES's following matvec (w = A z) run in the same launch.
+ * One count is one matvec launch, one full sweep, one factorisation, or one
+ * level. */
 int chidg_gpu_ctx_set_profiling(chidg_gpu_ctx* ctx, int32_t on);
 int chidg_gpu_ctx_kernel_time(chidg_gpu_ctx* ctx, int32_t kernel_class, double* total_ms, int64_t* count);
 /* Page-locked host memory for the upload / download calls. */
