@@ -7,31 +7,37 @@
 // process exactly as fgmres_t%solve runs it (type_fgmres.f90:81-310): its own
 // dot products, selective re-orthogonalisation, Givens rotations, convergence
 // test and solution update.  Systems advance in lockstep through the Krylov
-// index j; a converged system is frozen (its coefficients become zero) while
-// the others continue, and all systems restart together at j = nkrylov.
+// index j; a converged system is frozen while the others continue, and all
+// systems restart together at j = nkrylov.
+//
+// The Arnoldi bookkeeping runs on the device in FP64, one thread per system
+// (k_bat_*): the re-orthogonalisation test (:203-223), the Givens rotations
+// with hypot (:234-270), the convergence tests (:272-280) and the least
+// squares y = inv(H) p (:287-288, mod_inv::inv semantics).  The second
+// Gram-Schmidt pass is always launched and skips the systems that do not need
+// it, so one Arnoldi step is a fixed sequence of launches with no host
+// synchronisation; the host only reads the count of active systems, without
+// waiting for it, to stop early, and synchronises once per restart cycle.
+//
+// A batch solved again with the same structure (the Newton steps of the same
+// set of systems: new values, same pattern and buffers) replays each Arnoldi
+// step and the cycle boundaries from CUDA graphs captured on the second call.
 #include "chidg_gpu_internal.cuh"
 
 #include <algorithm>
 #include <cfloat>
 #include <chrono>
+#include <cstdlib>
 #include <cstring>
+#include <functional>
+#include <memory>
 
 using namespace chidg;
 
 namespace {
 
 constexpr int64_t kChunk = 2048;
-
-// the segment layout of one batched call; its device buffers belong to the
-// context and are reused by the next call
-struct Seg {
-    int nsys = 0, nchunk = 0;
-    Buffer &cstart, &csys, &sys_chunk, &sys_row, &d_out, &d_coef, &d_scale, &partial, &rowsq;
-    std::vector<int32_t> h_sys_chunk;
-    explicit Seg(BatchBuffers& b)
-        : cstart(b.cstart), csys(b.csys), sys_chunk(b.sys_chunk), sys_row(b.sys_row), d_out(b.d_out), d_coef(b.d_coef),
-          d_scale(b.d_scale), partial(b.partial), rowsq(b.rowsq) {}
-};
+constexpr int kSysThreads = 64;
 
 template <typename T>
 int upload_vec(chidg_gpu_ctx* ctx, Buffer& b, const std::vector<T>& v) {
@@ -44,52 +50,282 @@ int upload_vec(chidg_gpu_ctx* ctx, Buffer& b, const std::vector<T>& v) {
     return CHIDG_GPU_OK;
 }
 
-// Explicit inverse with partial pivoting of a small dense matrix (the
-// Hessenberg least squares, mod_inv::inv semantics).
-int small_inverse(int n, std::vector<double>& a) {
-    std::vector<int> piv(n), used(n, 0);
+// Per-system Arnoldi state in device memory (one array per field).
+struct BatState {
+    int32_t *active, *member, *reo, *fin, *niter, *nrestart, *nvecs, *nhist, *err;   // nsys each
+    int32_t* count;           // [0] active systems, [1] error flag (1 + system of the first error)
+    double *r0init, *res, *res_est, *nb, *wn, *wn2, *scale;                         // nsys each
+    double *p, *c, *sn;       // nsys x (m + 1)
+    double* H;                // nsys x (m + 1) x m, column-major per system
+    double* work;             // nsys x m x m (least-squares inverse)
+    int32_t* piv;             // nsys x 2m
+    double* hist;             // nsys x hcap
+    double* coef;             // nsys x hst: h of pass 1, then the solution coefficients y
+    double* coef2;            // nsys x hst: h of pass 2
+};
+
+struct BatOpts {
+    int m, hst, hcap, nmax;
+    double tol, rtol;
+};
+
+// ---- device epilogue, one thread per system ------------------------------------
+__global__ void k_bat_cycle_start(BatState S, BatOpts o, int nsys, const double* __restrict__ r0sq) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsys) return;
+    const int m = o.m;
+    double* p = S.p + (size_t)s * (m + 1);
+    double* c = S.c + (size_t)s * (m + 1);
+    double* sn = S.sn + (size_t)s * (m + 1);
+    double* H = S.H + (size_t)s * (m + 1) * m;
+    for (int i = 0; i <= m; ++i) { p[i] = 0.0; c[i] = 0.0; sn[i] = 0.0; }
+    for (int i = 0; i < (m + 1) * m; ++i) H[i] = 0.0;
+    S.scale[s] = 0.0;
+    S.fin[s] = 0;
+    S.member[s] = 0;
+    if (!S.active[s]) return;
+    const double r0n = sqrt(r0sq[s]);
+    if (!isfinite(r0n)) {
+        S.err[s] = CHIDG_GPU_ENONFINITE;
+        atomicCAS(S.count + 1, 0, s + 1);
+        S.active[s] = 0;
+        return;
+    }
+    if (S.niter[s] == 0) S.r0init[s] = r0n;
+    if (r0n == 0.0) {             // zero right-hand side: x = 0
+        S.active[s] = 0;
+        S.res_est[s] = 0.0;
+        return;
+    }
+    p[0] = r0n;
+    S.scale[s] = 1.0 / r0n;
+    S.nvecs[s] = 0;
+    S.member[s] = 1;
+}
+
+// selective re-orthogonalisation test (type_fgmres.f90:203-223): pass 1's h and
+// ||A z|| decide whether the system takes a second Gram-Schmidt pass
+__global__ void k_bat_reorth_test(BatState S, BatOpts o, int nsys, int j) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsys) return;
+    S.reo[s] = 0;
+    if (!S.active[s]) return;
+    const double nb = sqrt(S.nb[s]);
+    if (!isfinite(nb)) {
+        S.err[s] = CHIDG_GPU_ENONFINITE;
+        atomicCAS(S.count + 1, 0, s + 1);
+        S.active[s] = 0;
+        return;
+    }
+    const double* h1 = S.coef + (size_t)s * o.hst;
+    double crit = 0.0;
+    for (int i = 0; i < j; ++i) crit += fabs(h1[i]);
+    crit /= nb;
+    S.reo[s] = crit >= 1.0;
+}
+
+// y = inv(H(1:n,1:n)) p(1:n) into coef (type_fgmres.f90:287-288)
+__device__ int bat_least_squares(BatState& S, const BatOpts& o, int s, int n) {
+    const int m = o.m;
+    const double* H = S.H + (size_t)s * (m + 1) * m;
+    double* a = S.work + (size_t)s * m * m;
+    int32_t* piv = S.piv + (size_t)s * 2 * m;
+    int32_t* used = piv + m;
+    // Gauss-Jordan with partial pivoting on a copy of H (mod_inv::inv
+    // semantics, as the host solver's explicit inverse): row p is the pivot
+    // row of column k; rows are never swapped, the permutation is undone below
+    for (int jj = 0; jj < n; ++jj)
+        for (int ii = 0; ii < n; ++ii) a[ii + jj * n] = H[ii + jj * (m + 1)];
+    for (int i = 0; i < n; ++i) used[i] = 0;
     for (int k = 0; k < n; ++k) {
         int p = -1;
         double best = -1.0;
         for (int i = 0; i < n; ++i) {
             if (used[i]) continue;
-            double v = std::fabs(a[i + (size_t)k * n]);
+            double v = fabs(a[i + k * n]);
             if (!(v == v)) v = INFINITY;
             if (v > best) { best = v; p = i; }
         }
         piv[k] = p;
         used[p] = 1;
-        const double pv = a[p + (size_t)k * n];
+        const double pv = a[p + k * n];
         if (pv == 0.0) return k + 1;
         const double rp = 1.0 / pv;
-        std::vector<double> row(n), col(n);
-        for (int j = 0; j < n; ++j) row[j] = ((j == k) ? 1.0 : a[p + (size_t)j * n]) * rp;
-        for (int i = 0; i < n; ++i) col[i] = (i == p) ? 0.0 : a[i + (size_t)k * n];
-        for (int j = 0; j < n; ++j)
+        for (int jj = 0; jj < n; ++jj) {
+            const double row = ((jj == k) ? 1.0 : a[p + jj * n]) * rp;
+            if (jj == k) continue;
             for (int i = 0; i < n; ++i) {
-                if (i == p) a[i + (size_t)j * n] = row[j];
-                else {
-                    const double base = (j == k) ? 0.0 : a[i + (size_t)j * n];
-                    a[i + (size_t)j * n] = base - col[i] * row[j];
-                }
+                if (i == p) continue;
+                a[i + jj * n] = a[i + jj * n] - a[i + k * n] * row;
             }
+        }
+        // column k: -col * row(k) with row(k) = rp, rows i != p
+        for (int i = 0; i < n; ++i)
+            if (i != p) a[i + k * n] = 0.0 - a[i + k * n] * rp;
+        for (int jj = 0; jj < n; ++jj) a[p + jj * n] = ((jj == k) ? 1.0 : a[p + jj * n]) * rp;
     }
-    std::vector<int> q(n);
+    // inverse(q[i], piv[jj]) = a(i, jj) with q = piv^-1, so inverse row ii is
+    // a's row piv[ii] and inverse column col is a's column q[col]; y = inverse p
+    // summed over the columns in order
+    int32_t* q = used;
     for (int k = 0; k < n; ++k) q[piv[k]] = k;
-    std::vector<double> out((size_t)n * n);
-    for (int j = 0; j < n; ++j)
-        for (int i = 0; i < n; ++i) out[q[i] + (size_t)piv[j] * n] = a[i + (size_t)j * n];
-    a.swap(out);
+    const double* pp = S.p + (size_t)s * (m + 1);
+    double* y = S.coef + (size_t)s * o.hst;
+    for (int ii = 0; ii < n; ++ii) {
+        const int i = piv[ii];
+        double acc = 0.0;
+        for (int col = 0; col < n; ++col) acc += a[i + q[col] * n] * pp[col];
+        y[ii] = acc;
+    }
+    for (int ii = n; ii < o.hst; ++ii) y[ii] = 0.0;
     return 0;
 }
 
-struct SysState {
-    bool active = true;
-    int niter = 0, nrestart = 0, nvecs = 0;
-    double r0norm_initial = 0.0, res = DBL_MAX, res_est = 0.0, residual_norm = 0.0;
-    std::vector<double> p, c, s, h;
-    std::vector<double> hist;
+// h(:, j) from the passes, Givens rotations, the convergence tests and, for a
+// system that converges now, its least squares (the step's x update)
+__global__ void k_bat_givens(BatState S, BatOpts o, int nsys, int j) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsys) return;
+    S.fin[s] = 0;
+    if (!S.active[s]) { S.scale[s] = 0.0; return; }
+    const int m = o.m;
+    double* H = S.H + (size_t)s * (m + 1) * m;
+    double* p = S.p + (size_t)s * (m + 1);
+    double* c = S.c + (size_t)s * (m + 1);
+    double* sn = S.sn + (size_t)s * (m + 1);
+    auto h = [&](int i, int jj) -> double& { return H[(size_t)i + (size_t)jj * (m + 1)]; };
+    const double* h1 = S.coef + (size_t)s * o.hst;
+    const double* h2 = S.coef2 + (size_t)s * o.hst;
+    const bool reo = S.reo[s] != 0;
+    for (int i = 0; i < j; ++i) {
+        double v = 0.0;
+        v += h1[i];
+        if (reo) v += h2[i];
+        h(i, j - 1) = v;
+    }
+    h(j, j - 1) = sqrt(reo ? S.wn2[s] : S.wn[s]);
+    const double inv_h = 1.0 / h(j, j - 1);
+    for (int i = 0; i < j - 1; ++i) {
+        const double hij = c[i] * h(i, j - 1) + sn[i] * h(i + 1, j - 1);
+        const double hipj = -sn[i] * h(i, j - 1) + c[i] * h(i + 1, j - 1);
+        h(i, j - 1) = hij;
+        h(i + 1, j - 1) = hipj;
+    }
+    const double gam = hypot(h(j - 1, j - 1), h(j, j - 1));
+    c[j - 1] = h(j - 1, j - 1) / gam;
+    sn[j - 1] = h(j, j - 1) / gam;
+    h(j - 1, j - 1) = gam;
+    h(j, j - 1) = 0.0;
+    const double pj = c[j - 1] * p[j - 1];
+    const double pjp = -sn[j - 1] * p[j - 1];
+    p[j - 1] = pj;
+    p[j] = pjp;
+    const int it = ++S.niter[s];
+    S.nvecs[s] = j;
+    const double res = fabs(p[j]);
+    S.res[s] = res;
+    if (it - 1 < o.hcap) S.hist[(size_t)s * o.hcap + it - 1] = res;
+    S.nhist[s] = min(it, o.hcap);
+    const bool cabs = res < o.tol;
+    const bool crel = res / S.r0init[s] < o.rtol;
+    const bool cmax = (it >= o.nmax) && (o.nmax > 0);
+    S.scale[s] = inv_h;
+    if (cabs || crel || cmax) {
+        if (bat_least_squares(S, o, s, j) != 0) {
+            S.err[s] = CHIDG_GPU_ESINGULAR;
+            atomicCAS(S.count + 1, 0, s + 1);
+        }
+        S.res_est[s] = res;
+        S.active[s] = 0;
+        S.fin[s] = 1;
+        S.scale[s] = 0.0;
+    }
+}
+
+// end of a full cycle: least squares of the systems still active (restart)
+__global__ void k_bat_cycle_end(BatState S, BatOpts o, int nsys) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsys) return;
+    S.fin[s] = 0;
+    if (!S.active[s] || !S.member[s]) return;
+    if (bat_least_squares(S, o, s, S.nvecs[s]) != 0) {
+        S.err[s] = CHIDG_GPU_ESINGULAR;
+        atomicCAS(S.count + 1, 0, s + 1);
+        S.active[s] = 0;
+    }
+    S.res_est[s] = S.res[s];
+    S.nrestart[s]++;
+    S.fin[s] = 1;
+}
+
+// a new solve: every system active
+__global__ void k_bat_reset(BatState S, int nsys) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < nsys) S.active[s] = 1;
+}
+
+// count[0] = number of active systems
+__global__ void k_bat_count(BatState S, int nsys) {
+    __shared__ int tot;
+    if (threadIdx.x == 0) tot = 0;
+    __syncthreads();
+    int a = 0;
+    for (int s = threadIdx.x; s < nsys; s += blockDim.x) a += S.active[s];
+    atomicAdd(&tot, a);
+    __syncthreads();
+    if (threadIdx.x == 0) S.count[0] = tot;
+}
+
+// a graph of one piece of the batched solve, captured on the context's stream
+struct GraphPiece {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t x = nullptr;
+    ~GraphPiece() {
+        if (x) cudaGraphExecDestroy(x);
+        if (g) cudaGraphDestroy(g);
+    }
 };
+
+}  // namespace
+
+// Captured graphs of a batch structure, kept by the context for the next call
+// with the same key (matrix, preconditioner, systems, options and buffers).
+struct BatchGraphs {
+    std::vector<int64_t> key;
+    int seen = 0;                                   // calls with this key so far
+    std::unique_ptr<GraphPiece> start, end;         // cycle start (r0, scale), cycle end (restart update)
+    std::vector<std::unique_ptr<GraphPiece>> step;  // Arnoldi step j = 1..m
+};
+
+void chidg::release_batch_graphs(chidg_gpu_ctx* ctx) {
+    delete ctx->batch_graphs;
+    ctx->batch_graphs = nullptr;
+}
+
+namespace {
+
+// CHIDG_BATCH_GRAPHS=0 keeps every batched solve on eager launches
+bool graphs_enabled() {
+    static const bool v = [] {
+        const char* e = std::getenv("CHIDG_BATCH_GRAPHS");
+        return !(e && e[0] == '0');
+    }();
+    return v;
+}
+
+int capture(chidg_gpu_ctx* ctx, GraphPiece& gp, const std::function<int()>& body) {
+    cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "batch graph capture");
+    const int st = body();
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(ctx->stream, &g);
+    if (st) { if (g) cudaGraphDestroy(g); return st; }
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "batch graph capture end");
+    gp.g = g;
+    e = cudaGraphInstantiate(&gp.x, g, 0);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "batch graph instantiate");
+    return CHIDG_GPU_OK;
+}
 
 }  // namespace
 
@@ -110,9 +346,10 @@ extern "C" int chidg_gpu_fgmres_solve_batched(chidg_gpu_matrix* A, chidg_gpu_pre
     // preconditioner with FP32 copies of its blocks
     if (o.precision != CHIDG_GPU_FP64 && o.precision != CHIDG_GPU_MIXED_PRECON_FP32)
         return fail(ctx, CHIDG_GPU_EINVAL, "batched fgmres: precision must be FP64 or MIXED_PRECON_FP32");
+    if (o.orthogonalization != CHIDG_ORTH_CGS) return fail(ctx, CHIDG_GPU_EINVAL, "batched fgmres: CGS only");
     const int prec = o.precision;
     const int m = o.nkrylov;
-    if (m < 1 || m > kMaxKrylov) return fail(ctx, CHIDG_GPU_EINVAL, "batched fgmres: nkrylov outside [1, 4000]");
+    if (m < 1 || m > 256) return fail(ctx, CHIDG_GPU_EINVAL, "batched fgmres: nkrylov outside [1, 256]");
     // segments: systems must tile the elements and not couple to each other
     if (sys_elem[0] != 0 || sys_elem[nsys] != A->nelem) return fail(ctx, CHIDG_GPU_EINVAL, "batched fgmres: systems must cover all elements");
     std::vector<int> elem_sys(A->nelem);
@@ -122,8 +359,7 @@ extern "C" int chidg_gpu_fgmres_solve_batched(chidg_gpu_matrix* A, chidg_gpu_pre
     }
     for (int64_t k = 0; k < A->nblk; ++k)
         if (elem_sys[A->re[k]] != elem_sys[A->ce[k]]) return fail(ctx, CHIDG_GPU_EINVAL, "batched fgmres: a block couples two systems");
-    Seg G(ctx->batch);
-    G.nsys = nsys;
+    BatchBuffers& BB = ctx->batch;
     std::vector<int64_t> cstart;
     std::vector<int32_t> csys, sys_chunk(nsys + 1), sys_row(nsys + 1);
     for (int s = 0; s < nsys; ++s) {
@@ -136,27 +372,54 @@ extern "C" int chidg_gpu_fgmres_solve_batched(chidg_gpu_matrix* A, chidg_gpu_pre
     sys_chunk[nsys] = (int32_t)csys.size();
     sys_row[nsys] = A->nrow;
     cstart.push_back(A->n);
-    G.nchunk = (int)csys.size();
+    const int nchunk = (int)csys.size();
     int st;
-    if ((st = upload_vec(ctx, G.cstart, cstart)) || (st = upload_vec(ctx, G.csys, csys)) ||
-        (st = upload_vec(ctx, G.sys_chunk, sys_chunk)) || (st = upload_vec(ctx, G.sys_row, sys_row)))
+    const int hst = m + 2;                 // per-system stride of the coefficient rows
+    const int hcap = std::max(1, std::min(hist_cap > 0 ? hist_cap : 1, 8192));
+    // device state: ints then doubles, in one buffer kept by the context
+    const size_t ni = (size_t)nsys * 9 + 2 + (size_t)nsys * 2 * m;
+    const size_t nd = (size_t)nsys * 7 + (size_t)nsys * (m + 1) * 3 + (size_t)nsys * (m + 1) * m + (size_t)nsys * m * m +
+                      (size_t)nsys * hcap + (size_t)nsys * hst * 2;
+    const size_t ibytes = ((sizeof(int32_t) * ni + 255) / 256) * 256;
+    if ((st = upload_vec(ctx, BB.cstart, cstart)) || (st = upload_vec(ctx, BB.csys, csys)) ||
+        (st = upload_vec(ctx, BB.sys_chunk, sys_chunk)) || (st = upload_vec(ctx, BB.sys_row, sys_row)) ||
+        (st = ensure(ctx, BB.state, ibytes + sizeof(double) * nd)) ||
+        (st = ensure(ctx, BB.partial, sizeof(double) * (size_t)nchunk * std::max(m, 1))) ||
+        (st = ensure(ctx, BB.rowsq, sizeof(double) * (size_t)A->nrow)) ||
+        (st = ensure(ctx, BB.out, sizeof(double) * (size_t)nsys)))
         return st;
-    const int hst = m + 2;   // per-system stride of the device output / coefficient rows
-    if ((st = ensure(ctx, G.d_out, sizeof(double) * (size_t)nsys * hst)) ||
-        (st = ensure(ctx, G.d_coef, sizeof(double) * (size_t)nsys * hst)) ||
-        (st = ensure(ctx, G.d_scale, sizeof(double) * (size_t)nsys)) ||
-        (st = ensure(ctx, G.partial, sizeof(double) * (size_t)G.nchunk * std::max(m, 1))) ||
-        (st = ensure(ctx, G.rowsq, sizeof(double) * (size_t)A->nrow)))
-        return st;
-    const int64_t* CS = (const int64_t*)G.cstart.ptr;
-    const int32_t* CY = (const int32_t*)G.csys.ptr;
-    const int32_t* SC = (const int32_t*)G.sys_chunk.ptr;
-    const int32_t* SR = (const int32_t*)G.sys_row.ptr;
-    double* OUT = (double*)G.d_out.ptr;
-    double* COEF = (double*)G.d_coef.ptr;
-    double* SCALE = (double*)G.d_scale.ptr;
-    double* PART = (double*)G.partial.ptr;
-    double* ROWSQ = (double*)G.rowsq.ptr;
+    if (!BB.h_count) {
+        if (cudaHostAlloc((void**)&BB.h_count, 4 * sizeof(int32_t), cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(ctx, CHIDG_GPU_ENOMEM, "batched fgmres: pinned counter");
+        }
+        for (int i = 0; i < 2; ++i)
+            if (cudaEventCreateWithFlags(&BB.ev[i], cudaEventDisableTiming) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(ctx, CHIDG_GPU_ECUDA, "batched fgmres: events");
+            }
+    }
+    BatState S{};
+    {
+        int32_t* ip = (int32_t*)BB.state.ptr;
+        S.active = ip; S.member = ip + nsys; S.reo = ip + 2 * nsys; S.fin = ip + 3 * nsys; S.niter = ip + 4 * nsys;
+        S.nrestart = ip + 5 * nsys; S.nvecs = ip + 6 * nsys; S.nhist = ip + 7 * nsys; S.err = ip + 8 * nsys;
+        S.count = ip + 9 * nsys;
+        S.piv = ip + 9 * nsys + 2;
+        double* dp = (double*)((unsigned char*)BB.state.ptr + ibytes);
+        S.r0init = dp; S.res = dp + nsys; S.res_est = dp + 2 * nsys; S.nb = dp + 3 * nsys; S.wn = dp + 4 * nsys;
+        S.wn2 = dp + 5 * nsys; S.scale = dp + 6 * nsys;
+        dp += 7 * (size_t)nsys;
+        S.p = dp; dp += (size_t)nsys * (m + 1);
+        S.c = dp; dp += (size_t)nsys * (m + 1);
+        S.sn = dp; dp += (size_t)nsys * (m + 1);
+        S.H = dp; dp += (size_t)nsys * (m + 1) * m;
+        S.work = dp; dp += (size_t)nsys * m * m;
+        S.hist = dp; dp += (size_t)nsys * hcap;
+        S.coef = dp; dp += (size_t)nsys * hst;
+        S.coef2 = dp;
+    }
+    const BatOpts bo{m, hst, hcap, o.nmax, o.tol, o.rtol};
 
     // M%update as the controller decides (type_fgmres.f90:118-122)
     if (!(o.use_controller && M->stamp == A->stamp && M->precision == prec))
@@ -174,218 +437,211 @@ extern "C" int chidg_gpu_fgmres_solve_batched(chidg_gpu_matrix* A, chidg_gpu_pre
     Buffer& Z = ctx->ws64.Z;
     Buffer& X0 = ctx->ws64.x0;
     Buffer& TMP = ctx->ws64.tmp;
-    auto cleanup = [&]() {};
     if ((st = ensure(ctx, V, sizeof(double) * (size_t)(m + 1) * n)) || (st = ensure(ctx, Z, sizeof(double) * (size_t)(m + 1) * n)) ||
-        (st = ensure(ctx, X0, sizeof(double) * (size_t)n)) || (st = ensure(ctx, TMP, sizeof(double) * (size_t)n))) {
-        cleanup();
+        (st = ensure(ctx, X0, sizeof(double) * (size_t)n)) || (st = ensure(ctx, TMP, sizeof(double) * (size_t)n)))
         return st;
-    }
     double* Vb = (double*)V.ptr;
     double* Zb = (double*)Z.ptr;
     double* x0 = (double*)X0.ptr;
     double* xx = (double*)x->buf.ptr;
     const double* bb = (const double*)b->buf.ptr;
+    const int64_t* CS = (const int64_t*)BB.cstart.ptr;
+    const int32_t* CY = (const int32_t*)BB.csys.ptr;
+    const int32_t* SC = (const int32_t*)BB.sys_chunk.ptr;
+    const int32_t* SR = (const int32_t*)BB.sys_row.ptr;
+    double* PART = (double*)BB.partial.ptr;
+    double* ROWSQ = (double*)BB.rowsq.ptr;
+    double* OUT = (double*)BB.out.ptr;
+    const int TH = 256;
+    const int sgrid = (nsys + kSysThreads - 1) / kSysThreads;
+    auto check = [&](const char* what) { return check_launch(ctx, what); };
+
+    // ---- the launch sequences ---------------------------------------------------
+    // cycle start: r0 = b - A x0 into V(1), per-system norms, v1 = r0 / ||r0||
+    auto seq_start = [&]() -> int {
+        int s2;
+        if ((s2 = matvec_launch<double, double>(A, (const double*)A->val.ptr, x0, Vb, bb, -1.0, 1.0, ROWSQ))) return s2;
+        k_seg_reduce<<<nsys, 32, 0, ctx->stream>>>(ROWSQ, A->nrow, SR, 1, OUT, 1);
+        if ((s2 = check("k_seg_reduce r0"))) return s2;
+        k_bat_cycle_start<<<sgrid, kSysThreads, 0, ctx->stream>>>(S, bo, nsys, OUT);
+        if ((s2 = check("k_bat_cycle_start"))) return s2;
+        k_seg_scale<double><<<nchunk, TH, 0, ctx->stream>>>(CS, CY, Vb, Vb, S.scale);
+        return check("k_seg_scale v1");
+    };
+    // one Arnoldi step j: z_j = M v_j, w = A z_j, two CGS passes (the second
+    // only for the systems the test selects), the epilogue, the solution of the
+    // systems that converged now, v(j+1) = w / h(j+1,j), the active count
+    auto seq_step = [&](int j) -> int {
+        int s2;
+        double* vj = Vb + (int64_t)(j - 1) * n;
+        double* zj = Zb + (int64_t)(j - 1) * n;
+        double* w = Vb + (int64_t)j * n;
+        s2 = precon_apply_mv<double, double>(M, vj, zj, prec, A, (const double*)A->val.ptr, w, ROWSQ);
+        if (s2 == 1) {
+            if ((s2 = precon_apply_impl<double>(M, vj, zj, prec)) ||
+                (s2 = matvec_launch<double, double>(A, (const double*)A->val.ptr, zj, w, nullptr, 1.0, 0.0, ROWSQ)))
+                return s2;
+        } else if (s2) {
+            return s2;
+        }
+        k_seg_reduce<<<nsys, 32, 0, ctx->stream>>>(ROWSQ, A->nrow, SR, 1, S.nb, 1);
+        k_seg_mdot<double><<<nchunk, TH, 0, ctx->stream>>>(CS, nchunk, w, Vb, n, j, PART);
+        k_seg_reduce<<<nsys, 128, 0, ctx->stream>>>(PART, nchunk, SC, j, S.coef, hst);
+        k_seg_maxpy<double><<<nchunk, TH, 0, ctx->stream>>>(CS, CY, w, Vb, n, j, S.coef, hst, PART);
+        k_seg_reduce<<<nsys, 32, 0, ctx->stream>>>(PART, nchunk, SC, 1, S.wn, 1);
+        k_bat_reorth_test<<<sgrid, kSysThreads, 0, ctx->stream>>>(S, bo, nsys, j);
+        k_seg_mdot<double><<<nchunk, TH, 0, ctx->stream>>>(CS, nchunk, w, Vb, n, j, PART, CY, S.reo);
+        k_seg_reduce<<<nsys, 128, 0, ctx->stream>>>(PART, nchunk, SC, j, S.coef2, hst, S.reo);
+        k_seg_maxpy<double><<<nchunk, TH, 0, ctx->stream>>>(CS, CY, w, Vb, n, j, S.coef2, hst, PART, S.reo);
+        k_seg_reduce<<<nsys, 32, 0, ctx->stream>>>(PART, nchunk, SC, 1, S.wn2, 1, S.reo);
+        k_bat_givens<<<sgrid, kSysThreads, 0, ctx->stream>>>(S, bo, nsys, j);
+        // x = x0 + sum y_i z_i and x0 likewise for the systems that converged now
+        k_seg_lincomb<double><<<nchunk, TH, 0, ctx->stream>>>(CS, CY, xx, x0, Zb, n, j, S.coef, hst, S.fin);
+        k_seg_lincomb<double><<<nchunk, TH, 0, ctx->stream>>>(CS, CY, x0, x0, Zb, n, j, S.coef, hst, S.fin);
+        k_seg_scale<double><<<nchunk, TH, 0, ctx->stream>>>(CS, CY, w, w, S.scale);
+        k_bat_count<<<1, 256, 0, ctx->stream>>>(S, nsys);
+        return check("batched Arnoldi step");
+    };
+    // cycle end: the systems still active update x and x0 with their m vectors
+    auto seq_end = [&]() -> int {
+        k_bat_cycle_end<<<sgrid, kSysThreads, 0, ctx->stream>>>(S, bo, nsys);
+        k_seg_lincomb<double><<<nchunk, TH, 0, ctx->stream>>>(CS, CY, xx, x0, Zb, n, m, S.coef, hst, S.fin);
+        k_seg_lincomb<double><<<nchunk, TH, 0, ctx->stream>>>(CS, CY, x0, x0, Zb, n, m, S.coef, hst, S.fin);
+        k_bat_count<<<1, 256, 0, ctx->stream>>>(S, nsys);
+        return check("batched cycle end");
+    };
+
+    // ---- graphs: captured on the second call with the same structure ------------
+    std::vector<int64_t> key = {A->uid, (int64_t)(intptr_t)M, (int64_t)M->kind, (int64_t)M->schedule, nsys, m, prec,
+                                o.nmax, (int64_t)(intptr_t)bb, (int64_t)(intptr_t)xx, (int64_t)(intptr_t)Vb,
+                                (int64_t)(intptr_t)Zb, (int64_t)(intptr_t)x0, (int64_t)(intptr_t)BB.state.ptr,
+                                (int64_t)(intptr_t)BB.partial.ptr, (int64_t)(intptr_t)BB.rowsq.ptr,
+                                (int64_t)(intptr_t)BB.cstart.ptr, hcap, (int64_t)M->P.nprow, M->P.ntask_bmv};
+    int64_t tolbits, rtolbits;
+    std::memcpy(&tolbits, &o.tol, 8);
+    std::memcpy(&rtolbits, &o.rtol, 8);
+    key.push_back(tolbits);
+    key.push_back(rtolbits);
+    key.insert(key.end(), sys_elem, sys_elem + nsys + 1);
+    if (!ctx->batch_graphs) ctx->batch_graphs = new BatchGraphs();
+    BatchGraphs& GR = *ctx->batch_graphs;
+    if (GR.key != key) {
+        GR.key = key;
+        GR.seen = 0;
+        GR.start.reset();
+        GR.end.reset();
+        GR.step.clear();
+    }
+    GR.seen++;
+    // graphs need the streamed sweeps' flags reset inside each replay; the
+    // preconditioner records that it runs in captured sequences
+    // only the streamed sweeps clear their flags inside a sequence
+    const bool sweeps_ok = M->kind == CHIDG_PRECON_IDENTITY ||
+                           (M->schedule == CHIDG_SCHED_STREAM && M->P.max_b <= SS_MAX_B);
+    const bool graphs = GR.seen >= 2 && !ctx->profiling && sweeps_ok && graphs_enabled();
+    if (graphs && !GR.start) {
+        M->graph_safe = true;
+        GR.start.reset(new GraphPiece());
+        GR.end.reset(new GraphPiece());
+        if ((st = capture(ctx, *GR.start, seq_start)) || (st = capture(ctx, *GR.end, seq_end))) {
+            M->graph_safe = false;
+            GR.start.reset();
+            GR.end.reset();
+            return st;
+        }
+        GR.step.resize(m);
+        for (int j = 1; j <= m; ++j) {
+            GR.step[j - 1].reset(new GraphPiece());
+            if ((st = capture(ctx, *GR.step[j - 1], [&]() { return seq_step(j); }))) {
+                M->graph_safe = false;
+                GR.start.reset();
+                GR.end.reset();
+                GR.step.clear();
+                return st;
+            }
+        }
+        M->graph_safe = false;
+    }
+    auto run = [&](GraphPiece* gp, const std::function<int()>& eager) -> int {
+        if (gp) {
+            const cudaError_t e = cudaGraphLaunch(gp->x, ctx->stream);
+            return e == cudaSuccess ? CHIDG_GPU_OK : cuda_fail(ctx, e, "batch graph launch");
+        }
+        return eager();
+    };
+    const bool use_graphs = graphs && GR.start;
+
+    // ---- solve --------------------------------------------------------------------
     cudaMemsetAsync(x0, 0, sizeof(double) * n, ctx->stream);
     cudaMemsetAsync(xx, 0, sizeof(double) * n, ctx->stream);
-
-    std::vector<SysState> S(nsys);
-    for (auto& q : S) {
-        q.p.assign(m + 1, 0.0); q.c.assign(m + 1, 0.0); q.s.assign(m + 1, 0.0);
-        q.h.assign((size_t)(m + 1) * m, 0.0);
-    }
-    std::vector<double> hout((size_t)nsys * hst), coef((size_t)nsys * hst), scale(nsys);
-    const int TH = 256;
-    auto check = [&](const char* what) { return check_launch(ctx, what); };
-    // per-system sums of squares of the rows just written by the matvec
-    auto rows_to_sys = [&](double* dst) {
-        k_seg_reduce<<<nsys, 32, 0, ctx->stream>>>(ROWSQ, A->nrow, SR, 1, dst, 1);
-        return check("k_seg_reduce rows");
-    };
-    auto fetch = [&](const double* dsrc, size_t count, double* hdst) -> int {
-        cudaError_t e = cudaMemcpyAsync(hdst, dsrc, sizeof(double) * count, cudaMemcpyDeviceToHost, ctx->stream);
+    cudaMemsetAsync(BB.state.ptr, 0, ibytes, ctx->stream);       // every int field, the counters included
+    k_bat_reset<<<sgrid, kSysThreads, 0, ctx->stream>>>(S, nsys);
+    if ((st = check("k_bat_reset"))) return st;
+    int32_t* hc = BB.h_count;
+    for (;;) {
+        if ((st = run(use_graphs ? GR.start.get() : nullptr, seq_start))) return st;
+        bool all_done = false;
+        int j = 1;
+        for (; j <= m; ++j) {
+            if ((st = run(use_graphs ? GR.step[j - 1].get() : nullptr, [&]() { return seq_step(j); }))) return st;
+            // the active count of this step, read without waiting; the previous
+            // step's count (if it has landed) ends the cycle early
+            const int slot = j & 1;
+            cudaMemcpyAsync(hc + slot, S.count, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream);
+            cudaEventRecord(BB.ev[slot], ctx->stream);
+            if (j >= 2 && cudaEventQuery(BB.ev[slot ^ 1]) == cudaSuccess && hc[slot ^ 1] == 0) { all_done = true; break; }
+        }
+        if (!all_done) {
+            if ((st = run(use_graphs ? GR.end.get() : nullptr, seq_end))) return st;
+        }
+        int32_t cnt[2] = {0, 0};
+        cudaError_t e = cudaMemcpyAsync(cnt, S.count, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-        return e == cudaSuccess ? CHIDG_GPU_OK : cuda_fail(ctx, e, "batched fgmres scalars");
-    };
-    auto push = [&](double* ddst, const double* hsrc, size_t count) -> int {
-        const cudaError_t e = cudaMemcpyAsync(ddst, hsrc, sizeof(double) * count, cudaMemcpyHostToDevice, ctx->stream);
-        if (e == cudaSuccess) return cudaStreamSynchronize(ctx->stream) == cudaSuccess ? CHIDG_GPU_OK : CHIDG_GPU_ECUDA;
-        return cuda_fail(ctx, e, "batched fgmres coefficients");
-    };
-    // x (and x0) += sum_q coef[s][q] z_q for the systems with nonzero rows of coef
-    auto update_solution = [&](int nq) -> int {
-        if ((st = push(COEF, coef.data(), coef.size()))) return st;
-        k_seg_lincomb<double><<<G.nchunk, TH, 0, ctx->stream>>>(CS, CY, xx, x0, Zb, n, nq, COEF, hst);
-        if ((st = check("k_seg_lincomb x"))) return st;
-        k_seg_lincomb<double><<<G.nchunk, TH, 0, ctx->stream>>>(CS, CY, x0, x0, Zb, n, nq, COEF, hst);
-        return check("k_seg_lincomb x0");
-    };
-    auto solve_ls = [&](SysState& q, int nv, double* y) -> int {
-        std::vector<double> Hn((size_t)nv * nv);
-        for (int jj = 0; jj < nv; ++jj)
-            for (int ii = 0; ii < nv; ++ii) Hn[ii + (size_t)jj * nv] = q.h[ii + (size_t)jj * (m + 1)];
-        if (small_inverse(nv, Hn) != 0) return fail(ctx, CHIDG_GPU_ESINGULAR, "batched fgmres: singular Hessenberg matrix");
-        for (int ii = 0; ii < nv; ++ii) {
-            double acc = 0.0;
-            for (int jj = 0; jj < nv; ++jj) acc += Hn[ii + (size_t)jj * nv] * q.p[jj];
-            y[ii] = acc;
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "batched fgmres");
+        if (cnt[1] != 0) {
+            int32_t code = 0;
+            cudaMemcpy(&code, S.err + (cnt[1] - 1), sizeof(int32_t), cudaMemcpyDeviceToHost);
+            ctx->err_elem = sys_elem[cnt[1] - 1];
+            return fail(ctx, code ? code : CHIDG_GPU_ENONFINITE,
+                        code == CHIDG_GPU_ESINGULAR ? "batched fgmres: singular Hessenberg matrix"
+                                                    : "batched fgmres: non-finite residual");
         }
-        return CHIDG_GPU_OK;
-    };
-
-    int nactive = nsys;
-    while (nactive > 0) {
-        // r0 = b - A x0 into V(1), per-system norms
-        if ((st = matvec_launch<double, double>(A, (const double*)A->val.ptr, x0, Vb, bb, -1.0, 1.0, ROWSQ)) ||
-            (st = rows_to_sys(OUT)) || (st = fetch(OUT, nsys, hout.data()))) { cleanup(); return st; }
-        for (int s = 0; s < nsys; ++s) {
-            SysState& q = S[s];
-            std::fill(q.p.begin(), q.p.end(), 0.0); std::fill(q.c.begin(), q.c.end(), 0.0);
-            std::fill(q.s.begin(), q.s.end(), 0.0); std::fill(q.h.begin(), q.h.end(), 0.0);
-            scale[s] = 0.0;
-            if (!q.active) continue;
-            const double r0n = std::sqrt(hout[s]);
-            if (!std::isfinite(r0n)) { cleanup(); ctx->err_elem = sys_elem[s]; return fail(ctx, CHIDG_GPU_ENONFINITE, "batched fgmres: non-finite initial residual"); }
-            if (q.niter == 0) q.r0norm_initial = r0n;
-            if (r0n == 0.0) { q.active = false; nactive--; q.res_est = 0.0; continue; }   // zero right-hand side: x = 0
-            q.p[0] = r0n;
-            scale[s] = 1.0 / r0n;
-            q.nvecs = 0;
-        }
-        if (nactive == 0) break;
-        if ((st = push(SCALE, scale.data(), nsys))) { cleanup(); return st; }
-        k_seg_scale<double><<<G.nchunk, TH, 0, ctx->stream>>>(CS, CY, Vb, Vb, SCALE);
-        if ((st = check("k_seg_scale v1"))) { cleanup(); return st; }
-        std::vector<char> cycle_member(nsys);
-        for (int s = 0; s < nsys; ++s) cycle_member[s] = S[s].active;
-        for (int j = 1; j <= m; ++j) {
-            double* vj = Vb + (int64_t)(j - 1) * n;
-            double* zj = Zb + (int64_t)(j - 1) * n;
-            double* w = Vb + (int64_t)j * n;
-            if ((st = precon_apply_impl<double>(M, vj, zj, prec))) { cleanup(); return st; }
-            if ((st = matvec_launch<double, double>(A, (const double*)A->val.ptr, zj, w, nullptr, 1.0, 0.0, ROWSQ)) ||
-                (st = rows_to_sys(OUT + (size_t)nsys * 0))) { cleanup(); return st; }
-            std::vector<double> norm_before(nsys);
-            if ((st = fetch(OUT, nsys, norm_before.data()))) { cleanup(); return st; }
-            // CGS pass 1 with the fresh dot products as coefficients
-            k_seg_mdot<double><<<G.nchunk, TH, 0, ctx->stream>>>(CS, G.nchunk, w, Vb, n, j, PART);
-            if ((st = check("k_seg_mdot"))) { cleanup(); return st; }
-            k_seg_reduce<<<nsys, 128, 0, ctx->stream>>>(PART, G.nchunk, SC, j, COEF, hst);
-            if ((st = check("k_seg_reduce h"))) { cleanup(); return st; }
-            k_seg_maxpy<double><<<G.nchunk, TH, 0, ctx->stream>>>(CS, CY, w, Vb, n, j, COEF, hst, PART);
-            if ((st = check("k_seg_maxpy"))) { cleanup(); return st; }
-            k_seg_reduce<<<nsys, 32, 0, ctx->stream>>>(PART, G.nchunk, SC, 1, OUT, 1);
-            if ((st = check("k_seg_reduce wn"))) { cleanup(); return st; }
-            std::vector<double> h1((size_t)nsys * hst), wn(nsys);
-            if ((st = fetch(COEF, h1.size(), h1.data())) || (st = fetch(OUT, nsys, wn.data()))) { cleanup(); return st; }
-            // selective re-orthogonalisation, per system
-            bool any_reorth = false;
-            std::vector<char> reorth(nsys, 0);
-            for (int s = 0; s < nsys; ++s) {
-                if (!S[s].active) continue;
-                const double nb = std::sqrt(norm_before[s]);
-                if (!std::isfinite(nb)) { cleanup(); ctx->err_elem = sys_elem[s]; return fail(ctx, CHIDG_GPU_ENONFINITE, "batched fgmres: non-finite A*z"); }
-                double crit = 0.0;
-                for (int i = 0; i < j; ++i) crit += std::fabs(h1[(size_t)s * hst + i]);
-                if (crit / nb >= 1.0) { reorth[s] = 1; any_reorth = true; }
-            }
-            std::vector<double> h2((size_t)nsys * hst, 0.0);
-            if (any_reorth) {
-                k_seg_mdot<double><<<G.nchunk, TH, 0, ctx->stream>>>(CS, G.nchunk, w, Vb, n, j, PART);
-                if ((st = check("k_seg_mdot 2"))) { cleanup(); return st; }
-                k_seg_reduce<<<nsys, 128, 0, ctx->stream>>>(PART, G.nchunk, SC, j, OUT, hst);
-                if ((st = check("k_seg_reduce h2")) || (st = fetch(OUT, h2.size(), h2.data()))) { cleanup(); return st; }
-                for (int s = 0; s < nsys; ++s)
-                    if (!reorth[s]) std::fill(h2.begin() + (size_t)s * hst, h2.begin() + (size_t)(s + 1) * hst, 0.0);
-                if ((st = push(COEF, h2.data(), h2.size()))) { cleanup(); return st; }
-                k_seg_maxpy<double><<<G.nchunk, TH, 0, ctx->stream>>>(CS, CY, w, Vb, n, j, COEF, hst, PART);
-                if ((st = check("k_seg_maxpy 2"))) { cleanup(); return st; }
-                k_seg_reduce<<<nsys, 32, 0, ctx->stream>>>(PART, G.nchunk, SC, 1, OUT, 1);
-                if ((st = check("k_seg_reduce wn2")) || (st = fetch(OUT, nsys, wn.data()))) { cleanup(); return st; }
-            }
-            // Givens and convergence, per system
-            bool any_finish = false;
-            std::fill(coef.begin(), coef.end(), 0.0);
-            for (int s = 0; s < nsys; ++s) {
-                SysState& q = S[s];
-                scale[s] = 0.0;
-                if (!q.active) continue;
-                auto H = [&](int i, int jj) -> double& { return q.h[(size_t)i + (size_t)jj * (m + 1)]; };
-                for (int i = 0; i < j; ++i) H(i, j - 1) = h1[(size_t)s * hst + i] + h2[(size_t)s * hst + i];
-                H(j, j - 1) = std::sqrt(wn[s]);
-                scale[s] = 1.0 / H(j, j - 1);
-                for (int i = 0; i < j - 1; ++i) {
-                    const double hij = q.c[i] * H(i, j - 1) + q.s[i] * H(i + 1, j - 1);
-                    const double hipj = -q.s[i] * H(i, j - 1) + q.c[i] * H(i + 1, j - 1);
-                    H(i, j - 1) = hij;
-                    H(i + 1, j - 1) = hipj;
-                }
-                const double gam = std::hypot(H(j - 1, j - 1), H(j, j - 1));
-                q.c[j - 1] = H(j - 1, j - 1) / gam;
-                q.s[j - 1] = H(j, j - 1) / gam;
-                H(j - 1, j - 1) = gam;
-                H(j, j - 1) = 0.0;
-                const double pj = q.c[j - 1] * q.p[j - 1];
-                const double pjp = -q.s[j - 1] * q.p[j - 1];
-                q.p[j - 1] = pj;
-                q.p[j] = pjp;
-                q.niter++;
-                q.nvecs = j;
-                q.res = std::fabs(q.p[j]);
-                q.hist.push_back(q.res);
-                const bool cabs = q.res < o.tol;
-                const bool crel = q.res / q.r0norm_initial < o.rtol;
-                const bool cmax = (q.niter >= o.nmax) && (o.nmax > 0);
-                if (cabs || crel || cmax) {
-                    // x = x0 + sum y_i z_i for this system, then freeze it
-                    if ((st = solve_ls(q, j, coef.data() + (size_t)s * hst))) { cleanup(); return st; }
-                    q.res_est = q.res;
-                    q.active = false;
-                    nactive--;
-                    scale[s] = 0.0;
-                    any_finish = true;
-                }
-            }
-            if (any_finish && (st = update_solution(j))) { cleanup(); return st; }
-            if ((st = push(SCALE, scale.data(), nsys))) { cleanup(); return st; }
-            k_seg_scale<double><<<G.nchunk, TH, 0, ctx->stream>>>(CS, CY, w, w, SCALE);
-            if ((st = check("k_seg_scale v"))) { cleanup(); return st; }
-            if (nactive == 0) break;
-        }
-        // end of a full cycle: update and restart the systems still active
-        if (nactive > 0) {
-            std::fill(coef.begin(), coef.end(), 0.0);
-            for (int s = 0; s < nsys; ++s) {
-                SysState& q = S[s];
-                if (!q.active || !cycle_member[s]) continue;
-                if ((st = solve_ls(q, q.nvecs, coef.data() + (size_t)s * hst))) { cleanup(); return st; }
-                q.res_est = q.res;
-                q.nrestart++;
-            }
-            if ((st = update_solution(m))) { cleanup(); return st; }
-        }
+        if (cnt[0] == 0) break;
     }
     // print_report: true residual per system
-    if ((st = matvec_launch<double, double>(A, (const double*)A->val.ptr, xx, (double*)TMP.ptr, bb, -1.0, 1.0, ROWSQ)) ||
-        (st = rows_to_sys(OUT)) || (st = fetch(OUT, nsys, hout.data()))) { cleanup(); return st; }
+    if ((st = matvec_launch<double, double>(A, (const double*)A->val.ptr, xx, (double*)TMP.ptr, bb, -1.0, 1.0, ROWSQ)))
+        return st;
+    k_seg_reduce<<<nsys, 32, 0, ctx->stream>>>(ROWSQ, A->nrow, SR, 1, OUT, 1);
+    if ((st = check("k_seg_reduce true residual"))) return st;
+    std::vector<double> tres(nsys), r0i(nsys), rest(nsys), hh((size_t)nsys * hcap);
+    std::vector<int32_t> nit(nsys), nrs(nsys), nh(nsys);
     double sw = 0.0;
-    if ((st = fetch(ctx->d_scal + kSlotStatus, 1, &sw)) || (st = status_word(ctx, sw))) { cleanup(); return st; }
-    cleanup();
+    cudaError_t e = cudaMemcpyAsync(tres.data(), OUT, sizeof(double) * nsys, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(r0i.data(), S.r0init, sizeof(double) * nsys, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(rest.data(), S.res_est, sizeof(double) * nsys, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(nit.data(), S.niter, sizeof(int32_t) * nsys, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(nrs.data(), S.nrestart, sizeof(int32_t) * nsys, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(nh.data(), S.nhist, sizeof(int32_t) * nsys, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess && hist) e = cudaMemcpyAsync(hh.data(), S.hist, sizeof(double) * hh.size(), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&sw, ctx->d_scal + kSlotStatus, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "batched fgmres results");
+    if ((st = status_word(ctx, sw))) return st;
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     for (int s = 0; s < nsys; ++s) {
-        S[s].residual_norm = std::sqrt(hout[s]);
         if (results) {
             chidg_gpu_fgmres_result& r = results[s];
-            r.niter = S[s].niter;
-            r.nrestart = S[s].nrestart;
+            r.niter = nit[s];
+            r.nrestart = nrs[s];
             r.inner_iters = 0;
-            r.nhist = (int32_t)std::min<size_t>(S[s].hist.size(), (size_t)std::max(hist_cap, 0));
-            r.residual_norm = S[s].residual_norm;
-            r.res_estimate = S[s].res_est;
-            r.r0norm_initial = S[s].r0norm_initial;
+            r.nhist = std::min(nh[s], std::max(hist_cap, 0));
+            r.residual_norm = std::sqrt(tres[s]);
+            r.res_estimate = rest[s];
+            r.r0norm_initial = r0i[s];
             r.seconds = secs;
         }
         if (hist)
-            for (int i = 0; i < (int)S[s].hist.size() && i < hist_cap; ++i) hist[(size_t)s * hist_cap + i] = S[s].hist[i];
+            for (int i = 0; i < nh[s] && i < hist_cap; ++i) hist[(size_t)s * hist_cap + i] = hh[(size_t)s * hcap + i];
     }
     return CHIDG_GPU_OK;
 }

@@ -4,6 +4,7 @@
 // level-scheduled GPU sweeps.  The FGMRES driver lives in fgmres.cu.
 #include "chidg_gpu_internal.cuh"
 
+#include <tuple>
 #include <type_traits>
 
 #include <atomic>
@@ -237,9 +238,13 @@ extern "C" int chidg_gpu_ctx_destroy(chidg_gpu_ctx* ctx) {
         for (Buffer* b : {&w->V, &w->Z, &w->x0, &w->zr, &w->dz, &w->tmp, &w->rowsq}) release(*b);
     release(ctx->mix_v32);
     release(ctx->mix_z32);
-    for (Buffer* b : {&ctx->batch.cstart, &ctx->batch.csys, &ctx->batch.sys_chunk, &ctx->batch.sys_row, &ctx->batch.d_out,
-                      &ctx->batch.d_coef, &ctx->batch.d_scale, &ctx->batch.partial, &ctx->batch.rowsq})
+    release_batch_graphs(ctx);
+    for (Buffer* b : {&ctx->batch.cstart, &ctx->batch.csys, &ctx->batch.sys_chunk, &ctx->batch.sys_row, &ctx->batch.state,
+                      &ctx->batch.partial, &ctx->batch.rowsq, &ctx->batch.out})
         release(*b);
+    for (cudaEvent_t& e : ctx->batch.ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->batch.h_count) cudaFreeHost(ctx->batch.h_count);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);   // the frees above are ordered on this stream
     if (ctx->d_status) cudaFree(ctx->d_status);
     if (ctx->d_scal) cudaFree(ctx->d_scal);
@@ -693,24 +698,28 @@ int chidg::matvec_launch(chidg_gpu_matrix* A, const TA* val, const TV* x, TV* y,
     const int ph = prof_begin(ctx, sizeof(TA) == 8 ? kProfMatvec : kProfMatvec32);
     if (A->max_b <= SS_MAX_B && A->rows_contiguous && !matvec_rows_env()) {
         // streamed: persistent CTAs, row values prefetched by bulk copies
-        constexpr int CW = 8, NST = 2, SB = 24 * 1024;
-        const size_t smem = matvec_stream_smem(sizeof(ACC), NST, SB, A->max_row_cols, 32 * CW);
-        auto k = k_matvec_stream<TA, TV, ACC, CW>;
-        int st;
-        if ((st = raise_smem_limit((const void*)k, smem))) return fail(ctx, st, "streamed matvec shared memory");
-        int& grid = A->mvs_grid[sizeof(TA) == 8 ? 0 : sizeof(TA) == 4 ? 1 : 2];
-        if (grid == 0) {
-            int per_sm = 0;
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 32 * CW + 32, smem) != cudaSuccess || per_sm < 1) {
-                cudaGetLastError();
-                per_sm = 1;
-            }
-            grid = std::max(1, std::min(A->nrow, per_sm * ctx->nsm));
-        }
+        const StreamShape sh = stream_shape_for(kShapeMatvec, A->max_b, (int)sizeof(TA));
         MatvecRows R{(const int64_t*)A->d_row_ptr.ptr, (const int64_t*)A->d_blk_voff.ptr, (const int64_t*)A->d_blk_xoff.ptr,
                      (const int32_t*)A->d_blk_nc.ptr, (const int64_t*)A->d_row_yoff.ptr, (const int32_t*)A->d_row_b.ptr};
-        k<<<grid, 32 * CW + 32, smem, ctx->stream>>>(R, A->nrow, val, x, y, z, alpha, beta, row_sq,
-                                                     (int*)(ctx->d_scal + kSlotStatus), kSpinLimit, NST, SB, A->max_row_cols);
+        auto launch = [&](auto k, int cw) -> int {
+            const size_t smem = matvec_stream_smem(sizeof(ACC), sh.nstage, sh.stage_bytes, A->max_row_cols, 32 * cw);
+            int st2;
+            if ((st2 = raise_smem_limit((const void*)k, smem))) return fail(ctx, st2, "streamed matvec shared memory");
+            const int per_sm = resident_ctas((const void*)k, 32 * cw + 32, smem);
+            if (per_sm < 1) return fail(ctx, CHIDG_GPU_EINVAL, "streamed matvec: shape does not fit an SM");
+            const int grid = std::max(1, std::min(A->nrow, per_sm * ctx->nsm));
+            k<<<grid, 32 * cw + 32, smem, ctx->stream>>>(R, A->nrow, val, x, y, z, alpha, beta, row_sq,
+                                                         (int*)(ctx->d_scal + kSlotStatus), kSpinLimit, sh.nstage,
+                                                         sh.stage_bytes, A->max_row_cols);
+            return CHIDG_GPU_OK;
+        };
+        int st2;
+        switch (sh.cw) {
+            case 16: st2 = launch(k_matvec_stream<TA, TV, ACC, 16>, 16); break;
+            case 4: st2 = launch(k_matvec_stream<TA, TV, ACC, 4>, 4); break;
+            default: st2 = launch(k_matvec_stream<TA, TV, ACC, 8>, 8);
+        }
+        if (st2) return st2;
     } else {
         const size_t smem = sizeof(ACC) * ((size_t)A->max_row_cols + A->mv_threads) + 512;
         k_matvec<TA, TV, TV, ACC><<<A->nrow, A->mv_threads, smem, ctx->stream>>>(
@@ -1818,21 +1827,62 @@ static int task_sweeps(chidg_gpu_precon* M, const TL* LD, const TU* U, const TV*
     return CHIDG_GPU_OK;
 }
 
-// Shape of the streamed sweeps: consumer warps per CTA, ring stages and stage
-// size.  Read once from CHIDG_STREAM_SHAPE="warps,stages,kbytes" when set.
-struct StreamShape { int cw = 8, nstage = 2, stage_bytes = 24 * 1024; };
-static StreamShape stream_shape() {
-    static StreamShape sh = [] {
-        StreamShape d;
-        if (const char* e = std::getenv("CHIDG_STREAM_SHAPE")) {
-            int cw = 0, ns = 0, kb = 0;
-            if (std::sscanf(e, "%d,%d,%d", &cw, &ns, &kb) == 3 && (cw == 4 || cw == 8 || cw == 16) && ns >= 2 &&
-                ns <= SS_MAX_STAGES && kb >= 2 && kb <= 96)
-                d = StreamShape{cw, ns, kb * 1024};
+// The shape table: per kernel kind, block-size class and value width.
+// Defaults: 8 consumer warps, 2 stages of 24 KB; the backward sweep with the
+// matvec rows 2 stages of 20 KB, so that its wider staged segment still lets
+// 4 CTAs share an SM (measured: 3.62 against 3.80 ms at 24^3 P2 with 24 KB
+// and 3 CTAs).  CHIDG_STREAM_SHAPE="warps,stages,kbytes" overrides the
+// sweeps' defaults (comparison runs).
+namespace {
+std::mutex g_shape_mu;
+StreamShape g_shape[kShapeKinds][kShapeClasses][3];
+bool g_shape_init = false;
+int width_slot(int esz) { return esz >= 8 ? 0 : esz == 4 ? 1 : 2; }
+void init_shapes() {
+    StreamShape sweep;
+    if (const char* e = std::getenv("CHIDG_STREAM_SHAPE")) {
+        int cw = 0, ns = 0, kb = 0;
+        if (std::sscanf(e, "%d,%d,%d", &cw, &ns, &kb) == 3 && (cw == 4 || cw == 8 || cw == 16) && ns >= 2 &&
+            ns <= SS_MAX_STAGES && kb >= 2 && kb <= 96)
+            sweep = StreamShape{cw, ns, kb * 1024};
+    }
+    for (int c = 0; c < kShapeClasses; ++c)
+        for (int w = 0; w < 3; ++w) {
+            g_shape[kShapeForward][c][w] = sweep;
+            g_shape[kShapeBackward][c][w] = sweep;
+            g_shape[kShapeBackwardMv][c][w] = StreamShape{8, 2, 20 * 1024};
+            g_shape[kShapeMatvec][c][w] = StreamShape{8, 2, 24 * 1024};
         }
-        return d;
-    }();
-    return sh;
+    g_shape_init = true;
+}
+}  // namespace
+
+StreamShape chidg::stream_shape_for(int kind, int max_b, int esz) {
+    std::lock_guard<std::mutex> lk(g_shape_mu);
+    if (!g_shape_init) init_shapes();
+    return g_shape[kind][shape_class(max_b)][width_slot(esz)];
+}
+void chidg::set_stream_shape(int kind, int max_b, int esz, const StreamShape& sh) {
+    std::lock_guard<std::mutex> lk(g_shape_mu);
+    if (!g_shape_init) init_shapes();
+    g_shape[kind][shape_class(max_b)][width_slot(esz)] = sh;
+}
+int chidg::resident_ctas(const void* func, int threads, size_t smem) {
+    static std::mutex mu;
+    static std::map<std::tuple<int, const void*, int, size_t>, int> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    auto key = std::make_tuple(dev, func, threads, smem);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, threads, smem) != cudaSuccess || per_sm < 1) {
+        cudaGetLastError();
+        per_sm = 0;
+    }
+    cache[key] = per_sm;
+    return per_sm;
 }
 
 template <typename TL, typename TU, typename TV, bool FWD, int CW, typename TA = double, bool MV = false>
@@ -1846,15 +1896,10 @@ static int stream_launch(chidg_gpu_precon* M, const TL* LD, const TU* U, StreamT
     auto k = k_ilu_stream<TL, TU, TV, ACC, FWD, CW, TA, MV>;
     int st;
     if ((st = raise_smem_limit((const void*)k, smem))) return fail(ctx, st, "streamed sweep shared memory");
-    int& grid = M->ss_grid[variant][MV ? 2 : FWD ? 0 : 1];
-    if (grid == 0) {
-        int per_sm = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 32 * CW + 32, smem) != cudaSuccess || per_sm < 1) {
-            cudaGetLastError();
-            per_sm = 1;
-        }
-        grid = per_sm * ctx->nsm;
-    }
+    const int per_sm = resident_ctas((const void*)k, 32 * CW + 32, smem);
+    if (per_sm < 1) return fail(ctx, CHIDG_GPU_EINVAL, "streamed sweep: shape does not fit an SM");
+    const int grid = per_sm * ctx->nsm;
+    (void)variant;
     k<<<std::max(1, std::min(grid, ntask)), 32 * CW + 32, smem, ctx->stream>>>(M->P.rows, LD, U, Tk, ntask, v, zx, (ACC*)part,
                                                                               S, sh.nstage, sh.stage_bytes, xcols, F);
     return check_launch(ctx, MV ? "k_ilu_stream backward + matvec" : FWD ? "k_ilu_stream forward" : "k_ilu_stream backward");
@@ -1933,7 +1978,9 @@ static int stream_sweeps(chidg_gpu_precon* M, const TL* LD, const TU* U, const T
     chidg_gpu_ctx* ctx = M->ctx;
     IluProgram& P = M->P;
     using ACC = typename AccOf<TV>::type;
-    const StreamShape sh = stream_shape();
+    constexpr int esz = (int)sizeof(TL);
+    const StreamShape sh = stream_shape_for(kShapeForward, P.max_b, esz);
+    const StreamShape shb = stream_shape_for(F ? kShapeBackwardMv : kShapeBackward, P.max_b, esz);
     Buffer& pb = (sizeof(ACC) == 8) ? M->part64 : M->part32;
     int st = ensure(ctx, pb, sizeof(ACC) * (size_t)std::max<int64_t>(1, std::max(P.part_f, P.part_b)));
     if (st) return st;
@@ -1943,7 +1990,22 @@ static int stream_sweeps(chidg_gpu_precon* M, const TL* LD, const TU* U, const T
     cudaError_t e = cudaMemsetAsync(sync, 0, 2 * sizeof(unsigned), ctx->stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "sweep counters");
     int ph = prof_begin(ctx, sizeof(TV) == 8 ? kProfIluForward : kProfIlu32);
-    S.epoch = ++M->epoch;
+    // inside a captured sequence: clear the row flags (and the backward
+    // sweep's ready flags) in the sequence itself and publish fixed epochs,
+    // which no host epoch reaches
+    constexpr unsigned kGraphEpochF = 0xF0000001u, kGraphEpochB = 0xF0000002u;
+    auto clear_flags = [&](bool backward) -> int {
+        cudaError_t e2 = cudaMemsetAsync(flags, 0, sizeof(unsigned) * (size_t)P.nprow, ctx->stream);
+        if (e2 == cudaSuccess && backward)
+            e2 = cudaMemsetAsync(flags + 3 * P.nprow, 0, sizeof(unsigned) * (size_t)P.nprow, ctx->stream);
+        return e2 == cudaSuccess ? CHIDG_GPU_OK : cuda_fail(ctx, e2, "sweep flags");
+    };
+    if (M->graph_safe) {
+        if ((st = clear_flags(false))) return st;
+        S.epoch = kGraphEpochF;
+    } else {
+        S.epoch = ++M->epoch;
+    }
     S.counter = sync;
     StreamTasks Tf{(const int32_t*)P.d_tf_row.ptr, (const int32_t*)P.d_tf_ent.ptr, (const int64_t*)P.d_poff_f.ptr,
                    flags + P.nprow, flags + 3 * P.nprow};
@@ -1957,15 +2019,20 @@ static int stream_sweeps(chidg_gpu_precon* M, const TL* LD, const TU* U, const T
         prof_end(ctx, ph);
         ph = prof_begin(ctx, F ? kProfIluBackwardMv : kProfIluBackward);
     }
-    S.epoch = ++M->epoch;
+    if (M->graph_safe) {
+        if ((st = clear_flags(true))) return st;
+        S.epoch = kGraphEpochB;
+    } else {
+        S.epoch = ++M->epoch;
+    }
     S.counter = sync + 1;
     if (F) {
         StreamTasks Tm{(const int32_t*)P.d_bmv_row.ptr, (const int32_t*)P.d_bmv_ent.ptr, (const int64_t*)P.d_poff_b.ptr,
                        flags + 2 * P.nprow, flags + 3 * P.nprow};
-        switch (sh.cw) {
-            case 16: st = stream_launch<TL, TU, TV, false, 16, TA, true>(M, LD, U, Tm, P.ntask_bmv, v, zx, pb.ptr, S, sh, variant, *F, mv_cols); break;
-            case 4: st = stream_launch<TL, TU, TV, false, 4, TA, true>(M, LD, U, Tm, P.ntask_bmv, v, zx, pb.ptr, S, sh, variant, *F, mv_cols); break;
-            default: st = stream_launch<TL, TU, TV, false, 8, TA, true>(M, LD, U, Tm, P.ntask_bmv, v, zx, pb.ptr, S, sh, variant, *F, mv_cols);
+        switch (shb.cw) {
+            case 16: st = stream_launch<TL, TU, TV, false, 16, TA, true>(M, LD, U, Tm, P.ntask_bmv, v, zx, pb.ptr, S, shb, variant, *F, mv_cols); break;
+            case 4: st = stream_launch<TL, TU, TV, false, 4, TA, true>(M, LD, U, Tm, P.ntask_bmv, v, zx, pb.ptr, S, shb, variant, *F, mv_cols); break;
+            default: st = stream_launch<TL, TU, TV, false, 8, TA, true>(M, LD, U, Tm, P.ntask_bmv, v, zx, pb.ptr, S, shb, variant, *F, mv_cols);
         }
         if (st) return st;
         prof_end(ctx, ph);
@@ -1973,10 +2040,10 @@ static int stream_sweeps(chidg_gpu_precon* M, const TL* LD, const TU* U, const T
     }
     StreamTasks Tb{(const int32_t*)P.d_sb_row.ptr, (const int32_t*)P.d_sb_ent.ptr, (const int64_t*)P.d_poff_b.ptr,
                    flags + 2 * P.nprow, flags + 3 * P.nprow};
-    switch (sh.cw) {
-        case 16: st = stream_launch<TL, TU, TV, false, 16>(M, LD, U, Tb, P.ntask_sb, v, zx, pb.ptr, S, sh, variant); break;
-        case 4: st = stream_launch<TL, TU, TV, false, 4>(M, LD, U, Tb, P.ntask_sb, v, zx, pb.ptr, S, sh, variant); break;
-        default: st = stream_launch<TL, TU, TV, false, 8>(M, LD, U, Tb, P.ntask_sb, v, zx, pb.ptr, S, sh, variant);
+    switch (shb.cw) {
+        case 16: st = stream_launch<TL, TU, TV, false, 16>(M, LD, U, Tb, P.ntask_sb, v, zx, pb.ptr, S, shb, variant); break;
+        case 4: st = stream_launch<TL, TU, TV, false, 4>(M, LD, U, Tb, P.ntask_sb, v, zx, pb.ptr, S, shb, variant); break;
+        default: st = stream_launch<TL, TU, TV, false, 8>(M, LD, U, Tb, P.ntask_sb, v, zx, pb.ptr, S, shb, variant);
     }
     if (st) return st;
     prof_end(ctx, ph);

@@ -88,6 +88,20 @@ struct IluProgram {
 }  // namespace chidg
 
 namespace chidg {
+// Launch shape of a streamed kernel: consumer warps, ring stages, bytes per
+// stage.  One shape per kernel kind, block-size class and value width: the
+// defaults below, or what the autotuner measured best (chidg_gpu_autotune).
+struct StreamShape { int cw = 8, nstage = 2, stage_bytes = 24 * 1024; };
+enum { kShapeForward = 0, kShapeBackward = 1, kShapeBackwardMv = 2, kShapeMatvec = 3, kShapeKinds = 4 };
+constexpr int kShapeClasses = 4;                 // largest block: <= 64, <= 160, <= 384, <= 1024 rows
+inline int shape_class(int max_b) { return max_b <= 64 ? 0 : max_b <= 160 ? 1 : max_b <= 384 ? 2 : 3; }
+StreamShape stream_shape_for(int kind, int max_b, int esz);
+void set_stream_shape(int kind, int max_b, int esz, const StreamShape& sh);
+// resident CTAs per SM of `func` (cached per function, block size and shared memory)
+int resident_ctas(const void* func, int threads, size_t smem);
+}  // namespace chidg
+
+namespace chidg {
 // kernel classes timed with CUDA events when profiling is on
 enum { kProfMatvec = 0, kProfIluForward = 1, kProfIluBackward = 2, kProfFactor = 3, kProfMatvec32 = 4, kProfIlu32 = 5,
        kProfFactorGemm = 6, kProfFactorInv = 7, kProfIluBackwardMv = 8, kProfClasses = 9 };
@@ -101,12 +115,18 @@ namespace chidg {
 struct Workspace {
     Buffer V, Z, x0, zr, dz, tmp, rowsq;
 };
-// device buffers of the batched solver's per-system segments, kept by the
-// context (they only grow) so that a batched solve allocates nothing
+// device buffers of the batched solver's per-system segments and Arnoldi
+// state, kept by the context (they only grow) so that a batched solve
+// allocates nothing once they have grown; a pinned counter and two events
+// let the host read the active-system count without waiting
 struct BatchBuffers {
-    Buffer cstart, csys, sys_chunk, sys_row, d_out, d_coef, d_scale, partial, rowsq;
+    Buffer cstart, csys, sys_chunk, sys_row, state, partial, rowsq, out;
+    int32_t* h_count = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
 };
 }  // namespace chidg
+
+struct BatchGraphs;   // captured launch sequences of the last batch structure (batch.cu)
 
 struct chidg_gpu_ctx {
     int device = 0;
@@ -124,6 +144,7 @@ struct chidg_gpu_ctx {
     chidg::Workspace ws64, ws32;
     chidg::Buffer mix_v32, mix_z32;   // mixed precision: FP32 copies of the outer loop's v and z
     chidg::BatchBuffers batch;
+    BatchGraphs* batch_graphs = nullptr;
     bool profiling = false;
     std::vector<chidg::EvPair> prof_pending;
     std::vector<cudaEvent_t> prof_pool;
@@ -142,7 +163,6 @@ struct chidg_gpu_matrix {
     std::vector<int32_t> diag;
     int max_row_cols = 0, max_b = 0, mv_threads = 32;
     bool rows_contiguous = true;             // each row's blocks follow one another in val (the streamed matvec's layout)
-    int mvs_grid[3] = {0, 0, 0};             // resident CTAs of the streamed matvec per value type
     chidg::Buffer val, val32, val16;
     int64_t val32_stamp = -1, val16_stamp = -1;
     chidg::Buffer d_row_ptr, d_blk_voff, d_blk_xoff, d_blk_nc, d_row_yoff, d_row_b, d_diag_voff, d_elem_nvars,
@@ -184,7 +204,10 @@ struct chidg_gpu_precon {
     unsigned epoch = 0;
     int sf_grid[3] = {0, 0, 0};            // resident CTAs of the dataflow sweep per vector type
     int tk_grid[4] = {0, 0, 0, 0};         // resident CTAs of the task-split sweep per variant
-    int ss_grid[4][3] = {};                // resident CTAs of the streamed sweeps (forward, backward, backward + matvec)
+    // the sweeps are being captured into a CUDA graph: each sweep clears its
+    // row flags and publishes with a fixed epoch, so that every replay starts
+    // from cleared flags (a host epoch would be frozen into the graph)
+    bool graph_safe = false;
 };
 
 namespace chidg {
@@ -223,6 +246,7 @@ int precon_apply_mv(chidg_gpu_precon* M, const TV* v, TV* z, int precision, chid
 int precon_set_smem(chidg_gpu_precon* M);
 void release_program(IluProgram& P);
 int status_word(chidg_gpu_ctx* ctx, double slot_value);
+void release_batch_graphs(chidg_gpu_ctx* ctx);
 int prof_begin(chidg_gpu_ctx* ctx, int cls);        // -1 when profiling is off
 void prof_end(chidg_gpu_ctx* ctx, int handle);
 void prof_resolve(chidg_gpu_ctx* ctx);              // after a stream sync

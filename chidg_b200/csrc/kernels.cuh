@@ -1374,9 +1374,11 @@ __global__ void __launch_bounds__(1024) k_ilu_backward(IluRows R, const TL* __re
 // partial[q * nchunk + c] = sum over chunk c of x * y_q
 template <typename T>
 __global__ void k_seg_mdot(const int64_t* __restrict__ cstart, int nchunk, const T* __restrict__ x,
-                           const T* __restrict__ y, int64_t ystride, int nq, double* __restrict__ partial) {
+                           const T* __restrict__ y, int64_t ystride, int nq, double* __restrict__ partial,
+                           const int32_t* __restrict__ csys = nullptr, const int32_t* __restrict__ mask = nullptr) {
     __shared__ double scratch[32];
     const int c = blockIdx.x;
+    if (mask != nullptr && !mask[csys[c]]) return;     // system not in this pass: its partials are not read
     const int64_t i0 = cstart[c], i1 = cstart[c + 1];
     for (int q = 0; q < nq; ++q) {
         const T* yq = y + (int64_t)q * ystride;
@@ -1388,8 +1390,9 @@ __global__ void k_seg_mdot(const int64_t* __restrict__ cstart, int nchunk, const
 }
 // out[s * ostride + q] = sum over the chunks [sys_chunk[s], sys_chunk[s+1]) of partial[q * nchunk + c]
 static __global__ void k_seg_reduce(const double* __restrict__ partial, int nchunk, const int32_t* __restrict__ sys_chunk,
-                                    int nq, double* __restrict__ out, int ostride) {
+                                    int nq, double* __restrict__ out, int ostride, const int32_t* __restrict__ mask = nullptr) {
     const int s = blockIdx.x;
+    if (mask != nullptr && !mask[s]) return;
     const int c0 = sys_chunk[s], c1 = sys_chunk[s + 1];
     for (int q = threadIdx.x; q < nq; q += blockDim.x) {
         double acc = 0.0;
@@ -1401,10 +1404,11 @@ static __global__ void k_seg_reduce(const double* __restrict__ partial, int nchu
 template <typename T>
 __global__ void k_seg_maxpy(const int64_t* __restrict__ cstart, const int32_t* __restrict__ csys, T* __restrict__ w,
                             const T* __restrict__ v, int64_t vstride, int nq, const double* __restrict__ coef,
-                            int cstride, double* __restrict__ sumsq) {
+                            int cstride, double* __restrict__ sumsq, const int32_t* __restrict__ mask = nullptr) {
     __shared__ double scratch[32];
     __shared__ double cs[256];
     const int c = blockIdx.x;
+    if (mask != nullptr && !mask[csys[c]]) return;
     const int64_t i0 = cstart[c], i1 = cstart[c + 1];
     const double* cf = coef + (int64_t)csys[c] * cstride;
     double sq = 0.0;
@@ -1432,8 +1436,9 @@ __global__ void k_seg_maxpy(const int64_t* __restrict__ cstart, const int32_t* _
 template <typename T>
 __global__ void k_seg_lincomb(const int64_t* __restrict__ cstart, const int32_t* __restrict__ csys, T* __restrict__ x,
                               const T* __restrict__ x0, const T* __restrict__ z, int64_t zstride, int nq,
-                              const double* __restrict__ coef, int cstride) {
+                              const double* __restrict__ coef, int cstride, const int32_t* __restrict__ mask = nullptr) {
     const int c = blockIdx.x;
+    if (mask != nullptr && !mask[csys[c]]) return;
     const int64_t i0 = cstart[c], i1 = cstart[c + 1];
     const double* cf = coef + (int64_t)csys[c] * cstride;
     for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {

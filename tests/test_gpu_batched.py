@@ -112,3 +112,48 @@ def test_batched_harmonic_balance_systems():
         xo, ro = O.fgmres(Ao, O.OraclePrecon(Ao, "ilu0"), r, O.default_opts(**opts))
         assert res[s]["niter"] == ro["niter"]
         assert relerr(xb[eo[sys_elem[s]]:eo[sys_elem[s + 1]]], xo) < 1e-10
+
+
+def test_batched_graph_replay_matches_eager_solves():
+    """The same batch structure solved again (new values, the next Newton
+    step) replays its Arnoldi steps from captured graphs: the second and later
+    calls give bitwise the result an eager solve of the same values gives
+    (CHIDG_BATCH_GRAPHS=0 in a process of its own), restarts included."""
+    import json
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    child = r"""
+import json, sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+from chidg_b200 import api, mesh
+pats = [mesh.box_pattern(*s, 5, mesh.nterms_of_order(P)) for s, P in (((3, 3, 2), 1), ((2, 2, 2), 2), ((4, 2, 2), 1))]
+union, sys_elem = mesh.concat_patterns(pats)
+A = api.ChidgMatrix(union)
+b = api.ChidgVector(A, mesh.synth_vector(union.vector_size(), seed=7))
+x = api.ChidgVector(A)
+M = api.create_preconditioner("ilu0")
+solver = api.create_linear_solver("fgmres", tol=0.0, rtol=1e-9, nkrylov=6, inner_fgmres=0, nmax=300)
+out = []
+for step in range(4):
+    A.upload(mesh.synth_values(union, seed=20 + step))
+    res = solver.solve_batched(A, x, b, M, sys_elem)
+    out.append({"x": x.download().tolist(), "niter": [r["niter"] for r in res],
+                "hist": [r["hist"].tolist() for r in res], "res": [r["residual_norm"] for r in res]})
+print(json.dumps(out))
+"""
+
+    def run(graphs):
+        env = dict(os.environ, CHIDG_BATCH_GRAPHS="1" if graphs else "0")
+        p = subprocess.run([sys.executable, "-c", child, root], capture_output=True, text=True, env=env, timeout=600)
+        assert p.returncode == 0, p.stderr[-2000:]
+        return json.loads(p.stdout.strip().splitlines()[-1])
+
+    g, e = run(True), run(False)
+    for step in range(4):
+        assert g[step]["niter"] == e[step]["niter"], step
+        assert max(g[step]["niter"]) > 6            # restarts happen
+        assert g[step]["hist"] == e[step]["hist"], step
+        assert np.array_equal(np.array(g[step]["x"]), np.array(e[step]["x"])), step

@@ -1,9 +1,13 @@
 """The matvec rows run inside the streamed backward sweep (the fused pass that
-FGMRES takes for z = M v followed by w = A z) give bitwise the results of the
-separate launches: the same chunks and per-thread order in every product.
-Checked on whole FGMRES solves against a process that runs the separate
-launches (CHIDG_FUSED_MV=0), for FP64, FP32 preconditioner blocks and the FP32
-and BF16 inner solves, with ILU0 and Jacobi, on one and three time levels."""
+FGMRES takes for z = M v followed by w = A z) agree with the separate launches
+to rounding: the fused launch streams its blocks in 20 KB stages where the
+separate launches use 24 KB ones, so only the chunk boundaries of each
+product's two interleaved partial sums differ.  Checked on whole FGMRES
+solves against a process that runs the separate launches (CHIDG_FUSED_MV=0):
+FP64 and FP32 preconditioner blocks take the same iterations with the residual
+history within 1e-10 and x within 1e-12; the FP32 and BF16 inner solves reach
+the same FP64 residual with x within 1e-6.  ILU0 and Jacobi, one and three
+time levels."""
 import json
 import os
 import subprocess
@@ -36,7 +40,8 @@ for kind, prec, nt, P in json.loads(sys.argv[2]):
         opts.update(nkrylov=8, mixed_inner_nkrylov=10, mixed_inner_rtol=1e-2, mixed_inner_nmax=30)
     s = api.create_linear_solver("fgmres", **opts)
     s.solve(A, x, b, api.create_preconditioner(kind))
-    out[f"{kind}-{prec}-{nt}-{P}"] = {"x": x.download().tolist(), "hist": s.hist.tolist(), "niter": s.niter}
+    out[f"{kind}-{prec}-{nt}-{P}"] = {"x": x.download().tolist(), "hist": s.hist.tolist(), "niter": s.niter,
+                                      "rel_res": s.residual_norm / s.r0norm_initial}
 print(json.dumps(out))
 """
 
@@ -49,9 +54,19 @@ def _run(fused):
     return json.loads(p.stdout.strip().splitlines()[-1])
 
 
-def test_fused_sweep_and_matvec_are_bitwise_the_separate_launches():
+def relerr(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def test_fused_sweep_and_matvec_agree_with_the_separate_launches():
     fused, split = _run(True), _run(False)
     for key in split:
-        assert fused[key]["niter"] == split[key]["niter"], key
-        assert np.array_equal(np.array(fused[key]["hist"]), np.array(split[key]["hist"])), key
-        assert np.array_equal(np.array(fused[key]["x"]), np.array(split[key]["x"])), key
+        f, s = fused[key], split[key]
+        if "mixed_fp32" in key or "mixed_bf16" in key:
+            assert f["rel_res"] <= 1e-9 * 1.0001 and s["rel_res"] <= 1e-9 * 1.0001, key
+            assert relerr(f["x"], s["x"]) <= 1e-6, key
+            continue
+        assert f["niter"] == s["niter"], key
+        assert relerr(f["hist"], s["hist"]) <= 1e-10, key
+        assert relerr(f["x"], s["x"]) <= 1e-12, key
