@@ -816,6 +816,15 @@ def run_gpu(args):
     M = api.create_preconditioner("ilu0", schedule=args.schedule)
     solver = api.create_linear_solver("fgmres", **SOLVER)
     L = ctx.L
+    # the project autotuner picks the streamed kernels' launch shapes for this
+    # block size (before the warm-up; not timed)
+    tuned, tune_s = None, None
+    if args.schedule == "stream" and not args.no_tune:
+        from chidg_b200 import tuning
+        M.update(A)
+        t0 = time.perf_counter()
+        tuned = tuning.autotune(A, M, "fp64", reps=2, cache=os.environ.get("CHIDG_TUNE_CACHE"))
+        tune_s = time.perf_counter() - t0
 
     def solve():
         solver.solve(A, x, b, M)
@@ -939,6 +948,10 @@ def run_gpu(args):
             opts = {**SOLVER, "precision": prec} if prec == "mixed_precon_fp32" else {**SOLVER, **MIXED, "precision": prec}
             ms = api.create_linear_solver("fgmres", **opts)
             xm = api.ChidgVector(A)
+            if tuned is not None:                      # this precision's value widths get their own shapes
+                from chidg_b200 import tuning
+                M.update(A, precision=prec)
+                tuning.autotune(A, M, prec, reps=2, cache=os.environ.get("CHIDG_TUNE_CACHE"))
             ms.solve(A, xm, b, M)                      # warm-up
             torch.cuda.synchronize()
             m0 = torch.cuda.Event(enable_timing=True)
@@ -1034,7 +1047,7 @@ def run_gpu(args):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_config({"precision": "fp64", "ilu_schedule": args.schedule, "fgmres_iterations": niters,
                                    "bump_centre": [float(c) for c in centre], "device_assembly_s": assembly_s,
-                                   "true_rel_residual": resid,
+                                   "true_rel_residual": resid, "stream_shapes": tuned, "autotune_s": tune_s,
                                    "rel_err_vs_oracle": oracle_check["rel_err_vs_oracle"] if oracle_check else None}),
         "oracle_check": oracle_check,
         "latency_ms": {"p50": float(np.percentile(lat_sorted, 50)), "p99": float(np.percentile(lat_sorted, 99))},
@@ -1080,6 +1093,7 @@ def main():
     ap.add_argument("--no-assembly", action="store_true",
                     help="skip the device Euler assembly leg (24^3 P2, overwrites the 24^3 matrix)")
     ap.add_argument("--no-cfg3", action="store_true", help="skip the 32^3 P2 legs (ILU0 and RAS, FP64 and mixed)")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuning)")
     ap.add_argument("--serve-only", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--serve-device", type=int, default=0, help=argparse.SUPPRESS)
     args = ap.parse_args()

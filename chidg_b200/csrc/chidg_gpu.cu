@@ -701,6 +701,8 @@ int chidg::matvec_launch(chidg_gpu_matrix* A, const TA* val, const TV* x, TV* y,
         const StreamShape sh = stream_shape_for(kShapeMatvec, A->max_b, (int)sizeof(TA));
         MatvecRows R{(const int64_t*)A->d_row_ptr.ptr, (const int64_t*)A->d_blk_voff.ptr, (const int64_t*)A->d_blk_xoff.ptr,
                      (const int32_t*)A->d_blk_nc.ptr, (const int64_t*)A->d_row_yoff.ptr, (const int32_t*)A->d_row_b.ptr};
+        if ((size_t)sh.stage_bytes < (size_t)A->max_b * sizeof(TA) + 16)
+            return fail(ctx, CHIDG_GPU_EINVAL, "streamed matvec: stage smaller than one block column");
         auto launch = [&](auto k, int cw) -> int {
             const size_t smem = matvec_stream_smem(sizeof(ACC), sh.nstage, sh.stage_bytes, A->max_row_cols, 32 * cw);
             int st2;
@@ -1892,6 +1894,10 @@ static int stream_launch(chidg_gpu_precon* M, const TL* LD, const TU* U, StreamT
     chidg_gpu_ctx* ctx = M->ctx;
     using ACC = typename AccOf<TV>::type;
     const int xcols = std::max(M->P.max_b, mv_cols);    // the widest segment staged in shared memory
+    // a stage must hold one column of the widest block (plus the 16-byte rounding)
+    if ((size_t)sh.stage_bytes < (size_t)M->P.max_b * std::max(sizeof(TL), sizeof(TU)) + 16 ||
+        (MV && (size_t)sh.stage_bytes < (size_t)M->P.max_b * sizeof(TA) + 16))
+        return fail(ctx, CHIDG_GPU_EINVAL, "streamed sweep: stage smaller than one block column");
     const size_t smem = stream_smem_bytes(sizeof(ACC), sh.nstage, sh.stage_bytes, xcols, 32 * CW);
     auto k = k_ilu_stream<TL, TU, TV, ACC, FWD, CW, TA, MV>;
     int st;
@@ -1974,7 +1980,7 @@ static int fused_mv_lag() {
 // backward launch also runs the matvec rows of F (task list d_bmv_*).
 template <typename TL, typename TU, typename TV, typename TA = double>
 static int stream_sweeps(chidg_gpu_precon* M, const TL* LD, const TU* U, const TV* v, TV* zx, int variant,
-                         const FusedMv<TA, TV>* F = nullptr, int mv_cols = 0) {
+                         const FusedMv<TA, TV>* F = nullptr, int mv_cols = 0, int which = 3) {
     chidg_gpu_ctx* ctx = M->ctx;
     IluProgram& P = M->P;
     using ACC = typename AccOf<TV>::type;
@@ -2000,21 +2006,27 @@ static int stream_sweeps(chidg_gpu_precon* M, const TL* LD, const TU* U, const T
             e2 = cudaMemsetAsync(flags + 3 * P.nprow, 0, sizeof(unsigned) * (size_t)P.nprow, ctx->stream);
         return e2 == cudaSuccess ? CHIDG_GPU_OK : cuda_fail(ctx, e2, "sweep flags");
     };
-    if (M->graph_safe) {
-        if ((st = clear_flags(false))) return st;
-        S.epoch = kGraphEpochF;
-    } else {
-        S.epoch = ++M->epoch;
+    if (which & 1) {
+        if (M->graph_safe) {
+            if ((st = clear_flags(false))) return st;
+            S.epoch = kGraphEpochF;
+        } else {
+            S.epoch = ++M->epoch;
+        }
+        S.counter = sync;
+        StreamTasks Tf{(const int32_t*)P.d_tf_row.ptr, (const int32_t*)P.d_tf_ent.ptr, (const int64_t*)P.d_poff_f.ptr,
+                       flags + P.nprow, flags + 3 * P.nprow};
+        switch (sh.cw) {
+            case 16: st = stream_launch<TL, TU, TV, true, 16>(M, LD, U, Tf, P.ntask_f, v, zx, pb.ptr, S, sh, variant); break;
+            case 4: st = stream_launch<TL, TU, TV, true, 4>(M, LD, U, Tf, P.ntask_f, v, zx, pb.ptr, S, sh, variant); break;
+            default: st = stream_launch<TL, TU, TV, true, 8>(M, LD, U, Tf, P.ntask_f, v, zx, pb.ptr, S, sh, variant);
+        }
+        if (st) return st;
     }
-    S.counter = sync;
-    StreamTasks Tf{(const int32_t*)P.d_tf_row.ptr, (const int32_t*)P.d_tf_ent.ptr, (const int64_t*)P.d_poff_f.ptr,
-                   flags + P.nprow, flags + 3 * P.nprow};
-    switch (sh.cw) {
-        case 16: st = stream_launch<TL, TU, TV, true, 16>(M, LD, U, Tf, P.ntask_f, v, zx, pb.ptr, S, sh, variant); break;
-        case 4: st = stream_launch<TL, TU, TV, true, 4>(M, LD, U, Tf, P.ntask_f, v, zx, pb.ptr, S, sh, variant); break;
-        default: st = stream_launch<TL, TU, TV, true, 8>(M, LD, U, Tf, P.ntask_f, v, zx, pb.ptr, S, sh, variant);
+    if (!(which & 2)) {
+        prof_end(ctx, ph);
+        return CHIDG_GPU_OK;
     }
-    if (st) return st;
     if (sizeof(TV) == 8) {
         prof_end(ctx, ph);
         ph = prof_begin(ctx, F ? kProfIluBackwardMv : kProfIluBackward);
@@ -2257,5 +2269,183 @@ extern "C" int chidg_gpu_precon_download_LD(chidg_gpu_precon* M, double* host) {
         for (const auto& en : P.lo[pr])
             if (en.blk >= 0) std::memcpy(host + A->voff[en.blk], ld.data() + en.l_off, sizeof(double) * (size_t)b * en.nc);
     }
+    return CHIDG_GPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner of the streamed kernels' launch shapes
+// ---------------------------------------------------------------------------
+namespace {
+__global__ void k_fill(double* x, int64_t n, double v) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) x[i] = v;
+}
+__global__ void k_fill32(float* x, int64_t n, float v) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) x[i] = v;
+}
+}  // namespace
+
+// Candidate shapes: 4, 8 or 16 consumer warps; 2 to 4 stages of 8 to 48 KB
+// (ring at most 96 KB); a stage holds at least one column of the widest block.
+static std::vector<StreamShape> shape_candidates(int max_b, int esz) {
+    std::vector<StreamShape> out;
+    for (int cw : {4, 8, 16})
+        for (int ns : {2, 3, 4})
+            for (int kb : {8, 12, 16, 20, 24, 32, 40, 48}) {
+                if (ns * kb > 96) continue;
+                if ((size_t)kb * 1024 < (size_t)max_b * esz + 16) continue;
+                out.push_back(StreamShape{cw, ns, kb * 1024});
+            }
+    return out;
+}
+
+extern "C" int chidg_gpu_autotune(chidg_gpu_precon* M, chidg_gpu_matrix* A, int32_t precision, int32_t reps) {
+    if (!M || !A || M->A != A || reps < 1 || reps > 100) return CHIDG_GPU_EINVAL;
+    chidg_gpu_ctx* ctx = M->ctx;
+    cudaSetDevice(ctx->device);
+    if (precision != CHIDG_GPU_FP64 && precision != CHIDG_GPU_MIXED_PRECON_FP32 && precision != CHIDG_GPU_MIXED_FP32 &&
+        precision != CHIDG_GPU_MIXED_BF16)
+        return fail(ctx, CHIDG_GPU_EINVAL, "autotune: bad precision");
+    if (M->kind == CHIDG_PRECON_IDENTITY || M->stamp == 0 || M->precision != precision)
+        return fail(ctx, CHIDG_GPU_ESTATE, "autotune: update the preconditioner for A in this precision first");
+    if (M->schedule != CHIDG_SCHED_STREAM || M->P.max_b > SS_MAX_B)
+        return fail(ctx, CHIDG_GPU_EINVAL, "autotune: the streamed schedule only");
+    chidg_gpu_matrix* Aop = nullptr;
+    int st;
+    if ((st = matrix_op(A, &Aop))) return st;
+    if ((st = matrix_lowp(Aop, precision))) return st;
+    set_matvec_smem(Aop);
+    precon_set_smem(M);
+    const bool lowp_vec = precision == CHIDG_GPU_MIXED_FP32 || precision == CHIDG_GPU_MIXED_BF16;
+    const int esz_blocks = precision == CHIDG_GPU_FP64 ? 8 : precision == CHIDG_GPU_MIXED_BF16 ? 2 : 4;
+    const int esz_matvec = precision == CHIDG_GPU_MIXED_PRECON_FP32 ? 8 : esz_blocks;
+    const int64_t n = std::max<int64_t>(M->P.n_ext, Aop->n);
+    Buffer bv, bz, bw, brs;
+    auto cleanup = [&]() { for (Buffer* b : {&bv, &bz, &bw, &brs}) release(*b); };
+    const size_t vb = (lowp_vec ? sizeof(float) : sizeof(double)) * (size_t)n;
+    if ((st = ensure(ctx, bv, vb)) || (st = ensure(ctx, bz, vb)) || (st = ensure(ctx, bw, vb)) ||
+        (st = ensure(ctx, brs, sizeof(double) * (size_t)Aop->nrow))) {
+        cleanup();
+        return st;
+    }
+    if (lowp_vec) k_fill32<<<ctx->nsm * 4, 256, 0, ctx->stream>>>((float*)bv.ptr, n, 1.0f);
+    else k_fill<<<ctx->nsm * 4, 256, 0, ctx->stream>>>((double*)bv.ptr, n, 1.0);
+    cudaMemsetAsync(bz.ptr, 0, vb, ctx->stream);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const bool prof = ctx->profiling;
+    ctx->profiling = false;
+    cudaMemsetAsync(ctx->d_scal + kSlotStatus, 0, sizeof(double), ctx->stream);
+    // one run of the kernel kind, launched with the table's current shape
+    auto run_kind = [&](int kind) -> int {
+        if (!lowp_vec) {
+            const double* v = (const double*)bv.ptr;
+            double* z = (double*)bz.ptr;
+            double* w = (double*)bw.ptr;
+            if (kind == kShapeMatvec) return matvec_launch<double, double>(Aop, (const double*)Aop->val.ptr, z, w, nullptr, 1.0, 0.0, (double*)brs.ptr);
+            const bool p32 = precision == CHIDG_GPU_MIXED_PRECON_FP32;
+            chidg_gpu_matrix* S = nullptr;
+            int s2 = precon_source(M, &S);
+            if (s2) return s2;
+            if (kind == kShapeBackwardMv) {
+                if (M->kind != CHIDG_PRECON_ILU0 && M->kind != CHIDG_PRECON_JACOBI) return 1;
+                if (S != Aop || M->P.n_ext != Aop->n || M->P.nprow != Aop->nrow || !Aop->rows_contiguous) return 1;
+                if ((s2 = build_bwd_mv_tasks(M, Aop, fused_mv_lag()))) return s2;
+                MatvecRowsView R{(const int64_t*)Aop->d_row_ptr.ptr, (const int64_t*)Aop->d_blk_voff.ptr,
+                                 (const int64_t*)Aop->d_blk_xoff.ptr, (const int32_t*)Aop->d_blk_nc.ptr,
+                                 (const int64_t*)Aop->d_row_yoff.ptr, (const int32_t*)Aop->d_row_b.ptr};
+                const FusedMv<double, double> F{R, (const double*)Aop->val.ptr, w, (double*)brs.ptr, (const int32_t*)M->P.d_col_prow.ptr};
+                return p32 ? stream_sweeps(M, (const float*)M->LD32.ptr, (const float*)S->val32.ptr, v, z, 3, &F, Aop->max_row_cols, 2)
+                           : stream_sweeps(M, (const double*)M->LD.ptr, (const double*)S->val.ptr, v, z, 0, &F, Aop->max_row_cols, 2);
+            }
+            const int which = kind == kShapeForward ? 1 : 2;
+            return p32 ? stream_sweeps<float, float, double>(M, (const float*)M->LD32.ptr, (const float*)S->val32.ptr, v, z, 3, (const FusedMv<double, double>*)nullptr, 0, which)
+                       : stream_sweeps<double, double, double>(M, (const double*)M->LD.ptr, (const double*)S->val.ptr, v, z, 0, (const FusedMv<double, double>*)nullptr, 0, which);
+        }
+        const float* v = (const float*)bv.ptr;
+        float* z = (float*)bz.ptr;
+        float* w = (float*)bw.ptr;
+        chidg_gpu_matrix* S = nullptr;
+        int s2 = precon_source(M, &S);
+        if (s2) return s2;
+        const bool bf = precision == CHIDG_GPU_MIXED_BF16;
+        if (kind == kShapeMatvec)
+            return bf ? matvec_launch<__nv_bfloat16, float>(Aop, (const __nv_bfloat16*)Aop->val16.ptr, z, w, nullptr, 1.0, 0.0, (double*)brs.ptr)
+                      : matvec_launch<float, float>(Aop, (const float*)Aop->val32.ptr, z, w, nullptr, 1.0, 0.0, (double*)brs.ptr);
+        if (kind == kShapeBackwardMv) {
+            if (M->kind != CHIDG_PRECON_ILU0 && M->kind != CHIDG_PRECON_JACOBI) return 1;
+            if (S != Aop || M->P.n_ext != Aop->n || M->P.nprow != Aop->nrow || !Aop->rows_contiguous) return 1;
+            if ((s2 = build_bwd_mv_tasks(M, Aop, fused_mv_lag()))) return s2;
+            MatvecRowsView R{(const int64_t*)Aop->d_row_ptr.ptr, (const int64_t*)Aop->d_blk_voff.ptr,
+                             (const int64_t*)Aop->d_blk_xoff.ptr, (const int32_t*)Aop->d_blk_nc.ptr,
+                             (const int64_t*)Aop->d_row_yoff.ptr, (const int32_t*)Aop->d_row_b.ptr};
+            if (bf) {
+                const FusedMv<__nv_bfloat16, float> F{R, (const __nv_bfloat16*)Aop->val16.ptr, w, (double*)brs.ptr, (const int32_t*)M->P.d_col_prow.ptr};
+                return stream_sweeps(M, (const __nv_bfloat16*)M->LD16.ptr, (const __nv_bfloat16*)S->val16.ptr, v, z, 2, &F, Aop->max_row_cols, 2);
+            }
+            const FusedMv<float, float> F{R, (const float*)Aop->val32.ptr, w, (double*)brs.ptr, (const int32_t*)M->P.d_col_prow.ptr};
+            return stream_sweeps(M, (const float*)M->LD32.ptr, (const float*)S->val32.ptr, v, z, 1, &F, Aop->max_row_cols, 2);
+        }
+        const int which = kind == kShapeForward ? 1 : 2;
+        return bf ? stream_sweeps<__nv_bfloat16, __nv_bfloat16, float>(M, (const __nv_bfloat16*)M->LD16.ptr, (const __nv_bfloat16*)S->val16.ptr, v, z, 2, (const FusedMv<double, float>*)nullptr, 0, which)
+                  : stream_sweeps<float, float, float>(M, (const float*)M->LD32.ptr, (const float*)S->val32.ptr, v, z, 1, (const FusedMv<double, float>*)nullptr, 0, which);
+    };
+    for (int kind = 0; kind < kShapeKinds && st == CHIDG_GPU_OK; ++kind) {
+        const int max_b = kind == kShapeMatvec ? Aop->max_b : M->P.max_b;
+        const int esz = kind == kShapeMatvec ? esz_matvec : esz_blocks;
+        if (kind == kShapeMatvec && (Aop->max_b > SS_MAX_B || !Aop->rows_contiguous)) continue;
+        const StreamShape keep = stream_shape_for(kind, max_b, esz);
+        StreamShape best = keep;
+        float best_ms = 1e30f;
+        bool any = false;
+        for (const StreamShape& cand : shape_candidates(std::max(max_b, kind == kShapeBackwardMv ? Aop->max_b : 0), esz)) {
+            set_stream_shape(kind, max_b, esz, cand);
+            int s2 = run_kind(kind);                              // warm-up (and the shared-memory limit)
+            if (s2 == 1) break;                                   // this kind does not apply here
+            if (s2 == CHIDG_GPU_EINVAL) { ctx->err.clear(); continue; }   // does not fit an SM
+            if (s2) { st = s2; break; }
+            cudaEventRecord(e0, ctx->stream);
+            for (int r = 0; r < reps && !s2; ++r) s2 = run_kind(kind);
+            cudaEventRecord(e1, ctx->stream);
+            if (s2) { st = s2; break; }
+            const cudaError_t e = cudaEventSynchronize(e1);
+            if (e != cudaSuccess) { st = cuda_fail(ctx, e, "autotune"); break; }
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            any = true;
+            if (ms < best_ms) { best_ms = ms; best = cand; }
+        }
+        set_stream_shape(kind, max_b, esz, any ? best : keep);
+    }
+    ctx->profiling = prof;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st == CHIDG_GPU_OK) {
+        double w = 0.0;
+        if ((st = fetch_scalars(ctx, kSlotStatus, 1, &w)) == CHIDG_GPU_OK) st = status_word(ctx, w);
+    }
+    cleanup();
+    return st;
+}
+
+extern "C" int chidg_gpu_stream_shape_get(int32_t kind, int32_t max_b, int32_t value_bytes, int32_t* warps, int32_t* stages,
+                                          int32_t* stage_bytes) {
+    if (kind < 0 || kind >= kShapeKinds || max_b < 1 || max_b > SS_MAX_B || !warps || !stages || !stage_bytes ||
+        (value_bytes != 8 && value_bytes != 4 && value_bytes != 2))
+        return CHIDG_GPU_EINVAL;
+    const StreamShape sh = stream_shape_for(kind, max_b, value_bytes);
+    *warps = sh.cw;
+    *stages = sh.nstage;
+    *stage_bytes = sh.stage_bytes;
+    return CHIDG_GPU_OK;
+}
+
+extern "C" int chidg_gpu_stream_shape_set(int32_t kind, int32_t max_b, int32_t value_bytes, int32_t warps, int32_t stages,
+                                          int32_t stage_bytes) {
+    if (kind < 0 || kind >= kShapeKinds || max_b < 1 || max_b > SS_MAX_B ||
+        (value_bytes != 8 && value_bytes != 4 && value_bytes != 2) || (warps != 4 && warps != 8 && warps != 16) ||
+        stages < 2 || stages > SS_MAX_STAGES || stage_bytes < 2048 || stage_bytes > 96 * 1024 || stage_bytes % 16 != 0)
+        return CHIDG_GPU_EINVAL;
+    set_stream_shape(kind, max_b, value_bytes, StreamShape{warps, stages, stage_bytes});
     return CHIDG_GPU_OK;
 }

@@ -356,6 +356,23 @@ int chidg_gpu_fgmres_default_opts(chidg_gpu_fgmres_opts* opts);
  * did (3: both detected).  The context stays usable. */
 int chidg_gpu_selftest_bounded_waits(chidg_gpu_ctx* ctx, int64_t limit_cycles, int32_t* bits);
 
+/* ---- launch shapes of the streamed kernels and their autotuner ------------- */
+/* No counterpart in the reference (its loops have no launch shapes).  The
+ * streamed kernels (forward sweep, backward sweep, backward sweep with
+ * FGMRES's following matvec rows, matvec) each run with a shape: consumer
+ * warps (4, 8, 16), ring stages (2..8) and bytes per stage, kept per kernel
+ * kind, block-size class (largest block <= 64, 160, 384, 1024 rows) and value
+ * width (8, 4, 2 bytes).  chidg_gpu_autotune times every candidate shape of
+ * the four kinds on M (updated for A in `precision`, streamed schedule) and A,
+ * `reps` runs each, and keeps the fastest in the table for this process; the
+ * get / set calls let a host layer persist the table.  Kinds: 0 forward
+ * sweep, 1 backward sweep, 2 backward sweep with matvec rows, 3 matvec. */
+int chidg_gpu_autotune(chidg_gpu_precon* M, chidg_gpu_matrix* A, int32_t precision, int32_t reps);
+int chidg_gpu_stream_shape_get(int32_t kind, int32_t max_b, int32_t value_bytes, int32_t* warps, int32_t* stages,
+                               int32_t* stage_bytes);
+int chidg_gpu_stream_shape_set(int32_t kind, int32_t max_b, int32_t value_bytes, int32_t warps, int32_t stages,
+                               int32_t stage_bytes);
+
 typedef struct chidg_gpu_server chidg_gpu_server;
 int chidg_gpu_serve_create(int device, int32_t slots, int64_t mem_budget, int32_t max_batch,
                            int32_t precon_kind, const chidg_gpu_fgmres_opts* opts, chidg_gpu_server** out);

@@ -387,6 +387,23 @@ module chidg_gpu_mod
             real(c_double)                :: hist(*)
             integer(c_int32_t), value     :: hist_cap
         end function
+        ! ---- launch shapes of the streamed kernels and their autotuner --------
+        integer(c_int) function chidg_gpu_autotune(M, mat, precision, reps) bind(c, name='chidg_gpu_autotune')
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr),        value :: M, mat
+            integer(c_int32_t), value :: precision, reps
+        end function
+        integer(c_int) function chidg_gpu_stream_shape_get(kind, max_b, value_bytes, warps, stages, stage_bytes) &
+                bind(c, name='chidg_gpu_stream_shape_get')
+            import :: c_int, c_int32_t
+            integer(c_int32_t), value :: kind, max_b, value_bytes
+            integer(c_int32_t)        :: warps, stages, stage_bytes
+        end function
+        integer(c_int) function chidg_gpu_stream_shape_set(kind, max_b, value_bytes, warps, stages, stage_bytes) &
+                bind(c, name='chidg_gpu_stream_shape_set')
+            import :: c_int, c_int32_t
+            integer(c_int32_t), value :: kind, max_b, value_bytes, warps, stages, stage_bytes
+        end function
         ! ---- request server ----------------------------------------------------
         integer(c_int) function chidg_gpu_serve_create(device, slots, mem_budget, max_batch, precon_kind, opts, srv) &
                 bind(c, name='chidg_gpu_serve_create')
