@@ -37,16 +37,21 @@ constexpr double kGamma = 1.4;          // mod_fluid.f90:10
 constexpr double kRgas = 287.15;        // mod_fluid.f90:9
 constexpr double kRkTol = 20.0 * 2.220446049250313e-16;   // RKTOL, mod_constants.f90:241
 constexpr double kFixEps = 0.01;        // entropy-fix width, euler_roe_operator.f90
-constexpr int kMaxOrder = 2;
+constexpr int kMaxOrder = 3;
 constexpr int kThreads = 256;
 
-// Legendre degrees (xi, eta, zeta) of the first 27 modes in the reference's
+// Legendre degrees (xi, eta, zeta) of the first 64 modes in the reference's
 // order (mod_ordering.f90, xi/eta/zeta_order_3d, 0-based); each prefix of
 // (P+1)^3 modes is the full order-P set.
-constexpr int kModes[27][3] = {
+constexpr int kModes[64][3] = {
     {0, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 0}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}, {0, 2, 0},
     {0, 0, 2}, {2, 0, 0}, {0, 2, 1}, {0, 1, 2}, {1, 2, 0}, {1, 0, 2}, {2, 1, 0}, {2, 0, 1}, {0, 2, 2},
-    {1, 2, 1}, {1, 1, 2}, {2, 2, 0}, {2, 0, 2}, {2, 1, 1}, {1, 2, 2}, {2, 2, 1}, {2, 1, 2}, {2, 2, 2}};
+    {1, 2, 1}, {1, 1, 2}, {2, 2, 0}, {2, 0, 2}, {2, 1, 1}, {1, 2, 2}, {2, 2, 1}, {2, 1, 2}, {2, 2, 2},
+    {3, 0, 0}, {0, 3, 0}, {0, 0, 3}, {3, 1, 0}, {3, 0, 1}, {1, 3, 0}, {1, 0, 3}, {0, 3, 1}, {0, 1, 3},
+    {3, 2, 0}, {3, 0, 2}, {3, 1, 1}, {2, 3, 0}, {2, 0, 3}, {1, 3, 1}, {1, 1, 3}, {0, 3, 2}, {0, 2, 3},
+    {3, 2, 1}, {3, 1, 2}, {3, 3, 0}, {3, 0, 3}, {2, 3, 1}, {2, 1, 3}, {1, 3, 2}, {1, 2, 3}, {0, 3, 3},
+    {3, 2, 2}, {3, 3, 1}, {3, 1, 3}, {2, 3, 2}, {2, 2, 3}, {1, 3, 3}, {3, 3, 2}, {3, 2, 3}, {2, 3, 3},
+    {3, 3, 3}};
 
 // ---- forward-mode dual numbers ------------------------------------------------
 template <int N>
@@ -255,9 +260,118 @@ __device__ __forceinline__ int neighbour(const BoxGeom& g, int e, int face) {
 }
 
 // Shared memory (doubles): U[7][5 nt] | WF[qv][3][5] | WdF[qv][3][5][5] |
-// FI[6][qf][5] | Fs[6][qf][5][5] | Fn[6][qf][5][5]
+// FI[6][qf][5] | Fs[6][qf][5][5] | Fn[6][qf][5][5].  At P3 the volume data
+// and the face data do not fit together: the element runs a volume pass and
+// then a face pass over the same space after U (two_pass below).
+__host__ __device__ constexpr bool two_pass(int nt) { return nt > 27; }
 __host__ __device__ inline size_t smem_doubles(int nt, int qv, int qf) {
-    return (size_t)7 * 5 * nt + (size_t)qv * 15 + (size_t)qv * 75 + (size_t)6 * qf * 5 + (size_t)12 * qf * 25;
+    const size_t vol = (size_t)qv * 15 + (size_t)qv * 75, face = (size_t)6 * qf * 5 + (size_t)12 * qf * 25;
+    return (size_t)7 * 5 * nt + (two_pass(nt) ? (vol > face ? vol : face) : vol + face);
+}
+
+// the pointwise data of volume node t (flux and its 5x5 derivatives, weighted)
+template <int NT>
+__device__ __forceinline__ void volume_node(const Tables& tb, const double* sU, int t, int nt, double* sWF, double* sWdF) {
+    const int b = 5 * nt;
+    Dual<5> Q[5];
+#pragma unroll
+    for (int f = 0; f < 5; ++f) {
+        double s = 0.0;
+        for (int m = 0; m < nt; ++m) s += tb.phi[t * nt + m] * sU[6 * b + f * nt + m];
+        Q[f] = mk<5>(s);
+        Q[f].d[f] = 1.0;
+    }
+    const double w = tb.wv[t];
+    for (int d = 0; d < 3; ++d) {
+        Dual<5> F[5];
+        flux_dir(Q, d, F);
+#pragma unroll
+        for (int f = 0; f < 5; ++f) {
+            sWF[(t * 3 + d) * 5 + f] = w * F[f].v;
+#pragma unroll
+            for (int gg = 0; gg < 5; ++gg) sWdF[((t * 3 + d) * 5 + f) * 5 + gg] = w * F[f].d[gg];
+        }
+    }
+}
+
+// the pointwise data of face node qq of face `face` (integrand and its
+// derivatives with respect to the own and the neighbour's state, weighted)
+template <int NT>
+__device__ __forceinline__ void face_node(const BoxGeom& g, const Tables& tb, const double* sU, const int* nbr, int face,
+                                          int qq, int nt, double* sFI, double* sFs, double* sFn) {
+    const int b = 5 * nt, qf = g.qf;
+    const int d = face >> 1;
+    const double s = (face & 1) ? 1.0 : -1.0;
+    const double a = g.area[d];
+    double n[3] = {0.0, 0.0, 0.0};
+    n[d] = s;
+    const double w = tb.wf[qq];
+    const double* pm = tb.phif + ((size_t)face * qf + qq) * nt;
+    double Qm0[5], Qp0[5];
+#pragma unroll
+    for (int f = 0; f < 5; ++f) {
+        double sm_ = 0.0;
+        for (int m = 0; m < nt; ++m) sm_ += pm[m] * sU[6 * b + f * nt + m];
+        Qm0[f] = sm_;
+    }
+    double* FI = sFI + ((size_t)face * qf + qq) * 5;
+    double* Fs = sFs + ((size_t)face * qf + qq) * 25;
+    double* Fn = sFn + ((size_t)face * qf + qq) * 25;
+    if (nbr[face] >= 0) {
+        const double* pp = tb.phif + ((size_t)(face ^ 1) * qf + qq) * nt;
+#pragma unroll
+        for (int f = 0; f < 5; ++f) {
+            double sp_ = 0.0;
+            for (int m = 0; m < nt; ++m) sp_ += pp[m] * sU[face * b + f * nt + m];
+            Qp0[f] = sp_;
+        }
+        // two passes: derivatives with respect to the own state, then the neighbour's
+        for (int side = 0; side < 2; ++side) {
+            Dual<5> Qm[5], Qp[5];
+#pragma unroll
+            for (int f = 0; f < 5; ++f) {
+                Qm[f] = mk<5>(Qm0[f]);
+                Qp[f] = mk<5>(Qp0[f]);
+                if (side == 0) Qm[f].d[f] = 1.0; else Qp[f].d[f] = 1.0;
+            }
+            Dual<5> Fm[5], Fp[5], up[5];
+            flux_dir(Qm, d, Fm);
+            flux_dir(Qp, d, Fp);
+            roe_upwind(Qm, Qp, n, up);
+            double* dst = side == 0 ? Fs : Fn;
+#pragma unroll
+            for (int f = 0; f < 5; ++f) {
+                const Dual<5> I = (0.5 * s * a) * (Fm[f] + Fp[f]) + a * up[f];
+                if (side == 0) FI[f] = w * I.v;
+#pragma unroll
+                for (int gg = 0; gg < 5; ++gg) dst[f * 5 + gg] = w * I.d[gg];
+            }
+        }
+    } else {
+        Dual<5> Qm[5], Qb[5];
+#pragma unroll
+        for (int f = 0; f < 5; ++f) {
+            Qm[f] = mk<5>(Qm0[f]);
+            Qm[f].d[f] = 1.0;
+        }
+        if (g.bc[face] == CHIDG_EULER_FARFIELD) {
+            farfield_state(Qm, n, g.fs, Qb);
+        } else {
+#pragma unroll
+            for (int f = 0; f < 5; ++f) Qb[f] = Qm[f];
+        }
+        Dual<5> F[5];
+        flux_dir(Qb, d, F);
+#pragma unroll
+        for (int f = 0; f < 5; ++f) {
+            FI[f] = w * s * a * F[f].v;
+#pragma unroll
+            for (int gg = 0; gg < 5; ++gg) {
+                Fs[f * 5 + gg] = w * s * a * F[f].d[gg];
+                Fn[f * 5 + gg] = 0.0;
+            }
+        }
+    }
 }
 
 template <int NT>
@@ -267,10 +381,12 @@ __global__ void __launch_bounds__(kThreads) k_euler_assemble(BoxGeom g, Tables t
     extern __shared__ double sm[];
     const int e = blockIdx.x;
     const int nt = NT, b = 5 * NT, qv = g.qv, qf = g.qf;
+    constexpr bool TWO = two_pass(NT);
     double* sU = sm;                            // [7][5 nt]: own (slot 6) and face neighbours (slots 0..5)
     double* sWF = sU + 7 * 5 * nt;              // [qv][3][5]
     double* sWdF = sWF + (size_t)qv * 15;       // [qv][3][5][5]
-    double* sFI = sWdF + (size_t)qv * 75;       // [6][qf][5]
+    // face data after the volume data, or over it in the two-pass form
+    double* sFI = TWO ? sWF : sWdF + (size_t)qv * 75;   // [6][qf][5]
     double* sFs = sFI + (size_t)6 * qf * 5;     // [6][qf][5][5]  d integrand / d own state
     double* sFn = sFs + (size_t)6 * qf * 25;    // [6][qf][5][5]  d integrand / d neighbour state
     int nbr[6];
@@ -285,189 +401,192 @@ __global__ void __launch_bounds__(kThreads) k_euler_assemble(BoxGeom g, Tables t
     }
     __syncthreads();
 
-    // 2. pointwise data at volume nodes and face nodes
-    for (int t = threadIdx.x; t < qv + 6 * qf; t += blockDim.x) {
-        if (t < qv) {
-            Dual<5> Q[5];
-#pragma unroll
-            for (int f = 0; f < 5; ++f) {
-                double s = 0.0;
-                for (int m = 0; m < nt; ++m) s += tb.phi[t * nt + m] * sU[6 * b + f * nt + m];
-                Q[f] = mk<5>(s);
-                Q[f].d[f] = 1.0;
-            }
-            const double w = tb.wv[t];
-            for (int d = 0; d < 3; ++d) {
-                Dual<5> F[5];
-                flux_dir(Q, d, F);
-#pragma unroll
-                for (int f = 0; f < 5; ++f) {
-                    sWF[(t * 3 + d) * 5 + f] = w * F[f].v;
-#pragma unroll
-                    for (int gg = 0; gg < 5; ++gg) sWdF[((t * 3 + d) * 5 + f) * 5 + gg] = w * F[f].d[gg];
-                }
-            }
-        } else {
-            const int u = t - qv, face = u / qf, qq = u - face * qf;
-            const int d = face >> 1;
-            const double s = (face & 1) ? 1.0 : -1.0;
-            const double a = g.area[d];
-            double n[3] = {0.0, 0.0, 0.0};
-            n[d] = s;
-            const double w = tb.wf[qq];
-            const double* pm = tb.phif + ((size_t)face * qf + qq) * nt;
-            double Qm0[5], Qp0[5];
-#pragma unroll
-            for (int f = 0; f < 5; ++f) {
-                double sm_ = 0.0;
-                for (int m = 0; m < nt; ++m) sm_ += pm[m] * sU[6 * b + f * nt + m];
-                Qm0[f] = sm_;
-            }
-            double* FI = sFI + ((size_t)face * qf + qq) * 5;
-            double* Fs = sFs + ((size_t)face * qf + qq) * 25;
-            double* Fn = sFn + ((size_t)face * qf + qq) * 25;
-            if (nbr[face] >= 0) {
-                const double* pp = tb.phif + ((size_t)(face ^ 1) * qf + qq) * nt;
-#pragma unroll
-                for (int f = 0; f < 5; ++f) {
-                    double sp_ = 0.0;
-                    for (int m = 0; m < nt; ++m) sp_ += pp[m] * sU[face * b + f * nt + m];
-                    Qp0[f] = sp_;
-                }
-                // two passes: derivatives with respect to the own state, then the neighbour's
-                for (int side = 0; side < 2; ++side) {
-                    Dual<5> Qm[5], Qp[5];
-#pragma unroll
-                    for (int f = 0; f < 5; ++f) {
-                        Qm[f] = mk<5>(Qm0[f]);
-                        Qp[f] = mk<5>(Qp0[f]);
-                        if (side == 0) Qm[f].d[f] = 1.0; else Qp[f].d[f] = 1.0;
-                    }
-                    Dual<5> Fm[5], Fp[5], up[5];
-                    flux_dir(Qm, d, Fm);
-                    flux_dir(Qp, d, Fp);
-                    roe_upwind(Qm, Qp, n, up);
-                    double* dst = side == 0 ? Fs : Fn;
-#pragma unroll
-                    for (int f = 0; f < 5; ++f) {
-                        const Dual<5> I = (0.5 * s * a) * (Fm[f] + Fp[f]) + a * up[f];
-                        if (side == 0) FI[f] = w * I.v;
-#pragma unroll
-                        for (int gg = 0; gg < 5; ++gg) dst[f * 5 + gg] = w * I.d[gg];
-                    }
-                }
-            } else {
-                Dual<5> Qm[5], Qb[5];
-#pragma unroll
-                for (int f = 0; f < 5; ++f) {
-                    Qm[f] = mk<5>(Qm0[f]);
-                    Qm[f].d[f] = 1.0;
-                }
-                if (g.bc[face] == CHIDG_EULER_FARFIELD) {
-                    farfield_state(Qm, n, g.fs, Qb);
-                } else {
-#pragma unroll
-                    for (int f = 0; f < 5; ++f) Qb[f] = Qm[f];
-                }
-                Dual<5> F[5];
-                flux_dir(Qb, d, F);
-#pragma unroll
-                for (int f = 0; f < 5; ++f) {
-                    FI[f] = w * s * a * F[f].v;
-#pragma unroll
-                    for (int gg = 0; gg < 5; ++gg) {
-                        Fs[f * 5 + gg] = w * s * a * F[f].d[gg];
-                        Fn[f * 5 + gg] = 0.0;
-                    }
-                }
+    if constexpr (!TWO) {
+        // 2. pointwise data at volume nodes and face nodes
+        for (int t = threadIdx.x; t < qv + 6 * qf; t += blockDim.x) {
+            if (t < qv) volume_node<NT>(tb, sU, t, nt, sWF, sWdF);
+            else {
+                const int u = t - qv, face = u / qf, qq = u - face * qf;
+                face_node<NT>(g, tb, sU, nbr, face, qq, nt, sFI, sFs, sFn);
             }
         }
-    }
-    __syncthreads();
+        __syncthreads();
 
-    // 3. residual: R[f, m] = -sum_q sum_d grad_d[q, m] WF[q, d, f] + sum_faces sum_q phif[q, m] FI[q, f]
-    for (int t = threadIdx.x; t < b; t += blockDim.x) {
-        const int f = t / nt, m = t - f * nt;
-        double r = 0.0;
-        for (int qq = 0; qq < qv; ++qq)
-            r -= tb.grad[(0 * qv + qq) * nt + m] * sWF[(qq * 3 + 0) * 5 + f]
-               + tb.grad[(1 * qv + qq) * nt + m] * sWF[(qq * 3 + 1) * 5 + f]
-               + tb.grad[(2 * qv + qq) * nt + m] * sWF[(qq * 3 + 2) * 5 + f];
-        for (int face = 0; face < 6; ++face)
-            for (int qq = 0; qq < qf; ++qq)
-                r += tb.phif[((size_t)face * qf + qq) * nt + m] * sFI[((size_t)face * qf + qq) * 5 + f];
-        rhs[(int64_t)e * b + t] = r;
-    }
+        // 3. residual: R[f, m] = -sum_q sum_d grad_d[q, m] WF[q, d, f] + sum_faces sum_q phif[q, m] FI[q, f]
+        for (int t = threadIdx.x; t < b; t += blockDim.x) {
+            const int f = t / nt, m = t - f * nt;
+            double r = 0.0;
+            for (int qq = 0; qq < qv; ++qq)
+                r -= tb.grad[(0 * qv + qq) * nt + m] * sWF[(qq * 3 + 0) * 5 + f]
+                   + tb.grad[(1 * qv + qq) * nt + m] * sWF[(qq * 3 + 1) * 5 + f]
+                   + tb.grad[(2 * qv + qq) * nt + m] * sWF[(qq * 3 + 2) * 5 + f];
+            for (int face = 0; face < 6; ++face)
+                for (int qq = 0; qq < qf; ++qq)
+                    r += tb.phif[((size_t)face * qf + qq) * nt + m] * sFI[((size_t)face * qf + qq) * 5 + f];
+            rhs[(int64_t)e * b + t] = r;
+        }
 
-    // 4. DIAG block and 5. face blocks (skipped for a residual-only call): one
-    // thread per pair of (f, m, g) rows with the same f and g and modes m0,
-    // m0 + 1, all nt columns n of both in registers, so each basis value
-    // loaded feeds two FMAs; block entry (f nt + m, g nt + n) stored
-    // column-major.  Lanes of a warp take consecutive mode pairs.
-    if (val == nullptr) return;
-    const int npair = (nt + 1) >> 1;
-    for (int blk = 6; blk >= 0; --blk) {
-        if (blk < 6 && nbr[blk] < 0) continue;
-        double* out = val + blk_off[(int64_t)e * 7 + blk];
-        for (int item = threadIdx.x; item < 25 * npair; item += blockDim.x) {
-            const int mp = item % npair, fg = item / npair, f = fg % 5, gg = fg / 5;
-            const int m0 = 2 * mp;
-            const bool two = m0 + 1 < nt;
-            const int m1 = two ? m0 + 1 : m0;
-            double a0[NT], a1[NT];
+        // 4. DIAG block and 5. face blocks (skipped for a residual-only call): one
+        // thread per pair of (f, m, g) rows with the same f and g and modes m0,
+        // m0 + 1, all nt columns n of both in registers, so each basis value
+        // loaded feeds two FMAs; block entry (f nt + m, g nt + n) stored
+        // column-major.  Lanes of a warp take consecutive mode pairs.
+        if (val == nullptr) return;
+        const int npair = (nt + 1) >> 1;
+        for (int blk = 6; blk >= 0; --blk) {
+            if (blk < 6 && nbr[blk] < 0) continue;
+            double* out = val + blk_off[(int64_t)e * 7 + blk];
+            for (int item = threadIdx.x; item < 25 * npair; item += blockDim.x) {
+                const int mp = item % npair, fg = item / npair, f = fg % 5, gg = fg / 5;
+                const int m0 = 2 * mp;
+                const bool two = m0 + 1 < nt;
+                const int m1 = two ? m0 + 1 : m0;
+                double a0[NT], a1[NT];
 #pragma unroll
-            for (int n = 0; n < NT; ++n) { a0[n] = 0.0; a1[n] = 0.0; }
-            if (blk == 6) {
-                for (int qq = 0; qq < qv; ++qq) {
-                    const double w0 = sWdF[((qq * 3 + 0) * 5 + f) * 5 + gg];
-                    const double w1 = sWdF[((qq * 3 + 1) * 5 + f) * 5 + gg];
-                    const double w2 = sWdF[((qq * 3 + 2) * 5 + f) * 5 + gg];
-                    const double* g0 = tb.grad + (size_t)(0 * qv + qq) * nt;
-                    const double* g1 = tb.grad + (size_t)(1 * qv + qq) * nt;
-                    const double* g2 = tb.grad + (size_t)(2 * qv + qq) * nt;
-                    const double t0 = -(g0[m0] * w0 + g1[m0] * w1 + g2[m0] * w2);
-                    const double t1 = -(g0[m1] * w0 + g1[m1] * w1 + g2[m1] * w2);
-                    const double* ph = tb.phi + (size_t)qq * nt;
+                for (int n = 0; n < NT; ++n) { a0[n] = 0.0; a1[n] = 0.0; }
+                if (blk == 6) {
+                    for (int qq = 0; qq < qv; ++qq) {
+                        const double w0 = sWdF[((qq * 3 + 0) * 5 + f) * 5 + gg];
+                        const double w1 = sWdF[((qq * 3 + 1) * 5 + f) * 5 + gg];
+                        const double w2 = sWdF[((qq * 3 + 2) * 5 + f) * 5 + gg];
+                        const double* g0 = tb.grad + (size_t)(0 * qv + qq) * nt;
+                        const double* g1 = tb.grad + (size_t)(1 * qv + qq) * nt;
+                        const double* g2 = tb.grad + (size_t)(2 * qv + qq) * nt;
+                        const double t0 = -(g0[m0] * w0 + g1[m0] * w1 + g2[m0] * w2);
+                        const double t1 = -(g0[m1] * w0 + g1[m1] * w1 + g2[m1] * w2);
+                        const double* ph = tb.phi + (size_t)qq * nt;
 #pragma unroll
-                    for (int n = 0; n < NT; ++n) {
-                        const double p = ph[n];
-                        a0[n] += t0 * p;
-                        a1[n] += t1 * p;
+                        for (int n = 0; n < NT; ++n) {
+                            const double p = ph[n];
+                            a0[n] += t0 * p;
+                            a1[n] += t1 * p;
+                        }
                     }
-                }
-                for (int face = 0; face < 6; ++face) {
+                    for (int face = 0; face < 6; ++face) {
+                        for (int qq = 0; qq < qf; ++qq) {
+                            const double* pf = tb.phif + ((size_t)face * qf + qq) * nt;
+                            const double w = sFs[((size_t)face * qf + qq) * 25 + f * 5 + gg];
+                            const double t0 = pf[m0] * w, t1 = pf[m1] * w;
+#pragma unroll
+                            for (int n = 0; n < NT; ++n) {
+                                const double p = pf[n];
+                                a0[n] += t0 * p;
+                                a1[n] += t1 * p;
+                            }
+                        }
+                    }
+                } else {
                     for (int qq = 0; qq < qf; ++qq) {
-                        const double* pf = tb.phif + ((size_t)face * qf + qq) * nt;
-                        const double w = sFs[((size_t)face * qf + qq) * 25 + f * 5 + gg];
+                        const double* pf = tb.phif + ((size_t)blk * qf + qq) * nt;
+                        const double* pn = tb.phif + ((size_t)(blk ^ 1) * qf + qq) * nt;
+                        const double w = sFn[((size_t)blk * qf + qq) * 25 + f * 5 + gg];
                         const double t0 = pf[m0] * w, t1 = pf[m1] * w;
 #pragma unroll
                         for (int n = 0; n < NT; ++n) {
-                            const double p = pf[n];
+                            const double p = pn[n];
                             a0[n] += t0 * p;
                             a1[n] += t1 * p;
                         }
                     }
                 }
-            } else {
-                for (int qq = 0; qq < qf; ++qq) {
-                    const double* pf = tb.phif + ((size_t)blk * qf + qq) * nt;
-                    const double* pn = tb.phif + ((size_t)(blk ^ 1) * qf + qq) * nt;
-                    const double w = sFn[((size_t)blk * qf + qq) * 25 + f * 5 + gg];
-                    const double t0 = pf[m0] * w, t1 = pf[m1] * w;
+                const int row = f * nt + m0;
 #pragma unroll
-                    for (int n = 0; n < NT; ++n) {
-                        const double p = pn[n];
-                        a0[n] += t0 * p;
-                        a1[n] += t1 * p;
-                    }
+                for (int n = 0; n < NT; ++n) {
+                    double* col = out + (int64_t)(gg * nt + n) * b + row;
+                    col[0] = a0[n];
+                    if (two) col[1] = a1[n];
                 }
             }
-            const int row = f * nt + m0;
+        }
+    } else {
+        // Two passes over the same shared memory.  Every value is accumulated in
+        // the single-pass order: the volume pass leaves the residual's and the
+        // DIAG block's volume sums in the outputs, and the face pass reloads and
+        // continues them (each output value is read back by the thread that
+        // wrote it).  Block rows: one (f, m, g) row and one half of its nt
+        // columns per item, so the accumulators fit in registers.
+        constexpr int NH = NT / 2;
+        const int64_t* bo = blk_off + (int64_t)e * 7;
+        // ---- volume pass
+        for (int t = threadIdx.x; t < qv; t += blockDim.x) volume_node<NT>(tb, sU, t, nt, sWF, sWdF);
+        __syncthreads();
+        for (int t = threadIdx.x; t < b; t += blockDim.x) {
+            const int f = t / nt, m = t - f * nt;
+            double r = 0.0;
+            for (int qq = 0; qq < qv; ++qq)
+                r -= tb.grad[(0 * qv + qq) * nt + m] * sWF[(qq * 3 + 0) * 5 + f]
+                   + tb.grad[(1 * qv + qq) * nt + m] * sWF[(qq * 3 + 1) * 5 + f]
+                   + tb.grad[(2 * qv + qq) * nt + m] * sWF[(qq * 3 + 2) * 5 + f];
+            rhs[(int64_t)e * b + t] = r;
+        }
+        if (val != nullptr) {
+            double* out = val + bo[6];
+            for (int item = threadIdx.x; item < 25 * nt * 2; item += blockDim.x) {
+                const int h = item & 1, m = (item >> 1) % nt, fg = (item >> 1) / nt, f = fg % 5, gg = fg / 5;
+                double a0[NH];
 #pragma unroll
-            for (int n = 0; n < NT; ++n) {
-                double* col = out + (int64_t)(gg * nt + n) * b + row;
-                col[0] = a0[n];
-                if (two) col[1] = a1[n];
+                for (int n = 0; n < NH; ++n) a0[n] = 0.0;
+                for (int qq = 0; qq < qv; ++qq) {
+                    const double w0 = sWdF[((qq * 3 + 0) * 5 + f) * 5 + gg];
+                    const double w1 = sWdF[((qq * 3 + 1) * 5 + f) * 5 + gg];
+                    const double w2 = sWdF[((qq * 3 + 2) * 5 + f) * 5 + gg];
+                    const double t0 = -(tb.grad[(size_t)(0 * qv + qq) * nt + m] * w0 +
+                                        tb.grad[(size_t)(1 * qv + qq) * nt + m] * w1 +
+                                        tb.grad[(size_t)(2 * qv + qq) * nt + m] * w2);
+                    const double* ph = tb.phi + (size_t)qq * nt + h * NH;
+#pragma unroll
+                    for (int n = 0; n < NH; ++n) a0[n] += t0 * ph[n];
+                }
+#pragma unroll
+                for (int n = 0; n < NH; ++n) out[(int64_t)(gg * nt + h * NH + n) * b + f * nt + m] = a0[n];
+            }
+        }
+        __syncthreads();
+        // ---- face pass
+        for (int t = threadIdx.x; t < 6 * qf; t += blockDim.x) {
+            const int face = t / qf, qq = t - face * qf;
+            face_node<NT>(g, tb, sU, nbr, face, qq, nt, sFI, sFs, sFn);
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < b; t += blockDim.x) {
+            const int f = t / nt, m = t - f * nt;
+            double r = rhs[(int64_t)e * b + t];
+            for (int face = 0; face < 6; ++face)
+                for (int qq = 0; qq < qf; ++qq)
+                    r += tb.phif[((size_t)face * qf + qq) * nt + m] * sFI[((size_t)face * qf + qq) * 5 + f];
+            rhs[(int64_t)e * b + t] = r;
+        }
+        if (val == nullptr) return;
+        for (int blk = 6; blk >= 0; --blk) {
+            if (blk < 6 && nbr[blk] < 0) continue;
+            double* out = val + bo[blk];
+            for (int item = threadIdx.x; item < 25 * nt * 2; item += blockDim.x) {
+                const int h = item & 1, m = (item >> 1) % nt, fg = (item >> 1) / nt, f = fg % 5, gg = fg / 5;
+                double a0[NH];
+                double* dst = out + (int64_t)(gg * nt + h * NH) * b + f * nt + m;
+                if (blk == 6) {
+#pragma unroll
+                    for (int n = 0; n < NH; ++n) a0[n] = dst[(int64_t)n * b];
+                    for (int face = 0; face < 6; ++face)
+                        for (int qq = 0; qq < qf; ++qq) {
+                            const double* pf = tb.phif + ((size_t)face * qf + qq) * nt;
+                            const double t0 = pf[m] * sFs[((size_t)face * qf + qq) * 25 + f * 5 + gg];
+#pragma unroll
+                            for (int n = 0; n < NH; ++n) a0[n] += t0 * pf[h * NH + n];
+                        }
+                } else {
+#pragma unroll
+                    for (int n = 0; n < NH; ++n) a0[n] = 0.0;
+                    for (int qq = 0; qq < qf; ++qq) {
+                        const double* pf = tb.phif + ((size_t)blk * qf + qq) * nt;
+                        const double* pn = tb.phif + ((size_t)(blk ^ 1) * qf + qq) * nt + h * NH;
+                        const double t0 = pf[m] * sFn[((size_t)blk * qf + qq) * 25 + f * 5 + gg];
+#pragma unroll
+                        for (int n = 0; n < NH; ++n) a0[n] += t0 * pn[n];
+                    }
+                }
+#pragma unroll
+                for (int n = 0; n < NH; ++n) dst[(int64_t)n * b] = a0[n];
             }
         }
     }
@@ -556,7 +675,7 @@ extern "C" int chidg_gpu_euler_create(chidg_gpu_ctx* ctx, const chidg_gpu_euler_
     if (!ctx || !box || !out) return CHIDG_GPU_EINVAL;
     *out = nullptr;
     if (box->nx < 1 || box->ny < 1 || box->nz < 1 || box->order < 0 || box->order > kMaxOrder)
-        return fail(ctx, CHIDG_GPU_EINVAL, "euler_create: box sizes must be >= 1 and order 0..2");
+        return fail(ctx, CHIDG_GPU_EINVAL, "euler_create: box sizes must be >= 1 and order 0..3");
     for (int d = 0; d < 3; ++d)
         if (!(box->hi[d] > box->lo[d])) return fail(ctx, CHIDG_GPU_EINVAL, "euler_create: empty extent");
     for (int f = 0; f < 6; ++f)
@@ -650,7 +769,7 @@ extern "C" int chidg_gpu_euler_create(chidg_gpu_ctx* ctx, const chidg_gpu_euler_
     const size_t smem = smem_doubles(nt, qv, qf) * sizeof(double);
     if (!st) {
         const void* fn = P == 0 ? (const void*)k_euler_assemble<1> : P == 1 ? (const void*)k_euler_assemble<8>
-                                                                            : (const void*)k_euler_assemble<27>;
+                         : P == 2 ? (const void*)k_euler_assemble<27> : (const void*)k_euler_assemble<64>;
         st = raise_smem_limit(fn, smem);
     }
     if (st) {
@@ -748,7 +867,8 @@ extern "C" int chidg_gpu_euler_assemble(chidg_gpu_euler* E, chidg_gpu_vector* q,
     const dim3 grid(E->nelem), block(kThreads);
     if (P == 0) k_euler_assemble<1><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, (const double*)q->buf.ptr, (double*)rhs->buf.ptr, val, off);
     else if (P == 1) k_euler_assemble<8><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, (const double*)q->buf.ptr, (double*)rhs->buf.ptr, val, off);
-    else k_euler_assemble<27><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, (const double*)q->buf.ptr, (double*)rhs->buf.ptr, val, off);
+    else if (P == 2) k_euler_assemble<27><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, (const double*)q->buf.ptr, (double*)rhs->buf.ptr, val, off);
+    else k_euler_assemble<64><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, (const double*)q->buf.ptr, (double*)rhs->buf.ptr, val, off);
     st = check_launch(E->ctx, "k_euler_assemble");
     if (st) return st;
     if (jac) A->stamp++;
@@ -767,7 +887,8 @@ extern "C" int chidg_gpu_euler_pseudo_timestep(chidg_gpu_euler* E, chidg_gpu_vec
     double* out = (double*)E->dtau.ptr;
     if (E->order == 0) k_euler_dtau<1><<<grid, block, 0, E->ctx->stream>>>(E->g, tb, qp, E->h, cfl[0], cfl[1], cfl[2], cfl[3], cfl[4], out);
     else if (E->order == 1) k_euler_dtau<8><<<grid, block, 0, E->ctx->stream>>>(E->g, tb, qp, E->h, cfl[0], cfl[1], cfl[2], cfl[3], cfl[4], out);
-    else k_euler_dtau<27><<<grid, block, 0, E->ctx->stream>>>(E->g, tb, qp, E->h, cfl[0], cfl[1], cfl[2], cfl[3], cfl[4], out);
+    else if (E->order == 2) k_euler_dtau<27><<<grid, block, 0, E->ctx->stream>>>(E->g, tb, qp, E->h, cfl[0], cfl[1], cfl[2], cfl[3], cfl[4], out);
+    else k_euler_dtau<64><<<grid, block, 0, E->ctx->stream>>>(E->g, tb, qp, E->h, cfl[0], cfl[1], cfl[2], cfl[3], cfl[4], out);
     st = check_launch(E->ctx, "k_euler_dtau");
     if (st) return st;
     cudaError_t ce = cudaMemcpyAsync(dtau, out, (size_t)E->nelem * 5 * sizeof(double), cudaMemcpyDeviceToHost,

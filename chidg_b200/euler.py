@@ -603,15 +603,15 @@ class EulerSystem:
 class EulerDevice:
     """The same discretisation assembled on the GPU (chidg_gpu_euler_*): the
     residual into a device vector and the Jacobian straight into the device
-    matrix's blocks, orders 0..2.  The extent, boundary conditions and
+    matrix's blocks, orders 0..3.  The extent, boundary conditions and
     freestream are the EulerBox's."""
 
     def __init__(self, box: EulerBox, ctx: api.Context | None = None):
         import ctypes as C
 
         from . import _lib
-        if box.order > 2:
-            raise ValueError("EulerDevice: orders 0..2")
+        if box.order > 3:
+            raise ValueError("EulerDevice: orders 0..3")
         self.box = box
         self.ctx = ctx or api.default_context()
         d = _lib.EulerBoxDesc()

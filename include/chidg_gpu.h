@@ -393,7 +393,7 @@ int chidg_gpu_serve_destroy(chidg_gpu_server* s);
  * device: rhs = R(q) as the reference stores it (volume integrals negated,
  * face integrals added, mod_integrate.f90:652-1022), and the Jacobian dR/dq
  * into the DIAG and interior-face blocks of a matrix holding exactly the box
- * pattern (one time level, 5 fields, (P+1)^3 modes).  Orders 0..2; modal
+ * pattern (one time level, 5 fields, (P+1)^3 modes).  Orders 0..3; modal
  * Legendre basis in the reference's mode order (mod_ordering.f90),
  * Gauss-Legendre quadrature with ceil(3 (P+1) / 2) nodes per direction
  * (gq_rule = 2).  Not in the reference's C-callable surface: its assembly is

@@ -129,7 +129,8 @@ def test_newton_on_euler_matches_dense(shape, P, amp):
 
 
 DEVICE_CASES = [((3, 2, 2), 0, "farfield"), ((4, 3, 2), 1, "farfield"), ((3, 3, 2), 2, "farfield"),
-                ((3, 2, 2), 1, ["farfield", "extrapolate"] * 3), ((2, 2, 3), 2, "extrapolate"), ((1, 1, 1), 1, "farfield")]
+                ((3, 2, 2), 1, ["farfield", "extrapolate"] * 3), ((2, 2, 3), 2, "extrapolate"), ((1, 1, 1), 1, "farfield"),
+                ((3, 2, 2), 3, "farfield"), ((2, 2, 2), 3, ["extrapolate", "farfield"] * 3)]
 
 
 @pytest.mark.parametrize("shape,P,bcs", DEVICE_CASES)
