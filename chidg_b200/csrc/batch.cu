@@ -74,12 +74,7 @@ __global__ void k_bat_cycle_start(BatState S, BatOpts o, int nsys, const double*
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nsys) return;
     const int m = o.m;
-    double* p = S.p + (size_t)s * (m + 1);
-    double* c = S.c + (size_t)s * (m + 1);
-    double* sn = S.sn + (size_t)s * (m + 1);
-    double* H = S.H + (size_t)s * (m + 1) * m;
-    for (int i = 0; i <= m; ++i) { p[i] = 0.0; c[i] = 0.0; sn[i] = 0.0; }
-    for (int i = 0; i < (m + 1) * m; ++i) H[i] = 0.0;
+    double* p = S.p + (size_t)s * (m + 1);      // p, c, sn and H were cleared by the caller
     S.scale[s] = 0.0;
     S.fin[s] = 0;
     S.member[s] = 0;
@@ -124,61 +119,86 @@ __global__ void k_bat_reorth_test(BatState S, BatOpts o, int nsys, int j) {
     S.reo[s] = crit >= 1.0;
 }
 
-// y = inv(H(1:n,1:n)) p(1:n) into coef (type_fgmres.f90:287-288)
-__device__ int bat_least_squares(BatState& S, const BatOpts& o, int s, int n) {
-    const int m = o.m;
+// y = inv(H(1:n,1:n)) p(1:n) into coef (type_fgmres.f90:287-288) for every
+// system with fin set, n = nvecs: one warp per system.  Gauss-Jordan with
+// partial pivoting on a copy of H (mod_inv::inv semantics, as the host
+// solver's explicit inverse): row p is the pivot row of column k, the first
+// unused row of largest magnitude; rows are never swapped and the permutation
+// is undone when y is formed.  The lanes split the rows (or the columns) of
+// each update; every entry is computed as the one-thread loop computes it.
+__global__ void k_bat_lsq(BatState S, BatOpts o, int nsys) {
+    const int s = blockIdx.x;
+    if (s >= nsys || !S.fin[s]) return;
+    const int lane = threadIdx.x;
+    const int m = o.m, n = S.nvecs[s];
     const double* H = S.H + (size_t)s * (m + 1) * m;
     double* a = S.work + (size_t)s * m * m;
     int32_t* piv = S.piv + (size_t)s * 2 * m;
     int32_t* used = piv + m;
-    // Gauss-Jordan with partial pivoting on a copy of H (mod_inv::inv
-    // semantics, as the host solver's explicit inverse): row p is the pivot
-    // row of column k; rows are never swapped, the permutation is undone below
-    for (int jj = 0; jj < n; ++jj)
-        for (int ii = 0; ii < n; ++ii) a[ii + jj * n] = H[ii + jj * (m + 1)];
-    for (int i = 0; i < n; ++i) used[i] = 0;
+    for (int idx = lane; idx < n * n; idx += 32) {
+        const int ii = idx % n, jj = idx / n;
+        a[ii + jj * n] = H[ii + jj * (m + 1)];
+    }
+    for (int i = lane; i < n; i += 32) used[i] = 0;
+    __syncwarp();
     for (int k = 0; k < n; ++k) {
-        int p = -1;
+        // pivot: largest |a(i,k)| over unused rows, NaN as infinity, first on ties
         double best = -1.0;
-        for (int i = 0; i < n; ++i) {
+        int p = n;
+        for (int i = lane; i < n; i += 32) {
             if (used[i]) continue;
             double v = fabs(a[i + k * n]);
             if (!(v == v)) v = INFINITY;
             if (v > best) { best = v; p = i; }
         }
-        piv[k] = p;
-        used[p] = 1;
+        for (int off = 16; off > 0; off >>= 1) {
+            const double ob = __shfl_xor_sync(0xffffffffu, best, off);
+            const int op = __shfl_xor_sync(0xffffffffu, p, off);
+            if (ob > best || (ob == best && op < p)) { best = ob; p = op; }
+        }
         const double pv = a[p + k * n];
-        if (pv == 0.0) return k + 1;
+        __syncwarp();
+        if (pv == 0.0) {
+            if (lane == 0) {
+                S.err[s] = CHIDG_GPU_ESINGULAR;
+                atomicCAS(S.count + 1, 0, s + 1);
+            }
+            return;
+        }
         const double rp = 1.0 / pv;
-        for (int jj = 0; jj < n; ++jj) {
-            const double row = ((jj == k) ? 1.0 : a[p + jj * n]) * rp;
-            if (jj == k) continue;
-            for (int i = 0; i < n; ++i) {
-                if (i == p) continue;
-                a[i + jj * n] = a[i + jj * n] - a[i + k * n] * row;
+        // columns jj != k of the rows i != p, with the old column k and row p
+        for (int i = lane; i < n; i += 32) {
+            if (i == p) continue;
+            const double aik = a[i + k * n];
+            for (int jj = 0; jj < n; ++jj) {
+                if (jj == k) continue;
+                const double row = a[p + jj * n] * rp;
+                a[i + jj * n] = a[i + jj * n] - aik * row;
             }
         }
-        // column k: -col * row(k) with row(k) = rp, rows i != p
-        for (int i = 0; i < n; ++i)
+        __syncwarp();
+        for (int i = lane; i < n; i += 32)
             if (i != p) a[i + k * n] = 0.0 - a[i + k * n] * rp;
-        for (int jj = 0; jj < n; ++jj) a[p + jj * n] = ((jj == k) ? 1.0 : a[p + jj * n]) * rp;
+        __syncwarp();
+        for (int jj = lane; jj < n; jj += 32) a[p + jj * n] = ((jj == k) ? 1.0 : a[p + jj * n]) * rp;
+        if (lane == 0) { piv[k] = p; used[p] = 1; }
+        __syncwarp();
     }
-    // inverse(q[i], piv[jj]) = a(i, jj) with q = piv^-1, so inverse row ii is
-    // a's row piv[ii] and inverse column col is a's column q[col]; y = inverse p
+    // inverse(q[i], piv[jj]) = a(i, jj) with q = piv^-1: inverse row ii is a's
+    // row piv[ii], inverse column col is a's column q[col]; y = inverse p,
     // summed over the columns in order
     int32_t* q = used;
-    for (int k = 0; k < n; ++k) q[piv[k]] = k;
+    for (int k = lane; k < n; k += 32) q[piv[k]] = k;
+    __syncwarp();
     const double* pp = S.p + (size_t)s * (m + 1);
     double* y = S.coef + (size_t)s * o.hst;
-    for (int ii = 0; ii < n; ++ii) {
+    for (int ii = lane; ii < n; ii += 32) {
         const int i = piv[ii];
         double acc = 0.0;
         for (int col = 0; col < n; ++col) acc += a[i + q[col] * n] * pp[col];
         y[ii] = acc;
     }
-    for (int ii = n; ii < o.hst; ++ii) y[ii] = 0.0;
-    return 0;
+    for (int ii = n + lane; ii < o.hst; ii += 32) y[ii] = 0.0;
 }
 
 // h(:, j) from the passes, Givens rotations, the convergence tests and, for a
@@ -230,11 +250,7 @@ __global__ void k_bat_givens(BatState S, BatOpts o, int nsys, int j) {
     const bool crel = res / S.r0init[s] < o.rtol;
     const bool cmax = (it >= o.nmax) && (o.nmax > 0);
     S.scale[s] = inv_h;
-    if (cabs || crel || cmax) {
-        if (bat_least_squares(S, o, s, j) != 0) {
-            S.err[s] = CHIDG_GPU_ESINGULAR;
-            atomicCAS(S.count + 1, 0, s + 1);
-        }
+    if (cabs || crel || cmax) {       // least squares in k_bat_lsq, x update in this step
         S.res_est[s] = res;
         S.active[s] = 0;
         S.fin[s] = 1;
@@ -248,14 +264,9 @@ __global__ void k_bat_cycle_end(BatState S, BatOpts o, int nsys) {
     if (s >= nsys) return;
     S.fin[s] = 0;
     if (!S.active[s] || !S.member[s]) return;
-    if (bat_least_squares(S, o, s, S.nvecs[s]) != 0) {
-        S.err[s] = CHIDG_GPU_ESINGULAR;
-        atomicCAS(S.count + 1, 0, s + 1);
-        S.active[s] = 0;
-    }
     S.res_est[s] = S.res[s];
     S.nrestart[s]++;
-    S.fin[s] = 1;
+    S.fin[s] = 1;                     // least squares in k_bat_lsq
 }
 
 // a new solve: every system active
@@ -463,6 +474,9 @@ extern "C" int chidg_gpu_fgmres_solve_batched(chidg_gpu_matrix* A, chidg_gpu_pre
         if ((s2 = matvec_launch<double, double>(A, (const double*)A->val.ptr, x0, Vb, bb, -1.0, 1.0, ROWSQ))) return s2;
         k_seg_reduce<<<nsys, 32, 0, ctx->stream>>>(ROWSQ, A->nrow, SR, 1, OUT, 1);
         if ((s2 = check("k_seg_reduce r0"))) return s2;
+        // p, c, sn and H of every system, one contiguous range of the state
+        const cudaError_t ce = cudaMemsetAsync(S.p, 0, sizeof(double) * (size_t)nsys * (m + 1) * (3 + m), ctx->stream);
+        if (ce != cudaSuccess) return cuda_fail(ctx, ce, "batched fgmres state");
         k_bat_cycle_start<<<sgrid, kSysThreads, 0, ctx->stream>>>(S, bo, nsys, OUT);
         if ((s2 = check("k_bat_cycle_start"))) return s2;
         k_seg_scale<double><<<nchunk, TH, 0, ctx->stream>>>(CS, CY, Vb, Vb, S.scale);
@@ -495,6 +509,7 @@ extern "C" int chidg_gpu_fgmres_solve_batched(chidg_gpu_matrix* A, chidg_gpu_pre
         k_seg_maxpy<double><<<nchunk, TH, 0, ctx->stream>>>(CS, CY, w, Vb, n, j, S.coef2, hst, PART, S.reo);
         k_seg_reduce<<<nsys, 32, 0, ctx->stream>>>(PART, nchunk, SC, 1, S.wn2, 1, S.reo);
         k_bat_givens<<<sgrid, kSysThreads, 0, ctx->stream>>>(S, bo, nsys, j);
+        k_bat_lsq<<<nsys, 32, 0, ctx->stream>>>(S, bo, nsys);
         // x = x0 + sum y_i z_i and x0 likewise for the systems that converged now
         k_seg_lincomb<double><<<nchunk, TH, 0, ctx->stream>>>(CS, CY, xx, x0, Zb, n, j, S.coef, hst, S.fin);
         k_seg_lincomb<double><<<nchunk, TH, 0, ctx->stream>>>(CS, CY, x0, x0, Zb, n, j, S.coef, hst, S.fin);
@@ -505,6 +520,7 @@ extern "C" int chidg_gpu_fgmres_solve_batched(chidg_gpu_matrix* A, chidg_gpu_pre
     // cycle end: the systems still active update x and x0 with their m vectors
     auto seq_end = [&]() -> int {
         k_bat_cycle_end<<<sgrid, kSysThreads, 0, ctx->stream>>>(S, bo, nsys);
+        k_bat_lsq<<<nsys, 32, 0, ctx->stream>>>(S, bo, nsys);
         k_seg_lincomb<double><<<nchunk, TH, 0, ctx->stream>>>(CS, CY, xx, x0, Zb, n, m, S.coef, hst, S.fin);
         k_seg_lincomb<double><<<nchunk, TH, 0, ctx->stream>>>(CS, CY, x0, x0, Zb, n, m, S.coef, hst, S.fin);
         k_bat_count<<<1, 256, 0, ctx->stream>>>(S, nsys);
@@ -584,12 +600,17 @@ extern "C" int chidg_gpu_fgmres_solve_batched(chidg_gpu_matrix* A, chidg_gpu_pre
         int j = 1;
         for (; j <= m; ++j) {
             if ((st = run(use_graphs ? GR.step[j - 1].get() : nullptr, [&]() { return seq_step(j); }))) return st;
-            // the active count of this step, read without waiting; the previous
-            // step's count (if it has landed) ends the cycle early
+            // the active count of this step lands in pinned memory; with step j
+            // queued, the host waits for step j - 1's count, so the device is
+            // never idle and at most one step runs after the last system converged
             const int slot = j & 1;
             cudaMemcpyAsync(hc + slot, S.count, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream);
             cudaEventRecord(BB.ev[slot], ctx->stream);
-            if (j >= 2 && cudaEventQuery(BB.ev[slot ^ 1]) == cudaSuccess && hc[slot ^ 1] == 0) { all_done = true; break; }
+            if (j >= 2) {
+                const cudaError_t e = cudaEventSynchronize(BB.ev[slot ^ 1]);
+                if (e != cudaSuccess) return cuda_fail(ctx, e, "batched fgmres");
+                if (hc[slot ^ 1] == 0) { all_done = true; break; }
+            }
         }
         if (!all_done) {
             if ((st = run(use_graphs ? GR.end.get() : nullptr, seq_end))) return st;

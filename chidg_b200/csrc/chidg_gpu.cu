@@ -1523,11 +1523,24 @@ static int launch_inverse(chidg_gpu_precon* M, int row_begin, int count, int cls
         case 3: CHIDG_INV2(5, 9); break;
         case 4: CHIDG_INV2(5, 10); break;
         default: {
+            // 161..1024 rows: panels of 32 columns (16 above 352 rows, 8 above
+            // 704), (2 NB + 1) b doubles of shared memory
             int st = ensure(ctx, M->piv_scratch, sizeof(int) * 1024 * (size_t)std::max(count, 1));
             if (st) return st;
-            k_block_inverse_global<<<count, 512, 0, ctx->stream>>>(LD, (const int64_t*)P.d_dinv_off.ptr, (const int32_t*)P.d_prow_b.ptr,
-                                                                 (const int32_t*)P.d_prow_elem.ptr, (const int32_t*)P.d_fwd_rows.ptr, row_begin,
-                                                                 ctx->d_status, (int*)M->piv_scratch.ptr);
+            const int bmax = P.max_b;
+            auto go = [&](auto kern, int nbw) -> int {
+                const size_t smem = sizeof(double) * (size_t)(2 * nbw + 1) * bmax;
+                int s2 = raise_smem_limit((const void*)kern, smem);
+                if (s2) return fail(ctx, s2, "panel inverse shared memory");
+                kern<<<count, 256, smem, ctx->stream>>>(LD, (const int64_t*)P.d_dinv_off.ptr, (const int32_t*)P.d_prow_b.ptr,
+                                                        (const int32_t*)P.d_prow_elem.ptr, (const int32_t*)P.d_fwd_rows.ptr,
+                                                        row_begin, ctx->d_status, (int*)M->piv_scratch.ptr);
+                return CHIDG_GPU_OK;
+            };
+            if (bmax <= 352) st = go(k_block_inverse_panels<32>, 32);
+            else if (bmax <= 704) st = go(k_block_inverse_panels<16>, 16);
+            else st = go(k_block_inverse_panels<8>, 8);
+            if (st) return st;
         }
     }
 #undef CHIDG_INV2

@@ -669,6 +669,7 @@ struct chidg_gpu_euler {
     Buffer phi, grad, wv, phif, wf, dtau;
     Buffer blk_off;
     int64_t off_uid = 0;                           // matrix (uid) the block-offset table was built for
+    int32_t off_elem0 = -1;                        // and the element the box starts at in it
 };
 
 extern "C" int chidg_gpu_euler_create(chidg_gpu_ctx* ctx, const chidg_gpu_euler_box* box, chidg_gpu_euler** out) {
@@ -800,34 +801,49 @@ int check_vector(chidg_gpu_euler* E, const chidg_gpu_vector* v, const char* what
     return CHIDG_GPU_OK;
 }
 
+// The box placed at elements elem0 .. elem0 + nelem - 1 of A's layout: its
+// elements must have 5 fields and the box's modes on one time level; returns
+// the vector offset of its first element.
+int box_in_layout(chidg_gpu_euler* E, const chidg_gpu_matrix* A, int32_t elem0, int64_t* voff) {
+    if (!A || A->ctx != E->ctx) return fail(E->ctx, CHIDG_GPU_EINVAL, "euler: matrix of another context");
+    if (elem0 < 0 || (int64_t)elem0 + E->nelem > A->nelem || A->ntime != 1)
+        return fail(E->ctx, CHIDG_GPU_EINVAL, "euler: the box does not fit the matrix's elements");
+    for (int e = 0; e < E->nelem; ++e)
+        if (A->nvars[elem0 + e] != 5 || A->nterms[elem0 + e] != E->g.nt)
+            return fail(E->ctx, CHIDG_GPU_EINVAL, "euler: element fields or modes differ from the box");
+    *voff = A->eoff[elem0];
+    return CHIDG_GPU_OK;
+}
+
 // Offsets of each element's blocks in A's values: [e][face 0..5, DIAG], -1 on
 // boundary faces.  A must hold exactly the box pattern: one time level, 5
 // fields and (P+1)^3 modes per element, and in every row the DIAG block and
 // one block per interior face.
-int block_offsets(chidg_gpu_euler* E, chidg_gpu_matrix* A) {
-    if (E->off_uid == A->uid) return CHIDG_GPU_OK;
+int block_offsets(chidg_gpu_euler* E, chidg_gpu_matrix* A, int32_t elem0) {
+    if (E->off_uid == A->uid && E->off_elem0 == elem0) return CHIDG_GPU_OK;
     const int nt = E->g.nt;
-    if (A->nelem != E->nelem || A->ntime != 1)
+    if (elem0 < 0 || (int64_t)elem0 + E->nelem > A->nelem || A->ntime != 1)
         return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble: matrix is not this box's (elements or time levels)");
     std::vector<int64_t> off((size_t)E->nelem * 7, -1);
     BoxGeom g = E->g;
     for (int e = 0; e < E->nelem; ++e) {
-        if (A->nvars[e] != 5 || A->nterms[e] != nt)
+        const int ea = elem0 + e;                 // the element in A
+        if (A->nvars[ea] != 5 || A->nterms[ea] != nt)
             return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble: element fields or modes differ from the box");
         const int i = e % g.nx, j = (e / g.nx) % g.ny, k = e / (g.nx * g.ny);
-        const int nb[6] = {i > 0 ? e - 1 : -1, i < g.nx - 1 ? e + 1 : -1, j > 0 ? e - g.nx : -1,
-                           j < g.ny - 1 ? e + g.nx : -1, k > 0 ? e - g.nx * g.ny : -1,
-                           k < g.nz - 1 ? e + g.nx * g.ny : -1};
+        const int nb[6] = {i > 0 ? ea - 1 : -1, i < g.nx - 1 ? ea + 1 : -1, j > 0 ? ea - g.nx : -1,
+                           j < g.ny - 1 ? ea + g.nx : -1, k > 0 ? ea - g.nx * g.ny : -1,
+                           k < g.nz - 1 ? ea + g.nx * g.ny : -1};
         int expect = 1;
         for (int f = 0; f < 6; ++f) expect += nb[f] >= 0;
-        const std::vector<int32_t>& row = A->rowblk[A->row(e, 0)];
+        const std::vector<int32_t>& row = A->rowblk[A->row(ea, 0)];
         if ((int)row.size() != expect)
             return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble: matrix row is not the box pattern");
         for (int32_t kb : row) {
             if (A->kind[kb] != CHIDG_BLK_LOCAL)
                 return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble: matrix has non-local blocks");
             int slot = -1;
-            if (A->ce[kb] == e) slot = 6;
+            if (A->ce[kb] == ea) slot = 6;
             for (int f = 0; f < 6 && slot < 0; ++f)
                 if (nb[f] == A->ce[kb]) slot = f;
             if (slot < 0 || off[(size_t)e * 7 + slot] >= 0)
@@ -842,7 +858,46 @@ int block_offsets(chidg_gpu_euler* E, chidg_gpu_matrix* A) {
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(E->ctx->stream);
     if (ce != cudaSuccess) return cuda_fail(E->ctx, ce, "euler block offsets");
     E->off_uid = A->uid;
+    E->off_elem0 = elem0;
     return CHIDG_GPU_OK;
+}
+
+// rhs(box) = R(q(box)) and, with val, A's blocks of the box = dR/dq: q and rhs
+// point at the box's first element
+int assemble_ptrs(chidg_gpu_euler* E, const double* q, double* rhs, chidg_gpu_matrix* A, int32_t elem0) {
+    const bool jac = A != nullptr;
+    int st;
+    if (jac && (st = block_offsets(E, A, elem0))) return st;
+    const int P = E->order, nt = E->g.nt;
+    const size_t smem = smem_doubles(nt, E->g.qv, E->g.qf) * sizeof(double);
+    const Tables tb = tables_of(E);
+    double* val = jac ? (double*)A->val.ptr : nullptr;
+    const int64_t* off = jac ? (const int64_t*)E->blk_off.ptr : nullptr;
+    const dim3 grid(E->nelem), block(kThreads);
+    if (P == 0) k_euler_assemble<1><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, q, rhs, val, off);
+    else if (P == 1) k_euler_assemble<8><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, q, rhs, val, off);
+    else if (P == 2) k_euler_assemble<27><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, q, rhs, val, off);
+    else k_euler_assemble<64><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, q, rhs, val, off);
+    st = check_launch(E->ctx, "k_euler_assemble");
+    if (st) return st;
+    if (jac) A->stamp++;
+    return CHIDG_GPU_OK;
+}
+
+int dtau_ptrs(chidg_gpu_euler* E, const double* qp, const double* cfl, double* dtau) {
+    const dim3 grid(E->nelem), block(kThreads);
+    const Tables tb = tables_of(E);
+    double* out = (double*)E->dtau.ptr;
+    if (E->order == 0) k_euler_dtau<1><<<grid, block, 0, E->ctx->stream>>>(E->g, tb, qp, E->h, cfl[0], cfl[1], cfl[2], cfl[3], cfl[4], out);
+    else if (E->order == 1) k_euler_dtau<8><<<grid, block, 0, E->ctx->stream>>>(E->g, tb, qp, E->h, cfl[0], cfl[1], cfl[2], cfl[3], cfl[4], out);
+    else if (E->order == 2) k_euler_dtau<27><<<grid, block, 0, E->ctx->stream>>>(E->g, tb, qp, E->h, cfl[0], cfl[1], cfl[2], cfl[3], cfl[4], out);
+    else k_euler_dtau<64><<<grid, block, 0, E->ctx->stream>>>(E->g, tb, qp, E->h, cfl[0], cfl[1], cfl[2], cfl[3], cfl[4], out);
+    int st = check_launch(E->ctx, "k_euler_dtau");
+    if (st) return st;
+    cudaError_t ce = cudaMemcpyAsync(dtau, out, (size_t)E->nelem * 5 * sizeof(double), cudaMemcpyDeviceToHost,
+                                     E->ctx->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(E->ctx->stream);
+    return ce == cudaSuccess ? CHIDG_GPU_OK : cuda_fail(E->ctx, ce, "euler_pseudo_timestep");
 }
 }  // namespace
 
@@ -853,26 +908,21 @@ extern "C" int chidg_gpu_euler_assemble(chidg_gpu_euler* E, chidg_gpu_vector* q,
     if (!st) st = check_vector(E, rhs, "rhs");
     if (st) return st;
     if (q == rhs) return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble: q and rhs must differ");
-    const bool jac = A != nullptr;
-    if (jac) {
-        if (A->ctx != E->ctx) return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble: matrix of another context");
-        st = block_offsets(E, A);
-        if (st) return st;
-    }
-    const int P = E->order, nt = E->g.nt;
-    const size_t smem = smem_doubles(nt, E->g.qv, E->g.qf) * sizeof(double);
-    const Tables tb = tables_of(E);
-    double* val = jac ? (double*)A->val.ptr : nullptr;
-    const int64_t* off = jac ? (const int64_t*)E->blk_off.ptr : nullptr;
-    const dim3 grid(E->nelem), block(kThreads);
-    if (P == 0) k_euler_assemble<1><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, (const double*)q->buf.ptr, (double*)rhs->buf.ptr, val, off);
-    else if (P == 1) k_euler_assemble<8><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, (const double*)q->buf.ptr, (double*)rhs->buf.ptr, val, off);
-    else if (P == 2) k_euler_assemble<27><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, (const double*)q->buf.ptr, (double*)rhs->buf.ptr, val, off);
-    else k_euler_assemble<64><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, (const double*)q->buf.ptr, (double*)rhs->buf.ptr, val, off);
-    st = check_launch(E->ctx, "k_euler_assemble");
+    if (A && A->ctx != E->ctx) return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble: matrix of another context");
+    if (A && (A->nelem != E->nelem || A->ntime != 1))
+        return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble: matrix is not this box's (elements or time levels)");
+    return assemble_ptrs(E, (const double*)q->buf.ptr, (double*)rhs->buf.ptr, A, 0);
+}
+
+extern "C" int chidg_gpu_euler_assemble_at(chidg_gpu_euler* E, chidg_gpu_matrix* A, int32_t elem0, chidg_gpu_vector* q,
+                                           chidg_gpu_vector* rhs, int32_t jacobian) {
+    if (!E || !A || !q || !rhs) return E ? fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble_at: null argument") : CHIDG_GPU_EINVAL;
+    if (q == rhs) return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble_at: q and rhs must differ");
+    if (q->A != A || rhs->A != A) return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble_at: q and rhs must be vectors of A");
+    int64_t voff = 0;
+    int st = box_in_layout(E, A, elem0, &voff);
     if (st) return st;
-    if (jac) A->stamp++;
-    return CHIDG_GPU_OK;
+    return assemble_ptrs(E, (const double*)q->buf.ptr + voff, (double*)rhs->buf.ptr + voff, jacobian ? A : nullptr, elem0);
 }
 
 extern "C" int chidg_gpu_euler_pseudo_timestep(chidg_gpu_euler* E, chidg_gpu_vector* q, const double* cfl,
@@ -881,18 +931,16 @@ extern "C" int chidg_gpu_euler_pseudo_timestep(chidg_gpu_euler* E, chidg_gpu_vec
                                       : CHIDG_GPU_EINVAL;
     int st = check_vector(E, q, "q");
     if (st) return st;
-    const dim3 grid(E->nelem), block(kThreads);
-    const Tables tb = tables_of(E);
-    const double* qp = (const double*)q->buf.ptr;
-    double* out = (double*)E->dtau.ptr;
-    if (E->order == 0) k_euler_dtau<1><<<grid, block, 0, E->ctx->stream>>>(E->g, tb, qp, E->h, cfl[0], cfl[1], cfl[2], cfl[3], cfl[4], out);
-    else if (E->order == 1) k_euler_dtau<8><<<grid, block, 0, E->ctx->stream>>>(E->g, tb, qp, E->h, cfl[0], cfl[1], cfl[2], cfl[3], cfl[4], out);
-    else if (E->order == 2) k_euler_dtau<27><<<grid, block, 0, E->ctx->stream>>>(E->g, tb, qp, E->h, cfl[0], cfl[1], cfl[2], cfl[3], cfl[4], out);
-    else k_euler_dtau<64><<<grid, block, 0, E->ctx->stream>>>(E->g, tb, qp, E->h, cfl[0], cfl[1], cfl[2], cfl[3], cfl[4], out);
-    st = check_launch(E->ctx, "k_euler_dtau");
+    return dtau_ptrs(E, (const double*)q->buf.ptr, cfl, dtau);
+}
+
+extern "C" int chidg_gpu_euler_pseudo_timestep_at(chidg_gpu_euler* E, chidg_gpu_matrix* A, int32_t elem0,
+                                                  chidg_gpu_vector* q, const double* cfl, double* dtau) {
+    if (!E || !A || !q || !cfl || !dtau)
+        return E ? fail(E->ctx, CHIDG_GPU_EINVAL, "euler_pseudo_timestep_at: null argument") : CHIDG_GPU_EINVAL;
+    if (q->A != A) return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_pseudo_timestep_at: q must be a vector of A");
+    int64_t voff = 0;
+    int st = box_in_layout(E, A, elem0, &voff);
     if (st) return st;
-    cudaError_t ce = cudaMemcpyAsync(dtau, out, (size_t)E->nelem * 5 * sizeof(double), cudaMemcpyDeviceToHost,
-                                     E->ctx->stream);
-    if (ce == cudaSuccess) ce = cudaStreamSynchronize(E->ctx->stream);
-    return ce == cudaSuccess ? CHIDG_GPU_OK : cuda_fail(E->ctx, ce, "euler_pseudo_timestep");
+    return dtau_ptrs(E, (const double*)q->buf.ptr + voff, cfl, dtau);
 }

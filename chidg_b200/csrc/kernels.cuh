@@ -1244,6 +1244,166 @@ static __global__ void k_block_inverse_global(double* __restrict__ LD, const int
     if (singular && threadIdx.x == 0) atomicMin(status, prow_elem[prow]);
 }
 
+// Blocks of 161..1024 rows: the same Gauss-Jordan with row interchanges,
+// blocked by panels of NB columns.  A panel is factored in shared memory (its
+// pivot searches, row interchanges, scaling and eliminations restricted to
+// the panel's columns; the interchanges are applied to the rest of the rows in
+// global memory at once).  Afterwards the panel holds G e_k for its pivot
+// columns, G the product of the panel's elementary transformations, and every
+// other column becomes D[:, j] + (G - I) D[k0:k0+nb, j]: a rank-nb update
+// computed from the panel and the pivot rows staged in shared memory, 8 x 4
+// outputs per thread.  Column interchanges undo the row interchanges at the
+// end, as in k_block_inverse_global.  Dynamic shared memory:
+// (2 NB + 1) b doubles.
+template <int NB>
+__global__ void __launch_bounds__(256) k_block_inverse_panels(double* __restrict__ LD, const int64_t* __restrict__ dinv_off,
+                                                          const int32_t* __restrict__ prow_b,
+                                                          const int32_t* __restrict__ prow_elem,
+                                                          const int32_t* __restrict__ rows, int row_begin,
+                                                          int* __restrict__ status, int* __restrict__ piv_scratch) {
+    extern __shared__ double ip_smem[];
+    __shared__ double sv[8];
+    __shared__ int si[8];
+    __shared__ int s_p;
+    const int prow = rows[row_begin + blockIdx.x];
+    const int b = prow_b[prow];
+    double* D = LD + dinv_off[prow];
+    int* piv = piv_scratch + (int64_t)blockIdx.x * 1024;
+    double* Pn = ip_smem;                      // [nb][b]: panel column t at Pn[t * b]
+    double* Rw = Pn + (size_t)NB * b;          // [b][NB]: pivot row t at column j in Rw[j * NB + t]
+    double* colk = Rw + (size_t)NB * b;        // [b]: multipliers of one step
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    bool singular = false;
+    for (int k0 = 0; k0 < b; k0 += NB) {
+        const int nb = min(NB, b - k0);
+        for (int idx = tid; idx < nb * b; idx += nthr) {
+            const int t = idx / b, i = idx - t * b;
+            Pn[idx] = D[i + (int64_t)(k0 + t) * b];
+        }
+        __syncthreads();
+        for (int t = 0; t < nb; ++t) {
+            const int k = k0 + t;
+            double best = -1.0;
+            int bi = 0x7fffffff;
+            for (int i = k + tid; i < b; i += nthr) {
+                double v = fabs(Pn[t * b + i]);
+                if (!(v == v)) v = INFINITY;
+                if (v > best || (v == best && i < bi)) { best = v; bi = i; }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+            }
+            if ((tid & 31) == 0) { sv[tid >> 5] = best; si[tid >> 5] = bi; }
+            __syncthreads();
+            if (tid == 0) {
+                double bb = -1.0;
+                int ii = 0x7fffffff;
+                for (int q = 0; q < (nthr >> 5); ++q)
+                    if (sv[q] > bb || (sv[q] == bb && si[q] < ii)) { bb = sv[q]; ii = si[q]; }
+                s_p = ii;
+                piv[k] = ii;
+            }
+            __syncthreads();
+            const int p = s_p;
+            if (p != k) {
+                for (int tt = tid; tt < nb; tt += nthr) {
+                    const double x = Pn[tt * b + k];
+                    Pn[tt * b + k] = Pn[tt * b + p];
+                    Pn[tt * b + p] = x;
+                }
+                for (int j = tid; j < b; j += nthr) {
+                    if (j >= k0 && j < k0 + nb) continue;
+                    const double x = D[k + (int64_t)j * b];
+                    D[k + (int64_t)j * b] = D[p + (int64_t)j * b];
+                    D[p + (int64_t)j * b] = x;
+                }
+            }
+            __syncthreads();
+            double pv = Pn[t * b + k];
+            if (pv == 0.0) { singular = true; pv = 1.0; }
+            const double rp = 1.0 / pv;
+            for (int i = tid; i < b; i += nthr) colk[i] = (i == k) ? 0.0 : Pn[t * b + i];
+            __syncthreads();
+            for (int tt = tid; tt < nb; tt += nthr) Pn[tt * b + k] = ((tt == t) ? 1.0 : Pn[tt * b + k]) * rp;
+            __syncthreads();
+            for (int idx = tid; idx < nb * b; idx += nthr) {
+                const int tt = idx / b, i = idx - tt * b;
+                if (i == k) continue;
+                const double base = (tt == t) ? 0.0 : Pn[idx];
+                Pn[idx] = base - colk[i] * Pn[tt * b + k];
+            }
+            __syncthreads();
+        }
+        // the pivot rows outside the panel, then the panel back to memory
+        const int nout = b - nb;
+        for (int idx = tid; idx < nb * nout; idx += nthr) {
+            const int t = idx % nb, jj = idx / nb;
+            const int j = jj < k0 ? jj : jj + nb;
+            Rw[j * NB + t] = D[(k0 + t) + (int64_t)j * b];
+        }
+        for (int idx = tid; idx < nb * b; idx += nthr) {
+            const int t = idx / b, i = idx - t * b;
+            D[i + (int64_t)(k0 + t) * b] = Pn[idx];
+        }
+        __syncthreads();
+        // D[:, j] += (G - I)[:, panel] D[panel rows, j] for every j outside the panel
+        const int ni = (b + 7) / 8, nj = (nout + 3) / 4;
+        for (int w = tid; w < ni * nj; w += nthr) {
+            const int i0 = (w % ni) * 8, jj0 = (w / ni) * 4;
+            double acc[8][4];
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
+            int jcol[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int jj = min(jj0 + c, nout - 1);
+                jcol[c] = jj < k0 ? jj : jj + nb;
+            }
+            for (int t = 0; t < nb; ++t) {
+                double pr[8], rw[4];
+#pragma unroll
+                for (int r = 0; r < 8; ++r) {
+                    const int i = min(i0 + r, b - 1);
+                    pr[r] = Pn[t * b + i] - ((i == k0 + t) ? 1.0 : 0.0);
+                }
+#pragma unroll
+                for (int c = 0; c < 4; ++c) rw[c] = Rw[jcol[c] * NB + t];
+#pragma unroll
+                for (int r = 0; r < 8; ++r)
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) acc[r][c] += pr[r] * rw[c];
+            }
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                if (jj0 + c >= nout) continue;
+                double* col = D + (int64_t)jcol[c] * b;
+#pragma unroll
+                for (int r = 0; r < 8; ++r) {
+                    const int i = i0 + r;
+                    if (i < b) col[i] = col[i] + acc[r][c];
+                }
+            }
+        }
+        __syncthreads();
+    }
+    // undo the row interchanges as column interchanges, last first
+    for (int k = b - 1; k >= 0; --k) {
+        const int p = piv[k];
+        if (p != k)
+            for (int i = tid; i < b; i += nthr) {
+                const double t = D[i + (int64_t)k * b];
+                D[i + (int64_t)k * b] = D[i + (int64_t)p * b];
+                D[i + (int64_t)p * b] = t;
+            }
+        __syncthreads();
+    }
+    if (singular && tid == 0) atomicMin(status, prow_elem[prow]);
+}
+
 // ---------------------------------------------------------------------------
 // ILU programme: triangular sweeps, one CTA per programme row of a level.
 //  forward:  z_r = v_r - sum_lower L z_parent                 (precon_ILU0.f90:336-359)

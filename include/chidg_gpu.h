@@ -420,6 +420,16 @@ int chidg_gpu_euler_assemble(chidg_gpu_euler* E, chidg_gpu_vector* q, chidg_gpu_
  * nodes, h = vol^(1/3) (src/equations/fluid/type_fluid_pseudo_timestep.f90);
  * cfl holds 5 values, dtau nelem * 5 (host). */
 int chidg_gpu_euler_pseudo_timestep(chidg_gpu_euler* E, chidg_gpu_vector* q, const double* cfl, double* dtau);
+/* The same two calls for a box placed inside a larger layout, such as the
+ * block-diagonal arena of many systems that chidg_gpu_fgmres_solve_batched
+ * solves: the box's elements are A's elements elem0 .. elem0 + nelem - 1 (each
+ * with 5 fields and the box's modes, A's rows there holding the box pattern);
+ * q and rhs are vectors of A, of which only the box's segment is read or
+ * written; with `jacobian` nonzero the box's blocks of A are overwritten. */
+int chidg_gpu_euler_assemble_at(chidg_gpu_euler* E, chidg_gpu_matrix* A, int32_t elem0, chidg_gpu_vector* q,
+                                chidg_gpu_vector* rhs, int32_t jacobian);
+int chidg_gpu_euler_pseudo_timestep_at(chidg_gpu_euler* E, chidg_gpu_matrix* A, int32_t elem0, chidg_gpu_vector* q,
+                                       const double* cfl, double* dtau);
 
 #ifdef __cplusplus
 }

@@ -387,6 +387,23 @@ module chidg_gpu_mod
             real(c_double)                :: hist(*)
             integer(c_int32_t), value     :: hist_cap
         end function
+        ! the Euler box at elements elem0.. of a larger layout (a batch arena)
+        integer(c_int) function chidg_gpu_euler_assemble_at(E, mat, elem0, q, rhs, jacobian) &
+                bind(c, name='chidg_gpu_euler_assemble_at')
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr),        value :: E, mat
+            integer(c_int32_t), value :: elem0
+            type(c_ptr),        value :: q, rhs
+            integer(c_int32_t), value :: jacobian
+        end function
+        integer(c_int) function chidg_gpu_euler_pseudo_timestep_at(E, mat, elem0, q, cfl, dtau) &
+                bind(c, name='chidg_gpu_euler_pseudo_timestep_at')
+            import :: c_int, c_ptr, c_int32_t, c_double
+            type(c_ptr),        value :: E, mat
+            integer(c_int32_t), value :: elem0
+            type(c_ptr),        value :: q
+            real(c_double)            :: cfl(5), dtau(*)
+        end function
         ! ---- launch shapes of the streamed kernels and their autotuner --------
         integer(c_int) function chidg_gpu_autotune(M, mat, precision, reps) bind(c, name='chidg_gpu_autotune')
             import :: c_int, c_ptr, c_int32_t
