@@ -612,6 +612,157 @@ def run_cfg3_leg(ctx, stream, schedule, reps=2):
             "setup_s": setup_s, "device_bytes_in_use_at_end": int(total - free), "modes": out}
 
 
+CFG4_SYSTEMS = 512
+CFG4_SEED = 41
+CFG4_OPTS = dict(tol=0.0, rtol=1e-8, nkrylov=30, inner_fgmres=0, nmax=1000, use_controller=0)
+CFG4_WAVE_BYTES = 45e9      # FP64 matrix bytes per wave (the wave's device footprint is about 2.5 times that)
+CFG4_SAMPLE = 24            # systems solved one at a time by the plain FP64 path (every 21st draw)
+
+
+def cfg4_draws(count=CFG4_SYSTEMS, seed=CFG4_SEED):
+    """The scope table's many-solve workload: each box side uniform in
+    {4..16}, P uniform in {1, 2, 3} (40, 135, 320-row blocks), freestream Mach
+    uniform in [0.2, 0.6], bump amplitude uniform in [1e-3, 1e-2], bump centre
+    uniform in [0.3, 0.7]^3 (width 0.1)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        shape = tuple(int(v) for v in rng.integers(4, 17, size=3))
+        P_ = int(rng.integers(1, 4))
+        mach, amp = float(rng.uniform(0.2, 0.6)), float(rng.uniform(1e-3, 1e-2))
+        centre = tuple(float(c) for c in rng.uniform(0.3, 0.7, 3))
+        out.append((shape, P_, mach, amp, centre))
+    return out
+
+
+def box_matrix_bytes(shape, order):
+    nx, ny, nz = shape
+    b = NVARS * (order + 1) ** 3
+    nl = (nx - 1) * ny * nz + nx * (ny - 1) * nz + nx * ny * (nz - 1)
+    return (nx * ny * nz + 2 * nl) * b * b * 8
+
+
+def cfg4_waves(draws, wave_bytes=CFG4_WAVE_BYTES):
+    """Consecutive draws grouped into waves of at most wave_bytes of FP64
+    matrix values (memory admission)."""
+    waves, cur, cur_b = [], [], 0
+    for d in draws:
+        nb = box_matrix_bytes(d[0], d[1])
+        if cur and cur_b + nb > wave_bytes:
+            waves.append(cur)
+            cur, cur_b = [], 0
+        cur.append(d)
+        cur_b += nb
+    if cur:
+        waves.append(cur)
+    return waves
+
+
+def cfg4_arena(ctx, draws):
+    """One wave's systems packed block-diagonally into one matrix, each
+    system's first Newton step assembled on the device straight into its
+    slice (chidg_gpu_euler_assemble_at), the pseudo-transient term at cfl 10
+    added, b = -R(q0).  Returns (A, b, sys_elem, seconds)."""
+    from chidg_b200 import api, euler, mesh
+    boxes, q0s = [], []
+    for shape, order, mach, amp, centre in draws:
+        bx = euler.EulerBox(*shape, order, vel_inf=(mach, 0.0, 0.0))
+        boxes.append(bx)
+        q0s.append(bx.density_bump(amplitude=amp, width=0.1, centre=centre))
+    union, sys_elem = mesh.concat_patterns([bx.pattern for bx in boxes])
+    t0 = time.perf_counter()
+    A = api.ChidgMatrix(union, ctx)
+    q = api.ChidgVector(A, np.concatenate(q0s))
+    rhs = api.ChidgVector(A)
+    scale = []
+    for bx, e0 in zip(boxes, sys_elem[:-1]):
+        dev = euler.EulerDevice(bx, ctx)
+        dev.assemble_at(A, int(e0), q, rhs, True)
+        scale.append(np.repeat(1.0 / dev.pseudo_timestep_at(A, int(e0), q, CFL_PTC).min(axis=1), NVARS))
+        dev.release()
+    A.scale_diagonal(np.concatenate([bx.mass for bx in boxes]), np.concatenate(scale))
+    rhs.scale(-1.0)
+    ctx.sync()
+    q.release()
+    return A, rhs, sys_elem, time.perf_counter() - t0
+
+
+def run_cfg4_leg(ctx, schedule):
+    """The many-solve configuration as stated: 512 Euler Newton systems of
+    uneven size and order in memory-admitted waves, each wave packed into one
+    arena and solved by the batched FGMRES(30) + ILU0 to rtol 1e-8 (FP64
+    residual), with FP32 preconditioner blocks and in plain FP64; a sample of
+    the draws also solved one at a time by the plain FP64 path."""
+    from chidg_b200 import api, tuning
+    draws = cfg4_draws()
+    waves = cfg4_waves(draws)
+    out = {"workload": f"{CFG4_SYSTEMS} Euler Newton systems: box sides uniform in 4..16, P uniform in 1..3 "
+                       "(40/135/320-row blocks), Mach U[0.2, 0.6], bump amplitude U[1e-3, 1e-2]; memory-admitted "
+                       f"waves of at most {CFG4_WAVE_BYTES / 1e9:.0f} GB of FP64 blocks, each packed into one arena; "
+                       "batched FGMRES(30) + ILU0 to rtol 1e-8 (FP64 true residual); factorisation inside the timed solve",
+           "systems": len(draws), "waves": len(waves),
+           "orders": {str(p): sum(1 for d in draws if d[1] == p) for p in (1, 2, 3)},
+           "matrix_bytes_fp64": int(sum(box_matrix_bytes(d[0], d[1]) for d in draws))}
+    modes = {"mixed_precon_fp32": 0.0, "fp64": 0.0}
+    iters = {k: [] for k in modes}
+    worst = {k: 0.0 for k in modes}
+    assembly_s = 0.0
+    tuned = {}
+    for wave in waves:
+        A, b, sys_elem, asm = cfg4_arena(ctx, wave)
+        assembly_s += asm
+        x = api.ChidgVector(A)
+        for prec in modes:
+            M = api.create_preconditioner("ilu0", schedule=schedule)
+            solver = api.create_linear_solver("fgmres", **CFG4_OPTS, precision=prec)
+            if schedule == "stream":
+                M.update(A, precision=prec)
+                key = (int(A.pattern.bsize().max()), prec)
+                if key not in tuned:
+                    tuned[key] = tuning.autotune(A, M, prec, reps=1, cache=os.environ.get("CHIDG_TUNE_CACHE"))
+            ctx.sync()
+            t0 = time.perf_counter()
+            res = solver.solve_batched(A, x, b, M, sys_elem)
+            ctx.sync()
+            modes[prec] += time.perf_counter() - t0
+            iters[prec] += [r["niter"] for r in res]
+            worst[prec] = max(worst[prec], max(r["residual_norm"] / r["r0norm_initial"] for r in res))
+            M.tear_down()
+        x.release()
+        b.release()
+        A.release()
+    # the plain FP64 path, one system at a time, on a sample of the draws
+    sample = draws[::max(1, len(draws) // CFG4_SAMPLE)][:CFG4_SAMPLE]
+    one = {"seconds": 0.0, "iterations": []}
+    for d in sample:
+        A, b, sys_elem, _ = cfg4_arena(ctx, [d])
+        x = api.ChidgVector(A)
+        M = api.create_preconditioner("ilu0", schedule=schedule)
+        solver = api.create_linear_solver("fgmres", **CFG4_OPTS)
+        ctx.sync()
+        t0 = time.perf_counter()
+        solver.solve(A, x, b, M)
+        ctx.sync()
+        one["seconds"] += time.perf_counter() - t0
+        one["iterations"].append(solver.niter)
+        M.tear_down()
+        for o in (x, b, A):
+            o.release()
+    n = len(draws)
+    out["device_assembly_s"] = assembly_s
+    for prec, secs in modes.items():
+        out[f"batched_{prec}"] = {"solves_per_s": n / secs, "seconds": secs, "mean_iterations": float(np.mean(iters[prec])),
+                                  "max_iterations": int(max(iters[prec])), "max_true_rel_residual": worst[prec]}
+    sample_bytes = sum(box_matrix_bytes(d[0], d[1]) for d in sample)
+    out["one_at_a_time_fp64_sample"] = {
+        "systems": len(sample), "seconds": one["seconds"], "solves_per_s": len(sample) / one["seconds"],
+        "matrix_bytes_fp64": int(sample_bytes), "mean_iterations": float(np.mean(one["iterations"])),
+        "note": "every 21st draw; its solves/s is for the sample's own size mix"}
+    out["speedup_batched_mixed_vs_batched_fp64"] = modes["fp64"] / modes["mixed_precon_fp32"]
+    out["stream_shapes"] = {f"b<={k[0]}/{k[1]}": v for k, v in tuned.items()}
+    return out
+
+
 CFL_PTC = 10.0          # pseudo-transient cfl of the Newton systems solved
 
 
@@ -991,6 +1142,7 @@ def run_gpu(args):
     batch = run_batch_leg(ctx, args.schedule) if not args.no_batch else None
     serving = run_serve_subprocess(local) if not args.no_serve else None
     assembly = run_assembly_leg(ctx, stream, A) if not args.no_assembly else None
+    cfg4 = run_cfg4_leg(ctx, args.schedule) if not args.no_cfg4 else None
     cfg3 = None
     if not args.no_cfg3 and world == 1:
         # the 24^3 objects leave the device first: the 32^3 legs hold ~120 GB
@@ -1068,6 +1220,7 @@ def run_gpu(args):
         "newton": newton,
         "euler_assembly": assembly,
         "cfg3": cfg3,
+        "cfg4": cfg4,
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
@@ -1094,6 +1247,8 @@ def main():
                     help="skip the device Euler assembly leg (24^3 P2, overwrites the 24^3 matrix)")
     ap.add_argument("--no-cfg3", action="store_true", help="skip the 32^3 P2 legs (ILU0 and RAS, FP64 and mixed)")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuning)")
+    ap.add_argument("--no-cfg4", action="store_true",
+                    help="skip the 512-system many-solve leg (sides 4..16, P 1..3, memory-admitted waves)")
     ap.add_argument("--serve-only", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--serve-device", type=int, default=0, help=argparse.SUPPRESS)
     args = ap.parse_args()

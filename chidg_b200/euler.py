@@ -642,6 +642,23 @@ class EulerDevice:
                                                                   out.ctypes.data_as(_lib.DP)), "euler_pseudo_timestep")
         return out
 
+    def assemble_at(self, A: api.ChidgMatrix, elem0: int, q: api.ChidgVector, rhs: api.ChidgVector,
+                    jacobian: bool = True):
+        """The box as elements elem0.. of a larger layout A (a batch arena):
+        rhs's segment of the box = R(q), and with `jacobian` A's blocks of the box."""
+        self.ctx.check(self.ctx.L.chidg_gpu_euler_assemble_at(self.h, A.h, int(elem0), q.h, rhs.h, int(bool(jacobian))),
+                       "euler_assemble_at")
+
+    def pseudo_timestep_at(self, A: api.ChidgMatrix, elem0: int, q: api.ChidgVector, cfl) -> np.ndarray:
+        cfl = np.ascontiguousarray(np.broadcast_to(np.asarray(cfl, dtype=np.float64), (NFIELDS,)))
+        out = np.empty((self.box.nelem, NFIELDS))
+        from . import _lib
+        self.ctx.check(self.ctx.L.chidg_gpu_euler_pseudo_timestep_at(self.h, A.h, int(elem0), q.h,
+                                                                     cfl.ctypes.data_as(_lib.DP),
+                                                                     out.ctypes.data_as(_lib.DP)),
+                       "euler_pseudo_timestep_at")
+        return out
+
     def release(self):
         if getattr(self, "h", None):
             self.ctx.L.chidg_gpu_euler_destroy(self.h)

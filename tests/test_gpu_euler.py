@@ -11,7 +11,7 @@ Newton residual history within 1e-6 relative while the iteration contracts
 import numpy as np
 import pytest
 
-from chidg_b200 import api, euler
+from chidg_b200 import api, euler, mesh
 from chidg_b200.newton import Newton, NewtonOptions
 from oracle import oracle as O
 
@@ -220,3 +220,37 @@ def test_hb_newton_system_solve_parity(kind):
     assert solver.niter == ro["niter"]
     assert relerr(solver.hist, ro["hist"]) < 1e-8
     assert relerr(xg.download(), xo) < 1e-10
+
+
+def test_assembly_into_a_batch_arena_matches_each_box():
+    """Boxes of different sizes and orders assembled in place into their
+    slices of one block-diagonal arena (chidg_gpu_euler_assemble_at): every
+    slice is bitwise the box assembled alone, and the pseudo time steps too."""
+    boxes = [euler.EulerBox(3, 2, 2, 1, vel_inf=(0.4, 0.0, 0.0)), euler.EulerBox(2, 2, 2, 3),
+             euler.EulerBox(2, 3, 2, 2, vel_inf=(0.25, 0.05, 0.0))]
+    qs = [bx.density_bump(amplitude=0.03, width=0.3, centre=(0.4, 0.5, 0.6)) for bx in boxes]
+    union, sys_elem = mesh.concat_patterns([bx.pattern for bx in boxes])
+    A = api.ChidgMatrix(union)
+    q = api.ChidgVector(A, np.concatenate(qs))
+    rhs = api.ChidgVector(A)
+    dts = []
+    for bx, e0 in zip(boxes, sys_elem[:-1]):
+        dev = euler.EulerDevice(bx, A.ctx)
+        dev.assemble_at(A, int(e0), q, rhs, True)
+        dts.append(dev.pseudo_timestep_at(A, int(e0), q, 10.0))
+        dev.release()
+    vals, r = A.download(), rhs.download()
+    voff, nval = union.value_offsets()
+    eo = union.elem_offsets()
+    first_blk = np.searchsorted(union.blk_row_elem, sys_elem[:-1])
+    for s, (bx, qq) in enumerate(zip(boxes, qs)):
+        Ab = api.ChidgMatrix(bx.pattern, A.ctx)
+        qb, rb = api.ChidgVector(Ab, qq), api.ChidgVector(Ab)
+        dev = euler.EulerDevice(bx, A.ctx)
+        dev.assemble(qb, rb, Ab)
+        v0 = voff[first_blk[s]]
+        vb = Ab.download()
+        assert np.array_equal(vals[v0:v0 + vb.size], vb), s
+        assert np.array_equal(r[eo[sys_elem[s]]:eo[sys_elem[s]] + rb.n], rb.download()), s
+        assert np.array_equal(dts[s], dev.pseudo_timestep(qb, 10.0)), s
+        dev.release()
