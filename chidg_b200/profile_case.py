@@ -10,6 +10,10 @@ for multi-pass profiler captures.
 With --euler: `--reps` device assemblies of the Euler DG residual and
 Jacobian of the n^3 box at order p (farfield, M 0.3, a density bump) into the
 box's matrix (k_euler_assemble).
+
+With --fgmres k: `--reps` FGMRES(50) + ILU0 solves stopped after k iterations
+(the factorisation, then per iteration the forward sweep and the backward
+sweep with the matvec rows in one launch, k_ilu_stream with MV = true).
 """
 from __future__ import annotations
 
@@ -33,9 +37,13 @@ def main():
                          "the FP64 apply)")
     ap.add_argument("--euler", action="store_true",
                     help="run the device Euler DG assembly (residual + Jacobian) instead of the solver kernels")
+    ap.add_argument("--fgmres", type=int, default=0, help="run FGMRES solves of this many iterations instead")
+    ap.add_argument("--tune", action="store_true", help="autotune the streamed kernels' shapes first (--fgmres)")
     args = ap.parse_args()
     if args.euler:
         return euler_case(args)
+    if args.fgmres:
+        return fgmres_case(args)
     pat = mesh.box_pattern(args.n, args.n, args.n, 5, mesh.nterms_of_order(args.p))
     A = api.ChidgMatrix(pat)
     A.upload(mesh.synth_values(pat, seed=1))
@@ -95,6 +103,33 @@ def solve_timings(n=24, p=2, reps=6, precisions=("fp64", "mixed_fp32", "mixed_bf
         out[prec] = (times, s.niter, s.inner_iters)
         print(f"  {prec:10s} iters {s.niter:3d}+{s.inner_iters:3d}  " + " ".join(f"{1e3 * t:7.1f}" for t in times) + " ms")
     return out
+
+
+def fgmres_case(args):
+    pat = mesh.box_pattern(args.n, args.n, args.n, 5, mesh.nterms_of_order(args.p))
+    A = api.ChidgMatrix(pat)
+    A.upload(mesh.synth_values(pat, seed=1))
+    b = api.ChidgVector(A, mesh.synth_vector(A.n, seed=2))
+    x = api.ChidgVector(A)
+    M = api.create_preconditioner(args.precon, schedule=args.schedule)
+    s = api.create_linear_solver("fgmres", tol=0.0, rtol=1e-30, nkrylov=50, inner_fgmres=0, nmax=args.fgmres)
+    if args.tune:
+        from . import tuning
+        M.update(A)
+        print("shapes", tuning.autotune(A, M, "fp64", reps=2))
+    if args.time:
+        s.solve(A, x, b, M)
+        A.ctx.sync()
+        A.ctx.set_profiling(True)
+    for _ in range(args.reps):
+        s.solve(A, x, b, M)
+    A.ctx.sync()
+    print(f"profile_case fgmres n={args.n} p={args.p}: {args.reps} solves of {s.niter} iterations, "
+          f"{A.ctx.launches()} launches")
+    if args.time:
+        for name, (ms, cnt) in A.ctx.kernel_times().items():
+            if cnt:
+                print(f"  {name:20s} {cnt:4d} x {ms / cnt:9.3f} ms")
 
 
 def euler_case(args):
