@@ -102,9 +102,10 @@ def factor_flops(pat):
 # DRAM bytes of one launch (dram__bytes_read.sum + dram__bytes_write.sum)
 # from ncu captures of the 14^3 P2 case (2744 elements, 18 032 blocks; the
 # 24^3 workload is too large for a multi-pass capture), scaled to a launch of
-# the workload by its block count.  ilu_apply = both streamed sweeps.
+# the workload by its block count.
 TRAFFIC_14CUBE_BLOCKS = 18032
-TRAFFIC_14CUBE = {"ilu_forward": 1.119160e9 + 14.508288e6, "ilu_backward": 1.520102e9 + 14.406656e6}
+TRAFFIC_14CUBE = {"ilu_forward": 1.119160e9 + 14.508288e6, "ilu_backward": 1.520102e9 + 14.406656e6,
+                  "ilu_backward_matvec": 4.141639e9 + 18.169344e6}
 
 
 def measured_traffic(kind, pat):
@@ -731,8 +732,24 @@ def run_cfg4_leg(ctx, schedule):
         x.release()
         b.release()
         A.release()
-    # the plain FP64 path, one system at a time, on a sample of the draws
+    # the plain FP64 path, one system at a time, on a sample of the draws, and
+    # the same sample batched (its own waves), for a comparison on equal work
     sample = draws[::max(1, len(draws) // CFG4_SAMPLE)][:CFG4_SAMPLE]
+    sample_batched = {"mixed_precon_fp32": 0.0, "fp64": 0.0}
+    for wave in cfg4_waves(sample):
+        A, b, sys_elem, _ = cfg4_arena(ctx, wave)
+        x = api.ChidgVector(A)
+        for prec in sample_batched:
+            M = api.create_preconditioner("ilu0", schedule=schedule)
+            solver = api.create_linear_solver("fgmres", **CFG4_OPTS, precision=prec)
+            ctx.sync()
+            t0 = time.perf_counter()
+            solver.solve_batched(A, x, b, M, sys_elem)
+            ctx.sync()
+            sample_batched[prec] += time.perf_counter() - t0
+            M.tear_down()
+        for o in (x, b, A):
+            o.release()
     one = {"seconds": 0.0, "iterations": []}
     for d in sample:
         A, b, sys_elem, _ = cfg4_arena(ctx, [d])
@@ -757,7 +774,10 @@ def run_cfg4_leg(ctx, schedule):
     out["one_at_a_time_fp64_sample"] = {
         "systems": len(sample), "seconds": one["seconds"], "solves_per_s": len(sample) / one["seconds"],
         "matrix_bytes_fp64": int(sample_bytes), "mean_iterations": float(np.mean(one["iterations"])),
-        "note": "every 21st draw; its solves/s is for the sample's own size mix"}
+        "batched_mixed_precon_fp32_solves_per_s": len(sample) / sample_batched["mixed_precon_fp32"],
+        "batched_fp64_solves_per_s": len(sample) / sample_batched["fp64"],
+        "speedup_batched_mixed_vs_one_at_a_time_fp64": one["seconds"] / sample_batched["mixed_precon_fp32"],
+        "note": "every 21st draw, solved one at a time and batched (the same systems)"}
     out["speedup_batched_mixed_vs_batched_fp64"] = modes["fp64"] / modes["mixed_precon_fp32"]
     out["stream_shapes"] = {f"b<={k[0]}/{k[1]}": v for k, v in tuned.items()}
     return out

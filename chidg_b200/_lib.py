@@ -111,6 +111,9 @@ PROTOTYPES = {
     "chidg_gpu_autotune": (C.c_int, [VP, VP, C.c_int32, C.c_int32]),
     "chidg_gpu_euler_assemble_at": (C.c_int, [VP, VP, C.c_int32, VP, VP, C.c_int32]),
     "chidg_gpu_euler_pseudo_timestep_at": (C.c_int, [VP, VP, C.c_int32, VP, DP, DP]),
+    "chidg_gpu_euler_assemble_level": (C.c_int, [VP, VP, C.c_int32, VP, VP, C.c_int32]),
+    "chidg_gpu_euler_pseudo_timestep_level": (C.c_int, [VP, VP, C.c_int32, VP, DP, DP]),
+    "chidg_gpu_hb_coupling": (C.c_int, [VP, C.c_int32, DP, DP, VP, VP, C.c_int32]),
     "chidg_gpu_stream_shape_get": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, I32P, I32P, I32P]),
     "chidg_gpu_stream_shape_set": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
     "chidg_gpu_euler_create": (C.c_int, [VP, VP, C.POINTER(VP)]),

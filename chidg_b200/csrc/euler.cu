@@ -26,6 +26,7 @@
 // two agree to rounding since the numerical flux is antisymmetric).
 #include "chidg_gpu_internal.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -374,10 +375,12 @@ __device__ __forceinline__ void face_node(const BoxGeom& g, const Tables& tb, co
     }
 }
 
+// q and rhs: an element's segment at e * vs (vs = b for one time level, the
+// element's stride over all its levels under harmonic balance)
 template <int NT>
 __global__ void __launch_bounds__(kThreads) k_euler_assemble(BoxGeom g, Tables tb, const double* __restrict__ q,
                                                             double* __restrict__ rhs, double* __restrict__ val,
-                                                            const int64_t* __restrict__ blk_off) {
+                                                            const int64_t* __restrict__ blk_off, int64_t vs) {
     extern __shared__ double sm[];
     const int e = blockIdx.x;
     const int nt = NT, b = 5 * NT, qv = g.qv, qf = g.qf;
@@ -397,7 +400,7 @@ __global__ void __launch_bounds__(kThreads) k_euler_assemble(BoxGeom g, Tables t
     for (int t = threadIdx.x; t < 7 * b; t += blockDim.x) {
         const int slot = t / b, i = t - slot * b;
         const int src = slot == 6 ? e : nbr[slot];
-        sU[t] = src >= 0 ? q[(int64_t)src * b + i] : 0.0;
+        sU[t] = src >= 0 ? q[(int64_t)src * vs + i] : 0.0;
     }
     __syncthreads();
 
@@ -423,7 +426,7 @@ __global__ void __launch_bounds__(kThreads) k_euler_assemble(BoxGeom g, Tables t
             for (int face = 0; face < 6; ++face)
                 for (int qq = 0; qq < qf; ++qq)
                     r += tb.phif[((size_t)face * qf + qq) * nt + m] * sFI[((size_t)face * qf + qq) * 5 + f];
-            rhs[(int64_t)e * b + t] = r;
+            rhs[(int64_t)e * vs + t] = r;
         }
 
         // 4. DIAG block and 5. face blocks (skipped for a residual-only call): one
@@ -517,7 +520,7 @@ __global__ void __launch_bounds__(kThreads) k_euler_assemble(BoxGeom g, Tables t
                 r -= tb.grad[(0 * qv + qq) * nt + m] * sWF[(qq * 3 + 0) * 5 + f]
                    + tb.grad[(1 * qv + qq) * nt + m] * sWF[(qq * 3 + 1) * 5 + f]
                    + tb.grad[(2 * qv + qq) * nt + m] * sWF[(qq * 3 + 2) * 5 + f];
-            rhs[(int64_t)e * b + t] = r;
+            rhs[(int64_t)e * vs + t] = r;
         }
         if (val != nullptr) {
             double* out = val + bo[6];
@@ -550,11 +553,11 @@ __global__ void __launch_bounds__(kThreads) k_euler_assemble(BoxGeom g, Tables t
         __syncthreads();
         for (int t = threadIdx.x; t < b; t += blockDim.x) {
             const int f = t / nt, m = t - f * nt;
-            double r = rhs[(int64_t)e * b + t];
+            double r = rhs[(int64_t)e * vs + t];
             for (int face = 0; face < 6; ++face)
                 for (int qq = 0; qq < qf; ++qq)
                     r += tb.phif[((size_t)face * qf + qq) * nt + m] * sFI[((size_t)face * qf + qq) * 5 + f];
-            rhs[(int64_t)e * b + t] = r;
+            rhs[(int64_t)e * vs + t] = r;
         }
         if (val == nullptr) return;
         for (int blk = 6; blk >= 0; --blk) {
@@ -595,17 +598,17 @@ __global__ void __launch_bounds__(kThreads) k_euler_assemble(BoxGeom g, Tables t
 // dtau[e, f] = cfl[f] h / (mean |u| + mean c) over the volume nodes
 // (type_fluid_pseudo_timestep.f90, compute)
 template <int NT>
-__global__ void __launch_bounds__(kThreads) k_euler_dtau(BoxGeom g, Tables tb, const double* __restrict__ q,
+__global__ void __launch_bounds__(kThreads) k_euler_dtau(BoxGeom g, Tables tb, const double* __restrict__ q, int64_t vs,
                                                         double h, double c0, double c1, double c2, double c3, double c4,
                                                         double* __restrict__ dtau) {
     __shared__ double red[2][kThreads / 32];
-    const int e = blockIdx.x, nt = NT, b = 5 * NT;
+    const int e = blockIdx.x, nt = NT;
     double sv = 0.0, sc = 0.0;
     for (int qq = threadIdx.x; qq < g.qv; qq += blockDim.x) {
         double Q[5];
         for (int f = 0; f < 5; ++f) {
             double s = 0.0;
-            for (int m = 0; m < nt; ++m) s += tb.phi[qq * nt + m] * q[(int64_t)e * b + f * nt + m];
+            for (int m = 0; m < nt; ++m) s += tb.phi[qq * nt + m] * q[(int64_t)e * vs + f * nt + m];
             Q[f] = s;
         }
         const double p = (kGamma - 1.0) * (Q[4] - 0.5 * (Q[1] * Q[1] + Q[2] * Q[2] + Q[3] * Q[3]) / Q[0]);
@@ -670,6 +673,7 @@ struct chidg_gpu_euler {
     Buffer blk_off;
     int64_t off_uid = 0;                           // matrix (uid) the block-offset table was built for
     int32_t off_elem0 = -1;                        // and the element the box starts at in it
+    int32_t off_itime = -1;                        // and the time level of the rows
 };
 
 extern "C" int chidg_gpu_euler_create(chidg_gpu_ctx* ctx, const chidg_gpu_euler_box* box, chidg_gpu_euler** out) {
@@ -819,10 +823,10 @@ int box_in_layout(chidg_gpu_euler* E, const chidg_gpu_matrix* A, int32_t elem0, 
 // boundary faces.  A must hold exactly the box pattern: one time level, 5
 // fields and (P+1)^3 modes per element, and in every row the DIAG block and
 // one block per interior face.
-int block_offsets(chidg_gpu_euler* E, chidg_gpu_matrix* A, int32_t elem0) {
-    if (E->off_uid == A->uid && E->off_elem0 == elem0) return CHIDG_GPU_OK;
+int block_offsets(chidg_gpu_euler* E, chidg_gpu_matrix* A, int32_t elem0, int32_t itime = 0) {
+    if (E->off_uid == A->uid && E->off_elem0 == elem0 && E->off_itime == itime) return CHIDG_GPU_OK;
     const int nt = E->g.nt;
-    if (elem0 < 0 || (int64_t)elem0 + E->nelem > A->nelem || A->ntime != 1)
+    if (elem0 < 0 || (int64_t)elem0 + E->nelem > A->nelem || itime < 0 || itime >= A->ntime)
         return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble: matrix is not this box's (elements or time levels)");
     std::vector<int64_t> off((size_t)E->nelem * 7, -1);
     BoxGeom g = E->g;
@@ -836,12 +840,19 @@ int block_offsets(chidg_gpu_euler* E, chidg_gpu_matrix* A, int32_t elem0) {
                            k < g.nz - 1 ? ea + g.nx * g.ny : -1};
         int expect = 1;
         for (int f = 0; f < 6; ++f) expect += nb[f] >= 0;
-        const std::vector<int32_t>& row = A->rowblk[A->row(ea, 0)];
-        if ((int)row.size() != expect)
+        // the row's LOCAL blocks are the box pattern; harmonic-balance blocks
+        // (coupling the element's time levels) may follow
+        const std::vector<int32_t>& row = A->rowblk[A->row(ea, itime)];
+        int nlocal = 0;
+        for (int32_t kb : row) {
+            if (A->kind[kb] == CHIDG_BLK_LOCAL) ++nlocal;
+            else if (A->kind[kb] != CHIDG_BLK_HB || A->ce[kb] != ea)
+                return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble: matrix has chimera or boundary blocks");
+        }
+        if (nlocal != expect)
             return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble: matrix row is not the box pattern");
         for (int32_t kb : row) {
-            if (A->kind[kb] != CHIDG_BLK_LOCAL)
-                return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble: matrix has non-local blocks");
+            if (A->kind[kb] != CHIDG_BLK_LOCAL) continue;
             int slot = -1;
             if (A->ce[kb] == ea) slot = 6;
             for (int f = 0; f < 6 && slot < 0; ++f)
@@ -859,39 +870,43 @@ int block_offsets(chidg_gpu_euler* E, chidg_gpu_matrix* A, int32_t elem0) {
     if (ce != cudaSuccess) return cuda_fail(E->ctx, ce, "euler block offsets");
     E->off_uid = A->uid;
     E->off_elem0 = elem0;
+    E->off_itime = itime;
     return CHIDG_GPU_OK;
 }
 
 // rhs(box) = R(q(box)) and, with val, A's blocks of the box = dR/dq: q and rhs
 // point at the box's first element
-int assemble_ptrs(chidg_gpu_euler* E, const double* q, double* rhs, chidg_gpu_matrix* A, int32_t elem0) {
+int assemble_ptrs(chidg_gpu_euler* E, const double* q, double* rhs, chidg_gpu_matrix* A, int32_t elem0,
+                  int32_t itime = 0, int64_t vs = 0) {
     const bool jac = A != nullptr;
+    if (vs == 0) vs = (int64_t)5 * E->g.nt;
     int st;
-    if (jac && (st = block_offsets(E, A, elem0))) return st;
+    if (jac && (st = block_offsets(E, A, elem0, itime))) return st;
     const int P = E->order, nt = E->g.nt;
     const size_t smem = smem_doubles(nt, E->g.qv, E->g.qf) * sizeof(double);
     const Tables tb = tables_of(E);
     double* val = jac ? (double*)A->val.ptr : nullptr;
     const int64_t* off = jac ? (const int64_t*)E->blk_off.ptr : nullptr;
     const dim3 grid(E->nelem), block(kThreads);
-    if (P == 0) k_euler_assemble<1><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, q, rhs, val, off);
-    else if (P == 1) k_euler_assemble<8><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, q, rhs, val, off);
-    else if (P == 2) k_euler_assemble<27><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, q, rhs, val, off);
-    else k_euler_assemble<64><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, q, rhs, val, off);
+    if (P == 0) k_euler_assemble<1><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, q, rhs, val, off, vs);
+    else if (P == 1) k_euler_assemble<8><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, q, rhs, val, off, vs);
+    else if (P == 2) k_euler_assemble<27><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, q, rhs, val, off, vs);
+    else k_euler_assemble<64><<<grid, block, smem, E->ctx->stream>>>(E->g, tb, q, rhs, val, off, vs);
     st = check_launch(E->ctx, "k_euler_assemble");
     if (st) return st;
     if (jac) A->stamp++;
     return CHIDG_GPU_OK;
 }
 
-int dtau_ptrs(chidg_gpu_euler* E, const double* qp, const double* cfl, double* dtau) {
+int dtau_ptrs(chidg_gpu_euler* E, const double* qp, const double* cfl, double* dtau, int64_t vs = 0) {
+    if (vs == 0) vs = (int64_t)5 * E->g.nt;
     const dim3 grid(E->nelem), block(kThreads);
     const Tables tb = tables_of(E);
     double* out = (double*)E->dtau.ptr;
-    if (E->order == 0) k_euler_dtau<1><<<grid, block, 0, E->ctx->stream>>>(E->g, tb, qp, E->h, cfl[0], cfl[1], cfl[2], cfl[3], cfl[4], out);
-    else if (E->order == 1) k_euler_dtau<8><<<grid, block, 0, E->ctx->stream>>>(E->g, tb, qp, E->h, cfl[0], cfl[1], cfl[2], cfl[3], cfl[4], out);
-    else if (E->order == 2) k_euler_dtau<27><<<grid, block, 0, E->ctx->stream>>>(E->g, tb, qp, E->h, cfl[0], cfl[1], cfl[2], cfl[3], cfl[4], out);
-    else k_euler_dtau<64><<<grid, block, 0, E->ctx->stream>>>(E->g, tb, qp, E->h, cfl[0], cfl[1], cfl[2], cfl[3], cfl[4], out);
+    if (E->order == 0) k_euler_dtau<1><<<grid, block, 0, E->ctx->stream>>>(E->g, tb, qp, vs, E->h, cfl[0], cfl[1], cfl[2], cfl[3], cfl[4], out);
+    else if (E->order == 1) k_euler_dtau<8><<<grid, block, 0, E->ctx->stream>>>(E->g, tb, qp, vs, E->h, cfl[0], cfl[1], cfl[2], cfl[3], cfl[4], out);
+    else if (E->order == 2) k_euler_dtau<27><<<grid, block, 0, E->ctx->stream>>>(E->g, tb, qp, vs, E->h, cfl[0], cfl[1], cfl[2], cfl[3], cfl[4], out);
+    else k_euler_dtau<64><<<grid, block, 0, E->ctx->stream>>>(E->g, tb, qp, vs, E->h, cfl[0], cfl[1], cfl[2], cfl[3], cfl[4], out);
     int st = check_launch(E->ctx, "k_euler_dtau");
     if (st) return st;
     cudaError_t ce = cudaMemcpyAsync(dtau, out, (size_t)E->nelem * 5 * sizeof(double), cudaMemcpyDeviceToHost,
@@ -943,4 +958,127 @@ extern "C" int chidg_gpu_euler_pseudo_timestep_at(chidg_gpu_euler* E, chidg_gpu_
     int st = box_in_layout(E, A, elem0, &voff);
     if (st) return st;
     return dtau_ptrs(E, (const double*)q->buf.ptr + voff, cfl, dtau);
+}
+
+// ---- harmonic balance --------------------------------------------------------------
+extern "C" int chidg_gpu_euler_assemble_level(chidg_gpu_euler* E, chidg_gpu_matrix* A, int32_t itime, chidg_gpu_vector* q,
+                                              chidg_gpu_vector* rhs, int32_t jacobian) {
+    if (!E || !A || !q || !rhs) return E ? fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble_level: null argument") : CHIDG_GPU_EINVAL;
+    if (q == rhs) return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble_level: q and rhs must differ");
+    if (q->A != A || rhs->A != A) return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble_level: q and rhs must be vectors of A");
+    if (A->ctx != E->ctx || A->nelem != E->nelem || itime < 0 || itime >= A->ntime)
+        return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble_level: matrix is not this box's or no such time level");
+    for (int e = 0; e < E->nelem; ++e)
+        if (A->nvars[e] != 5 || A->nterms[e] != E->g.nt)
+            return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble_level: element fields or modes differ from the box");
+    const int64_t b = (int64_t)5 * E->g.nt, vs = b * A->ntime;
+    return assemble_ptrs(E, (const double*)q->buf.ptr + itime * b, (double*)rhs->buf.ptr + itime * b, jacobian ? A : nullptr,
+                         0, itime, vs);
+}
+
+extern "C" int chidg_gpu_euler_pseudo_timestep_level(chidg_gpu_euler* E, chidg_gpu_matrix* A, int32_t itime,
+                                                     chidg_gpu_vector* q, const double* cfl, double* dtau) {
+    if (!E || !A || !q || !cfl || !dtau)
+        return E ? fail(E->ctx, CHIDG_GPU_EINVAL, "euler_pseudo_timestep_level: null argument") : CHIDG_GPU_EINVAL;
+    if (q->A != A || A->nelem != E->nelem || itime < 0 || itime >= A->ntime)
+        return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_pseudo_timestep_level: q of another layout or no such time level");
+    const int64_t b = (int64_t)5 * E->g.nt;
+    return dtau_ptrs(E, (const double*)q->buf.ptr + itime * b, cfl, dtau, b * A->ntime);
+}
+
+namespace {
+template <typename T>
+int upload_array(chidg_gpu_ctx* ctx, Buffer& buf, const std::vector<T>& v) {
+    int st = ensure(ctx, buf, std::max<size_t>(v.size(), 1) * sizeof(T));
+    if (st) return st;
+    if (v.empty()) return CHIDG_GPU_OK;
+    const cudaError_t e = cudaMemcpyAsync(buf.ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream);
+    return e == cudaSuccess ? CHIDG_GPU_OK : cuda_fail(ctx, e, "hb tables");
+}
+
+// rhs(e, t) += sum_t' D(t, t') (I_fields x M) q(e, t'), one CTA per element
+__global__ void k_hb_residual(const double* __restrict__ q, double* __restrict__ rhs, const int64_t* __restrict__ eoff,
+                              const int32_t* __restrict__ nvars, int ntime, int nt, const double* __restrict__ D,
+                              const double* __restrict__ M) {
+    const int e = blockIdx.x;
+    const int b = nvars[e] * nt;
+    const double* qe = q + eoff[e];
+    double* re = rhs + eoff[e];
+    for (int r = threadIdx.x; r < ntime * b; r += blockDim.x) {
+        const int t = r / b, fm = r - t * b, f = fm / nt, m = fm - f * nt;
+        double acc = 0.0;
+        for (int tp = 0; tp < ntime; ++tp) {
+            const double* qf = qe + (int64_t)tp * b + f * nt;
+            double mq = 0.0;
+            for (int n = 0; n < nt; ++n) mq += M[m + n * nt] * qf[n];
+            acc += D[t + tp * ntime] * mq;
+        }
+        re[r] += acc;
+    }
+}
+// the hb block of row (e, t), column (e, t'): D(t, t') (I_fields x M), one CTA per block
+__global__ void k_hb_blocks(double* __restrict__ val, const int64_t* __restrict__ voff, const int32_t* __restrict__ rt,
+                            const int32_t* __restrict__ ct, const int32_t* __restrict__ bsz, int ntime, int nt,
+                            const double* __restrict__ D, const double* __restrict__ M) {
+    const int k = blockIdx.x;
+    const int b = bsz[k];
+    const double d = D[rt[k] + ct[k] * ntime];
+    double* out = val + voff[k];
+    for (int idx = threadIdx.x; idx < b * b; idx += blockDim.x) {
+        const int r = idx % b, c = idx / b;
+        const int fr = r / nt, fc = c / nt;
+        out[idx] = (fr == fc) ? d * M[(r - fr * nt) + (c - fc * nt) * nt] : 0.0;
+    }
+}
+}  // namespace
+
+extern "C" int chidg_gpu_hb_coupling(chidg_gpu_matrix* A, int32_t nterms, const double* D, const double* mass,
+                                     chidg_gpu_vector* q, chidg_gpu_vector* rhs, int32_t jacobian) {
+    if (!A || !D || !mass || !q || !rhs || q == rhs || q->A != A || rhs->A != A || nterms < 1)
+        return A ? fail(A->ctx, CHIDG_GPU_EINVAL, "hb_coupling: bad argument") : CHIDG_GPU_EINVAL;
+    chidg_gpu_ctx* ctx = A->ctx;
+    cudaSetDevice(ctx->device);
+    const int T = A->ntime;
+    for (int e = 0; e < A->nelem; ++e)
+        if (A->nterms[e] != nterms) return fail(ctx, CHIDG_GPU_EINVAL, "hb_coupling: elements of another mode count");
+    std::vector<int32_t> hb_rt, hb_ct, hb_b;
+    std::vector<int64_t> hb_off;
+    if (jacobian)
+        for (int64_t k = 0; k < A->nblk; ++k)
+            if (A->kind[k] == CHIDG_BLK_HB) {
+                if (A->re[k] != A->ce[k]) return fail(ctx, CHIDG_GPU_EINVAL, "hb_coupling: an hb block couples two elements");
+                hb_rt.push_back(A->rt[k]);
+                hb_ct.push_back(A->ct[k]);
+                hb_b.push_back(A->bsize(A->re[k]));
+                hb_off.push_back(A->voff[k]);
+            }
+    Buffer dD, dM, dE, dV, bo, br, bc, bb;
+    auto cleanup = [&]() { for (Buffer* x : {&dD, &dM, &dE, &dV, &bo, &br, &bc, &bb}) release(*x); };
+    int st;
+    std::vector<double> hD(D, D + (size_t)T * T), hM(mass, mass + (size_t)nterms * nterms);
+    if ((st = upload_array(ctx, dD, hD)) || (st = upload_array(ctx, dM, hM)) || (st = upload_array(ctx, dE, A->eoff)) ||
+        (st = upload_array(ctx, dV, A->nvars))) {
+        cleanup();
+        return st;
+    }
+    k_hb_residual<<<A->nelem, 256, 0, ctx->stream>>>((const double*)q->buf.ptr, (double*)rhs->buf.ptr, (const int64_t*)dE.ptr,
+                                                     (const int32_t*)dV.ptr, T, nterms, (const double*)dD.ptr,
+                                                     (const double*)dM.ptr);
+    if ((st = check_launch(ctx, "k_hb_residual"))) { cleanup(); return st; }
+    if (jacobian && !hb_off.empty()) {
+        if ((st = upload_array(ctx, bo, hb_off)) || (st = upload_array(ctx, br, hb_rt)) || (st = upload_array(ctx, bc, hb_ct)) ||
+            (st = upload_array(ctx, bb, hb_b))) {
+            cleanup();
+            return st;
+        }
+        k_hb_blocks<<<(int)hb_off.size(), 256, 0, ctx->stream>>>((double*)A->val.ptr, (const int64_t*)bo.ptr,
+                                                                 (const int32_t*)br.ptr, (const int32_t*)bc.ptr,
+                                                                 (const int32_t*)bb.ptr, T, nterms, (const double*)dD.ptr,
+                                                                 (const double*)dM.ptr);
+        if ((st = check_launch(ctx, "k_hb_blocks"))) { cleanup(); return st; }
+        A->stamp++;
+    }
+    const cudaError_t ce = cudaStreamSynchronize(ctx->stream);     // the host copies and buffers go out of scope
+    cleanup();
+    return ce == cudaSuccess ? CHIDG_GPU_OK : cuda_fail(ctx, ce, "hb_coupling");
 }

@@ -374,7 +374,10 @@ struct GemmTask {            // C(m x n) = [Cinit] + sgn * sum_q A_q(m x k_q) B_
     int32_t m, n;
     int32_t q_begin, q_end;  // pairs
     int32_t elem;            // element id for status reporting
-    int32_t pad;
+    // k_task_gemm_dmma: the task may be the tile of rows r0.. and columns c0..
+    // of an output block of ldm rows (the A operands have ldm rows too);
+    // ldm = m, r0 = c0 = 0 for a whole block, which every other kernel takes
+    int32_t ldm, r0, c0;
 };
 struct GemmPair {
     int64_t a_off, b_off;
@@ -492,6 +495,7 @@ __global__ void __launch_bounds__(DM_THREADS, 1) k_task_gemm_dmma(const GemmTask
     double* As = reinterpret_cast<double*>(smem_raw);      // 2 stages x {A [DM_KC][DM_LD], B [DM_KC][DM_LD]}
     static_assert(sizeof(TA) == 8 && sizeof(TB) == 8, "FP64 operands");
     const GemmTask t = tasks[blockIdx.x];
+    const int ldm = t.ldm;                        // rows of the whole output block and of A
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int wm = w % DM_WM, wn = w / DM_WM;
     const int g = lane >> 2, tq = lane & 3;
@@ -509,15 +513,15 @@ __global__ void __launch_bounds__(DM_THREADS, 1) k_task_gemm_dmma(const GemmTask
     int lq = t.q_begin, lk0 = 0;                  // next chunk to load
     auto issue = [&](int stage) {
         const GemmPair pr = pairs[lq];
-        const TA* A = Abase + pr.a_off;           // m x k, column-major
-        const TB* B = Bbase + pr.b_off;           // k x n, column-major
+        const TA* A = Abase + pr.a_off + t.r0;                  // the tile's rows of ldm x k, column-major
+        const TB* B = Bbase + pr.b_off + (int64_t)t.c0 * pr.k;  // the tile's columns of k x N, column-major
         const int kc = min(DM_KC, pr.k - lk0);
         double* as = As + stage * 2 * DM_KC * DM_LD;
         double* bs = as + DM_KC * DM_LD;
         for (int idx = threadIdx.x; idx < DM_KC * DM_MAX; idx += blockDim.x) {
             const int i = idx % DM_MAX, kk = idx / DM_MAX;
             const bool ok = i < t.m && kk < kc;
-            cp_async8(as + kk * DM_LD + i, ok ? (const void*)(A + i + (int64_t)(lk0 + kk) * t.m) : (const void*)A, ok);
+            cp_async8(as + kk * DM_LD + i, ok ? (const void*)(A + i + (int64_t)(lk0 + kk) * ldm) : (const void*)A, ok);
         }
         for (int idx = threadIdx.x; idx < DM_KC * DM_MAX; idx += blockDim.x) {
             const int kk = idx % DM_KC, j = idx / DM_KC;
@@ -571,7 +575,7 @@ __global__ void __launch_bounds__(DM_THREADS, 1) k_task_gemm_dmma(const GemmTask
             for (int e = 0; e < 2; ++e) {
                 const int col = (wn + DM_WN * j) * 8 + 2 * tq + e;
                 if (col >= t.n) continue;
-                const int64_t o = row + (int64_t)col * t.m;
+                const int64_t o = (t.r0 + row) + (int64_t)(t.c0 + col) * ldm;
                 double v = sgn * acc[i][j][e];
                 if (t.cinit_off >= 0) v = Cinit[t.cinit_off + o] + v;
                 Cbase[t.c_off + o] = from_d<TC>(v);

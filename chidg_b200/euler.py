@@ -671,6 +671,46 @@ class EulerDevice:
             pass
 
 
+class EulerHBDevice:
+    """The harmonic-balance system of an EulerHB assembled on the GPU: every
+    time level's spatial residual and Jacobian by the device kernel of that
+    level's box (chidg_gpu_euler_assemble_level), then the time coupling
+    sum_t' D(t, t') M q_t' and the hb blocks D(t, t') M (chidg_gpu_hb_coupling),
+    into a matrix holding hb.pattern and vectors of it; the pseudo time steps
+    are those of level 1 (chidg_gpu_euler_pseudo_timestep_level)."""
+
+    def __init__(self, hb: "EulerHB", ctx: api.Context | None = None):
+        self.hb = hb
+        self.ctx = ctx or api.default_context()
+        self.levels = [EulerDevice(lv, self.ctx) for lv in hb.levels]
+        self._D = np.asfortranarray(hb.D, dtype=np.float64)
+        self._M = np.asfortranarray(hb.base.mass_block, dtype=np.float64)
+
+    def assemble(self, q: api.ChidgVector, rhs: api.ChidgVector, A: api.ChidgMatrix, jacobian: bool = True):
+        from . import _lib
+        L = self.ctx.L
+        for t, dev in enumerate(self.levels):
+            self.ctx.check(L.chidg_gpu_euler_assemble_level(dev.h, A.h, t, q.h, rhs.h, int(bool(jacobian))),
+                           "euler_assemble_level")
+        self.ctx.check(L.chidg_gpu_hb_coupling(A.h, int(self.hb.nterms), self._D.ctypes.data_as(_lib.DP),
+                                               self._M.ctypes.data_as(_lib.DP), q.h, rhs.h, int(bool(jacobian))),
+                       "hb_coupling")
+
+    def pseudo_timestep(self, q: api.ChidgVector, A: api.ChidgMatrix, cfl) -> np.ndarray:
+        from . import _lib
+        cfl = np.ascontiguousarray(np.broadcast_to(np.asarray(cfl, dtype=np.float64), (NFIELDS,)))
+        out = np.empty((self.hb.nelem, NFIELDS))
+        self.ctx.check(self.ctx.L.chidg_gpu_euler_pseudo_timestep_level(self.levels[0].h, A.h, 0, q.h,
+                                                                        cfl.ctypes.data_as(_lib.DP),
+                                                                        out.ctypes.data_as(_lib.DP)),
+                       "euler_pseudo_timestep_level")
+        return out
+
+    def release(self):
+        for dev in self.levels:
+            dev.release()
+
+
 class EulerDeviceSystem:
     """The Newton driver's `system` with the assembly on the GPU: q, rhs and
     the Jacobian never leave the device; only the pseudo time steps (nelem x 5)

@@ -39,6 +39,8 @@ def main():
                     help="run the device Euler DG assembly (residual + Jacobian) instead of the solver kernels")
     ap.add_argument("--fgmres", type=int, default=0, help="run FGMRES solves of this many iterations instead")
     ap.add_argument("--tune", action="store_true", help="autotune the streamed kernels' shapes first (--fgmres)")
+    ap.add_argument("--tune-cache", default=None,
+                    help="JSON file of tuned shapes: loaded when it holds this case's shapes, written otherwise")
     args = ap.parse_args()
     if args.euler:
         return euler_case(args)
@@ -116,7 +118,7 @@ def fgmres_case(args):
     if args.tune:
         from . import tuning
         M.update(A)
-        print("shapes", tuning.autotune(A, M, "fp64", reps=2))
+        print("shapes", tuning.autotune(A, M, "fp64", reps=2, cache=args.tune_cache))
     if args.time:
         s.solve(A, x, b, M)
         A.ctx.sync()

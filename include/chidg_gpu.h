@@ -430,6 +430,26 @@ int chidg_gpu_euler_assemble_at(chidg_gpu_euler* E, chidg_gpu_matrix* A, int32_t
                                 chidg_gpu_vector* rhs, int32_t jacobian);
 int chidg_gpu_euler_pseudo_timestep_at(chidg_gpu_euler* E, chidg_gpu_matrix* A, int32_t elem0, chidg_gpu_vector* q,
                                        const double* cfl, double* dtau);
+/* Harmonic balance (assemble_harmonic_balance_t%assemble,
+ * type_harmonic_balance.f90:127-229) on the device.  A holds the box's
+ * pattern with ntime levels and hb_blks (every element's level t coupled to
+ * its levels t' != t); vectors are element-major, then level, field, mode.
+ * chidg_gpu_euler_assemble_level: level itime's spatial residual into its
+ * segments of rhs and, with `jacobian`, its Jacobian into the LOCAL blocks of
+ * the rows (e, itime); E is the box of that level (its own farfield state).
+ * chidg_gpu_euler_pseudo_timestep_level: that level's dtau (nelem x 5).
+ * chidg_gpu_hb_coupling: rhs(e, t) += sum_t' D(t, t') M q(e, t') per field, and
+ * with `jacobian` every hb block (e, t) -> (e, t') = D(t, t') M on each field's
+ * diagonal (the t' = t term stays in the residual, as the reference stores
+ * it); D is ntime x ntime column-major (the pseudo-spectral operator,
+ * mod_HB_matrices.f90), mass nterms x nterms column-major (every element has
+ * nterms modes). */
+int chidg_gpu_euler_assemble_level(chidg_gpu_euler* E, chidg_gpu_matrix* A, int32_t itime, chidg_gpu_vector* q,
+                                   chidg_gpu_vector* rhs, int32_t jacobian);
+int chidg_gpu_euler_pseudo_timestep_level(chidg_gpu_euler* E, chidg_gpu_matrix* A, int32_t itime, chidg_gpu_vector* q,
+                                          const double* cfl, double* dtau);
+int chidg_gpu_hb_coupling(chidg_gpu_matrix* A, int32_t nterms, const double* D, const double* mass, chidg_gpu_vector* q,
+                          chidg_gpu_vector* rhs, int32_t jacobian);
 
 #ifdef __cplusplus
 }

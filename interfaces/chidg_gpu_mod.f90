@@ -404,6 +404,32 @@ module chidg_gpu_mod
             type(c_ptr),        value :: q
             real(c_double)            :: cfl(5), dtau(*)
         end function
+        ! harmonic balance: one level's spatial part, that level's dtau, the time coupling
+        integer(c_int) function chidg_gpu_euler_assemble_level(E, mat, itime, q, rhs, jacobian) &
+                bind(c, name='chidg_gpu_euler_assemble_level')
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr),        value :: E, mat
+            integer(c_int32_t), value :: itime
+            type(c_ptr),        value :: q, rhs
+            integer(c_int32_t), value :: jacobian
+        end function
+        integer(c_int) function chidg_gpu_euler_pseudo_timestep_level(E, mat, itime, q, cfl, dtau) &
+                bind(c, name='chidg_gpu_euler_pseudo_timestep_level')
+            import :: c_int, c_ptr, c_int32_t, c_double
+            type(c_ptr),        value :: E, mat
+            integer(c_int32_t), value :: itime
+            type(c_ptr),        value :: q
+            real(c_double)            :: cfl(5), dtau(*)
+        end function
+        integer(c_int) function chidg_gpu_hb_coupling(mat, nterms, D, mass, q, rhs, jacobian) &
+                bind(c, name='chidg_gpu_hb_coupling')
+            import :: c_int, c_ptr, c_int32_t, c_double
+            type(c_ptr),        value :: mat
+            integer(c_int32_t), value :: nterms
+            real(c_double)            :: D(*), mass(*)
+            type(c_ptr),        value :: q, rhs
+            integer(c_int32_t), value :: jacobian
+        end function
         ! ---- launch shapes of the streamed kernels and their autotuner --------
         integer(c_int) function chidg_gpu_autotune(M, mat, precision, reps) bind(c, name='chidg_gpu_autotune')
             import :: c_int, c_ptr, c_int32_t
