@@ -826,15 +826,27 @@ def hb_system(i, seed):
     1e-2, a Gaussian density bump at a centre seeded by (request index, stream
     seed), so that streams of different seeds hold different systems; the
     first Newton step's system (pseudo-transient term at cfl 10), assembled on
-    the host and cached: (pattern, values, right-hand side)."""
+    the device and cached as host arrays: (pattern, values, right-hand side)."""
     key = (i, seed)
     if key not in _HB_SYSTEMS:
-        from chidg_b200 import euler
+        from chidg_b200 import api, euler
         centre = tuple(float(c) for c in np.random.default_rng((5000 + i, seed)).uniform(0.3, 0.7, 3))
         hb = euler.EulerHB(8, 8, 8, 1, [1.0, 2.0, 3.0], amplitude=1e-2)
         q0 = hb.density_bump(amplitude=1e-2, width=0.1, centre=centre)
-        R, vals = hb.residual(q0, jacobian=True)
-        _HB_SYSTEMS[key] = (hb.pattern, hb.add_pseudo_time(vals, hb.pseudo_timestep(q0, CFL_PTC)), -R)
+        # assembled on the device (every level, the time coupling, the
+        # pseudo-transient term of level 1 on every level's diagonal)
+        ctx = api.default_context()
+        A = api.ChidgMatrix(hb.pattern, ctx)
+        q, r = api.ChidgVector(A, q0), api.ChidgVector(A)
+        dev = euler.EulerHBDevice(hb, ctx)
+        dev.assemble(q, r, A)
+        dtau = dev.pseudo_timestep(q, A, CFL_PTC)
+        A.scale_diagonal(hb.mass, np.repeat(1.0 / dtau.min(axis=1), NVARS))
+        r.scale(-1.0)
+        _HB_SYSTEMS[key] = (hb.pattern, A.download(), r.download())
+        dev.release()
+        for o in (q, r, A):
+            o.release()
     return _HB_SYSTEMS[key]
 
 
