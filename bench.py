@@ -277,30 +277,6 @@ def run_batch_leg(ctx, schedule, reps=3):
             "batched": batched}
 
 
-def serve_requests(count, seed, pinned=True, device=0):
-    """Requests of the batch leg's sizes, every 10th a harmonic-balance one
-    (8^3 box, P1, 7 coupled time levels: 3 harmonics).  The values and
-    right-hand sides arrive in page-locked host memory, as a front end's
-    receive buffers hold them, so the upload is a DMA with no host staging."""
-    import torch
-
-    from chidg_b200 import mesh, serve
-
-    def pin(a):
-        if not pinned:
-            return a
-        t = torch.empty(a.size, dtype=torch.float64, pin_memory=True).numpy()
-        t[:] = a
-        return t
-
-    out = []
-    for i, (p, v, r) in enumerate(uneven_systems(count, seed=seed, device=device)):
-        if i % 10 == 9:
-            p, v, r = hb_system(i, seed)
-        out.append(serve.SolveRequest(p, pin(v), pin(r), tag=i))
-    return out
-
-
 def run_serve_subprocess(device, timeout=900):
     """The serving leg in a fresh process on the same GPU: a request server is
     a process of its own, and its latencies must not depend on what the earlier
@@ -318,30 +294,106 @@ def run_serve_subprocess(device, timeout=900):
     return json.loads(lines[-1])["serving"]
 
 
-def run_serve_leg(device, requests=64, rate=200.0):
+CFG5_REQUESTS = 512
+CFG5_RATE = 200.0           # requests per second, Poisson
+CFG5_SEED = 53
+CFG5_BUDGET = 100 << 30     # device bytes the server admits at once (request_bytes estimates)
+CFG5_SLOTS = 2
+CFG5_MAX_BATCH = 16
+CFG5_UNDER = (96, 12.0)     # a second stream below the GPU's capacity: requests, rate
+
+
+def cfg5_requests(count=CFG5_REQUESTS, seed=CFG5_SEED):
+    """The scope table's serving stream: systems drawn as the many-solve
+    workload's (box sides uniform in 4..16, P in 1..3, Mach U[0.2, 0.6], bump
+    amplitude U[1e-3, 1e-2]), every 10th request instead an Euler
+    harmonic-balance system (8^3 P1, 3 harmonics: 7 coupled time levels, 280
+    rows per element over the levels, sinusoidal inflow of amplitude 1e-2, the
+    draw's Mach and bump).  Each request is the description of its first Newton
+    step's system (euler.NewtonSystem); the server writes the system on the
+    device when it admits the request (chidg_gpu_euler_fill_system), so no
+    request's matrix is ever in host memory."""
+    from chidg_b200 import euler, serve
+    out = []
+    for i, (shape, order, mach, amp, centre) in enumerate(cfg4_draws(count, seed)):
+        if i % 10 == 9:
+            sysm = euler.EulerHB(8, 8, 8, 1, [1.0, 2.0, 3.0], amplitude=1e-2, vel_inf=(mach, 0.0, 0.0))
+        else:
+            sysm = euler.EulerBox(*shape, order, vel_inf=(mach, 0.0, 0.0))
+        desc = euler.NewtonSystem(sysm, sysm.density_bump(amplitude=amp, width=0.1, centre=centre), CFL_PTC)
+        out.append(serve.SolveRequest(desc.pattern, None, None, tag=i, system=desc))
+    return out
+
+
+def batch_phases(log, t0):
+    """Per-phase totals and maxima over a server's batch records (seconds), and
+    the slowest batch's record with its times relative to the stream's start."""
+    keys = [("queued", "formed", "taken"), ("on_device", "taken", "on_device"), ("set_up", "on_device", "set_up"),
+            ("solve", "set_up", "solved"), ("to_host", "solved", "on_host")]
+    out = {}
+    for name, a, b in keys:
+        d = [r[b] - r[a] for r in log]
+        out[name] = {"sum_s": float(np.sum(d)), "max_s": float(np.max(d))} if d else None
+    out["solve_device_s"] = float(np.sum([r["device_ms"] for r in log])) / 1e3 if log else None
+    if log:
+        worst = max(log, key=lambda r: r["on_host"] - r["taken"])
+        out["slowest_batch"] = {k: (round(v - t0, 4) if k not in ("device_ms", "systems", "slot") else v)
+                                for k, v in worst.items()}
+    return out
+
+
+def run_serve_leg(device, runs=1):
+    """The serving configuration as stated: CFG5_REQUESTS requests arriving as
+    a Poisson process at CFG5_RATE per second through the native server (two
+    worker slots, admission by a device-memory budget), FGMRES(30) + ILU0 to
+    rtol 1e-8 (FP64 residual), with FP32 preconditioner blocks and in plain
+    FP64; then a shorter stream at a rate below the GPU's capacity.  Each
+    run's batch records split the time into its phases."""
     from chidg_b200 import serve
-    out = {"arrival_rate_per_s": rate, "requests": requests, "slots": 2, "max_batch": 16,
-           "workload": "Poisson arrivals; Euler Newton systems of boxes 4..8 per side, P in {1,2}, Mach in "
-                       "[0.2, 0.6]; every 10th request an Euler harmonic-balance system (8^3, P1, 7 time levels); "
-                       "FGMRES(30)+ILU0 to rtol 1e-8 (FP64 residual); request values in page-locked host memory; "
-                       "the server in a process of its own"}
-    out["server"] = "native (chidg_gpu_serve_*: dispatcher and worker slots as native threads)"
-    for key, cls, prec in (("fp64", serve.NativeServer, "fp64"),
-                           ("mixed_precon_fp32", serve.NativeServer, "mixed_precon_fp32"),
-                           ("python_server_fp64", serve.Server, "fp64")):
-        reqs = serve_requests(requests, seed=11, device=device)
-        srv = cls(device=device, slots=2, max_batch=16, mem_budget=40 << 30, **BATCH_OPTS, precision=prec)
+    reqs = cfg5_requests()
+    under = cfg5_requests(CFG5_UNDER[0], seed=CFG5_SEED + 1)
+    # warm-up: the smallest request of each kind (order, time levels) among a few draws
+    kinds = {}
+    for r in cfg5_requests(40, seed=CFG5_SEED + 2):
+        k = (int(r.pattern.elem_nterms[0]), r.pattern.ntime)
+        if k not in kinds or r.pattern.nelem < kinds[k].pattern.nelem:
+            kinds[k] = r
+    warm = list(kinds.values())
+    out = {"workload": "Poisson arrivals of Euler Newton systems drawn as the many-solve workload (box sides 4..16, "
+                       "P 1..3, Mach U[0.2, 0.6]), every 10th an Euler harmonic-balance system (8^3 P1, 7 levels); "
+                       "each written on the device when admitted; FGMRES(30) + ILU0 to rtol 1e-8 (FP64 residual); "
+                       "the server in a process of its own",
+           "requests": len(reqs), "arrival_rate_per_s": CFG5_RATE, "slots": CFG5_SLOTS, "max_batch": CFG5_MAX_BATCH,
+           "mem_budget_bytes": CFG5_BUDGET, "server": "native (chidg_gpu_serve_*, chidg_gpu_serve_submit_fill)",
+           "harmonic_balance_requests": sum(1 for r in reqs if r.pattern.ntime > 1),
+           "matrix_bytes_fp64": int(sum(8 * r.pattern.value_offsets()[1] for r in reqs)),
+           "below_capacity": {"requests": CFG5_UNDER[0], "arrival_rate_per_s": CFG5_UNDER[1]}}
+
+    def stream(prec, rq, rate, seed):
+        srv = serve.NativeServer(device=device, slots=CFG5_SLOTS, max_batch=CFG5_MAX_BATCH, mem_budget=CFG5_BUDGET,
+                                 **CFG4_OPTS, precision=prec)
         try:
-            # warm-up: a batch of the stream's kinds (P1 and P2 boxes, one harmonic-balance system)
-            for f in [srv.submit(r) for r in serve_requests(10, seed=12, device=device)]:
+            for f in [srv.submit(r) for r in warm]:
                 f.result()
-            st = serve.run_stream(srv, reqs, serve.poisson_arrivals(requests, rate, seed=5))
+            nwarm = srv.batches
+            t0 = time.perf_counter()
+            st = serve.run_stream(srv, rq, serve.poisson_arrivals(len(rq), rate, seed=seed))
+            log = srv.batch_log()[nwarm:]
         finally:
             srv.close()
         res = st.pop("results")
         st["max_true_rel_residual"] = max(r.residual_norm / r.r0norm_initial for r in res)
-        st.pop("requests", None)
-        out[key] = st
+        st["mean_iterations"] = float(np.mean([r.niter for r in res]))
+        st["batches"] = len(log)
+        st["phases"] = batch_phases(log, t0)
+        return st
+
+    for prec in ("mixed_precon_fp32", "fp64"):
+        results = [stream(prec, reqs, CFG5_RATE, 5) for _ in range(runs)]
+        out[prec] = results[0] if runs == 1 else {"runs": results}
+        out["below_capacity"][prec] = stream(prec, under, CFG5_UNDER[1], 6)
+    first = (lambda v: v if "runs" not in v else v["runs"][0])
+    out["speedup_mixed_vs_fp64"] = first(out["mixed_precon_fp32"])["solves_per_s"] / first(out["fp64"])["solves_per_s"]
     return out
 
 
@@ -661,30 +713,22 @@ def cfg4_waves(draws, wave_bytes=CFG4_WAVE_BYTES):
 
 def cfg4_arena(ctx, draws):
     """One wave's systems packed block-diagonally into one matrix, each
-    system's first Newton step assembled on the device straight into its
-    slice (chidg_gpu_euler_assemble_at), the pseudo-transient term at cfl 10
-    added, b = -R(q0).  Returns (A, b, sys_elem, seconds)."""
+    system's first Newton step written on the device straight into its slice
+    (chidg_gpu_euler_fill_system: dR/dq(q0) + the pseudo-transient term at cfl
+    CFL_PTC, b = -R(q0)).  Returns (A, b, sys_elem, seconds)."""
     from chidg_b200 import api, euler, mesh
-    boxes, q0s = [], []
+    descs = []
     for shape, order, mach, amp, centre in draws:
         bx = euler.EulerBox(*shape, order, vel_inf=(mach, 0.0, 0.0))
-        boxes.append(bx)
-        q0s.append(bx.density_bump(amplitude=amp, width=0.1, centre=centre))
-    union, sys_elem = mesh.concat_patterns([bx.pattern for bx in boxes])
+        descs.append(euler.NewtonSystem(bx, bx.density_bump(amplitude=amp, width=0.1, centre=centre), CFL_PTC))
+    union, sys_elem = mesh.concat_patterns([d.pattern for d in descs])
     t0 = time.perf_counter()
     A = api.ChidgMatrix(union, ctx)
-    q = api.ChidgVector(A, np.concatenate(q0s))
-    rhs = api.ChidgVector(A)
-    scale = []
-    for bx, e0 in zip(boxes, sys_elem[:-1]):
-        dev = euler.EulerDevice(bx, ctx)
-        dev.assemble_at(A, int(e0), q, rhs, True)
-        scale.append(np.repeat(1.0 / dev.pseudo_timestep_at(A, int(e0), q, CFL_PTC).min(axis=1), NVARS))
-        dev.release()
-    A.scale_diagonal(np.concatenate([bx.mass for bx in boxes]), np.concatenate(scale))
-    rhs.scale(-1.0)
+    rhs, work = api.ChidgVector(A), api.ChidgVector(A)
+    for d, e0 in zip(descs, sys_elem[:-1]):
+        d.fill(A, rhs, work, int(e0))
     ctx.sync()
-    q.release()
+    work.release()
     return A, rhs, sys_elem, time.perf_counter() - t0
 
 
@@ -1172,16 +1216,16 @@ def run_gpu(args):
     hb = run_hb_leg(ctx, stream, args.schedule) if not args.no_hb else None
     newton = run_newton_leg(ctx) if not args.no_newton else None
     batch = run_batch_leg(ctx, args.schedule) if not args.no_batch else None
-    serving = run_serve_subprocess(local) if not args.no_serve else None
     assembly = run_assembly_leg(ctx, stream, A) if not args.no_assembly else None
     cfg4 = run_cfg4_leg(ctx, args.schedule) if not args.no_cfg4 else None
-    cfg3 = None
-    if not args.no_cfg3 and world == 1:
-        # the 24^3 objects leave the device first: the 32^3 legs hold ~120 GB
-        M.tear_down()
-        for o in (x, b, A):
-            o.release()
-        cfg3 = run_cfg3_leg(ctx, stream, args.schedule)
+    # the 24^3 objects leave the device first: the 32^3 legs hold ~120 GB, the
+    # serving process admits up to CFG5_BUDGET
+    M.tear_down()
+    for o in (x, b, A):
+        o.release()
+    ctx.sync()
+    cfg3 = run_cfg3_leg(ctx, stream, args.schedule) if not args.no_cfg3 and world == 1 else None
+    serving = run_serve_subprocess(local) if not args.no_serve else None
 
     if rank != 0:
         return 0
@@ -1283,11 +1327,12 @@ def main():
                     help="skip the 512-system many-solve leg (sides 4..16, P 1..3, memory-admitted waves)")
     ap.add_argument("--serve-only", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--serve-device", type=int, default=0, help=argparse.SUPPRESS)
+    ap.add_argument("--serve-runs", type=int, default=1, help="streams per precision in the serving leg")
     args = ap.parse_args()
     if args.serve_only:
         import torch
         torch.cuda.set_device(args.serve_device)
-        print(json.dumps({"serving": run_serve_leg(args.serve_device)}), flush=True)
+        print(json.dumps({"serving": run_serve_leg(args.serve_device, runs=args.serve_runs)}), flush=True)
         return 0
     if args.impl == "reference":
         return run_reference(args)

@@ -39,6 +39,16 @@ class EulerBoxDesc(C.Structure):
 EULER_FARFIELD, EULER_EXTRAPOLATE = 0, 1
 
 
+class EulerSystemDesc(C.Structure):
+    """chidg_gpu_euler_system"""
+    _fields_ = [("box", EulerBoxDesc), ("ntime", C.c_int32), ("level_vel", DP), ("D", DP), ("mass", DP),
+                ("q0", DP), ("cfl", C.c_double)]
+
+
+# chidg_gpu_fill_fn
+FILL_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32)
+
+
 class Pattern(C.Structure):
     _fields_ = [("nelem", C.c_int32), ("ntime", C.c_int32), ("elem_nvars", I32P), ("elem_nterms", I32P),
                 ("elem_proc", I32P), ("nblocks", C.c_int64), ("blk_row_elem", I32P), ("blk_row_time", I32P),
@@ -114,6 +124,10 @@ PROTOTYPES = {
     "chidg_gpu_euler_assemble_level": (C.c_int, [VP, VP, C.c_int32, VP, VP, C.c_int32]),
     "chidg_gpu_euler_pseudo_timestep_level": (C.c_int, [VP, VP, C.c_int32, VP, DP, DP]),
     "chidg_gpu_hb_coupling": (C.c_int, [VP, C.c_int32, DP, DP, VP, VP, C.c_int32]),
+    "chidg_gpu_euler_assemble_level_at": (C.c_int, [VP, VP, C.c_int32, C.c_int32, VP, VP, C.c_int32]),
+    "chidg_gpu_hb_coupling_at": (C.c_int, [VP, C.c_int32, C.c_int32, C.c_int32, DP, DP, VP, VP, C.c_int32]),
+    "chidg_gpu_euler_pseudo_transient_at": (C.c_int, [VP, VP, C.c_int32, VP, VP, DP, DP]),
+    "chidg_gpu_euler_fill_system": (C.c_int, [VP, VP, VP, VP, VP, C.c_int32]),
     "chidg_gpu_stream_shape_get": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, I32P, I32P, I32P]),
     "chidg_gpu_stream_shape_set": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
     "chidg_gpu_euler_create": (C.c_int, [VP, VP, C.POINTER(VP)]),
@@ -125,6 +139,8 @@ PROTOTYPES = {
     "chidg_gpu_serve_wait": (C.c_int, [VP, C.c_int64, VP, VP, VP]),
     "chidg_gpu_serve_stats": (C.c_int, [VP, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "chidg_gpu_serve_destroy": (C.c_int, [VP]),
+    "chidg_gpu_serve_submit_fill": (C.c_int, [VP, VP, VP, VP, C.POINTER(C.c_int64)]),
+    "chidg_gpu_serve_batch_log": (C.c_int, [VP, C.c_int64, DP]),
     "chidg_gpu_precon_create": (C.c_int, [VP, C.c_int32, C.POINTER(VP)]),
     "chidg_gpu_precon_destroy": (C.c_int, [VP]),
     "chidg_gpu_precon_update": (C.c_int, [VP, VP, C.c_int32]),

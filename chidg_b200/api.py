@@ -126,9 +126,17 @@ class ChidgMatrix:
             raise ValueError(f"expected {self.nvalues} values in total")
         first = 0
         for p in parts:
-            self.ctx.check(self.ctx.L.chidg_gpu_matrix_upload_range(self.h, _ptr(p), first, p.size), "matrix_upload_range")
+            self.upload_range(p, first)
             first += p.size
         self.ctx.sync()
+
+    def upload_range(self, values: np.ndarray, first: int):
+        """values into the packed entries first.. (queued on the context's
+        stream: from page-locked memory the array must live until a sync)."""
+        if values.dtype != np.float64 or not values.flags.c_contiguous:
+            raise ValueError("upload_range: a contiguous float64 array")
+        self.ctx.check(self.ctx.L.chidg_gpu_matrix_upload_range(self.h, _ptr(values), int(first), values.size),
+                       "matrix_upload_range")
 
     def upload_blocks(self, blocks):
         """One array per block (each densematrix_t%mat), in pattern order."""
@@ -244,9 +252,16 @@ class ChidgVector:
             raise ValueError("vector size mismatch")
         first = 0
         for p in parts:
-            self.ctx.check(self.ctx.L.chidg_gpu_vector_upload_range(self.h, _ptr(p), first, p.size), "vector_upload_range")
+            self.upload_range(p, first)
             first += p.size
         self.ctx.sync()
+
+    def upload_range(self, values: np.ndarray, first: int):
+        """values into entries first.. (queued, as ChidgMatrix.upload_range)."""
+        if values.dtype != np.float64 or not values.flags.c_contiguous:
+            raise ValueError("upload_range: a contiguous float64 array")
+        self.ctx.check(self.ctx.L.chidg_gpu_vector_upload_range(self.h, _ptr(values), int(first), values.size),
+                       "vector_upload_range")
 
     def download(self) -> np.ndarray:
         out = np.empty(self.n)

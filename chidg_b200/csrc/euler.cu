@@ -669,7 +669,7 @@ struct chidg_gpu_euler {
     BoxGeom g{};
     int order = 0, nelem = 0;
     double h = 0.0;
-    Buffer phi, grad, wv, phif, wf, dtau;
+    Buffer phi, grad, wv, phif, wf, dtau, mass;
     Buffer blk_off;
     int64_t off_uid = 0;                           // matrix (uid) the block-offset table was built for
     int32_t off_elem0 = -1;                        // and the element the box starts at in it
@@ -787,7 +787,7 @@ extern "C" int chidg_gpu_euler_create(chidg_gpu_ctx* ctx, const chidg_gpu_euler_
 
 extern "C" int chidg_gpu_euler_destroy(chidg_gpu_euler* E) {
     if (!E) return CHIDG_GPU_OK;
-    for (Buffer* b : {&E->phi, &E->grad, &E->wv, &E->phif, &E->wf, &E->dtau, &E->blk_off}) release(*b);
+    for (Buffer* b : {&E->phi, &E->grad, &E->wv, &E->phif, &E->wf, &E->dtau, &E->mass, &E->blk_off}) release(*b);
     delete E;
     return CHIDG_GPU_OK;
 }
@@ -808,15 +808,20 @@ int check_vector(chidg_gpu_euler* E, const chidg_gpu_vector* v, const char* what
 // The box placed at elements elem0 .. elem0 + nelem - 1 of A's layout: its
 // elements must have 5 fields and the box's modes on one time level; returns
 // the vector offset of its first element.
-int box_in_layout(chidg_gpu_euler* E, const chidg_gpu_matrix* A, int32_t elem0, int64_t* voff) {
+int box_fits(chidg_gpu_euler* E, const chidg_gpu_matrix* A, int32_t elem0, int64_t* voff) {
     if (!A || A->ctx != E->ctx) return fail(E->ctx, CHIDG_GPU_EINVAL, "euler: matrix of another context");
-    if (elem0 < 0 || (int64_t)elem0 + E->nelem > A->nelem || A->ntime != 1)
+    if (elem0 < 0 || (int64_t)elem0 + E->nelem > A->nelem)
         return fail(E->ctx, CHIDG_GPU_EINVAL, "euler: the box does not fit the matrix's elements");
     for (int e = 0; e < E->nelem; ++e)
         if (A->nvars[elem0 + e] != 5 || A->nterms[elem0 + e] != E->g.nt)
             return fail(E->ctx, CHIDG_GPU_EINVAL, "euler: element fields or modes differ from the box");
     *voff = A->eoff[elem0];
     return CHIDG_GPU_OK;
+}
+
+int box_in_layout(chidg_gpu_euler* E, const chidg_gpu_matrix* A, int32_t elem0, int64_t* voff) {
+    if (A && A->ntime != 1) return fail(E->ctx, CHIDG_GPU_EINVAL, "euler: the matrix has several time levels");
+    return box_fits(E, A, elem0, voff);
 }
 
 // Offsets of each element's blocks in A's values: [e][face 0..5, DIAG], -1 on
@@ -961,19 +966,26 @@ extern "C" int chidg_gpu_euler_pseudo_timestep_at(chidg_gpu_euler* E, chidg_gpu_
 }
 
 // ---- harmonic balance --------------------------------------------------------------
-extern "C" int chidg_gpu_euler_assemble_level(chidg_gpu_euler* E, chidg_gpu_matrix* A, int32_t itime, chidg_gpu_vector* q,
-                                              chidg_gpu_vector* rhs, int32_t jacobian) {
-    if (!E || !A || !q || !rhs) return E ? fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble_level: null argument") : CHIDG_GPU_EINVAL;
+extern "C" int chidg_gpu_euler_assemble_level_at(chidg_gpu_euler* E, chidg_gpu_matrix* A, int32_t elem0, int32_t itime,
+                                                 chidg_gpu_vector* q, chidg_gpu_vector* rhs, int32_t jacobian) {
+    if (!E || !A || !q || !rhs)
+        return E ? fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble_level: null argument") : CHIDG_GPU_EINVAL;
     if (q == rhs) return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble_level: q and rhs must differ");
     if (q->A != A || rhs->A != A) return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble_level: q and rhs must be vectors of A");
-    if (A->ctx != E->ctx || A->nelem != E->nelem || itime < 0 || itime >= A->ntime)
-        return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble_level: matrix is not this box's or no such time level");
-    for (int e = 0; e < E->nelem; ++e)
-        if (A->nvars[e] != 5 || A->nterms[e] != E->g.nt)
-            return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble_level: element fields or modes differ from the box");
+    if (itime < 0 || itime >= A->ntime) return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble_level: no such time level");
+    int64_t voff = 0;
+    int st = box_fits(E, A, elem0, &voff);
+    if (st) return st;
     const int64_t b = (int64_t)5 * E->g.nt, vs = b * A->ntime;
-    return assemble_ptrs(E, (const double*)q->buf.ptr + itime * b, (double*)rhs->buf.ptr + itime * b, jacobian ? A : nullptr,
-                         0, itime, vs);
+    return assemble_ptrs(E, (const double*)q->buf.ptr + voff + itime * b, (double*)rhs->buf.ptr + voff + itime * b,
+                         jacobian ? A : nullptr, elem0, itime, vs);
+}
+
+extern "C" int chidg_gpu_euler_assemble_level(chidg_gpu_euler* E, chidg_gpu_matrix* A, int32_t itime, chidg_gpu_vector* q,
+                                              chidg_gpu_vector* rhs, int32_t jacobian) {
+    if (E && A && A->nelem != E->nelem)
+        return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_assemble_level: matrix is not this box's");
+    return chidg_gpu_euler_assemble_level_at(E, A, 0, itime, q, rhs, jacobian);
 }
 
 extern "C" int chidg_gpu_euler_pseudo_timestep_level(chidg_gpu_euler* E, chidg_gpu_matrix* A, int32_t itime,
@@ -984,6 +996,68 @@ extern "C" int chidg_gpu_euler_pseudo_timestep_level(chidg_gpu_euler* E, chidg_g
         return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_pseudo_timestep_level: q of another layout or no such time level");
     const int64_t b = (int64_t)5 * E->g.nt;
     return dtau_ptrs(E, (const double*)q->buf.ptr + itime * b, cfl, dtau, b * A->ntime);
+}
+
+// ---- the pseudo-transient term and b = -R on the device -------------------------
+namespace {
+// rows (elem0 + e, t) of the box, one CTA each (t fastest): field f's diagonal
+// sub-block of the DIAG block += M / min_f' dtau(e, f') (contribute_pseudo_temporal
+// applies minval(elems(ielem)%dtau) to every field and time level)
+__global__ void k_ptc_add(double* __restrict__ val, const int64_t* __restrict__ diag_voff, int row0, int ntime, int nt,
+                          const double* __restrict__ dtau, const double* __restrict__ M) {
+    const int r = blockIdx.x;
+    const int e = r / ntime, b = 5 * nt;
+    const double* d = dtau + (int64_t)e * 5;
+    const double s = 1.0 / fmin(fmin(fmin(fmin(d[0], d[1]), d[2]), d[3]), d[4]);
+    double* D = val + diag_voff[row0 + r];
+    for (int idx = threadIdx.x; idx < 5 * nt * nt; idx += blockDim.x) {
+        const int f = idx / (nt * nt), rem = idx - f * nt * nt, i = rem % nt, j = rem / nt;
+        D[(int64_t)(f * nt + i) + (int64_t)(f * nt + j) * b] += s * M[i + j * nt];
+    }
+}
+
+__global__ void k_negate(double* __restrict__ x, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) x[i] = -x[i];
+}
+}  // namespace
+
+extern "C" int chidg_gpu_euler_pseudo_transient_at(chidg_gpu_euler* E, chidg_gpu_matrix* A, int32_t elem0,
+                                                   chidg_gpu_vector* q, chidg_gpu_vector* rhs, const double* cfl,
+                                                   const double* mass) {
+    if (!E || !A || !q || !cfl || !mass)
+        return E ? fail(E->ctx, CHIDG_GPU_EINVAL, "euler_pseudo_transient_at: null argument") : CHIDG_GPU_EINVAL;
+    if (q->A != A || (rhs && (rhs->A != A || rhs == q)))
+        return fail(E->ctx, CHIDG_GPU_EINVAL, "euler_pseudo_transient_at: q and rhs must be distinct vectors of A");
+    int64_t voff = 0;
+    int st = box_fits(E, A, elem0, &voff);
+    if (st) return st;
+    chidg_gpu_ctx* ctx = E->ctx;
+    const int nt = E->g.nt, T = A->ntime;
+    const int64_t b = (int64_t)5 * nt, vs = b * T;
+    const double c[5] = {cfl[0], cfl[1], cfl[2], cfl[3], cfl[4]};
+    const dim3 grid(E->nelem), block(kThreads);
+    const Tables tb = tables_of(E);
+    const double* qp = (const double*)q->buf.ptr + voff;
+    double* dt = (double*)E->dtau.ptr;
+    if (E->order == 0) k_euler_dtau<1><<<grid, block, 0, ctx->stream>>>(E->g, tb, qp, vs, E->h, c[0], c[1], c[2], c[3], c[4], dt);
+    else if (E->order == 1) k_euler_dtau<8><<<grid, block, 0, ctx->stream>>>(E->g, tb, qp, vs, E->h, c[0], c[1], c[2], c[3], c[4], dt);
+    else if (E->order == 2) k_euler_dtau<27><<<grid, block, 0, ctx->stream>>>(E->g, tb, qp, vs, E->h, c[0], c[1], c[2], c[3], c[4], dt);
+    else k_euler_dtau<64><<<grid, block, 0, ctx->stream>>>(E->g, tb, qp, vs, E->h, c[0], c[1], c[2], c[3], c[4], dt);
+    if ((st = check_launch(ctx, "k_euler_dtau"))) return st;
+    if ((st = ensure(ctx, E->mass, (size_t)nt * nt * sizeof(double)))) return st;
+    // from pageable memory the copy returns once the bytes are staged, so the caller's array may go
+    cudaError_t ce = cudaMemcpyAsync(E->mass.ptr, mass, (size_t)nt * nt * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+    if (ce != cudaSuccess) return cuda_fail(ctx, ce, "euler_pseudo_transient_at: mass");
+    k_ptc_add<<<E->nelem * T, 256, 0, ctx->stream>>>((double*)A->val.ptr, (const int64_t*)A->d_diag_voff.ptr, elem0 * T, T,
+                                                    nt, dt, (const double*)E->mass.ptr);
+    if ((st = check_launch(ctx, "k_ptc_add"))) return st;
+    A->stamp++;
+    if (rhs) {
+        const int64_t n = (int64_t)E->nelem * vs;
+        k_negate<<<(int)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, ctx->stream>>>((double*)rhs->buf.ptr + voff, n);
+        if ((st = check_launch(ctx, "k_negate"))) return st;
+    }
+    return CHIDG_GPU_OK;
 }
 
 namespace {
@@ -1032,20 +1106,22 @@ __global__ void k_hb_blocks(double* __restrict__ val, const int64_t* __restrict_
 }
 }  // namespace
 
-extern "C" int chidg_gpu_hb_coupling(chidg_gpu_matrix* A, int32_t nterms, const double* D, const double* mass,
-                                     chidg_gpu_vector* q, chidg_gpu_vector* rhs, int32_t jacobian) {
-    if (!A || !D || !mass || !q || !rhs || q == rhs || q->A != A || rhs->A != A || nterms < 1)
+extern "C" int chidg_gpu_hb_coupling_at(chidg_gpu_matrix* A, int32_t elem0, int32_t nelem, int32_t nterms, const double* D,
+                                        const double* mass, chidg_gpu_vector* q, chidg_gpu_vector* rhs, int32_t jacobian) {
+    if (!A || !D || !mass || !q || !rhs || q == rhs || q->A != A || rhs->A != A || nterms < 1 || elem0 < 0 || nelem < 1 ||
+        (int64_t)elem0 + nelem > A->nelem)
         return A ? fail(A->ctx, CHIDG_GPU_EINVAL, "hb_coupling: bad argument") : CHIDG_GPU_EINVAL;
     chidg_gpu_ctx* ctx = A->ctx;
     cudaSetDevice(ctx->device);
     const int T = A->ntime;
-    for (int e = 0; e < A->nelem; ++e)
+    const int e1 = elem0 + nelem;
+    for (int e = elem0; e < e1; ++e)
         if (A->nterms[e] != nterms) return fail(ctx, CHIDG_GPU_EINVAL, "hb_coupling: elements of another mode count");
     std::vector<int32_t> hb_rt, hb_ct, hb_b;
     std::vector<int64_t> hb_off;
     if (jacobian)
         for (int64_t k = 0; k < A->nblk; ++k)
-            if (A->kind[k] == CHIDG_BLK_HB) {
+            if (A->kind[k] == CHIDG_BLK_HB && A->re[k] >= elem0 && A->re[k] < e1) {
                 if (A->re[k] != A->ce[k]) return fail(ctx, CHIDG_GPU_EINVAL, "hb_coupling: an hb block couples two elements");
                 hb_rt.push_back(A->rt[k]);
                 hb_ct.push_back(A->ct[k]);
@@ -1056,12 +1132,14 @@ extern "C" int chidg_gpu_hb_coupling(chidg_gpu_matrix* A, int32_t nterms, const 
     auto cleanup = [&]() { for (Buffer* x : {&dD, &dM, &dE, &dV, &bo, &br, &bc, &bb}) release(*x); };
     int st;
     std::vector<double> hD(D, D + (size_t)T * T), hM(mass, mass + (size_t)nterms * nterms);
-    if ((st = upload_array(ctx, dD, hD)) || (st = upload_array(ctx, dM, hM)) || (st = upload_array(ctx, dE, A->eoff)) ||
-        (st = upload_array(ctx, dV, A->nvars))) {
+    const std::vector<int64_t> eo(A->eoff.begin() + elem0, A->eoff.begin() + e1);
+    const std::vector<int32_t> nv(A->nvars.begin() + elem0, A->nvars.begin() + e1);
+    if ((st = upload_array(ctx, dD, hD)) || (st = upload_array(ctx, dM, hM)) || (st = upload_array(ctx, dE, eo)) ||
+        (st = upload_array(ctx, dV, nv))) {
         cleanup();
         return st;
     }
-    k_hb_residual<<<A->nelem, 256, 0, ctx->stream>>>((const double*)q->buf.ptr, (double*)rhs->buf.ptr, (const int64_t*)dE.ptr,
+    k_hb_residual<<<nelem, 256, 0, ctx->stream>>>((const double*)q->buf.ptr, (double*)rhs->buf.ptr, (const int64_t*)dE.ptr,
                                                      (const int32_t*)dV.ptr, T, nterms, (const double*)dD.ptr,
                                                      (const double*)dM.ptr);
     if ((st = check_launch(ctx, "k_hb_residual"))) { cleanup(); return st; }
@@ -1081,4 +1159,48 @@ extern "C" int chidg_gpu_hb_coupling(chidg_gpu_matrix* A, int32_t nterms, const 
     const cudaError_t ce = cudaStreamSynchronize(ctx->stream);     // the host copies and buffers go out of scope
     cleanup();
     return ce == cudaSuccess ? CHIDG_GPU_OK : cuda_fail(ctx, ce, "hb_coupling");
+}
+
+extern "C" int chidg_gpu_hb_coupling(chidg_gpu_matrix* A, int32_t nterms, const double* D, const double* mass,
+                                     chidg_gpu_vector* q, chidg_gpu_vector* rhs, int32_t jacobian) {
+    if (!A) return CHIDG_GPU_EINVAL;
+    return chidg_gpu_hb_coupling_at(A, 0, A->nelem, nterms, D, mass, q, rhs, jacobian);
+}
+
+// ---- a Newton system written in place (the serving and batching callers) ---------
+extern "C" int chidg_gpu_euler_fill_system(void* user, chidg_gpu_ctx* ctx, chidg_gpu_matrix* A, chidg_gpu_vector* b,
+                                           chidg_gpu_vector* work, int32_t elem0) {
+    const auto* S = static_cast<const chidg_gpu_euler_system*>(user);
+    if (!S || !ctx || !A || !b || !work || A->ctx != ctx || b->A != A || work->A != A || b == work || !S->q0 || !S->mass)
+        return ctx ? fail(ctx, CHIDG_GPU_EINVAL, "euler_fill_system: bad argument") : CHIDG_GPU_EINVAL;
+    const int T = S->ntime;
+    if (T < 1 || T != A->ntime || (T > 1 && (!S->level_vel || !S->D)))
+        return fail(ctx, CHIDG_GPU_EINVAL, "euler_fill_system: time levels differ from the matrix's or no hb operator");
+    std::vector<chidg_gpu_euler*> lv((size_t)T, nullptr);
+    auto done = [&](int st) {
+        for (chidg_gpu_euler* E : lv) chidg_gpu_euler_destroy(E);
+        return st;
+    };
+    for (int t = 0; t < T; ++t) {
+        chidg_gpu_euler_box box = S->box;
+        if (T > 1)
+            for (int d = 0; d < 3; ++d) box.vel_inf[d] = S->level_vel[3 * t + d];
+        const int st = chidg_gpu_euler_create(ctx, &box, &lv[t]);
+        if (st) return done(st);
+    }
+    int64_t voff = 0;
+    int st = box_fits(lv[0], A, elem0, &voff);
+    if (st) return done(st);
+    const int nelem = lv[0]->nelem, nt = lv[0]->g.nt;
+    if ((st = chidg_gpu_vector_upload_range(work, S->q0, voff, (int64_t)nelem * T * 5 * nt))) return done(st);
+    for (int t = 0; t < T && !st; ++t) st = chidg_gpu_euler_assemble_level_at(lv[t], A, elem0, t, work, b, 1);
+    if (!st && T > 1) st = chidg_gpu_hb_coupling_at(A, elem0, nelem, nt, S->D, S->mass, work, b, 1);
+    const double cfl[5] = {S->cfl, S->cfl, S->cfl, S->cfl, S->cfl};
+    if (!st) st = chidg_gpu_euler_pseudo_transient_at(lv[0], A, elem0, work, b, cfl, S->mass);
+    if (!st) {
+        // the caller's arrays (q0, mass) are not read after this returns
+        const cudaError_t ce = cudaStreamSynchronize(ctx->stream);
+        if (ce != cudaSuccess) st = cuda_fail(ctx, ce, "euler_fill_system");
+    }
+    return done(st);
 }

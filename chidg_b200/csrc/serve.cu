@@ -10,8 +10,12 @@
 // own, so batches run concurrently; a batch is solved by
 // chidg_gpu_fgmres_solve_batched, whose
 // per-system arithmetic does not depend on the other systems of the batch.
+// A request either hands over host arrays (uploaded into the batch in place)
+// or a fill function that writes its system on the device when the batch is
+// formed.  Every batch leaves a record of its phases (host clock) and of its
+// solve's device time (CUDA events on the worker's stream).
 // Host code only: no kernel of its own.
-#include "../../include/chidg_gpu.h"
+#include "chidg_gpu_internal.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -33,6 +37,8 @@ struct Request {
     std::vector<int32_t> nvars, nterms, proc, re, rt, ce, ct, kind;
     const double* values = nullptr;      // caller-owned until the request's wait returns
     const double* rhs = nullptr;
+    chidg_gpu_fill_fn fill = nullptr;    // or: the system is written on the device by fill(user, ...)
+    void* user = nullptr;
     int64_t nval = 0, n = 0, bytes = 0;
     double arrival = 0, start = 0, finish = 0;
     int32_t batch_size = 0;
@@ -46,6 +52,15 @@ struct Request {
 struct Job {
     std::vector<std::shared_ptr<Request>> batch;
     int64_t bytes = 0;
+    int64_t index = 0;                   // the batch's number, in the order batches are formed
+};
+
+// formed, taken, on the device, set up, solved, on the host; device ms; systems; slot
+struct BatchRecord {
+    double t[6] = {0, 0, 0, 0, 0, 0};
+    double device_ms = 0;
+    int32_t nsys = 0, slot = -1;
+    bool finished = false;
 };
 
 }  // namespace
@@ -67,6 +82,7 @@ struct chidg_gpu_server {
     int idle = 0;                            // workers without a batch
     int64_t mem_used = 0, peak_mem = 0, batches = 0;
     std::vector<chidg_gpu_ctx*> all_ctx;
+    std::vector<BatchRecord> log;            // one per formed batch
     std::thread dispatcher;
     std::vector<std::thread> workers;
 
@@ -83,8 +99,11 @@ int64_t request_bytes(int64_t nval, int64_t n, int32_t nkrylov) {
     return 8 * nval * 2 + 8 * n * (2 * ((int64_t)nkrylov + 1) + 6);
 }
 
-void run_batch(chidg_gpu_server* S, chidg_gpu_ctx* ctx, std::vector<std::shared_ptr<Request>> batch, int64_t bytes) {
-    const double start = S->now();
+void run_batch(chidg_gpu_server* S, chidg_gpu_ctx* ctx, int slot, Job job) {
+    std::vector<std::shared_ptr<Request>>& batch = job.batch;
+    double ph[6] = {0, 0, 0, 0, 0, 0};
+    ph[1] = S->now();
+    cudaSetDevice(ctx->device);
     const int nsys = (int)batch.size();
     // the packed pattern: system s owns elements sys_elem[s] .. sys_elem[s+1]-1
     std::vector<int32_t> nv, nt, pr, re, rt, ce, ct, kd, sys_elem(nsys + 1, 0);
@@ -115,26 +134,46 @@ void run_batch(chidg_gpu_server* S, chidg_gpu_ctx* ctx, std::vector<std::shared_
     std::vector<chidg_gpu_fgmres_result> res(nsys);
     std::vector<double> xh;
     int st = chidg_gpu_matrix_create(ctx, &pat, &A);
-    if (!st) {
-        int64_t v0 = 0;
-        for (int s = 0; s < nsys && !st; ++s) { st = chidg_gpu_matrix_upload_range(A, batch[s]->values, v0, batch[s]->nval); v0 += batch[s]->nval; }
-    }
     if (!st) st = chidg_gpu_vector_create(A, &b);
     if (!st) st = chidg_gpu_vector_create(A, &x);
-    if (!st) {
-        int64_t o = 0;
-        for (int s = 0; s < nsys && !st; ++s) { st = chidg_gpu_vector_upload_range(b, batch[s]->rhs, o, batch[s]->n); o += batch[s]->n; }
+    {
+        int64_t v0 = 0, o = 0;
+        for (int s = 0; s < nsys && !st; ++s) {
+            const Request& q = *batch[s];
+            if (q.fill) {
+                st = q.fill(q.user, ctx, A, b, x, sys_elem[s]);
+            } else {
+                st = chidg_gpu_matrix_upload_range(A, q.values, v0, q.nval);
+                if (!st) st = chidg_gpu_vector_upload_range(b, q.rhs, o, q.n);
+            }
+            v0 += q.nval;
+            o += q.n;
+        }
     }
+    if (!st) st = chidg_gpu_vector_clear(x);        // the initial guess (fill functions may use x as scratch)
+    if (!st) st = chidg_gpu_ctx_sync(ctx);
+    ph[2] = S->now();
     if (!st) st = chidg_gpu_precon_create(A, S->precon_kind, &M);
+    ph[3] = S->now();
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    const bool timed = cudaEventCreate(&ev[0]) == cudaSuccess && cudaEventCreate(&ev[1]) == cudaSuccess;
+    if (timed) cudaEventRecord(ev[0], ctx->stream);
     if (!st) st = chidg_gpu_fgmres_solve_batched(A, M, nsys, sys_elem.data(), b, x, &S->opts, res.data(), nullptr, 0);
+    if (timed) cudaEventRecord(ev[1], ctx->stream);
+    ph[4] = S->now();
     if (!st) { xh.resize((size_t)n); st = chidg_gpu_vector_download(x, xh.data()); }
+    float dev_ms = 0.0f;
+    if (timed && (cudaEventSynchronize(ev[1]) != cudaSuccess || cudaEventElapsedTime(&dev_ms, ev[0], ev[1]) != cudaSuccess))
+        dev_ms = -1.0f;
+    for (cudaEvent_t e : ev)
+        if (e) cudaEventDestroy(e);
     std::string err;
     if (st) {
         char buf[512] = {0};
         chidg_gpu_last_error(ctx, buf, (int32_t)sizeof(buf));
         err = buf;
     }
-    const double finish = S->now();
+    ph[5] = S->now();
     if (M) chidg_gpu_precon_destroy(M);
     if (x) chidg_gpu_vector_destroy(x);
     if (b) chidg_gpu_vector_destroy(b);
@@ -146,8 +185,8 @@ void run_batch(chidg_gpu_server* S, chidg_gpu_ctx* ctx, std::vector<std::shared_
         Request& q = *batch[s];
         q.status = st;
         q.error = err;
-        q.start = start;
-        q.finish = finish;
+        q.start = ph[1];
+        q.finish = ph[5];
         q.batch_size = nsys;
         if (!st) {
             q.result = res[s];
@@ -156,12 +195,18 @@ void run_batch(chidg_gpu_server* S, chidg_gpu_ctx* ctx, std::vector<std::shared_
         o += q.n;
         q.done = true;
     }
-    S->mem_used -= bytes;
+    BatchRecord& r = S->log[(size_t)job.index];
+    for (int i = 1; i < 6; ++i) r.t[i] = ph[i];
+    r.device_ms = dev_ms;
+    r.nsys = nsys;
+    r.slot = slot;
+    r.finished = true;
+    S->mem_used -= job.bytes;
     ++S->idle;
     S->cv.notify_all();
 }
 
-void work(chidg_gpu_server* S, chidg_gpu_ctx* ctx) {
+void work(chidg_gpu_server* S, chidg_gpu_ctx* ctx, int slot) {
     std::unique_lock<std::mutex> lk(S->mu);
     for (;;) {
         S->cv.wait(lk, [S] { return !S->jobs.empty() || S->workers_stop; });
@@ -169,7 +214,7 @@ void work(chidg_gpu_server* S, chidg_gpu_ctx* ctx) {
         Job job = std::move(S->jobs.front());
         S->jobs.pop_front();
         lk.unlock();
-        run_batch(S, ctx, std::move(job.batch), job.bytes);
+        run_batch(S, ctx, slot, std::move(job));
         lk.lock();
     }
 }
@@ -193,9 +238,11 @@ void dispatch(chidg_gpu_server* S) {
         S->cv.wait(lk, [S, bytes] { return S->mem_used + bytes <= S->budget || S->mem_used == 0; });
         S->mem_used += bytes;
         S->peak_mem = std::max(S->peak_mem, S->mem_used);
-        ++S->batches;
+        const int64_t index = S->batches++;
         --S->idle;
-        S->jobs.push_back(Job{std::move(batch), bytes});
+        S->log.emplace_back();
+        S->log.back().t[0] = S->now();
+        S->jobs.push_back(Job{std::move(batch), bytes, index});
         S->cv.notify_all();
     }
 }
@@ -227,18 +274,18 @@ extern "C" int chidg_gpu_serve_create(int device, int32_t slots, int64_t mem_bud
         S->all_ctx.push_back(c);
     }
     S->idle = slots;
-    for (chidg_gpu_ctx* c : S->all_ctx) S->workers.emplace_back(work, S, c);
+    for (size_t i = 0; i < S->all_ctx.size(); ++i) S->workers.emplace_back(work, S, S->all_ctx[i], (int)i);
     S->dispatcher = std::thread(dispatch, S);
     *out = S;
     return CHIDG_GPU_OK;
 }
 
-extern "C" int chidg_gpu_serve_submit(chidg_gpu_server* S, const chidg_gpu_pattern* pat, const double* values,
-                                      const double* rhs, int64_t* ticket) {
-    if (!S || !pat || !values || !rhs || !ticket || pat->nelem <= 0 || pat->ntime <= 0 || pat->nblocks <= 0 ||
-        !pat->elem_nvars || !pat->elem_nterms || !pat->blk_row_elem || !pat->blk_row_time || !pat->blk_col_elem ||
-        !pat->blk_col_time || !pat->blk_kind)
-        return CHIDG_GPU_EINVAL;
+namespace {
+// a request's copy of the pattern and its sizes; nullptr for a pattern that is not valid
+std::shared_ptr<Request> new_request(const chidg_gpu_server* S, const chidg_gpu_pattern* pat) {
+    if (!pat || pat->nelem <= 0 || pat->ntime <= 0 || pat->nblocks <= 0 || !pat->elem_nvars || !pat->elem_nterms ||
+        !pat->blk_row_elem || !pat->blk_row_time || !pat->blk_col_elem || !pat->blk_col_time || !pat->blk_kind)
+        return nullptr;
     auto q = std::make_shared<Request>();
     const int32_t ne = pat->nelem;
     const int64_t nb = pat->nblocks;
@@ -252,28 +299,51 @@ extern "C" int chidg_gpu_serve_submit(chidg_gpu_server* S, const chidg_gpu_patte
     q->ct.assign(pat->blk_col_time, pat->blk_col_time + nb);
     q->kind.assign(pat->blk_kind, pat->blk_kind + nb);
     for (int32_t e = 0; e < ne; ++e) {
-        if (q->nvars[e] <= 0 || q->nterms[e] <= 0) return CHIDG_GPU_EINVAL;
+        if (q->nvars[e] <= 0 || q->nterms[e] <= 0) return nullptr;
         q->n += (int64_t)pat->ntime * q->nvars[e] * q->nterms[e];
     }
     for (int64_t k = 0; k < nb; ++k) {
-        if (q->re[k] < 0 || q->re[k] >= ne || q->ce[k] < 0 || q->ce[k] >= ne) return CHIDG_GPU_EINVAL;
+        if (q->re[k] < 0 || q->re[k] >= ne || q->ce[k] < 0 || q->ce[k] >= ne) return nullptr;
         q->nval += (int64_t)q->nvars[q->re[k]] * q->nterms[q->re[k]] * q->nvars[q->ce[k]] * q->nterms[q->ce[k]];
     }
     q->pat.nelem = pat->nelem;               // the arrays are copied above; keep only the sizes
     q->pat.ntime = pat->ntime;
     q->pat.nblocks = pat->nblocks;
-    q->values = values;
-    q->rhs = rhs;
     q->bytes = request_bytes(q->nval, q->n, S->opts.nkrylov);
+    return q;
+}
+
+int enqueue(chidg_gpu_server* S, std::shared_ptr<Request> q, int64_t* ticket) {
     std::lock_guard<std::mutex> lk(S->mu);
     if (S->stopping) return CHIDG_GPU_ESTATE;
     q->arrival = S->now();
     q->ticket = S->next_ticket++;
     *ticket = q->ticket;
     S->live[q->ticket] = q;
-    S->pending.push_back(q);
+    S->pending.push_back(std::move(q));
     S->cv.notify_all();
     return CHIDG_GPU_OK;
+}
+}  // namespace
+
+extern "C" int chidg_gpu_serve_submit(chidg_gpu_server* S, const chidg_gpu_pattern* pat, const double* values,
+                                      const double* rhs, int64_t* ticket) {
+    if (!S || !values || !rhs || !ticket) return CHIDG_GPU_EINVAL;
+    std::shared_ptr<Request> q = new_request(S, pat);
+    if (!q) return CHIDG_GPU_EINVAL;
+    q->values = values;
+    q->rhs = rhs;
+    return enqueue(S, std::move(q), ticket);
+}
+
+extern "C" int chidg_gpu_serve_submit_fill(chidg_gpu_server* S, const chidg_gpu_pattern* pat, chidg_gpu_fill_fn fill,
+                                           void* user, int64_t* ticket) {
+    if (!S || !fill || !ticket) return CHIDG_GPU_EINVAL;
+    std::shared_ptr<Request> q = new_request(S, pat);
+    if (!q) return CHIDG_GPU_EINVAL;
+    q->fill = fill;
+    q->user = user;
+    return enqueue(S, std::move(q), ticket);
 }
 
 extern "C" int chidg_gpu_serve_wait(chidg_gpu_server* S, int64_t ticket, double* x, chidg_gpu_fgmres_result* result,
@@ -296,6 +366,18 @@ extern "C" int chidg_gpu_serve_stats(chidg_gpu_server* S, int64_t* batches, int6
     std::lock_guard<std::mutex> lk(S->mu);
     if (batches) *batches = S->batches;
     if (peak_mem_bytes) *peak_mem_bytes = S->peak_mem;
+    return CHIDG_GPU_OK;
+}
+
+extern "C" int chidg_gpu_serve_batch_log(chidg_gpu_server* S, int64_t i, double* rec) {
+    if (!S || !rec) return CHIDG_GPU_EINVAL;
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (i < 0 || i >= (int64_t)S->log.size() || !S->log[(size_t)i].finished) return CHIDG_GPU_EINVAL;
+    const BatchRecord& r = S->log[(size_t)i];
+    for (int k = 0; k < 6; ++k) rec[k] = r.t[k];
+    rec[6] = r.device_ms;
+    rec[7] = r.nsys;
+    rec[8] = r.slot;
     return CHIDG_GPU_OK;
 }
 

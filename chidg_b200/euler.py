@@ -313,9 +313,9 @@ class EulerBox:
     def project(self, fn) -> np.ndarray:
         """L2 projection of fn(x) -> (..., 5) conserved variables onto the modes."""
         vals = fn(self.coords())                                           # (E, q, 5)
-        rhs = self.jinv * np.einsum("q,qm,eqf->efm", self.w, self.phi, vals)
+        rhs = self.jinv * np.tensordot(vals, self.w[:, None] * self.phi, axes=([1], [0]))   # (E, 5, m)
         Minv = np.linalg.inv(self.mass_block)
-        return np.einsum("mn,efn->efm", Minv, rhs).reshape(-1)
+        return np.tensordot(rhs, Minv, axes=([2], [1])).reshape(-1)
 
     def freestream(self) -> np.ndarray:
         u = np.array(self.vel_inf)
@@ -600,6 +600,22 @@ class EulerSystem:
         return self.box.pseudo_timestep(q.download(), cfl)
 
 
+def box_desc(box: EulerBox):
+    """The chidg_gpu_euler_box of an EulerBox."""
+    from . import _lib
+    d = _lib.EulerBoxDesc()
+    d.nx, d.ny, d.nz = box.shape
+    d.order = box.order
+    for i in range(3):
+        d.lo[i] = float(box.lo[i])
+        d.hi[i] = float(box.lo[i] + box.h[i] * box.shape[i])
+        d.vel_inf[i] = box.vel_inf[i]
+    for f in range(6):
+        d.bc[f] = _lib.EULER_FARFIELD if box.bcs[f] == "farfield" else _lib.EULER_EXTRAPOLATE
+    d.rho_inf, d.p_inf = box.rho_inf, box.p_inf
+    return d
+
+
 class EulerDevice:
     """The same discretisation assembled on the GPU (chidg_gpu_euler_*): the
     residual into a device vector and the Jacobian straight into the device
@@ -614,16 +630,7 @@ class EulerDevice:
             raise ValueError("EulerDevice: orders 0..3")
         self.box = box
         self.ctx = ctx or api.default_context()
-        d = _lib.EulerBoxDesc()
-        d.nx, d.ny, d.nz = box.shape
-        d.order = box.order
-        for i in range(3):
-            d.lo[i] = float(box.lo[i])
-            d.hi[i] = float(box.lo[i] + box.h[i] * box.shape[i])
-            d.vel_inf[i] = box.vel_inf[i]
-        for f in range(6):
-            d.bc[f] = _lib.EULER_FARFIELD if box.bcs[f] == "farfield" else _lib.EULER_EXTRAPOLATE
-        d.rho_inf, d.p_inf = box.rho_inf, box.p_inf
+        d = box_desc(box)
         self._desc = d
         h = C.c_void_p()
         self.ctx.check(self.ctx.L.chidg_gpu_euler_create(self.ctx.h, C.byref(d), C.byref(h)), "euler_create")
@@ -709,6 +716,50 @@ class EulerHBDevice:
     def release(self):
         for dev in self.levels:
             dev.release()
+
+
+class NewtonSystem:
+    """The first Newton step's system of an EulerBox or an EulerHB at the state
+    q0, described for chidg_gpu_euler_fill_system: A = dR/dq(q0) (every level
+    and the hb blocks) + mass / dtau (dtau of level 1 at `cfl`, its minimum over
+    the fields), b = -R(q0), written on the device into elements elem0.. of a
+    larger layout (a batch arena, or a served batch through
+    chidg_gpu_serve_submit_fill).  Keeps the arrays the description points at."""
+
+    def __init__(self, system, q0: np.ndarray, cfl: float):
+        import ctypes as C
+
+        from . import _lib
+        hb = system if isinstance(system, EulerHB) else None
+        box = hb.levels[0] if hb is not None else system
+        if box.order > 3:
+            raise ValueError("NewtonSystem: orders 0..3")
+        self.pattern = system.pattern
+        self.nelem = box.nelem
+        self.ntime = hb.ntime if hb is not None else 1
+        self.q0 = np.ascontiguousarray(q0, dtype=np.float64)
+        if self.q0.size != self.pattern.vector_size():
+            raise ValueError("NewtonSystem: q0 does not match the pattern")
+        self.mass = np.asfortranarray(box.mass_block, dtype=np.float64)
+        d = _lib.EulerSystemDesc()
+        d.box = box_desc(box)
+        d.ntime = self.ntime
+        d.mass = self.mass.ctypes.data_as(_lib.DP)
+        d.q0 = self.q0.ctypes.data_as(_lib.DP)
+        d.cfl = float(cfl)
+        if hb is not None:
+            self.D = np.asfortranarray(hb.D, dtype=np.float64)
+            self.level_vel = np.ascontiguousarray([lv.vel_inf for lv in hb.levels], dtype=np.float64)
+            d.D = self.D.ctypes.data_as(_lib.DP)
+            d.level_vel = self.level_vel.ctypes.data_as(_lib.DP)
+        self.desc = d
+        self.user = C.c_void_p(C.addressof(d))
+
+    def fill(self, A: api.ChidgMatrix, b: api.ChidgVector, work: api.ChidgVector, elem0: int):
+        """Write the system into elements elem0.. of A and its segment of b;
+        work's segment is overwritten."""
+        A.ctx.check(A.ctx.L.chidg_gpu_euler_fill_system(self.user, A.ctx.h, A.h, b.h, work.h, int(elem0)),
+                    "euler_fill_system")
 
 
 class EulerDeviceSystem:

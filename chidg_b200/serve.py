@@ -31,11 +31,17 @@ from . import _lib, api, mesh
 
 @dataclass
 class SolveRequest:
+    """A system to solve: its assembled values and right-hand side in host
+    memory, or (values and rhs None) `system`, an object with a `fill(A, b,
+    work, elem0)` method that writes the system on the device when its batch
+    is formed (euler.NewtonSystem: the native server then calls
+    chidg_gpu_euler_fill_system itself)."""
     pattern: mesh.BlockPattern
-    values: np.ndarray
-    rhs: np.ndarray
+    values: np.ndarray | None
+    rhs: np.ndarray | None
     tag: object = None
     arrival: float = field(default_factory=time.perf_counter)
+    system: object = None
 
 
 @dataclass
@@ -158,16 +164,27 @@ class Server:
             pats = [r.pattern for r, _ in batch]
             union, sys_elem = mesh.concat_patterns(pats)
             A = api.ChidgMatrix(union, ctx)
-            A.upload_parts([r.values for r, _ in batch])      # each request in place, no host copy
             b = api.ChidgVector(A)
-            b.upload_parts([r.rhs for r, _ in batch])
             x = api.ChidgVector(A)
+            eo = union.elem_offsets()
+            v0 = o = 0
+            for s, (r, _) in enumerate(batch):               # each request in place, no host copy
+                n_s = int(eo[sys_elem[s + 1]] - eo[sys_elem[s]])
+                nv_s = r.pattern.value_offsets()[1]
+                if r.values is None:
+                    r.system.fill(A, b, x, int(sys_elem[s]))
+                else:
+                    A.upload_range(np.ascontiguousarray(r.values, dtype=np.float64), v0)
+                    b.upload_range(np.ascontiguousarray(r.rhs, dtype=np.float64), o)
+                v0 += nv_s
+                o += n_s
+            x.clear()
+            ctx.sync()
             M = api.create_preconditioner(self.precon)
             solver = api.create_linear_solver("fgmres", **self.options)
             res = solver.solve_batched(A, x, b, M, sys_elem)
             xh = x.download()
             finish = time.perf_counter()
-            eo = union.elem_offsets()
             for s, (req, fut) in enumerate(batch):
                 xs = xh[eo[sys_elem[s]]:eo[sys_elem[s + 1]]].copy()
                 fut.set_result(SolveResult(xs, res[s]["niter"], res[s]["residual_norm"], res[s]["r0norm_initial"],
@@ -208,6 +225,8 @@ class NativeServer:
         self.h = h
 
     def submit(self, req: SolveRequest) -> "NativeFuture":
+        if req.values is None:
+            return self._submit_fill(req)
         values = np.ascontiguousarray(req.values, dtype=np.float64)
         rhs = np.ascontiguousarray(req.rhs, dtype=np.float64)
         pat = req.pattern.as_struct()
@@ -217,6 +236,33 @@ class NativeServer:
         if st:
             raise _lib.ChidgGpuError(st, "serve_submit")
         return NativeFuture(self, req, ticket.value, (values, rhs))
+
+    def _submit_fill(self, req: SolveRequest) -> "NativeFuture":
+        """chidg_gpu_serve_submit_fill with chidg_gpu_euler_fill_system and the
+        request's euler.NewtonSystem as its description."""
+        sysd = req.system
+        if not hasattr(sysd, "user"):
+            raise TypeError("the native server fills requests described by euler.NewtonSystem")
+        pat = req.pattern.as_struct()
+        ticket = C.c_int64()
+        fn = C.cast(self.L.chidg_gpu_euler_fill_system, C.c_void_p)
+        st = self.L.chidg_gpu_serve_submit_fill(self.h, C.byref(pat), fn, sysd.user, C.byref(ticket))
+        if st:
+            raise _lib.ChidgGpuError(st, "serve_submit_fill")
+        return NativeFuture(self, req, ticket.value, (sysd,))
+
+    def batch_log(self) -> list[dict]:
+        """The finished batches' records (chidg_gpu_serve_batch_log), times in
+        seconds on the perf_counter clock of the requests' arrivals."""
+        out = []
+        rec = (C.c_double * 9)()
+        for i in range(self.batches):
+            if self.L.chidg_gpu_serve_batch_log(self.h, i, rec):
+                continue
+            t = [self._t0 + rec[k] for k in range(6)]
+            out.append({"formed": t[0], "taken": t[1], "on_device": t[2], "set_up": t[3], "solved": t[4],
+                        "on_host": t[5], "device_ms": rec[6], "systems": int(rec[7]), "slot": int(rec[8])})
+        return out
 
     def _stats(self):
         if getattr(self, "h", None) is None:

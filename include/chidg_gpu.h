@@ -382,6 +382,27 @@ int chidg_gpu_serve_wait(chidg_gpu_server* s, int64_t ticket, double* x, chidg_g
                          double* timing);
 int chidg_gpu_serve_stats(chidg_gpu_server* s, int64_t* batches, int64_t* peak_mem_bytes);
 int chidg_gpu_serve_destroy(chidg_gpu_server* s);
+/* A request whose system is written on the device when its batch is formed,
+ * so that its values never exist in host memory: the worker creates the
+ * batch's matrix A and vectors b and work (all of the packed layout), then
+ * calls fill(user, ctx, A, b, work, elem0) on the worker's context, which must
+ * write the request's blocks of A (its elements are A's elements elem0 ..
+ * elem0 + nelem - 1), its segment of b (the right-hand side) and may use its
+ * segment of work as scratch; a nonzero return fails the batch with that
+ * status.  `user` must stay valid until the request's wait returns.
+ * chidg_gpu_euler_fill_system is such a function. */
+typedef int (*chidg_gpu_fill_fn)(void* user, chidg_gpu_ctx* ctx, chidg_gpu_matrix* A, chidg_gpu_vector* b,
+                                 chidg_gpu_vector* work, int32_t elem0);
+int chidg_gpu_serve_submit_fill(chidg_gpu_server* s, const chidg_gpu_pattern* pat, chidg_gpu_fill_fn fill, void* user,
+                                int64_t* ticket);
+/* Record of the server's batch i (0-based, in the order batches were formed):
+ * rec[0] formed, rec[1] taken by a worker, rec[2] its systems on the device
+ * (uploaded or filled), rec[3] preconditioner set up, rec[4] solved, rec[5]
+ * solution on the host (seconds since the server's creation); rec[6] the
+ * solve's device time in ms (CUDA events on the worker's stream); rec[7]
+ * systems; rec[8] worker slot.  CHIDG_GPU_EINVAL for a batch not formed or
+ * not yet finished. */
+int chidg_gpu_serve_batch_log(chidg_gpu_server* s, int64_t i, double* rec);
 
 /* ---- Euler DG assembly on hex boxes (the caller side of the solves) ------- */
 /* The residual and Jacobian of ChiDG's Euler discretisation
@@ -403,7 +424,7 @@ int chidg_gpu_serve_destroy(chidg_gpu_server* s);
 #define CHIDG_EULER_EXTRAPOLATE 1   /* bc_state_fluid_extrapolate: exterior state = interior state               */
 typedef struct chidg_gpu_euler_box {
     int32_t nx, ny, nz;        /* elements per direction                                          */
-    int32_t order;             /* polynomial order P, 0..2                                        */
+    int32_t order;             /* polynomial order P, 0..3                                        */
     double lo[3], hi[3];       /* box extent                                                      */
     int32_t bc[6];             /* CHIDG_EULER_* on faces XI_MIN, XI_MAX, ETA_MIN, ..., ZETA_MAX     */
     double rho_inf, p_inf;     /* farfield density and pressure                                   */
@@ -450,6 +471,48 @@ int chidg_gpu_euler_pseudo_timestep_level(chidg_gpu_euler* E, chidg_gpu_matrix* 
                                           const double* cfl, double* dtau);
 int chidg_gpu_hb_coupling(chidg_gpu_matrix* A, int32_t nterms, const double* D, const double* mass, chidg_gpu_vector* q,
                           chidg_gpu_vector* rhs, int32_t jacobian);
+/* The same for a box (or its hb levels) at elements elem0 .. of a larger
+ * layout: the level call writes level itime of the box's rows, the coupling
+ * acts on elements elem0 .. elem0 + nelem - 1 only. */
+int chidg_gpu_euler_assemble_level_at(chidg_gpu_euler* E, chidg_gpu_matrix* A, int32_t elem0, int32_t itime,
+                                      chidg_gpu_vector* q, chidg_gpu_vector* rhs, int32_t jacobian);
+int chidg_gpu_hb_coupling_at(chidg_gpu_matrix* A, int32_t elem0, int32_t nelem, int32_t nterms, const double* D,
+                             const double* mass, chidg_gpu_vector* q, chidg_gpu_vector* rhs, int32_t jacobian);
+/* The Newton step's pseudo-transient term and right-hand side on the device
+ * (newton_t%solve, type_newton.f90:181-190, contribute_pseudo_temporal :320-352):
+ * dtau of the box's elements from level 0 of q (as
+ * chidg_gpu_euler_pseudo_timestep), then on every time level of each element
+ * field f's diagonal sub-block of the DIAG block += mass / min over the fields
+ * of dtau (what chidg_gpu_matrix_scale_diagonal adds with that scale), and,
+ * with rhs non-NULL, rhs = -rhs on the box's segment (b = -R).  mass: nterms x
+ * nterms column-major, the same for every element; cfl: 5 values.  No host
+ * round trip: the result equals chidg_gpu_euler_pseudo_timestep_at +
+ * chidg_gpu_matrix_scale_diagonal + chidg_gpu_vector_scale(rhs, -1) on the box. */
+int chidg_gpu_euler_pseudo_transient_at(chidg_gpu_euler* E, chidg_gpu_matrix* A, int32_t elem0, chidg_gpu_vector* q,
+                                        chidg_gpu_vector* rhs, const double* cfl, const double* mass);
+/* A Newton system of an Euler box, described for chidg_gpu_euler_fill_system:
+ * the box (with ntime > 1, level t's farfield velocity replaces vel_inf:
+ * harmonic balance with the levels' own inflow), the state q0 (host: the
+ * box's segment, element-major, then level, field, mode), the
+ * pseudo-transient cfl of every field and the element mass matrix (nterms x
+ * nterms column-major); with ntime > 1 also the pseudo-spectral operator D
+ * (ntime x ntime column-major) and level_vel (ntime x 3). */
+typedef struct chidg_gpu_euler_system {
+    chidg_gpu_euler_box box;
+    int32_t ntime;
+    const double* level_vel;
+    const double* D;
+    const double* mass;
+    const double* q0;
+    double cfl;
+} chidg_gpu_euler_system;
+/* The first Newton step's system of `user` (a chidg_gpu_euler_system) at
+ * elements elem0 .. of A: A's blocks of the box = dR/dq(q0) (every level,
+ * with the hb blocks) + the pseudo-transient term, b's segment = -R(q0); the
+ * box's segment of work is overwritten (it holds q0).  The signature is
+ * chidg_gpu_fill_fn's.  Returns once the work is done on ctx's stream. */
+int chidg_gpu_euler_fill_system(void* user, chidg_gpu_ctx* ctx, chidg_gpu_matrix* A, chidg_gpu_vector* b,
+                                chidg_gpu_vector* work, int32_t elem0);
 
 #ifdef __cplusplus
 }

@@ -50,6 +50,14 @@ module chidg_gpu_mod
         real(c_double)     :: vel_inf(3)
     end type chidg_gpu_euler_box
 
+    ! chidg_gpu_euler_system: a Newton system of chidg_gpu_euler_fill_system
+    type, bind(c) :: chidg_gpu_euler_system
+        type(chidg_gpu_euler_box) :: box
+        integer(c_int32_t)        :: ntime
+        type(c_ptr)               :: level_vel, D, mass, q0
+        real(c_double)            :: cfl
+    end type chidg_gpu_euler_system
+
     type, bind(c) :: chidg_gpu_fgmres_result
         integer(c_int32_t) :: niter, nrestart, inner_iters, nhist
         real(c_double)     :: residual_norm, res_estimate, r0norm_initial, seconds
@@ -430,6 +438,40 @@ module chidg_gpu_mod
             type(c_ptr),        value :: q, rhs
             integer(c_int32_t), value :: jacobian
         end function
+        integer(c_int) function chidg_gpu_euler_assemble_level_at(E, mat, elem0, itime, q, rhs, jacobian) &
+                bind(c, name='chidg_gpu_euler_assemble_level_at')
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr),        value :: E, mat
+            integer(c_int32_t), value :: elem0, itime
+            type(c_ptr),        value :: q, rhs
+            integer(c_int32_t), value :: jacobian
+        end function
+        integer(c_int) function chidg_gpu_hb_coupling_at(mat, elem0, nelem, nterms, D, mass, q, rhs, jacobian) &
+                bind(c, name='chidg_gpu_hb_coupling_at')
+            import :: c_int, c_ptr, c_int32_t, c_double
+            type(c_ptr),        value :: mat
+            integer(c_int32_t), value :: elem0, nelem, nterms
+            real(c_double)            :: D(*), mass(*)
+            type(c_ptr),        value :: q, rhs
+            integer(c_int32_t), value :: jacobian
+        end function
+        ! pass c_null_ptr as rhs to leave the right-hand side as it is
+        integer(c_int) function chidg_gpu_euler_pseudo_transient_at(E, mat, elem0, q, rhs, cfl, mass) &
+                bind(c, name='chidg_gpu_euler_pseudo_transient_at')
+            import :: c_int, c_ptr, c_int32_t, c_double
+            type(c_ptr),        value :: E, mat
+            integer(c_int32_t), value :: elem0
+            type(c_ptr),        value :: q, rhs
+            real(c_double)            :: cfl(5), mass(*)
+        end function
+        ! user: c_loc of a chidg_gpu_euler_system; also usable as a chidg_gpu_fill_fn
+        ! (c_funloc(chidg_gpu_euler_fill_system)) for chidg_gpu_serve_submit_fill
+        integer(c_int) function chidg_gpu_euler_fill_system(user, ctx, mat, b, work, elem0) &
+                bind(c, name='chidg_gpu_euler_fill_system')
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr),        value :: user, ctx, mat, b, work
+            integer(c_int32_t), value :: elem0
+        end function
         ! ---- launch shapes of the streamed kernels and their autotuner --------
         integer(c_int) function chidg_gpu_autotune(M, mat, precision, reps) bind(c, name='chidg_gpu_autotune')
             import :: c_int, c_ptr, c_int32_t
@@ -481,6 +523,23 @@ module chidg_gpu_mod
         integer(c_int) function chidg_gpu_serve_destroy(srv) bind(c, name='chidg_gpu_serve_destroy')
             import :: c_int, c_ptr
             type(c_ptr), value :: srv
+        end function
+        ! fill: c_funloc of a function with chidg_gpu_fill_fn's interface; user stays
+        ! valid until the request's wait returns
+        integer(c_int) function chidg_gpu_serve_submit_fill(srv, pat, fill, user, ticket) &
+                bind(c, name='chidg_gpu_serve_submit_fill')
+            import :: c_int, c_ptr, c_funptr, c_int64_t, chidg_gpu_pattern
+            type(c_ptr),    value   :: srv
+            type(chidg_gpu_pattern) :: pat
+            type(c_funptr), value   :: fill
+            type(c_ptr),    value   :: user
+            integer(c_int64_t)      :: ticket
+        end function
+        integer(c_int) function chidg_gpu_serve_batch_log(srv, i, rec) bind(c, name='chidg_gpu_serve_batch_log')
+            import :: c_int, c_ptr, c_int64_t, c_double
+            type(c_ptr),        value :: srv
+            integer(c_int64_t), value :: i
+            real(c_double)            :: rec(9)
         end function
     end interface
 

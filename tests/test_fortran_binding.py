@@ -11,6 +11,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 C_KIND = {"int": "c_int", "int32_t": "c_int32_t", "int64_t": "c_int64_t", "double": "c_double",
           "size_t": "c_size_t"}
+FUNPTR_TYPES = {"chidg_gpu_fill_fn"}     # C function pointer typedefs: type(c_funptr), value
 
 
 def header_prototypes():
@@ -64,4 +65,7 @@ def test_fortran_arguments_match_the_prototypes():
             else:
                 ctype = carg.replace("const ", "").split()[0]
                 assert by_value, (name, carg, decl)
-                assert f"({C_KIND[ctype]})" in decl, (name, carg, decl)
+                if ctype in FUNPTR_TYPES:
+                    assert decl.startswith("type(c_funptr)"), (name, carg, decl)
+                else:
+                    assert f"({C_KIND[ctype]})" in decl, (name, carg, decl)

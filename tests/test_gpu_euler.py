@@ -275,3 +275,84 @@ def test_harmonic_balance_device_assembly_matches_host(order, freqs):
     dt = dev.pseudo_timestep(q, A, 10.0)
     assert relerr(dt, hb.pseudo_timestep(q0, 10.0)) < 1e-13
     dev.release()
+
+
+def host_driven_system(A, rhs, q, systems, sys_elem, cfl):
+    """The Newton systems written the way the host drives it: assembly into
+    each slice, dtau to the host, chidg_gpu_matrix_scale_diagonal over A with
+    1 / min_f dtau, rhs = -rhs."""
+    from chidg_b200 import _lib
+    scale, mass = [], []
+    for sysm, e0 in zip(systems, sys_elem[:-1]):
+        if isinstance(sysm, euler.EulerHB):
+            dev = euler.EulerHBDevice(sysm, A.ctx)
+            L = A.ctx.L
+            for t, lv in enumerate(dev.levels):
+                A.ctx.check(L.chidg_gpu_euler_assemble_level_at(lv.h, A.h, int(e0), t, q.h, rhs.h, 1), "level_at")
+            A.ctx.check(L.chidg_gpu_hb_coupling_at(A.h, int(e0), sysm.nelem, sysm.nterms, dev._D.ctypes.data_as(_lib.DP),
+                                                   dev._M.ctypes.data_as(_lib.DP), q.h, rhs.h, 1), "hb_coupling_at")
+            # level 1's dtau of this system, from a matrix of its own layout
+            Ab = api.ChidgMatrix(sysm.pattern, A.ctx)
+            eo = A.pattern.elem_offsets()
+            qb = api.ChidgVector(Ab, q.download()[eo[e0]:eo[e0] + Ab.n])
+            dt = dev.pseudo_timestep(qb, Ab, cfl)
+            for o in (qb, Ab):
+                o.release()
+            dev.release()
+        else:
+            dev = euler.EulerDevice(sysm, A.ctx)
+            dev.assemble_at(A, int(e0), q, rhs, True)
+            dt = dev.pseudo_timestep_at(A, int(e0), q, cfl)
+            dev.release()
+        mass.append(sysm.mass)
+        scale.append(np.repeat(1.0 / dt.min(axis=1), 5))
+    A.scale_diagonal(np.concatenate(mass), np.concatenate(scale))
+    rhs.scale(-1.0)
+
+
+@pytest.mark.parametrize("kind", ["boxes", "hb"])
+def test_fill_system_matches_host_driven_assembly(kind):
+    """chidg_gpu_euler_fill_system (assembly, hb coupling, the pseudo-transient
+    term and b = -R on the device, no host round trip) writes bitwise the
+    system that the host-driven sequence writes, into each slice of a packed
+    layout of several systems."""
+    if kind == "boxes":
+        systems = [euler.EulerBox(3, 2, 2, 1, vel_inf=(0.4, 0.0, 0.0)), euler.EulerBox(2, 2, 2, 3),
+                   euler.EulerBox(2, 3, 2, 2, vel_inf=(0.25, 0.05, 0.0))]
+    else:
+        systems = [euler.EulerHB(2, 2, 2, 1, [1.0], amplitude=2e-2, vel_inf=(0.35, 0.05, 0.0)),
+                   euler.EulerHB(3, 2, 1, 1, [1.5], amplitude=1e-2, vel_inf=(0.3, 0.0, 0.0))]
+    qs = [s.density_bump(amplitude=0.03, width=0.3, centre=(0.4, 0.5, 0.6)) for s in systems]
+    union, sys_elem = mesh.concat_patterns([s.pattern for s in systems])
+    A1 = api.ChidgMatrix(union)
+    q1, r1 = api.ChidgVector(A1, np.concatenate(qs)), api.ChidgVector(A1)
+    host_driven_system(A1, r1, q1, systems, sys_elem, 10.0)
+    A2 = api.ChidgMatrix(union, A1.ctx)
+    b2, w2 = api.ChidgVector(A2), api.ChidgVector(A2)
+    descs = [euler.NewtonSystem(s, qq, 10.0) for s, qq in zip(systems, qs)]
+    for d, e0 in zip(descs, sys_elem[:-1]):
+        d.fill(A2, b2, w2, int(e0))
+    assert np.array_equal(A2.download(), A1.download())
+    assert np.array_equal(b2.download(), r1.download())
+    assert np.array_equal(w2.download(), np.concatenate(qs))   # work holds each q0
+    for o in (q1, r1, A1, b2, w2, A2):
+        o.release()
+
+
+def test_fill_system_refuses_mismatched_layouts():
+    box = euler.EulerBox(2, 2, 2, 1)
+    d = euler.NewtonSystem(box, box.freestream(), 10.0)
+    other = euler.EulerBox(2, 2, 2, 2)
+    A = api.ChidgMatrix(other.pattern)
+    b, w = api.ChidgVector(A), api.ChidgVector(A)
+    with pytest.raises(api.ChidgGpuError):
+        d.fill(A, b, w, 0)                       # modes differ
+    Ab = api.ChidgMatrix(box.pattern, A.ctx)
+    bb, wb = api.ChidgVector(Ab), api.ChidgVector(Ab)
+    with pytest.raises(api.ChidgGpuError):
+        d.fill(Ab, bb, wb, 1)                    # does not fit from element 1
+    with pytest.raises(api.ChidgGpuError):
+        d.fill(Ab, bb, bb, 0)                    # b and work must differ
+    hb = euler.EulerHB(2, 2, 2, 1, [1.0])
+    with pytest.raises(api.ChidgGpuError):
+        euler.NewtonSystem(hb, hb.freestream(), 10.0).fill(Ab, bb, wb, 0)   # time levels differ

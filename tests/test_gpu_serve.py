@@ -4,7 +4,7 @@ alone and in a mix (the batched solver never mixes systems' arithmetic)."""
 import numpy as np
 import pytest
 
-from chidg_b200 import mesh, serve
+from chidg_b200 import api, euler, mesh, serve
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -62,3 +62,44 @@ def test_server_admission_respects_memory_budget(server):
     assert srv.peak_mem_used <= one
     assert srv.batches >= 2
     assert all(r.residual_norm <= 2e-8 * r.r0norm_initial for r in res)
+
+
+def fill_requests():
+    out = []
+    for i, (shape, P) in enumerate([((3, 2, 2), 1), ((2, 2, 2), 2), ((2, 3, 2), 1), ((2, 2, 2), 3)]):
+        box = euler.EulerBox(*shape, P, vel_inf=(0.3 + 0.05 * i, 0.0, 0.0))
+        q0 = box.density_bump(amplitude=0.02, width=0.3, centre=(0.5, 0.4, 0.5))
+        out.append(serve.SolveRequest(box.pattern, None, None, tag=i, system=euler.NewtonSystem(box, q0, 10.0)))
+    return out
+
+
+@pytest.mark.parametrize("server", SERVERS)
+def test_filled_requests_match_uploaded_ones(server):
+    """Requests whose systems are written on the device when their batch is
+    formed (chidg_gpu_serve_submit_fill with chidg_gpu_euler_fill_system) give
+    bitwise the answers of the same systems handed over as host arrays, and
+    every batch of the native server leaves a record of its phases."""
+    reqs = fill_requests()
+    uploaded = []
+    for r in reqs:
+        A = api.ChidgMatrix(r.pattern)
+        b, w = api.ChidgVector(A), api.ChidgVector(A)
+        r.system.fill(A, b, w, 0)
+        uploaded.append(serve.SolveRequest(r.pattern, A.download(), b.download(), tag=r.tag))
+        for o in (w, b, A):
+            o.release()
+    srv = server(slots=2, max_batch=3, **OPTS)
+    try:
+        filled = [f.result() for f in [srv.submit(r) for r in reqs]]
+        up = [f.result() for f in [srv.submit(r) for r in uploaded]]
+        log = srv.batch_log() if isinstance(srv, serve.NativeServer) else None
+    finally:
+        srv.close()
+    for a, c in zip(filled, up):
+        assert a.niter == c.niter and np.array_equal(a.x, c.x)
+        assert a.residual_norm <= 2e-8 * a.r0norm_initial
+    if log is not None:
+        assert sum(r["systems"] for r in log) == 2 * len(reqs)
+        for r in log:
+            assert r["formed"] <= r["taken"] <= r["on_device"] <= r["set_up"] <= r["solved"] <= r["on_host"]
+            assert r["device_ms"] > 0 and r["slot"] in (0, 1)
