@@ -299,8 +299,8 @@ CFG5_RATE = 200.0           # requests per second, Poisson
 CFG5_SEED = 53
 CFG5_BUDGET = 100 << 30     # device bytes the server admits at once (request_bytes estimates)
 CFG5_SLOTS = 2
-CFG5_MAX_BATCH = 16
-CFG5_UNDER = (96, 12.0)     # a second stream below the GPU's capacity: requests, rate
+CFG5_MAX_BATCH = 32
+CFG5_UNDER = (96, 8.0)      # a second stream below the GPU's capacity: requests, rate
 
 
 def cfg5_requests(count=CFG5_REQUESTS, seed=CFG5_SEED):
@@ -342,6 +342,33 @@ def batch_phases(log, t0):
     return out
 
 
+def tune_for_serving(device):
+    """The streamed kernels' shapes for the block-size classes of the served
+    batches (largest block 40: P1 boxes and the harmonic-balance batches; 135;
+    320: batches with P3 systems), in both precisions, measured by the project
+    autotuner on arenas of each class.  The shape table is the process's, so
+    the server's workers use them."""
+    from chidg_b200 import api, tuning
+    ctx = api.default_context(device)
+    c = (0.5, 0.5, 0.5)
+    arenas = ([((10, 10, 10), 1, 0.4, 5e-3, c)],
+              [((8, 8, 8), 2, 0.4, 5e-3, c), ((10, 10, 10), 1, 0.3, 5e-3, c)],
+              [((6, 6, 6), 3, 0.4, 5e-3, c), ((8, 8, 8), 2, 0.3, 5e-3, c), ((10, 10, 10), 1, 0.5, 5e-3, c)])
+    shapes = {}
+    t0 = time.perf_counter()
+    for draws in arenas:
+        A, b, _, _ = cfg4_arena(ctx, draws)
+        for prec in ("mixed_precon_fp32", "fp64"):
+            M = api.create_preconditioner("ilu0")
+            M.update(A, precision=prec)
+            shapes.update(tuning.autotune(A, M, prec, reps=1))
+            M.tear_down()
+        b.release()
+        A.release()
+    ctx.sync()
+    return shapes, time.perf_counter() - t0
+
+
 def run_serve_leg(device, runs=1):
     """The serving configuration as stated: CFG5_REQUESTS requests arriving as
     a Poisson process at CFG5_RATE per second through the native server (two
@@ -359,6 +386,7 @@ def run_serve_leg(device, runs=1):
         if k not in kinds or r.pattern.nelem < kinds[k].pattern.nelem:
             kinds[k] = r
     warm = list(kinds.values())
+    shapes, tune_s = tune_for_serving(device)
     out = {"workload": "Poisson arrivals of Euler Newton systems drawn as the many-solve workload (box sides 4..16, "
                        "P 1..3, Mach U[0.2, 0.6]), every 10th an Euler harmonic-balance system (8^3 P1, 7 levels); "
                        "each written on the device when admitted; FGMRES(30) + ILU0 to rtol 1e-8 (FP64 residual); "
@@ -367,7 +395,8 @@ def run_serve_leg(device, runs=1):
            "mem_budget_bytes": CFG5_BUDGET, "server": "native (chidg_gpu_serve_*, chidg_gpu_serve_submit_fill)",
            "harmonic_balance_requests": sum(1 for r in reqs if r.pattern.ntime > 1),
            "matrix_bytes_fp64": int(sum(8 * r.pattern.value_offsets()[1] for r in reqs)),
-           "below_capacity": {"requests": CFG5_UNDER[0], "arrival_rate_per_s": CFG5_UNDER[1]}}
+           "below_capacity": {"requests": CFG5_UNDER[0], "arrival_rate_per_s": CFG5_UNDER[1]},
+           "stream_shapes": shapes, "autotune_s": tune_s}
 
     def stream(prec, rq, rate, seed):
         srv = serve.NativeServer(device=device, slots=CFG5_SLOTS, max_batch=CFG5_MAX_BATCH, mem_budget=CFG5_BUDGET,

@@ -128,6 +128,7 @@ PROTOTYPES = {
     "chidg_gpu_hb_coupling_at": (C.c_int, [VP, C.c_int32, C.c_int32, C.c_int32, DP, DP, VP, VP, C.c_int32]),
     "chidg_gpu_euler_pseudo_transient_at": (C.c_int, [VP, VP, C.c_int32, VP, VP, DP, DP]),
     "chidg_gpu_euler_fill_system": (C.c_int, [VP, VP, VP, VP, VP, C.c_int32]),
+    "chidg_gpu_vector_mass_scale": (C.c_int, [VP, VP, DP, DP]),
     "chidg_gpu_stream_shape_get": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, I32P, I32P, I32P]),
     "chidg_gpu_stream_shape_set": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
     "chidg_gpu_euler_create": (C.c_int, [VP, VP, C.POINTER(VP)]),
@@ -146,6 +147,7 @@ PROTOTYPES = {
     "chidg_gpu_precon_update": (C.c_int, [VP, VP, C.c_int32]),
     "chidg_gpu_precon_apply": (C.c_int, [VP, VP, VP, VP]),
     "chidg_gpu_precon_download_LD": (C.c_int, [VP, VP]),
+    "chidg_gpu_precon_download_LD32": (C.c_int, [VP, VP]),
     "chidg_gpu_precon_stamp": (C.c_int, [VP, I64P]),
     "chidg_gpu_precon_set_schedule": (C.c_int, [VP, C.c_int32]),
     "chidg_gpu_fgmres_solve": (C.c_int, [VP, VP, VP, VP, C.POINTER(FgmresOpts), C.POINTER(FgmresResult), DP,

@@ -276,6 +276,15 @@ class ChidgVector:
     def clear(self):
         self.ctx.check(self.ctx.L.chidg_gpu_vector_clear(self.h), "vector_clear")
 
+    def assign_mass_scaled(self, x: "ChidgVector", mass: np.ndarray, scale: np.ndarray):
+        """self = scale[e, f] mass_e x on every element, time level and field
+        segment (pseudo_transient_scaling); mass and scale packed as
+        ChidgMatrix.scale_diagonal takes them."""
+        mass = np.ascontiguousarray(mass, dtype=np.float64)
+        scale = np.ascontiguousarray(scale, dtype=np.float64)
+        self.ctx.check(self.ctx.L.chidg_gpu_vector_mass_scale(x.h, self.h, mass.ctypes.data_as(_lib.DP),
+                                                              scale.ctypes.data_as(_lib.DP)), "vector_mass_scale")
+
     def copy_from(self, other: "ChidgVector"):
         self.ctx.check(self.ctx.L.chidg_gpu_vector_copy(self.h, other.h), "vector_copy")
 
@@ -405,6 +414,12 @@ class Preconditioner:
     def LD(self) -> np.ndarray:
         out = np.empty(self.A.nvalues)
         self.A.ctx.check(self.A.ctx.L.chidg_gpu_precon_download_LD(self.h, _ptr(out)), "LD")
+        return out
+
+    def LD32(self) -> np.ndarray:
+        """The FP32 factors of the last mixed-precision update."""
+        out = np.empty(self.A.nvalues, dtype=np.float32)
+        self.A.ctx.check(self.A.ctx.L.chidg_gpu_precon_download_LD32(self.h, _ptr(out)), "LD32")
         return out
 
     @property

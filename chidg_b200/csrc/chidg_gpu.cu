@@ -518,6 +518,7 @@ extern "C" int chidg_gpu_matrix_clear(chidg_gpu_matrix* A) {
     A->stamp++;
     return CHIDG_GPU_OK;
 }
+static int mass_scale_offsets(chidg_gpu_matrix* A);
 extern "C" int chidg_gpu_matrix_scale_diagonal(chidg_gpu_matrix* A, const double* mass, const double* scale) {
     if (!A || !mass || !scale) return CHIDG_GPU_EINVAL;
     chidg_gpu_ctx* ctx = A->ctx;
@@ -527,19 +528,8 @@ extern "C" int chidg_gpu_matrix_scale_diagonal(chidg_gpu_matrix* A, const double
         m += (int64_t)A->nterms[e] * A->nterms[e];
         s += A->nvars[e];
     }
-    int st;
-    if (!A->d_mass_off.ptr) {                // per-element offsets of mass and scale: fixed by the pattern
-        std::vector<int64_t> moff(A->nelem), soff(A->nelem);
-        int64_t mm = 0, ss = 0;
-        for (int e = 0; e < A->nelem; ++e) {
-            moff[e] = mm; mm += (int64_t)A->nterms[e] * A->nterms[e];
-            soff[e] = ss; ss += A->nvars[e];
-        }
-        if ((st = upload_array(ctx, A->d_mass_off, moff)) || (st = upload_array(ctx, A->d_scale_off, soff))) {
-            release(A->d_mass_off); release(A->d_scale_off);
-            return st;
-        }
-    }
+    int st = mass_scale_offsets(A);
+    if (st) return st;
     const Buffer& dmo = A->d_mass_off;
     const Buffer& dso = A->d_scale_off;
     Buffer dm, ds;
@@ -559,6 +549,54 @@ extern "C" int chidg_gpu_matrix_scale_diagonal(chidg_gpu_matrix* A, const double
     if (st) return st;
     A->stamp++;
     return CHIDG_GPU_OK;
+}
+
+// the per-element offsets of packed mass matrices and scales (fixed by the pattern)
+static int mass_scale_offsets(chidg_gpu_matrix* A) {
+    if (A->d_mass_off.ptr) return CHIDG_GPU_OK;
+    std::vector<int64_t> moff(A->nelem), soff(A->nelem);
+    int64_t mm = 0, ss = 0;
+    for (int e = 0; e < A->nelem; ++e) {
+        moff[e] = mm; mm += (int64_t)A->nterms[e] * A->nterms[e];
+        soff[e] = ss; ss += A->nvars[e];
+    }
+    int st;
+    if ((st = upload_array(A->ctx, A->d_mass_off, moff)) || (st = upload_array(A->ctx, A->d_scale_off, soff))) {
+        release(A->d_mass_off); release(A->d_scale_off);
+        return st;
+    }
+    return CHIDG_GPU_OK;
+}
+
+extern "C" int chidg_gpu_vector_mass_scale(const chidg_gpu_vector* x, chidg_gpu_vector* y, const double* mass,
+                                           const double* scale) {
+    if (!x || !y || !mass || !scale || x == y || x->A != y->A) return CHIDG_GPU_EINVAL;
+    chidg_gpu_matrix* A = x->A;
+    chidg_gpu_ctx* ctx = A->ctx;
+    cudaSetDevice(ctx->device);
+    int64_t m = 0, s = 0;
+    for (int e = 0; e < A->nelem; ++e) {
+        m += (int64_t)A->nterms[e] * A->nterms[e];
+        s += A->nvars[e];
+    }
+    int st = mass_scale_offsets(A);
+    if (st) return st;
+    Buffer dm, ds;
+    if ((st = ensure(ctx, dm, sizeof(double) * m)) || (st = ensure(ctx, ds, sizeof(double) * s))) {
+        release(dm); release(ds);
+        return st;
+    }
+    cudaMemcpyAsync(dm.ptr, mass, sizeof(double) * m, cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(ds.ptr, scale, sizeof(double) * s, cudaMemcpyHostToDevice, ctx->stream);
+    k_mass_scale<<<A->nrow, 128, 0, ctx->stream>>>((const double*)x->buf.ptr, (double*)y->buf.ptr,
+                                                  (const int64_t*)A->d_row_yoff.ptr, (const int32_t*)A->d_elem_nvars.ptr,
+                                                  (const int32_t*)A->d_elem_nterms.ptr, (const int64_t*)A->d_mass_off.ptr,
+                                                  (const double*)dm.ptr, (const double*)ds.ptr,
+                                                  (const int64_t*)A->d_scale_off.ptr, A->ntime);
+    st = check_launch(ctx, "k_mass_scale");
+    cudaStreamSynchronize(ctx->stream);
+    release(dm); release(ds);
+    return st;
 }
 
 // ---------------------------------------------------------------------------
@@ -1555,11 +1593,15 @@ static int launch_inverse(chidg_gpu_precon* M, int row_begin, int count, int cls
 // inverses in FP64 (the products' D blocks are written in FP64, inverted by the
 // tensor-core kernel and copied to FP32 per wavefront).  Only the FP32 (and
 // BF16) factors are produced; LD's FP64 L blocks are not.
-// CHIDG_FACTOR32_SIMT=1 selects the FP32 SIMT products (comparison runs)
-static bool factor32_simt_env() {
-    static const bool v = [] {
-        const char* e = std::getenv("CHIDG_FACTOR32_SIMT");
-        return e && e[0] == '1';
+// The products run on the tcgen05 tensor cores (k_task_gemm_umma);
+// CHIDG_FACTOR32_MMA=sync selects the mma.sync TF32 kernel and
+// CHIDG_FACTOR32_SIMT=1 the FP32 SIMT products (comparison runs)
+static int factor32_kernel_env() {       // 0 tcgen05, 1 mma.sync, 2 SIMT
+    static const int v = [] {
+        const char* s = std::getenv("CHIDG_FACTOR32_SIMT");
+        if (s && s[0] == '1') return 2;
+        const char* m = std::getenv("CHIDG_FACTOR32_MMA");
+        return (m && std::strcmp(m, "sync") == 0) ? 1 : 0;
     }();
     return v;
 }
@@ -1573,12 +1615,16 @@ static int factor_fp32(chidg_gpu_precon* M, chidg_gpu_matrix* A, int precision) 
     if ((st = ensure(ctx, M->LD, sizeof(double) * (size_t)P.ld_size)) ||
         (st = ensure(ctx, M->LD32, sizeof(float) * (size_t)P.ld_size)))
         return st;
-    const bool simt = factor32_simt_env();
+    const int kern = factor32_kernel_env();
     if ((st = raise_smem_limit((const void*)k_task_gemm_f32<float>, SF_SMEM)) ||
         (st = raise_smem_limit((const void*)k_task_gemm_f32<double>, SF_SMEM)) ||
         (st = raise_smem_limit((const void*)k_task_gemm_tf32<float>, ST_SMEM)) ||
-        (st = raise_smem_limit((const void*)k_task_gemm_tf32<double>, ST_SMEM)))
+        (st = raise_smem_limit((const void*)k_task_gemm_tf32<double>, ST_SMEM)) ||
+        (st = raise_smem_limit((const void*)k_task_gemm_umma<float>, UM_SMEM)) ||
+        (st = raise_smem_limit((const void*)k_task_gemm_umma<double>, UM_SMEM)))
         return fail(ctx, st, "FP32 factor GEMM shared memory");
+    int* wstat = (int*)(ctx->d_scal + kSlotStatus);
+    cudaMemsetAsync(ctx->d_scal + kSlotStatus, 0, sizeof(double), ctx->stream);
     const int nlev = (int)P.fwd_ptr.size() - 1;
     const float* A32 = (const float*)A->val32.ptr;
     float* L32 = (float*)M->LD32.ptr;
@@ -1590,22 +1636,29 @@ static int factor_fp32(chidg_gpu_precon* M, chidg_gpu_matrix* A, int precision) 
         const GemmTask* lt = (const GemmTask*)P.d_ltasks.ptr + P.ltask_ptr[l];
         const GemmTask* stt = (const GemmTask*)P.d_stasks.ptr + P.stask_ptr[l];
         if (nl > 0) {
-            if (simt)
+            if (kern == 2)
                 k_task_gemm_f32<float><<<nl, 256, SF_SMEM, ctx->stream>>>(lt, (const GemmPair*)P.d_lpairs.ptr, A32, L32,
                                                                          nullptr, L32, 1.0);
-            else
+            else if (kern == 1)
                 k_task_gemm_tf32<float><<<nl, ST_THREADS, ST_SMEM, ctx->stream>>>(lt, (const GemmPair*)P.d_lpairs.ptr, A32,
                                                                                  L32, nullptr, L32, 1.0);
+            else
+                k_task_gemm_umma<float><<<nl, UM_THREADS, UM_SMEM, ctx->stream>>>(lt, (const GemmPair*)P.d_lpairs.ptr, A32,
+                                                                                 L32, nullptr, L32, 1.0, wstat, kSpinLimit);
             if ((st = check_launch(ctx, "factor L products (FP32 / TF32)"))) return st;
         }
         const int ns = P.stask_ptr[l + 1] - P.stask_ptr[l];
         if (ns > 0) {
-            if (simt)
+            if (kern == 2)
                 k_task_gemm_f32<double><<<ns, 256, SF_SMEM, ctx->stream>>>(stt, (const GemmPair*)P.d_spairs.ptr, L32, A32,
                                                                           (const double*)A->val.ptr, LD, -1.0);
-            else
+            else if (kern == 1)
                 k_task_gemm_tf32<double><<<ns, ST_THREADS, ST_SMEM, ctx->stream>>>(stt, (const GemmPair*)P.d_spairs.ptr, L32,
                                                                                   A32, (const double*)A->val.ptr, LD, -1.0);
+            else
+                k_task_gemm_umma<double><<<ns, UM_THREADS, UM_SMEM, ctx->stream>>>(stt, (const GemmPair*)P.d_spairs.ptr, L32,
+                                                                                  A32, (const double*)A->val.ptr, LD, -1.0,
+                                                                                  wstat, kSpinLimit);
             if ((st = check_launch(ctx, "factor S products (FP32 / TF32)"))) return st;
         }
         prof_end(ctx, pg);
@@ -1664,6 +1717,11 @@ extern "C" int chidg_gpu_precon_update(chidg_gpu_precon* M, chidg_gpu_matrix* A,
         cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
         const cudaError_t e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "precon update");
+        double w = 0.0;
+        if ((st = fetch_scalars(ctx, kSlotStatus, 1, &w))) return st;
+        int wi = 0;
+        std::memcpy(&wi, &w, sizeof(int));
+        if (wi != 0) return fail(ctx, CHIDG_GPU_ETIMEOUT, "factor: a bounded wait for the tensor cores ran out");
         if (ctx->h_status[0] != INT_MAX) {
             ctx->err_elem = ctx->h_status[0];
             return fail(ctx, CHIDG_GPU_ESINGULAR, "inv: Matrix is numerically singular! (element " + std::to_string(ctx->h_status[0]) + ")");
@@ -2262,30 +2320,46 @@ extern "C" int chidg_gpu_precon_apply(chidg_gpu_precon* M, chidg_gpu_matrix* A, 
     return status_word(ctx, w);
 }
 
-extern "C" int chidg_gpu_precon_download_LD(chidg_gpu_precon* M, double* host) {
+// The factors in the matrix's block positions, from LD (FP64) or LD32 (FP32)
+template <typename T>
+static int download_factors(chidg_gpu_precon* M, T* host, const Buffer& src, bool valid, const char* what) {
     if (!M || !host) return CHIDG_GPU_EINVAL;
     chidg_gpu_ctx* ctx = M->ctx;
     cudaSetDevice(ctx->device);
     chidg_gpu_matrix* A = M->A;
-    if (M->kind == CHIDG_PRECON_IDENTITY || M->stamp == 0) return fail(ctx, CHIDG_GPU_ESTATE, "download_LD: no factors");
-    if (!M->ld64_valid) return fail(ctx, CHIDG_GPU_ESTATE, "download_LD: the factors were computed in FP32 (mixed precision)");
+    if (M->kind == CHIDG_PRECON_IDENTITY || M->stamp == 0) return fail(ctx, CHIDG_GPU_ESTATE, std::string(what) + ": no factors");
+    if (!valid || !src.ptr) return fail(ctx, CHIDG_GPU_ESTATE, std::string(what) + ": no factors of this precision since the last update");
     if (M->kind == CHIDG_PRECON_HB)
-        return fail(ctx, CHIDG_GPU_EINVAL, "download_LD: the HB preconditioner's element blocks span time levels");
+        return fail(ctx, CHIDG_GPU_EINVAL, std::string(what) + ": the HB preconditioner's element blocks span time levels");
     if (M->kind != CHIDG_PRECON_RASILU0 && M->built_transposed) A = A->T;   // factors of A^T, in A^T's block order
-    std::vector<double> ld((size_t)M->P.ld_size);
-    cudaError_t e = cudaMemcpyAsync(ld.data(), M->LD.ptr, sizeof(double) * ld.size(), cudaMemcpyDeviceToHost, ctx->stream);
+    std::vector<T> ld((size_t)M->P.ld_size);
+    cudaError_t e = cudaMemcpyAsync(ld.data(), src.ptr, sizeof(T) * ld.size(), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "LD download");
-    std::memset(host, 0, sizeof(double) * (size_t)A->nval);
+    std::memset(host, 0, sizeof(T) * (size_t)A->nval);
     const IluProgram& P = M->P;
     for (int pr = 0; pr < P.nprow; ++pr) {
         if (P.diag_blk[pr] < 0) continue;   // overlap rows live only inside the preconditioner
         const int b = P.prow_b[pr];
-        std::memcpy(host + A->voff[P.diag_blk[pr]], ld.data() + P.dinv_off[pr], sizeof(double) * b * b);
+        std::memcpy(host + A->voff[P.diag_blk[pr]], ld.data() + P.dinv_off[pr], sizeof(T) * b * b);
         for (const auto& en : P.lo[pr])
-            if (en.blk >= 0) std::memcpy(host + A->voff[en.blk], ld.data() + en.l_off, sizeof(double) * (size_t)b * en.nc);
+            if (en.blk >= 0) std::memcpy(host + A->voff[en.blk], ld.data() + en.l_off, sizeof(T) * (size_t)b * en.nc);
     }
     return CHIDG_GPU_OK;
+}
+
+extern "C" int chidg_gpu_precon_download_LD(chidg_gpu_precon* M, double* host) {
+    if (M && M->stamp != 0 && !M->ld64_valid)
+        return fail(M->ctx, CHIDG_GPU_ESTATE, "download_LD: the factors were computed in FP32 (mixed precision)");
+    return M ? download_factors<double>(M, host, M->LD, M->ld64_valid, "download_LD") : CHIDG_GPU_EINVAL;
+}
+
+extern "C" int chidg_gpu_precon_download_LD32(chidg_gpu_precon* M, float* host) {
+    if (!M) return CHIDG_GPU_EINVAL;
+    // BF16 factors come through FP32 ones only on the FP32 factorisation's path
+    const bool fp32 = M->precision == CHIDG_GPU_MIXED_FP32 || M->precision == CHIDG_GPU_MIXED_PRECON_FP32 ||
+                      (M->precision == CHIDG_GPU_MIXED_BF16 && M->P.max_b <= SF_MAX && !M->P.assembled);
+    return download_factors<float>(M, host, M->LD32, fp32, "download_LD32");
 }
 
 // ---------------------------------------------------------------------------

@@ -5,6 +5,7 @@
 #include "stream_sweep.cuh"
 #include "inverse_tc.cuh"
 #include "stream_matvec.cuh"
+#include "umma_gemm.cuh"
 
 #include <array>
 #include <cmath>

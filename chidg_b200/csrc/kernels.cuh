@@ -307,6 +307,31 @@ static __global__ void k_scale_diagonal(double* __restrict__ val, const int64_t*
 }
 
 // ---------------------------------------------------------------------------
+// y(e, t, f) = scale[e*nvars+f] M_e x(e, t, f) per field segment
+// (pseudo_transient_scaling): one CTA per (element, time), one thread per row
+// (f, i), the sum over the element's modes j in increasing order.
+// ---------------------------------------------------------------------------
+static __global__ void k_mass_scale(const double* __restrict__ x, double* __restrict__ y,
+                                    const int64_t* __restrict__ row_yoff, const int32_t* __restrict__ elem_nvars,
+                                    const int32_t* __restrict__ elem_nterms, const int64_t* __restrict__ mass_off,
+                                    const double* __restrict__ mass, const double* __restrict__ scale,
+                                    const int64_t* __restrict__ scale_off, int ntime) {
+    const int row = blockIdx.x;
+    const int e = row / ntime;
+    const int nv = elem_nvars[e], nt = elem_nterms[e];
+    const int64_t o = row_yoff[row];
+    const double* M = mass + mass_off[e];
+    for (int r = threadIdx.x; r < nv * nt; r += blockDim.x) {
+        const int f = r / nt, i = r - f * nt;
+        const double s = scale[scale_off[e] + f];
+        const double* xf = x + o + (int64_t)f * nt;
+        double acc = 0.0;
+        for (int j = 0; j < nt; ++j) acc += (s * M[i + j * nt]) * xf[j];
+        y[o + r] = acc;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // A^T in block-row storage: block k of A^T (nr x nc, column-major) is the
 // transpose of its source block of A (nc x nr).  32 x 32 tiles pass through
 // shared memory so that the reads and the writes are both coalesced; CTAs of

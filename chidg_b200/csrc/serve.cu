@@ -3,9 +3,9 @@
 // Requests (one assembled system each: pattern, packed block values, right-
 // hand side) are submitted at any time and wait in arrival order.  A
 // dispatcher thread forms a batch whenever a worker slot is free: the oldest
-// request and the ones after it that share its number of time levels, up to
-// max_batch systems and the device-memory budget (a batch of one may exceed
-// it).  Admission waits while the batches on the device already hold the
+// request and, in arrival order, the later ones that share its number of time
+// levels and fit the part of the device-memory budget that running batches do
+// not hold, up to max_batch systems (a batch of one may exceed the budget).  Admission waits while the batches on the device already hold the
 // budget.  Each slot is a worker thread with a context (and stream) of its
 // own, so batches run concurrently; a batch is solved by
 // chidg_gpu_fgmres_solve_batched, whose
@@ -224,15 +224,21 @@ void dispatch(chidg_gpu_server* S) {
     for (;;) {
         S->cv.wait(lk, [S] { return (!S->pending.empty() && S->idle > 0) || (S->stopping && S->pending.empty()); });
         if (S->pending.empty()) break;       // stopping, queue drained
+        // the oldest request, then the later ones of its number of time levels
+        // that fit the memory not held by running batches, in arrival order;
+        // requests passed over keep their place
         std::vector<std::shared_ptr<Request>> batch{S->pending.front()};
         S->pending.pop_front();
         int64_t bytes = batch[0]->bytes;
-        while (!S->pending.empty() && (int32_t)batch.size() < S->max_batch) {
-            const auto& nxt = S->pending.front();
-            if (bytes + nxt->bytes > S->budget || nxt->pat.ntime != batch[0]->pat.ntime) break;
-            bytes += nxt->bytes;
-            batch.push_back(nxt);
-            S->pending.pop_front();
+        const int64_t room = S->budget - S->mem_used;
+        for (auto it = S->pending.begin(); it != S->pending.end() && (int32_t)batch.size() < S->max_batch;) {
+            if ((*it)->pat.ntime == batch[0]->pat.ntime && bytes + (*it)->bytes <= room) {
+                bytes += (*it)->bytes;
+                batch.push_back(*it);
+                it = S->pending.erase(it);
+            } else {
+                ++it;
+            }
         }
         // admission by device memory: wait for running batches to finish
         S->cv.wait(lk, [S, bytes] { return S->mem_used + bytes <= S->budget || S->mem_used == 0; });

@@ -19,15 +19,24 @@ Assembly of the residual and its Jacobian stays with the caller, through a
     system.mass -> packed per-element mass matrices (nterms x nterms,
                    column-major), as chidg_gpu_matrix_scale_diagonal takes them
 
-Options and defaults are those of nonlinear_solver_t
-(src/nonlinear_solvers/type_nonlinear_solver.f90:21-36) except residual
-smoothing (Mavriplis 2018, type_newton.f90:160-182), which needs the equation
-set's mass and time step applied to vectors and is not restated: `smooth`
-defaults to False here and True is refused.
+Options are those of nonlinear_solver_t (src/nonlinear_solvers/
+type_nonlinear_solver.f90:21-36), with the defaults of the input namelist
+(src/io/mod_io.f90:58-77): residual smoothing off.  With `smooth` and `ptc`
+the right-hand side is smoothed as type_newton.f90:160-172 does (Mavriplis
+2018): the smoother (a block-Jacobi preconditioner, or the linear solver's own
+preconditioner) is updated on the Jacobian before the pseudo-transient term is
+added, then b = -R - smooth_relax * smoother(M / dtau R), where M / dtau scales
+every field segment by the element mass over the element's smallest pseudo
+time step (pseudo_transient_scaling, :394-441, on the device through
+chidg_gpu_vector_mass_scale).  `nsmooth` is accepted and, as in the
+reference's Newton loop, not used.  With `smooth` and not `ptc` the reference
+prints a warning and leaves b unassigned; here smoothing is skipped with the
+same warning and b = -R.
 """
 from __future__ import annotations
 
 import math
+import sys
 import time
 from dataclasses import dataclass, field
 
@@ -48,6 +57,9 @@ class NewtonOptions:
     ptc: bool = True
     search: str = "backtrack"    # 'backtrack' or 'none'
     smooth: bool = False
+    smoother: str = "jacobi"     # 'jacobi' or 'preconditioner'
+    nsmooth: int = 3
+    smooth_relax: float = 1.0
 
 
 @dataclass
@@ -70,8 +82,8 @@ class Newton:
 
     def __init__(self, **options):
         self.options = NewtonOptions(**options)
-        if self.options.smooth:
-            raise NotImplementedError("newton: residual smoothing is not restated (smooth=False)")
+        if self.options.smoother.lower() not in ("jacobi", "preconditioner"):
+            raise ValueError("newton%solve: invalid smoother. 'default' or 'jacobi'.")
         if self.options.search.lower() not in ("backtrack", "none", ""):
             raise ValueError(f"Invalid nonlinear search algorithm in newton iteration routine: '{self.options.search}'")
 
@@ -90,6 +102,14 @@ class Newton:
         resid, resid_prev, resid0 = 1.0, 1.0, 1.0
         cfln = np.full(nfields, o.cfl0)
         niter = 0
+        smoother, fs, scaled = None, None, None
+        if o.smooth:                                         # :101-110
+            smoother = preconditioner if o.smoother.lower() == "preconditioner" else api.create_preconditioner("jacobi")
+            fs, scaled = api.ChidgVector(A), api.ChidgVector(A)
+            if not o.ptc:
+                print("WARNING: residual smoothing expects pseudo-transient continuation, but pseudo-transient "
+                      "continuation was found to be turned off. Residual smoothing is being turned off for "
+                      "consistency.", file=sys.stderr)
         while True:
             niter += 1
             qold.copy_from(q)
@@ -103,13 +123,16 @@ class Newton:
             resid_prev, resid = resid, rhs.norm()
             b.copy_from(rhs)                                 # b = -rhs (:180)
             b.scale(-1.0)
+            if o.smooth and o.ptc:                           # residual smoothing (:160-172, :360-441)
+                t0 = time.perf_counter()
+                smoother.update(A)                           # before the pseudo-transient term
+                scaled.assign_mass_scaled(rhs, system.mass, self._ptc_scale(system, q, cfln, A))
+                smoother.apply(A, scaled, fs)
+                b.axpy(-o.smooth_relax, fs)                  # b = -rhs - smooth_relax * f_smooth
+                ph["ptc"] += time.perf_counter() - t0
             if o.ptc:                                        # contribute_pseudo_temporal (:320-352)
                 t0 = time.perf_counter()
-                dtau = np.asarray(system.pseudo_timestep(q, cfln), dtype=np.float64)
-                if dtau.ndim == 2:                           # minval(elems(ielem)%dtau) over the fields
-                    dtau = dtau.min(axis=1)
-                scale = np.repeat(1.0 / dtau, A.pattern.elem_nvars)
-                A.scale_diagonal(system.mass, scale)
+                A.scale_diagonal(system.mass, self._ptc_scale(system, q, cfln, A))
                 ph["ptc"] += time.perf_counter() - t0
             if niter == 1:
                 res.residual_norm.append(resid)
@@ -175,9 +198,20 @@ class Newton:
         res.seconds = time.perf_counter() - t_start
         ph["other"] = res.seconds - sum(ph.values())
         res.phase_seconds = ph
-        for v in (rhs, dq, b, qold, qn):
+        for v in (rhs, dq, b, qold, qn) + ((fs, scaled) if fs is not None else ()):
             v.release()
+        if smoother is not None and smoother is not preconditioner:
+            smoother.tear_down()
         return res
+
+    @staticmethod
+    def _ptc_scale(system, q, cfln, A):
+        """1 / dtau per element and field, dtau the element's smallest pseudo
+        time step over its fields (minval(elems(ielem)%dtau), :336-342)."""
+        dtau = np.asarray(system.pseudo_timestep(q, cfln), dtype=np.float64)
+        if dtau.ndim == 2:
+            dtau = dtau.min(axis=1)
+        return np.repeat(1.0 / dtau, A.pattern.elem_nvars)
 
 
 class SyntheticSystem:

@@ -137,16 +137,25 @@ class Server:
                 continue
             self._free.acquire()                       # a worker slot is free
             drain(block=False)                         # requests that arrived meanwhile join
+            # the oldest request, then the later ones of its number of time
+            # levels that fit the memory not held by running batches, in arrival
+            # order; requests passed over keep their place
             first = pending.popleft()
             batch = [first]
             nbytes = request_bytes(first[0].pattern, self.options["nkrylov"])
-            while pending and len(batch) < self.max_batch:
-                nxt = pending[0]
+            with self._mem_lock:
+                room = self.mem_budget - self._mem_used
+            keep = collections.deque()
+            while pending:
+                nxt = pending.popleft()
                 need = request_bytes(nxt[0].pattern, self.options["nkrylov"])
-                if nbytes + need > self.mem_budget or nxt[0].pattern.ntime != first[0].pattern.ntime:
-                    break
-                batch.append(pending.popleft())
-                nbytes += need
+                if (len(batch) < self.max_batch and nbytes + need <= room
+                        and nxt[0].pattern.ntime == first[0].pattern.ntime):
+                    batch.append(nxt)
+                    nbytes += need
+                else:
+                    keep.append(nxt)
+            pending.extend(keep)
             with self._mem_lock:                        # admission by device memory
                 while self._mem_used + nbytes > self.mem_budget and self._mem_used > 0:
                     self._mem_lock.wait()

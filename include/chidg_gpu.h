@@ -245,6 +245,13 @@ int chidg_gpu_vector_clear(chidg_gpu_vector* x);                               /
 int chidg_gpu_vector_copy(chidg_gpu_vector* dst, const chidg_gpu_vector* src); /* =       */
 int chidg_gpu_vector_axpy(chidg_gpu_vector* y, double a, const chidg_gpu_vector* x); /* y += a x */
 int chidg_gpu_vector_scale(chidg_gpu_vector* x, double a);                      /* x = a x */
+/* pseudo_transient_scaling (type_newton.f90:394-441), the vector side of the
+ * pseudo-transient term that residual smoothing applies: for every element e,
+ * time level t and field f, y's segment = scale[e,f] * mass_e * x's segment
+ * (mass and scale packed as chidg_gpu_matrix_scale_diagonal takes them: mass
+ * nterms x nterms column-major per element, nvars(e) scales per element).
+ * x and y are distinct vectors of one matrix. */
+int chidg_gpu_vector_mass_scale(const chidg_gpu_vector* x, chidg_gpu_vector* y, const double* mass, const double* scale);
 /* operator_chidg_dot.f90:30-97 (dot) and type_chidg_vector.f90:1237-1305 (norm) */
 int chidg_gpu_vector_dot(const chidg_gpu_vector* x, const chidg_gpu_vector* y, double* out);
 int chidg_gpu_vector_norm(const chidg_gpu_vector* x, double* out);
@@ -306,6 +313,11 @@ int chidg_gpu_precon_set_schedule(chidg_gpu_precon* M, int32_t schedule);
  * For a transposed matrix the positions are those of A^T's blocks (the same
  * as A's for a structurally symmetric pattern). */
 int chidg_gpu_precon_download_LD(chidg_gpu_precon* M, double* host);
+/* The FP32 factors of the last update in a mixed precision (MIXED_FP32 and
+ * MIXED_BF16: computed in FP32 with TF32 tensor-core products; MIXED_PRECON_FP32:
+ * the FP64 factors rounded), in the same positions; no counterpart in the
+ * reference.  CHIDG_GPU_ESTATE after an FP64 update. */
+int chidg_gpu_precon_download_LD32(chidg_gpu_precon* M, float* host);
 int chidg_gpu_precon_stamp(chidg_gpu_precon* M, int64_t* stamp);
 
 /* ---- fgmres_t%solve (src/linear_solvers/type_fgmres.f90:81-310) ----------- */

@@ -351,6 +351,11 @@ module chidg_gpu_mod
             type(c_ptr),    value :: x
             real(c_double), value :: a
         end function
+        integer(c_int) function chidg_gpu_vector_mass_scale(x, y, mass, scale) bind(c, name='chidg_gpu_vector_mass_scale')
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: x, y
+            real(c_double)     :: mass(*), scale(*)
+        end function
         ! dot (operator_chidg_dot.f90:30-97)
         integer(c_int) function chidg_gpu_vector_dot(x, y, res) bind(c, name='chidg_gpu_vector_dot')
             import :: c_int, c_ptr, c_double
@@ -375,6 +380,11 @@ module chidg_gpu_mod
             import :: c_int, c_ptr, c_double
             type(c_ptr), value :: M
             real(c_double)     :: vals(*)
+        end function
+        integer(c_int) function chidg_gpu_precon_download_LD32(M, vals) bind(c, name='chidg_gpu_precon_download_LD32')
+            import :: c_int, c_ptr, c_float
+            type(c_ptr), value :: M
+            real(c_float)      :: vals(*)
         end function
         ! preconditioner_t%stamp (type_preconditioner.f90:21-121)
         integer(c_int) function chidg_gpu_precon_stamp(M, stamp) bind(c, name='chidg_gpu_precon_stamp')

@@ -13,11 +13,21 @@ the backtracking line search with its acceptance tests and the cfl update
 (:466-549), and the stopping rules (:244-266).  Norms are the oracle's serial
 FP64 norms (type_chidg_vector.f90:1237-1305).
 
+Residual smoothing (:160-172 with apply_residual_smoother and
+pseudo_transient_scaling, :360-441): the smoother (the oracle's block Jacobi,
+or the linear solve's preconditioner kind) is built on the Jacobian before the
+pseudo-transient term, and b = -R - smooth_relax * smoother(M / dtau R), every
+field segment of R scaled by the element mass over the element's smallest
+pseudo time step.  Without ptc the reference warns and leaves b unassigned;
+this restatement then skips smoothing (b = -R), as the device driver does.
+
 The host system provides
     residual(q, jacobian) -> R or (R, values)    packed block values of dR/dq
     pseudo_timestep(q, cfl) -> dtau              nelem x nfields
     add_pseudo_time(values, dtau) -> values      values + mass / dtau_e on the
                                                  diagonal blocks
+    mass_block                                   the element mass matrix (nterms
+                                                 x nterms; smoothing only)
 """
 from __future__ import annotations
 
@@ -28,8 +38,22 @@ import numpy as np
 from . import oracle as O
 
 
+def mass_scale(pattern, x, mass_block, dtau_min):
+    """(M / dtau) x on every element, time level and field segment
+    (pseudo_transient_scaling, type_newton.f90:394-441): y_i = sum_j
+    (s M_ij) x_j with s = 1 / dtau_e, j in increasing order."""
+    nt = mass_block.shape[0]
+    ne, T = int(pattern.nelem), int(pattern.ntime)
+    X = np.asarray(x, dtype=np.float64).reshape(ne, T, -1, nt)
+    S = (1.0 / np.asarray(dtau_min, dtype=np.float64))[:, None, None] * mass_block[None, :, :]    # (e, i, j)
+    Y = np.zeros_like(X)
+    for j in range(nt):
+        Y += S[:, None, None, :, j] * X[:, :, :, j:j + 1]
+    return Y.reshape(-1)
+
+
 def newton(system, pattern, q0, *, cfl0=1.0, cfl_up=1.5, cfl_down=0.1, cfl_max=-1.0, tol=1e-10, rtol=1e-10,
-           nmax=-1, ptc=True, linear_opts=None, precon="ilu0"):
+           nmax=-1, ptc=True, linear_opts=None, precon="ilu0", smooth=False, smoother="jacobi", smooth_relax=1.0):
     """Returns a dict: residual_norm (|R(q0)| then |R| after each step),
     alphas, linear_iterations, linear_rel_residual, q."""
     A = O.OracleMatrix(pattern)
@@ -49,6 +73,14 @@ def newton(system, pattern, q0, *, cfl0=1.0, cfl_up=1.5, cfl_down=0.1, cfl_max=-
             resid0 = resid
             out["residual_norm"].append(resid)
         b = -R
+        if smooth and ptc:
+            A.set_values(vals)                               # the smoother sees the Jacobian before ptc
+            Ms = O.OraclePrecon(A, "jacobi" if smoother == "jacobi" else precon)
+            Ms.update()
+            dmin = np.asarray(system.pseudo_timestep(q, cfl)).min(axis=1)
+            f_smooth = smooth_relax * Ms.apply(mass_scale(pattern, R, system.mass_block, dmin))
+            b = -R - f_smooth
+            del Ms
         if ptc:
             vals = system.add_pseudo_time(vals, system.pseudo_timestep(q, cfl))
         if resid < tol:

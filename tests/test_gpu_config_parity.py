@@ -57,6 +57,10 @@ class _HostEuler:
     def add_pseudo_time(self, vals, dtau):
         return euler.add_pseudo_time(self.box, vals, dtau)
 
+    @property
+    def mass_block(self):
+        return self.box.mass_block
+
 
 def test_cfg1_newton_history_matches_the_oracle_newton():
     centre = tuple(float(c) for c in np.random.default_rng(bench.SEED_A + 11).uniform(0.3, 0.7, 3))

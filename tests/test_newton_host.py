@@ -5,15 +5,18 @@ from chidg_b200.newton import Newton, NewtonOptions
 
 
 def test_defaults_follow_nonlinear_solver_t():
-    """type_nonlinear_solver.f90:21-36 (residual smoothing is not restated)."""
+    """type_nonlinear_solver.f90:21-36, smoothing off as the input namelist
+    sets it (mod_io.f90:74-77)."""
     o = NewtonOptions()
     assert (o.cfl0, o.cfl_max, o.cfl_up, o.cfl_down, o.tol, o.rtol, o.nmax, o.ptc, o.search) == \
         (1.0, -1.0, 1.5, 0.1, 1e-10, 1e-10, -1, True, "backtrack")
+    assert (o.smooth, o.smoother, o.nsmooth, o.smooth_relax) == (False, "jacobi", 3, 1.0)
 
 
-def test_refuses_smoothing_and_unknown_search():
-    with pytest.raises(NotImplementedError):
-        Newton(smooth=True)
+def test_refuses_unknown_smoother_and_search():
+    Newton(smooth=True, smoother="preconditioner")
+    with pytest.raises(ValueError):
+        Newton(smooth=True, smoother="gauss-seidel")
     with pytest.raises(ValueError):
         Newton(search="linesearch")
 
@@ -64,9 +67,16 @@ class _HostSynthetic:
         v[self.pos] += 1.0 / dtau[0, 0]
         return v
 
+    @property
+    def mass_block(self):
+        import numpy as np
+        return np.eye(int(self.pat.elem_nterms[0]))
 
-@pytest.mark.parametrize("ptc,c,cfl0", [(True, 0.2, 100.0), (False, 0.2, 100.0), (True, 2.0, 1.0)])
-def test_host_newton_oracle_matches_dense_loop(ptc, c, cfl0):
+
+@pytest.mark.parametrize("ptc,c,cfl0,smooth", [(True, 0.2, 100.0, False), (False, 0.2, 100.0, False),
+                                                (True, 2.0, 1.0, False), (True, 0.2, 100.0, True),
+                                                (True, 1.0, 5.0, True)])
+def test_host_newton_oracle_matches_dense_loop(ptc, c, cfl0, smooth):
     import numpy as np
 
     from chidg_b200 import mesh
@@ -74,7 +84,7 @@ def test_host_newton_oracle_matches_dense_loop(ptc, c, cfl0):
     from tests.test_gpu_newton import newton_numpy
     pat = mesh.box_pattern(3, 3, 2, 5, mesh.nterms_of_order(1))
     sysm = _HostSynthetic(pat, seed=121, c=c, root_seed=122)
-    opts = dict(tol=1e-9, rtol=1e-12, nmax=40, ptc=ptc, cfl0=cfl0)
+    opts = dict(tol=1e-9, rtol=1e-12, nmax=40, ptc=ptc, cfl0=cfl0, smooth=smooth, smooth_relax=0.5 if smooth else 1.0)
     res = newton_oracle.newton(sysm, pat, np.zeros(pat.vector_size()), **opts,
                                linear_opts=dict(tol=0.0, rtol=1e-12, nkrylov=40, inner_fgmres=0, nmax=400))
     qn, hist, alphas = newton_numpy(sysm, np.zeros(pat.vector_size()), NewtonOptions(**opts))
