@@ -297,7 +297,7 @@ def run_serve_subprocess(device, timeout=900):
 CFG5_REQUESTS = 512
 CFG5_RATE = 200.0           # requests per second, Poisson
 CFG5_SEED = 53
-CFG5_BUDGET = 100 << 30     # device bytes the server admits at once (request_bytes estimates)
+CFG5_BUDGET = 120 << 30     # device bytes the server admits at once (request_bytes estimates)
 CFG5_SLOTS = 2
 CFG5_MAX_BATCH = 32
 CFG5_UNDER = (96, 8.0)      # a second stream below the GPU's capacity: requests, rate

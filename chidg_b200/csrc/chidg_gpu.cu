@@ -1643,8 +1643,8 @@ static int factor_fp32(chidg_gpu_precon* M, chidg_gpu_matrix* A, int precision) 
                 k_task_gemm_tf32<float><<<nl, ST_THREADS, ST_SMEM, ctx->stream>>>(lt, (const GemmPair*)P.d_lpairs.ptr, A32,
                                                                                  L32, nullptr, L32, 1.0);
             else
-                k_task_gemm_umma<float><<<nl, UM_THREADS, UM_SMEM, ctx->stream>>>(lt, (const GemmPair*)P.d_lpairs.ptr, A32,
-                                                                                 L32, nullptr, L32, 1.0, wstat, kSpinLimit);
+                k_task_gemm_umma<float><<<std::min(2 * nl, 2 * ctx->nsm), UM_THREADS, UM_SMEM, ctx->stream>>>(
+                    lt, 2 * nl, (const GemmPair*)P.d_lpairs.ptr, A32, L32, nullptr, L32, 1.0, wstat, kSpinLimit);
             if ((st = check_launch(ctx, "factor L products (FP32 / TF32)"))) return st;
         }
         const int ns = P.stask_ptr[l + 1] - P.stask_ptr[l];
@@ -1656,9 +1656,9 @@ static int factor_fp32(chidg_gpu_precon* M, chidg_gpu_matrix* A, int precision) 
                 k_task_gemm_tf32<double><<<ns, ST_THREADS, ST_SMEM, ctx->stream>>>(stt, (const GemmPair*)P.d_spairs.ptr, L32,
                                                                                   A32, (const double*)A->val.ptr, LD, -1.0);
             else
-                k_task_gemm_umma<double><<<ns, UM_THREADS, UM_SMEM, ctx->stream>>>(stt, (const GemmPair*)P.d_spairs.ptr, L32,
-                                                                                  A32, (const double*)A->val.ptr, LD, -1.0,
-                                                                                  wstat, kSpinLimit);
+                k_task_gemm_umma<double><<<std::min(2 * ns, 2 * ctx->nsm), UM_THREADS, UM_SMEM, ctx->stream>>>(
+                    stt, 2 * ns, (const GemmPair*)P.d_spairs.ptr, L32, A32, (const double*)A->val.ptr, LD, -1.0, wstat,
+                    kSpinLimit);
             if ((st = check_launch(ctx, "factor S products (FP32 / TF32)"))) return st;
         }
         prof_end(ctx, pg);

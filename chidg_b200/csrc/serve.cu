@@ -95,21 +95,23 @@ namespace {
 
 // device bytes one request needs: A, the factors (at most A), the Krylov
 // basis (V and Z) and a few vectors
-int64_t request_bytes(int64_t nval, int64_t n, int32_t nkrylov) {
-    return 8 * nval * 2 + 8 * n * (2 * ((int64_t)nkrylov + 1) + 6);
+int64_t request_bytes(int64_t nval, int64_t n, int32_t nkrylov, int32_t precision) {
+    // FP64 blocks and factors (at most as many), their FP32 copies in a mixed mode
+    const int64_t blocks = 8 * nval * 2 + (precision != CHIDG_GPU_FP64 ? 4 * nval * 2 : 0);
+    return blocks + 8 * n * (2 * ((int64_t)nkrylov + 1) + 6);
 }
 
-void run_batch(chidg_gpu_server* S, chidg_gpu_ctx* ctx, int slot, Job job) {
-    std::vector<std::shared_ptr<Request>>& batch = job.batch;
-    double ph[6] = {0, 0, 0, 0, 0, 0};
-    ph[1] = S->now();
-    cudaSetDevice(ctx->device);
-    const int nsys = (int)batch.size();
+// Solve requests [first, last) of a batch as one packed system on ctx; on
+// success each request's result and solution are filled in.  ph[2..4] and
+// *dev_ms accumulate the phases of the parts solved.
+int solve_group(chidg_gpu_server* S, chidg_gpu_ctx* ctx, std::vector<std::shared_ptr<Request>>& batch, int first,
+                int last, double* ph, float* dev_ms, std::string& err) {
+    const int nsys = last - first;
     // the packed pattern: system s owns elements sys_elem[s] .. sys_elem[s+1]-1
     std::vector<int32_t> nv, nt, pr, re, rt, ce, ct, kd, sys_elem(nsys + 1, 0);
-    int64_t nval = 0, n = 0;
+    int64_t n = 0;
     for (int s = 0; s < nsys; ++s) {
-        const Request& q = *batch[s];
+        const Request& q = *batch[first + s];
         const int32_t e0 = sys_elem[s];
         nv.insert(nv.end(), q.nvars.begin(), q.nvars.end());
         nt.insert(nt.end(), q.nterms.begin(), q.nterms.end());
@@ -119,11 +121,10 @@ void run_batch(chidg_gpu_server* S, chidg_gpu_ctx* ctx, int slot, Job job) {
             rt.push_back(q.rt[k]); ct.push_back(q.ct[k]); kd.push_back(q.kind[k]);
         }
         sys_elem[s + 1] = e0 + q.pat.nelem;
-        nval += q.nval;
         n += q.n;
     }
     chidg_gpu_pattern pat{};
-    pat.nelem = sys_elem[nsys]; pat.ntime = batch[0]->pat.ntime; pat.nblocks = (int64_t)re.size();
+    pat.nelem = sys_elem[nsys]; pat.ntime = batch[first]->pat.ntime; pat.nblocks = (int64_t)re.size();
     pat.elem_nvars = nv.data(); pat.elem_nterms = nt.data(); pat.elem_proc = pr.data();
     pat.blk_row_elem = re.data(); pat.blk_row_time = rt.data(); pat.blk_col_elem = ce.data();
     pat.blk_col_time = ct.data(); pat.blk_kind = kd.data();
@@ -133,13 +134,14 @@ void run_batch(chidg_gpu_server* S, chidg_gpu_ctx* ctx, int slot, Job job) {
     chidg_gpu_precon* M = nullptr;
     std::vector<chidg_gpu_fgmres_result> res(nsys);
     std::vector<double> xh;
+    double t0 = S->now();
     int st = chidg_gpu_matrix_create(ctx, &pat, &A);
     if (!st) st = chidg_gpu_vector_create(A, &b);
     if (!st) st = chidg_gpu_vector_create(A, &x);
     {
         int64_t v0 = 0, o = 0;
         for (int s = 0; s < nsys && !st; ++s) {
-            const Request& q = *batch[s];
+            const Request& q = *batch[first + s];
             if (q.fill) {
                 st = q.fill(q.user, ctx, A, b, x, sys_elem[s]);
             } else {
@@ -152,35 +154,70 @@ void run_batch(chidg_gpu_server* S, chidg_gpu_ctx* ctx, int slot, Job job) {
     }
     if (!st) st = chidg_gpu_vector_clear(x);        // the initial guess (fill functions may use x as scratch)
     if (!st) st = chidg_gpu_ctx_sync(ctx);
-    ph[2] = S->now();
+    double t1 = S->now();
+    ph[2] += t1 - t0;
     if (!st) st = chidg_gpu_precon_create(A, S->precon_kind, &M);
-    ph[3] = S->now();
+    double t2 = S->now();
+    ph[3] += t2 - t1;
     cudaEvent_t ev[2] = {nullptr, nullptr};
     const bool timed = cudaEventCreate(&ev[0]) == cudaSuccess && cudaEventCreate(&ev[1]) == cudaSuccess;
     if (timed) cudaEventRecord(ev[0], ctx->stream);
     if (!st) st = chidg_gpu_fgmres_solve_batched(A, M, nsys, sys_elem.data(), b, x, &S->opts, res.data(), nullptr, 0);
     if (timed) cudaEventRecord(ev[1], ctx->stream);
-    ph[4] = S->now();
+    ph[4] += S->now() - t2;
     if (!st) { xh.resize((size_t)n); st = chidg_gpu_vector_download(x, xh.data()); }
-    float dev_ms = 0.0f;
-    if (timed && (cudaEventSynchronize(ev[1]) != cudaSuccess || cudaEventElapsedTime(&dev_ms, ev[0], ev[1]) != cudaSuccess))
-        dev_ms = -1.0f;
+    float ms = 0.0f;
+    if (timed && cudaEventSynchronize(ev[1]) == cudaSuccess && cudaEventElapsedTime(&ms, ev[0], ev[1]) == cudaSuccess)
+        *dev_ms += ms;
     for (cudaEvent_t e : ev)
         if (e) cudaEventDestroy(e);
-    std::string err;
     if (st) {
         char buf[512] = {0};
         chidg_gpu_last_error(ctx, buf, (int32_t)sizeof(buf));
         err = buf;
     }
-    ph[5] = S->now();
     if (M) chidg_gpu_precon_destroy(M);
     if (x) chidg_gpu_vector_destroy(x);
     if (b) chidg_gpu_vector_destroy(b);
     if (A) chidg_gpu_matrix_destroy(A);
+    if (st == CHIDG_GPU_ENOMEM && nsys > 1) {
+        // the estimate let in more than the device holds: solve the halves in turn
+        chidg_gpu_ctx_sync(ctx);
+        const int mid = first + nsys / 2;
+        std::string e2;
+        st = solve_group(S, ctx, batch, first, mid, ph, dev_ms, e2);
+        if (!st) st = solve_group(S, ctx, batch, mid, last, ph, dev_ms, e2);
+        err = e2;
+        return st;
+    }
+    if (!st) {
+        int64_t o = 0;
+        for (int s = 0; s < nsys; ++s) {
+            Request& q = *batch[first + s];
+            q.result = res[s];
+            q.x.assign(xh.begin() + o, xh.begin() + o + q.n);
+            o += q.n;
+        }
+    }
+    return st;
+}
+
+void run_batch(chidg_gpu_server* S, chidg_gpu_ctx* ctx, int slot, Job job) {
+    std::vector<std::shared_ptr<Request>>& batch = job.batch;
+    double ph[6] = {0, 0, 0, 0, 0, 0};
+    ph[1] = S->now();
+    cudaSetDevice(ctx->device);
+    const int nsys = (int)batch.size();
+    float dev_ms = 0.0f;
+    std::string err;
+    const int st = solve_group(S, ctx, batch, 0, nsys, ph, &dev_ms, err);
+    ph[5] = S->now();
+    // phases as times: on the device, set up, solved (parts solved in turn add up)
+    ph[2] += ph[1];
+    ph[3] += ph[2];
+    ph[4] += ph[3];
 
     std::lock_guard<std::mutex> lk(S->mu);
-    int64_t o = 0;
     for (int s = 0; s < nsys; ++s) {
         Request& q = *batch[s];
         q.status = st;
@@ -188,11 +225,7 @@ void run_batch(chidg_gpu_server* S, chidg_gpu_ctx* ctx, int slot, Job job) {
         q.start = ph[1];
         q.finish = ph[5];
         q.batch_size = nsys;
-        if (!st) {
-            q.result = res[s];
-            q.x.assign(xh.begin() + o, xh.begin() + o + q.n);
-        }
-        o += q.n;
+        if (st) q.x.clear();
         q.done = true;
     }
     BatchRecord& r = S->log[(size_t)job.index];
@@ -315,7 +348,7 @@ std::shared_ptr<Request> new_request(const chidg_gpu_server* S, const chidg_gpu_
     q->pat.nelem = pat->nelem;               // the arrays are copied above; keep only the sizes
     q->pat.ntime = pat->ntime;
     q->pat.nblocks = pat->nblocks;
-    q->bytes = request_bytes(q->nval, q->n, S->opts.nkrylov);
+    q->bytes = request_bytes(q->nval, q->n, S->opts.nkrylov, S->opts.precision);
     return q;
 }
 

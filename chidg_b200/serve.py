@@ -61,11 +61,13 @@ class SolveResult:
         return self.finish - self.arrival
 
 
-def request_bytes(pat: mesh.BlockPattern, nkrylov: int) -> int:
-    """Device bytes one request needs: A, factors (<= A), Krylov basis, vectors."""
+def request_bytes(pat: mesh.BlockPattern, nkrylov: int, precision: str = "fp64") -> int:
+    """Device bytes one request needs: A and its factors (at most as many
+    blocks), their FP32 copies in a mixed mode, the Krylov basis and vectors."""
     _, nval = pat.value_offsets()
     n = pat.vector_size()
-    return int(8 * nval * 2 + 8 * n * (2 * (nkrylov + 1) + 6))
+    blocks = 8 * nval * 2 + (4 * nval * 2 if precision != "fp64" else 0)
+    return int(blocks + 8 * n * (2 * (nkrylov + 1) + 6))
 
 
 class Server:
@@ -142,13 +144,13 @@ class Server:
             # order; requests passed over keep their place
             first = pending.popleft()
             batch = [first]
-            nbytes = request_bytes(first[0].pattern, self.options["nkrylov"])
+            nbytes = request_bytes(first[0].pattern, self.options["nkrylov"], self.options.get("precision", "fp64"))
             with self._mem_lock:
                 room = self.mem_budget - self._mem_used
             keep = collections.deque()
             while pending:
                 nxt = pending.popleft()
-                need = request_bytes(nxt[0].pattern, self.options["nkrylov"])
+                need = request_bytes(nxt[0].pattern, self.options["nkrylov"], self.options.get("precision", "fp64"))
                 if (len(batch) < self.max_batch and nbytes + need <= room
                         and nxt[0].pattern.ntime == first[0].pattern.ntime):
                     batch.append(nxt)
@@ -252,13 +254,19 @@ class NativeServer:
         sysd = req.system
         if not hasattr(sysd, "user"):
             raise TypeError("the native server fills requests described by euler.NewtonSystem")
+        return self.submit_fill(req, C.cast(self.L.chidg_gpu_euler_fill_system, C.c_void_p), sysd.user, keep=sysd)
+
+    def submit_fill(self, req: SolveRequest, fill, user, keep=None) -> "NativeFuture":
+        """chidg_gpu_serve_submit_fill with any chidg_gpu_fill_fn (a function
+        address, or a _lib.FILL_FN callback) and its user pointer; `keep` (and
+        the callback) stay referenced until the request's result is taken."""
         pat = req.pattern.as_struct()
         ticket = C.c_int64()
-        fn = C.cast(self.L.chidg_gpu_euler_fill_system, C.c_void_p)
-        st = self.L.chidg_gpu_serve_submit_fill(self.h, C.byref(pat), fn, sysd.user, C.byref(ticket))
+        fn = fill if isinstance(fill, C.c_void_p) else C.cast(fill, C.c_void_p)
+        st = self.L.chidg_gpu_serve_submit_fill(self.h, C.byref(pat), fn, user, C.byref(ticket))
         if st:
             raise _lib.ChidgGpuError(st, "serve_submit_fill")
-        return NativeFuture(self, req, ticket.value, (sysd,))
+        return NativeFuture(self, req, ticket.value, (keep, fill))
 
     def batch_log(self) -> list[dict]:
         """The finished batches' records (chidg_gpu_serve_batch_log), times in

@@ -1,10 +1,13 @@
 """Continuous-batching server: requests of different sizes arriving while
 others run are solved correctly, and each request's answer is the same
 alone and in a mix (the batched solver never mixes systems' arithmetic)."""
+import threading
+import time
+
 import numpy as np
 import pytest
 
-from chidg_b200 import api, euler, mesh, serve
+from chidg_b200 import _lib, api, euler, mesh, serve
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -103,3 +106,44 @@ def test_filled_requests_match_uploaded_ones(server):
         for r in log:
             assert r["formed"] <= r["taken"] <= r["on_device"] <= r["set_up"] <= r["solved"] <= r["on_host"]
             assert r["device_ms"] > 0 and r["slot"] in (0, 1)
+
+
+def test_native_server_splits_a_batch_that_runs_out_of_memory():
+    """A batch whose systems do not fit on the device (here: a fill function
+    that reports ENOMEM for every system but the first of a packed group) is
+    solved in halves, in turn, down to single systems; every request still
+    gets the answer it gets when uploaded."""
+    reqs = fill_requests()[:3]
+    blocker = fill_requests()[3]
+    L = _lib.lib()
+    seen = []
+    gate = threading.Event()
+
+    @_lib.FILL_FN
+    def hold(user, ctx, A, b, work, elem0):
+        gate.wait(60)                                 # keeps the only worker busy
+        return L.chidg_gpu_euler_fill_system(user, ctx, A, b, work, elem0)
+
+    @_lib.FILL_FN
+    def tight(user, ctx, A, b, work, elem0):
+        seen.append(elem0)
+        if elem0 > 0:
+            return _lib.ENOMEM
+        return L.chidg_gpu_euler_fill_system(user, ctx, A, b, work, elem0)
+
+    srv = serve.NativeServer(slots=1, max_batch=3, **OPTS)
+    try:
+        f0 = srv.submit_fill(blocker, hold, blocker.system.user, keep=blocker.system)
+        time.sleep(0.5)
+        futs = [srv.submit_fill(r, tight, r.system.user, keep=r.system) for r in reqs]
+        gate.set()
+        f0.result()
+        got = [f.result() for f in futs]
+        log = srv.batch_log()
+        ref = [f.result() for f in [srv.submit(r) for r in fill_requests()[:3]]]
+    finally:
+        srv.close()
+    assert any(r["systems"] == 3 for r in log)        # the three formed one batch
+    assert any(e > 0 for e in seen)                   # which ran out and was split
+    for a, c in zip(got, ref):
+        assert a.niter == c.niter and np.array_equal(a.x, c.x)
