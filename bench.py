@@ -420,7 +420,8 @@ def run_serve_leg(device, runs=1):
     for prec in ("mixed_precon_fp32", "fp64"):
         results = [stream(prec, reqs, CFG5_RATE, 5) for _ in range(runs)]
         out[prec] = results[0] if runs == 1 else {"runs": results}
-        out["below_capacity"][prec] = stream(prec, under, CFG5_UNDER[1], 6)
+        under_runs = [stream(prec, under, CFG5_UNDER[1], 6) for _ in range(runs)]
+        out["below_capacity"][prec] = under_runs[0] if runs == 1 else {"runs": under_runs}
     first = (lambda v: v if "runs" not in v else v["runs"][0])
     out["speedup_mixed_vs_fp64"] = first(out["mixed_precon_fp32"])["solves_per_s"] / first(out["fp64"])["solves_per_s"]
     return out

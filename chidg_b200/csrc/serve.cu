@@ -95,15 +95,20 @@ namespace {
 
 // device bytes one request needs: A, the factors (at most A), the Krylov
 // basis (V and Z) and a few vectors
-int64_t request_bytes(int64_t nval, int64_t n, int32_t nkrylov, int32_t precision) {
-    // FP64 blocks and factors (at most as many), their FP32 copies in a mixed mode
-    const int64_t blocks = 8 * nval * 2 + (precision != CHIDG_GPU_FP64 ? 4 * nval * 2 : 0);
+// Device bytes one request needs: its blocks (nval values), the ILU factors
+// (the values of its diagonal and lower blocks, nlow), their FP32 copies in a
+// mixed mode, the Krylov basis and a few vectors.  An estimate for admission:
+// a batch that does not fit after all is solved in halves.
+int64_t request_bytes(int64_t nval, int64_t nlow, int64_t n, int32_t nkrylov, int32_t precision) {
+    const int64_t blocks = 8 * (nval + nlow) + (precision != CHIDG_GPU_FP64 ? 4 * (nval + nlow) : 0);
     return blocks + 8 * n * (2 * ((int64_t)nkrylov + 1) + 6);
 }
 
 // Solve requests [first, last) of a batch as one packed system on ctx; on
-// success each request's result and solution are filled in.  ph[2..4] and
-// *dev_ms accumulate the phases of the parts solved.
+// success each request's result and solution are filled in.  ph[2..5]
+// accumulate the durations of the phases (on the device, set up, solved,
+// solution on the host) and *dev_ms the solves' device time, over the parts
+// solved; freeing the batch's objects afterwards is not counted.
 int solve_group(chidg_gpu_server* S, chidg_gpu_ctx* ctx, std::vector<std::shared_ptr<Request>>& batch, int first,
                 int last, double* ph, float* dev_ms, std::string& err) {
     const int nsys = last - first;
@@ -165,7 +170,9 @@ int solve_group(chidg_gpu_server* S, chidg_gpu_ctx* ctx, std::vector<std::shared
     if (!st) st = chidg_gpu_fgmres_solve_batched(A, M, nsys, sys_elem.data(), b, x, &S->opts, res.data(), nullptr, 0);
     if (timed) cudaEventRecord(ev[1], ctx->stream);
     ph[4] += S->now() - t2;
+    const double t3 = S->now();
     if (!st) { xh.resize((size_t)n); st = chidg_gpu_vector_download(x, xh.data()); }
+    ph[5] += S->now() - t3;
     float ms = 0.0f;
     if (timed && cudaEventSynchronize(ev[1]) == cudaSuccess && cudaEventElapsedTime(&ms, ev[0], ev[1]) == cudaSuccess)
         *dev_ms += ms;
@@ -211,11 +218,8 @@ void run_batch(chidg_gpu_server* S, chidg_gpu_ctx* ctx, int slot, Job job) {
     float dev_ms = 0.0f;
     std::string err;
     const int st = solve_group(S, ctx, batch, 0, nsys, ph, &dev_ms, err);
-    ph[5] = S->now();
-    // phases as times: on the device, set up, solved (parts solved in turn add up)
-    ph[2] += ph[1];
-    ph[3] += ph[2];
-    ph[4] += ph[3];
+    // phases as times from the durations (parts solved in turn add up)
+    for (int i = 2; i < 6; ++i) ph[i] += ph[i - 1];
 
     std::lock_guard<std::mutex> lk(S->mu);
     for (int s = 0; s < nsys; ++s) {
@@ -341,14 +345,17 @@ std::shared_ptr<Request> new_request(const chidg_gpu_server* S, const chidg_gpu_
         if (q->nvars[e] <= 0 || q->nterms[e] <= 0) return nullptr;
         q->n += (int64_t)pat->ntime * q->nvars[e] * q->nterms[e];
     }
+    int64_t nlow = 0;                        // values of the diagonal and lower blocks (natural order)
     for (int64_t k = 0; k < nb; ++k) {
         if (q->re[k] < 0 || q->re[k] >= ne || q->ce[k] < 0 || q->ce[k] >= ne) return nullptr;
-        q->nval += (int64_t)q->nvars[q->re[k]] * q->nterms[q->re[k]] * q->nvars[q->ce[k]] * q->nterms[q->ce[k]];
+        const int64_t v = (int64_t)q->nvars[q->re[k]] * q->nterms[q->re[k]] * q->nvars[q->ce[k]] * q->nterms[q->ce[k]];
+        q->nval += v;
+        if (q->ce[k] < q->re[k] || (q->ce[k] == q->re[k] && q->ct[k] <= q->rt[k])) nlow += v;
     }
     q->pat.nelem = pat->nelem;               // the arrays are copied above; keep only the sizes
     q->pat.ntime = pat->ntime;
     q->pat.nblocks = pat->nblocks;
-    q->bytes = request_bytes(q->nval, q->n, S->opts.nkrylov, S->opts.precision);
+    q->bytes = request_bytes(q->nval, nlow, q->n, S->opts.nkrylov, S->opts.precision);
     return q;
 }
 

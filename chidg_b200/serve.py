@@ -62,11 +62,18 @@ class SolveResult:
 
 
 def request_bytes(pat: mesh.BlockPattern, nkrylov: int, precision: str = "fp64") -> int:
-    """Device bytes one request needs: A and its factors (at most as many
-    blocks), their FP32 copies in a mixed mode, the Krylov basis and vectors."""
+    """Device bytes one request needs (an estimate for admission, as the
+    native server makes it): its blocks, the ILU factors (the values of the
+    diagonal and lower blocks in natural order), their FP32 copies in a mixed
+    mode, the Krylov basis and a few vectors."""
     _, nval = pat.value_offsets()
+    nr, nc = pat.block_dims()
+    re, ce = np.asarray(pat.blk_row_elem), np.asarray(pat.blk_col_elem)
+    rt, ct = np.asarray(pat.blk_row_time), np.asarray(pat.blk_col_time)
+    low = (ce < re) | ((ce == re) & (ct <= rt))
+    nlow = int((np.asarray(nr, dtype=np.int64) * np.asarray(nc, dtype=np.int64))[low].sum())
     n = pat.vector_size()
-    blocks = 8 * nval * 2 + (4 * nval * 2 if precision != "fp64" else 0)
+    blocks = 8 * (nval + nlow) + (4 * (nval + nlow) if precision != "fp64" else 0)
     return int(blocks + 8 * n * (2 * (nkrylov + 1) + 6))
 
 

@@ -4,8 +4,8 @@ cores (k_task_gemm_umma: TF32 operands, FP32 accumulation in tensor memory).
 Its FP32 factors are checked against the FP64 factors (TF32 rounding bound)
 and against the same products by the mma.sync TF32 kernel, computed in a
 child process (CHIDG_FACTOR32_MMA=sync): both round the operands to TF32 the
-same way, whose products are exact in FP32, so the two differ only by the
-order of the FP32 sums."""
+same way and accumulate K in the same steps of 8 in FP32, and they give the
+same factors bit for bit."""
 import os
 import subprocess
 import sys
@@ -62,7 +62,7 @@ def test_tcgen05_factor_products(shape, P, nvars, tmp_path):
         worst_sync = max(worst_sync, np.linalg.norm(g - s) / np.linalg.norm(s))
     assert np.all(np.isfinite(ld32))
     assert worst64 < 5e-3, worst64          # TF32 operands (11-bit significands)
-    assert worst_sync < 2e-5, worst_sync    # the same TF32 products summed in another order
+    assert worst_sync == 0.0 and np.array_equal(ld32, ld_sync), worst_sync
 
 
 def test_download_ld32_refused_after_fp64_update():
