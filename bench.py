@@ -300,7 +300,7 @@ CFG5_SEED = 53
 CFG5_BUDGET = 120 << 30     # device bytes the server admits at once (request_bytes estimates)
 CFG5_SLOTS = 2
 CFG5_MAX_BATCH = 32
-CFG5_UNDER = (96, 8.0)      # a second stream below the GPU's capacity: requests, rate
+CFG5_UNDER = (64, 4.0)      # a second stream below the GPU's capacity: requests, rate
 
 
 def cfg5_requests(count=CFG5_REQUESTS, seed=CFG5_SEED):
