@@ -8,8 +8,9 @@ admitted while others are still on the GPU run concurrently with them.
 Inside a batch the systems are solved together by
 chidg_gpu_fgmres_solve_batched: one launch per matvec / ILU sweep /
 reduction for all of them, and an independent Arnoldi process per system.
-A system's arithmetic never depends on which other systems share its batch,
-so a request gets the same answer alone and in a mix.
+A system's arithmetic depends on the other systems of its batch only through
+the launch shape of the batch's block-size class, so with one shape for every
+class (the default) a request gets bitwise the same answer alone and in a mix.
 
 Latency is measured from arrival to the result being back on the host.
 """

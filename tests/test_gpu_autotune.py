@@ -16,6 +16,17 @@ pytestmark = pytest.mark.gpu
 OPTS = dict(tol=0.0, rtol=1e-10, nkrylov=20, inner_fgmres=0, nmax=400)
 
 
+@pytest.fixture(autouse=True)
+def _restore_shapes():
+    """The shape table belongs to the process: put it back as it was, so the
+    tests that run later see the default shapes."""
+    keys = [(k, b, w) for k in tuning.KINDS for b in tuning.CLASSES for w in (8, 4, 2)]
+    saved = {key: tuning.get_shape(*key) for key in keys}
+    yield
+    for key, sh in saved.items():
+        tuning.set_shape(*key, sh)
+
+
 def _system(P=2):
     pat = mesh.box_pattern(6, 5, 4, 5, mesh.nterms_of_order(P))
     return pat, mesh.synth_values(pat, seed=61), mesh.synth_vector(pat.vector_size(), seed=62)
