@@ -80,6 +80,9 @@ struct chidg_gpu_server {
     bool stopping = false;                   // no more submissions; the dispatcher drains the queue
     bool workers_stop = false;               // the workers exit once the job queue is empty
     int idle = 0;                            // workers without a batch
+    int nslots = 0;
+    int exclusive = 0;                       // a batch runs alone after running out of memory
+    int waiting = 0;                         // batches waiting to run alone (form and admit nothing meanwhile)
     int64_t mem_used = 0, peak_mem = 0, batches = 0;
     std::vector<chidg_gpu_ctx*> all_ctx;
     std::vector<BatchRecord> log;            // one per formed batch
@@ -110,7 +113,7 @@ int64_t request_bytes(int64_t nval, int64_t nlow, int64_t n, int32_t nkrylov, in
 // solution on the host) and *dev_ms the solves' device time, over the parts
 // solved; freeing the batch's objects afterwards is not counted.
 int solve_group(chidg_gpu_server* S, chidg_gpu_ctx* ctx, std::vector<std::shared_ptr<Request>>& batch, int first,
-                int last, double* ph, float* dev_ms, std::string& err) {
+                int last, double* ph, float* dev_ms, std::string& err, bool alone = false) {
     const int nsys = last - first;
     // the packed pattern: system s owns elements sys_elem[s] .. sys_elem[s+1]-1
     std::vector<int32_t> nv, nt, pr, re, rt, ce, ct, kd, sys_elem(nsys + 1, 0);
@@ -197,6 +200,30 @@ int solve_group(chidg_gpu_server* S, chidg_gpu_ctx* ctx, std::vector<std::shared
         err = e2;
         return st;
     }
+    if (st == CHIDG_GPU_ENOMEM && !alone) {
+        // one system that does not fit beside the other batches on the device:
+        // admit nothing new, wait (bounded) until it is the only batch left, and
+        // try once more
+        chidg_gpu_ctx_sync(ctx);
+        {
+            // every other worker idle or waiting too (a waiting worker holds no
+            // device memory), and no other batch running alone
+            std::unique_lock<std::mutex> lk(S->mu);
+            ++S->waiting;
+            S->cv.notify_all();
+            S->cv.wait_for(lk, std::chrono::seconds(600),
+                           [S] { return S->exclusive == 0 && S->idle + S->waiting >= S->nslots; });
+            --S->waiting;
+            ++S->exclusive;
+        }
+        std::string e2;
+        st = solve_group(S, ctx, batch, first, last, ph, dev_ms, e2, true);
+        err = e2;
+        std::lock_guard<std::mutex> lk(S->mu);
+        --S->exclusive;
+        S->cv.notify_all();
+        return st;
+    }
     if (!st) {
         int64_t o = 0;
         for (int s = 0; s < nsys; ++s) {
@@ -259,7 +286,10 @@ void work(chidg_gpu_server* S, chidg_gpu_ctx* ctx, int slot) {
 void dispatch(chidg_gpu_server* S) {
     std::unique_lock<std::mutex> lk(S->mu);
     for (;;) {
-        S->cv.wait(lk, [S] { return (!S->pending.empty() && S->idle > 0) || (S->stopping && S->pending.empty()); });
+        S->cv.wait(lk, [S] {
+            return (!S->pending.empty() && S->idle > 0 && S->exclusive == 0 && S->waiting == 0) ||
+                   (S->stopping && S->pending.empty());
+        });
         if (S->pending.empty()) break;       // stopping, queue drained
         // the oldest request, then the later ones of its number of time levels
         // that fit the memory not held by running batches, in arrival order;
@@ -278,7 +308,9 @@ void dispatch(chidg_gpu_server* S) {
             }
         }
         // admission by device memory: wait for running batches to finish
-        S->cv.wait(lk, [S, bytes] { return S->mem_used + bytes <= S->budget || S->mem_used == 0; });
+        S->cv.wait(lk, [S, bytes] {
+            return (S->mem_used + bytes <= S->budget || S->mem_used == 0) && S->exclusive == 0 && S->waiting == 0;
+        });
         S->mem_used += bytes;
         S->peak_mem = std::max(S->peak_mem, S->mem_used);
         const int64_t index = S->batches++;
@@ -317,6 +349,7 @@ extern "C" int chidg_gpu_serve_create(int device, int32_t slots, int64_t mem_bud
         S->all_ctx.push_back(c);
     }
     S->idle = slots;
+    S->nslots = slots;
     for (size_t i = 0; i < S->all_ctx.size(); ++i) S->workers.emplace_back(work, S, S->all_ctx[i], (int)i);
     S->dispatcher = std::thread(dispatch, S);
     *out = S;

@@ -99,6 +99,27 @@ struct Pattern {
         p.blk_kind = blk_kind.data();
         return p;
     }
+    // Patterns of independent systems packed block-diagonally (the layout of
+    // chidg_gpu_fgmres_solve_batched); sys_elem[s] is system s's first element,
+    // sys_elem[n] the total.  All systems must have the same time levels.
+    static Pattern concat(const std::vector<const Pattern*>& parts, std::vector<int32_t>* sys_elem) {
+        Pattern p;
+        if (sys_elem) sys_elem->assign(1, 0);
+        for (const Pattern* q : parts) {
+            if (p.nelem == 0) p.ntime = q->ntime;
+            else if (q->ntime != p.ntime) throw Error(CHIDG_GPU_EINVAL, "Pattern::concat: systems of different time levels");
+            const int32_t e0 = p.nelem;
+            p.elem_nvars.insert(p.elem_nvars.end(), q->elem_nvars.begin(), q->elem_nvars.end());
+            p.elem_nterms.insert(p.elem_nterms.end(), q->elem_nterms.begin(), q->elem_nterms.end());
+            p.elem_proc.insert(p.elem_proc.end(), q->elem_nvars.size(), 0);
+            for (int64_t k = 0; k < q->nblocks(); ++k)
+                p.add_block(q->blk_row_elem[k] + e0, q->blk_row_time[k], q->blk_col_elem[k] + e0, q->blk_col_time[k],
+                            q->blk_kind[k]);
+            p.nelem += q->nelem;
+            if (sys_elem) sys_elem->push_back(p.nelem);
+        }
+        return p;
+    }
     // The pattern of an nx x ny x nz hex box (elements i fastest), rows in the
     // reference's storage order: per (element, time) the interior faces in the
     // order XI_MIN, XI_MAX, ETA_MIN, ETA_MAX, ZETA_MIN, ZETA_MAX, then DIAG, then
@@ -369,6 +390,20 @@ public:
         res_estimate = r.res_estimate;
         r0norm_initial = r.r0norm_initial;
     }
+    // Independent systems packed block-diagonally in A (system s owns elements
+    // sys_elem[s] .. sys_elem[s+1]-1): one result per system
+    // (chidg_gpu_fgmres_solve_batched; no counterpart in the reference)
+    std::vector<chidg_gpu_fgmres_result> solve_batched(ChidgMatrix& A, ChidgVector& x, const ChidgVector& b,
+                                                       Preconditioner& M, const std::vector<int32_t>& sys_elem) {
+        if (!M.handle()) M.init(A);
+        if (sys_elem.size() < 2) throw Error(CHIDG_GPU_EINVAL, "solve_batched: no systems");
+        std::vector<chidg_gpu_fgmres_result> r(sys_elem.size() - 1);
+        detail::check(A.context().handle(),
+                      chidg_gpu_fgmres_solve_batched(A.handle(), M.handle(), (int32_t)r.size(), sys_elem.data(), b.handle(),
+                                                     x.handle(), &opts_, r.data(), nullptr, 0),
+                      "fgmres%solve (batched)");
+        return r;
+    }
     const std::vector<double>& hist() const { return hist_; }
     const chidg_gpu_fgmres_opts& options() const { return opts_; }
 
@@ -416,6 +451,68 @@ public:
 private:
     Context* ctx_ = nullptr;
     chidg_gpu_euler* h_ = nullptr;
+};
+
+// The first Newton step's system of a described Euler box (or harmonic-balance
+// box) written into elements elem0.. of A and its segment of b
+// (chidg_gpu_euler_fill_system; work's segment is overwritten)
+inline void fill_euler_system(const chidg_gpu_euler_system& sys, ChidgMatrix& A, ChidgVector& b, ChidgVector& work,
+                              int32_t elem0) {
+    detail::check(A.context().handle(),
+                  chidg_gpu_euler_fill_system(const_cast<chidg_gpu_euler_system*>(&sys), A.context().handle(), A.handle(),
+                                              b.handle(), work.handle(), elem0),
+                  "euler_fill_system");
+}
+
+// The continuous-batching server of the C ABI (chidg_gpu_serve_*; no
+// counterpart in the reference).  A request's arrays (submit) or description
+// (submit_fill's user pointer) must stay valid until its wait returns.
+class Server {
+public:
+    Server(int device, int32_t slots, int64_t mem_budget, int32_t max_batch, int32_t precon_kind,
+           const LinearSolver& solver) {
+        detail::check(nullptr,
+                      chidg_gpu_serve_create(device, slots, mem_budget, max_batch, precon_kind, &solver.options(), &h_),
+                      "serve_create");
+    }
+    ~Server() { if (h_) chidg_gpu_serve_destroy(h_); }
+    Server(const Server&) = delete;
+    Server& operator=(const Server&) = delete;
+
+    int64_t submit(const Pattern& pat, const double* values, const double* rhs) {
+        const chidg_gpu_pattern v = pat.view();
+        int64_t t = -1;
+        detail::check(nullptr, chidg_gpu_serve_submit(h_, &v, values, rhs, &t), "serve_submit");
+        return t;
+    }
+    int64_t submit_fill(const Pattern& pat, chidg_gpu_fill_fn fill, void* user) {
+        const chidg_gpu_pattern v = pat.view();
+        int64_t t = -1;
+        detail::check(nullptr, chidg_gpu_serve_submit_fill(h_, &v, fill, user, &t), "serve_submit_fill");
+        return t;
+    }
+    // an Euler system written on the device when its batch is formed
+    int64_t submit_euler(const Pattern& pat, const chidg_gpu_euler_system& sys) {
+        return submit_fill(pat, chidg_gpu_euler_fill_system, const_cast<chidg_gpu_euler_system*>(&sys));
+    }
+    // the request's solution into x (its vector length); timing: arrival,
+    // start, finish (seconds since the server's creation) and the batch size
+    chidg_gpu_fgmres_result wait(int64_t ticket, double* x, std::array<double, 4>* timing = nullptr) {
+        chidg_gpu_fgmres_result r{};
+        std::array<double, 4> t{};
+        detail::check(nullptr, chidg_gpu_serve_wait(h_, ticket, x, &r, t.data()), "serve_wait");
+        if (timing) *timing = t;
+        return r;
+    }
+    // batch i's record (chidg_gpu_serve_batch_log)
+    std::array<double, 9> batch_log(int64_t i) {
+        std::array<double, 9> rec{};
+        detail::check(nullptr, chidg_gpu_serve_batch_log(h_, i, rec.data()), "serve_batch_log");
+        return rec;
+    }
+
+private:
+    chidg_gpu_server* h_ = nullptr;
 };
 
 }  // namespace chidg_gpu

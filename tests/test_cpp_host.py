@@ -13,6 +13,7 @@ SRC = os.path.join(ROOT, "tests", "cpp", "test_reference_kats.cpp")
 
 
 EULER_SRC = os.path.join(ROOT, "tests", "cpp", "test_euler_freestream.cpp")
+BATCH_SRC = os.path.join(ROOT, "tests", "cpp", "test_batched_serve.cpp")
 
 
 def build(tmp_path, src=SRC):
@@ -40,6 +41,7 @@ def cases_text():
 def test_host_layer_compiles_and_links(tmp_path):
     assert os.path.exists(build(tmp_path))
     assert os.path.exists(build(tmp_path, EULER_SRC))
+    assert os.path.exists(build(tmp_path, BATCH_SRC))
 
 
 @pytest.mark.gpu
@@ -57,3 +59,11 @@ def test_euler_assembly_through_cpp_host_layer(tmp_path):
     exe = build(tmp_path, EULER_SRC)
     p = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     assert p.returncode == 0, p.stdout + p.stderr
+
+
+@pytest.mark.gpu
+def test_batched_and_served_solves_through_cpp_host_layer(tmp_path):
+    exe = build(tmp_path, BATCH_SRC)
+    p = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stdout + p.stderr
+    assert "0 failures" in p.stdout

@@ -147,3 +147,28 @@ def test_native_server_splits_a_batch_that_runs_out_of_memory():
     assert any(e > 0 for e in seen)                   # which ran out and was split
     for a, c in zip(got, ref):
         assert a.niter == c.niter and np.array_equal(a.x, c.x)
+
+
+def test_native_server_retries_a_system_alone_after_running_out_of_memory():
+    """One system that runs out of device memory beside other batches (here:
+    its fill function reports ENOMEM the first time) waits until it is the
+    only batch on the device and is solved then."""
+    req = fill_requests()[1]
+    L = _lib.lib()
+    calls = []
+
+    @_lib.FILL_FN
+    def once(user, ctx, A, b, work, elem0):
+        calls.append(elem0)
+        if len(calls) == 1:
+            return _lib.ENOMEM
+        return L.chidg_gpu_euler_fill_system(user, ctx, A, b, work, elem0)
+
+    srv = serve.NativeServer(slots=2, max_batch=3, **OPTS)
+    try:
+        got = srv.submit_fill(req, once, req.system.user, keep=req.system).result(timeout=300)
+        ref = srv.submit(fill_requests()[1]).result(timeout=300)
+    finally:
+        srv.close()
+    assert len(calls) == 2
+    assert got.niter == ref.niter and np.array_equal(got.x, ref.x)
