@@ -77,11 +77,6 @@ def matvec_bytes(pat, sA=8, sv=8):
     return NB * b * b * sA + (NB + E) * b * sv
 
 
-def ilu_apply_bytes(pat, sL=8, sA=8, sv=8):
-    b, E, nL, nU, NB = counts(pat)
-    return (nL + E) * b * b * sL + nU * b * b * sA + 4 * E * b * sv
-
-
 def ilu_forward_bytes(pat, sL=8, sv=8):
     """L blocks read, v read, z written."""
     b, E, nL, nU, NB = counts(pat)
@@ -92,6 +87,17 @@ def ilu_backward_bytes(pat, sL=8, sA=8, sv=8):
     """U blocks (from A) and inv(D) read, z read and written."""
     b, E, nL, nU, NB = counts(pat)
     return nU * b * b * sA + E * b * b * sL + 2 * E * b * sv
+
+
+def fused_matvec_bytes(pat, sA=8, sv=8, sp=8):
+    """The matvec rows inside the backward sweep: with the sweep's U partials
+    reused (CHIDG_FUSED_REUSE, on by default), the diagonal and lower blocks
+    and their x segments are read, the U partials (sp bytes a value) added,
+    y written; otherwise the whole matvec."""
+    if os.environ.get("CHIDG_FUSED_REUSE", "1").startswith("0"):
+        return matvec_bytes(pat, sA, sv)
+    b, E, nL, nU, NB = counts(pat)
+    return (NB - nU) * b * b * sA + (NB - nU + E) * b * sv + nU * b * sp
 
 
 def factor_flops(pat):
@@ -1279,7 +1285,6 @@ def run_gpu(args):
     bm_ms, bm_n = kt["ilu_backward_matvec"]
     fa_ms, fa_n = kt["factor"]
     mvb = matvec_bytes(pat)
-    ilub = ilu_apply_bytes(pat)
     fwb, bwb = ilu_forward_bytes(pat), ilu_backward_bytes(pat)
 
     def cls(ms, cnt, nbytes):
@@ -1292,15 +1297,16 @@ def run_gpu(args):
         "ilu_forward": cls(f_ms, f_n, fwb),
         "ilu_backward": cls(bw_ms, bw_n, bwb),
         # the backward sweep with the following matvec's rows in the same launch
-        "ilu_backward_matvec": cls(bm_ms, bm_n, bwb + mvb),
+        "ilu_backward_matvec": cls(bm_ms, bm_n, bwb + fused_matvec_bytes(pat)),
         "factor": {"launches": fa_n, "total_ms": fa_ms, "avg_ms": fa_ms / max(fa_n, 1),
                    "tflops": factor_flops(pat) / (fa_ms / max(fa_n, 1) / 1e3) / 1e12 if fa_n else None},
     }
     # one Arnoldi step's z = M v and w = A z: forward sweep + (backward sweep and matvec)
     step_ms = kernels["ilu_forward"]["avg_ms"] + (kernels["ilu_backward_matvec"]["avg_ms"] if bm_n else
                                                   kernels["ilu_backward"]["avg_ms"] + kernels["matvec"]["avg_ms"])
-    kernels["precon_and_matvec_per_iteration"] = {"ms": step_ms, "algorithmic_bytes": ilub + mvb,
-                                                  "gbs": (ilub + mvb) / (step_ms / 1e3) / 1e9}
+    step_bytes = fwb + (bwb + fused_matvec_bytes(pat) if bm_n else bwb + mvb)
+    kernels["precon_and_matvec_per_iteration"] = {"ms": step_ms, "algorithmic_bytes": step_bytes,
+                                                  "gbs": step_bytes / (step_ms / 1e3) / 1e9}
     # dominant memory-bound kernel class by total time
     sweep = {"stream": "k_ilu_stream", "tasks": "k_ilu_tasks", "dataflow": "k_ilu_sweep_sf", "levels": "k_ilu_forward/backward"}
     names = {"matvec": "matvec (k_matvec_stream)", "ilu_forward": f"ilu_forward ({sweep[args.schedule]} forward)",

@@ -1469,7 +1469,7 @@ void chidg::release_program(IluProgram& P) {
                       &P.d_bwd_rows, &P.d_ltasks, &P.d_lpairs, &P.d_stasks, &P.d_spairs, &P.d_tf_row, &P.d_tf_ent,
                       &P.d_tb_row, &P.d_tb_ent, &P.d_poff_f, &P.d_poff_b, &P.d_sb_row, &P.d_sb_ent, &P.d_asm_ptr,
                       &P.d_asm_src, &P.d_asm_r0, &P.d_asm_c0, &P.d_asm_nr, &P.d_asm_nc, &P.d_bmv_row, &P.d_bmv_ent,
-                      &P.d_col_prow})
+                      &P.d_col_prow, &P.d_mv_skip})
         release(*b);
     P.bmv_uid = -1;
 }
@@ -2006,13 +2006,27 @@ static int build_bwd_mv_tasks(chidg_gpu_precon* M, const chidg_gpu_matrix* A, in
     }
     std::vector<int32_t> col_prow;
     col_prow.reserve(A->nblk);
+    // the matrix blocks that are the sweep's U blocks (same values, same
+    // column segment), whose partials a matvec row reuses; reuse only when
+    // every U entry of every row is one of its row's blocks
+    std::vector<uint8_t> skip;
+    skip.reserve(A->nblk);
+    bool reuse = true;
     for (int r = 0; r < A->nrow; ++r) {
-        int last = -1;
+        int last = -1, matched = 0;
         for (int32_t k : A->rowblk[r]) {
             const int c = A->row(A->ce[k], A->ct[k]);
             col_prow.push_back(c);
             last = std::max(last, 2 * P.lb[c] - 1);
+            uint8_t u = 0;
+            for (const IluEntry& en : P.up[r])
+                if (en.a_off == A->voff[k] && en.parent == c && en.nc == A->bsize(A->ce[k]) &&
+                    P.z_off[c] == A->seg(A->ce[k], A->ct[k]))
+                    u = 1;
+            matched += u;
+            skip.push_back(u);
         }
+        if (matched != (int)P.up[r].size()) reuse = false;
         keyed.push_back({4LL * (last + 2 * lag) + 2, {r, -3}});
     }
     std::stable_sort(keyed.begin(), keyed.end(), [](const auto& a, const auto& c) { return a.first < c.first; });
@@ -2022,8 +2036,9 @@ static int build_bwd_mv_tasks(chidg_gpu_precon* M, const chidg_gpu_matrix* A, in
     for (auto& k : keyed) { tr.push_back(k.second.first); te.push_back(k.second.second); }
     int st;
     if ((st = upload_array(M->ctx, P.d_bmv_row, tr)) || (st = upload_array(M->ctx, P.d_bmv_ent, te)) ||
-        (st = upload_array(M->ctx, P.d_col_prow, col_prow)))
+        (st = upload_array(M->ctx, P.d_col_prow, col_prow)) || (st = upload_array(M->ctx, P.d_mv_skip, skip)))
         return st;
+    P.bmv_reuse = reuse;
     P.ntask_bmv = (int)tr.size();
     P.bmv_uid = A->uid;
     P.bmv_lag = lag;
@@ -2036,6 +2051,15 @@ static int build_bwd_mv_tasks(chidg_gpu_precon* M, const chidg_gpu_matrix* A, in
 static bool fused_mv_enabled() {
     static const bool v = [] {
         const char* e = std::getenv("CHIDG_FUSED_MV");
+        return !(e && e[0] == '0');
+    }();
+    return v;
+}
+// CHIDG_FUSED_REUSE=0: the fused matvec rows stream every block instead of
+// reusing the sweep's U partials (comparison runs)
+static bool fused_reuse_enabled() {
+    static const bool v = [] {
+        const char* e = std::getenv("CHIDG_FUSED_REUSE");
         return !(e && e[0] == '0');
     }();
     return v;
@@ -2115,10 +2139,17 @@ static int stream_sweeps(chidg_gpu_precon* M, const TL* LD, const TU* U, const T
     if (F) {
         StreamTasks Tm{(const int32_t*)P.d_bmv_row.ptr, (const int32_t*)P.d_bmv_ent.ptr, (const int64_t*)P.d_poff_b.ptr,
                        flags + 2 * P.nprow, flags + 3 * P.nprow};
+        // the sweep's U partials stand for the matvec's U blocks only when
+        // the sweep reads the matvec's own values
+        FusedMv<TA, TV> Fr = *F;
+        Fr.skip = (P.bmv_reuse && fused_reuse_enabled() && sizeof(TU) == sizeof(TA) &&
+                   (const void*)U == (const void*)F->val)
+                      ? (const uint8_t*)P.d_mv_skip.ptr
+                      : nullptr;
         switch (shb.cw) {
-            case 16: st = stream_launch<TL, TU, TV, false, 16, TA, true>(M, LD, U, Tm, P.ntask_bmv, v, zx, pb.ptr, S, shb, variant, *F, mv_cols); break;
-            case 4: st = stream_launch<TL, TU, TV, false, 4, TA, true>(M, LD, U, Tm, P.ntask_bmv, v, zx, pb.ptr, S, shb, variant, *F, mv_cols); break;
-            default: st = stream_launch<TL, TU, TV, false, 8, TA, true>(M, LD, U, Tm, P.ntask_bmv, v, zx, pb.ptr, S, shb, variant, *F, mv_cols);
+            case 16: st = stream_launch<TL, TU, TV, false, 16, TA, true>(M, LD, U, Tm, P.ntask_bmv, v, zx, pb.ptr, S, shb, variant, Fr, mv_cols); break;
+            case 4: st = stream_launch<TL, TU, TV, false, 4, TA, true>(M, LD, U, Tm, P.ntask_bmv, v, zx, pb.ptr, S, shb, variant, Fr, mv_cols); break;
+            default: st = stream_launch<TL, TU, TV, false, 8, TA, true>(M, LD, U, Tm, P.ntask_bmv, v, zx, pb.ptr, S, shb, variant, Fr, mv_cols);
         }
         if (st) return st;
         prof_end(ctx, ph);

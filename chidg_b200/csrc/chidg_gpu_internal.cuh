@@ -73,7 +73,8 @@ struct IluProgram {
     // built for one matrix structure (bmv_uid) on first use
     int ntask_bmv = 0, bmv_lag = -1;
     int64_t bmv_uid = -1;
-    Buffer d_bmv_row, d_bmv_ent, d_col_prow;
+    bool bmv_reuse = false;                    // every U entry is a block of its matrix row (d_mv_skip)
+    Buffer d_bmv_row, d_bmv_ent, d_col_prow, d_mv_skip;
     // rows whose D is assembled from several blocks of A (precon_HB) instead
     // of starting from one diagonal block: pieces per row, placed at (r0, c0)
     bool assembled = false;

@@ -85,8 +85,18 @@ __host__ __device__ constexpr size_t stream_smem_bytes(size_t acc_size, int stag
 // type_fgmres.f90:175-189), run inside the backward sweep's launch: one task
 // per matrix row (entry -3), handed out after the sweep tasks that publish
 // the rows its columns read, so the rows' values stream while the sweep's
-// dependency chain waits.  Row r computes y_r = A_r z and its sum of squares
-// exactly as k_matvec_stream does (same chunks, same per-thread order).
+// dependency chain waits.
+//
+// The sweep has already formed the products of row r's upper blocks with z
+// (the U partials U_rj z_j, ILU0's U being A's upper blocks,
+// precon_ILU0.f90:370-395), and z_j is final when they are formed.  With
+// `skip` set (the sweep's U blocks are the matvec's values, same type), the
+// matvec row streams only the blocks the sweep did not read -- the diagonal,
+// the lower blocks and any others -- and adds the row's U partials, in entry
+// order, to their product: y_r = (A_rr z_r + sum_lower A_rk z_k) + sum_U
+// part.  That drops the U blocks' second read (3/7 of the matrix on a hex
+// box).  Without `skip`, row r computes y_r exactly as k_matvec_stream does
+// (same chunks, same per-thread order).
 template <typename TA, typename TX>
 struct FusedMv {
     MatvecRowsView rows;         // the matrix rows (contiguous values per row)
@@ -94,6 +104,7 @@ struct FusedMv {
     TX* y;
     double* row_sumsq;
     const int32_t* col_prow;     // per block of the matrix: the programme row publishing its column segment
+    const uint8_t* skip = nullptr;   // per block of the matrix: 1 = a U block of the sweep, its partial reused
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -252,12 +263,48 @@ __global__ void __launch_bounds__(32 * CW + 32)
             const unsigned char* base = nullptr;
             int cols = 0, esz = 1;
             if (MV && q == -3) {
-                // matvec row pr: the row's blocks, one b x cols strip
+                // matvec row pr: the row's blocks, one b x cols strip; with
+                // F.skip, only its runs of blocks the sweep did not read
                 const int64_t k0 = F.rows.row_ptr[pr], k1 = F.rows.row_ptr[pr + 1];
                 b = F.rows.row_b[pr];
-                for (int64_t k = k0; k < k1; ++k) cols += F.rows.blk_nc[k];
                 base = reinterpret_cast<const unsigned char*>(F.val + (k1 > k0 ? F.rows.blk_voff[k0] : 0));
                 esz = sizeof(TA);
+                if (F.skip != nullptr) {
+                    const int kc = max(1, chunk_bytes / (b * esz));
+                    // the chunks of every run of streamed blocks: counted, then posted
+                    int nchunk = 0;
+                    for (int pass = 0; pass < 2; ++pass) {
+                        int col = 0, ch = 0;
+                        for (int64_t k = k0; k <= k1; ++k) {
+                            int run0 = col;
+                            while (k < k1 && !F.skip[k]) { col += F.rows.blk_nc[k]; ++k; }
+                            for (int c0 = run0; c0 < col; c0 += kc, ++ch) {
+                                if (pass == 0) continue;
+                                if (!mbar_wait(empty + stage, phase ^ 1u, S.spin_limit)) atomicExch(S.status, 1);
+                                StreamMeta m;
+                                m.task = (int)t; m.pr = pr; m.q = q; m.chunk = ch; m.nchunk = nchunk;
+                                m.col0 = c0;
+                                m.ncols = min(kc, col - c0);
+                                const uintptr_t src = reinterpret_cast<uintptr_t>(base + (size_t)c0 * b * esz);
+                                const uintptr_t a0 = src & ~(uintptr_t)15;
+                                const unsigned bytes = (unsigned)((size_t)m.ncols * b * esz);
+                                const unsigned len = (unsigned)(((src - a0) + bytes + 15) & ~(uintptr_t)15);
+                                m.shift = (int)((src - a0) / esz);
+                                meta[stage] = m;
+                                mbar_arrive_expect_tx(full + stage, len);
+                                bulk_copy_g2s(stages + (size_t)stage * stage_bytes, reinterpret_cast<const void*>(a0), len,
+                                              full + stage);
+                                if (++stage == nstage) { stage = 0; phase ^= 1u; }
+                            }
+                            if (k < k1) col += F.rows.blk_nc[k];      // a skipped block
+                        }
+                        nchunk = ch;
+                    }
+                    if (nchunk > 0) continue;
+                    cols = 0;                                        // nothing streamed: one empty chunk
+                } else {
+                    for (int64_t k = k0; k < k1; ++k) cols += F.rows.blk_nc[k];
+                }
             } else if (q >= 0) {
                 if (FORWARD) { base = reinterpret_cast<const unsigned char*>(LD + R.lo_L[q]); cols = R.lo_nc[q]; esz = sizeof(TL); }
                 else { base = reinterpret_cast<const unsigned char*>(Aval + R.up_U[q]); cols = R.up_nc[q]; esz = sizeof(TU); }
@@ -321,8 +368,10 @@ __global__ void __launch_bounds__(32 * CW + 32)
                 int off = 0;
                 for (int64_t k = k0; k < k1; ++k) {
                     const int nc = F.rows.blk_nc[k];
-                    const TX* xp = zx + F.rows.blk_xoff[k];
-                    for (int c = ctid; c < nc; c += NC) xs[off + c] = cvt<ACC>(ld_cg(xp + c));
+                    if (F.skip == nullptr || !F.skip[k]) {
+                        const TX* xp = zx + F.rows.blk_xoff[k];
+                        for (int c = ctid; c < nc; c += NC) xs[off + c] = cvt<ACC>(ld_cg(xp + c));
+                    }
                     off += nc;
                 }
                 consumers_sync<NC>();
@@ -369,13 +418,20 @@ __global__ void __launch_bounds__(32 * CW + 32)
         // ------------------------------------------------ the task's last chunk
         stream_reduce<NC, RPT>(red, b, r, g, G, ctid, acc);
         if (MV && q == -3) {
-            // y_r = A_r z and its sum of squares, as the streamed matvec writes them
+            // y_r = A_r z and its sum of squares, as the streamed matvec writes
+            // them (with F.skip: plus the row's U partials, in entry order)
             double sq = 0.0;
             const int64_t yo = F.rows.row_yoff[pr];
+            const int u0 = F.skip != nullptr ? R.up_ptr[pr] : 0, u1 = F.skip != nullptr ? R.up_ptr[pr + 1] : 0;
             #pragma unroll
             for (int rr = 0; rr < RPT; ++rr) {
                 const int i = (b <= NC) ? (rr == 0 ? ctid : b) : ctid + NC * rr;
                 if (i < b) {
+                    if (u1 > u0) {
+                        ACC s = 0;
+                        for (int u = u0; u < u1; ++u) s += ld_cg(part + T.part_off[u] + i);
+                        acc[rr] += s;
+                    }
                     const TX o = from_d<TX>((double)acc[rr]);
                     F.y[yo + i] = o;
                     const double od = to_d(o);

@@ -1,9 +1,12 @@
 """The matvec rows run inside the streamed backward sweep (the fused pass that
 FGMRES takes for z = M v followed by w = A z) agree with the separate launches
-to rounding: the fused launch streams its blocks in 20 KB stages where the
-separate launches use 24 KB ones, so only the chunk boundaries of each
-product's two interleaved partial sums differ.  Checked on whole FGMRES
-solves against a process that runs the separate launches (CHIDG_FUSED_MV=0):
+to rounding: the fused rows stream the diagonal and lower blocks and add the
+sweep's products of the upper blocks with z (the U partials the sweep formed),
+where the separate matvec sums every block of the row in one pass, and the
+launches' stages differ in size, so the chunk boundaries of the partial sums
+differ too.  Checked on whole FGMRES solves against a process that runs the
+separate launches (CHIDG_FUSED_MV=0), and against a process whose fused rows
+stream every block (CHIDG_FUSED_REUSE=0):
 FP64 and FP32 preconditioner blocks take the same iterations with the residual
 history within 1e-10 and x within 1e-12; the FP32 and BF16 inner solves reach
 the same FP64 residual with x within 1e-6.  ILU0 and Jacobi, one and three
@@ -46,8 +49,8 @@ print(json.dumps(out))
 """
 
 
-def _run(fused):
-    env = dict(os.environ, CHIDG_FUSED_MV="1" if fused else "0")
+def _run(fused, reuse=True):
+    env = dict(os.environ, CHIDG_FUSED_MV="1" if fused else "0", CHIDG_FUSED_REUSE="1" if reuse else "0")
     p = subprocess.run([sys.executable, "-c", _CHILD, ROOT, json.dumps(CASES)], capture_output=True, text=True,
                        env=env, timeout=600)
     assert p.returncode == 0, p.stderr[-2000:]
@@ -59,14 +62,19 @@ def relerr(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
+def _agree(f, s, key):
+    if "mixed_fp32" in key or "mixed_bf16" in key:
+        assert f["rel_res"] <= 1e-9 * 1.0001 and s["rel_res"] <= 1e-9 * 1.0001, key
+        assert relerr(f["x"], s["x"]) <= 1e-6, key
+        return
+    assert f["niter"] == s["niter"], key
+    assert relerr(f["hist"], s["hist"]) <= 1e-10, key
+    assert relerr(f["x"], s["x"]) <= 1e-12, key
+
+
 def test_fused_sweep_and_matvec_agree_with_the_separate_launches():
-    fused, split = _run(True), _run(False)
+    fused, whole, split = _run(True), _run(True, reuse=False), _run(False)
     for key in split:
-        f, s = fused[key], split[key]
-        if "mixed_fp32" in key or "mixed_bf16" in key:
-            assert f["rel_res"] <= 1e-9 * 1.0001 and s["rel_res"] <= 1e-9 * 1.0001, key
-            assert relerr(f["x"], s["x"]) <= 1e-6, key
-            continue
-        assert f["niter"] == s["niter"], key
-        assert relerr(f["hist"], s["hist"]) <= 1e-10, key
-        assert relerr(f["x"], s["x"]) <= 1e-12, key
+        _agree(fused[key], split[key], key)
+        _agree(whole[key], split[key], key)
+        _agree(fused[key], whole[key], key)
