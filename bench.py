@@ -111,12 +111,14 @@ def factor_flops(pat):
 # the workload by its block count.
 TRAFFIC_14CUBE_BLOCKS = 18032
 TRAFFIC_14CUBE = {"ilu_forward": 1.119160e9 + 14.508288e6, "ilu_backward": 1.520102e9 + 14.406656e6,
-                  "ilu_backward_matvec": 4.141639e9 + 18.169344e6}
+                  "ilu_backward_matvec": 3.051823e9 + 17.806592e6}
 
 
 def measured_traffic(kind, pat):
     if kind not in TRAFFIC_14CUBE:
         return None
+    if kind == "ilu_backward_matvec" and os.environ.get("CHIDG_FUSED_REUSE", "1").startswith("0"):
+        return None           # the capture is of the matvec rows that reuse the U partials
     return TRAFFIC_14CUBE[kind] * pat.nblocks / TRAFFIC_14CUBE_BLOCKS
 
 

@@ -180,14 +180,42 @@ __global__ void __launch_bounds__(1024) k_matvec(const TA* __restrict__ val, con
 template <typename T>
 __global__ void k_mdot_partial(int64_t n, const T* __restrict__ x, const T* __restrict__ y,
                                int64_t ystride, int nq, double* __restrict__ partial) {
-    __shared__ double scratch[32];
-    for (int q = 0; q < nq; ++q) {
-        const T* yq = y + (int64_t)q * ystride;
-        double s = 0.0;
-        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-            s += to_d(x[i]) * to_d(yq[i]);
-        s = block_sum(s, scratch);
-        if (threadIdx.x == 0) partial[(int64_t)q * gridDim.x + blockIdx.x] = s;
+    // eight vectors per pass over x: x[i] is read once for the eight, and the
+    // eight loads of y are in flight together; each sum is formed in the
+    // order of a pass per vector (thread's i in stride order, then the
+    // block_sum tree), so the partials do not depend on the grouping
+    constexpr int QG = 8;
+    __shared__ double scratch[QG][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int q0 = 0; q0 < nq; q0 += QG) {
+        const int qn = min(QG, nq - q0);
+        const T* yq = y + (int64_t)q0 * ystride;
+        double s[QG];
+        #pragma unroll
+        for (int k = 0; k < QG; ++k) s[k] = 0.0;
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+            const double xi = to_d(x[i]);
+            #pragma unroll
+            for (int k = 0; k < QG; ++k)
+                if (k < qn) s[k] += xi * to_d(yq[(int64_t)k * ystride + i]);
+        }
+        #pragma unroll
+        for (int k = 0; k < QG; ++k) s[k] = warp_sum(s[k]);
+        __syncthreads();
+        if (lane == 0) {
+            #pragma unroll
+            for (int k = 0; k < QG; ++k) scratch[k][w] = s[k];
+        }
+        __syncthreads();
+        if (w == 0) {
+            const int nw = (blockDim.x + 31) >> 5;
+            #pragma unroll
+            for (int k = 0; k < QG; ++k) {
+                double t = (lane < nw) ? scratch[k][lane] : 0.0;
+                t = warp_sum(t);
+                if (lane == 0 && k < qn) partial[(int64_t)(q0 + k) * gridDim.x + blockIdx.x] = t;
+            }
+        }
     }
 }
 // out[q] = sum_c partial[q * ncta + c]  (optionally sqrt)
