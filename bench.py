@@ -227,8 +227,9 @@ def uneven_systems(count, seed, max_n=8, device=0):
 
 def run_batch_leg(ctx, schedule, reps=3):
     """The same systems solved one at a time (the plain FP64 path, and the
-    FP32 inner solve) and batched (FP64, and FP64 Krylov with FP32
-    preconditioner blocks); every mode to the same FP64 rtol 1e-8."""
+    FP32 inner solve) and batched (FP64, FP64 Krylov with FP32 preconditioner
+    blocks, and FP64 outer steps preconditioned by batched FP32 inner solves);
+    every mode to the same FP64 rtol 1e-8."""
     from chidg_b200 import api, mesh
     systems = uneven_systems(BATCH_SYSTEMS, seed=7)
     union, sys_elem = mesh.concat_patterns([s[0] for s in systems])
@@ -238,8 +239,9 @@ def run_batch_leg(ctx, schedule, reps=3):
     x = api.ChidgVector(A)
     M = api.create_preconditioner("ilu0", schedule=schedule)
     batched = {}
-    for prec in ("fp64", "mixed_precon_fp32"):
-        solver = api.create_linear_solver("fgmres", **BATCH_OPTS, precision=prec)
+    for prec in ("fp64", "mixed_precon_fp32", "mixed_fp32"):
+        solver = api.create_linear_solver("fgmres", **{**BATCH_OPTS, **(MIXED if prec == "mixed_fp32" else {})},
+                                          precision=prec)
         solver.solve_batched(A, x, b, M, sys_elem)              # warm-up
         ctx.sync()
         t0 = time.perf_counter()
@@ -249,6 +251,7 @@ def run_batch_leg(ctx, schedule, reps=3):
         t = (time.perf_counter() - t0) / reps
         batched[prec] = {"solves_per_s": BATCH_SYSTEMS / t, "ms_per_batch": 1e3 * t,
                          "iterations": [r["niter"] for r in res],
+                         "inner_iterations": [r["inner_iters"] for r in res],
                          "max_true_rel_residual": max(r["residual_norm"] / r["r0norm_initial"] for r in res)}
     M.tear_down()
     for o in (x, b, A):
@@ -279,8 +282,10 @@ def run_batch_leg(ctx, schedule, reps=3):
             "solves_per_s_one_at_a_time_mixed_fp32": BATCH_SYSTEMS / single["mixed_fp32"],
             "solves_per_s_batched_fp64": batched["fp64"]["solves_per_s"],
             "solves_per_s_batched_mixed_precon_fp32": batched["mixed_precon_fp32"]["solves_per_s"],
+            "solves_per_s_batched_mixed_fp32": batched["mixed_fp32"]["solves_per_s"],
             "speedup_vs_plain_fp64": {"batched_fp64": batched["fp64"]["solves_per_s"] / plain,
                                       "batched_mixed_precon_fp32": batched["mixed_precon_fp32"]["solves_per_s"] / plain,
+                                      "batched_mixed_fp32": batched["mixed_fp32"]["solves_per_s"] / plain,
                                       "one_at_a_time_mixed_fp32": BATCH_SYSTEMS / single["mixed_fp32"] / plain},
             "batched": batched}
 
@@ -774,12 +779,19 @@ def cfg4_arena(ctx, draws):
     return A, rhs, sys_elem, time.perf_counter() - t0
 
 
+def cfg4_opts(prec):
+    """The many-solve options of a precision mode (the FP32 inner solves take
+    the mixed restart lengths and inner tolerance of the single solves)."""
+    return {**CFG4_OPTS, **(MIXED if prec in ("mixed_fp32", "mixed_bf16") else {}), "precision": prec}
+
+
 def run_cfg4_leg(ctx, schedule):
     """The many-solve configuration as stated: 512 Euler Newton systems of
     uneven size and order in memory-admitted waves, each wave packed into one
     arena and solved by the batched FGMRES(30) + ILU0 to rtol 1e-8 (FP64
-    residual), with FP32 preconditioner blocks and in plain FP64; a sample of
-    the draws also solved one at a time by the plain FP64 path."""
+    residual), with FP32 inner solves, with FP32 preconditioner blocks and in
+    plain FP64; a sample of the draws also solved one at a time by the plain
+    FP64 path."""
     from chidg_b200 import api, tuning
     draws = cfg4_draws()
     waves = cfg4_waves(draws)
@@ -790,8 +802,9 @@ def run_cfg4_leg(ctx, schedule):
            "systems": len(draws), "waves": len(waves),
            "orders": {str(p): sum(1 for d in draws if d[1] == p) for p in (1, 2, 3)},
            "matrix_bytes_fp64": int(sum(box_matrix_bytes(d[0], d[1]) for d in draws))}
-    modes = {"mixed_precon_fp32": 0.0, "fp64": 0.0}
+    modes = {"mixed_fp32": 0.0, "mixed_precon_fp32": 0.0, "fp64": 0.0}
     iters = {k: [] for k in modes}
+    inner = {k: [] for k in modes}
     worst = {k: 0.0 for k in modes}
     assembly_s = 0.0
     tuned = {}
@@ -801,7 +814,7 @@ def run_cfg4_leg(ctx, schedule):
         x = api.ChidgVector(A)
         for prec in modes:
             M = api.create_preconditioner("ilu0", schedule=schedule)
-            solver = api.create_linear_solver("fgmres", **CFG4_OPTS, precision=prec)
+            solver = api.create_linear_solver("fgmres", **cfg4_opts(prec))
             if schedule == "stream":
                 M.update(A, precision=prec)
                 key = (int(A.pattern.bsize().max()), prec)
@@ -813,6 +826,7 @@ def run_cfg4_leg(ctx, schedule):
             ctx.sync()
             modes[prec] += time.perf_counter() - t0
             iters[prec] += [r["niter"] for r in res]
+            inner[prec] += [r["inner_iters"] for r in res]
             worst[prec] = max(worst[prec], max(r["residual_norm"] / r["r0norm_initial"] for r in res))
             M.tear_down()
         x.release()
@@ -821,13 +835,13 @@ def run_cfg4_leg(ctx, schedule):
     # the plain FP64 path, one system at a time, on a sample of the draws, and
     # the same sample batched (its own waves), for a comparison on equal work
     sample = draws[::max(1, len(draws) // CFG4_SAMPLE)][:CFG4_SAMPLE]
-    sample_batched = {"mixed_precon_fp32": 0.0, "fp64": 0.0}
+    sample_batched = {"mixed_fp32": 0.0, "mixed_precon_fp32": 0.0, "fp64": 0.0}
     for wave in cfg4_waves(sample):
         A, b, sys_elem, _ = cfg4_arena(ctx, wave)
         x = api.ChidgVector(A)
         for prec in sample_batched:
             M = api.create_preconditioner("ilu0", schedule=schedule)
-            solver = api.create_linear_solver("fgmres", **CFG4_OPTS, precision=prec)
+            solver = api.create_linear_solver("fgmres", **cfg4_opts(prec))
             ctx.sync()
             t0 = time.perf_counter()
             solver.solve_batched(A, x, b, M, sys_elem)
@@ -856,14 +870,19 @@ def run_cfg4_leg(ctx, schedule):
     for prec, secs in modes.items():
         out[f"batched_{prec}"] = {"solves_per_s": n / secs, "seconds": secs, "mean_iterations": float(np.mean(iters[prec])),
                                   "max_iterations": int(max(iters[prec])), "max_true_rel_residual": worst[prec]}
+        if prec == "mixed_fp32":
+            out[f"batched_{prec}"]["mean_inner_iterations"] = float(np.mean(inner[prec]))
     sample_bytes = sum(box_matrix_bytes(d[0], d[1]) for d in sample)
     out["one_at_a_time_fp64_sample"] = {
         "systems": len(sample), "seconds": one["seconds"], "solves_per_s": len(sample) / one["seconds"],
         "matrix_bytes_fp64": int(sample_bytes), "mean_iterations": float(np.mean(one["iterations"])),
+        "batched_mixed_fp32_solves_per_s": len(sample) / sample_batched["mixed_fp32"],
         "batched_mixed_precon_fp32_solves_per_s": len(sample) / sample_batched["mixed_precon_fp32"],
         "batched_fp64_solves_per_s": len(sample) / sample_batched["fp64"],
+        "speedup_batched_mixed_fp32_vs_one_at_a_time_fp64": one["seconds"] / sample_batched["mixed_fp32"],
         "speedup_batched_mixed_vs_one_at_a_time_fp64": one["seconds"] / sample_batched["mixed_precon_fp32"],
         "note": "every 21st draw, solved one at a time and batched (the same systems)"}
+    out["speedup_batched_mixed_fp32_vs_batched_fp64"] = modes["fp64"] / modes["mixed_fp32"]
     out["speedup_batched_mixed_vs_batched_fp64"] = modes["fp64"] / modes["mixed_precon_fp32"]
     out["stream_shapes"] = {f"b<={k[0]}/{k[1]}": v for k, v in tuned.items()}
     return out

@@ -511,8 +511,9 @@ class FGMRES:
         out = []
         for s in range(ns):
             r = res[s]
-            out.append({"niter": r.niter, "nrestart": r.nrestart, "residual_norm": r.residual_norm,
-                        "res_estimate": r.res_estimate, "r0norm_initial": r.r0norm_initial, "seconds": r.seconds,
+            out.append({"niter": r.niter, "nrestart": r.nrestart, "inner_iters": r.inner_iters,
+                        "residual_norm": r.residual_norm, "res_estimate": r.res_estimate,
+                        "r0norm_initial": r.r0norm_initial, "seconds": r.seconds,
                         "hist": hist[s * hist_cap:s * hist_cap + r.nhist].copy()})
         return out
 

@@ -239,12 +239,14 @@ extern "C" int chidg_gpu_ctx_destroy(chidg_gpu_ctx* ctx) {
     release(ctx->mix_v32);
     release(ctx->mix_z32);
     release_batch_graphs(ctx);
-    for (Buffer* b : {&ctx->batch.cstart, &ctx->batch.csys, &ctx->batch.sys_chunk, &ctx->batch.sys_row, &ctx->batch.state,
-                      &ctx->batch.partial, &ctx->batch.rowsq, &ctx->batch.out})
-        release(*b);
-    for (cudaEvent_t& e : ctx->batch.ev)
-        if (e) cudaEventDestroy(e);
-    if (ctx->batch.h_count) cudaFreeHost(ctx->batch.h_count);
+    for (BatchBuffers* bb : {&ctx->batch, &ctx->batch_inner}) {
+        for (Buffer* b : {&bb->cstart, &bb->csys, &bb->sys_chunk, &bb->sys_row, &bb->row_sys, &bb->state, &bb->partial,
+                          &bb->rowsq, &bb->out})
+            release(*b);
+        for (cudaEvent_t& e : bb->ev)
+            if (e) cudaEventDestroy(e);
+        if (bb->h_count) cudaFreeHost(bb->h_count);
+    }
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);   // the frees above are ordered on this stream
     if (ctx->d_status) cudaFree(ctx->d_status);
     if (ctx->d_scal) cudaFree(ctx->d_scal);
@@ -748,9 +750,10 @@ int chidg::matvec_launch(chidg_gpu_matrix* A, const TA* val, const TV* x, TV* y,
             const int per_sm = resident_ctas((const void*)k, 32 * cw + 32, smem);
             if (per_sm < 1) return fail(ctx, CHIDG_GPU_EINVAL, "streamed matvec: shape does not fit an SM");
             const int grid = std::max(1, std::min(A->nrow, per_sm * ctx->nsm));
+            const RowMask mk = ctx->row_mask.nrow == A->nrow ? ctx->row_mask : RowMask{};
             k<<<grid, 32 * cw + 32, smem, ctx->stream>>>(R, A->nrow, val, x, y, z, alpha, beta, row_sq,
                                                          (int*)(ctx->d_scal + kSlotStatus), kSpinLimit, sh.nstage,
-                                                         sh.stage_bytes, A->max_row_cols);
+                                                         sh.stage_bytes, A->max_row_cols, mk);
             return CHIDG_GPU_OK;
         };
         int st2;
@@ -1980,8 +1983,11 @@ static int stream_launch(chidg_gpu_precon* M, const TL* LD, const TU* U, StreamT
     if (per_sm < 1) return fail(ctx, CHIDG_GPU_EINVAL, "streamed sweep: shape does not fit an SM");
     const int grid = per_sm * ctx->nsm;
     (void)variant;
+    // ILU0 and Jacobi: programme row r is matrix row r
+    const bool rows_match = (M->kind == CHIDG_PRECON_ILU0 || M->kind == CHIDG_PRECON_JACOBI) && M->P.nprow == ctx->row_mask.nrow;
+    const RowMask mk = rows_match ? ctx->row_mask : RowMask{};
     k<<<std::max(1, std::min(grid, ntask)), 32 * CW + 32, smem, ctx->stream>>>(M->P.rows, LD, U, Tk, ntask, v, zx, (ACC*)part,
-                                                                              S, sh.nstage, sh.stage_bytes, xcols, F);
+                                                                              S, sh.nstage, sh.stage_bytes, xcols, F, mk);
     return check_launch(ctx, MV ? "k_ilu_stream backward + matvec" : FWD ? "k_ilu_stream forward" : "k_ilu_stream backward");
 }
 

@@ -122,7 +122,7 @@ struct Workspace {
 // allocates nothing once they have grown; a pinned counter and two events
 // let the host read the active-system count without waiting
 struct BatchBuffers {
-    Buffer cstart, csys, sys_chunk, sys_row, state, partial, rowsq, out;
+    Buffer cstart, csys, sys_chunk, sys_row, row_sys, state, partial, rowsq, out;
     int32_t* h_count = nullptr;
     cudaEvent_t ev[2] = {nullptr, nullptr};
 };
@@ -146,7 +146,12 @@ struct chidg_gpu_ctx {
     chidg::Workspace ws64, ws32;
     chidg::Buffer mix_v32, mix_z32;   // mixed precision: FP32 copies of the outer loop's v and z
     chidg::BatchBuffers batch;
+    chidg::BatchBuffers batch_inner;  // the FP32 inner solves of a mixed-precision batched solve
     BatchGraphs* batch_graphs = nullptr;
+    BatchGraphs* batch_graphs_inner = nullptr;
+    // frozen systems' rows, skipped by the streamed kernels while a batched
+    // solve's Arnoldi step runs (empty otherwise)
+    chidg::RowMask row_mask;
     bool profiling = false;
     std::vector<chidg::EvPair> prof_pending;
     std::vector<cudaEvent_t> prof_pool;

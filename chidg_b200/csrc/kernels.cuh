@@ -1664,14 +1664,17 @@ __global__ void k_seg_lincomb(const int64_t* __restrict__ cstart, const int32_t*
         x[i] = from_d<T>(acc);
     }
 }
-// y = scale[sys] * x per chunk (in place allowed)
+// y = scale[sys] * x per chunk (in place allowed).  A scale of 0 (a system
+// that is inactive) writes zeros whatever x holds: the rows of a frozen
+// system are skipped by the streamed kernels, so its x may be stale, and its
+// next basis vector must stay 0 (a zero right-hand side for an inner solve).
 template <typename T>
 __global__ void k_seg_scale(const int64_t* __restrict__ cstart, const int32_t* __restrict__ csys, const T* x, T* y,
                             const double* __restrict__ scale) {
     const int c = blockIdx.x;
     const int64_t i0 = cstart[c], i1 = cstart[c + 1];
     const double a = scale[csys[c]];
-    for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) y[i] = from_d<T>(a * to_d(x[i]));
+    for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) y[i] = from_d<T>(a == 0.0 ? 0.0 : a * to_d(x[i]));
 }
 
 // ---------------------------------------------------------------------------

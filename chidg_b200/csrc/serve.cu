@@ -96,8 +96,6 @@ struct chidg_gpu_server {
 
 namespace {
 
-// device bytes one request needs: A, the factors (at most A), the Krylov
-// basis (V and Z) and a few vectors
 // Device bytes one request needs: its blocks (nval values), the ILU factors
 // (the values of its diagonal and lower blocks, nlow), their FP32 copies in a
 // mixed mode, the Krylov basis and a few vectors.  An estimate for admission:

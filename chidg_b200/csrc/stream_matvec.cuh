@@ -35,7 +35,7 @@ __global__ void __launch_bounds__(32 * CW + 32)
     k_matvec_stream(MatvecRows R, int nrow, const TA* __restrict__ val, const TX* __restrict__ x, TX* __restrict__ y,
                     const TX* __restrict__ z, double alpha, double beta, double* __restrict__ row_sumsq,
                     int* __restrict__ status, long long spin_limit, int nstage,
-                    int stage_bytes, int max_cols) {
+                    int stage_bytes, int max_cols, RowMask mask) {
     constexpr int NC = 32 * CW;
     constexpr int RPT = (SS_MAX_B + NC - 1) / NC;
     extern __shared__ __align__(128) unsigned char ss_smem[];
@@ -70,6 +70,17 @@ __global__ void __launch_bounds__(32 * CW + 32)
                 mbar_arrive(full + stage);
                 return;
             }
+            if (row_frozen(mask, row)) {
+                // a frozen system's row: one empty chunk, nothing read or written
+                if (!mbar_wait(empty + stage, phase ^ 1u, spin_limit)) atomicExch(status, 1);
+                StreamMeta m;
+                m.task = row; m.pr = row; m.q = 0; m.chunk = 0; m.nchunk = 1;
+                m.col0 = 0; m.ncols = 0; m.shift = 0; m.skip = 1;
+                meta[stage] = m;
+                mbar_arrive(full + stage);
+                if (++stage == nstage) { stage = 0; phase ^= 1u; }
+                continue;
+            }
             const int64_t k0 = R.row_ptr[row], k1 = R.row_ptr[row + 1];
             const int b = R.row_b[row];
             int cols = 0;
@@ -82,6 +93,7 @@ __global__ void __launch_bounds__(32 * CW + 32)
                 if (!mbar_wait(empty + stage, phase ^ 1u, spin_limit)) atomicExch(status, 1);
                 StreamMeta m;
                 m.task = row; m.pr = row; m.q = 0; m.chunk = ch; m.nchunk = nchunk;
+                m.skip = 0;
                 m.col0 = ch * kc;
                 m.ncols = cols > 0 ? min(kc, cols - ch * kc) : 0;
                 m.shift = 0;
@@ -113,6 +125,12 @@ __global__ void __launch_bounds__(32 * CW + 32)
         if (!mbar_wait(full + stage, phase, spin_limit)) { if (ctid == 0) atomicExch(status, 1); }
         const StreamMeta m = meta[stage];
         if (m.task < 0) break;
+        if (m.skip) {
+            __syncwarp();
+            if (lane == 0) mbar_arrive(empty + stage);
+            if (++stage == nstage) { stage = 0; phase ^= 1u; }
+            continue;
+        }
         if (m.chunk == 0) {
             row = m.pr;
             b = R.row_b[row];

@@ -48,7 +48,25 @@ struct StreamMeta {
     int chunk, nchunk;
     int col0, ncols;
     int shift;     // element offset of the chunk inside the stage
+    int skip;      // the row's system is frozen: nothing is read, computed or written
 };
+
+// Rows of frozen systems in a batched solve (a system whose Arnoldi process
+// has converged while the others go on): row r belongs to system row_sys[r],
+// frozen when active[row_sys[r]] == 0.  The streamed kernels skip such rows:
+// no block is copied, no wait is taken, nothing is written, so a step costs
+// what its active systems read.  The rows of a system depend only on rows of
+// the same system, and a frozen system's vectors are not read again before
+// its next restart, so skipping them changes no active system's values.
+// Empty (active == nullptr): every row runs.
+struct RowMask {
+    const int32_t* row_sys = nullptr;
+    const int32_t* active = nullptr;
+    int nrow = 0;              // rows the map covers
+};
+__device__ __forceinline__ bool row_frozen(const RowMask& mk, int row) {
+    return mk.active != nullptr && mk.active[mk.row_sys[row]] == 0;
+}
 
 struct StreamTasks {
     const int32_t* task_row;
@@ -219,7 +237,7 @@ template <typename TL, typename TU, typename TX, typename ACC, bool FORWARD, int
 __global__ void __launch_bounds__(32 * CW + 32)
     k_ilu_stream(IluRows R, const TL* __restrict__ LD, const TU* __restrict__ Aval, StreamTasks T, int ntasks,
                  const TX* __restrict__ v, TX* __restrict__ zx, ACC* __restrict__ part, SweepSync S, int nstage,
-                 int stage_bytes, int max_b, FusedMv<TA, TX> F) {
+                 int stage_bytes, int max_b, FusedMv<TA, TX> F, RowMask mask) {
     constexpr int NC = 32 * CW;                  // consumer threads
     static_assert(NC <= SS_MAX_NC, "row-sum scratch");
     static_assert(!(MV && FORWARD), "matvec rows run in the backward sweep");
@@ -259,6 +277,16 @@ __global__ void __launch_bounds__(32 * CW + 32)
                 return;
             }
             const int pr = T.task_row[t], q = T.task_ent[t];
+            if (row_frozen(mask, pr)) {
+                if (!mbar_wait(empty + stage, phase ^ 1u, S.spin_limit)) atomicExch(S.status, 1);
+                StreamMeta m;
+                m.task = (int)t; m.pr = pr; m.q = q; m.chunk = 0; m.nchunk = 1;
+                m.col0 = 0; m.ncols = 0; m.shift = 0; m.skip = 1;
+                meta[stage] = m;
+                mbar_arrive(full + stage);
+                if (++stage == nstage) { stage = 0; phase ^= 1u; }
+                continue;
+            }
             int b = R.prow_b[pr];
             const unsigned char* base = nullptr;
             int cols = 0, esz = 1;
@@ -283,6 +311,7 @@ __global__ void __launch_bounds__(32 * CW + 32)
                                 if (!mbar_wait(empty + stage, phase ^ 1u, S.spin_limit)) atomicExch(S.status, 1);
                                 StreamMeta m;
                                 m.task = (int)t; m.pr = pr; m.q = q; m.chunk = ch; m.nchunk = nchunk;
+                                m.skip = 0;
                                 m.col0 = c0;
                                 m.ncols = min(kc, col - c0);
                                 const uintptr_t src = reinterpret_cast<uintptr_t>(base + (size_t)c0 * b * esz);
@@ -319,6 +348,7 @@ __global__ void __launch_bounds__(32 * CW + 32)
                 if (!mbar_wait(empty + stage, phase ^ 1u, S.spin_limit)) atomicExch(S.status, 1);
                 StreamMeta m;
                 m.task = (int)t; m.pr = pr; m.q = q; m.chunk = ch; m.nchunk = nchunk;
+                m.skip = 0;
                 m.col0 = ch * kc;
                 m.ncols = cols > 0 ? min(kc, cols - ch * kc) : 0;
                 m.shift = 0;
@@ -350,6 +380,13 @@ __global__ void __launch_bounds__(32 * CW + 32)
         if (!mbar_wait(full + stage, phase, S.spin_limit)) { if (ctid == 0) atomicExch(S.status, 1); }
         const StreamMeta m = meta[stage];
         if (m.task < 0) break;
+        if (m.skip) {
+            // a frozen system's row: release the stage, nothing else
+            __syncwarp();
+            if (lane == 0) mbar_arrive(empty + stage);
+            if (++stage == nstage) { stage = 0; phase ^= 1u; }
+            continue;
+        }
         if (m.chunk == 0) {
             pr = m.pr;
             q = m.q;

@@ -334,9 +334,13 @@ int chidg_gpu_fgmres_solve(chidg_gpu_matrix* A, chidg_gpu_precon* M,
  * its own fgmres_t%solve Arnoldi process (dot products, re-orthogonalisation
  * test, Givens rotations, convergence, restarts) while each matvec, ILU sweep
  * and reduction is one launch for the whole batch.  results[s] and
- * hist[s * hist_cap ...] are per system.  FP64 Krylov vectors: precision
- * CHIDG_GPU_FP64 or CHIDG_GPU_MIXED_PRECON_FP32 (FP32 preconditioner
- * blocks); no inner FGMRES. */
+ * hist[s * hist_cap ...] are per system.  FP64 Krylov vectors for the outer
+ * solve in every precision: CHIDG_GPU_FP64; CHIDG_GPU_MIXED_PRECON_FP32
+ * (FP32 preconditioner blocks); CHIDG_GPU_MIXED_FP32 / _BF16 (each outer
+ * step preconditioned by a batched FP32 inner FGMRES with the mixed_inner_*
+ * options, FP32 or BF16 factors and copy of A; results[s].inner_iters
+ * counts system s's inner iterations).  No FP64 inner FGMRES
+ * (opts.inner_fgmres). */
 int chidg_gpu_fgmres_solve_batched(chidg_gpu_matrix* A, chidg_gpu_precon* M, int32_t nsys,
                                    const int32_t* sys_elem, const chidg_gpu_vector* b,
                                    chidg_gpu_vector* x, const chidg_gpu_fgmres_opts* opts,
