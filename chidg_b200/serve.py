@@ -56,6 +56,7 @@ class SolveResult:
     finish: float
     batch_size: int
     tag: object = None
+    inner_iters: int = 0          # FP32 inner-solve iterations (mixed_fp32 / mixed_bf16)
 
     @property
     def latency(self) -> float:
@@ -207,7 +208,7 @@ class Server:
             for s, (req, fut) in enumerate(batch):
                 xs = xh[eo[sys_elem[s]]:eo[sys_elem[s + 1]]].copy()
                 fut.set_result(SolveResult(xs, res[s]["niter"], res[s]["residual_norm"], res[s]["r0norm_initial"],
-                                           req.arrival, start, finish, len(batch), req.tag))
+                                           req.arrival, start, finish, len(batch), req.tag, res[s]["inner_iters"]))
             M.tear_down()
             for o in (x, b, A):
                 o.release()
@@ -329,7 +330,7 @@ class NativeFuture:
                 raise _lib.ChidgGpuError(st, "serve_wait")
             t0 = self.server._t0
             self._result = SolveResult(x, res.niter, res.residual_norm, res.r0norm_initial, t0 + timing[0],
-                                       t0 + timing[1], t0 + timing[2], int(timing[3]), self.req.tag)
+                                       t0 + timing[1], t0 + timing[2], int(timing[3]), self.req.tag, res.inner_iters)
         return self._result
 
 

@@ -172,3 +172,26 @@ def test_native_server_retries_a_system_alone_after_running_out_of_memory():
         srv.close()
     assert len(calls) == 2
     assert got.niter == ref.niter and np.array_equal(got.x, ref.x)
+
+
+def test_native_server_with_fp32_inner_solves():
+    """The native server in the FP32-inner-solve mode: every request reaches
+    the FP64 1e-8 residual, counts its inner iterations and agrees with its
+    FP64 oracle solve."""
+    reqs = make_requests()
+    srv = serve.NativeServer(slots=2, max_batch=3, **OPTS, precision="mixed_fp32", mixed_inner_nkrylov=10,
+                             mixed_inner_rtol=1e-2, mixed_inner_nmax=30)
+    try:
+        stats = serve.run_stream(srv, reqs, serve.poisson_arrivals(len(reqs), rate=200.0, seed=3))
+    finally:
+        srv.close()
+    got = {r.tag: r for r in stats["results"]}
+    for req in make_requests():
+        r = got[req.tag]
+        assert r.residual_norm <= 1.5e-8 * r.r0norm_initial, req.tag
+        assert r.inner_iters >= r.niter > 0, req.tag
+        Ao = O.OracleMatrix(req.pattern)
+        Ao.set_values(req.values)
+        xo, _ = O.fgmres(Ao, O.OraclePrecon(Ao, "ilu0"), req.rhs, O.default_opts(tol=0.0, rtol=1e-10, nkrylov=30,
+                                                                                  inner_fgmres=0, nmax=300))
+        assert np.linalg.norm(r.x - xo) <= 1e-6 * np.linalg.norm(xo), req.tag
