@@ -16,7 +16,7 @@
 // the caller.  Each call writes every partial it reads before reading it, so
 // nothing needs clearing between calls.  The first call on a device looks up
 // the array's device address (cudaGetSymbolAddress with that device
-// current); make that first call before any stream capture.
+// current, a synchronous query).
 #include "chidg_gpu_internal.cuh"
 
 #include <mutex>

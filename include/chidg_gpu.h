@@ -269,9 +269,9 @@ int chidg_gpu_vector_norm_fields(const chidg_gpu_vector* x, double* out, int32_t
  * default stream) and result is written asynchronously.  Partial sums live in
  * a fixed 128 KiB array inside this library on every GPU that loads it, so
  * n <= 67 108 864 (larger n returns CHIDG_GPU_EINVAL).  The first call on a
- * device looks up that array's device address; make it before any stream
- * capture.  All calls share the array: calls that overlap on the GPU race
- * and must be serialised by the caller. */
+ * device also looks up that array's device address (a synchronous query).
+ * All calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller. */
 int chidg_gpu_dot_noalloc(int device, const double* x, const double* y, int64_t n, double* result, void* stream);
 
 /* ---- chidg_mv (src/containers/operator_chidg_mv.f90:46-645) --------------- */
