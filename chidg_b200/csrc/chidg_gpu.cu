@@ -997,6 +997,16 @@ int find_trans(const chidg_gpu_matrix* A, int p, int t, int e) {
 
 }  // namespace
 
+// CHIDG_FACTOR_TILES=1: factor products of blocks above 144 rows on the FP64
+// tensor cores in 136 x 136 tiles instead of the SIMT tiled kernel
+static bool factor_tiles_env() {
+    static const bool v = [] {
+        const char* e = std::getenv("CHIDG_FACTOR_TILES");
+        return e && e[0] == '1';
+    }();
+    return v;
+}
+
 // ILU0 / Jacobi on a single rank: one programme row per matrix row.
 static int build_ilu0(const chidg_gpu_matrix* A, bool jacobi, IluProgram& P, std::string& err) {
     P = IluProgram();
@@ -1391,38 +1401,55 @@ static int finalize_program(chidg_gpu_ctx* ctx, const chidg_gpu_matrix* A, IluPr
             i = j;
         }
         P.inv_seg_ptr[l + 1] = (int)P.inv_seg.size();
-        // pass 0: products that fit one tensor-core CTA (<= 136 x 136 outputs),
-        // pass 1: the rest on the SIMT tiled kernel (measured faster than 136-wide
-        // tensor-core tiles for 320-row blocks: 29 against 32 ms per P3 10^3 box)
+        // pass 0: products on the FP64 tensor cores, one CTA per output block of
+        // up to 136 x 136 and, with CHIDG_FACTOR_TILES=1, one CTA per 136 x 136
+        // tile (r0, c0) of outputs of programmes whose blocks exceed 144 rows
+        // (the FP32 factorisation, which takes whole blocks up to 144, never
+        // sees a tile); pass 1: the larger outputs on the SIMT tiled kernel
+        // otherwise
+        const bool tiles = factor_tiles_env() && P.max_b > SF_MAX;
         for (int pass = 0; pass < 2; ++pass) {
             for (int i = P.fwd_ptr[l]; i < P.fwd_ptr[l + 1]; ++i) {
                 const int pr = P.fwd_rows[i];
                 const int b = P.prow_b[pr];
+                // the tasks of one output (b rows, n columns): whole, or cut
+                // into tiles of up to 136 x 136
+                auto add = [&](std::vector<GemmTask>& tasks, const GemmTask& t, int n, bool whole) {
+                    for (int r0 = 0; r0 < b; r0 += whole ? b : DM_MAX)
+                        for (int c0 = 0; c0 < n; c0 += whole ? n : DM_MAX) {
+                            GemmTask u = t;
+                            u.r0 = whole ? 0 : r0;
+                            u.c0 = whole ? 0 : c0;
+                            u.m = whole ? b : std::min(DM_MAX, b - r0);
+                            u.n = whole ? n : std::min(DM_MAX, n - c0);
+                            tasks.push_back(u);
+                        }
+                };
                 for (auto& en : P.lo[pr]) {
                     // L = A_lower * inv(D_parent)      (precon_ILU0.f90:231)
                     const bool small = b <= DM_MAX && en.nc <= DM_MAX;
-                    if (small != (pass == 0)) continue;
+                    if ((small || tiles) != (pass == 0)) continue;
                     GemmTask t{};
-                    t.c_off = en.l_off; t.cinit_off = -1; t.m = b; t.n = en.nc; t.ldm = b;
+                    t.c_off = en.l_off; t.cinit_off = -1; t.ldm = b;
                     t.q_begin = (int32_t)lpairs.size();
                     lpairs.push_back(GemmPair{en.a_off, P.dinv_off[en.parent], en.nc, 0});
                     t.q_end = (int32_t)lpairs.size();
                     t.elem = P.prow_elem[pr];
-                    ltasks.push_back(t);
+                    add(ltasks, t, en.nc, small || pass == 1);
                 }
                 // D = A_diag - sum L * A(parent, itranspose)   (:238-239);
                 // assembled rows get their D from k_assemble_rows instead
                 if (P.assembled) continue;
                 bool small = b <= DM_MAX;
                 for (auto& en : P.lo[pr]) small = small && en.nc <= DM_MAX;
-                if (small != (pass == 0)) continue;
+                if ((small || tiles) != (pass == 0)) continue;
                 GemmTask t{};
-                t.c_off = P.dinv_off[pr]; t.cinit_off = P.diagA_off[pr]; t.m = b; t.n = b; t.ldm = b;
+                t.c_off = P.dinv_off[pr]; t.cinit_off = P.diagA_off[pr]; t.ldm = b;
                 t.q_begin = (int32_t)spairs.size();
                 for (auto& en : P.lo[pr]) spairs.push_back(GemmPair{en.l_off, en.t_off, en.nc, 0});
                 t.q_end = (int32_t)spairs.size();
                 t.elem = P.prow_elem[pr];
-                stasks.push_back(t);
+                add(stasks, t, b, small || pass == 1);
             }
             if (pass == 0) {
                 P.ltask_dmma[l + 1] = (int)ltasks.size() - P.ltask_ptr[l];

@@ -510,13 +510,17 @@ __global__ void __launch_bounds__(256) k_task_gemm(const GemmTask* __restrict__ 
 }
 
 // FP64 tensor-core version of k_task_gemm for blocks up to 136 x 136: one CTA
-// computes a whole output block with mma.sync m8n8k4 (DMMA).  8 warps on a
-// 2 x 4 grid; warp (wm, wn) owns the 8x8 output tiles (wm + 2i, wn + 4j),
-// i < 9, j < 5 (45 accumulators, up to 255 registers a thread), so each A
-// fragment loaded from shared memory feeds five MMAs and each B fragment
-// nine.  K is staged 32 at a time through shared memory in the same k-major
-// layout for both operands, leading dimension 140 (= 12 mod 16 doubles: the
-// fragment loads of a half-warp hit 16 distinct bank pairs).
+// computes a whole output block on the FP64 tensor cores (DMMA).  8 warps on
+// a 2 x 4 grid.  The 17 row tiles of 8 are taken in pairs (rows 16p ..
+// 16p+15, p < 8) by mma.sync m16n8k8, warp row wm owning pairs wm + 2i
+// (i < 4), and the last tile (rows 128..135) by m8n8k4 in warp row 0; warp
+// column wn owns the column tiles wn + 4j (j < 5).  Per slice of K = 8 a
+// warp loads its five B fragments once and each pair's A fragment once: 20
+// m16n8k8 (and 10 m8n8k4 in warp row 0) per slice, a third of the
+// instructions of the same work in m8n8k4.  K is staged 32 at a time through
+// shared memory in the same k-major layout for both operands, leading
+// dimension 140 (= 12 mod 16 doubles: the fragment loads of a half-warp hit
+// 16 distinct bank pairs); past the operands' K the stage holds zeros.
 constexpr int DM_MAX = 136, DM_LD = 140, DM_KC = 32, DM_WM = 2, DM_WN = 4, DM_TI = 9, DM_TJ = 5;
 constexpr int DM_THREADS = 32 * DM_WM * DM_WN;
 constexpr size_t DM_SMEM = 4 * sizeof(double) * DM_KC * DM_LD;   // two stages of (A, B) panels
@@ -594,23 +598,38 @@ __global__ void __launch_bounds__(DM_THREADS, 1) k_task_gemm_dmma(const GemmTask
         const int kc = min(DM_KC, pairs[cq].k - ck0);
         const double* as = As + (c & 1) * 2 * DM_KC * DM_LD;
         const double* bs = as + DM_KC * DM_LD;
-        for (int k4 = 0; k4 < kc; k4 += 4) {
-            double af[DM_TI], bf[DM_TJ];
-            // tiles past the 17th (rows/columns >= 136) exist only in the
-            // warp grid: never read them
+        for (int k8 = 0; k8 < kc; k8 += 8) {
+            // slices past kc read the stage's zeros (rows kc..31)
+            const double* a_lo = as + (k8 + tq) * DM_LD + g;       // A(., k8 + t)
+            const double* a_hi = a_lo + 4 * DM_LD;                 // A(., k8 + t + 4)
+            double b0[DM_TJ], b1[DM_TJ];
             #pragma unroll
-            for (int i = 0; i < DM_TI; ++i)
-                af[i] = (wm + DM_WM * i < tm) ? as[(k4 + tq) * DM_LD + (wm + DM_WM * i) * 8 + g] : 0.0;
+            for (int j = 0; j < DM_TJ; ++j) {
+                // column tiles past the 17th exist only in the warp grid: never read them
+                const bool ok = wn + DM_WN * j < tn;
+                const int col = (wn + DM_WN * j) * 8 + g;
+                b0[j] = ok ? bs[(k8 + tq) * DM_LD + col] : 0.0;
+                b1[j] = ok ? bs[(k8 + tq + 4) * DM_LD + col] : 0.0;
+            }
             #pragma unroll
-            for (int j = 0; j < DM_TJ; ++j)
-                bf[j] = (wn + DM_WN * j < tn) ? bs[(k4 + tq) * DM_LD + (wn + DM_WN * j) * 8 + g] : 0.0;
-            #pragma unroll
-            for (int i = 0; i < DM_TI; ++i) {
-                if (wm + DM_WM * i >= tm) continue;
+            for (int i = 0; i < 4; ++i) {
+                const int p = wm + DM_WM * i;                      // rows 16p .. 16p + 15
+                if (2 * p >= tm) continue;
+                const double a0 = a_lo[16 * p], a1 = a_lo[16 * p + 8], a2 = a_hi[16 * p], a3 = a_hi[16 * p + 8];
                 #pragma unroll
                 for (int j = 0; j < DM_TJ; ++j) {
                     if (wn + DM_WN * j >= tn) continue;
-                    dmma_8x8x4(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+                    dmma_16x8x8(acc[2 * i][j][0], acc[2 * i][j][1], acc[2 * i + 1][j][0], acc[2 * i + 1][j][1], a0, a1,
+                                a2, a3, b0[j], b1[j]);
+                }
+            }
+            if (wm == 0 && tm > 16) {                               // rows 128 .. 135
+                const double a0 = a_lo[128], a1 = a_hi[128];
+                #pragma unroll
+                for (int j = 0; j < DM_TJ; ++j) {
+                    if (wn + DM_WN * j >= tn) continue;
+                    dmma_8x8x4(acc[8][j][0], acc[8][j][1], a0, b0[j]);
+                    dmma_8x8x4(acc[8][j][0], acc[8][j][1], a1, b1[j]);
                 }
             }
         }
@@ -618,9 +637,10 @@ __global__ void __launch_bounds__(DM_THREADS, 1) k_task_gemm_dmma(const GemmTask
         if (ck0 >= pairs[cq].k) { ++cq; ck0 = 0; }
         __syncthreads();                          // stage (c & 1) is refilled two chunks later
     }
+    // acc[2i + h]: rows 16 (wm + 2i) + 8h + g; acc[8] (warp row 0): rows 128 + g
     #pragma unroll
     for (int i = 0; i < DM_TI; ++i) {
-        const int row = (wm + DM_WM * i) * 8 + g;
+        const int row = (i < 8) ? 16 * (wm + DM_WM * (i >> 1)) + 8 * (i & 1) + g : (wm == 0 ? 128 + g : DM_MAX);
         if (row >= t.m) continue;
         #pragma unroll
         for (int j = 0; j < DM_TJ; ++j) {
@@ -1593,16 +1613,43 @@ template <typename T>
 __global__ void k_seg_mdot(const int64_t* __restrict__ cstart, int nchunk, const T* __restrict__ x,
                            const T* __restrict__ y, int64_t ystride, int nq, double* __restrict__ partial,
                            const int32_t* __restrict__ csys = nullptr, const int32_t* __restrict__ mask = nullptr) {
-    __shared__ double scratch[32];
+    // eight vectors per pass over the chunk of x, each sum formed in the
+    // order of a pass per vector (as k_mdot_partial)
+    constexpr int QG = 8;
+    __shared__ double scratch[QG][32];
     const int c = blockIdx.x;
     if (mask != nullptr && !mask[csys[c]]) return;     // system not in this pass: its partials are not read
     const int64_t i0 = cstart[c], i1 = cstart[c + 1];
-    for (int q = 0; q < nq; ++q) {
-        const T* yq = y + (int64_t)q * ystride;
-        double s = 0.0;
-        for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) s += to_d(x[i]) * to_d(yq[i]);
-        s = block_sum(s, scratch);
-        if (threadIdx.x == 0) partial[(int64_t)q * nchunk + c] = s;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int q0 = 0; q0 < nq; q0 += QG) {
+        const int qn = min(QG, nq - q0);
+        const T* yq = y + (int64_t)q0 * ystride;
+        double s[QG];
+        #pragma unroll
+        for (int k = 0; k < QG; ++k) s[k] = 0.0;
+        for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+            const double xi = to_d(x[i]);
+            #pragma unroll
+            for (int k = 0; k < QG; ++k)
+                if (k < qn) s[k] += xi * to_d(yq[(int64_t)k * ystride + i]);
+        }
+        #pragma unroll
+        for (int k = 0; k < QG; ++k) s[k] = warp_sum(s[k]);
+        __syncthreads();
+        if (lane == 0) {
+            #pragma unroll
+            for (int k = 0; k < QG; ++k) scratch[k][w] = s[k];
+        }
+        __syncthreads();
+        if (w == 0) {
+            const int nw = (blockDim.x + 31) >> 5;
+            #pragma unroll
+            for (int k = 0; k < QG; ++k) {
+                double t = (lane < nw) ? scratch[k][lane] : 0.0;
+                t = warp_sum(t);
+                if (lane == 0 && k < qn) partial[(int64_t)(q0 + k) * nchunk + c] = t;
+            }
+        }
     }
 }
 // out[s * ostride + q] = sum over the chunks [sys_chunk[s], sys_chunk[s+1]) of partial[q * nchunk + c]
