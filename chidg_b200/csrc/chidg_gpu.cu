@@ -1573,6 +1573,219 @@ extern "C" int chidg_gpu_precon_stamp(chidg_gpu_precon* M, int64_t* s) {
     return CHIDG_GPU_OK;
 }
 
+namespace chidg {
+// Blocks of 161..352 rows (P3 with five fields: 320): Gauss-Jordan with
+// partial pivoting, one row of the block per thread.  The pivot search, the
+// scaling and the elimination of a panel's columns then run in registers,
+// with one barrier a step (each warp posts its best candidate row and key in
+// a buffer of the step's parity; every warp then picks the winner), and
+// rows are never interchanged: as in the 136-row tensor-core kernel, the
+// pivot of column k is the entry of largest magnitude among the rows not yet
+// used as pivots (the first such row on ties), step k records its row p_k,
+// and the permutation is undone at the end.  Panels of RP_NB columns: after a
+// panel's steps, every other column c becomes c with rows {p_k} zeroed plus
+// P X_c, P the eliminated panel and X_c the old values of c in rows p_k (a
+// rank-RP_NB update on the FP64 tensor cores, m16n8k8 tiles).  The stored
+// matrix S then satisfies S(p_k, j) = inv(A)(k, p_j): the write-back permutes
+// each column's rows (a warp a column, through registers) and then the
+// columns along the cycles of the pivot order (a thread a row).  Dynamic
+// shared memory: 2 RP_NB max_b doubles (the panel and the pivot rows' values).
+constexpr int RP_NB = 32, RP_THREADS = 512, RP_MAX = 352;
+static __global__ void __launch_bounds__(RP_THREADS, 1)
+    k_block_inverse_rows(double* __restrict__ LD, const int64_t* __restrict__ dinv_off, const int32_t* __restrict__ prow_b,
+                         const int32_t* __restrict__ prow_elem, const int32_t* __restrict__ rows, int row_begin,
+                         int* __restrict__ status, int max_b) {
+    extern __shared__ double rp_smem[];
+    constexpr int NW = RP_THREADS / 32;
+    // per step (double-buffered by step parity): each warp's best candidate,
+    // its key and its row values
+    __shared__ double cand_row[2][NW][RP_NB];
+    __shared__ unsigned ck_hi[2][NW], ck_lo[2][NW];
+    __shared__ int ck_row[2][NW];
+    __shared__ int piv[RP_MAX], stepof[RP_MAX];
+    __shared__ unsigned char visited[RP_MAX];
+    const int prow = rows[row_begin + blockIdx.x];
+    const int b = prow_b[prow];
+    double* D = LD + dinv_off[prow];
+    double* Pn = rp_smem;                         // [RP_NB][max_b]: eliminated panel, column t at Pn[t * max_b]
+    double* X = Pn + (size_t)RP_NB * max_b;       // [RP_NB][max_b]: X[t * max_b + j] = old D(p_t, j)
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int i = tid;                            // this thread's row
+    const bool mine = i < b;
+    bool used = false, singular = false;
+    for (int q = tid; q < RP_MAX; q += RP_THREADS) { stepof[q] = -1; visited[q] = 0; }
+    __syncthreads();
+    for (int k0 = 0; k0 < b; k0 += RP_NB) {
+        const int nb = min(RP_NB, b - k0);
+        double r[RP_NB];
+#pragma unroll
+        for (int c = 0; c < RP_NB; ++c) r[c] = (mine && c < nb) ? D[i + (int64_t)(k0 + c) * b] : 0.0;
+#pragma unroll
+        for (int t = 0; t < RP_NB; ++t) {
+            if (t >= nb) break;
+            const int k = k0 + t;
+            // pivot: the largest |r[t]| among unused rows (integer keys: the
+            // bits of |v| are monotone in |v|, a NaN sorts above +inf; key + 1
+            // marks a candidate), first row on ties
+            const unsigned long long kb = (unsigned long long)__double_as_longlong(fabs(r[t]));
+            const unsigned long long key = (mine && !used) ? kb + 1ull : 0ull;
+            const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+            const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+            const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+            const unsigned cand = (hi == mhi && lo == mlo) ? (unsigned)i : 0xffffffffu;
+            const unsigned mrow = __reduce_min_sync(0xffffffffu, cand);
+            // the warp's candidate row and key, in this step's buffer; one
+            // barrier, then every warp picks the winner among the 16
+            const int buf = k & 1;
+            if ((unsigned)i == mrow) {
+#pragma unroll
+                for (int c = 0; c < RP_NB; ++c) cand_row[buf][w][c] = r[c];
+            }
+            if (lane == 0) { ck_hi[buf][w] = mhi; ck_lo[buf][w] = mlo; ck_row[buf][w] = (int)mrow; }
+            __syncthreads();
+            const unsigned qh = lane < NW ? ck_hi[buf][lane] : 0u, ql = lane < NW ? ck_lo[buf][lane] : 0u;
+            const unsigned qr = lane < NW ? (unsigned)ck_row[buf][lane] : 0xffffffffu;
+            const unsigned gh = __reduce_max_sync(0xffffffffu, qh);
+            const unsigned gl = __reduce_max_sync(0xffffffffu, qh == gh ? ql : 0u);
+            // b - k >= 1 unused rows: some key is nonzero and p is a row
+            const int p = (int)__reduce_min_sync(0xffffffffu, (qh == gh && ql == gl) ? qr : 0xffffffffu);
+            const double* prow_s = cand_row[buf][p >> 5];
+            if (i == p) {
+                used = true;
+                piv[k] = p;
+                stepof[p] = k;
+            }
+            double pv = prow_s[t];
+            if (pv == 0.0) { singular = true; pv = 1.0; }
+            const double rcp = 1.0 / pv;
+            if (i == p) {
+#pragma unroll
+                for (int c = 0; c < RP_NB; ++c) r[c] = (c == t) ? rcp : r[c] * rcp;
+            } else {
+                const double f = r[t];
+#pragma unroll
+                for (int c = 0; c < RP_NB; ++c) r[c] = (c == t) ? -f * rcp : r[c] - f * (prow_s[c] * rcp);
+            }
+        }
+        // the eliminated panel: back to its columns, and into shared memory;
+        // the old values of the panel's pivot rows in every other column
+        if (mine) {
+#pragma unroll
+            for (int c = 0; c < RP_NB; ++c)
+                if (c < nb) {
+                    D[i + (int64_t)(k0 + c) * b] = r[c];
+                    Pn[c * max_b + i] = r[c];
+                }
+        }
+        const int nout = b - nb;
+        for (int idx = tid; idx < nb * nout; idx += RP_THREADS) {
+            const int t = idx / nout, jj = idx - t * nout;
+            const int j = jj < k0 ? jj : jj + nb;
+            X[t * max_b + jj] = D[piv[k0 + t] + (int64_t)j * b];
+        }
+        __syncthreads();
+        // c <- c with rows {p_t} zeroed + P X_c for every column c outside the
+        // panel, on the FP64 tensor cores: a warp takes 16 x 8 output tiles
+        // (rows 16 tr.., outside-panel columns 8 tc..) with mma.sync m16n8k8
+        // over the panel's nb <= 32 steps, P and X read from shared memory
+        // (entries past b rows, nb steps or the outside columns read as 0)
+        {
+            const int g = lane >> 2, tq = lane & 3;
+            const int ntr = (b + 15) / 16, ntc = (nout + 7) / 8;
+            for (int tile = w; tile < ntr * ntc; tile += NW) {
+                const int r0 = 16 * (tile % ntr), jj0 = 8 * (tile / ntr);
+                double d[4];
+                int rowv[4], colv[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int row = r0 + g + 8 * (e >> 1), jj = jj0 + 2 * tq + (e & 1);
+                    rowv[e] = row;
+                    colv[e] = jj;
+                    double base = 0.0;
+                    if (row < b && jj < nout) {
+                        const int st = stepof[row];
+                        base = (st >= k0 && st < k0 + nb) ? 0.0 : D[row + (int64_t)(jj < k0 ? jj : jj + nb) * b];
+                    }
+                    d[e] = base;
+                }
+#pragma unroll
+                for (int k8 = 0; k8 < RP_NB; k8 += 8) {
+                    if (k8 >= nb) break;
+                    const int ka = k8 + tq, kb2 = k8 + tq + 4;
+                    const int ra = r0 + g, rb = r0 + g + 8, cj = jj0 + g;
+                    const double a0 = (ka < nb && ra < b) ? Pn[ka * max_b + ra] : 0.0;
+                    const double a1 = (ka < nb && rb < b) ? Pn[ka * max_b + rb] : 0.0;
+                    const double a2 = (kb2 < nb && ra < b) ? Pn[kb2 * max_b + ra] : 0.0;
+                    const double a3 = (kb2 < nb && rb < b) ? Pn[kb2 * max_b + rb] : 0.0;
+                    const double b0 = (ka < nb && cj < nout) ? X[ka * max_b + cj] : 0.0;
+                    const double b1 = (kb2 < nb && cj < nout) ? X[kb2 * max_b + cj] : 0.0;
+                    dmma_16x8x8(d[0], d[1], d[2], d[3], a0, a1, a2, a3, b0, b1);
+                }
+#pragma unroll
+                for (int e = 0; e < 4; ++e)
+                    if (rowv[e] < b && colv[e] < nout)
+                        D[rowv[e] + (int64_t)(colv[e] < k0 ? colv[e] : colv[e] + nb) * b] = d[e];
+            }
+        }
+        __syncthreads();
+    }
+    // the cycles of the pivot order, marked once: visited[j] = 2 where a
+    // cycle of length > 1 starts (its smallest column), 1 elsewhere
+    if (tid == 0)
+        for (int j0 = 0; j0 < b; ++j0) {
+            if (visited[j0]) continue;
+            int cur = j0, n = 0;                          // piv is a permutation: at most b hops
+            do { visited[cur] = 1; cur = piv[cur]; } while (cur != j0 && ++n < b);
+            if (piv[j0] != j0) visited[j0] = 2;
+        }
+    // rows: S(i, j) -> (stepof[i], j), a warp per column through registers
+    constexpr int RPL = (RP_MAX + 31) / 32;
+    for (int j = w; j < b; j += RP_THREADS / 32) {
+        double* col = D + (int64_t)j * b;
+        double v[RPL];
+#pragma unroll
+        for (int q = 0; q < RPL; ++q) {
+            const int row = lane + 32 * q;
+            v[q] = row < b ? col[row] : 0.0;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < RPL; ++q) {
+            const int row = lane + 32 * q;
+            if (row < b) col[stepof[row]] = v[q];
+        }
+    }
+    __syncthreads();
+    // columns: column j -> column piv[j], along the cycles of piv; thread i
+    // carries row i (every thread follows the same cycles)
+    for (int j0 = 0; j0 < b; ++j0) {
+        if (visited[j0] != 2) continue;
+        double carry = mine ? D[i + (int64_t)j0 * b] : 0.0;
+        int cur = j0, n = 0;
+        do {
+            const int dst = piv[cur];
+            if (mine) {
+                const double tmp = D[i + (int64_t)dst * b];
+                D[i + (int64_t)dst * b] = carry;
+                carry = tmp;
+            }
+            cur = dst;
+        } while (cur != j0 && ++n < b);
+    }
+    if (singular && tid == 0) atomicMin(status, prow_elem[prow]);
+}
+}  // namespace chidg
+
+// CHIDG_INVERSE_PANELS=1: blocks of 161..352 rows on the shared-memory panel
+// kernel instead of the row-per-thread kernel (comparison runs)
+static bool inverse_panels_env() {
+    static const bool v = [] {
+        const char* e = std::getenv("CHIDG_INVERSE_PANELS");
+        return e && e[0] == '1';
+    }();
+    return v;
+}
+
 static int launch_inverse(chidg_gpu_precon* M, int row_begin, int count, int cls) {
     chidg_gpu_ctx* ctx = M->ctx;
     IluProgram& P = M->P;
@@ -1608,7 +1821,15 @@ static int launch_inverse(chidg_gpu_precon* M, int row_begin, int count, int cls
                                                         row_begin, ctx->d_status, (int*)M->piv_scratch.ptr);
                 return CHIDG_GPU_OK;
             };
-            if (bmax <= 352) st = go(k_block_inverse_panels<32>, 32);
+            if (bmax <= RP_MAX && !inverse_panels_env()) {
+                // a row per thread, panels in registers (k_block_inverse_rows)
+                const size_t smem = sizeof(double) * 2 * RP_NB * (size_t)bmax;
+                if ((st = raise_smem_limit((const void*)k_block_inverse_rows, smem)))
+                    return fail(ctx, st, "row inverse shared memory");
+                k_block_inverse_rows<<<count, RP_THREADS, smem, ctx->stream>>>(
+                    LD, (const int64_t*)P.d_dinv_off.ptr, (const int32_t*)P.d_prow_b.ptr, (const int32_t*)P.d_prow_elem.ptr,
+                    (const int32_t*)P.d_fwd_rows.ptr, row_begin, ctx->d_status, bmax);
+            } else if (bmax <= 352) st = go(k_block_inverse_panels<32>, 32);
             else if (bmax <= 704) st = go(k_block_inverse_panels<16>, 16);
             else st = go(k_block_inverse_panels<8>, 8);
             if (st) return st;

@@ -182,6 +182,42 @@ def test_factor_tensor_core_inverse_sizes(nvars, P):
     assert worst < 1e-10
 
 
+@pytest.mark.parametrize("nvars", [3, 4, 5])
+def test_factor_row_inverse_sizes(nvars):
+    """Diagonal inverses of 192..320-row blocks (P3; Gauss-Jordan with a row
+    of the block per thread and panels in registers) and the L blocks built
+    from them, against the oracle's DGETRF/DGETRI and ILU0."""
+    pat, vals, Ao, Ag = setup((2, 2, 1), 3, seed=36, nvars=nvars)
+    Mo = O.OraclePrecon(Ao, "ilu0")
+    Mo.update()
+    Mg = api.create_preconditioner("ilu0")
+    Mg.update(Ag)
+    LDo, LDg = Mo.LD(), Mg.LD()
+    voff, _ = pat.value_offsets()
+    nr, nc = pat.block_dims()
+    worst = 0.0
+    for k in range(pat.nblocks):
+        a = LDo[voff[k]:voff[k] + nr[k] * nc[k]]
+        if np.any(a):
+            worst = max(worst, relerr(LDg[voff[k]:voff[k] + nr[k] * nc[k]], a))
+    assert worst < 1e-10
+
+
+def test_singular_block_reports_element_row_inverse():
+    pat, vals, Ao, Ag = setup((2, 2, 1), 3, seed=37)
+    voff, _ = pat.value_offsets()
+    nr, nc = pat.block_dims()
+    k = int(np.nonzero((pat.blk_row_elem == 2) & (pat.blk_col_elem == 2))[0][0])
+    bad = vals.copy()
+    blk = bad[voff[k]:voff[k] + nr[k] * nc[k]].reshape(nc[k], nr[k])
+    blk[:, 5] = 0.0                     # a zero row: singular
+    Ag.upload(bad)
+    M = api.create_preconditioner("jacobi")
+    with pytest.raises(_lib.ChidgGpuError) as ei:
+        M.update(Ag)
+    assert ei.value.code == _lib.ESINGULAR and ei.value.element == 2
+
+
 def test_singular_block_reports_element_tensor_core_inverse():
     pat, vals, Ao, Ag = setup((3, 2, 2), 2, seed=31)
     voff, _ = pat.value_offsets()
