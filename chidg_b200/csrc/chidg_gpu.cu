@@ -1599,7 +1599,7 @@ static __global__ void __launch_bounds__(RP_THREADS, 1)
     constexpr int NW = RP_THREADS / 32;
     // per step (double-buffered by step parity): each warp's best candidate,
     // its key and its row values
-    __shared__ double cand_row[2][NW][RP_NB];
+    __shared__ __align__(16) double cand_row[2][NW][RP_NB];
     __shared__ unsigned ck_hi[2][NW], ck_lo[2][NW];
     __shared__ int ck_row[2][NW];
     __shared__ int piv[RP_MAX], stepof[RP_MAX];
@@ -1639,7 +1639,8 @@ static __global__ void __launch_bounds__(RP_THREADS, 1)
             const int buf = k & 1;
             if ((unsigned)i == mrow) {
 #pragma unroll
-                for (int c = 0; c < RP_NB; ++c) cand_row[buf][w][c] = r[c];
+                for (int c = 0; c < RP_NB; c += 2)
+                    reinterpret_cast<double2*>(cand_row[buf][w])[c >> 1] = make_double2(r[c], r[c + 1]);
             }
             if (lane == 0) { ck_hi[buf][w] = mhi; ck_lo[buf][w] = mlo; ck_row[buf][w] = (int)mrow; }
             __syncthreads();
@@ -1664,7 +1665,11 @@ static __global__ void __launch_bounds__(RP_THREADS, 1)
             } else {
                 const double f = r[t];
 #pragma unroll
-                for (int c = 0; c < RP_NB; ++c) r[c] = (c == t) ? -f * rcp : r[c] - f * (prow_s[c] * rcp);
+                for (int c = 0; c < RP_NB; c += 2) {
+                    const double2 pr2 = reinterpret_cast<const double2*>(prow_s)[c >> 1];
+                    r[c] = (c == t) ? -f * rcp : r[c] - f * (pr2.x * rcp);
+                    r[c + 1] = (c + 1 == t) ? -f * rcp : r[c + 1] - f * (pr2.y * rcp);
+                }
             }
         }
         // the eliminated panel: back to its columns, and into shared memory;
@@ -1685,46 +1690,53 @@ static __global__ void __launch_bounds__(RP_THREADS, 1)
         }
         __syncthreads();
         // c <- c with rows {p_t} zeroed + P X_c for every column c outside the
-        // panel, on the FP64 tensor cores: a warp takes 16 x 8 output tiles
-        // (rows 16 tr.., outside-panel columns 8 tc..) with mma.sync m16n8k8
-        // over the panel's nb <= 32 steps, P and X read from shared memory
-        // (entries past b rows, nb steps or the outside columns read as 0)
+        // panel, on the FP64 tensor cores: a warp takes 16 x 16 output tiles
+        // (rows 16 tr.., outside-panel columns 16 tc..), two mma.sync m16n8k8
+        // per slice of 8 steps sharing the A fragment, P and X read from
+        // shared memory (entries past b rows, nb steps or the outside columns
+        // read as 0)
         {
             const int g = lane >> 2, tq = lane & 3;
-            const int ntr = (b + 15) / 16, ntc = (nout + 7) / 8;
+            const int ntr = (b + 15) / 16, ntc = (nout + 15) / 16;
             for (int tile = w; tile < ntr * ntc; tile += NW) {
-                const int r0 = 16 * (tile % ntr), jj0 = 8 * (tile / ntr);
-                double d[4];
-                int rowv[4], colv[4];
+                const int r0 = 16 * (tile % ntr), jj0 = 16 * (tile / ntr);
+                double d[2][4];
 #pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    const int row = r0 + g + 8 * (e >> 1), jj = jj0 + 2 * tq + (e & 1);
-                    rowv[e] = row;
-                    colv[e] = jj;
-                    double base = 0.0;
-                    if (row < b && jj < nout) {
-                        const int st = stepof[row];
-                        base = (st >= k0 && st < k0 + nb) ? 0.0 : D[row + (int64_t)(jj < k0 ? jj : jj + nb) * b];
+                for (int h = 0; h < 2; ++h)
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const int row = r0 + g + 8 * (e >> 1), jj = jj0 + 8 * h + 2 * tq + (e & 1);
+                        double base = 0.0;
+                        if (row < b && jj < nout) {
+                            const int st = stepof[row];
+                            base = (st >= k0 && st < k0 + nb) ? 0.0 : D[row + (int64_t)(jj < k0 ? jj : jj + nb) * b];
+                        }
+                        d[h][e] = base;
                     }
-                    d[e] = base;
-                }
 #pragma unroll
                 for (int k8 = 0; k8 < RP_NB; k8 += 8) {
                     if (k8 >= nb) break;
                     const int ka = k8 + tq, kb2 = k8 + tq + 4;
-                    const int ra = r0 + g, rb = r0 + g + 8, cj = jj0 + g;
+                    const int ra = r0 + g, rb = r0 + g + 8;
                     const double a0 = (ka < nb && ra < b) ? Pn[ka * max_b + ra] : 0.0;
                     const double a1 = (ka < nb && rb < b) ? Pn[ka * max_b + rb] : 0.0;
                     const double a2 = (kb2 < nb && ra < b) ? Pn[kb2 * max_b + ra] : 0.0;
                     const double a3 = (kb2 < nb && rb < b) ? Pn[kb2 * max_b + rb] : 0.0;
-                    const double b0 = (ka < nb && cj < nout) ? X[ka * max_b + cj] : 0.0;
-                    const double b1 = (kb2 < nb && cj < nout) ? X[kb2 * max_b + cj] : 0.0;
-                    dmma_16x8x8(d[0], d[1], d[2], d[3], a0, a1, a2, a3, b0, b1);
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int cj = jj0 + 8 * h + g;
+                        const double b0 = (ka < nb && cj < nout) ? X[ka * max_b + cj] : 0.0;
+                        const double b1 = (kb2 < nb && cj < nout) ? X[kb2 * max_b + cj] : 0.0;
+                        dmma_16x8x8(d[h][0], d[h][1], d[h][2], d[h][3], a0, a1, a2, a3, b0, b1);
+                    }
                 }
 #pragma unroll
-                for (int e = 0; e < 4; ++e)
-                    if (rowv[e] < b && colv[e] < nout)
-                        D[rowv[e] + (int64_t)(colv[e] < k0 ? colv[e] : colv[e] + nb) * b] = d[e];
+                for (int h = 0; h < 2; ++h)
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const int row = r0 + g + 8 * (e >> 1), jj = jj0 + 8 * h + 2 * tq + (e & 1);
+                        if (row < b && jj < nout) D[row + (int64_t)(jj < k0 ? jj : jj + nb) * b] = d[h][e];
+                    }
             }
         }
         __syncthreads();
