@@ -203,6 +203,36 @@ def test_factor_row_inverse_sizes(nvars):
     assert worst < 1e-10
 
 
+@pytest.mark.parametrize("P", [2, 3])
+def test_inverse_with_row_permuted_blocks(P):
+    """Diagonal blocks whose rows are shuffled, so that partial pivoting takes
+    off-diagonal pivots and the inverse kernels undo a long permutation
+    (135 rows: tensor-core kernel; 320 rows: row-per-thread kernel), against
+    the oracle's DGETRF/DGETRI (block Jacobi: the inverses alone)."""
+    pat, vals, Ao, Ag = setup((2, 2, 1), P, seed=38)
+    voff, _ = pat.value_offsets()
+    nr, nc = pat.block_dims()
+    rng = np.random.default_rng(39)
+    bad = vals.copy()
+    for k in range(pat.nblocks):
+        if pat.blk_row_elem[k] == pat.blk_col_elem[k]:
+            blk = bad[voff[k]:voff[k] + nr[k] * nc[k]].reshape(nc[k], nr[k])   # [column][row]
+            blk[:, :] = blk[:, rng.permutation(nr[k])]
+    Ao.set_values(bad)
+    Ag.upload(bad)
+    Mo = O.OraclePrecon(Ao, "jacobi")
+    Mo.update()
+    Mg = api.create_preconditioner("jacobi")
+    Mg.update(Ag)
+    LDo, LDg = Mo.LD(), Mg.LD()
+    worst = 0.0
+    for k in range(pat.nblocks):
+        a = LDo[voff[k]:voff[k] + nr[k] * nc[k]]
+        if np.any(a):
+            worst = max(worst, relerr(LDg[voff[k]:voff[k] + nr[k] * nc[k]], a))
+    assert worst < 1e-10
+
+
 def test_singular_block_reports_element_row_inverse():
     pat, vals, Ao, Ag = setup((2, 2, 1), 3, seed=37)
     voff, _ = pat.value_offsets()
