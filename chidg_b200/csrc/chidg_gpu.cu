@@ -1402,8 +1402,8 @@ static int finalize_program(chidg_gpu_ctx* ctx, const chidg_gpu_matrix* A, IluPr
         }
         P.inv_seg_ptr[l + 1] = (int)P.inv_seg.size();
         // pass 0: products on the FP64 tensor cores, one CTA per output block of
-        // up to 136 x 136 and, with CHIDG_FACTOR_TILES=1, one CTA per 136 x 136
-        // tile (r0, c0) of outputs of programmes whose blocks exceed 144 rows
+        // up to 136 x 136 and, with CHIDG_FACTOR_TILES=1, one CTA per tile
+        // (r0, c0) of outputs of programmes whose blocks exceed 144 rows
         // (the FP32 factorisation, which takes whole blocks up to 144, never
         // sees a tile); pass 1: the larger outputs on the SIMT tiled kernel
         // otherwise
@@ -1413,15 +1413,21 @@ static int finalize_program(chidg_gpu_ctx* ctx, const chidg_gpu_matrix* A, IluPr
                 const int pr = P.fwd_rows[i];
                 const int b = P.prow_b[pr];
                 // the tasks of one output (b rows, n columns): whole, or cut
-                // into tiles of up to 136 x 136
+                // into balanced tiles of at most 136 x 136 (a multiple of 8
+                // rows and columns each, but the last)
+                auto span = [](int len) {
+                    const int parts = (len + DM_MAX - 1) / DM_MAX;
+                    return std::min(DM_MAX, ((len + parts - 1) / parts + 7) / 8 * 8);
+                };
                 auto add = [&](std::vector<GemmTask>& tasks, const GemmTask& t, int n, bool whole) {
-                    for (int r0 = 0; r0 < b; r0 += whole ? b : DM_MAX)
-                        for (int c0 = 0; c0 < n; c0 += whole ? n : DM_MAX) {
+                    const int tm = whole ? b : span(b), tn = whole ? n : span(n);
+                    for (int r0 = 0; r0 < b; r0 += tm)
+                        for (int c0 = 0; c0 < n; c0 += tn) {
                             GemmTask u = t;
-                            u.r0 = whole ? 0 : r0;
-                            u.c0 = whole ? 0 : c0;
-                            u.m = whole ? b : std::min(DM_MAX, b - r0);
-                            u.n = whole ? n : std::min(DM_MAX, n - c0);
+                            u.r0 = r0;
+                            u.c0 = c0;
+                            u.m = std::min(tm, b - r0);
+                            u.n = std::min(tn, n - c0);
                             tasks.push_back(u);
                         }
                 };
