@@ -1899,11 +1899,20 @@ static int factor_fp32(chidg_gpu_precon* M, chidg_gpu_matrix* A, int precision) 
     float* L32 = (float*)M->LD32.ptr;
     double* LD = (double*)M->LD.ptr;
     const int ph = prof_begin(ctx, kProfFactor);
+    // products of blocks above 136 rows (the tasks after the first
+    // ltask_dmma / stask_dmma of a level): the SIMT tiled kernel in FP32
+    const int tiles_1d = (P.max_b + GT_M - 1) / GT_M;
     for (int l = 0; l < nlev; ++l) {
         const int pg = prof_begin(ctx, kProfFactorGemm);
-        const int nl = P.ltask_ptr[l + 1] - P.ltask_ptr[l];
+        const int nl_all = P.ltask_ptr[l + 1] - P.ltask_ptr[l], nl = P.ltask_dmma[l + 1];
+        const int ns_all = P.stask_ptr[l + 1] - P.stask_ptr[l];
         const GemmTask* lt = (const GemmTask*)P.d_ltasks.ptr + P.ltask_ptr[l];
         const GemmTask* stt = (const GemmTask*)P.d_stasks.ptr + P.stask_ptr[l];
+        if (nl_all > nl) {
+            k_task_gemm<float, float, float, float><<<(nl_all - nl) * tiles_1d * tiles_1d, 256, 0, ctx->stream>>>(
+                lt + nl, (const GemmPair*)P.d_lpairs.ptr, tiles_1d, tiles_1d, A32, L32, nullptr, L32, 1.0);
+            if ((st = check_launch(ctx, "factor L products (FP32, large blocks)"))) return st;
+        }
         if (nl > 0) {
             if (kern == 2)
                 k_task_gemm_f32<float><<<nl, 256, SF_SMEM, ctx->stream>>>(lt, (const GemmPair*)P.d_lpairs.ptr, A32, L32,
@@ -1916,7 +1925,12 @@ static int factor_fp32(chidg_gpu_precon* M, chidg_gpu_matrix* A, int precision) 
                     lt, 2 * nl, (const GemmPair*)P.d_lpairs.ptr, A32, L32, nullptr, L32, 1.0, wstat, kSpinLimit);
             if ((st = check_launch(ctx, "factor L products (FP32 / TF32)"))) return st;
         }
-        const int ns = P.stask_ptr[l + 1] - P.stask_ptr[l];
+        const int ns = P.stask_dmma[l + 1];
+        if (ns_all > ns) {
+            k_task_gemm<float, float, double, float><<<(ns_all - ns) * tiles_1d * tiles_1d, 256, 0, ctx->stream>>>(
+                stt + ns, (const GemmPair*)P.d_spairs.ptr, tiles_1d, tiles_1d, L32, A32, (const double*)A->val.ptr, LD, -1.0);
+            if ((st = check_launch(ctx, "factor S products (FP32, large blocks)"))) return st;
+        }
         if (ns > 0) {
             if (kern == 2)
                 k_task_gemm_f32<double><<<ns, 256, SF_SMEM, ctx->stream>>>(stt, (const GemmPair*)P.d_spairs.ptr, L32, A32,
@@ -1980,7 +1994,8 @@ extern "C" int chidg_gpu_precon_update(chidg_gpu_precon* M, chidg_gpu_matrix* A,
     // error would otherwise leave them out of step)
     if (M->sync.ptr)
         cudaMemsetAsync((unsigned*)M->sync.ptr + 2 + P.nprow, 0, sizeof(unsigned) * 3 * (size_t)P.nprow, ctx->stream);
-    if ((precision == CHIDG_GPU_MIXED_FP32 || precision == CHIDG_GPU_MIXED_BF16) && P.max_b <= SF_MAX && !P.assembled) {
+    if ((precision == CHIDG_GPU_MIXED_FP32 || precision == CHIDG_GPU_MIXED_BF16) && !P.assembled &&
+        (P.max_b <= SF_MAX || !factor_tiles_env())) {
         // the inner solves only read FP32 / BF16 factors: compute them in FP32
         if ((st = factor_fp32(M, A, precision))) return st;
         cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);

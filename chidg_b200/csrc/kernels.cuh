@@ -438,28 +438,29 @@ struct GemmPair {
     int32_t pad;
 };
 
-// Tiled FP64 SIMT GEMM over a list of tasks.  64x64 output tile per CTA,
-// 256 threads each accumulating a 4x4 register tile, K staged 16 at a time.
-// All operands column-major with leading dimension = their row count.
+// Tiled SIMT GEMM over a list of tasks.  64x64 output tile per CTA, 256
+// threads each accumulating a 4x4 register tile, K staged 16 at a time, in
+// TS (FP64; FP32 for the FP32 factors of the mixed modes).  All operands
+// column-major with leading dimension = their row count.
 constexpr int GT_M = 64, GT_N = 64, GT_K = 16;
-template <typename TA, typename TB, typename TC>
+template <typename TA, typename TB, typename TC, typename TS = double>
 __global__ void __launch_bounds__(256) k_task_gemm(const GemmTask* __restrict__ tasks, const GemmPair* __restrict__ pairs,
                                                    int tiles_m, int tiles_n,
                                                    const TA* Abase, const TB* Bbase,
                                                    const double* Cinit, TC* Cbase, double sgn) {
-    __shared__ double As[GT_K][GT_M + 1];
-    __shared__ double Bs[GT_K][GT_N + 1];
+    __shared__ TS As[GT_K][GT_M + 1];
+    __shared__ TS Bs[GT_K][GT_N + 1];
     const int tiles = tiles_m * tiles_n;
     const GemmTask t = tasks[blockIdx.x / tiles];
     const int tile = blockIdx.x % tiles;
     const int i0 = (tile % tiles_m) * GT_M, j0 = (tile / tiles_m) * GT_N;
     if (i0 >= t.m || j0 >= t.n) return;
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    double acc[4][4];
+    TS acc[4][4];
     #pragma unroll
     for (int a = 0; a < 4; ++a)
         #pragma unroll
-        for (int c = 0; c < 4; ++c) acc[a][c] = 0.0;
+        for (int c = 0; c < 4; ++c) acc[a][c] = TS(0);
     for (int q = t.q_begin; q < t.q_end; ++q) {
         const GemmPair pr = pairs[q];
         const TA* A = Abase + pr.a_off;   // m x k
@@ -469,18 +470,18 @@ __global__ void __launch_bounds__(256) k_task_gemm(const GemmTask* __restrict__ 
             for (int idx = threadIdx.x; idx < GT_M * GT_K; idx += 256) {
                 const int ii = idx % GT_M, kk = idx / GT_M;
                 const int gi = i0 + ii, gk = k0 + kk;
-                As[kk][ii] = (gi < t.m && gk < pr.k) ? to_d(A[gi + (int64_t)gk * t.m]) : 0.0;
+                As[kk][ii] = (gi < t.m && gk < pr.k) ? cvt<TS>(A[gi + (int64_t)gk * t.m]) : TS(0);
             }
             // B tile: 16 k x 64 cols
             for (int idx = threadIdx.x; idx < GT_K * GT_N; idx += 256) {
                 const int kk = idx % GT_K, jj = idx / GT_K;
                 const int gk = k0 + kk, gj = j0 + jj;
-                Bs[kk][jj] = (gk < pr.k && gj < t.n) ? to_d(B[gk + (int64_t)gj * pr.k]) : 0.0;
+                Bs[kk][jj] = (gk < pr.k && gj < t.n) ? cvt<TS>(B[gk + (int64_t)gj * pr.k]) : TS(0);
             }
             __syncthreads();
             #pragma unroll
             for (int kk = 0; kk < GT_K; ++kk) {
-                double av[4], bv[4];
+                TS av[4], bv[4];
                 #pragma unroll
                 for (int a = 0; a < 4; ++a) av[a] = As[kk][tx + 16 * a];
                 #pragma unroll
@@ -502,7 +503,7 @@ __global__ void __launch_bounds__(256) k_task_gemm(const GemmTask* __restrict__ 
             const int gi = i0 + tx + 16 * a;
             if (gi >= t.m) continue;
             const int64_t o = gi + (int64_t)gj * t.m;
-            double v = sgn * acc[a][c];
+            double v = sgn * (double)acc[a][c];
             if (t.cinit_off >= 0) v = Cinit[t.cinit_off + o] + v;
             Cbase[t.c_off + o] = from_d<TC>(v);
         }

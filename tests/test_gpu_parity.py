@@ -148,9 +148,13 @@ def test_stream_sweeps_deterministic():
     assert relerr(M.apply(Ag, v).download(), z1) < 1e-13
 
 
-@pytest.mark.parametrize("precision", ["mixed_fp32", "mixed_bf16", "mixed_precon_fp32"])
-def test_stream_sweeps_mixed_precision(precision):
-    pat, vals, Ao, Ag = setup((4, 4, 4), 2, seed=28)
+@pytest.mark.parametrize("precision,P", [("mixed_fp32", 2), ("mixed_bf16", 2), ("mixed_precon_fp32", 2),
+                                         ("mixed_fp32", 3), ("mixed_bf16", 3)])
+def test_stream_sweeps_mixed_precision(precision, P):
+    """Every mixed mode reaches the FP64 residual target; with P3 (320-row
+    blocks) the FP32 factorisation takes the large blocks' products on the
+    FP32 SIMT kernel."""
+    pat, vals, Ao, Ag = setup((4, 4, 4) if P == 2 else (3, 2, 2), P, seed=28)
     b = mesh.synth_vector(Ao.n, seed=29)
     solver = api.create_linear_solver("fgmres", tol=0.0, rtol=1e-8, nkrylov=10, inner_fgmres=0, nmax=50,
                                       precision=precision, mixed_inner_nkrylov=20, mixed_inner_rtol=1e-2,
